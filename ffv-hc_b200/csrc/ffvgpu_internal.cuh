@@ -1,0 +1,113 @@
+// ffvgpu_internal.cuh -- device functions shared by the FP64 kernels:
+// guide-cell values of the in-kernel block-to-block exchange.
+#pragma once
+#include "ffvgpu_layout.h"
+
+namespace ffvgpu {
+
+// ---------------------------------------------------------------------------
+// Guide-cell values (the exchange), one cell at a time.
+// ---------------------------------------------------------------------------
+
+// sup_get_intp_index (src/CGMfuncs/sup.f90:1-16), 1-based i in [1, 2n].
+__device__ __forceinline__ void intp_index(int i, int n, int& ic, double& r) {
+  ic = i / 2;
+  r = 0.25 + 0.5 * (double)(i % 2);
+  if (i < 2) {
+    ic = 1;
+    r = -0.25;
+  } else if (i > 2 * n - 1) {
+    ic = n - 1;
+    r = 1.25;
+  }
+}
+
+__device__ __forceinline__ double ld(const double* __restrict__ x, int blk, int i, int j, int k) {
+  return __ldg(x + (size_t)blk * BLOCK_CELLS + sidx(i, j, k));
+}
+
+// Value of guide cell (layer L = 1 or 2) of face 'face' of block 'blk' at
+// transverse position (a, b) in [0,16)^2, computed from interior values of x.
+__device__ __noinline__ double guide_value(const double* __restrict__ x, int blk, int face,
+                                           int a, int b, int L, const FaceNbr& nb,
+                                           const BCSet& bc, double dx) {
+  const int axis = face >> 1;
+  const bool plus = face & 1;
+  // 0-based coordinates of the guide cell in this block's frame
+  int g[3];
+  if (axis == 0) { g[1] = a; g[2] = b; } else if (axis == 1) { g[0] = a; g[2] = b; } else { g[0] = a; g[1] = b; }
+  g[axis] = plus ? (15 + L) : (-L);
+  switch (nb.kind) {
+    case NB_SAME: {
+      int s[3] = {g[0], g[1], g[2]};
+      s[axis] = plus ? (L - 1) : (16 - L);
+      return ld(x, nb.id[0], s[0], s[1], s[2]);
+    }
+    case NB_COARSE: {
+      // sup_copy_from_neighbor_c2f (sup.f90:54-120) with the windows of
+      // Scalar3DUpdater1::copyFromNeighborC2F (Scalar3DUpdater1.cpp:245-347):
+      // 1-based fine positions inside the coarse block, in [1, 32].
+      int f[3];
+      const int ta = (axis == 0) ? 1 : 0, tb = (axis == 2) ? 1 : 2;
+      f[ta] = g[ta] + 1 + 16 * nb.so_u;
+      f[tb] = g[tb] + 1 + 16 * nb.so_v;
+      f[axis] = plus ? L : (33 - L);
+      int i1, j1, k1;
+      double r, s, t;
+      intp_index(f[0], 16, i1, r);
+      intp_index(f[1], 16, j1, s);
+      intp_index(f[2], 16, k1, t);
+      const int c = nb.id[0];
+      --i1; --j1; --k1;  // to 0-based interior indices
+      const double nnn = ld(x, c, i1, j1, k1);
+      const double pnn = ld(x, c, i1 + 1, j1, k1);
+      const double npn = ld(x, c, i1, j1 + 1, k1);
+      const double nnp = ld(x, c, i1, j1, k1 + 1);
+      const double npp = ld(x, c, i1, j1 + 1, k1 + 1);
+      const double pnp = ld(x, c, i1 + 1, j1, k1 + 1);
+      const double ppn = ld(x, c, i1 + 1, j1 + 1, k1);
+      const double ppp = ld(x, c, i1 + 1, j1 + 1, k1 + 1);
+      return (1.0 - t) * ((1.0 - s) * ((1.0 - r) * nnn + r * pnn) +
+                          s * ((1.0 - r) * npn + r * ppn)) +
+             t * ((1.0 - s) * ((1.0 - r) * nnp + r * pnp) +
+                  s * ((1.0 - r) * npp + r * ppp));
+    }
+    case NB_FINE: {
+      // sup_copy_from_neighbor_f2c (sup.f90:122-179) with the windows of
+      // Scalar3DUpdater1::copyFromNeighborF2C (Scalar3DUpdater1.cpp:430-520).
+      const int ta = (axis == 0) ? 1 : 0, tb = (axis == 2) ? 1 : 2;
+      const int qu = g[ta] >> 3, qv = g[tb] >> 3;
+      const int fb = nb.id[qu + 2 * qv];
+      int lo[3];
+      lo[ta] = 2 * (g[ta] & 7);
+      lo[tb] = 2 * (g[tb] & 7);
+      lo[axis] = plus ? (2 * L - 2) : (16 - 2 * L);
+      const int i1 = lo[0], j1 = lo[1], k1 = lo[2];
+      const double nnn = ld(x, fb, i1, j1, k1);
+      const double pnn = ld(x, fb, i1 + 1, j1, k1);
+      const double npn = ld(x, fb, i1, j1 + 1, k1);
+      const double nnp = ld(x, fb, i1, j1, k1 + 1);
+      const double npp = ld(x, fb, i1, j1 + 1, k1 + 1);
+      const double pnp = ld(x, fb, i1 + 1, j1, k1 + 1);
+      const double ppn = ld(x, fb, i1 + 1, j1 + 1, k1);
+      const double ppp = ld(x, fb, i1 + 1, j1 + 1, k1 + 1);
+      return 0.125 * (nnn + pnn + npn + nnp + npp + pnp + ppn + ppp);
+    }
+    default: {
+      // bcx.f90: bc_x?_d (5-147) / bc_x?_n (294-436) on the outer face
+      int s[3] = {g[0], g[1], g[2]};
+      s[axis] = plus ? 15 : 0;
+      const double x0 = ld(x, blk, s[0], s[1], s[2]);
+      const int type = bc.type[face];
+      if (type == BC_DIRICHLET) {
+        const double xc = bc.value[face];
+        return (L == 1) ? (2.0 * xc - x0) : xc;
+      }
+      const double xc = bc.value[face] * dx;
+      if (plus) return (L == 1) ? (x0 + xc) : (x0 + xc * 2.0);
+      return (L == 1) ? (x0 - xc) : (x0 - xc * 2.0);
+    }
+  }
+}
+
+}  // namespace ffvgpu

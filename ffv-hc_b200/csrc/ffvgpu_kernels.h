@@ -1,0 +1,53 @@
+// ffvgpu_kernels.h -- host-side launchers of the FP64 kernels.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ffvgpu_layout.h"
+
+namespace ffvgpu {
+
+
+// Parameters every block kernel needs: neighbour table, cell sizes and the
+// outer BCs of the field being staged.
+struct KCtx {
+  const FaceNbr* nbr;  // [nb][6]
+  const double* dx;    // [nb]
+  BCSet bc;
+  int nb;
+};
+
+void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
+                 double* xout, const double* A, const double* b, const double* gst,
+                 double omega, double* partials, SolveState* st, int fin, int iter);
+void launch_jacobi(cudaStream_t s, const KCtx& C, bool from_zero, bool dot, const double* xin,
+                   double* xout, const double* A, const double* b, double omega,
+                   double* partials, SolveState* st);
+void launch_calc_r(cudaStream_t s, const KCtx& C, const double* x, const double* gst,
+                   const double* A, const double* b, double* r, SolveState* st);
+void launch_p_update(cudaStream_t s, const KCtx& C, const double* z, double* p, int first,
+                     SolveState* st);
+void launch_ax_dot(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
+                   double* partials, SolveState* st);
+void launch_cg_update(cudaStream_t s, const KCtx& C, double* x, const double* p, double* r,
+                      const double* q, double* partials, SolveState* st, int iter);
+void launch_dot(cudaStream_t s, const KCtx& C, const double* x, const double* y,
+                double* partials, SolveState* st, int fin, int iter);
+void launch_exchange(cudaStream_t s, const KCtx& C, const double* x, double* g);
+void launch_pack(cudaStream_t s, int nb, const double* stage, int vc, double* dst, size_t stride,
+                 double* gdst);
+void launch_pack_flag(cudaStream_t s, int nb, const int32_t* stage, int vc, uint8_t* flags,
+                      int bit, int mode);
+void launch_unpack_flag(cudaStream_t s, int nb, const uint8_t* flags, int vc, int32_t* stage,
+                        int bit);
+void launch_unpack(cudaStream_t s, const KCtx& C, const double* src, size_t stride, int vc,
+                   int with_guides, double* stage);
+void launch_assemble(cudaStream_t s, const KCtx& C, const double* ux, const double* uy,
+                     const double* uz, const double* gux, const double* guy, const double* guz,
+                     const double* cut, const uint8_t* flags, double* A, double* b,
+                     double* vface, double rhof, double dt, size_t field_stride);
+void launch_fold_bc(cudaStream_t s, const KCtx& C, double* A, double* b);
+void launch_fill(cudaStream_t s, int nb, double* x, size_t stride, double* g, double value);
+
+}  // namespace ffvgpu

@@ -1,0 +1,725 @@
+// kernels_fp64.cu -- FP64 kernels of the pressure-Poisson path (sm_100a).
+//
+// Compiled with --fmad=false: every product and sum is rounded separately,
+// and every expression keeps the reference's left-to-right order, so a
+// kernel's per-cell results equal the reference's bit for bit
+// (src/CGMfuncs/bils.f90, blas.f90, sup.f90, bcx.f90, bca.f90 and
+// src/FFV/bcut.f90, all built by the reference without FMA contraction).
+//
+// One CTA of 256 threads owns one 16^3 leaf block.  Stencil kernels stage
+// the block's vector in shared memory as an 18^3 tile whose guide layer is
+// computed from the neighbours' interiors (the exchange) or, on the first
+// use of a field, read from its stored guide layer.  Sums use a fixed tree:
+// per thread two serial sums over its 8 cells of each colour, an xor
+// butterfly over the warp, a serial sum over the 8 warps, and across blocks
+// the same shape over the per-block partials, run by the CTA that finishes
+// last (ticket counter), which also advances the solver state.
+#include <cfloat>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "ffvgpu_internal.cuh"
+#include "ffvgpu_kernels.h"
+
+namespace ffvgpu {
+
+constexpr int TW = 18;          // tile edge (16 + 2 guide cells)
+constexpr int TP = TW * TW;     // tile plane
+constexpr int TILE = TW * TW * TW;
+
+__device__ __forceinline__ int tix(int i, int j, int k) {  // 0-based interior coords
+  return (i + 1) + TW * (j + 1) + TP * (k + 1);
+}
+
+__device__ __forceinline__ bool solve_done(const SolveState* st) {
+  return *((volatile const int32_t*)&st->done) != 0;
+}
+
+// Guide-cell position of face f at transverse (a, b), layer 1.
+__device__ __forceinline__ int guide_tix(int f, int a, int b) {
+  switch (f) {
+    case X_M: return tix(-1, a, b);
+    case X_P: return tix(16, a, b);
+    case Y_M: return tix(a, -1, b);
+    case Y_P: return tix(a, 16, b);
+    case Z_M: return tix(a, b, -1);
+    default:  return tix(a, b, 16);
+  }
+}
+
+// Stage block 'blk' of x in the shared tile, guide layer included.
+__device__ __forceinline__ void stage_tile(double* __restrict__ xs, const double* __restrict__ x,
+                                           int blk, const KCtx& C, const double* __restrict__ gst) {
+  const int tid = threadIdx.x;
+  const double* xb = x + (size_t)blk * BLOCK_CELLS;
+#pragma unroll 4
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;
+    int i, j, k;
+    cell_of(s, i, j, k);
+    xs[tix(i, j, k)] = __ldg(xb + s);
+  }
+  const int a = tid & 15, b = tid >> 4;
+  for (int f = 0; f < 6; ++f) {
+    double v;
+    if (gst) {
+      v = __ldg(gst + ((size_t)blk * 6 + f) * FACE_CELLS + b * 16 + a);
+    } else {
+      const FaceNbr nb = C.nbr[blk * 6 + f];
+      v = guide_value(x, blk, f, a, b, 1, nb, C.bc, C.dx[blk]);
+    }
+    xs[guide_tix(f, a, b)] = v;
+  }
+}
+
+// FFVILS.h:24-47 IsConverged residual
+__device__ __forceinline__ double resid_of(double rr, double bb) {
+  return (fabs(bb) > (double)FLT_MIN) ? sqrt(fabs(rr) / fabs(bb)) : sqrt(fabs(rr));
+}
+
+__device__ void finalize(SolveState* st, double total, int fin, int iter) {
+  switch (fin) {
+    case FIN_STORE:
+      st->rr = total;
+      break;
+    case FIN_BB:
+      st->bb = total;
+      break;
+    case FIN_RBGS:
+    case FIN_CG_RR: {
+      const double res = resid_of(total, st->bb);
+      st->rr = total;
+      st->residual = res;
+      if (st->hist) st->hist[iter - 1] = res;
+      st->count = iter;
+      if (res <= st->eps) {
+        st->done = 1;
+      } else if (isnan(res) || isinf(res)) {
+        st->done = 1;
+        st->status = 2;
+      } else if (iter >= st->count_max) {
+        st->done = 1;
+        st->count = st->count_max + 1;  // loop variable after the last pass
+      } else if (fin == FIN_CG_RR) {
+        st->rr0 = st->rr1;
+      }
+      break;
+    }
+    case FIN_CG_RR1:
+      st->rr1 = total;
+      if (fabs(total) < (double)FLT_MIN) {  // FFVILS.h:720-724
+        st->residual = total;
+        st->count = 0;
+        st->done = 1;
+      } else {
+        st->beta = total / st->rr0;
+      }
+      break;
+    case FIN_CG_QP:
+      st->qp = total;
+      st->alpha = st->rr1 / total;
+      break;
+  }
+}
+
+// Canonical block reduction + last-CTA cross-block reduction + finaliser.
+__device__ void reduce_finalize(double v, double* __restrict__ partials, SolveState* st,
+                                int fin, int iter) {
+  __shared__ double ws[8];
+  __shared__ int amlast;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((tid & 31) == 0) ws[tid >> 5] = v;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) s += ws[w];
+    __stcg(partials + blockIdx.x, s);
+    __threadfence();
+    const unsigned t = atomicAdd(&st->ticket, 1u);
+    amlast = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!amlast) return;
+  __threadfence();
+  double S = 0.0;
+  for (int b = tid; b < (int)gridDim.x; b += THREADS) S += __ldcg(partials + b);
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) S += __shfl_xor_sync(0xffffffffu, S, off);
+  __syncthreads();
+  if ((tid & 31) == 0) ws[tid >> 5] = S;
+  __syncthreads();
+  if (tid == 0) {
+    double total = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) total += ws[w];
+    finalize(st, total, fin, iter);
+    st->ticket = 0;
+    __threadfence();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// RBGS: fused "residual of x_in" + "red-black sweep x_in -> x_out".
+// FFVILS.h:104-162 (RBGS_Smoother -> rbgs_smoother, bils.f90:57-108) and
+// FFVILS.h:247-296 (CalcR2 -> calc_r2, bils.f90:256-304).  Both colours'
+// residuals are formed from x_in before any update; colour 0 is then
+// updated, and colour 1 is updated against the new colour-0 values, as the
+// reference's serial colour-0-then-colour-1 loop does within a block.
+// ---------------------------------------------------------------------------
+template <bool DO_RES, bool DO_SWEEP>
+__global__ void __launch_bounds__(THREADS, 3)
+rbgs_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
+            const double* __restrict__ A, const double* __restrict__ bvec,
+            const double* __restrict__ gst, double omega, double* __restrict__ partials,
+            SolveState* st, int fin, int iter) {
+  if (solve_done(st)) return;
+  __shared__ double xs[TILE];
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  stage_tile(xs, xin, blk, C, gst);
+  __syncthreads();
+  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+  const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
+  double acc0 = 0.0, acc1 = 0.0;
+  double xn0[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const int q = tid + THREADS * m;
+    {
+      int i, j, k;
+      cell_of(q, i, j, k);
+      const int t = tix(i, j, k);
+      const double ap = __ldg(Ab + q), aw = __ldg(Ab + 4096 + q), ae = __ldg(Ab + 8192 + q);
+      const double as = __ldg(Ab + 12288 + q), an = __ldg(Ab + 16384 + q);
+      const double ab = __ldg(Ab + 20480 + q), at = __ldg(Ab + 24576 + q);
+      const double rs = __ldg(bb + q) - aw * xs[t - 1] - ae * xs[t + 1] - as * xs[t - TW] -
+                        an * xs[t + TW] - ab * xs[t - TP] - at * xs[t + TP];
+      const double xp = xs[t];
+      if (DO_RES) {
+        const double r = rs - ap * xp;
+        acc0 += r * r;
+      }
+      if (DO_SWEEP) {
+        const double xt = rs / ap;
+        xn0[m] = xp - omega * (xp - xt);
+      }
+    }
+    if (DO_RES) {
+      const int s = HALF_CELLS + q;
+      int i, j, k;
+      cell_of(s, i, j, k);
+      const int t = tix(i, j, k);
+      const double r = __ldg(bb + s) - __ldg(Ab + 4096 + s) * xs[t - 1] -
+                       __ldg(Ab + 8192 + s) * xs[t + 1] - __ldg(Ab + 12288 + s) * xs[t - TW] -
+                       __ldg(Ab + 16384 + s) * xs[t + TW] - __ldg(Ab + 20480 + s) * xs[t - TP] -
+                       __ldg(Ab + 24576 + s) * xs[t + TP] - __ldg(Ab + s) * xs[t];
+      acc1 += r * r;
+    }
+  }
+  if (DO_SWEEP) {
+    double* xo = xout + (size_t)blk * BLOCK_CELLS;
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int q = tid + THREADS * m;
+      int i, j, k;
+      cell_of(q, i, j, k);
+      xs[tix(i, j, k)] = xn0[m];
+      xo[q] = xn0[m];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int m = 0; m < 8; ++m) {
+      const int s = HALF_CELLS + tid + THREADS * m;
+      int i, j, k;
+      cell_of(s, i, j, k);
+      const int t = tix(i, j, k);
+      const double rs = __ldg(bb + s) - __ldg(Ab + 4096 + s) * xs[t - 1] -
+                        __ldg(Ab + 8192 + s) * xs[t + 1] - __ldg(Ab + 12288 + s) * xs[t - TW] -
+                        __ldg(Ab + 16384 + s) * xs[t + TW] - __ldg(Ab + 20480 + s) * xs[t - TP] -
+                        __ldg(Ab + 24576 + s) * xs[t + TP];
+      const double xp = xs[t];
+      const double xt = rs / __ldg(Ab + s);
+      xo[s] = xp - omega * (xp - xt);
+    }
+  }
+  if (DO_RES) reduce_finalize(acc0 + acc1, partials, st, fin, iter);
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi smoother (bils.f90:5-55) with b = bvec.  FROM_ZERO: x0 is the
+// zero field of FFVILS::Fill(z, 0) (blas.f90:5-33, guides included).
+// DOT: also forms b.x1 (FFVILS.h:712-718 DOT(r, z), r = bvec).
+// ---------------------------------------------------------------------------
+template <bool FROM_ZERO, bool DOT>
+__global__ void __launch_bounds__(THREADS, 3)
+jacobi_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
+              const double* __restrict__ A, const double* __restrict__ bvec, double omega,
+              double* __restrict__ partials, SolveState* st) {
+  if (solve_done(st)) return;
+  __shared__ double xs[FROM_ZERO ? 1 : TILE];
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  if (!FROM_ZERO) {
+    stage_tile(xs, xin, blk, C, nullptr);
+    __syncthreads();
+  }
+  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+  const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
+  double* xo = xout + (size_t)blk * BLOCK_CELLS;
+  double acc[2] = {0.0, 0.0};
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll 4
+    for (int m = 0; m < 8; ++m) {
+      const int s = c * HALF_CELLS + tid + THREADS * m;
+      double xw, xe, xS, xn, xb, xt, xp;
+      if (FROM_ZERO) {
+        xw = xe = xS = xn = xb = xt = xp = 0.0;
+      } else {
+        int i, j, k;
+        cell_of(s, i, j, k);
+        const int t = tix(i, j, k);
+        xw = xs[t - 1]; xe = xs[t + 1]; xS = xs[t - TW]; xn = xs[t + TW];
+        xb = xs[t - TP]; xt = xs[t + TP]; xp = xs[t];
+      }
+      const double bv = __ldg(bb + s);
+      const double r = bv - __ldg(Ab + 4096 + s) * xw - __ldg(Ab + 8192 + s) * xe -
+                       __ldg(Ab + 12288 + s) * xS - __ldg(Ab + 16384 + s) * xn -
+                       __ldg(Ab + 20480 + s) * xb - __ldg(Ab + 24576 + s) * xt;
+      const double x_tmp = r / __ldg(Ab + s);
+      const double x1 = xp - omega * (xp - x_tmp);
+      xo[s] = x1;
+      if (DOT) acc[c] += bv * x1;
+    }
+  }
+  if (DOT) reduce_finalize(acc[0] + acc[1], partials, st, FIN_CG_RR1, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Element-wise and stencil helpers of FFVILS::CG.
+// ---------------------------------------------------------------------------
+
+// r = b - A x (calc_r, bils.f90:208-254); x guides from 'gst' when given.
+__global__ void __launch_bounds__(THREADS, 3)
+calc_r_kernel(KCtx C, const double* __restrict__ x, const double* __restrict__ gst,
+              const double* __restrict__ A, const double* __restrict__ bvec,
+              double* __restrict__ rout, SolveState* st) {
+  if (st && solve_done(st)) return;
+  __shared__ double xs[TILE];
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  stage_tile(xs, x, blk, C, gst);
+  __syncthreads();
+  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+  const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
+  double* ro = rout + (size_t)blk * BLOCK_CELLS;
+#pragma unroll 4
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;
+    int i, j, k;
+    cell_of(s, i, j, k);
+    const int t = tix(i, j, k);
+    ro[s] = __ldg(bb + s) - __ldg(Ab + 4096 + s) * xs[t - 1] - __ldg(Ab + 8192 + s) * xs[t + 1] -
+            __ldg(Ab + 12288 + s) * xs[t - TW] - __ldg(Ab + 16384 + s) * xs[t + TW] -
+            __ldg(Ab + 20480 + s) * xs[t - TP] - __ldg(Ab + 24576 + s) * xs[t + TP] -
+            __ldg(Ab + s) * xs[t];
+  }
+}
+
+// p = z (first iteration, copy) or p = z + beta*p (xpay, blas.f90:363-395).
+__global__ void __launch_bounds__(THREADS)
+p_update_kernel(const double* __restrict__ z, double* __restrict__ p, int first, SolveState* st) {
+  if (solve_done(st)) return;
+  const double beta = st->beta;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+#pragma unroll 4
+  for (int m = 0; m < 16; ++m) {
+    const size_t s = base + threadIdx.x + THREADS * m;
+    p[s] = first ? z[s] : (z[s] + beta * p[s]);
+  }
+}
+
+// q = A p (calc_ax, bils.f90:162-206) and q.p (FFVILS.h:750-756 DOT(q, p)).
+__global__ void __launch_bounds__(THREADS, 3)
+ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A,
+              double* __restrict__ q, double* __restrict__ partials, SolveState* st) {
+  if (solve_done(st)) return;
+  __shared__ double xs[TILE];
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  stage_tile(xs, p, blk, C, nullptr);
+  __syncthreads();
+  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+  double* qo = q + (size_t)blk * BLOCK_CELLS;
+  double acc[2] = {0.0, 0.0};
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll 4
+    for (int m = 0; m < 8; ++m) {
+      const int s = c * HALF_CELLS + tid + THREADS * m;
+      int i, j, k;
+      cell_of(s, i, j, k);
+      const int t = tix(i, j, k);
+      const double v = __ldg(Ab + 4096 + s) * xs[t - 1] + __ldg(Ab + 8192 + s) * xs[t + 1] +
+                       __ldg(Ab + 12288 + s) * xs[t - TW] + __ldg(Ab + 16384 + s) * xs[t + TW] +
+                       __ldg(Ab + 20480 + s) * xs[t - TP] + __ldg(Ab + 24576 + s) * xs[t + TP] +
+                       __ldg(Ab + s) * xs[t];
+      qo[s] = v;
+      acc[c] += v * xs[t];
+    }
+  }
+  reduce_finalize(acc[0] + acc[1], partials, st, FIN_CG_QP, 0);
+}
+
+// x = x + alpha p; r = r + (-alpha) q (axpy, blas.f90:329-361); r.r.
+__global__ void __launch_bounds__(THREADS)
+cg_update_kernel(double* __restrict__ x, const double* __restrict__ p, double* __restrict__ r,
+                 const double* __restrict__ q, double* __restrict__ partials, SolveState* st,
+                 int iter) {
+  if (solve_done(st)) return;
+  const double alpha = st->alpha, malpha = -alpha;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+  double acc[2] = {0.0, 0.0};
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll 4
+    for (int m = 0; m < 8; ++m) {
+      const size_t s = base + c * HALF_CELLS + threadIdx.x + THREADS * m;
+      x[s] = x[s] + alpha * p[s];
+      const double rn = r[s] + malpha * q[s];
+      r[s] = rn;
+      acc[c] += rn * rn;
+    }
+  }
+  reduce_finalize(acc[0] + acc[1], partials, st, FIN_CG_RR, iter);
+}
+
+// x.y over interior cells (dot, blas.f90:466-499) with a finaliser.
+__global__ void __launch_bounds__(THREADS)
+dot_kernel(const double* __restrict__ x, const double* __restrict__ y,
+           double* __restrict__ partials, SolveState* st, int fin, int iter) {
+  if (solve_done(st)) return;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+  double acc[2] = {0.0, 0.0};
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll 4
+    for (int m = 0; m < 8; ++m) {
+      const size_t s = base + c * HALF_CELLS + threadIdx.x + THREADS * m;
+      acc[c] += __ldg(x + s) * __ldg(y + s);
+    }
+  }
+  reduce_finalize(acc[0] + acc[1], partials, st, fin, iter);
+}
+
+// ---------------------------------------------------------------------------
+// Exchange into a stored guide layer, layout conversion and set-up kernels.
+// ---------------------------------------------------------------------------
+
+// Writes layer-1 guide values of every face of every block into g.
+__global__ void __launch_bounds__(THREADS)
+exchange_kernel(KCtx C, const double* __restrict__ x, double* __restrict__ g) {
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  const int a = tid & 15, b = tid >> 4;
+  for (int f = 0; f < 6; ++f) {
+    const FaceNbr nb = C.nbr[blk * 6 + f];
+    g[((size_t)blk * 6 + f) * FACE_CELLS + b * 16 + a] =
+        guide_value(x, blk, f, a, b, 1, nb, C.bc, C.dx[blk]);
+  }
+}
+
+// Host layout block (n+2vc)^3 -> colour-split interior (+ layer-1 guides).
+__global__ void __launch_bounds__(THREADS)
+pack_kernel(const double* __restrict__ stage, int vc, double* __restrict__ dst, size_t stride,
+            double* __restrict__ gdst) {
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  const int w = 16 + 2 * vc;
+  const double* sb = stage + (size_t)blk * w * w * w;
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;
+    int i, j, k;
+    cell_of(s, i, j, k);
+    dst[(size_t)blk * stride + s] = sb[(i + vc) + w * ((j + vc) + w * (k + vc))];
+  }
+  if (gdst) {
+    const int a = tid & 15, b = tid >> 4;
+    for (int f = 0; f < 6; ++f) {
+      int g[3];
+      const int axis = f >> 1;
+      if (axis == 0) { g[1] = a; g[2] = b; } else if (axis == 1) { g[0] = a; g[2] = b; } else { g[0] = a; g[1] = b; }
+      g[axis] = (f & 1) ? 16 : -1;
+      gdst[((size_t)blk * 6 + f) * FACE_CELLS + b * 16 + a] =
+          sb[(g[0] + vc) + w * ((g[1] + vc) + w * (g[2] + vc))];
+    }
+  }
+}
+
+// Integer host field -> bit 'bit' of the per-cell flag byte.
+// mode 0: bit set where value != 0 (cut ids); mode 1: bit set where value == 1 (fluid).
+__global__ void __launch_bounds__(THREADS)
+pack_flag_kernel(const int32_t* __restrict__ stage, int vc, uint8_t* __restrict__ flags, int bit,
+                 int mode) {
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  const int w = 16 + 2 * vc;
+  const int32_t* sb = stage + (size_t)blk * w * w * w;
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;
+    int i, j, k;
+    cell_of(s, i, j, k);
+    const int32_t v = sb[(i + vc) + w * ((j + vc) + w * (k + vc))];
+    const bool on = mode ? (v == 1) : (v != 0);
+    uint8_t& f = flags[(size_t)blk * BLOCK_CELLS + s];
+    f = on ? (uint8_t)(f | (1u << bit)) : (uint8_t)(f & ~(1u << bit));
+  }
+}
+
+// Flag byte -> integer host field (inverse of pack_flag_kernel).
+__global__ void __launch_bounds__(THREADS)
+unpack_flag_kernel(const uint8_t* __restrict__ flags, int vc, int32_t* __restrict__ stage, int bit) {
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  const int w = 16 + 2 * vc;
+  int32_t* sb = stage + (size_t)blk * w * w * w;
+  for (int m = tid; m < w * w * w; m += THREADS) sb[m] = 0;
+  __syncthreads();
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;
+    int i, j, k;
+    cell_of(s, i, j, k);
+    sb[(i + vc) + w * ((j + vc) + w * (k + vc))] = (flags[(size_t)blk * BLOCK_CELLS + s] >> bit) & 1;
+  }
+}
+
+// Colour-split interior -> host layout, with vc guide layers per face
+// computed as the reference's exchange + outer BC would (layers 1..vc).
+__global__ void __launch_bounds__(THREADS)
+unpack_kernel(KCtx C, const double* __restrict__ src, size_t stride, int vc, int with_guides,
+              double* __restrict__ stage) {
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  const int w = 16 + 2 * vc;
+  double* sb = stage + (size_t)blk * w * w * w;
+  for (int m = tid; m < w * w * w; m += THREADS) sb[m] = 0.0;
+  __syncthreads();
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;
+    int i, j, k;
+    cell_of(s, i, j, k);
+    sb[(i + vc) + w * ((j + vc) + w * (k + vc))] = src[(size_t)blk * stride + s];
+  }
+  if (!with_guides) return;
+  const int a = tid & 15, b = tid >> 4;
+  for (int f = 0; f < 6; ++f) {
+    const FaceNbr nb = C.nbr[blk * 6 + f];
+    const int axis = f >> 1;
+    for (int L = 1; L <= vc; ++L) {
+      int g[3];
+      if (axis == 0) { g[1] = a; g[2] = b; } else if (axis == 1) { g[0] = a; g[2] = b; } else { g[0] = a; g[1] = b; }
+      g[axis] = (f & 1) ? (15 + L) : (-L);
+      sb[(g[0] + vc) + w * ((g[1] + vc) + w * (g[2] + vc))] =
+          guide_value(src, blk, f, a, b, L, nb, C.bc, C.dx[blk]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// bcut_calc_ab_p (src/FFV/bcut.f90:608-832), one cell per thread-iteration.
+// u guide values come from the stored guide layers of UX/UY/UZ.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double u_at(const double* __restrict__ u, const double* __restrict__ gu,
+                                       int blk, int i, int j, int k) {
+  int f = -1, a = 0, b = 0;
+  if (i < 0) { f = X_M; a = j; b = k; } else if (i > 15) { f = X_P; a = j; b = k; }
+  else if (j < 0) { f = Y_M; a = i; b = k; } else if (j > 15) { f = Y_P; a = i; b = k; }
+  else if (k < 0) { f = Z_M; a = i; b = j; } else if (k > 15) { f = Z_P; a = i; b = j; }
+  if (f < 0) return __ldg(u + (size_t)blk * BLOCK_CELLS + sidx(i, j, k));
+  return __ldg(gu + ((size_t)blk * 6 + f) * FACE_CELLS + b * 16 + a);
+}
+
+__global__ void __launch_bounds__(THREADS)
+assemble_kernel(KCtx C, const double* __restrict__ ux, const double* __restrict__ uy,
+                const double* __restrict__ uz, const double* __restrict__ gux,
+                const double* __restrict__ guy, const double* __restrict__ guz,
+                const double* __restrict__ cut /* [6][nb*4096] */,
+                const uint8_t* __restrict__ flags, double* __restrict__ A,
+                double* __restrict__ bvec, double* __restrict__ vface /* [6][nb*4096] or null */,
+                double rhof, double dt, size_t field_stride) {
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  const double dx = C.dx[blk];
+  double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;
+    int i, j, k;
+    cell_of(s, i, j, k);
+    const size_t gs = (size_t)blk * BLOCK_CELLS + s;
+    double r0 = 1.0 / rhof, r1 = 1.0 / rhof, r2 = 1.0 / rhof;
+    double r3 = 1.0 / rhof, r4 = 1.0 / rhof, r5 = 1.0 / rhof;
+    const double uxp = __ldg(ux + gs), uyp = __ldg(uy + gs), uzp = __ldg(uz + gs);
+    double vx0 = 0.5 * (uxp + u_at(ux, gux, blk, i - 1, j, k));
+    double vx1 = 0.5 * (uxp + u_at(ux, gux, blk, i + 1, j, k));
+    double vy2 = 0.5 * (uyp + u_at(uy, guy, blk, i, j - 1, k));
+    double vy3 = 0.5 * (uyp + u_at(uy, guy, blk, i, j + 1, k));
+    double vz4 = 0.5 * (uzp + u_at(uz, guz, blk, i, j, k - 1));
+    double vz5 = 0.5 * (uzp + u_at(uz, guz, blk, i, j, k + 1));
+    const double d0 = __ldg(cut + gs), d1 = __ldg(cut + field_stride + gs);
+    const double d2 = __ldg(cut + 2 * field_stride + gs), d3 = __ldg(cut + 3 * field_stride + gs);
+    const double d4 = __ldg(cut + 4 * field_stride + gs), d5 = __ldg(cut + 5 * field_stride + gs);
+    const unsigned fl = flags[gs];
+    const bool c0 = fl & 1, c1 = fl & 2, c2 = fl & 4, c3 = fl & 8, c4 = fl & 16, c5 = fl & 32;
+    const bool fluid = fl & 128;
+    if (c0) { r0 = 0.0; vx0 = vx1 * (d0 - 0.5) / (d0 + 0.5); r1 = (1.0 / rhof) / (d0 + 0.5); }
+    if (c1) { r1 = 0.0; vx1 = vx0 * (d1 - 0.5) / (d1 + 0.5); r0 = (1.0 / rhof) / (d1 + 0.5); }
+    if (c2) { r2 = 0.0; vy2 = vy3 * (d2 - 0.5) / (d2 + 0.5); r3 = (1.0 / rhof) / (d2 + 0.5); }
+    if (c3) { r3 = 0.0; vy3 = vy2 * (d3 - 0.5) / (d3 + 0.5); r2 = (1.0 / rhof) / (d3 + 0.5); }
+    if (c4) { r4 = 0.0; vz4 = vz5 * (d4 - 0.5) / (d4 + 0.5); r5 = (1.0 / rhof) / (d4 + 0.5); }
+    if (c5) { r5 = 0.0; vz5 = vz4 * (d5 - 0.5) / (d5 + 0.5); r4 = (1.0 / rhof) / (d5 + 0.5); }
+    if (c0 && c1) { r0 = 0.0; r1 = 0.0; vx0 = 0.0; vx1 = 0.0; }
+    if (c2 && c3) { r2 = 0.0; r3 = 0.0; vy2 = 0.0; vy3 = 0.0; }
+    if (c4 && c5) { r4 = 0.0; r5 = 0.0; vz4 = 0.0; vz5 = 0.0; }
+    const double l0 = r0 / (dx * dx), l1 = r1 / (dx * dx), l2 = r2 / (dx * dx);
+    const double l3 = r3 / (dx * dx), l4 = r4 / (dx * dx), l5 = r5 / (dx * dx);
+    const double divv = (vx1 - vx0 + vy3 - vy2 + vz5 - vz4) / dx;
+    double ap = -(l0 + l1) - (l2 + l3) - (l4 + l5);
+    double aw = l0, ae = l1, as = l2, an = l3, ab = l4, at = l5;
+    double bv = divv / dt;
+    if (!fluid) {
+      ap = -6.0; aw = ae = as = an = ab = at = 1.0; bv = 0.0;
+      vx0 = vx1 = vy2 = vy3 = vz4 = vz5 = 0.0;
+    }
+    Ab[s] = ap; Ab[4096 + s] = aw; Ab[8192 + s] = ae; Ab[12288 + s] = as;
+    Ab[16384 + s] = an; Ab[20480 + s] = ab; Ab[24576 + s] = at;
+    bvec[gs] = bv;
+    if (vface) {
+      vface[gs] = vx0; vface[field_stride + gs] = vx1; vface[2 * field_stride + gs] = vy2;
+      vface[3 * field_stride + gs] = vy3; vface[4 * field_stride + gs] = vz4;
+      vface[5 * field_stride + gs] = vz5;
+    }
+  }
+}
+
+// Outer-BC folding (bca.f90:5-388) in the order w, e, s, n, b, t
+// (BlockScalar3D.h:183-190) for every cell on an outer face.
+__global__ void __launch_bounds__(THREADS)
+fold_bc_kernel(KCtx C, double* __restrict__ A, double* __restrict__ bvec) {
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  const double dx = C.dx[blk];
+  int outer = 0;
+  for (int f = 0; f < 6; ++f)
+    if (C.nbr[blk * 6 + f].kind == NB_OUTER) outer |= 1 << f;
+  if (!outer) return;
+  double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;
+    int i, j, k;
+    cell_of(s, i, j, k);
+    const int on[6] = {i == 0, i == 15, j == 0, j == 15, k == 0, k == 15};
+    for (int f = 0; f < 6; ++f) {
+      if (!((outer >> f) & 1) || !on[f]) continue;
+      double* Af = Ab + (size_t)(1 + f) * BLOCK_CELLS;
+      double* bp = bvec + (size_t)blk * BLOCK_CELLS + s;
+      const double af = Af[s];
+      if (C.bc.type[f] == BC_DIRICHLET) {
+        const double xc = C.bc.value[f];
+        Ab[s] = Ab[s] - af;
+        *bp = *bp - af * xc * 2.0;
+      } else {
+        const double xc = C.bc.value[f] * dx;
+        Ab[s] = Ab[s] + af;
+        if (f & 1) *bp = *bp - af * xc;
+        else *bp = *bp + af * xc;
+      }
+      Af[s] = 0.0;
+    }
+  }
+}
+
+// FFVILS::Fill (blas.f90:5-33): interior and stored guide layer.
+__global__ void __launch_bounds__(THREADS)
+fill_kernel(double* __restrict__ x, size_t stride, double* __restrict__ g, double value) {
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  for (int m = 0; m < 16; ++m) x[(size_t)blk * stride + tid + THREADS * m] = value;
+  if (g)
+    for (int f = 0; f < 6; ++f) g[((size_t)blk * 6 + f) * FACE_CELLS + tid] = value;
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
+                 double* xout, const double* A, const double* b, const double* gst,
+                 double omega, double* partials, SolveState* st, int fin, int iter) {
+  const dim3 grid(C.nb), block(THREADS);
+  if (res && sweep)
+    rbgs_kernel<true, true><<<grid, block, 0, s>>>(C, xin, xout, A, b, gst, omega, partials, st, fin, iter);
+  else if (sweep)
+    rbgs_kernel<false, true><<<grid, block, 0, s>>>(C, xin, xout, A, b, gst, omega, partials, st, fin, iter);
+  else
+    rbgs_kernel<true, false><<<grid, block, 0, s>>>(C, xin, xout, A, b, gst, omega, partials, st, fin, iter);
+}
+
+void launch_jacobi(cudaStream_t s, const KCtx& C, bool from_zero, bool dot, const double* xin,
+                   double* xout, const double* A, const double* b, double omega,
+                   double* partials, SolveState* st) {
+  const dim3 grid(C.nb), block(THREADS);
+  if (from_zero && dot)
+    jacobi_kernel<true, true><<<grid, block, 0, s>>>(C, xin, xout, A, b, omega, partials, st);
+  else if (from_zero)
+    jacobi_kernel<true, false><<<grid, block, 0, s>>>(C, xin, xout, A, b, omega, partials, st);
+  else if (dot)
+    jacobi_kernel<false, true><<<grid, block, 0, s>>>(C, xin, xout, A, b, omega, partials, st);
+  else
+    jacobi_kernel<false, false><<<grid, block, 0, s>>>(C, xin, xout, A, b, omega, partials, st);
+}
+
+void launch_calc_r(cudaStream_t s, const KCtx& C, const double* x, const double* gst,
+                   const double* A, const double* b, double* r, SolveState* st) {
+  calc_r_kernel<<<C.nb, THREADS, 0, s>>>(C, x, gst, A, b, r, st);
+}
+void launch_p_update(cudaStream_t s, const KCtx& C, const double* z, double* p, int first,
+                     SolveState* st) {
+  p_update_kernel<<<C.nb, THREADS, 0, s>>>(z, p, first, st);
+}
+void launch_ax_dot(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
+                   double* partials, SolveState* st) {
+  ax_dot_kernel<<<C.nb, THREADS, 0, s>>>(C, p, A, q, partials, st);
+}
+void launch_cg_update(cudaStream_t s, const KCtx& C, double* x, const double* p, double* r,
+                      const double* q, double* partials, SolveState* st, int iter) {
+  cg_update_kernel<<<C.nb, THREADS, 0, s>>>(x, p, r, q, partials, st, iter);
+}
+void launch_dot(cudaStream_t s, const KCtx& C, const double* x, const double* y,
+                double* partials, SolveState* st, int fin, int iter) {
+  dot_kernel<<<C.nb, THREADS, 0, s>>>(x, y, partials, st, fin, iter);
+}
+void launch_exchange(cudaStream_t s, const KCtx& C, const double* x, double* g) {
+  exchange_kernel<<<C.nb, THREADS, 0, s>>>(C, x, g);
+}
+void launch_pack(cudaStream_t s, int nb, const double* stage, int vc, double* dst, size_t stride,
+                 double* gdst) {
+  pack_kernel<<<nb, THREADS, 0, s>>>(stage, vc, dst, stride, gdst);
+}
+void launch_pack_flag(cudaStream_t s, int nb, const int32_t* stage, int vc, uint8_t* flags,
+                      int bit, int mode) {
+  pack_flag_kernel<<<nb, THREADS, 0, s>>>(stage, vc, flags, bit, mode);
+}
+void launch_unpack_flag(cudaStream_t s, int nb, const uint8_t* flags, int vc, int32_t* stage,
+                        int bit) {
+  unpack_flag_kernel<<<nb, THREADS, 0, s>>>(flags, vc, stage, bit);
+}
+void launch_unpack(cudaStream_t s, const KCtx& C, const double* src, size_t stride, int vc,
+                   int with_guides, double* stage) {
+  unpack_kernel<<<C.nb, THREADS, 0, s>>>(C, src, stride, vc, with_guides, stage);
+}
+void launch_assemble(cudaStream_t s, const KCtx& C, const double* ux, const double* uy,
+                     const double* uz, const double* gux, const double* guy, const double* guz,
+                     const double* cut, const uint8_t* flags, double* A, double* b,
+                     double* vface, double rhof, double dt, size_t field_stride) {
+  assemble_kernel<<<C.nb, THREADS, 0, s>>>(C, ux, uy, uz, gux, guy, guz, cut, flags, A, b, vface,
+                                           rhof, dt, field_stride);
+}
+void launch_fill(cudaStream_t s, int nb, double* x, size_t stride, double* g, double value) {
+  fill_kernel<<<nb, THREADS, 0, s>>>(x, stride, g, value);
+}
+void launch_fold_bc(cudaStream_t s, const KCtx& C, double* A, double* b) {
+  fold_bc_kernel<<<C.nb, THREADS, 0, s>>>(C, A, b);
+}
+
+}  // namespace ffvgpu

@@ -1,0 +1,337 @@
+"""ctypes binding of libffvhc_b200.so (include/ffvgpu.h).
+
+Thin plumbing for tests and benchmarks: every call goes through the C ABI;
+nothing here computes.  Loading fails loudly when the library is missing:
+there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libffvhc_b200.so")
+
+OK, NOT_CONVERGED, NAN_DETECTED, TIMEOUT, OOM, BAD_ARG, CUDA_ERROR, NO_DEVICE = range(8)
+BC_DIRICHLET, BC_NEUMANN = 0, 1
+NB_OUTER, NB_SAME, NB_COARSE, NB_FINE = range(4)
+
+FIELD = {
+    "X": 0, "AP": 1, "AW": 2, "AE": 3, "AS": 4, "AN": 5, "AB": 6, "AT": 7, "B": 8,
+    "UX": 9, "UY": 10, "UZ": 11,
+    "C0": 12, "C1": 13, "C2": 14, "C3": 15, "C4": 16, "C5": 17,
+    "VW": 18, "VE": 19, "VS": 20, "VN": 21, "VB": 22, "VT": 23,
+    "CID0": 100, "CID1": 101, "CID2": 102, "CID3": 103, "CID4": 104, "CID5": 105,
+    "PID": 106,
+}
+
+# Declared entry points of include/ffvgpu.h (checked by the CPU tests).
+EXPORTS = [
+    "ffvgpu_pool_create", "ffvgpu_pool_destroy", "ffvgpu_pool_num_blocks",
+    "ffvgpu_pool_set_stream", "ffvgpu_fill", "ffvgpu_grid_neighbors",
+    "ffvgpu_pool_neighbors", "ffvgpu_pool_device_bytes", "ffvgpu_pool_upload",
+    "ffvgpu_pool_download", "ffvgpu_exchange", "ffvgpu_assemble_p", "ffvgpu_fold_bc",
+    "ffvgpu_solve_rbgs", "ffvgpu_solve_cg", "ffvgpu_rbgs_sweep", "ffvgpu_calc_r2",
+    "ffvgpu_dot", "ffvgpu_version", "ffvgpu_last_error", "ffvgpu_sphere_grid_create",
+    "ffvgpu_sphere_grid_destroy", "ffvgpu_sphere_grid_num_blocks",
+    "ffvgpu_sphere_grid_blocks", "ffvgpu_sphere_grid_fill",
+]
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [
+        ("num_blocks", ctypes.c_int32), ("cells", ctypes.c_int32),
+        ("level", ctypes.c_void_p), ("block_index", ctypes.c_void_p),
+        ("domain_origin", ctypes.c_double * 3), ("root_length", ctypes.c_double),
+        ("root_grid", ctypes.c_int32 * 3),
+        ("neighbor_kind", ctypes.c_void_p), ("neighbor_ids", ctypes.c_void_p),
+        ("bc_type", ctypes.c_int32 * 6), ("bc_value", ctypes.c_double * 6),
+    ]
+
+
+class IterParams(ctypes.Structure):
+    _fields_ = [
+        ("omega", ctypes.c_double), ("count_max", ctypes.c_int32),
+        ("epsilon", ctypes.c_double), ("pre_count", ctypes.c_int32),
+        ("check_every", ctypes.c_int32), ("history", ctypes.c_void_p),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("count", ctypes.c_int32), ("residual", ctypes.c_double),
+        ("elapsed_ms", ctypes.c_double), ("sweep_ms", ctypes.c_double),
+        ("sweep_launches", ctypes.c_int32), ("bytes_moved", ctypes.c_int64),
+        ("kernel_launches", ctypes.c_int32),
+    ]
+
+
+class SphereParams(ctypes.Structure):
+    _fields_ = [
+        ("domain_origin", ctypes.c_double * 3), ("root_grid", ctypes.c_int32 * 3),
+        ("root_length", ctypes.c_double), ("max_level", ctypes.c_int32),
+        ("center", ctypes.c_double * 3), ("radius", ctypes.c_double),
+        ("margin", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Loads the library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `make -C ffv-hc_b200` (or "
+                               "__graft_entry__.build()); there is no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_double
+        L.ffvgpu_last_error.restype = ctypes.c_char_p
+        L.ffvgpu_pool_create.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(vp)]
+        L.ffvgpu_pool_destroy.argtypes = [vp]
+        L.ffvgpu_pool_destroy.restype = None
+        L.ffvgpu_pool_num_blocks.argtypes = [vp]
+        L.ffvgpu_pool_device_bytes.argtypes = [vp]
+        L.ffvgpu_pool_device_bytes.restype = ctypes.c_int64
+        L.ffvgpu_pool_neighbors.argtypes = [vp, i32, vp, vp]
+        L.ffvgpu_pool_set_stream.argtypes = [vp, vp]
+        L.ffvgpu_fill.argtypes = [vp, i32, dbl]
+        L.ffvgpu_grid_neighbors.argtypes = [ctypes.POINTER(GridDesc), vp, vp]
+        L.ffvgpu_pool_upload.argtypes = [vp, i32, vp, i32]
+        L.ffvgpu_pool_download.argtypes = [vp, i32, vp, i32]
+        L.ffvgpu_exchange.argtypes = [vp, i32, vp, vp]
+        L.ffvgpu_assemble_p.argtypes = [vp, dbl, dbl]
+        L.ffvgpu_fold_bc.argtypes = [vp]
+        L.ffvgpu_solve_rbgs.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
+        L.ffvgpu_solve_cg.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
+        L.ffvgpu_rbgs_sweep.argtypes = [vp, dbl]
+        L.ffvgpu_calc_r2.argtypes = [vp, ctypes.POINTER(dbl)]
+        L.ffvgpu_dot.argtypes = [vp, i32, i32, ctypes.POINTER(dbl)]
+        L.ffvgpu_sphere_grid_create.argtypes = [ctypes.POINTER(SphereParams), ctypes.POINTER(vp)]
+        L.ffvgpu_sphere_grid_destroy.argtypes = [vp]
+        L.ffvgpu_sphere_grid_destroy.restype = None
+        L.ffvgpu_sphere_grid_num_blocks.argtypes = [vp]
+        L.ffvgpu_sphere_grid_blocks.argtypes = [vp, vp, vp]
+        L.ffvgpu_sphere_grid_blocks.restype = None
+        L.ffvgpu_sphere_grid_fill.argtypes = [vp, ctypes.c_uint64, dbl, i32, vp, vp, vp, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+class FFVGPUError(RuntimeError):
+    def __init__(self, status, what):
+        msg = lib().ffvgpu_last_error().decode(errors="replace")
+        super().__init__(f"{what} failed with status {status}: {msg}")
+        self.status = status
+
+
+def _check(status, what, allow=(OK,)):
+    if status not in allow:
+        raise FFVGPUError(status, what)
+    return status
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+# ---------------------------------------------------------------------------
+# Synthetic sphere grids (host only)
+# ---------------------------------------------------------------------------
+FLOW_PAST_SPHERE = dict(domain_origin=(-4.0, -4.0, -4.0), root_grid=(4, 2, 2), root_length=4.0,
+                        center=(0.0, 0.0, 0.0), radius=0.5, margin=0.5)
+
+# Pressure BCs of the sphere example (examples/FlowPastASphere/sphere.tpp):
+# Neumann 0 at the inlet (X_M) and side walls, Dirichlet 0 at the outlet (X_P).
+P_BC_TYPE = (BC_NEUMANN, BC_DIRICHLET, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN)
+P_BC_VALUE = (0.0,) * 6
+# Velocity BCs: inlet Dirichlet (1,0,0); outlet and walls Neumann 0.
+U_BC_TYPE = (BC_DIRICHLET, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN)
+U_BC_VALUE = {"UX": (1.0, 0, 0, 0, 0, 0), "UY": (0.0,) * 6, "UZ": (0.0,) * 6}
+
+
+class SphereGrid:
+    """2:1-balanced octree of 16^3 leaf blocks refined around a sphere."""
+
+    def __init__(self, max_level, **kw):
+        p = dict(FLOW_PAST_SPHERE)
+        p.update(kw)
+        self.params = p
+        self.max_level = max_level
+        sp = SphereParams(p["domain_origin"], p["root_grid"], p["root_length"], max_level,
+                          p["center"], p["radius"], p["margin"])
+        self._h = ctypes.c_void_p()
+        _check(lib().ffvgpu_sphere_grid_create(ctypes.byref(sp), ctypes.byref(self._h)),
+               "sphere_grid_create")
+        self.nb = lib().ffvgpu_sphere_grid_num_blocks(self._h)
+        self.level = np.zeros(self.nb, np.int32)
+        self.index = np.zeros((self.nb, 3), np.int32)
+        lib().ffvgpu_sphere_grid_blocks(self._h, _ptr(self.level), _ptr(self.index))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.ffvgpu_sphere_grid_destroy(self._h)
+            self._h = None
+
+    @property
+    def cells(self):
+        return self.nb * 4096
+
+    def fill(self, seed=0, sigma=0.01, vc=2):
+        """Per-cell inputs in the reference layout: dict of numpy arrays."""
+        w = 16 + 2 * vc
+        shape = (self.nb, w, w, w)  # [block][k][j][i]
+        out = {k: np.zeros(shape, np.float64) for k in ("UX", "UY", "UZ")}
+        for f in range(6):
+            out[f"C{f}"] = np.zeros(shape, np.float64)
+            out[f"CID{f}"] = np.zeros(shape, np.int32)
+        out["PID"] = np.zeros(shape, np.int32)
+        c6 = (ctypes.c_void_p * 6)(*[out[f"C{f}"].ctypes.data for f in range(6)])
+        i6 = (ctypes.c_void_p * 6)(*[out[f"CID{f}"].ctypes.data for f in range(6)])
+        _check(lib().ffvgpu_sphere_grid_fill(self._h, seed, sigma, vc, _ptr(out["UX"]),
+                                             _ptr(out["UY"]), _ptr(out["UZ"]),
+                                             ctypes.cast(c6, ctypes.c_void_p),
+                                             ctypes.cast(i6, ctypes.c_void_p), _ptr(out["PID"])),
+               "sphere_grid_fill")
+        return out
+
+    def neighbors(self):
+        """Host-only derived neighbour table: (kind [nb][6], ids [nb][6][4])."""
+        d = self.desc()
+        kind = np.zeros((self.nb, 6), np.int32)
+        ids = np.zeros((self.nb, 6, 4), np.int32)
+        _check(lib().ffvgpu_grid_neighbors(ctypes.byref(d), _ptr(kind), _ptr(ids)),
+               "grid_neighbors")
+        return kind, ids
+
+    def desc(self, bc_type=P_BC_TYPE, bc_value=P_BC_VALUE):
+        p = self.params
+        d = GridDesc()
+        d.num_blocks = self.nb
+        d.cells = 16
+        self._lev_keep = np.ascontiguousarray(self.level)
+        self._idx_keep = np.ascontiguousarray(self.index.reshape(-1))
+        d.level = self._lev_keep.ctypes.data
+        d.block_index = self._idx_keep.ctypes.data
+        d.domain_origin = tuple(p["domain_origin"])
+        d.root_length = p["root_length"]
+        d.root_grid = tuple(p["root_grid"])
+        d.neighbor_kind = None
+        d.neighbor_ids = None
+        d.bc_type = tuple(bc_type)
+        d.bc_value = tuple(bc_value)
+        return d
+
+
+# ---------------------------------------------------------------------------
+# Device pool
+# ---------------------------------------------------------------------------
+class Pool:
+    """A device-resident leaf-block pool (ffvgpu_pool)."""
+
+    def __init__(self, desc):
+        self._desc = desc
+        self._h = ctypes.c_void_p()
+        _check(lib().ffvgpu_pool_create(ctypes.byref(desc), ctypes.byref(self._h)), "pool_create")
+        self.nb = lib().ffvgpu_pool_num_blocks(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None and self._h.value:
+            _lib.ffvgpu_pool_destroy(self._h)
+        self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def device_bytes(self):
+        return lib().ffvgpu_pool_device_bytes(self._h)
+
+    def neighbors(self, b):
+        kind = np.zeros(6, np.int32)
+        ids = np.zeros(24, np.int32)
+        _check(lib().ffvgpu_pool_neighbors(self._h, b, _ptr(kind), _ptr(ids)), "pool_neighbors")
+        return kind, ids.reshape(6, 4)
+
+    def upload(self, field, arr, vc=2):
+        fid = FIELD[field]
+        dt = np.int32 if fid >= 100 else np.float64
+        a = np.ascontiguousarray(arr, dtype=dt)
+        assert a.size == self.nb * (16 + 2 * vc) ** 3, (a.shape, vc)
+        _check(lib().ffvgpu_pool_upload(self._h, fid, _ptr(a), vc), f"upload {field}")
+
+    def upload_ptr(self, field, host_ptr, vc=2):
+        """Upload from a raw host pointer (e.g. pinned memory)."""
+        _check(lib().ffvgpu_pool_upload(self._h, FIELD[field], ctypes.c_void_p(host_ptr), vc),
+               f"upload {field}")
+
+    def download(self, field, vc=2):
+        fid = FIELD[field]
+        w = 16 + 2 * vc
+        a = np.zeros((self.nb, w, w, w), np.int32 if fid >= 100 else np.float64)
+        _check(lib().ffvgpu_pool_download(self._h, fid, _ptr(a), vc), f"download {field}")
+        return a
+
+    def download_ptr(self, field, host_ptr, vc=2):
+        _check(lib().ffvgpu_pool_download(self._h, FIELD[field], ctypes.c_void_p(host_ptr), vc),
+               f"download {field}")
+
+    def exchange(self, field, bc_type=None, bc_value=None):
+        if bc_type is None:
+            _check(lib().ffvgpu_exchange(self._h, FIELD[field], None, None), f"exchange {field}")
+            return
+        t = np.asarray(bc_type, np.int32)
+        v = np.asarray(bc_value, np.float64)
+        _check(lib().ffvgpu_exchange(self._h, FIELD[field], _ptr(t), _ptr(v)), f"exchange {field}")
+
+    def assemble_p(self, rhof=1.0, dt=0.002):
+        _check(lib().ffvgpu_assemble_p(self._h, rhof, dt), "assemble_p")
+
+    def fold_bc(self):
+        _check(lib().ffvgpu_fold_bc(self._h), "fold_bc")
+
+    def _solve(self, fn, what, omega, count_max, epsilon, pre_count, history, check_every):
+        hist = np.zeros(max(count_max, 1), np.float64) if history else None
+        prm = IterParams(omega, count_max, epsilon, pre_count, check_every,
+                         hist.ctypes.data if history else None)
+        res = Result()
+        st = fn(self._h, ctypes.byref(prm), ctypes.byref(res))
+        _check(st, what, allow=(OK, NOT_CONVERGED, NAN_DETECTED))
+        out = dict(status=st, count=res.count, residual=res.residual, elapsed_ms=res.elapsed_ms,
+                   sweep_ms=res.sweep_ms, sweep_launches=res.sweep_launches,
+                   bytes_moved=res.bytes_moved, kernel_launches=res.kernel_launches)
+        if history:
+            n = res.count if 1 <= res.count <= count_max else (count_max if res.count > 0 else 0)
+            out["history"] = hist[:n].copy()
+        return out
+
+    def solve_rbgs(self, omega=1.5, count_max=200, epsilon=0.0, history=True, check_every=0):
+        return self._solve(lib().ffvgpu_solve_rbgs, "solve_rbgs", omega, count_max, epsilon, 0,
+                           history, check_every)
+
+    def solve_cg(self, omega=1.0, pre_count=2, count_max=10000, epsilon=1e-10, history=True,
+                 check_every=0):
+        return self._solve(lib().ffvgpu_solve_cg, "solve_cg", omega, count_max, epsilon,
+                           pre_count, history, check_every)
+
+    def set_stream(self, stream_handle):
+        """Enqueue on a caller's CUDA stream (an int cudaStream_t, 0/None = own)."""
+        _check(lib().ffvgpu_pool_set_stream(self._h, ctypes.c_void_p(stream_handle or None)),
+               "pool_set_stream")
+
+    def fill(self, field, value):
+        _check(lib().ffvgpu_fill(self._h, FIELD[field], float(value)), "fill")
+
+    def rbgs_sweep(self, omega):
+        _check(lib().ffvgpu_rbgs_sweep(self._h, omega), "rbgs_sweep")
+
+    def calc_r2(self):
+        v = ctypes.c_double()
+        _check(lib().ffvgpu_calc_r2(self._h, ctypes.byref(v)), "calc_r2")
+        return v.value
+
+    def dot(self, fx, fy):
+        v = ctypes.c_double()
+        _check(lib().ffvgpu_dot(self._h, FIELD[fx], FIELD[fy], ctypes.byref(v)), "dot")
+        return v.value

@@ -1,0 +1,239 @@
+/* ffvgpu.h -- C ABI of the B200 pressure-Poisson path for FFV-HC.
+ *
+ * The reference calls its pressure solver once per time step through
+ * FFVILS (src/FFV/FFVILS.h) on a BCMTools block manager whose leaf blocks
+ * each hold (n+2*vc)^3 reals per field (src/FFV/LocalScalar3D.h:21-84).
+ * This header replaces that per-solve surface with a device-resident block
+ * pool: the caller describes the leaf blocks once, uploads fields in the
+ * reference's own per-block layout, and calls the solve entry points, which
+ * keep every iteration on the GPU.
+ *
+ * Conventions
+ *  - All functions return ffvgpu_status; nothing calls exit().
+ *  - One pool is used from one host thread at a time (thread-compatible).
+ *  - Host arrays use the reference layout: per block (n+2*vc)^3 doubles
+ *    (int32 for integer fields), i fastest, blocks back to back, with
+ *    n = 16 and vc >= 1 (the reference default is vc = 2,
+ *    src/FFV/FFVConfig.cpp:43-44).
+ *  - Faces are numbered X_M=0, X_P=1, Y_M=2, Y_P=3, Z_M=4, Z_P=5 as in
+ *    BCMTools' Face enum used by src/FFV/BlockScalar3D.h:42-172.
+ */
+#ifndef FFVGPU_H
+#define FFVGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FFVGPU_OK = 0,
+  FFVGPU_NOT_CONVERGED = 1, /* countMax reached (reference: silent, FFVILS.h:44-45) */
+  FFVGPU_NAN_DETECTED = 2,  /* residual NaN/Inf (reference: Exit(0), FFVILS.h:36-43) */
+  FFVGPU_TIMEOUT = 3,       /* a bounded device wait gave up */
+  FFVGPU_OOM = 4,           /* device allocation failed */
+  FFVGPU_BAD_ARG = 5,       /* invalid argument or grid description */
+  FFVGPU_CUDA_ERROR = 6,    /* a CUDA runtime call failed */
+  FFVGPU_NO_DEVICE = 7      /* no CUDA device visible */
+} ffvgpu_status;
+
+/* Outer boundary types, src/FFV/FFVBC.h:6-14. */
+enum { FFVGPU_BC_DIRICHLET = 0, FFVGPU_BC_NEUMANN = 1 };
+
+/* Neighbour kinds of one block face. */
+enum {
+  FFVGPU_NB_OUTER = 0,  /* outer boundary of the domain */
+  FFVGPU_NB_SAME = 1,   /* one block of the same level */
+  FFVGPU_NB_COARSE = 2, /* one block one level coarser (2:1) */
+  FFVGPU_NB_FINE = 3    /* four blocks one level finer */
+};
+
+/* Pool fields.  Vectors carry guide cells; matrix fields are interior only. */
+typedef enum {
+  FFVGPU_FIELD_X = 0, /* pressure p (solution) */
+  FFVGPU_FIELD_AP, FFVGPU_FIELD_AW, FFVGPU_FIELD_AE, FFVGPU_FIELD_AS,
+  FFVGPU_FIELD_AN, FFVGPU_FIELD_AB, FFVGPU_FIELD_AT,
+  FFVGPU_FIELD_B,
+  FFVGPU_FIELD_UX, FFVGPU_FIELD_UY, FFVGPU_FIELD_UZ,
+  FFVGPU_FIELD_C0, FFVGPU_FIELD_C1, FFVGPU_FIELD_C2, FFVGPU_FIELD_C3,
+  FFVGPU_FIELD_C4, FFVGPU_FIELD_C5,
+  FFVGPU_FIELD_VW, FFVGPU_FIELD_VE, FFVGPU_FIELD_VS, FFVGPU_FIELD_VN,
+  FFVGPU_FIELD_VB, FFVGPU_FIELD_VT,
+  FFVGPU_FIELD_NUM_REAL,
+  /* integer fields */
+  FFVGPU_IFIELD_CID0 = 100, FFVGPU_IFIELD_CID1, FFVGPU_IFIELD_CID2,
+  FFVGPU_IFIELD_CID3, FFVGPU_IFIELD_CID4, FFVGPU_IFIELD_CID5,
+  FFVGPU_IFIELD_PID
+} ffvgpu_field;
+
+/* Leaf-block layout, the information BCMTools' BlockManager holds
+ * (BlockBase size/origin/level and NeighborInfo, used at
+ * src/FFV/Solver.cpp:338-386). */
+typedef struct {
+  int32_t num_blocks;
+  int32_t cells;               /* cells per block edge; must be 16 */
+  const int32_t* level;        /* [num_blocks] octree level */
+  const int32_t* block_index;  /* [num_blocks][3] block position, in units of
+                                  this level's block edge, from domain_origin */
+  double domain_origin[3];
+  double root_length;          /* edge of a level-0 (root) block */
+  int32_t root_grid[3];        /* root blocks per axis */
+  /* Optional explicit neighbour table; NULL derives it from level and
+   * block_index.  kind: [num_blocks][6]; ids: [num_blocks][6][4], where a
+   * FINE face lists its four blocks in transverse order (u + 2v) and a
+   * COARSE face lists the coarse block in ids[0]. */
+  const int32_t* neighbor_kind;
+  const int32_t* neighbor_ids;
+  /* Outer boundary condition of the pressure, per face (FFVBC.h types).
+   * Neumann values are multiplied by each block's cell size as in
+   * src/FFV/BlockScalar3D.h:72-77. */
+  int32_t bc_type[6];
+  double bc_value[6];
+} ffvgpu_grid_desc;
+
+typedef struct ffvgpu_pool ffvgpu_pool;
+
+/* Iteration parameters (src/FFV/FFVConfig.cpp:133-160 keys). */
+typedef struct {
+  double omega;          /* relaxation factor (Omega) */
+  int32_t count_max;     /* MaxIteration */
+  double epsilon;        /* ConvergenceCriterion (relative residual) */
+  int32_t pre_count;     /* PreCount: Jacobi preconditioner sweeps (CG) */
+  int32_t check_every;   /* host polls convergence every this many iterations
+                            (0 = default); does not change results */
+  double* history;       /* optional host array [count_max]: residual per iteration */
+} ffvgpu_iter_params;
+
+typedef struct {
+  int32_t count;         /* iterations, with the reference's loop-variable meaning */
+  double residual;       /* sqrt(|rr|/|bb|) of the last iteration */
+  double elapsed_ms;     /* device time of the solve (CUDA events) */
+  double sweep_ms;       /* device time of the steady-state sweep passes only */
+  int32_t sweep_launches;/* number of launches sweep_ms covers */
+  int64_t bytes_moved;   /* algorithmic HBM bytes of the solve */
+  int32_t kernel_launches;
+} ffvgpu_result;
+
+/* ---- pool lifetime ------------------------------------------------------ */
+
+/* Creates a pool on the current CUDA device.  Replaces the per-field
+ * LocalScalar3D allocation and VCUpdater registration
+ * (src/FFV/LocalScalar3D.h:24-84, src/FFV/Solver.cpp:1967-2043). */
+ffvgpu_status ffvgpu_pool_create(const ffvgpu_grid_desc* desc, ffvgpu_pool** out);
+void ffvgpu_pool_destroy(ffvgpu_pool* pool);
+int32_t ffvgpu_pool_num_blocks(const ffvgpu_pool* pool);
+/* Runs the pool's work on the caller's CUDA stream (cudaStream_t passed as
+ * void*; NULL = the pool's own stream).  All later calls enqueue there. */
+ffvgpu_status ffvgpu_pool_set_stream(ffvgpu_pool* pool, void* stream);
+/* Neighbour table as derived (kind [6], ids [6][4]); for tests. */
+ffvgpu_status ffvgpu_pool_neighbors(const ffvgpu_pool* pool, int32_t block,
+                                    int32_t* kind6, int32_t* ids24);
+/* Device bytes held by the pool. */
+int64_t ffvgpu_pool_device_bytes(const ffvgpu_pool* pool);
+
+/* ---- host <-> device ------------------------------------------------------
+ * host: num_blocks * (16+2*vc)^3 values, reference layout.  Upload reads the
+ * interior and, for vector fields, the first guide layer.  Download writes
+ * the interior and vc guide layers of every face (the values the
+ * reference's exchange would hold, src/FFV/Scalar3DUpdater1.cpp); edge and
+ * corner guide cells, which no kernel of the path reads, are written as 0. */
+ffvgpu_status ffvgpu_pool_upload(ffvgpu_pool* pool, ffvgpu_field field,
+                                 const void* host, int32_t vc);
+ffvgpu_status ffvgpu_pool_download(ffvgpu_pool* pool, ffvgpu_field field,
+                                   void* host, int32_t vc);
+
+/* ---- operations -------------------------------------------------------- */
+
+/* Guide-cell exchange of a vector field plus outer BC with the given types
+ * and values: LocalScalar3D<real>::ImposeBoundaryCondition()
+ * (src/FFV/LocalScalar3D.h:266-296) with updater 1
+ * (src/FFV/Scalar3DUpdater1.cpp:9-661, src/CGMfuncs/sup.f90:1-179) and
+ * src/CGMfuncs/bcx.f90.  bc_type/bc_value NULL = the pool's pressure BCs. */
+ffvgpu_status ffvgpu_exchange(ffvgpu_pool* pool, ffvgpu_field field,
+                              const int32_t* bc_type6, const double* bc_value6);
+
+/* Cut-cell coefficients and RHS: per block bcut_calc_ab_p_
+ * (src/FFV/bcut.f90:608-832) as called at src/FFV/Solver.cpp:5471-5481.
+ * Reads UX/UY/UZ (with guide cells, exchange them first), C0..C5, CID0..5,
+ * PID; writes AP..AT, B and VW..VT. */
+ffvgpu_status ffvgpu_assemble_p(ffvgpu_pool* pool, double rhof, double dt);
+
+/* Folds the pool's outer pressure BCs into A and b:
+ * LocalScalar3D::ImposeBoundaryCondition(A..., b) (src/FFV/LocalScalar3D.h:298-323,
+ * src/FFV/BlockScalar3D.h:183-190, src/CGMfuncs/bca.f90:5-388), as called
+ * at src/FFV/Solver.cpp:5574. */
+ffvgpu_status ffvgpu_fold_bc(ffvgpu_pool* pool);
+
+/* Red-black SOR / Gauss-Seidel solve of A x = b on FIELD_X:
+ * FFVILS::RBGS (src/FFV/FFVILS.h:547-594). */
+ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* pool, const ffvgpu_iter_params* prm,
+                                ffvgpu_result* res);
+
+/* Jacobi-preconditioned CG on FIELD_X: FFVILS::CG (src/FFV/FFVILS.h:661-791). */
+ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* pool, const ffvgpu_iter_params* prm,
+                              ffvgpu_result* res);
+
+/* FFVILS::Fill (src/FFV/FFVILS.h:425-445, blas.f90:5-33): every cell of a
+ * real field, guide cells included, set to value. */
+ffvgpu_status ffvgpu_fill(ffvgpu_pool* pool, ffvgpu_field field, double value);
+
+/* Single kernels of the path, for parity tests and for callers that drive
+ * their own loop.  Each matches one FFVILS helper. */
+/* RBGS_Smoother (FFVILS.h:104-162): both colours on every block + exchange. */
+ffvgpu_status ffvgpu_rbgs_sweep(ffvgpu_pool* pool, double omega);
+/* CalcR2 (FFVILS.h:247-296): sum over interior cells of (b - A x)^2. */
+ffvgpu_status ffvgpu_calc_r2(ffvgpu_pool* pool, double* rr);
+/* DOT (FFVILS.h:298-328) of two real fields. */
+ffvgpu_status ffvgpu_dot(ffvgpu_pool* pool, ffvgpu_field x, ffvgpu_field y, double* xy);
+
+/* Sums (CalcR2, DOT, the norms inside the solves) use one fixed reduction
+ * tree, so every result is bit-reproducible run to run. */
+int32_t ffvgpu_version(void);
+/* Last CUDA error string of this thread, for diagnostics. */
+const char* ffvgpu_last_error(void);
+
+/* Host-only neighbour derivation from a grid description (no device
+ * needed): kind [num_blocks][6], ids [num_blocks][6][4] with the
+ * conventions of ffvgpu_grid_desc.  Fails with BAD_ARG on a grid that is not
+ * 2:1 face balanced. */
+ffvgpu_status ffvgpu_grid_neighbors(const ffvgpu_grid_desc* desc, int32_t* kind,
+                                    int32_t* ids);
+
+/* ---- synthetic sphere grids (host only; no device needed) ----------------
+ * Leaf blocks of a 2:1 face-balanced octree refined around a sphere, with
+ * analytic cut-cell fractions in place of Cutlib (src/FFV/Solver.cpp:530-663)
+ * and a seeded intermediate velocity u* = (1,0,0) + N(0, sigma^2). */
+typedef struct {
+  double domain_origin[3];
+  int32_t root_grid[3];
+  double root_length;
+  int32_t max_level;
+  double center[3];
+  double radius;
+  double margin;  /* refine while a block lies within radius + margin of center */
+} ffvgpu_sphere_params;
+
+typedef struct ffvgpu_sphere_grid ffvgpu_sphere_grid;
+
+ffvgpu_status ffvgpu_sphere_grid_create(const ffvgpu_sphere_params* prm,
+                                        ffvgpu_sphere_grid** out);
+void ffvgpu_sphere_grid_destroy(ffvgpu_sphere_grid* g);
+int32_t ffvgpu_sphere_grid_num_blocks(const ffvgpu_sphere_grid* g);
+/* Copies level[num_blocks] and block_index[num_blocks][3]. */
+void ffvgpu_sphere_grid_blocks(const ffvgpu_sphere_grid* g, int32_t* level,
+                               int32_t* block_index);
+/* Fills the per-cell inputs of the pressure assembly in the reference layout
+ * (vc guide layers, guide cells set to 0):
+ * ux,uy,uz: u*; c[6]: cut distance in (0,1] (1 where uncut, rounded through
+ * float as Cutlib's CutPos32 does); cid[6]: 1 where cut; pid: 1 fluid, 0 solid.
+ * Any pointer may be NULL to skip that output. */
+ffvgpu_status ffvgpu_sphere_grid_fill(const ffvgpu_sphere_grid* g, uint64_t seed,
+                                      double sigma, int32_t vc, double* ux,
+                                      double* uy, double* uz, double* const* c6,
+                                      int32_t* const* cid6, int32_t* pid);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FFVGPU_H */

@@ -1,0 +1,200 @@
+"""ctypes binding of the CPU oracle (oracle/libffvoracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU baseline / reference legs, never by the product.  The oracle
+restates FFV-HC's pressure path in C++ (ffv_oracle.cpp); parity is unpinned
+by reference tests because the reference ships none and cannot be compiled
+here (see the header of ffv_oracle.cpp).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libffvoracle.so")
+
+F = dict(X=0, AP=1, AW=2, AE=3, AS=4, AN=5, AB=6, AT=7, B=8, UX=9, UY=10, UZ=11,
+         C0=12, C1=13, C2=14, C3=15, C4=16, C5=17, VW=18, VE=19, VS=20, VN=21, VB=22, VT=23,
+         R=24, P=25, Q=26, Z=27, X0=28, R0=29, P_=30, Q_=31, S=32, S_=33, T_=34)
+FI = dict(CID0=0, CID1=1, CID2=2, CID3=3, CID4=4, CID5=5, PID=6)
+RED_REFERENCE, RED_CANONICAL = 0, 1
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, dbl = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.orc_create.restype = vp
+        L.orc_create.argtypes = [i32, i32, i32, vp, vp, vp, dbl, vp]
+        L.orc_destroy.argtypes = [vp]
+        L.orc_field.restype = ctypes.POINTER(ctypes.c_double)
+        L.orc_field.argtypes = [vp, i32]
+        L.orc_ifield.restype = ctypes.POINTER(ctypes.c_int)
+        L.orc_ifield.argtypes = [vp, i32]
+        L.orc_cells_per_block.restype = ctypes.c_long
+        L.orc_cells_per_block.argtypes = [vp]
+        L.orc_set_threads.argtypes = [vp, i32]
+        L.orc_set_reduction.argtypes = [vp, i32]
+        L.orc_neighbor.argtypes = [vp, i32, i32, vp, vp, vp]
+        L.orc_block_dx.restype = dbl
+        L.orc_block_dx.argtypes = [vp, i32]
+        L.orc_set_bc.argtypes = [vp, vp, vp]
+        L.orc_exchange.argtypes = [vp, i32, vp, vp]
+        L.orc_assemble_p.argtypes = [vp, dbl, dbl]
+        L.orc_fold_bc.argtypes = [vp]
+        L.orc_rbgs_sweep.argtypes = [vp, dbl]
+        L.orc_calc_r2.restype = dbl
+        L.orc_calc_r2.argtypes = [vp]
+        L.orc_dot.restype = dbl
+        L.orc_dot.argtypes = [vp, i32, i32]
+        L.orc_calc_ax.argtypes = [vp, i32, i32]
+        L.orc_calc_r.argtypes = [vp, i32, i32, i32]
+        L.orc_jacobi_smoother.argtypes = [vp, i32, i32, i32, dbl]
+        L.orc_slot.argtypes = [vp, i32]
+        for fn in (L.orc_rbgs,):
+            fn.argtypes = [vp, dbl, i32, dbl, vp, vp, vp]
+        for fn in (L.orc_cg, L.orc_bicgstab):
+            fn.argtypes = [vp, dbl, i32, i32, dbl, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """Block pool in the reference layout (vc guide layers) + FFVILS drivers."""
+
+    def __init__(self, level, index, domain_origin, root_length, root_grid, vc=2,
+                 bc_type=None, bc_value=None, threads=1, reduction=RED_CANONICAL):
+        L = lib()
+        self.nb = len(level)
+        self.vc = vc
+        self.w = 16 + 2 * vc
+        lev = np.ascontiguousarray(level, np.int32)
+        idx = np.ascontiguousarray(np.asarray(index).reshape(-1), np.int64)
+        org = np.ascontiguousarray(domain_origin, np.float64)
+        rg = np.ascontiguousarray(root_grid, np.int32)
+        self._h = L.orc_create(self.nb, 16, vc, lev.ctypes.data, idx.ctypes.data, org.ctypes.data,
+                               float(root_length), rg.ctypes.data)
+        if not self._h:
+            raise ValueError("oracle: grid is not 2:1 face balanced")
+        self.set_threads(threads)
+        self.set_reduction(reduction)
+        if bc_type is not None:
+            self.set_bc(bc_type, bc_value)
+
+    @classmethod
+    def from_grid(cls, grid, **kw):
+        p = grid.params
+        return cls(grid.level, grid.index, p["domain_origin"], p["root_length"], p["root_grid"],
+                   **kw)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_threads(self, n):
+        lib().orc_set_threads(self._h, int(n))
+
+    def set_reduction(self, mode):
+        lib().orc_set_reduction(self._h, int(mode))
+
+    def set_bc(self, bc_type, bc_value):
+        t = np.ascontiguousarray(bc_type, np.int32)
+        v = np.ascontiguousarray(bc_value, np.float64)
+        lib().orc_set_bc(self._h, t.ctypes.data, v.ctypes.data)
+
+    def field(self, name):
+        """Live numpy view [block][k][j][i] of a field (follows LSSwap slots)."""
+        n = self.nb * self.w ** 3
+        if name in FI:
+            p = lib().orc_ifield(self._h, FI[name])
+            return np.ctypeslib.as_array(p, shape=(n,)).reshape(self.nb, self.w, self.w, self.w)
+        p = lib().orc_field(self._h, F[name])
+        return np.ctypeslib.as_array(p, shape=(n,)).reshape(self.nb, self.w, self.w, self.w)
+
+    def set_field(self, name, arr):
+        self.field(name)[...] = arr
+
+    def neighbor(self, b, face):
+        kind = ctypes.c_int()
+        nbr = np.zeros(4, np.int32)
+        so = np.zeros(2, np.int32)
+        lib().orc_neighbor(self._h, b, face, ctypes.byref(kind), nbr.ctypes.data, so.ctypes.data)
+        return kind.value, nbr, so
+
+    def exchange(self, name, bc_type, bc_value):
+        t = np.ascontiguousarray(bc_type, np.int32)
+        v = np.ascontiguousarray(bc_value, np.float64)
+        lib().orc_exchange(self._h, F[name], t.ctypes.data, v.ctypes.data)
+
+    def assemble_p(self, rhof=1.0, dt=0.002):
+        lib().orc_assemble_p(self._h, rhof, dt)
+
+    def fold_bc(self):
+        lib().orc_fold_bc(self._h)
+
+    def rbgs_sweep(self, omega):
+        lib().orc_rbgs_sweep(self._h, omega)
+
+    def calc_r2(self):
+        return lib().orc_calc_r2(self._h)
+
+    def dot(self, a, b):
+        return lib().orc_dot(self._h, F[a], F[b])
+
+    def _solve(self, fn, args, count_max):
+        count = ctypes.c_int()
+        res = ctypes.c_double()
+        hist = np.zeros(max(count_max, 1), np.float64)
+        st = fn(self._h, *args, ctypes.byref(count), ctypes.byref(res), hist.ctypes.data)
+        n = count.value if 1 <= count.value <= count_max else (count_max if count.value > 0 else 0)
+        return dict(status=st, count=count.value, residual=res.value, history=hist[:n].copy())
+
+    def solve_rbgs(self, omega=1.5, count_max=200, epsilon=0.0):
+        return self._solve(lib().orc_rbgs, (float(omega), int(count_max), float(epsilon)), count_max)
+
+    def solve_cg(self, omega=1.0, pre_count=2, count_max=10000, epsilon=1e-10):
+        return self._solve(lib().orc_cg, (float(omega), int(pre_count), int(count_max),
+                                          float(epsilon)), count_max)
+
+    def solve_bicgstab(self, omega=1.0, pre_count=2, count_max=1000, epsilon=1e-10):
+        return self._solve(lib().orc_bicgstab, (float(omega), int(pre_count), int(count_max),
+                                                float(epsilon)), count_max)
+
+
+def interior(a, vc=2):
+    """Interior cells [block][k][j][i] of a reference-layout array."""
+    return a[:, vc:vc + 16, vc:vc + 16, vc:vc + 16]
+
+
+def face_guides(a, vc=2, layers=1):
+    """Face guide slabs (layers nearest the interior first) of a reference-layout array,
+    as a dict face -> array [block][layer][v][u]."""
+    s = slice(vc, vc + 16)
+    out = {}
+    for L in range(1, layers + 1):
+        lo, hi = vc - L, vc + 15 + L
+        out.setdefault(0, []).append(a[:, s, s, lo])
+        out.setdefault(1, []).append(a[:, s, s, hi])
+        out.setdefault(2, []).append(a[:, s, lo, s])
+        out.setdefault(3, []).append(a[:, s, hi, s])
+        out.setdefault(4, []).append(a[:, lo, s, s])
+        out.setdefault(5, []).append(a[:, hi, s, s])
+    return {f: np.stack(v, axis=1) for f, v in out.items()}
