@@ -1,0 +1,505 @@
+"""CPU tests (no GPU): the oracle against known answers written out
+independently from the reference's Fortran, the synthetic grid generator,
+the host-side neighbour derivation, and the C ABI's exported symbols.
+
+The reference ships no tests or golden vectors, so these known answers are
+derived here from the reference's source text: each Python expression below
+restates one Fortran statement in its evaluation order, and Python floats
+are IEEE doubles, so oracle and restatement must agree bit for bit.
+"""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import ffvgpu
+import ffv_oracle as fo
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+VC = 2
+W = 16 + 2 * VC
+
+
+def I(i, j, k):
+    """Fortran (i, j, k), 1-based with lower bound 1-g, -> numpy [k][j][i]."""
+    return (k - 1 + VC, j - 1 + VC, i - 1 + VC)
+
+
+# ---------------------------------------------------------------------------
+# C ABI surface
+# ---------------------------------------------------------------------------
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "ffvgpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ffvgpu_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = ffvgpu.lib()
+    names = header_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert sorted(ffvgpu.EXPORTS) == sorted(n for n in names if n in ffvgpu.EXPORTS)
+    assert set(names) == set(ffvgpu.EXPORTS), set(names) ^ set(ffvgpu.EXPORTS)
+
+
+def test_pool_create_without_device_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is visible")
+    g = ffvgpu.SphereGrid(1)
+    with pytest.raises(ffvgpu.FFVGPUError) as e:
+        ffvgpu.Pool(g.desc())
+    assert e.value.status in (ffvgpu.NO_DEVICE, ffvgpu.CUDA_ERROR)
+
+
+# ---------------------------------------------------------------------------
+# Synthetic grid generator
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("level,nb,hist", [
+    (3, 548, [4, 64, 224, 256]),
+    (4, 1164, [4, 64, 224, 168, 704]),
+    (5, 4692, [4, 64, 200, 312, 656, 3456]),
+])
+def test_sphere_grid_block_counts(level, nb, hist):
+    g = ffvgpu.SphereGrid(level)
+    assert g.nb == nb
+    assert np.bincount(g.level).tolist() == hist
+
+
+def test_sphere_grid_is_2to1_balanced_and_tiles_domain():
+    g = ffvgpu.SphereGrid(4)
+    vol = sum((4.0 / 2 ** L) ** 3 for L in g.level)
+    assert vol == pytest.approx(16.0 * 8 * 8)
+    kind, ids = g.neighbors()  # raises on a 2:1 violation
+    for b in range(g.nb):
+        for f in range(6):
+            if kind[b, f] == ffvgpu.NB_SAME:
+                assert g.level[ids[b, f, 0]] == g.level[b]
+            elif kind[b, f] == ffvgpu.NB_COARSE:
+                assert g.level[ids[b, f, 0]] == g.level[b] - 1
+            elif kind[b, f] == ffvgpu.NB_FINE:
+                assert all(g.level[i] == g.level[b] + 1 for i in ids[b, f])
+
+
+def test_sphere_inputs_deterministic_and_distributed():
+    g = ffvgpu.SphereGrid(2)
+    a = g.fill(seed=5, sigma=0.01)
+    b = g.fill(seed=5, sigma=0.01)
+    c = g.fill(seed=6, sigma=0.01)
+    for k in a:
+        assert np.array_equal(a[k], b[k])
+    assert not np.array_equal(a["UX"], c["UX"])
+    ux = fo.interior(a["UX"])
+    uy = fo.interior(a["UY"])
+    assert abs(ux.mean() - 1.0) < 1e-4 and abs(ux.std() - 0.01) < 1e-4
+    assert abs(uy.mean()) < 1e-4 and abs(uy.std() - 0.01) < 1e-4
+    # guide cells are zero
+    assert a["UX"][:, :VC].max() == 0.0
+
+
+def test_sphere_cut_information():
+    g = ffvgpu.SphereGrid(3)
+    inp = g.fill(seed=1)
+    pid = fo.interior(inp["PID"])
+    solid = int((pid == 0).sum())
+    dx3 = sum(((4.0 / 2 ** L) / 16) ** 3 * int((fo.interior(inp["PID"])[b] == 0).sum())
+              for b, L in enumerate(g.level))
+    assert solid > 0
+    assert dx3 == pytest.approx(4.0 / 3.0 * np.pi * 0.5 ** 3, rel=0.05)
+    for f in range(6):
+        c = fo.interior(inp[f"C{f}"])
+        cid = fo.interior(inp[f"CID{f}"])
+        assert np.all(c[cid == 0] == 1.0)
+        cut = c[cid != 0]
+        assert cut.size > 0 and np.all((cut > 0.0) & (cut <= 1.0))
+        assert np.array_equal(cut, cut.astype(np.float32).astype(np.float64))
+
+
+def test_neighbour_tables_agree_with_oracle():
+    g = ffvgpu.SphereGrid(3, center=(0.7, -0.3, 0.2))
+    kind, ids = g.neighbors()
+    O = fo.Oracle.from_grid(g)
+    for b in range(g.nb):
+        for f in range(6):
+            ok, onb, so = O.neighbor(b, f)
+            assert ok == kind[b, f]
+            if ok in (ffvgpu.NB_SAME, ffvgpu.NB_COARSE):
+                assert onb[0] == ids[b, f, 0]
+            elif ok == ffvgpu.NB_FINE:
+                assert sorted(onb) == sorted(ids[b, f])
+
+
+# ---------------------------------------------------------------------------
+# Exchange (sup.f90 + Scalar3DUpdater1.cpp + bcx.f90)
+# ---------------------------------------------------------------------------
+def centres(g, b):
+    p = g.params
+    L = g.level[b]
+    bl = p["root_length"] / 2 ** L
+    dx = bl / 16
+    org = np.array(p["domain_origin"]) + bl * g.index[b]
+    c = org[:, None] + (np.arange(-VC, 16 + VC) + 0.5)[None, :] * dx
+    return np.meshgrid(c[2], c[1], c[0], indexing="ij")  # Z, Y, X
+
+
+def test_exchange_reproduces_linear_fields():
+    g = ffvgpu.SphereGrid(3, center=(0.3, 0.1, -0.2))
+    O = fo.Oracle.from_grid(g)
+    X = O.field("X")
+    ref = np.empty_like(X)
+    for b in range(g.nb):
+        Z, Y, XX = centres(g, b)
+        ref[b] = 0.3 + 1.1 * XX - 0.7 * Y + 0.45 * Z
+    X[...] = 0.0
+    X[:, VC:VC + 16, VC:VC + 16, VC:VC + 16] = fo.interior(ref)
+    O.exchange("X", [1] * 6, [0.0] * 6)
+    worst = 0.0
+    for b in range(g.nb):
+        for f in range(6):
+            if O.neighbor(b, f)[0] == ffvgpu.NB_OUTER:
+                continue
+            got = fo.face_guides(X[b:b + 1], VC, 2)[f]
+            want = fo.face_guides(ref[b:b + 1], VC, 2)[f]
+            worst = max(worst, np.abs(got - want).max())
+    assert worst < 1e-13
+
+
+def two_level_grid(axis, coarse_minus):
+    """Root grid of 2 blocks along 'axis': one coarse root block and the 8
+    children of the other, so the two share a 2:1 face."""
+    rg = [1, 1, 1]
+    rg[axis] = 2
+    lev, idx = [0], []
+    c = [0, 0, 0]
+    c[axis] = 0 if coarse_minus else 1
+    idx.append(c)
+    for q in range(8):
+        ch = [(q >> 0) & 1, (q >> 1) & 1, (q >> 2) & 1]
+        ch[axis] += 2 * (1 if coarse_minus else 0)
+        lev.append(1)
+        idx.append(ch)
+    return np.array(lev), np.array(idx), rg
+
+
+def intp_index(i, n):
+    """sup.f90:1-16 sup_get_intp_index."""
+    ic = i // 2
+    r = 0.25 + 0.5 * (i % 2)
+    if i < 2:
+        ic, r = 1, -0.25
+    elif i > 2 * n - 1:
+        ic, r = n - 1, 1.25
+    return ic, r
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+@pytest.mark.parametrize("coarse_minus", [True, False])
+def test_c2f_and_f2c_known_answers(axis, coarse_minus):
+    lev, idx, rg = two_level_grid(axis, coarse_minus)
+    O = fo.Oracle(lev, idx, (0.0, 0.0, 0.0), 1.0, rg)
+    rng = np.random.default_rng(axis + 10 * coarse_minus)
+    X = O.field("X")
+    X[...] = rng.standard_normal(X.shape)
+    src = X.copy()
+    O.exchange("X", [1] * 6, [0.0] * 6)
+    n = 16
+    # every fine block touching the coarse one: C2F into its guide layers
+    cface = 2 * axis + (1 if coarse_minus else 0)   # coarse block's face towards the fine ones
+    fface = 2 * axis + (0 if coarse_minus else 1)   # fine blocks' face towards the coarse one
+    kind, nbr, so = O.neighbor(0, cface)
+    assert kind == ffvgpu.NB_FINE
+    t = [a for a in range(3) if a != axis]
+    for fb in range(1, 9):
+        fk, fn, fso = O.neighbor(fb, fface)
+        if fk != ffvgpu.NB_COARSE:
+            continue
+        off = [idx[fb][a] & 1 for a in range(3)]
+        for L in (1, 2):
+            for v in range(1, n + 1):
+                for u in range(1, n + 1):
+                    g = [0, 0, 0]       # 1-based guide cell in the fine block
+                    g[t[0]], g[t[1]] = u, v
+                    g[axis] = (1 - L) if fface % 2 == 0 else (n + L)
+                    pos = [0, 0, 0]     # 1-based fine position inside the coarse block
+                    for a in t:
+                        pos[a] = g[a] + n * off[a]
+                    pos[axis] = (2 * n + 1 - L) if fface % 2 == 0 else L
+                    (i1, r), (j1, s), (k1, tt) = (intp_index(p, n) for p in pos)
+                    c = src[0]
+                    nnn, pnn = c[I(i1, j1, k1)], c[I(i1 + 1, j1, k1)]
+                    npn, nnp = c[I(i1, j1 + 1, k1)], c[I(i1, j1, k1 + 1)]
+                    npp, pnp = c[I(i1, j1 + 1, k1 + 1)], c[I(i1 + 1, j1, k1 + 1)]
+                    ppn, ppp = c[I(i1 + 1, j1 + 1, k1)], c[I(i1 + 1, j1 + 1, k1 + 1)]
+                    want = ((1.0 - tt) * ((1.0 - s) * ((1.0 - r) * nnn + r * pnn)
+                                          + s * ((1.0 - r) * npn + r * ppn))
+                            + tt * ((1.0 - s) * ((1.0 - r) * nnp + r * pnp)
+                                    + s * ((1.0 - r) * npp + r * ppp)))
+                    assert X[fb][I(*g)] == want
+    # F2C into the coarse block's guide layers (sup.f90:122-179)
+    for L in (1, 2):
+        for v in range(1, n + 1):
+            for u in range(1, n + 1):
+                g = [0, 0, 0]
+                g[t[0]], g[t[1]] = u, v
+                g[axis] = (1 - L) if cface % 2 == 0 else (n + L)
+                child = [0, 0, 0]
+                child[axis] = 2 if coarse_minus else 1  # the fine layer touching the coarse block
+                for a in t:
+                    child[a] = (g[a] - 1) // (n // 2)
+                fb = [q for q in range(1, 9) if list(idx[q]) == child][0]
+                lo = [0, 0, 0]
+                for a in t:
+                    lo[a] = 2 * ((g[a] - 1) % (n // 2)) + 1
+                lo[axis] = (2 * L - 1) if cface % 2 == 1 else (n - 2 * L + 1)
+                f = src[fb]
+                i1, j1, k1 = lo
+                vals = [f[I(i1, j1, k1)], f[I(i1 + 1, j1, k1)], f[I(i1, j1 + 1, k1)],
+                        f[I(i1, j1, k1 + 1)], f[I(i1, j1 + 1, k1 + 1)], f[I(i1 + 1, j1, k1 + 1)],
+                        f[I(i1 + 1, j1 + 1, k1)], f[I(i1 + 1, j1 + 1, k1 + 1)]]
+                acc = vals[0]
+                for x in vals[1:]:
+                    acc = acc + x
+                assert X[0][I(*g)] == 0.125 * acc
+
+
+def test_outer_bc_ghost_values():
+    """bcx.f90 bc_x?_d / bc_x?_n on a single block with every face outer."""
+    O = fo.Oracle([0], [[0, 0, 0]], (0.0, 0.0, 0.0), 2.0, (1, 1, 1))
+    rng = np.random.default_rng(3)
+    X = O.field("X")
+    X[...] = rng.standard_normal(X.shape)
+    src = X.copy()
+    types = [0, 1, 1, 0, 1, 0]
+    vals = [0.5, -0.25, 2.0, -1.5, 0.75, 3.0]
+    O.exchange("X", types, vals)
+    dx = 2.0 / 16
+    n = 16
+    for f in range(6):
+        ax, plus = f // 2, f % 2
+        xc = vals[f] * dx if types[f] == 1 else vals[f]
+        for v in range(1, n + 1):
+            for u in range(1, n + 1):
+                t = [a for a in range(3) if a != ax]
+                c = [0, 0, 0]
+                c[t[0]], c[t[1]] = u, v
+                c[ax] = n if plus else 1
+                g1, g2 = list(c), list(c)
+                g1[ax] = n + 1 if plus else 0
+                g2[ax] = n + 2 if plus else -1
+                x1 = src[0][I(*c)]
+                if types[f] == 0:
+                    w1, w2 = 2.0 * xc - x1, xc
+                elif plus:
+                    w1, w2 = x1 + xc, x1 + xc * 2.0
+                else:
+                    w1, w2 = x1 - xc, x1 - xc * 2.0
+                assert X[0][I(*g1)] == w1 and X[0][I(*g2)] == w2
+
+
+# ---------------------------------------------------------------------------
+# Assembly (bcut.f90:608-832) and BC folding (bca.f90)
+# ---------------------------------------------------------------------------
+def calc_ab_p_cell(ux, uy, uz, c, cid, pid, i, j, k, rhof, dx, dt):
+    """bcut.f90:666-825 for one cell, statement by statement."""
+    r0 = r1 = r2 = r3 = r4 = r5 = 1.0 / rhof
+    vx0 = 0.5 * (ux[I(i, j, k)] + ux[I(i - 1, j, k)])
+    vx1 = 0.5 * (ux[I(i, j, k)] + ux[I(i + 1, j, k)])
+    vy2 = 0.5 * (uy[I(i, j, k)] + uy[I(i, j - 1, k)])
+    vy3 = 0.5 * (uy[I(i, j, k)] + uy[I(i, j + 1, k)])
+    vz4 = 0.5 * (uz[I(i, j, k)] + uz[I(i, j, k - 1)])
+    vz5 = 0.5 * (uz[I(i, j, k)] + uz[I(i, j, k + 1)])
+    d = [c[f][I(i, j, k)] for f in range(6)]
+    q = [cid[f][I(i, j, k)] for f in range(6)]
+    if q[0] != 0:
+        r0 = 0.0; vx0 = vx1 * (d[0] - 0.5) / (d[0] + 0.5); r1 = (1.0 / rhof) / (d[0] + 0.5)
+    if q[1] != 0:
+        r1 = 0.0; vx1 = vx0 * (d[1] - 0.5) / (d[1] + 0.5); r0 = (1.0 / rhof) / (d[1] + 0.5)
+    if q[2] != 0:
+        r2 = 0.0; vy2 = vy3 * (d[2] - 0.5) / (d[2] + 0.5); r3 = (1.0 / rhof) / (d[2] + 0.5)
+    if q[3] != 0:
+        r3 = 0.0; vy3 = vy2 * (d[3] - 0.5) / (d[3] + 0.5); r2 = (1.0 / rhof) / (d[3] + 0.5)
+    if q[4] != 0:
+        r4 = 0.0; vz4 = vz5 * (d[4] - 0.5) / (d[4] + 0.5); r5 = (1.0 / rhof) / (d[4] + 0.5)
+    if q[5] != 0:
+        r5 = 0.0; vz5 = vz4 * (d[5] - 0.5) / (d[5] + 0.5); r4 = (1.0 / rhof) / (d[5] + 0.5)
+    if q[0] != 0 and q[1] != 0:
+        r0 = r1 = 0.0; vx0 = vx1 = 0.0
+    if q[2] != 0 and q[3] != 0:
+        r2 = r3 = 0.0; vy2 = vy3 = 0.0
+    if q[4] != 0 and q[5] != 0:
+        r4 = r5 = 0.0; vz4 = vz5 = 0.0
+    l = [r / (dx * dx) for r in (r0, r1, r2, r3, r4, r5)]
+    divv = (vx1 - vx0 + vy3 - vy2 + vz5 - vz4) / dx
+    ap = -(l[0] + l[1]) - (l[2] + l[3]) - (l[4] + l[5])
+    out = [ap] + l + [divv / dt]
+    if pid[I(i, j, k)] != 1:
+        out = [-6.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 0.0]
+    return out
+
+
+def test_assembly_known_answers():
+    g = ffvgpu.SphereGrid(2)
+    inp = g.fill(seed=9, sigma=0.05)
+    O = fo.Oracle.from_grid(g, bc_type=ffvgpu.P_BC_TYPE, bc_value=ffvgpu.P_BC_VALUE)
+    for k, v in inp.items():
+        O.field(k)[...] = v
+    for u in ("UX", "UY", "UZ"):
+        O.exchange(u, ffvgpu.U_BC_TYPE, ffvgpu.U_BC_VALUE[u])
+    O.assemble_p(1.3, 0.002)
+    names = ["AP", "AW", "AE", "AS", "AN", "AB", "AT", "B"]
+    rng = np.random.default_rng(0)
+    # every cut cell of a few blocks near the sphere, plus random cells elsewhere
+    near = [b for b in range(g.nb) if fo.interior(inp["CID0"])[b].any()][:3]
+    cells = []
+    for b in near:
+        kk, jj, ii = np.nonzero(np.any([fo.interior(inp[f"CID{f}"])[b] for f in range(6)], axis=0))
+        cells += [(b, i + 1, j + 1, k + 1) for i, j, k in zip(ii, jj, kk)]
+    cells += [(int(rng.integers(g.nb)), *map(int, rng.integers(1, 17, 3))) for _ in range(200)]
+    for b, i, j, k in cells:
+        dx = (4.0 / 2 ** g.level[b]) / 16
+        c = [O.field(f"C{f}")[b] for f in range(6)]
+        cid = [O.field(f"CID{f}")[b] for f in range(6)]
+        want = calc_ab_p_cell(O.field("UX")[b], O.field("UY")[b], O.field("UZ")[b], c, cid,
+                              O.field("PID")[b], i, j, k, 1.3, dx, 0.002)
+        got = [O.field(nm)[b][I(i, j, k)] for nm in names]
+        assert got == want, (b, i, j, k)
+
+
+def test_bc_folding_known_answers():
+    O = fo.Oracle([0], [[0, 0, 0]], (0.0, 0.0, 0.0), 2.0, (1, 1, 1))
+    rng = np.random.default_rng(4)
+    names = ["AP", "AW", "AE", "AS", "AN", "AB", "AT", "B"]
+    for nm in names:
+        O.field(nm)[...] = rng.uniform(0.5, 2.0, O.field(nm).shape)
+    before = {nm: O.field(nm).copy() for nm in names}
+    types = [0, 1, 1, 0, 1, 0]
+    vals = [0.5, -0.25, 2.0, -1.5, 0.75, 3.0]
+    O.set_bc(types, vals)
+    O.fold_bc()
+    dx = 2.0 / 16
+    for (i, j, k) in [(1, 1, 1), (16, 16, 16), (1, 7, 16), (5, 1, 9), (16, 3, 1), (8, 8, 8)]:
+        ap, b = before["AP"][0][I(i, j, k)], before["B"][0][I(i, j, k)]
+        A = {nm: before[nm][0][I(i, j, k)] for nm in names}
+        on = [i == 1, i == 16, j == 1, j == 16, k == 1, k == 16]
+        for f, nm in enumerate(["AW", "AE", "AS", "AN", "AB", "AT"]):
+            if not on[f]:
+                continue
+            af = A[nm]
+            if types[f] == 0:
+                xc = vals[f]
+                ap = ap - af
+                b = b - af * xc * 2.0
+            else:
+                xc = vals[f] * dx
+                ap = ap + af
+                b = (b + af * xc) if f % 2 == 0 else (b - af * xc)
+            A[nm] = 0.0
+        assert O.field("AP")[0][I(i, j, k)] == ap
+        assert O.field("B")[0][I(i, j, k)] == b
+        for nm in ["AW", "AE", "AS", "AN", "AB", "AT"]:
+            assert O.field(nm)[0][I(i, j, k)] == A[nm]
+
+
+# ---------------------------------------------------------------------------
+# Solvers (bils.f90, blas.f90, FFVILS.h)
+# ---------------------------------------------------------------------------
+def rbgs_block(x, A, b, omega):
+    """bils.f90:57-108 rbgs_smoother, colour 0 then 1, on one block array."""
+    Ap, Aw, Ae, As, An, Ab, At = A
+    for color in (0, 1):
+        for k in range(1, 17):
+            for j in range(1, 17):
+                for i in range(1 + (k + j + color) % 2, 17, 2):
+                    m = I(i, j, k)
+                    r = (b[m] - Aw[m] * x[I(i - 1, j, k)] - Ae[m] * x[I(i + 1, j, k)]
+                         - As[m] * x[I(i, j - 1, k)] - An[m] * x[I(i, j + 1, k)]
+                         - Ab[m] * x[I(i, j, k - 1)] - At[m] * x[I(i, j, k + 1)])
+                    x_tmp = r / Ap[m]
+                    x[m] = x[m] - omega * (x[m] - x_tmp)
+
+
+def test_rbgs_sweep_known_answer():
+    g = ffvgpu.SphereGrid(0, root_grid=(2, 1, 1))
+    inp = g.fill(seed=2)
+    O = fo.Oracle.from_grid(g, bc_type=ffvgpu.P_BC_TYPE, bc_value=ffvgpu.P_BC_VALUE)
+    for k, v in inp.items():
+        O.field(k)[...] = v
+    for u in ("UX", "UY", "UZ"):
+        O.exchange(u, ffvgpu.U_BC_TYPE, ffvgpu.U_BC_VALUE[u])
+    O.assemble_p(1.0, 0.002)
+    O.fold_bc()
+    rng = np.random.default_rng(1)
+    O.field("X")[...] = rng.standard_normal(O.field("X").shape)
+    x = O.field("X").copy()
+    A = [O.field(nm) for nm in ["AP", "AW", "AE", "AS", "AN", "AB", "AT"]]
+    b = O.field("B")
+    for blk in range(g.nb):
+        rbgs_block(x[blk], [a[blk] for a in A], b[blk], 1.5)
+    O.rbgs_sweep(1.5)
+    assert np.array_equal(fo.interior(O.field("X")), fo.interior(x))
+
+
+def test_rbgs_reference_behaviour_on_multiblock_grids():
+    """The reference sweeps each block against guide values from the previous
+    exchange (FFVILS.h:104-162): Gauss-Seidel inside a block, Jacobi across
+    blocks.  Over-relaxed (omega 1.5) this diverges once a grid has more than
+    one block; a single block converges.  The oracle (and the GPU path,
+    bit for bit) reproduces both."""
+    from helpers import problem
+    g, inp, O = problem(0, root_grid=(1, 1, 1), radius=0.0)
+    O.field("X")[...] = 0.0
+    h1 = O.solve_rbgs(1.5, 120, 0.0)["history"]
+    assert h1[-1] < 0.01 * h1[0]
+    g, inp, O = problem(0, radius=0.0)
+    O.field("X")[...] = 0.0
+    h2 = O.solve_rbgs(1.5, 120, 0.0)["history"]
+    assert h2[-1] > 10 * h2[0]
+    O.field("X")[...] = 0.0
+    h3 = O.solve_rbgs(1.0, 120, 0.0)["history"]
+    assert h3[-1] < 0.05 * h3[0]
+
+
+def test_cg_converges_on_symmetric_problem_and_sums_agree():
+    from helpers import problem
+    g, inp, O = problem(0, radius=0.5, reduction=fo.RED_CANONICAL)
+    O.field("X")[...] = 0.0
+    rc = O.solve_cg(1.0, 2, 500, 1e-10)
+    assert rc["status"] == 0 and rc["residual"] <= 1e-10 and rc["count"] < 500
+    xc = fo.interior(O.field("X")).copy()
+    g, inp, O = problem(0, radius=0.5, reduction=fo.RED_REFERENCE)
+    O.field("X")[...] = 0.0
+    rr = O.solve_cg(1.0, 2, 500, 1e-10)
+    assert abs(rr["count"] - rc["count"]) <= 2
+    n = min(len(rr["history"]), len(rc["history"])) // 2
+    np.testing.assert_allclose(rr["history"][:n], rc["history"][:n], rtol=1e-9)
+    assert np.abs(fo.interior(O.field("X")) - xc).max() <= 1e-9 * np.abs(xc).max()
+
+
+def test_dot_and_residual_reduction_orders_agree():
+    from helpers import problem
+    g, inp, O = problem(2)
+    rng = np.random.default_rng(2)
+    O.field("X")[...] = rng.standard_normal(O.field("X").shape)
+    O.exchange("X", ffvgpu.P_BC_TYPE, ffvgpu.P_BC_VALUE)
+    O.set_reduction(fo.RED_CANONICAL)
+    a, r2a = O.dot("X", "B"), O.calc_r2()
+    O.set_reduction(fo.RED_REFERENCE)
+    b, r2b = O.dot("X", "B"), O.calc_r2()
+    assert abs(a - b) <= 1e-12 * abs(b)
+    assert abs(r2a - r2b) <= 1e-13 * abs(r2b)
+    # the canonical order does not depend on the thread count
+    O.set_reduction(fo.RED_CANONICAL)
+    O.set_threads(1)
+    assert O.dot("X", "B") == a and O.calc_r2() == r2a
+
+
+def test_bicgstab_converges_on_refined_sphere_grid():
+    from helpers import problem
+    g, inp, O = problem(2)
+    O.field("X")[...] = 0.0
+    r = O.solve_bicgstab(1.0, 2, 600, 1e-8)
+    assert r["status"] == 0 and r["residual"] <= 1e-8
