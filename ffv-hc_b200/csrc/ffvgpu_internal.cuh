@@ -1,6 +1,8 @@
 // ffvgpu_internal.cuh -- device functions shared by the FP64 kernels:
 // guide-cell values of the in-kernel block-to-block exchange.
 #pragma once
+#include <cfloat>
+
 #include "ffvgpu_layout.h"
 
 namespace ffvgpu {
@@ -28,7 +30,7 @@ __device__ __forceinline__ double ld(const double* __restrict__ x, int blk, int 
 
 // Value of guide cell (layer L = 1 or 2) of face 'face' of block 'blk' at
 // transverse position (a, b) in [0,16)^2, computed from interior values of x.
-__device__ __noinline__ double guide_value(const double* __restrict__ x, int blk, int face,
+static __device__ __noinline__ double guide_value(const double* __restrict__ x, int blk, int face,
                                            int a, int b, int L, const FaceNbr& nb,
                                            const BCSet& bc, double dx) {
   const int axis = face >> 1;
@@ -107,6 +109,59 @@ __device__ __noinline__ double guide_value(const double* __restrict__ x, int blk
       if (plus) return (L == 1) ? (x0 + xc) : (x0 + xc * 2.0);
       return (L == 1) ? (x0 - xc) : (x0 - xc * 2.0);
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Convergence bookkeeping run by the last CTA of a reduction.
+// ---------------------------------------------------------------------------
+// FFVILS.h:24-47 IsConverged residual
+__device__ __forceinline__ double resid_of(double rr, double bb) {
+  return (fabs(bb) > (double)FLT_MIN) ? sqrt(fabs(rr) / fabs(bb)) : sqrt(fabs(rr));
+}
+
+__device__ __forceinline__ void finalize(SolveState* st, double total, int fin, int iter) {
+  switch (fin) {
+    case FIN_STORE:
+      st->rr = total;
+      break;
+    case FIN_BB:
+      st->bb = total;
+      break;
+    case FIN_RBGS:
+    case FIN_CG_RR: {
+      const double res = resid_of(total, st->bb);
+      st->rr = total;
+      st->residual = res;
+      if (st->hist) st->hist[iter - 1] = res;
+      st->count = iter;
+      if (res <= st->eps) {
+        st->done = 1;
+      } else if (isnan(res) || isinf(res)) {
+        st->done = 1;
+        st->status = 2;
+      } else if (iter >= st->count_max) {
+        st->done = 1;
+        st->count = st->count_max + 1;  // loop variable after the last pass
+      } else if (fin == FIN_CG_RR) {
+        st->rr0 = st->rr1;
+      }
+      break;
+    }
+    case FIN_CG_RR1:
+      st->rr1 = total;
+      if (fabs(total) < (double)FLT_MIN) {  // FFVILS.h:720-724
+        st->residual = total;
+        st->count = 0;
+        st->done = 1;
+      } else {
+        st->beta = total / st->rr0;
+      }
+      break;
+    case FIN_CG_QP:
+      st->qp = total;
+      st->alpha = st->rr1 / total;
+      break;
   }
 }
 

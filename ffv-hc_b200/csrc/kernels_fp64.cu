@@ -72,56 +72,6 @@ __device__ __forceinline__ void stage_tile(double* __restrict__ xs, const double
   }
 }
 
-// FFVILS.h:24-47 IsConverged residual
-__device__ __forceinline__ double resid_of(double rr, double bb) {
-  return (fabs(bb) > (double)FLT_MIN) ? sqrt(fabs(rr) / fabs(bb)) : sqrt(fabs(rr));
-}
-
-__device__ void finalize(SolveState* st, double total, int fin, int iter) {
-  switch (fin) {
-    case FIN_STORE:
-      st->rr = total;
-      break;
-    case FIN_BB:
-      st->bb = total;
-      break;
-    case FIN_RBGS:
-    case FIN_CG_RR: {
-      const double res = resid_of(total, st->bb);
-      st->rr = total;
-      st->residual = res;
-      if (st->hist) st->hist[iter - 1] = res;
-      st->count = iter;
-      if (res <= st->eps) {
-        st->done = 1;
-      } else if (isnan(res) || isinf(res)) {
-        st->done = 1;
-        st->status = 2;
-      } else if (iter >= st->count_max) {
-        st->done = 1;
-        st->count = st->count_max + 1;  // loop variable after the last pass
-      } else if (fin == FIN_CG_RR) {
-        st->rr0 = st->rr1;
-      }
-      break;
-    }
-    case FIN_CG_RR1:
-      st->rr1 = total;
-      if (fabs(total) < (double)FLT_MIN) {  // FFVILS.h:720-724
-        st->residual = total;
-        st->count = 0;
-        st->done = 1;
-      } else {
-        st->beta = total / st->rr0;
-      }
-      break;
-    case FIN_CG_QP:
-      st->qp = total;
-      st->alpha = st->rr1 / total;
-      break;
-  }
-}
-
 // Canonical block reduction + last-CTA cross-block reduction + finaliser.
 __device__ void reduce_finalize(double v, double* __restrict__ partials, SolveState* st,
                                 int fin, int iter) {
@@ -159,93 +109,6 @@ __device__ void reduce_finalize(double v, double* __restrict__ partials, SolveSt
     st->ticket = 0;
     __threadfence();
   }
-}
-
-// ---------------------------------------------------------------------------
-// RBGS: fused "residual of x_in" + "red-black sweep x_in -> x_out".
-// FFVILS.h:104-162 (RBGS_Smoother -> rbgs_smoother, bils.f90:57-108) and
-// FFVILS.h:247-296 (CalcR2 -> calc_r2, bils.f90:256-304).  Both colours'
-// residuals are formed from x_in before any update; colour 0 is then
-// updated, and colour 1 is updated against the new colour-0 values, as the
-// reference's serial colour-0-then-colour-1 loop does within a block.
-// ---------------------------------------------------------------------------
-template <bool DO_RES, bool DO_SWEEP>
-__global__ void __launch_bounds__(THREADS, 3)
-rbgs_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
-            const double* __restrict__ A, const double* __restrict__ bvec,
-            const double* __restrict__ gst, double omega, double* __restrict__ partials,
-            SolveState* st, int fin, int iter) {
-  if (solve_done(st)) return;
-  __shared__ double xs[TILE];
-  const int blk = blockIdx.x, tid = threadIdx.x;
-  stage_tile(xs, xin, blk, C, gst);
-  __syncthreads();
-  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
-  const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
-  double acc0 = 0.0, acc1 = 0.0;
-  double xn0[8];
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const int q = tid + THREADS * m;
-    {
-      int i, j, k;
-      cell_of(q, i, j, k);
-      const int t = tix(i, j, k);
-      const double ap = __ldg(Ab + q), aw = __ldg(Ab + 4096 + q), ae = __ldg(Ab + 8192 + q);
-      const double as = __ldg(Ab + 12288 + q), an = __ldg(Ab + 16384 + q);
-      const double ab = __ldg(Ab + 20480 + q), at = __ldg(Ab + 24576 + q);
-      const double rs = __ldg(bb + q) - aw * xs[t - 1] - ae * xs[t + 1] - as * xs[t - TW] -
-                        an * xs[t + TW] - ab * xs[t - TP] - at * xs[t + TP];
-      const double xp = xs[t];
-      if (DO_RES) {
-        const double r = rs - ap * xp;
-        acc0 += r * r;
-      }
-      if (DO_SWEEP) {
-        const double xt = rs / ap;
-        xn0[m] = xp - omega * (xp - xt);
-      }
-    }
-    if (DO_RES) {
-      const int s = HALF_CELLS + q;
-      int i, j, k;
-      cell_of(s, i, j, k);
-      const int t = tix(i, j, k);
-      const double r = __ldg(bb + s) - __ldg(Ab + 4096 + s) * xs[t - 1] -
-                       __ldg(Ab + 8192 + s) * xs[t + 1] - __ldg(Ab + 12288 + s) * xs[t - TW] -
-                       __ldg(Ab + 16384 + s) * xs[t + TW] - __ldg(Ab + 20480 + s) * xs[t - TP] -
-                       __ldg(Ab + 24576 + s) * xs[t + TP] - __ldg(Ab + s) * xs[t];
-      acc1 += r * r;
-    }
-  }
-  if (DO_SWEEP) {
-    double* xo = xout + (size_t)blk * BLOCK_CELLS;
-    __syncthreads();
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const int q = tid + THREADS * m;
-      int i, j, k;
-      cell_of(q, i, j, k);
-      xs[tix(i, j, k)] = xn0[m];
-      xo[q] = xn0[m];
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int m = 0; m < 8; ++m) {
-      const int s = HALF_CELLS + tid + THREADS * m;
-      int i, j, k;
-      cell_of(s, i, j, k);
-      const int t = tix(i, j, k);
-      const double rs = __ldg(bb + s) - __ldg(Ab + 4096 + s) * xs[t - 1] -
-                        __ldg(Ab + 8192 + s) * xs[t + 1] - __ldg(Ab + 12288 + s) * xs[t - TW] -
-                        __ldg(Ab + 16384 + s) * xs[t + TW] - __ldg(Ab + 20480 + s) * xs[t - TP] -
-                        __ldg(Ab + 24576 + s) * xs[t + TP];
-      const double xp = xs[t];
-      const double xt = rs / __ldg(Ab + s);
-      xo[s] = xp - omega * (xp - xt);
-    }
-  }
-  if (DO_RES) reduce_finalize(acc0 + acc1, partials, st, fin, iter);
 }
 
 // ---------------------------------------------------------------------------
@@ -643,18 +506,6 @@ fill_kernel(double* __restrict__ x, size_t stride, double* __restrict__ g, doubl
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
-void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
-                 double* xout, const double* A, const double* b, const double* gst,
-                 double omega, double* partials, SolveState* st, int fin, int iter) {
-  const dim3 grid(C.nb), block(THREADS);
-  if (res && sweep)
-    rbgs_kernel<true, true><<<grid, block, 0, s>>>(C, xin, xout, A, b, gst, omega, partials, st, fin, iter);
-  else if (sweep)
-    rbgs_kernel<false, true><<<grid, block, 0, s>>>(C, xin, xout, A, b, gst, omega, partials, st, fin, iter);
-  else
-    rbgs_kernel<true, false><<<grid, block, 0, s>>>(C, xin, xout, A, b, gst, omega, partials, st, fin, iter);
-}
-
 void launch_jacobi(cudaStream_t s, const KCtx& C, bool from_zero, bool dot, const double* xin,
                    double* xout, const double* A, const double* b, double omega,
                    double* partials, SolveState* st) {

@@ -1,0 +1,416 @@
+// rbgs_pipelined.cu -- persistent, TMA-pipelined fused residual + red-black
+// sweep for sm_100a (the hot kernel of FFVILS::RBGS).
+//
+// Per pass over the pool it computes, for every leaf block, the residual
+// sum of x_in (calc_r2, src/CGMfuncs/bils.f90:256-304) and the red-black
+// SOR sweep x_in -> x_out (rbgs_smoother, bils.f90:57-108, colour 0 then
+// colour 1 against guide values from the previous exchange), with the same
+// rounding as the reference (compiled with --fmad=false) and the same sum
+// tree as the rest of the path.
+//
+// One CTA per SM walks blocks blockIdx.x, blockIdx.x + gridDim.x, ...  Its
+// warps have fixed roles:
+//   warp 0      producer: one lane issues cp.async.bulk copies (global ->
+//               shared, completion on mbarriers): the next block's x into a
+//               staging buffer, and the coefficient stream -- for each
+//               colour and each pair of z planes, the 256 cells' Ap..At and
+//               b (8 x 2 KB) -- into a ring of STAGES slots;
+//   warps 1-4   gatherers: the next block's guide layer (the in-kernel
+//               exchange, computed from the neighbours' interiors of x_in)
+//               into a guide buffer;
+//   warps 5-12  consumers (256 threads): build the 18^3 tile of x_in, run the
+//               colour-0 pass (residual + update written to a second tile)
+//               and the colour-1 pass (residual from the first tile, update
+//               against the second), stream x_out to global memory, and sum
+//               the residual.
+// Every wait on an mbarrier is bounded; a wait that gives up raises the
+// CTA's abort flag, every role leaves its loop, the producer drains the
+// copies it has in flight, and the solver state reports TIMEOUT.
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ffvgpu_internal.cuh"
+#include "ffvgpu_kernels.h"
+
+namespace ffvgpu {
+
+namespace pipe {
+
+constexpr int TW = 18, TP = TW * TW, TILE = TW * TW * TW;
+constexpr int STAGES = 4;
+constexpr int NARR = 8;              // Ap, Aw, Ae, As, An, Ab, At, b
+constexpr int CHUNK_CELLS = 256;     // one colour, two z planes
+constexpr int CHUNK_BYTES = NARR * CHUNK_CELLS * 8;
+constexpr int CHUNKS = 16;           // 8 per colour
+constexpr int PRODUCER_WARPS = 1, GATHER_WARPS = 4, CONSUMER_WARPS = 8;
+constexpr int GATHER0 = 32 * PRODUCER_WARPS;
+constexpr int CONS0 = GATHER0 + 32 * GATHER_WARPS;
+constexpr int NTHREADS = CONS0 + 32 * CONSUMER_WARPS;  // 416
+constexpr int NGATHER = 32 * GATHER_WARPS;
+constexpr uint32_t WAIT_LIMIT = 1u << 22;
+
+struct __align__(128) Smem {
+  double ring[STAGES][NARR][CHUNK_CELLS];  // 64 KB
+  double xstage[BLOCK_CELLS];              // 32 KB
+  double tile_old[TILE];                   // 46.6 KB
+  double tile_new[TILE];                   // 46.6 KB
+  double gbuf[6 * FACE_CELLS];             // 12 KB
+  uint64_t full[STAGES], empty[STAGES];
+  uint64_t xfull, xempty, gfull, gempty;
+  double ws[8];
+  int abort_flag;
+  int last;
+};
+
+__device__ __forceinline__ uint32_t sa(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sa(b)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(sa(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait; false when it gave up or another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+  for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+    if (mbar_try_wait(b, parity)) return true;
+    if (*abort_flag) return false;
+  }
+  *abort_flag = 1;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          sa(dst)),
+      "l"(src), "r"(bytes), "r"(sa(bar))
+      : "memory");
+}
+__device__ __forceinline__ void consumer_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(32 * CONSUMER_WARPS) : "memory");
+}
+__device__ __forceinline__ int tix(int i, int j, int k) { return (i + 1) + TW * (j + 1) + TP * (k + 1); }
+__device__ __forceinline__ int guide_tix(int f, int a, int b) {
+  switch (f) {
+    case X_M: return tix(-1, a, b);
+    case X_P: return tix(16, a, b);
+    case Y_M: return tix(a, -1, b);
+    case Y_P: return tix(a, 16, b);
+    case Z_M: return tix(a, b, -1);
+    default:  return tix(a, b, 16);
+  }
+}
+
+}  // namespace pipe
+
+template <bool DO_RES, bool DO_SWEEP>
+__global__ void __launch_bounds__(pipe::NTHREADS, 1)
+rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
+                      const double* __restrict__ A, const double* __restrict__ bvec,
+                      const double* __restrict__ gst, double omega,
+                      double* __restrict__ partials, SolveState* st, int fin, int iter) {
+  using namespace pipe;
+  if (*((volatile const int32_t*)&st->done)) return;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int nb = C.nb;
+  volatile int* abort_flag = &S.abort_flag;
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&S.full[s], 1);
+      mbar_init(&S.empty[s], CONSUMER_WARPS);
+    }
+    mbar_init(&S.xfull, 1);
+    mbar_init(&S.xempty, 1);
+    mbar_init(&S.gfull, NGATHER);
+    mbar_init(&S.gempty, 1);
+    S.abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (tid < GATHER0) {
+    // ------------------------------------------------------------ producer
+    if (tid == 0) {
+      uint32_t g = 0;   // chunks issued
+      uint32_t nx = 0;  // x copies issued
+      bool ok = true;
+      int n = 0;
+      if (blockIdx.x < nb) {
+        ++nx;
+        mbar_expect_tx(&S.xfull, BLOCK_CELLS * 8);
+        bulk_g2s(S.xstage, xin + (size_t)blockIdx.x * BLOCK_CELLS, BLOCK_CELLS * 8, &S.xfull);
+      }
+      for (int blk = blockIdx.x; blk < nb && ok; blk += gridDim.x, ++n) {
+        const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+        const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
+        for (int j = 0; j < CHUNKS && ok; ++j) {
+          const int s = g % STAGES;
+          const uint32_t u = g / STAGES;
+          if (!(ok = mbar_wait(&S.empty[s], (u & 1) ^ 1, abort_flag))) break;
+          ++g;
+          mbar_expect_tx(&S.full[s], CHUNK_BYTES);
+          const int off = (j >> 3) * HALF_CELLS + (j & 7) * CHUNK_CELLS;  // colour, plane pair
+          for (int a = 0; a < 7; ++a)
+            bulk_g2s(S.ring[s][a], Ab + (size_t)a * BLOCK_CELLS + off, CHUNK_CELLS * 8, &S.full[s]);
+          bulk_g2s(S.ring[s][7], bb + off, CHUNK_CELLS * 8, &S.full[s]);
+          if (j == 1 && blk + (int)gridDim.x < nb) {
+            // next block's x once the consumers have taken this block's
+            if (!(ok = mbar_wait(&S.xempty, n & 1, abort_flag))) break;
+            ++nx;
+            mbar_expect_tx(&S.xfull, BLOCK_CELLS * 8);
+            bulk_g2s(S.xstage, xin + (size_t)(blk + gridDim.x) * BLOCK_CELLS, BLOCK_CELLS * 8,
+                     &S.xfull);
+          }
+        }
+      }
+      // Drain: every slot's last armed phase must complete before the CTA
+      // may exit (copies in flight write into this CTA's shared memory).
+      for (int s = 0; s < STAGES; ++s) {
+        const uint32_t issued = (g > (uint32_t)s) ? (g - 1 - s) / STAGES + 1 : 0;
+        if (issued) {
+          for (uint32_t i = 0; i < WAIT_LIMIT; ++i)
+            if (mbar_try_wait(&S.full[s], (issued - 1) & 1)) break;
+        }
+      }
+      if (nx) {  // and the last x copy
+        for (uint32_t i = 0; i < WAIT_LIMIT; ++i)
+          if (mbar_try_wait(&S.xfull, (nx - 1) & 1)) break;
+      }
+    }
+  } else if (tid < CONS0) {
+    // ----------------------------------------------------------- gatherers
+    const int gt = tid - GATHER0;
+    int n = 0;
+    for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++n) {
+      if (n > 0 && !mbar_wait(&S.gempty, (n - 1) & 1, abort_flag)) break;
+      const double dx = C.dx[blk];
+#pragma unroll 4
+      for (int r = 0; r < 6 * FACE_CELLS / NGATHER; ++r) {
+        const int p = gt + NGATHER * r;
+        const int f = p >> 8, ab = p & 255;
+        double v;
+        if (gst) {
+          v = __ldg(gst + (size_t)blk * 6 * FACE_CELLS + p);
+        } else {
+          const FaceNbr nbf = C.nbr[blk * 6 + f];
+          v = guide_value(xin, blk, f, ab & 15, ab >> 4, 1, nbf, C.bc, dx);
+        }
+        S.gbuf[p] = v;
+      }
+      mbar_arrive(&S.gfull);
+    }
+  } else {
+    // ----------------------------------------------------------- consumers
+    // Every consumer executes the same sequence of named barriers, warp
+    // syncs and shuffles whatever happens; only the work is predicated on
+    // 'live', which drops when a wait gives up.
+    const int ct = tid - CONS0;
+    const int lane = ct & 31, warp = ct >> 5;
+    uint32_t g = 0;
+    int n = 0;
+    bool live = true;
+    for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++n) {
+      live = live && mbar_wait(&S.xfull, n & 1, abort_flag);
+      if (live) {
+#pragma unroll 4
+        for (int m = 0; m < 16; ++m) {
+          const int s = ct + 256 * m;
+          int i, j, k;
+          cell_of(s, i, j, k);
+          S.tile_old[tix(i, j, k)] = S.xstage[s];
+        }
+      }
+      live = live && mbar_wait(&S.gfull, n & 1, abort_flag);
+      if (live) {
+        const int a = ct & 15, b = ct >> 4;
+        for (int f = 0; f < 6; ++f) {
+          const double v = S.gbuf[f * FACE_CELLS + ct];
+          const int t = guide_tix(f, a, b);
+          S.tile_old[t] = v;
+          S.tile_new[t] = v;
+        }
+      }
+      consumer_sync();
+      if (ct == 0 && live) {
+        mbar_arrive(&S.xempty);
+        mbar_arrive(&S.gempty);
+      }
+      double* xo = xout + (size_t)blk * BLOCK_CELLS;
+      double acc[2] = {0.0, 0.0};
+      // colour 0: neighbours are colour 1 (unchanged); update into tile_new
+      for (int m = 0; m < 8; ++m, ++g) {
+        const int s = g % STAGES;
+        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag);
+        double ap = 1.0, aw = 0.0, ae = 0.0, as = 0.0, an = 0.0, ab = 0.0, at = 0.0, bv = 0.0;
+        if (live) {
+          ap = S.ring[s][0][ct]; aw = S.ring[s][1][ct]; ae = S.ring[s][2][ct];
+          as = S.ring[s][3][ct]; an = S.ring[s][4][ct]; ab = S.ring[s][5][ct];
+          at = S.ring[s][6][ct]; bv = S.ring[s][7][ct];
+        }
+        __syncwarp();
+        if (lane == 0 && live) mbar_arrive(&S.empty[s]);
+        if (!live) continue;
+        const int q = m * CHUNK_CELLS + ct;
+        int i, j, k;
+        cell_of(q, i, j, k);
+        const int t = tix(i, j, k);
+        const double* T = S.tile_old;
+        const double rs = bv - aw * T[t - 1] - ae * T[t + 1] - as * T[t - TW] - an * T[t + TW] -
+                          ab * T[t - TP] - at * T[t + TP];
+        const double xp = T[t];
+        if (DO_RES) {
+          const double r = rs - ap * xp;
+          acc[0] += r * r;
+        }
+        if (DO_SWEEP) {
+          const double xt = rs / ap;
+          const double xn = xp - omega * (xp - xt);
+          S.tile_new[t] = xn;
+          xo[q] = xn;
+        }
+      }
+      consumer_sync();
+      // colour 1: residual against the old colour-0 values, update against the new
+      for (int m = 0; m < 8; ++m, ++g) {
+        const int s = g % STAGES;
+        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag);
+        double ap = 1.0, aw = 0.0, ae = 0.0, as = 0.0, an = 0.0, ab = 0.0, at = 0.0, bv = 0.0;
+        if (live) {
+          ap = S.ring[s][0][ct]; aw = S.ring[s][1][ct]; ae = S.ring[s][2][ct];
+          as = S.ring[s][3][ct]; an = S.ring[s][4][ct]; ab = S.ring[s][5][ct];
+          at = S.ring[s][6][ct]; bv = S.ring[s][7][ct];
+        }
+        __syncwarp();
+        if (lane == 0 && live) mbar_arrive(&S.empty[s]);
+        if (!live) continue;
+        const int q = HALF_CELLS + m * CHUNK_CELLS + ct;
+        int i, j, k;
+        cell_of(q, i, j, k);
+        const int t = tix(i, j, k);
+        const double xp = S.tile_old[t];
+        if (DO_RES) {
+          const double* T = S.tile_old;
+          const double r = bv - aw * T[t - 1] - ae * T[t + 1] - as * T[t - TW] - an * T[t + TW] -
+                           ab * T[t - TP] - at * T[t + TP] - ap * xp;
+          acc[1] += r * r;
+        }
+        if (DO_SWEEP) {
+          const double* T = S.tile_new;
+          const double rs = bv - aw * T[t - 1] - ae * T[t + 1] - as * T[t - TW] - an * T[t + TW] -
+                            ab * T[t - TP] - at * T[t + TP];
+          const double xt = rs / ap;
+          xo[q] = xp - omega * (xp - xt);
+        }
+      }
+      if (DO_RES) {
+        double v = acc[0] + acc[1];
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) S.ws[warp] = v;
+        consumer_sync();
+        if (ct == 0 && live) {
+          double sum = 0.0;
+#pragma unroll
+          for (int w = 0; w < 8; ++w) sum += S.ws[w];
+          __stcg(partials + blk, sum);
+        }
+      }
+      consumer_sync();  // tiles are rebuilt for the next block
+    }
+  }
+
+  __syncthreads();
+  if (*abort_flag) {
+    if (tid == 0) {
+      atomicExch(&st->status, 3);
+      atomicExch(&st->done, 1);
+    }
+    return;
+  }
+  if (!DO_RES) return;
+  if (tid == CONS0) {
+    __threadfence();
+    const unsigned t = atomicAdd(&st->ticket, 1u);
+    S.last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!S.last || tid < CONS0) return;
+  __threadfence();
+  const int ct = tid - CONS0;
+  double Ssum = 0.0;
+  for (int b = ct; b < nb; b += 256) Ssum += __ldcg(partials + b);
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) Ssum += __shfl_xor_sync(0xffffffffu, Ssum, off);
+  if ((ct & 31) == 0) S.ws[ct >> 5] = Ssum;
+  consumer_sync();
+  if (ct == 0) {
+    double total = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) total += S.ws[w];
+    finalize(st, total, fin, iter);
+    st->ticket = 0;
+    __threadfence();
+  }
+}
+
+namespace {
+int g_sm_count = 0;
+bool g_attr_set[4] = {false, false, false, false};
+
+template <bool R, bool W>
+void launch_one(cudaStream_t s, const KCtx& C, const double* xin, double* xout, const double* A,
+                const double* b, const double* gst, double omega, double* partials,
+                SolveState* st, int fin, int iter, int slot) {
+  const size_t smem = sizeof(pipe::Smem);
+  if (!g_attr_set[slot]) {
+    cudaFuncSetAttribute(rbgs_pipelined_kernel<R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    g_attr_set[slot] = true;
+  }
+  const int grid = C.nb < g_sm_count ? C.nb : g_sm_count;
+  rbgs_pipelined_kernel<R, W><<<grid, pipe::NTHREADS, smem, s>>>(C, xin, xout, A, b, gst, omega,
+                                                                 partials, st, fin, iter);
+}
+}  // namespace
+
+void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
+                 double* xout, const double* A, const double* b, const double* gst,
+                 double omega, double* partials, SolveState* st, int fin, int iter) {
+  if (g_sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 1;
+  }
+  if (res && sweep)
+    launch_one<true, true>(s, C, xin, xout, A, b, gst, omega, partials, st, fin, iter, 0);
+  else if (sweep)
+    launch_one<false, true>(s, C, xin, xout, A, b, gst, omega, partials, st, fin, iter, 1);
+  else
+    launch_one<true, false>(s, C, xin, xout, A, b, gst, omega, partials, st, fin, iter, 2);
+}
+
+size_t rbgs_pipelined_smem_bytes() { return sizeof(pipe::Smem); }
+
+}  // namespace ffvgpu
