@@ -68,7 +68,7 @@ struct SolveState {
   int32_t status;    // 0 ok, 2 NaN/Inf
   int32_t count_max;
   uint32_t ticket;   // last-block-done counter of the current reduction
-  int32_t pad;
+  int32_t timeout_where;  // roles whose bounded wait gave up (1 producer, 2 gatherer, 4 consumer)
   double* hist;      // device residual history [count_max] or null
 };
 

@@ -315,6 +315,19 @@ ffvgpu_status explicit_neighbors(ffvgpu_pool* P, const ffvgpu_grid_desc* d) {
   return FFVGPU_OK;
 }
 
+ffvgpu_status solve_status(const SolveState& h, const ffvgpu_iter_params* prm, int N, int count) {
+  if (h.status == 3) {
+    g_last_error = "a bounded device wait gave up (roles " + std::to_string(h.timeout_where) + ")";
+    return FFVGPU_TIMEOUT;
+  }
+  if (h.status == 2) {
+    g_last_error = "residual is NaN or Inf";
+    return FFVGPU_NAN_DETECTED;
+  }
+  if (prm->epsilon > 0.0 && count > N) return FFVGPU_NOT_CONVERGED;
+  return FFVGPU_OK;
+}
+
 int64_t interior_bytes(const ffvgpu_pool* P, int words) {
   return (int64_t)P->nb * (int64_t)BC * 8 * words;
 }
@@ -617,6 +630,7 @@ ffvgpu_status ffvgpu_calc_r2(ffvgpu_pool* P, double* rr) {
   SolveState h;
   if ((s = read_state(P, &h))) return s;
   *rr = h.rr;
+  if (h.status == 3) return bad("a bounded device wait gave up");
   return FFVGPU_OK;
 }
 
@@ -713,12 +727,7 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
     CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
   }
   if (res) *res = R;
-  if (h.status == 2) {
-    g_last_error = "residual is NaN or Inf";
-    return FFVGPU_NAN_DETECTED;
-  }
-  if (prm->epsilon > 0.0 && h.count > N) return FFVGPU_NOT_CONVERGED;
-  return FFVGPU_OK;
+  return solve_status(h, prm, N, R.count);
 }
 
 // FFVILS::CG (src/FFV/FFVILS.h:661-791) with Jacobi_PreConditioner
@@ -821,12 +830,7 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
       CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
   }
   if (res) *res = R;
-  if (h.status == 2) {
-    g_last_error = "residual is NaN or Inf";
-    return FFVGPU_NAN_DETECTED;
-  }
-  if (prm->epsilon > 0.0 && R.count > N) return FFVGPU_NOT_CONVERGED;
-  return FFVGPU_OK;
+  return solve_status(h, prm, N, R.count);
 }
 
 }  // extern "C"

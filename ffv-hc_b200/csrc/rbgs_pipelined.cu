@@ -48,7 +48,9 @@ constexpr int GATHER0 = 32 * PRODUCER_WARPS;
 constexpr int CONS0 = GATHER0 + 32 * GATHER_WARPS;
 constexpr int NTHREADS = CONS0 + 32 * CONSUMER_WARPS;  // 416
 constexpr int NGATHER = 32 * GATHER_WARPS;
-constexpr uint32_t WAIT_LIMIT = 1u << 22;
+constexpr uint64_t WAIT_NS = 4000000000ull;  // a wait gives up after 4 s
+constexpr uint32_t DRAIN_LIMIT = 1u << 24;    // polls while draining copies in flight
+enum { ROLE_PRODUCER = 1, ROLE_GATHER = 2, ROLE_CONSUMER = 4 };
 
 struct __align__(128) Smem {
   double ring[STAGES][NARR][CHUNK_CELLS];  // 64 KB
@@ -87,14 +89,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait; false when it gave up or another role aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
-  for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait; false when it gave up (recording its role) or another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag,
+                                          int role) {
+  if (mbar_try_wait(b, parity)) return true;
+  const uint64_t t0 = now_ns();
+  for (;;) {
     if (mbar_try_wait(b, parity)) return true;
     if (*abort_flag) return false;
+    if (now_ns() - t0 > WAIT_NS) {
+      atomicOr((int*)abort_flag, role);
+      return false;
+    }
   }
-  *abort_flag = 1;
-  return false;
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
@@ -102,6 +114,19 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
           sa(dst)),
       "l"(src), "r"(bytes), "r"(sa(bar))
       : "memory");
+}
+// Hands a ring slot back to the producer.  The slot's next contents arrive
+// by TMA (the async proxy), so each thread first waits for its loads of the
+// slot to land in registers and orders them before the async-proxy writes
+// with a proxy fence; then one lane per warp arrives on the slot's barrier.
+// Without this, a refill can overwrite a slot that a lane is still reading.
+__device__ __forceinline__ void release_slot(uint64_t* bar, int lane, bool live, double a0,
+                                             double a1, double a2, double a3, double a4,
+                                             double a5, double a6, double a7) {
+  asm volatile("" ::"d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(a4), "d"(a5), "d"(a6), "d"(a7));
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncwarp();
+  if (lane == 0 && live) mbar_arrive(bar);
 }
 __device__ __forceinline__ void consumer_sync() {
   asm volatile("bar.sync 1, %0;" ::"n"(32 * CONSUMER_WARPS) : "memory");
@@ -167,7 +192,7 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
         for (int j = 0; j < CHUNKS && ok; ++j) {
           const int s = g % STAGES;
           const uint32_t u = g / STAGES;
-          if (!(ok = mbar_wait(&S.empty[s], (u & 1) ^ 1, abort_flag))) break;
+          if (!(ok = mbar_wait(&S.empty[s], (u & 1) ^ 1, abort_flag, ROLE_PRODUCER))) break;
           ++g;
           mbar_expect_tx(&S.full[s], CHUNK_BYTES);
           const int off = (j >> 3) * HALF_CELLS + (j & 7) * CHUNK_CELLS;  // colour, plane pair
@@ -176,7 +201,7 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
           bulk_g2s(S.ring[s][7], bb + off, CHUNK_CELLS * 8, &S.full[s]);
           if (j == 1 && blk + (int)gridDim.x < nb) {
             // next block's x once the consumers have taken this block's
-            if (!(ok = mbar_wait(&S.xempty, n & 1, abort_flag))) break;
+            if (!(ok = mbar_wait(&S.xempty, n & 1, abort_flag, ROLE_PRODUCER))) break;
             ++nx;
             mbar_expect_tx(&S.xfull, BLOCK_CELLS * 8);
             bulk_g2s(S.xstage, xin + (size_t)(blk + gridDim.x) * BLOCK_CELLS, BLOCK_CELLS * 8,
@@ -189,12 +214,12 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       for (int s = 0; s < STAGES; ++s) {
         const uint32_t issued = (g > (uint32_t)s) ? (g - 1 - s) / STAGES + 1 : 0;
         if (issued) {
-          for (uint32_t i = 0; i < WAIT_LIMIT; ++i)
+          for (uint32_t i = 0; i < DRAIN_LIMIT; ++i)
             if (mbar_try_wait(&S.full[s], (issued - 1) & 1)) break;
         }
       }
       if (nx) {  // and the last x copy
-        for (uint32_t i = 0; i < WAIT_LIMIT; ++i)
+        for (uint32_t i = 0; i < DRAIN_LIMIT; ++i)
           if (mbar_try_wait(&S.xfull, (nx - 1) & 1)) break;
       }
     }
@@ -203,7 +228,7 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
     const int gt = tid - GATHER0;
     int n = 0;
     for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++n) {
-      if (n > 0 && !mbar_wait(&S.gempty, (n - 1) & 1, abort_flag)) break;
+      if (n > 0 && !mbar_wait(&S.gempty, (n - 1) & 1, abort_flag, ROLE_GATHER)) break;
       const double dx = C.dx[blk];
 #pragma unroll 4
       for (int r = 0; r < 6 * FACE_CELLS / NGATHER; ++r) {
@@ -231,7 +256,7 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
     int n = 0;
     bool live = true;
     for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++n) {
-      live = live && mbar_wait(&S.xfull, n & 1, abort_flag);
+      live = live && mbar_wait(&S.xfull, n & 1, abort_flag, ROLE_CONSUMER);
       if (live) {
 #pragma unroll 4
         for (int m = 0; m < 16; ++m) {
@@ -241,7 +266,7 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
           S.tile_old[tix(i, j, k)] = S.xstage[s];
         }
       }
-      live = live && mbar_wait(&S.gfull, n & 1, abort_flag);
+      live = live && mbar_wait(&S.gfull, n & 1, abort_flag, ROLE_CONSUMER);
       if (live) {
         const int a = ct & 15, b = ct >> 4;
         for (int f = 0; f < 6; ++f) {
@@ -251,6 +276,8 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
           S.tile_new[t] = v;
         }
       }
+      // the staging buffer is refilled by TMA: order these reads first
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       consumer_sync();
       if (ct == 0 && live) {
         mbar_arrive(&S.xempty);
@@ -261,15 +288,14 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       // colour 0: neighbours are colour 1 (unchanged); update into tile_new
       for (int m = 0; m < 8; ++m, ++g) {
         const int s = g % STAGES;
-        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag);
+        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
         double ap = 1.0, aw = 0.0, ae = 0.0, as = 0.0, an = 0.0, ab = 0.0, at = 0.0, bv = 0.0;
         if (live) {
           ap = S.ring[s][0][ct]; aw = S.ring[s][1][ct]; ae = S.ring[s][2][ct];
           as = S.ring[s][3][ct]; an = S.ring[s][4][ct]; ab = S.ring[s][5][ct];
           at = S.ring[s][6][ct]; bv = S.ring[s][7][ct];
         }
-        __syncwarp();
-        if (lane == 0 && live) mbar_arrive(&S.empty[s]);
+        release_slot(&S.empty[s], lane, live, ap, aw, ae, as, an, ab, at, bv);
         if (!live) continue;
         const int q = m * CHUNK_CELLS + ct;
         int i, j, k;
@@ -294,15 +320,14 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       // colour 1: residual against the old colour-0 values, update against the new
       for (int m = 0; m < 8; ++m, ++g) {
         const int s = g % STAGES;
-        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag);
+        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
         double ap = 1.0, aw = 0.0, ae = 0.0, as = 0.0, an = 0.0, ab = 0.0, at = 0.0, bv = 0.0;
         if (live) {
           ap = S.ring[s][0][ct]; aw = S.ring[s][1][ct]; ae = S.ring[s][2][ct];
           as = S.ring[s][3][ct]; an = S.ring[s][4][ct]; ab = S.ring[s][5][ct];
           at = S.ring[s][6][ct]; bv = S.ring[s][7][ct];
         }
-        __syncwarp();
-        if (lane == 0 && live) mbar_arrive(&S.empty[s]);
+        release_slot(&S.empty[s], lane, live, ap, aw, ae, as, an, ab, at, bv);
         if (!live) continue;
         const int q = HALF_CELLS + m * CHUNK_CELLS + ct;
         int i, j, k;
@@ -343,6 +368,7 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
   __syncthreads();
   if (*abort_flag) {
     if (tid == 0) {
+      atomicOr(&st->timeout_where, *abort_flag);
       atomicExch(&st->status, 3);
       atomicExch(&st->done, 1);
     }

@@ -9,6 +9,10 @@
 #include <cstdint>
 #include <vector>
 
+using std::fabs;
+using std::isinf;
+using std::isnan;
+using std::sqrt;
 #define __device__
 #define __host__
 #define __forceinline__ inline
