@@ -112,6 +112,86 @@ static __device__ __noinline__ double guide_value(const double* __restrict__ x, 
   }
 }
 
+// Two guide cells (layer 1) of the same face, positions p0 and p1 in
+// [0, 256) (p = v*16 + u), with every load of both issued before any is
+// used: the batched form of guide_value for the pipelined kernels.  Same
+// expressions, same evaluation order, same results as guide_value.
+__device__ __forceinline__ void guide_pair(const double* __restrict__ x, int blk, int face,
+                                           int p0, int p1, const FaceNbr& nb, const BCSet& bc,
+                                           double dx, double& v0, double& v1) {
+  const int axis = face >> 1;
+  const bool plus = face & 1;
+  const int ta = (axis == 0) ? 1 : 0, tb = (axis == 2) ? 1 : 2;
+  int g0[3], g1[3];
+  g0[ta] = p0 & 15; g0[tb] = p0 >> 4; g0[axis] = plus ? 16 : -1;
+  g1[ta] = p1 & 15; g1[tb] = p1 >> 4; g1[axis] = plus ? 16 : -1;
+  if (nb.kind == NB_SAME) {
+    g0[axis] = g1[axis] = plus ? 0 : 15;
+    v0 = ld(x, nb.id[0], g0[0], g0[1], g0[2]);
+    v1 = ld(x, nb.id[0], g1[0], g1[1], g1[2]);
+    return;
+  }
+  if (nb.kind == NB_COARSE) {
+    int f0[3], f1[3];
+    f0[ta] = g0[ta] + 1 + 16 * nb.so_u; f0[tb] = g0[tb] + 1 + 16 * nb.so_v;
+    f1[ta] = g1[ta] + 1 + 16 * nb.so_u; f1[tb] = g1[tb] + 1 + 16 * nb.so_v;
+    f0[axis] = f1[axis] = plus ? 1 : 32;
+    int i0, j0, k0, i1, j1, k1;
+    double r0, s0, t0, r1, s1, t1;
+    intp_index(f0[0], 16, i0, r0); intp_index(f0[1], 16, j0, s0); intp_index(f0[2], 16, k0, t0);
+    intp_index(f1[0], 16, i1, r1); intp_index(f1[1], 16, j1, s1); intp_index(f1[2], 16, k1, t1);
+    --i0; --j0; --k0; --i1; --j1; --k1;
+    const int c = nb.id[0];
+    const double a0 = ld(x, c, i0, j0, k0), a1 = ld(x, c, i0 + 1, j0, k0);
+    const double a2 = ld(x, c, i0, j0 + 1, k0), a3 = ld(x, c, i0, j0, k0 + 1);
+    const double a4 = ld(x, c, i0, j0 + 1, k0 + 1), a5 = ld(x, c, i0 + 1, j0, k0 + 1);
+    const double a6 = ld(x, c, i0 + 1, j0 + 1, k0), a7 = ld(x, c, i0 + 1, j0 + 1, k0 + 1);
+    const double b0 = ld(x, c, i1, j1, k1), b1 = ld(x, c, i1 + 1, j1, k1);
+    const double b2 = ld(x, c, i1, j1 + 1, k1), b3 = ld(x, c, i1, j1, k1 + 1);
+    const double b4 = ld(x, c, i1, j1 + 1, k1 + 1), b5 = ld(x, c, i1 + 1, j1, k1 + 1);
+    const double b6 = ld(x, c, i1 + 1, j1 + 1, k1), b7 = ld(x, c, i1 + 1, j1 + 1, k1 + 1);
+    // nnn, pnn, npn, nnp, npp, pnp, ppn, ppp = a0..a7
+    v0 = (1.0 - t0) * ((1.0 - s0) * ((1.0 - r0) * a0 + r0 * a1) + s0 * ((1.0 - r0) * a2 + r0 * a6)) +
+         t0 * ((1.0 - s0) * ((1.0 - r0) * a3 + r0 * a5) + s0 * ((1.0 - r0) * a4 + r0 * a7));
+    v1 = (1.0 - t1) * ((1.0 - s1) * ((1.0 - r1) * b0 + r1 * b1) + s1 * ((1.0 - r1) * b2 + r1 * b6)) +
+         t1 * ((1.0 - s1) * ((1.0 - r1) * b3 + r1 * b5) + s1 * ((1.0 - r1) * b4 + r1 * b7));
+    return;
+  }
+  if (nb.kind == NB_FINE) {
+    const int fb0 = nb.id[(g0[ta] >> 3) + 2 * (g0[tb] >> 3)];
+    const int fb1 = nb.id[(g1[ta] >> 3) + 2 * (g1[tb] >> 3)];
+    int l0[3], l1[3];
+    l0[ta] = 2 * (g0[ta] & 7); l0[tb] = 2 * (g0[tb] & 7);
+    l1[ta] = 2 * (g1[ta] & 7); l1[tb] = 2 * (g1[tb] & 7);
+    l0[axis] = l1[axis] = plus ? 0 : 14;
+    const int i0 = l0[0], j0 = l0[1], k0 = l0[2], i1 = l1[0], j1 = l1[1], k1 = l1[2];
+    const double a0 = ld(x, fb0, i0, j0, k0), a1 = ld(x, fb0, i0 + 1, j0, k0);
+    const double a2 = ld(x, fb0, i0, j0 + 1, k0), a3 = ld(x, fb0, i0, j0, k0 + 1);
+    const double a4 = ld(x, fb0, i0, j0 + 1, k0 + 1), a5 = ld(x, fb0, i0 + 1, j0, k0 + 1);
+    const double a6 = ld(x, fb0, i0 + 1, j0 + 1, k0), a7 = ld(x, fb0, i0 + 1, j0 + 1, k0 + 1);
+    const double b0 = ld(x, fb1, i1, j1, k1), b1 = ld(x, fb1, i1 + 1, j1, k1);
+    const double b2 = ld(x, fb1, i1, j1 + 1, k1), b3 = ld(x, fb1, i1, j1, k1 + 1);
+    const double b4 = ld(x, fb1, i1, j1 + 1, k1 + 1), b5 = ld(x, fb1, i1 + 1, j1, k1 + 1);
+    const double b6 = ld(x, fb1, i1 + 1, j1 + 1, k1), b7 = ld(x, fb1, i1 + 1, j1 + 1, k1 + 1);
+    v0 = 0.125 * (a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7);
+    v1 = 0.125 * (b0 + b1 + b2 + b3 + b4 + b5 + b6 + b7);
+    return;
+  }
+  // outer face: bcx.f90 bc_x?_d (5-147) / bc_x?_n (294-436), layer 1
+  g0[axis] = g1[axis] = plus ? 15 : 0;
+  const double x0 = ld(x, blk, g0[0], g0[1], g0[2]);
+  const double x1 = ld(x, blk, g1[0], g1[1], g1[2]);
+  if (bc.type[face] == BC_DIRICHLET) {
+    const double xc = bc.value[face];
+    v0 = 2.0 * xc - x0;
+    v1 = 2.0 * xc - x1;
+  } else {
+    const double xc = bc.value[face] * dx;
+    v0 = plus ? (x0 + xc) : (x0 - xc);
+    v1 = plus ? (x1 + xc) : (x1 - xc);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Convergence bookkeeping run by the last CTA of a reduction.
 // ---------------------------------------------------------------------------

@@ -15,10 +15,10 @@
 //               staging buffer, and the coefficient stream -- for each
 //               colour and each pair of z planes, the 256 cells' Ap..At and
 //               b (8 x 2 KB) -- into a ring of STAGES slots;
-//   warps 1-4   gatherers: the next block's guide layer (the in-kernel
+//   warps 1-8   gatherers: the next block's guide layer (the in-kernel
 //               exchange, computed from the neighbours' interiors of x_in)
 //               into a guide buffer;
-//   warps 5-12  consumers (256 threads): build the 18^3 tile of x_in, run the
+//   warps 9-16  consumers (256 threads): build the 18^3 tile of x_in, run the
 //               colour-0 pass (residual + update written to a second tile)
 //               and the colour-1 pass (residual from the first tile, update
 //               against the second), stream x_out to global memory, and sum
@@ -43,10 +43,10 @@ constexpr int NARR = 8;              // Ap, Aw, Ae, As, An, Ab, At, b
 constexpr int CHUNK_CELLS = 256;     // one colour, two z planes
 constexpr int CHUNK_BYTES = NARR * CHUNK_CELLS * 8;
 constexpr int CHUNKS = 16;           // 8 per colour
-constexpr int PRODUCER_WARPS = 1, GATHER_WARPS = 4, CONSUMER_WARPS = 8;
+constexpr int PRODUCER_WARPS = 1, GATHER_WARPS = 8, CONSUMER_WARPS = 8;
 constexpr int GATHER0 = 32 * PRODUCER_WARPS;
 constexpr int CONS0 = GATHER0 + 32 * GATHER_WARPS;
-constexpr int NTHREADS = CONS0 + 32 * CONSUMER_WARPS;  // 416
+constexpr int NTHREADS = CONS0 + 32 * CONSUMER_WARPS;  // 544
 constexpr int NGATHER = 32 * GATHER_WARPS;
 constexpr uint64_t WAIT_NS = 4000000000ull;  // a wait gives up after 4 s
 constexpr uint32_t DRAIN_LIMIT = 1u << 24;    // polls while draining copies in flight
@@ -230,18 +230,22 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
     for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++n) {
       if (n > 0 && !mbar_wait(&S.gempty, (n - 1) & 1, abort_flag, ROLE_GATHER)) break;
       const double dx = C.dx[blk];
-#pragma unroll 4
-      for (int r = 0; r < 6 * FACE_CELLS / NGATHER; ++r) {
-        const int p = gt + NGATHER * r;
-        const int f = p >> 8, ab = p & 255;
-        double v;
+      // two groups of 128 threads take alternate faces; each thread resolves
+      // two positions of its face with all their loads in flight
+      const int grp = gt >> 7, p0 = gt & 127, p1 = p0 + 128;
+      for (int r = 0; r < 3; ++r) {
+        const int f = 2 * r + grp;
+        double v0, v1;
         if (gst) {
-          v = __ldg(gst + (size_t)blk * 6 * FACE_CELLS + p);
+          const double* gs = gst + ((size_t)blk * 6 + f) * FACE_CELLS;
+          v0 = __ldg(gs + p0);
+          v1 = __ldg(gs + p1);
         } else {
           const FaceNbr nbf = C.nbr[blk * 6 + f];
-          v = guide_value(xin, blk, f, ab & 15, ab >> 4, 1, nbf, C.bc, dx);
+          guide_pair(xin, blk, f, p0, p1, nbf, C.bc, dx, v0, v1);
         }
-        S.gbuf[p] = v;
+        S.gbuf[f * FACE_CELLS + p0] = v0;
+        S.gbuf[f * FACE_CELLS + p1] = v1;
       }
       mbar_arrive(&S.gfull);
     }
@@ -266,6 +270,11 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
           S.tile_old[tix(i, j, k)] = S.xstage[s];
         }
       }
+      // the staging buffer is refilled by TMA: order these reads first, then
+      // hand it back before waiting for the guide layer
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      consumer_sync();
+      if (ct == 0 && live) mbar_arrive(&S.xempty);
       live = live && mbar_wait(&S.gfull, n & 1, abort_flag, ROLE_CONSUMER);
       if (live) {
         const int a = ct & 15, b = ct >> 4;
@@ -276,13 +285,8 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
           S.tile_new[t] = v;
         }
       }
-      // the staging buffer is refilled by TMA: order these reads first
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       consumer_sync();
-      if (ct == 0 && live) {
-        mbar_arrive(&S.xempty);
-        mbar_arrive(&S.gempty);
-      }
+      if (ct == 0 && live) mbar_arrive(&S.gempty);
       double* xo = xout + (size_t)blk * BLOCK_CELLS;
       double acc[2] = {0.0, 0.0};
       // colour 0: neighbours are colour 1 (unchanged); update into tile_new

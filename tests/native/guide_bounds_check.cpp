@@ -68,6 +68,25 @@ int main() {
             // a constant field must be reproduced by same/c2f/f2c exactly
             if (F.kind != NB_OUTER && val != 1.0) ++nonfinite;
           }
+  // guide_pair (the batched form used by the pipelined kernel) must equal
+  // guide_value bit for bit on arbitrary data
+  long pair_mismatch = 0;
+  uint64_t st = 88172645463325252ull;
+  for (double& v : x) {
+    st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+    v = (double)(int64_t)(st >> 11) * 1.0e-15 - 4.0;
+  }
+  for (int b = 0; b < nb; ++b)
+    for (int f = 0; f < 6; ++f)
+      for (int p = 0; p < 128; ++p) {
+        const FaceNbr& F = nbr[b * 6 + f];
+        double v0, v1;
+        guide_pair(x.data(), b, f, p, p + 128, F, bc, 0.1, v0, v1);
+        const double w0 = guide_value(x.data(), b, f, p & 15, p >> 4, 1, F, bc, 0.1);
+        const double w1 = guide_value(x.data(), b, f, (p + 128) & 15, (p + 128) >> 4, 1, F, bc, 0.1);
+        pair_mismatch += (v0 != w0) + (v1 != w1);
+      }
+  nonfinite += pair_mismatch;
   // sidx must be a bijection onto [0, 4096)
   std::vector<int> seen(BLOCK_CELLS, 0);
   for (int k = 0; k < 16; ++k)
