@@ -192,6 +192,31 @@ __device__ __forceinline__ void guide_pair(const double* __restrict__ x, int blk
   }
 }
 
+// The six stencil neighbours of cell q (in [0, 2048)) of colour c, read from
+// the other colour's half O of a colour-split block (every face neighbour
+// has the other colour), or from the guide layer G ([face][v][u]) where the
+// neighbour lies outside the block.
+struct Nbrs {
+  double w, e, s, n, b, t;
+};
+__device__ __forceinline__ Nbrs split_neighbours(const double* __restrict__ O,
+                                           const double* __restrict__ G, int q, int c) {
+  const int ih = q & 7, j = (q >> 3) & 15, k = q >> 7;
+  const int p = (j + k + c) & 1;
+  const int i = 2 * ih + p;
+  Nbrs r;
+  const double ow = O[max(q - 1 + p, 0)], oe = O[min(q + p, HALF_CELLS - 1)];
+  const double os = O[max(q - 8, 0)], on = O[min(q + 8, HALF_CELLS - 1)];
+  const double ob = O[max(q - 128, 0)], ot = O[min(q + 128, HALF_CELLS - 1)];
+  r.w = (i == 0) ? G[0 * FACE_CELLS + j + 16 * k] : ow;
+  r.e = (i == 15) ? G[1 * FACE_CELLS + j + 16 * k] : oe;
+  r.s = (j == 0) ? G[2 * FACE_CELLS + i + 16 * k] : os;
+  r.n = (j == 15) ? G[3 * FACE_CELLS + i + 16 * k] : on;
+  r.b = (k == 0) ? G[4 * FACE_CELLS + i + 16 * j] : ob;
+  r.t = (k == 15) ? G[5 * FACE_CELLS + i + 16 * j] : ot;
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // Convergence bookkeeping run by the last CTA of a reduction.
 // ---------------------------------------------------------------------------

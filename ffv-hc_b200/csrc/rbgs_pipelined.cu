@@ -11,20 +11,23 @@
 // One CTA per SM walks blocks blockIdx.x, blockIdx.x + gridDim.x, ...  Its
 // warps have fixed roles:
 //   warp 0      producer: one lane issues cp.async.bulk copies (global ->
-//               shared, completion on mbarriers): the next block's x into a
-//               staging buffer, and the coefficient stream -- for each
-//               colour and each pair of z planes, the 256 cells' Ap..At and
-//               b (8 x 2 KB) -- into a ring of STAGES slots;
-//   warps 1-8   gatherers: the next block's guide layer (the in-kernel
-//               exchange, computed from the neighbours' interiors of x_in)
-//               into a guide buffer;
-//   warps 9-16  consumers (256 threads): build the 18^3 tile of x_in, run the
-//               colour-0 pass (residual + update written to a second tile)
-//               and the colour-1 pass (residual from the first tile, update
-//               against the second), stream x_out to global memory, and sum
-//               the residual.
-// Every wait on an mbarrier is bounded; a wait that gives up raises the
-// CTA's abort flag, every role leaves its loop, the producer drains the
+//               shared, completion on mbarriers): each block's x (32 KB, the
+//               colour-split layout of HBM, copied as is) into one of two
+//               tile buffers a block ahead, and the coefficient stream -- for
+//               each colour and each pair of z planes, the 256 cells'
+//               Ap..At and b (8 x 2 KB) -- into a ring of STAGES slots;
+//   warps 1-8   gatherers: the guide layer of the block after the current
+//               one (the in-kernel exchange, computed from the neighbours'
+//               interiors of x_in) into one of two guide buffers;
+//   warps 9-16  consumers (256 threads): the colour-0 pass (residual, and
+//               the update kept in a colour-0 buffer and streamed to x_out),
+//               then the colour-1 pass (residual against the old colour-0
+//               values, update against the new), and the residual sum.
+// Stencil neighbours are read straight from the colour-split tile: every
+// neighbour of a cell of one colour lies in the other colour's half, and
+// cells on the block surface take the guide buffer instead.
+// Every wait on an mbarrier is bounded in time; a wait that gives up raises
+// the CTA's abort flag, every role leaves its loop, the producer drains the
 // copies it has in flight, and the solver state reports TIMEOUT.
 #include <cfloat>
 #include <cstdint>
@@ -37,12 +40,12 @@ namespace ffvgpu {
 
 namespace pipe {
 
-constexpr int TW = 18, TP = TW * TW, TILE = TW * TW * TW;
-constexpr int STAGES = 4;
+constexpr int STAGES = 7;
 constexpr int NARR = 8;              // Ap, Aw, Ae, As, An, Ab, At, b
 constexpr int CHUNK_CELLS = 256;     // one colour, two z planes
 constexpr int CHUNK_BYTES = NARR * CHUNK_CELLS * 8;
 constexpr int CHUNKS = 16;           // 8 per colour
+constexpr int X_ISSUE_AT = 8;        // chunk of block m after which x(m+1) is issued
 constexpr int PRODUCER_WARPS = 1, GATHER_WARPS = 8, CONSUMER_WARPS = 8;
 constexpr int GATHER0 = 32 * PRODUCER_WARPS;
 constexpr int CONS0 = GATHER0 + 32 * GATHER_WARPS;
@@ -53,13 +56,12 @@ constexpr uint32_t DRAIN_LIMIT = 1u << 24;    // polls while draining copies in 
 enum { ROLE_PRODUCER = 1, ROLE_GATHER = 2, ROLE_CONSUMER = 4 };
 
 struct __align__(128) Smem {
-  double ring[STAGES][NARR][CHUNK_CELLS];  // 64 KB
-  double xstage[BLOCK_CELLS];              // 32 KB
-  double tile_old[TILE];                   // 46.6 KB
-  double tile_new[TILE];                   // 46.6 KB
-  double gbuf[6 * FACE_CELLS];             // 12 KB
+  double ring[STAGES][NARR][CHUNK_CELLS];  // 112 KB
+  double xt[2][BLOCK_CELLS];               // 64 KB: x_in of the current / next block
+  double xnew0[HALF_CELLS];                // 16 KB: updated colour-0 values
+  double gbuf[2][6 * FACE_CELLS];          // 24 KB: guide layers, [face][v][u]
   uint64_t full[STAGES], empty[STAGES];
-  uint64_t xfull, xempty, gfull, gempty;
+  uint64_t xfull[2], xempty[2], gfull[2], gempty[2];
   double ws[8];
   int abort_flag;
   int last;
@@ -115,32 +117,24 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       "l"(src), "r"(bytes), "r"(sa(bar))
       : "memory");
 }
-// Hands a ring slot back to the producer.  The slot's next contents arrive
-// by TMA (the async proxy), so each thread first waits for its loads of the
-// slot to land in registers and orders them before the async-proxy writes
-// with a proxy fence; then one lane per warp arrives on the slot's barrier.
-// Without this, a refill can overwrite a slot that a lane is still reading.
+// Orders this thread's reads of shared memory before later async-proxy
+// (TMA) writes to it.  Buffers refilled by TMA must be released only after
+// it: without it a refill can overwrite data a lane is still reading.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// Hands a ring slot back to the producer: each thread waits for its loads of
+// the slot to land in registers and fences them; one lane per warp arrives.
 __device__ __forceinline__ void release_slot(uint64_t* bar, int lane, bool live, double a0,
                                              double a1, double a2, double a3, double a4,
                                              double a5, double a6, double a7) {
   asm volatile("" ::"d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(a4), "d"(a5), "d"(a6), "d"(a7));
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  fence_proxy_async();
   __syncwarp();
   if (lane == 0 && live) mbar_arrive(bar);
 }
 __device__ __forceinline__ void consumer_sync() {
   asm volatile("bar.sync 1, %0;" ::"n"(32 * CONSUMER_WARPS) : "memory");
-}
-__device__ __forceinline__ int tix(int i, int j, int k) { return (i + 1) + TW * (j + 1) + TP * (k + 1); }
-__device__ __forceinline__ int guide_tix(int f, int a, int b) {
-  switch (f) {
-    case X_M: return tix(-1, a, b);
-    case X_P: return tix(16, a, b);
-    case Y_M: return tix(a, -1, b);
-    case Y_P: return tix(a, 16, b);
-    case Z_M: return tix(a, b, -1);
-    default:  return tix(a, b, 16);
-  }
 }
 
 }  // namespace pipe
@@ -164,29 +158,31 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       mbar_init(&S.full[s], 1);
       mbar_init(&S.empty[s], CONSUMER_WARPS);
     }
-    mbar_init(&S.xfull, 1);
-    mbar_init(&S.xempty, 1);
-    mbar_init(&S.gfull, NGATHER);
-    mbar_init(&S.gempty, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&S.xfull[b], 1);
+      mbar_init(&S.xempty[b], 1);
+      mbar_init(&S.gfull[b], NGATHER);
+      mbar_init(&S.gempty[b], 1);
+    }
     S.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    fence_proxy_async();
   }
   __syncthreads();
 
   if (tid < GATHER0) {
     // ------------------------------------------------------------ producer
     if (tid == 0) {
-      uint32_t g = 0;   // chunks issued
-      uint32_t nx = 0;  // x copies issued
+      uint32_t g = 0;            // chunks issued
+      uint32_t nx[2] = {0, 0};   // x copies issued per tile buffer
       bool ok = true;
-      int n = 0;
+      int m = 0;
       if (blockIdx.x < nb) {
-        ++nx;
-        mbar_expect_tx(&S.xfull, BLOCK_CELLS * 8);
-        bulk_g2s(S.xstage, xin + (size_t)blockIdx.x * BLOCK_CELLS, BLOCK_CELLS * 8, &S.xfull);
+        ++nx[0];
+        mbar_expect_tx(&S.xfull[0], BLOCK_CELLS * 8);
+        bulk_g2s(S.xt[0], xin + (size_t)blockIdx.x * BLOCK_CELLS, BLOCK_CELLS * 8, &S.xfull[0]);
       }
-      for (int blk = blockIdx.x; blk < nb && ok; blk += gridDim.x, ++n) {
+      for (int blk = blockIdx.x; blk < nb && ok; blk += gridDim.x, ++m) {
         const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
         const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
         for (int j = 0; j < CHUNKS && ok; ++j) {
@@ -199,40 +195,44 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
           for (int a = 0; a < 7; ++a)
             bulk_g2s(S.ring[s][a], Ab + (size_t)a * BLOCK_CELLS + off, CHUNK_CELLS * 8, &S.full[s]);
           bulk_g2s(S.ring[s][7], bb + off, CHUNK_CELLS * 8, &S.full[s]);
-          if (j == 1 && blk + (int)gridDim.x < nb) {
-            // next block's x once the consumers have taken this block's
-            if (!(ok = mbar_wait(&S.xempty, n & 1, abort_flag, ROLE_PRODUCER))) break;
-            ++nx;
-            mbar_expect_tx(&S.xfull, BLOCK_CELLS * 8);
-            bulk_g2s(S.xstage, xin + (size_t)(blk + gridDim.x) * BLOCK_CELLS, BLOCK_CELLS * 8,
-                     &S.xfull);
+          if (j == X_ISSUE_AT && blk + (int)gridDim.x < nb) {
+            // x of block m+1 into the buffer block m-1 used (released by now:
+            // the consumers are in block m)
+            const int xb = (m + 1) & 1;
+            if (m >= 1 && !(ok = mbar_wait(&S.xempty[xb], ((m - 1) >> 1) & 1, abort_flag,
+                                           ROLE_PRODUCER)))
+              break;
+            ++nx[xb];
+            mbar_expect_tx(&S.xfull[xb], BLOCK_CELLS * 8);
+            bulk_g2s(S.xt[xb], xin + (size_t)(blk + gridDim.x) * BLOCK_CELLS, BLOCK_CELLS * 8,
+                     &S.xfull[xb]);
           }
         }
       }
-      // Drain: every slot's last armed phase must complete before the CTA
-      // may exit (copies in flight write into this CTA's shared memory).
+      // Drain: the last armed phase of every barrier a copy completes on must
+      // complete before the CTA may exit (copies land in its shared memory).
       for (int s = 0; s < STAGES; ++s) {
         const uint32_t issued = (g > (uint32_t)s) ? (g - 1 - s) / STAGES + 1 : 0;
-        if (issued) {
+        if (issued)
           for (uint32_t i = 0; i < DRAIN_LIMIT; ++i)
             if (mbar_try_wait(&S.full[s], (issued - 1) & 1)) break;
-        }
       }
-      if (nx) {  // and the last x copy
-        for (uint32_t i = 0; i < DRAIN_LIMIT; ++i)
-          if (mbar_try_wait(&S.xfull, (nx - 1) & 1)) break;
-      }
+      for (int b = 0; b < 2; ++b)
+        if (nx[b])
+          for (uint32_t i = 0; i < DRAIN_LIMIT; ++i)
+            if (mbar_try_wait(&S.xfull[b], (nx[b] - 1) & 1)) break;
     }
   } else if (tid < CONS0) {
     // ----------------------------------------------------------- gatherers
     const int gt = tid - GATHER0;
-    int n = 0;
-    for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++n) {
-      if (n > 0 && !mbar_wait(&S.gempty, (n - 1) & 1, abort_flag, ROLE_GATHER)) break;
+    const int grp = gt >> 7, p0 = gt & 127, p1 = p0 + 128;
+    int m = 0;
+    for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++m) {
+      const int gb = m & 1;
+      if (m >= 2 && !mbar_wait(&S.gempty[gb], ((m - 2) >> 1) & 1, abort_flag, ROLE_GATHER)) break;
       const double dx = C.dx[blk];
       // two groups of 128 threads take alternate faces; each thread resolves
       // two positions of its face with all their loads in flight
-      const int grp = gt >> 7, p0 = gt & 127, p1 = p0 + 128;
       for (int r = 0; r < 3; ++r) {
         const int f = 2 * r + grp;
         double v0, v1;
@@ -244,10 +244,10 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
           const FaceNbr nbf = C.nbr[blk * 6 + f];
           guide_pair(xin, blk, f, p0, p1, nbf, C.bc, dx, v0, v1);
         }
-        S.gbuf[f * FACE_CELLS + p0] = v0;
-        S.gbuf[f * FACE_CELLS + p1] = v1;
+        S.gbuf[gb][f * FACE_CELLS + p0] = v0;
+        S.gbuf[gb][f * FACE_CELLS + p1] = v1;
       }
-      mbar_arrive(&S.gfull);
+      mbar_arrive(&S.gfull[gb]);
     }
   } else {
     // ----------------------------------------------------------- consumers
@@ -257,40 +257,19 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
     const int ct = tid - CONS0;
     const int lane = ct & 31, warp = ct >> 5;
     uint32_t g = 0;
-    int n = 0;
+    int m = 0;
     bool live = true;
-    for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++n) {
-      live = live && mbar_wait(&S.xfull, n & 1, abort_flag, ROLE_CONSUMER);
-      if (live) {
-#pragma unroll 4
-        for (int m = 0; m < 16; ++m) {
-          const int s = ct + 256 * m;
-          int i, j, k;
-          cell_of(s, i, j, k);
-          S.tile_old[tix(i, j, k)] = S.xstage[s];
-        }
-      }
-      // the staging buffer is refilled by TMA: order these reads first, then
-      // hand it back before waiting for the guide layer
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      consumer_sync();
-      if (ct == 0 && live) mbar_arrive(&S.xempty);
-      live = live && mbar_wait(&S.gfull, n & 1, abort_flag, ROLE_CONSUMER);
-      if (live) {
-        const int a = ct & 15, b = ct >> 4;
-        for (int f = 0; f < 6; ++f) {
-          const double v = S.gbuf[f * FACE_CELLS + ct];
-          const int t = guide_tix(f, a, b);
-          S.tile_old[t] = v;
-          S.tile_new[t] = v;
-        }
-      }
-      consumer_sync();
-      if (ct == 0 && live) mbar_arrive(&S.gempty);
+    for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++m) {
+      const int xb = m & 1;
+      const uint32_t par = (m >> 1) & 1;
+      live = live && mbar_wait(&S.xfull[xb], par, abort_flag, ROLE_CONSUMER);
+      live = live && mbar_wait(&S.gfull[xb], par, abort_flag, ROLE_CONSUMER);
+      const double* T = S.xt[xb];
+      const double* G = S.gbuf[xb];
       double* xo = xout + (size_t)blk * BLOCK_CELLS;
       double acc[2] = {0.0, 0.0};
-      // colour 0: neighbours are colour 1 (unchanged); update into tile_new
-      for (int m = 0; m < 8; ++m, ++g) {
+      // colour 0: neighbours are colour 1 (unchanged)
+      for (int mm = 0; mm < 8; ++mm, ++g) {
         const int s = g % STAGES;
         live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
         double ap = 1.0, aw = 0.0, ae = 0.0, as = 0.0, an = 0.0, ab = 0.0, at = 0.0, bv = 0.0;
@@ -301,14 +280,10 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
         }
         release_slot(&S.empty[s], lane, live, ap, aw, ae, as, an, ab, at, bv);
         if (!live) continue;
-        const int q = m * CHUNK_CELLS + ct;
-        int i, j, k;
-        cell_of(q, i, j, k);
-        const int t = tix(i, j, k);
-        const double* T = S.tile_old;
-        const double rs = bv - aw * T[t - 1] - ae * T[t + 1] - as * T[t - TW] - an * T[t + TW] -
-                          ab * T[t - TP] - at * T[t + TP];
-        const double xp = T[t];
+        const int q = mm * CHUNK_CELLS + ct;
+        const Nbrs v = split_neighbours(T + HALF_CELLS, G, q, 0);
+        const double rs = bv - aw * v.w - ae * v.e - as * v.s - an * v.n - ab * v.b - at * v.t;
+        const double xp = T[q];
         if (DO_RES) {
           const double r = rs - ap * xp;
           acc[0] += r * r;
@@ -316,13 +291,13 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
         if (DO_SWEEP) {
           const double xt = rs / ap;
           const double xn = xp - omega * (xp - xt);
-          S.tile_new[t] = xn;
+          S.xnew0[q] = xn;
           xo[q] = xn;
         }
       }
       consumer_sync();
       // colour 1: residual against the old colour-0 values, update against the new
-      for (int m = 0; m < 8; ++m, ++g) {
+      for (int mm = 0; mm < 8; ++mm, ++g) {
         const int s = g % STAGES;
         live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
         double ap = 1.0, aw = 0.0, ae = 0.0, as = 0.0, an = 0.0, ab = 0.0, at = 0.0, bv = 0.0;
@@ -333,23 +308,19 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
         }
         release_slot(&S.empty[s], lane, live, ap, aw, ae, as, an, ab, at, bv);
         if (!live) continue;
-        const int q = HALF_CELLS + m * CHUNK_CELLS + ct;
-        int i, j, k;
-        cell_of(q, i, j, k);
-        const int t = tix(i, j, k);
-        const double xp = S.tile_old[t];
+        const int q = mm * CHUNK_CELLS + ct;
+        const double xp = T[HALF_CELLS + q];
         if (DO_RES) {
-          const double* T = S.tile_old;
-          const double r = bv - aw * T[t - 1] - ae * T[t + 1] - as * T[t - TW] - an * T[t + TW] -
-                           ab * T[t - TP] - at * T[t + TP] - ap * xp;
+          const Nbrs v = split_neighbours(T, G, q, 1);
+          const double r = bv - aw * v.w - ae * v.e - as * v.s - an * v.n - ab * v.b - at * v.t -
+                           ap * xp;
           acc[1] += r * r;
         }
         if (DO_SWEEP) {
-          const double* T = S.tile_new;
-          const double rs = bv - aw * T[t - 1] - ae * T[t + 1] - as * T[t - TW] - an * T[t + TW] -
-                            ab * T[t - TP] - at * T[t + TP];
+          const Nbrs v = split_neighbours(S.xnew0, G, q, 1);
+          const double rs = bv - aw * v.w - ae * v.e - as * v.s - an * v.n - ab * v.b - at * v.t;
           const double xt = rs / ap;
-          xo[q] = xp - omega * (xp - xt);
+          xo[HALF_CELLS + q] = xp - omega * (xp - xt);
         }
       }
       if (DO_RES) {
@@ -365,7 +336,13 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
           __stcg(partials + blk, sum);
         }
       }
-      consumer_sync();  // tiles are rebuilt for the next block
+      // the tile is refilled by TMA and the guide buffer by the gatherers
+      fence_proxy_async();
+      consumer_sync();
+      if (ct == 0 && live) {
+        mbar_arrive(&S.xempty[xb]);
+        mbar_arrive(&S.gempty[xb]);
+      }
     }
   }
 

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdint>
+#include <algorithm>
 #include <vector>
 
 using std::fabs;
@@ -18,6 +19,8 @@ using std::sqrt;
 #define __forceinline__ inline
 #define __noinline__
 #define __restrict__
+using std::max;
+using std::min;
 static const double* g_base = nullptr;
 static size_t g_count = 0;
 static long g_bad = 0;
@@ -87,6 +90,33 @@ int main() {
         pair_mismatch += (v0 != w0) + (v1 != w1);
       }
   nonfinite += pair_mismatch;
+  // split_neighbours (colour-split tile + guide layer) must return the same
+  // cells as direct (i, j, k) indexing with guide cells outside the block
+  long nbr_mismatch = 0;
+  {
+    std::vector<double> blkx(BLOCK_CELLS), G(6 * FACE_CELLS);
+    for (int s = 0; s < BLOCK_CELLS; ++s) blkx[s] = 1000.0 + s;
+    for (int q = 0; q < 6 * FACE_CELLS; ++q) G[q] = -1.0 - q;
+    auto at = [&](int i, int j, int k) -> double {
+      if (i < 0) return G[0 * 256 + j + 16 * k];
+      if (i > 15) return G[1 * 256 + j + 16 * k];
+      if (j < 0) return G[2 * 256 + i + 16 * k];
+      if (j > 15) return G[3 * 256 + i + 16 * k];
+      if (k < 0) return G[4 * 256 + i + 16 * j];
+      if (k > 15) return G[5 * 256 + i + 16 * j];
+      return blkx[sidx(i, j, k)];
+    };
+    for (int c = 0; c < 2; ++c)
+      for (int q = 0; q < HALF_CELLS; ++q) {
+        int i, j, k;
+        cell_of(c * HALF_CELLS + q, i, j, k);
+        const Nbrs r = split_neighbours(blkx.data() + (1 - c) * HALF_CELLS, G.data(), q, c);
+        nbr_mismatch += (r.w != at(i - 1, j, k)) + (r.e != at(i + 1, j, k)) +
+                        (r.s != at(i, j - 1, k)) + (r.n != at(i, j + 1, k)) +
+                        (r.b != at(i, j, k - 1)) + (r.t != at(i, j, k + 1));
+      }
+  }
+  g_bad += nbr_mismatch;
   // sidx must be a bijection onto [0, 4096)
   std::vector<int> seen(BLOCK_CELLS, 0);
   for (int k = 0; k < 16; ++k)
