@@ -18,9 +18,11 @@ struct KCtx {
   int nb;
 };
 
+// Fused residual + red-black sweep over the coefficient stream (rbgs_pipelined.cu).
 void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
-                 double* xout, const double* A, const double* b, const double* gst,
-                 double omega, double* partials, SolveState* st, int fin, int iter);
+                 double* xout, const double* stream, const double* gst, double omega,
+                 double* partials, SolveState* st, int fin, int iter);
+void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b, double* stream);
 void launch_jacobi(cudaStream_t s, const KCtx& C, bool from_zero, bool dot, const double* xin,
                    double* xout, const double* A, const double* b, double omega,
                    double* partials, SolveState* st);

@@ -32,6 +32,11 @@ constexpr int BLOCK_CELLS = 4096; // 16^3
 constexpr int HALF_CELLS = 2048;  // cells of one colour
 constexpr int FACE_CELLS = 256;   // 16^2
 constexpr int THREADS = 256;      // threads per CTA of every block kernel
+// Coefficient stream of the red-black sweep: per block 16 chunks (colour c,
+// plane pair m -> chunk c*8 + m), each holding Ap, Aw, Ae, As, An, Ab, At, b
+// of its 256 cells back to back (16 KB), so one bulk copy moves a chunk.
+constexpr int STREAM_CHUNK = 8 * 256;
+constexpr int STREAM_BLOCK = 16 * STREAM_CHUNK;
 
 enum { X_M = 0, X_P, Y_M, Y_P, Z_M, Z_P };
 enum { BC_DIRICHLET = 0, BC_NEUMANN = 1 };

@@ -494,6 +494,21 @@ fold_bc_kernel(KCtx C, double* __restrict__ A, double* __restrict__ bvec) {
   }
 }
 
+// A (7 arrays) and b -> the sweep's coefficient stream (STREAM_BLOCK per block).
+__global__ void __launch_bounds__(THREADS)
+pack_stream_kernel(const double* __restrict__ A, const double* __restrict__ b,
+                   double* __restrict__ stream) {
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+  double* sb = stream + (size_t)blk * STREAM_BLOCK;
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;  // chunk m, cell tid
+    double* dst = sb + (size_t)m * STREAM_CHUNK + tid;
+    for (int a = 0; a < 7; ++a) dst[a * 256] = Ab[(size_t)a * BLOCK_CELLS + s];
+    dst[7 * 256] = b[(size_t)blk * BLOCK_CELLS + s];
+  }
+}
+
 // FFVILS::Fill (blas.f90:5-33): interior and stored guide layer.
 __global__ void __launch_bounds__(THREADS)
 fill_kernel(double* __restrict__ x, size_t stride, double* __restrict__ g, double value) {
@@ -565,6 +580,9 @@ void launch_assemble(cudaStream_t s, const KCtx& C, const double* ux, const doub
                      double* vface, double rhof, double dt, size_t field_stride) {
   assemble_kernel<<<C.nb, THREADS, 0, s>>>(C, ux, uy, uz, gux, guy, guz, cut, flags, A, b, vface,
                                            rhof, dt, field_stride);
+}
+void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b, double* stream) {
+  pack_stream_kernel<<<nb, THREADS, 0, s>>>(A, b, stream);
 }
 void launch_fill(cudaStream_t s, int nb, double* x, size_t stride, double* g, double value) {
   fill_kernel<<<nb, THREADS, 0, s>>>(x, stride, g, value);

@@ -69,6 +69,9 @@ struct ffvgpu_pool {
   int xcur = 0;
   double* gx = nullptr;  // stored first guide layer of x
   double* A = nullptr;   // [nb][7][4096]
+  double* coef = nullptr;         // sweep coefficient stream [nb][STREAM_BLOCK]
+  int64_t sys_version = 1;        // bumped whenever A or b change
+  int64_t stream_version = 0;     // sys_version the stream was packed from
   double* b = nullptr;
   double* u[3] = {nullptr, nullptr, nullptr};
   double* gu[3] = {nullptr, nullptr, nullptr};
@@ -231,6 +234,18 @@ ffvgpu_status require_system(ffvgpu_pool* P) {
   double* xp;
   size_t st;
   return field_ptr(P, FFVGPU_FIELD_X, true, &xp, &st, nullptr);
+}
+
+// Repacks A and b into the sweep's coefficient stream when they changed.
+ffvgpu_status ensure_stream(ffvgpu_pool* P) {
+  ffvgpu_status s;
+  if ((s = dalloc_t(P, &P->coef, (size_t)P->nb * STREAM_BLOCK))) return s;
+  if (P->stream_version != P->sys_version) {
+    launch_pack_stream(P->stream, P->nb, P->A, P->b, P->coef);
+    CK(cudaGetLastError());
+    P->stream_version = P->sys_version;
+  }
+  return FFVGPU_OK;
 }
 
 // Derives the neighbour table from levels and block indices.
@@ -419,7 +434,7 @@ void ffvgpu_pool_destroy(ffvgpu_pool* P) {
   cudaSetDevice(P->device);
   if (P->stream) cudaStreamSynchronize(P->stream);
   if (P->own_stream) cudaStreamSynchronize(P->own_stream);
-  void* ptrs[] = {P->x[0], P->x[1], P->gx, P->A, P->b, P->u[0], P->u[1], P->u[2],
+  void* ptrs[] = {P->x[0], P->x[1], P->gx, P->A, P->coef, P->b, P->u[0], P->u[1], P->u[2],
                   P->gu[0], P->gu[1], P->gu[2], P->cut, P->vface, P->flags, P->r,
                   P->p, P->q, P->z[0], P->z[1], P->partials, P->st, P->hist_d,
                   P->stage, P->nbr_d, P->dx_d};
@@ -464,6 +479,7 @@ ffvgpu_status ffvgpu_fill(ffvgpu_pool* P, ffvgpu_field f, double value) {
   ffvgpu_status s;
   if ((s = field_ptr(P, f, true, &x, &stride, &g))) return s;
   launch_fill(P->stream, P->nb, x, stride, g, value);
+  if ((f >= FFVGPU_FIELD_AP && f <= FFVGPU_FIELD_AT) || f == FFVGPU_FIELD_B) P->sys_version++;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(P->stream));
   return FFVGPU_OK;
@@ -509,6 +525,7 @@ ffvgpu_status ffvgpu_pool_upload(ffvgpu_pool* P, ffvgpu_field f, const void* hos
                      P->stream));
   launch_pack(P->stream, P->nb, (const double*)P->stage, vc, dst, stride, g);
   CK(cudaGetLastError());
+  if ((f >= FFVGPU_FIELD_AP && f <= FFVGPU_FIELD_AT) || f == FFVGPU_FIELD_B) P->sys_version++;
   CK(cudaStreamSynchronize(P->stream));
   return FFVGPU_OK;
 }
@@ -585,6 +602,7 @@ ffvgpu_status ffvgpu_assemble_p(ffvgpu_pool* P, double rhof, double dt) {
     return s;
   launch_assemble(P->stream, P->ctx(P->bc_p), P->u[0], P->u[1], P->u[2], P->gu[0], P->gu[1],
                   P->gu[2], P->cut, P->flags, P->A, P->b, P->vface, rhof, dt, n);
+  P->sys_version++;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(P->stream));
   return FFVGPU_OK;
@@ -595,6 +613,7 @@ ffvgpu_status ffvgpu_fold_bc(ffvgpu_pool* P) {
   if (!P->A || !P->b) return bad("A and b must exist before folding BCs");
   cudaSetDevice(P->device);
   launch_fold_bc(P->stream, P->ctx(P->bc_p), P->A, P->b);
+  P->sys_version++;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(P->stream));
   return FFVGPU_OK;
@@ -624,7 +643,8 @@ ffvgpu_status ffvgpu_calc_r2(ffvgpu_pool* P, double* rr) {
   ffvgpu_status s;
   if ((s = require_system(P))) return s;
   if ((s = reset_state(P, 0.0, 0, nullptr))) return s;
-  launch_rbgs(P->stream, P->ctx(P->bc_p), true, false, P->x[P->xcur], nullptr, P->A, P->b, P->gx,
+  if ((s = ensure_stream(P))) return s;
+  launch_rbgs(P->stream, P->ctx(P->bc_p), true, false, P->x[P->xcur], nullptr, P->coef, P->gx,
               0.0, P->partials, P->st, FIN_STORE, 0);
   CK(cudaGetLastError());
   SolveState h;
@@ -640,8 +660,9 @@ ffvgpu_status ffvgpu_rbgs_sweep(ffvgpu_pool* P, double omega) {
   ffvgpu_status s;
   if ((s = require_system(P))) return s;
   if ((s = reset_state(P, 0.0, 0, nullptr))) return s;
-  launch_rbgs(P->stream, P->ctx(P->bc_p), false, true, P->x[P->xcur], P->x[1 - P->xcur], P->A,
-              P->b, P->gx, omega, P->partials, P->st, FIN_STORE, 0);
+  if ((s = ensure_stream(P))) return s;
+  launch_rbgs(P->stream, P->ctx(P->bc_p), false, true, P->x[P->xcur], P->x[1 - P->xcur],
+              P->coef, P->gx, omega, P->partials, P->st, FIN_STORE, 0);
   P->xcur = 1 - P->xcur;
   launch_exchange(P->stream, P->ctx(P->bc_p), P->x[P->xcur], P->gx);
   CK(cudaGetLastError());
@@ -668,6 +689,7 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
     return FFVGPU_OK;
   }
   if ((s = ensure_hist(P, N))) return s;
+  if ((s = ensure_stream(P))) return s;
   if ((s = reset_state(P, prm->epsilon, N, P->hist_d))) return s;
   const KCtx C = P->ctx(P->bc_p);
   const int every = prm->check_every > 0 ? prm->check_every : 32;
@@ -677,14 +699,14 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   int launches = 1;
   int64_t bytes = interior_bytes(P, 2);
   const int c0 = P->xcur;
-  launch_rbgs(P->stream, C, false, true, P->x[c0], P->x[1 - c0], P->A, P->b, P->gx, prm->omega,
+  launch_rbgs(P->stream, C, false, true, P->x[c0], P->x[1 - c0], P->coef, P->gx, prm->omega,
               P->partials, P->st, FIN_RBGS, 0);
   launches++;
   bytes += interior_bytes(P, 10);
   CK(cudaEventRecord(P->ev2, P->stream));
   int swept = 0;
   for (int n = 2; n <= N; ++n) {
-    launch_rbgs(P->stream, C, true, true, P->x[(c0 + n - 1) & 1], P->x[(c0 + n) & 1], P->A, P->b,
+    launch_rbgs(P->stream, C, true, true, P->x[(c0 + n - 1) & 1], P->x[(c0 + n) & 1], P->coef,
                 nullptr, prm->omega, P->partials, P->st, FIN_RBGS, n - 1);
     swept++;
     launches++;
@@ -696,7 +718,7 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
     }
   }
   CK(cudaEventRecord(P->ev3, P->stream));
-  launch_rbgs(P->stream, C, true, false, P->x[(c0 + N) & 1], nullptr, P->A, P->b, nullptr,
+  launch_rbgs(P->stream, C, true, false, P->x[(c0 + N) & 1], nullptr, P->coef, nullptr,
               prm->omega, P->partials, P->st, FIN_RBGS, N);
   launches++;
   CK(cudaEventRecord(P->ev1, P->stream));

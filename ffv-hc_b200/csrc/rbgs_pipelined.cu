@@ -15,7 +15,8 @@
 //               colour-split layout of HBM, copied as is) into one of two
 //               tile buffers a block ahead, and the coefficient stream -- for
 //               each colour and each pair of z planes, the 256 cells'
-//               Ap..At and b (8 x 2 KB) -- into a ring of STAGES slots;
+//               Ap..At and b, stored contiguously (16 KB) by
+//               pack_stream_kernel -- one copy per slot of a STAGES ring;
 //   warps 1-8   gatherers: the guide layer of the block after the current
 //               one (the in-kernel exchange, computed from the neighbours'
 //               interiors of x_in) into one of two guide buffers;
@@ -142,8 +143,8 @@ __device__ __forceinline__ void consumer_sync() {
 template <bool DO_RES, bool DO_SWEEP>
 __global__ void __launch_bounds__(pipe::NTHREADS, 1)
 rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
-                      const double* __restrict__ A, const double* __restrict__ bvec,
-                      const double* __restrict__ gst, double omega,
+                      const double* __restrict__ stream, const double* __restrict__ gst,
+                      double omega,
                       double* __restrict__ partials, SolveState* st, int fin, int iter) {
   using namespace pipe;
   if (*((volatile const int32_t*)&st->done)) return;
@@ -183,18 +184,15 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
         bulk_g2s(S.xt[0], xin + (size_t)blockIdx.x * BLOCK_CELLS, BLOCK_CELLS * 8, &S.xfull[0]);
       }
       for (int blk = blockIdx.x; blk < nb && ok; blk += gridDim.x, ++m) {
-        const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
-        const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
+        const double* sb = stream + (size_t)blk * STREAM_BLOCK;
         for (int j = 0; j < CHUNKS && ok; ++j) {
           const int s = g % STAGES;
           const uint32_t u = g / STAGES;
           if (!(ok = mbar_wait(&S.empty[s], (u & 1) ^ 1, abort_flag, ROLE_PRODUCER))) break;
           ++g;
+          // chunk j = colour * 8 + plane pair: Ap..At and b of its 256 cells
           mbar_expect_tx(&S.full[s], CHUNK_BYTES);
-          const int off = (j >> 3) * HALF_CELLS + (j & 7) * CHUNK_CELLS;  // colour, plane pair
-          for (int a = 0; a < 7; ++a)
-            bulk_g2s(S.ring[s][a], Ab + (size_t)a * BLOCK_CELLS + off, CHUNK_CELLS * 8, &S.full[s]);
-          bulk_g2s(S.ring[s][7], bb + off, CHUNK_CELLS * 8, &S.full[s]);
+          bulk_g2s(S.ring[s], sb + (size_t)j * STREAM_CHUNK, CHUNK_BYTES, &S.full[s]);
           if (j == X_ISSUE_AT && blk + (int)gridDim.x < nb) {
             // x of block m+1 into the buffer block m-1 used (released by now:
             // the consumers are in block m)
@@ -386,8 +384,8 @@ int g_sm_count = 0;
 bool g_attr_set[4] = {false, false, false, false};
 
 template <bool R, bool W>
-void launch_one(cudaStream_t s, const KCtx& C, const double* xin, double* xout, const double* A,
-                const double* b, const double* gst, double omega, double* partials,
+void launch_one(cudaStream_t s, const KCtx& C, const double* xin, double* xout,
+                const double* stream, const double* gst, double omega, double* partials,
                 SolveState* st, int fin, int iter, int slot) {
   const size_t smem = sizeof(pipe::Smem);
   if (!g_attr_set[slot]) {
@@ -396,14 +394,14 @@ void launch_one(cudaStream_t s, const KCtx& C, const double* xin, double* xout, 
     g_attr_set[slot] = true;
   }
   const int grid = C.nb < g_sm_count ? C.nb : g_sm_count;
-  rbgs_pipelined_kernel<R, W><<<grid, pipe::NTHREADS, smem, s>>>(C, xin, xout, A, b, gst, omega,
-                                                                 partials, st, fin, iter);
+  rbgs_pipelined_kernel<R, W><<<grid, pipe::NTHREADS, smem, s>>>(C, xin, xout, stream, gst,
+                                                                 omega, partials, st, fin, iter);
 }
 }  // namespace
 
 void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
-                 double* xout, const double* A, const double* b, const double* gst,
-                 double omega, double* partials, SolveState* st, int fin, int iter) {
+                 double* xout, const double* stream, const double* gst, double omega,
+                 double* partials, SolveState* st, int fin, int iter) {
   if (g_sm_count == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -411,11 +409,11 @@ void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const doub
     if (g_sm_count <= 0) g_sm_count = 1;
   }
   if (res && sweep)
-    launch_one<true, true>(s, C, xin, xout, A, b, gst, omega, partials, st, fin, iter, 0);
+    launch_one<true, true>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 0);
   else if (sweep)
-    launch_one<false, true>(s, C, xin, xout, A, b, gst, omega, partials, st, fin, iter, 1);
+    launch_one<false, true>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 1);
   else
-    launch_one<true, false>(s, C, xin, xout, A, b, gst, omega, partials, st, fin, iter, 2);
+    launch_one<true, false>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 2);
 }
 
 size_t rbgs_pipelined_smem_bytes() { return sizeof(pipe::Smem); }
