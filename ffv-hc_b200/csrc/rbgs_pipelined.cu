@@ -14,13 +14,14 @@
 //               shared, completion on mbarriers): each block's x (32 KB, the
 //               colour-split layout of HBM, copied as is) into one of two
 //               tile buffers a block ahead, and the coefficient stream -- for
-//               each colour and each pair of z planes, the 256 cells'
-//               Ap..At and b, stored contiguously (16 KB) by
-//               pack_stream_kernel -- one copy per slot of a STAGES ring;
+//               each colour and each four z planes, the 512 cells' Ap..At
+//               and b, stored contiguously (32 KB) by pack_stream_kernel --
+//               one copy per slot of a STAGES ring;
 //   warps 1-8   gatherers: the guide layer of the block after the current
 //               one (the in-kernel exchange, computed from the neighbours'
 //               interiors of x_in) into one of two guide buffers;
-//   warps 9-16  consumers (256 threads): the colour-0 pass (residual, and
+//   warps 9-16  consumers (256 threads, two cells each per slot for
+//               instruction-level parallelism): the colour-0 pass (residual, and
 //               the update kept in a colour-0 buffer and streamed to x_out),
 //               then the colour-1 pass (residual against the old colour-0
 //               values, update against the new), and the residual sum.
@@ -41,12 +42,13 @@ namespace ffvgpu {
 
 namespace pipe {
 
-constexpr int STAGES = 7;
+constexpr int CPT = 2;               // cells per consumer thread per slot
+constexpr int STAGES = 3;
 constexpr int NARR = 8;              // Ap, Aw, Ae, As, An, Ab, At, b
-constexpr int CHUNK_CELLS = 256;     // one colour, two z planes
-constexpr int CHUNK_BYTES = NARR * CHUNK_CELLS * 8;
-constexpr int CHUNKS = 16;           // 8 per colour
-constexpr int X_ISSUE_AT = 8;        // chunk of block m after which x(m+1) is issued
+constexpr int SUB_CELLS = 256;       // cells of one stream chunk (one colour, two z planes)
+constexpr int SLOT_BYTES = CPT * NARR * SUB_CELLS * 8;
+constexpr int SLOTS = 16 / CPT;      // slots per block (SLOTS / 2 per colour)
+constexpr int X_ISSUE_AT = SLOTS / 2;  // slot of block m after which x(m+1) is issued
 constexpr int PRODUCER_WARPS = 1, GATHER_WARPS = 8, CONSUMER_WARPS = 8;
 constexpr int GATHER0 = 32 * PRODUCER_WARPS;
 constexpr int CONS0 = GATHER0 + 32 * GATHER_WARPS;
@@ -57,7 +59,7 @@ constexpr uint32_t DRAIN_LIMIT = 1u << 24;    // polls while draining copies in 
 enum { ROLE_PRODUCER = 1, ROLE_GATHER = 2, ROLE_CONSUMER = 4 };
 
 struct __align__(128) Smem {
-  double ring[STAGES][NARR][CHUNK_CELLS];  // 112 KB
+  double ring[STAGES][CPT][NARR][SUB_CELLS];  // 96 KB
   double xt[2][BLOCK_CELLS];               // 64 KB: x_in of the current / next block
   double xnew0[HALF_CELLS];                // 16 KB: updated colour-0 values
   double gbuf[2][6 * FACE_CELLS];          // 24 KB: guide layers, [face][v][u]
@@ -124,12 +126,24 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-// Hands a ring slot back to the producer: each thread waits for its loads of
-// the slot to land in registers and fences them; one lane per warp arrives.
-__device__ __forceinline__ void release_slot(uint64_t* bar, int lane, bool live, double a0,
-                                             double a1, double a2, double a3, double a4,
-                                             double a5, double a6, double a7) {
-  asm volatile("" ::"d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(a4), "d"(a5), "d"(a6), "d"(a7));
+// The coefficients of one cell, read from a ring slot.
+struct Coef {
+  double ap, aw, ae, as, an, ab, at, b;
+};
+__device__ __forceinline__ Coef load_coef(const double (*slot)[SUB_CELLS], int t) {
+  Coef c;
+  c.ap = slot[0][t]; c.aw = slot[1][t]; c.ae = slot[2][t]; c.as = slot[3][t];
+  c.an = slot[4][t]; c.ab = slot[5][t]; c.at = slot[6][t]; c.b = slot[7][t];
+  return c;
+}
+__device__ __forceinline__ void hold(const Coef& c) {
+  asm volatile("" ::"d"(c.ap), "d"(c.aw), "d"(c.ae), "d"(c.as), "d"(c.an), "d"(c.ab), "d"(c.at),
+               "d"(c.b));
+}
+// Hands a ring slot back to the producer: each thread has waited for its
+// loads of the slot to land in registers (hold), fences them; one lane per
+// warp arrives.
+__device__ __forceinline__ void release_slot(uint64_t* bar, int lane, bool live) {
   fence_proxy_async();
   __syncwarp();
   if (lane == 0 && live) mbar_arrive(bar);
@@ -185,14 +199,15 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       }
       for (int blk = blockIdx.x; blk < nb && ok; blk += gridDim.x, ++m) {
         const double* sb = stream + (size_t)blk * STREAM_BLOCK;
-        for (int j = 0; j < CHUNKS && ok; ++j) {
+        for (int j = 0; j < SLOTS && ok; ++j) {
           const int s = g % STAGES;
           const uint32_t u = g / STAGES;
           if (!(ok = mbar_wait(&S.empty[s], (u & 1) ^ 1, abort_flag, ROLE_PRODUCER))) break;
           ++g;
-          // chunk j = colour * 8 + plane pair: Ap..At and b of its 256 cells
-          mbar_expect_tx(&S.full[s], CHUNK_BYTES);
-          bulk_g2s(S.ring[s], sb + (size_t)j * STREAM_CHUNK, CHUNK_BYTES, &S.full[s]);
+          // slot j: stream chunks CPT*j .. CPT*j+CPT-1 (colour = j / (SLOTS/2)),
+          // contiguous in the stream
+          mbar_expect_tx(&S.full[s], SLOT_BYTES);
+          bulk_g2s(S.ring[s], sb + (size_t)j * CPT * STREAM_CHUNK, SLOT_BYTES, &S.full[s]);
           if (j == X_ISSUE_AT && blk + (int)gridDim.x < nb) {
             // x of block m+1 into the buffer block m-1 used (released by now:
             // the consumers are in block m)
@@ -266,59 +281,72 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       const double* G = S.gbuf[xb];
       double* xo = xout + (size_t)blk * BLOCK_CELLS;
       double acc[2] = {0.0, 0.0};
-      // colour 0: neighbours are colour 1 (unchanged)
-      for (int mm = 0; mm < 8; ++mm, ++g) {
+      // colour 0: neighbours are colour 1 (unchanged).  Each thread takes the
+      // cells q = m*256 + ct of the slot's CPT stream chunks, in order m.
+      for (int mm = 0; mm < SLOTS / 2; ++mm, ++g) {
         const int s = g % STAGES;
         live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
-        double ap = 1.0, aw = 0.0, ae = 0.0, as = 0.0, an = 0.0, ab = 0.0, at = 0.0, bv = 0.0;
-        if (live) {
-          ap = S.ring[s][0][ct]; aw = S.ring[s][1][ct]; ae = S.ring[s][2][ct];
-          as = S.ring[s][3][ct]; an = S.ring[s][4][ct]; ab = S.ring[s][5][ct];
-          at = S.ring[s][6][ct]; bv = S.ring[s][7][ct];
+        Coef cf[CPT];
+#pragma unroll
+        for (int h = 0; h < CPT; ++h) {
+          if (live) cf[h] = load_coef(S.ring[s][h], ct);
+          else cf[h] = Coef{1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+          hold(cf[h]);
         }
-        release_slot(&S.empty[s], lane, live, ap, aw, ae, as, an, ab, at, bv);
+        release_slot(&S.empty[s], lane, live);
         if (!live) continue;
-        const int q = mm * CHUNK_CELLS + ct;
-        const Nbrs v = split_neighbours(T + HALF_CELLS, G, q, 0);
-        const double rs = bv - aw * v.w - ae * v.e - as * v.s - an * v.n - ab * v.b - at * v.t;
-        const double xp = T[q];
-        if (DO_RES) {
-          const double r = rs - ap * xp;
-          acc[0] += r * r;
-        }
-        if (DO_SWEEP) {
-          const double xt = rs / ap;
-          const double xn = xp - omega * (xp - xt);
-          S.xnew0[q] = xn;
-          xo[q] = xn;
+#pragma unroll
+        for (int h = 0; h < CPT; ++h) {
+          const int q = (mm * CPT + h) * SUB_CELLS + ct;
+          const Coef& c = cf[h];
+          const Nbrs v = split_neighbours(T + HALF_CELLS, G, q, 0);
+          const double rs = c.b - c.aw * v.w - c.ae * v.e - c.as * v.s - c.an * v.n - c.ab * v.b -
+                            c.at * v.t;
+          const double xp = T[q];
+          if (DO_RES) {
+            const double r = rs - c.ap * xp;
+            acc[0] += r * r;
+          }
+          if (DO_SWEEP) {
+            const double xt = rs / c.ap;
+            const double xn = xp - omega * (xp - xt);
+            S.xnew0[q] = xn;
+            xo[q] = xn;
+          }
         }
       }
       consumer_sync();
       // colour 1: residual against the old colour-0 values, update against the new
-      for (int mm = 0; mm < 8; ++mm, ++g) {
+      for (int mm = 0; mm < SLOTS / 2; ++mm, ++g) {
         const int s = g % STAGES;
         live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
-        double ap = 1.0, aw = 0.0, ae = 0.0, as = 0.0, an = 0.0, ab = 0.0, at = 0.0, bv = 0.0;
-        if (live) {
-          ap = S.ring[s][0][ct]; aw = S.ring[s][1][ct]; ae = S.ring[s][2][ct];
-          as = S.ring[s][3][ct]; an = S.ring[s][4][ct]; ab = S.ring[s][5][ct];
-          at = S.ring[s][6][ct]; bv = S.ring[s][7][ct];
+        Coef cf[CPT];
+#pragma unroll
+        for (int h = 0; h < CPT; ++h) {
+          if (live) cf[h] = load_coef(S.ring[s][h], ct);
+          else cf[h] = Coef{1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+          hold(cf[h]);
         }
-        release_slot(&S.empty[s], lane, live, ap, aw, ae, as, an, ab, at, bv);
+        release_slot(&S.empty[s], lane, live);
         if (!live) continue;
-        const int q = mm * CHUNK_CELLS + ct;
-        const double xp = T[HALF_CELLS + q];
-        if (DO_RES) {
-          const Nbrs v = split_neighbours(T, G, q, 1);
-          const double r = bv - aw * v.w - ae * v.e - as * v.s - an * v.n - ab * v.b - at * v.t -
-                           ap * xp;
-          acc[1] += r * r;
-        }
-        if (DO_SWEEP) {
-          const Nbrs v = split_neighbours(S.xnew0, G, q, 1);
-          const double rs = bv - aw * v.w - ae * v.e - as * v.s - an * v.n - ab * v.b - at * v.t;
-          const double xt = rs / ap;
-          xo[HALF_CELLS + q] = xp - omega * (xp - xt);
+#pragma unroll
+        for (int h = 0; h < CPT; ++h) {
+          const int q = (mm * CPT + h) * SUB_CELLS + ct;
+          const Coef& c = cf[h];
+          const double xp = T[HALF_CELLS + q];
+          if (DO_RES) {
+            const Nbrs v = split_neighbours(T, G, q, 1);
+            const double r = c.b - c.aw * v.w - c.ae * v.e - c.as * v.s - c.an * v.n -
+                             c.ab * v.b - c.at * v.t - c.ap * xp;
+            acc[1] += r * r;
+          }
+          if (DO_SWEEP) {
+            const Nbrs v = split_neighbours(S.xnew0, G, q, 1);
+            const double rs = c.b - c.aw * v.w - c.ae * v.e - c.as * v.s - c.an * v.n -
+                              c.ab * v.b - c.at * v.t;
+            const double xt = rs / c.ap;
+            xo[HALF_CELLS + q] = xp - omega * (xp - xt);
+          }
         }
       }
       if (DO_RES) {
