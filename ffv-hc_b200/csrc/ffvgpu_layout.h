@@ -77,6 +77,13 @@ struct SolveState {
   double* hist;      // device residual history [count_max] or null
 };
 
+// Sums over a block use one fixed tree of 512 virtual threads: virtual
+// thread t sums, serially from 0.0, the cells c*2048 + t + 512*m (m = 0..3)
+// of each colour c, and adds the two colour sums; the 32 virtual threads of
+// each of the 16 virtual warps are combined by an xor butterfly (16, 8, 4,
+// 2, 1); the 16 warp sums are added in order from 0.0.  Across blocks, 256
+// threads sum the per-block partials t, t+256, ... serially, then the same
+// butterfly and an in-order sum of the 8 warp sums.
 // Finalisers run by the last CTA of a reduction.
 enum Fin : int {
   FIN_STORE = 0,  // st->rr = total (plain dot product)

@@ -73,19 +73,30 @@ __device__ __forceinline__ void stage_tile(double* __restrict__ xs, const double
 }
 
 // Canonical block reduction + last-CTA cross-block reduction + finaliser.
-__device__ void reduce_finalize(double v, double* __restrict__ partials, SolveState* st,
-                                int fin, int iter) {
-  __shared__ double ws[8];
+// The block tree has 512 virtual threads (see the layout header); thread r
+// of a 256-thread CTA carries virtual threads r and r + 256, whose serial
+// per-colour sums are acc[c][0] and acc[c][1] (cells c*2048 + r + 256*m with
+// m even and odd respectively).
+__device__ void reduce_finalize(const double (&acc)[2][2], double* __restrict__ partials,
+                                SolveState* st, int fin, int iter) {
+  __shared__ double ws[16];
   __shared__ int amlast;
   const int tid = threadIdx.x;
+  double v0 = acc[0][0] + acc[1][0], v1 = acc[0][1] + acc[1][1];
 #pragma unroll
-  for (int off = 16; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  if ((tid & 31) == 0) ws[tid >> 5] = v;
+  for (int off = 16; off >= 1; off >>= 1) {
+    v0 += __shfl_xor_sync(0xffffffffu, v0, off);
+    v1 += __shfl_xor_sync(0xffffffffu, v1, off);
+  }
+  if ((tid & 31) == 0) {
+    ws[tid >> 5] = v0;
+    ws[8 + (tid >> 5)] = v1;
+  }
   __syncthreads();
   if (tid == 0) {
     double s = 0.0;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) s += ws[w];
+    for (int w = 0; w < 16; ++w) s += ws[w];
     __stcg(partials + blockIdx.x, s);
     __threadfence();
     const unsigned t = atomicAdd(&st->ticket, 1u);
@@ -131,7 +142,7 @@ jacobi_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
   const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
   double* xo = xout + (size_t)blk * BLOCK_CELLS;
-  double acc[2] = {0.0, 0.0};
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
 #pragma unroll 4
@@ -154,10 +165,10 @@ jacobi_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
       const double x_tmp = r / __ldg(Ab + s);
       const double x1 = xp - omega * (xp - x_tmp);
       xo[s] = x1;
-      if (DOT) acc[c] += bv * x1;
+      if (DOT) acc[c][m & 1] += bv * x1;
     }
   }
-  if (DOT) reduce_finalize(acc[0] + acc[1], partials, st, FIN_CG_RR1, 0);
+  if (DOT) reduce_finalize(acc, partials, st, FIN_CG_RR1, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -214,7 +225,7 @@ ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A
   __syncthreads();
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
   double* qo = q + (size_t)blk * BLOCK_CELLS;
-  double acc[2] = {0.0, 0.0};
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
 #pragma unroll 4
@@ -228,10 +239,10 @@ ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A
                        __ldg(Ab + 20480 + s) * xs[t - TP] + __ldg(Ab + 24576 + s) * xs[t + TP] +
                        __ldg(Ab + s) * xs[t];
       qo[s] = v;
-      acc[c] += v * xs[t];
+      acc[c][m & 1] += v * xs[t];
     }
   }
-  reduce_finalize(acc[0] + acc[1], partials, st, FIN_CG_QP, 0);
+  reduce_finalize(acc, partials, st, FIN_CG_QP, 0);
 }
 
 // x = x + alpha p; r = r + (-alpha) q (axpy, blas.f90:329-361); r.r.
@@ -242,7 +253,7 @@ cg_update_kernel(double* __restrict__ x, const double* __restrict__ p, double* _
   if (solve_done(st)) return;
   const double alpha = st->alpha, malpha = -alpha;
   const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
-  double acc[2] = {0.0, 0.0};
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
 #pragma unroll 4
@@ -251,10 +262,10 @@ cg_update_kernel(double* __restrict__ x, const double* __restrict__ p, double* _
       x[s] = x[s] + alpha * p[s];
       const double rn = r[s] + malpha * q[s];
       r[s] = rn;
-      acc[c] += rn * rn;
+      acc[c][m & 1] += rn * rn;
     }
   }
-  reduce_finalize(acc[0] + acc[1], partials, st, FIN_CG_RR, iter);
+  reduce_finalize(acc, partials, st, FIN_CG_RR, iter);
 }
 
 // x.y over interior cells (dot, blas.f90:466-499) with a finaliser.
@@ -263,16 +274,16 @@ dot_kernel(const double* __restrict__ x, const double* __restrict__ y,
            double* __restrict__ partials, SolveState* st, int fin, int iter) {
   if (solve_done(st)) return;
   const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
-  double acc[2] = {0.0, 0.0};
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
 #pragma unroll 4
     for (int m = 0; m < 8; ++m) {
       const size_t s = base + c * HALF_CELLS + threadIdx.x + THREADS * m;
-      acc[c] += __ldg(x + s) * __ldg(y + s);
+      acc[c][m & 1] += __ldg(x + s) * __ldg(y + s);
     }
   }
-  reduce_finalize(acc[0] + acc[1], partials, st, fin, iter);
+  reduce_finalize(acc, partials, st, fin, iter);
 }
 
 // ---------------------------------------------------------------------------

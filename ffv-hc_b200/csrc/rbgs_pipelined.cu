@@ -20,8 +20,8 @@
 //   warps 1-8   gatherers: the guide layer of the block after the current
 //               one (the in-kernel exchange, computed from the neighbours'
 //               interiors of x_in) into one of two guide buffers;
-//   warps 9-16  consumers (256 threads, two cells each per slot for
-//               instruction-level parallelism): the colour-0 pass (residual, and
+//   warps 9-24  consumers (512 threads, one cell each per slot): the
+//               colour-0 pass (residual, and
 //               the update kept in a colour-0 buffer and streamed to x_out),
 //               then the colour-1 pass (residual against the old colour-0
 //               values, update against the new), and the residual sum.
@@ -42,17 +42,18 @@ namespace ffvgpu {
 
 namespace pipe {
 
-constexpr int CPT = 2;               // cells per consumer thread per slot
+constexpr int CPT = 2;               // stream chunks per slot (512 cells)
 constexpr int STAGES = 3;
 constexpr int NARR = 8;              // Ap, Aw, Ae, As, An, Ab, At, b
 constexpr int SUB_CELLS = 256;       // cells of one stream chunk (one colour, two z planes)
 constexpr int SLOT_BYTES = CPT * NARR * SUB_CELLS * 8;
 constexpr int SLOTS = 16 / CPT;      // slots per block (SLOTS / 2 per colour)
 constexpr int X_ISSUE_AT = SLOTS / 2;  // slot of block m after which x(m+1) is issued
-constexpr int PRODUCER_WARPS = 1, GATHER_WARPS = 8, CONSUMER_WARPS = 8;
+constexpr int PRODUCER_WARPS = 1, GATHER_WARPS = 8, CONSUMER_WARPS = 16;
 constexpr int GATHER0 = 32 * PRODUCER_WARPS;
 constexpr int CONS0 = GATHER0 + 32 * GATHER_WARPS;
-constexpr int NTHREADS = CONS0 + 32 * CONSUMER_WARPS;  // 544
+constexpr int NTHREADS = CONS0 + 32 * CONSUMER_WARPS;  // 800
+constexpr int NCONS = 32 * CONSUMER_WARPS;            // one cell per consumer per slot
 constexpr int NGATHER = 32 * GATHER_WARPS;
 constexpr uint64_t WAIT_NS = 4000000000ull;  // a wait gives up after 4 s
 constexpr uint32_t DRAIN_LIMIT = 1u << 24;    // polls while draining copies in flight
@@ -65,7 +66,7 @@ struct __align__(128) Smem {
   double gbuf[2][6 * FACE_CELLS];          // 24 KB: guide layers, [face][v][u]
   uint64_t full[STAGES], empty[STAGES];
   uint64_t xfull[2], xempty[2], gfull[2], gempty[2];
-  double ws[8];
+  double ws[CONSUMER_WARPS];
   int abort_flag;
   int last;
 };
@@ -281,38 +282,31 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       const double* G = S.gbuf[xb];
       double* xo = xout + (size_t)blk * BLOCK_CELLS;
       double acc[2] = {0.0, 0.0};
-      // colour 0: neighbours are colour 1 (unchanged).  Each thread takes the
-      // cells q = m*256 + ct of the slot's CPT stream chunks, in order m.
+      // colour 0: neighbours are colour 1 (unchanged).  Consumer ct takes the
+      // cell q = mm*512 + ct of every slot (stream chunk ct >> 8 of the slot).
+      const int h = ct >> 8, t = ct & 255;
       for (int mm = 0; mm < SLOTS / 2; ++mm, ++g) {
         const int s = g % STAGES;
         live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
-        Coef cf[CPT];
-#pragma unroll
-        for (int h = 0; h < CPT; ++h) {
-          if (live) cf[h] = load_coef(S.ring[s][h], ct);
-          else cf[h] = Coef{1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-          hold(cf[h]);
-        }
+        Coef c = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (live) c = load_coef(S.ring[s][h], t);
+        hold(c);
         release_slot(&S.empty[s], lane, live);
         if (!live) continue;
-#pragma unroll
-        for (int h = 0; h < CPT; ++h) {
-          const int q = (mm * CPT + h) * SUB_CELLS + ct;
-          const Coef& c = cf[h];
-          const Nbrs v = split_neighbours(T + HALF_CELLS, G, q, 0);
-          const double rs = c.b - c.aw * v.w - c.ae * v.e - c.as * v.s - c.an * v.n - c.ab * v.b -
-                            c.at * v.t;
-          const double xp = T[q];
-          if (DO_RES) {
-            const double r = rs - c.ap * xp;
-            acc[0] += r * r;
-          }
-          if (DO_SWEEP) {
-            const double xt = rs / c.ap;
-            const double xn = xp - omega * (xp - xt);
-            S.xnew0[q] = xn;
-            xo[q] = xn;
-          }
+        const int q = mm * NCONS + ct;
+        const Nbrs v = split_neighbours(T + HALF_CELLS, G, q, 0);
+        const double rs = c.b - c.aw * v.w - c.ae * v.e - c.as * v.s - c.an * v.n - c.ab * v.b -
+                          c.at * v.t;
+        const double xp = T[q];
+        if (DO_RES) {
+          const double r = rs - c.ap * xp;
+          acc[0] += r * r;
+        }
+        if (DO_SWEEP) {
+          const double xt = rs / c.ap;
+          const double xn = xp - omega * (xp - xt);
+          S.xnew0[q] = xn;
+          xo[q] = xn;
         }
       }
       consumer_sync();
@@ -320,36 +314,30 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       for (int mm = 0; mm < SLOTS / 2; ++mm, ++g) {
         const int s = g % STAGES;
         live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
-        Coef cf[CPT];
-#pragma unroll
-        for (int h = 0; h < CPT; ++h) {
-          if (live) cf[h] = load_coef(S.ring[s][h], ct);
-          else cf[h] = Coef{1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-          hold(cf[h]);
-        }
+        Coef c = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (live) c = load_coef(S.ring[s][h], t);
+        hold(c);
         release_slot(&S.empty[s], lane, live);
         if (!live) continue;
-#pragma unroll
-        for (int h = 0; h < CPT; ++h) {
-          const int q = (mm * CPT + h) * SUB_CELLS + ct;
-          const Coef& c = cf[h];
-          const double xp = T[HALF_CELLS + q];
-          if (DO_RES) {
-            const Nbrs v = split_neighbours(T, G, q, 1);
-            const double r = c.b - c.aw * v.w - c.ae * v.e - c.as * v.s - c.an * v.n -
-                             c.ab * v.b - c.at * v.t - c.ap * xp;
-            acc[1] += r * r;
-          }
-          if (DO_SWEEP) {
-            const Nbrs v = split_neighbours(S.xnew0, G, q, 1);
-            const double rs = c.b - c.aw * v.w - c.ae * v.e - c.as * v.s - c.an * v.n -
-                              c.ab * v.b - c.at * v.t;
-            const double xt = rs / c.ap;
-            xo[HALF_CELLS + q] = xp - omega * (xp - xt);
-          }
+        const int q = mm * NCONS + ct;
+        const double xp = T[HALF_CELLS + q];
+        if (DO_RES) {
+          const Nbrs v = split_neighbours(T, G, q, 1);
+          const double r = c.b - c.aw * v.w - c.ae * v.e - c.as * v.s - c.an * v.n - c.ab * v.b -
+                           c.at * v.t - c.ap * xp;
+          acc[1] += r * r;
+        }
+        if (DO_SWEEP) {
+          const Nbrs v = split_neighbours(S.xnew0, G, q, 1);
+          const double rs = c.b - c.aw * v.w - c.ae * v.e - c.as * v.s - c.an * v.n - c.ab * v.b -
+                            c.at * v.t;
+          const double xt = rs / c.ap;
+          xo[HALF_CELLS + q] = xp - omega * (xp - xt);
         }
       }
       if (DO_RES) {
+        // block tree: virtual thread ct (512 per block), butterfly per warp,
+        // warp sums in order
         double v = acc[0] + acc[1];
 #pragma unroll
         for (int off = 16; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -358,7 +346,7 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
         if (ct == 0 && live) {
           double sum = 0.0;
 #pragma unroll
-          for (int w = 0; w < 8; ++w) sum += S.ws[w];
+          for (int w = 0; w < CONSUMER_WARPS; ++w) sum += S.ws[w];
           __stcg(partials + blk, sum);
         }
       }
@@ -390,12 +378,14 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
   __syncthreads();
   if (!S.last || tid < CONS0) return;
   __threadfence();
+  // cross-block tree: 256 threads over the partials, butterfly, 8 warp sums
   const int ct = tid - CONS0;
   double Ssum = 0.0;
-  for (int b = ct; b < nb; b += 256) Ssum += __ldcg(partials + b);
+  if (ct < 256)
+    for (int b = ct; b < nb; b += 256) Ssum += __ldcg(partials + b);
 #pragma unroll
   for (int off = 16; off >= 1; off >>= 1) Ssum += __shfl_xor_sync(0xffffffffu, Ssum, off);
-  if ((ct & 31) == 0) S.ws[ct >> 5] = Ssum;
+  if ((ct & 31) == 0 && ct < 256) S.ws[ct >> 5] = Ssum;
   consumer_sync();
   if (ct == 0) {
     double total = 0.0;

@@ -143,11 +143,12 @@ inline double r_cell(const double* Ap, const double* Aw, const double* Ae,
 // Canonical reduction order (the CUDA path's fixed tree).
 //   Storage index s = c*2048 + q of a 16^3 block, q = (k*16 + j)*8 + ih,
 //   i = 2*ih + ((j + k + c) & 1) with 0-based (i, j, k).
-//   Per block: thread t in [0,256) forms S_c = sum_{m=0..7} v[c*2048+t+256m]
-//   (serial, from 0.0) and T_t = S_0 + S_1; lanes of each 32-thread warp are
-//   combined by an xor butterfly (16, 8, 4, 2, 1); warp sums are added
-//   serially from 0.0.  Across blocks: thread t sums partial[t + 256*r]
-//   serially from 0.0, then the same butterfly and serial warp sum.
+//   Per block, 512 virtual threads t: S_c = sum_{m=0..3} v[c*2048 + t + 512m]
+//   (serial, from 0.0) and T_t = S_0 + S_1; the 32 virtual threads of each
+//   of the 16 virtual warps are combined by an xor butterfly (16, 8, 4, 2,
+//   1); the 16 warp sums are added serially from 0.0.  Across blocks: thread
+//   t in [0,256) sums partial[t + 256*r] serially from 0.0, then the same
+//   butterfly per warp and a serial sum over the 8 warps.
 // ---------------------------------------------------------------------------
 inline void cell_of_storage(int s, int& i, int& j, int& k) {
   const int c = s >> 11, q = s & 2047;
@@ -157,9 +158,9 @@ inline void cell_of_storage(int s, int& i, int& j, int& k) {
   i = 2 * ih + ((j + k + c) & 1);
 }
 
-double butterfly256(const double* T) {
+double butterfly_warps(const double* T, int nwarps) {
   double block = 0.0;
-  for (int w = 0; w < 8; ++w) {
+  for (int w = 0; w < nwarps; ++w) {
     double v[32];
     for (int l = 0; l < 32; ++l) v[l] = T[32 * w + l];
     for (int off = 16; off >= 1; off >>= 1) {
@@ -173,14 +174,14 @@ double butterfly256(const double* T) {
 }
 
 double canonical_block(const double* v /* 4096 values in storage order */) {
-  double T[256];
-  for (int t = 0; t < 256; ++t) {
+  double T[512];
+  for (int t = 0; t < 512; ++t) {
     double S0 = 0.0, S1 = 0.0;
-    for (int m = 0; m < 8; ++m) S0 += v[t + 256 * m];
-    for (int m = 0; m < 8; ++m) S1 += v[2048 + t + 256 * m];
+    for (int m = 0; m < 4; ++m) S0 += v[t + 512 * m];
+    for (int m = 0; m < 4; ++m) S1 += v[2048 + t + 512 * m];
     T[t] = S0 + S1;
   }
-  return butterfly256(T);
+  return butterfly_warps(T, 16);
 }
 
 double canonical_blocks(const std::vector<double>& partial) {
@@ -190,7 +191,7 @@ double canonical_blocks(const std::vector<double>& partial) {
     for (size_t b = t; b < partial.size(); b += 256) S += partial[b];
     T[t] = S;
   }
-  return butterfly256(T);
+  return butterfly_warps(T, 8);
 }
 
 // ---------------------------------------------------------------------------
