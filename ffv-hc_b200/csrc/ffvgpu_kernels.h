@@ -19,9 +19,12 @@ struct KCtx {
 };
 
 // Fused residual + red-black sweep over the coefficient stream (rbgs_pipelined.cu).
+// pdl: launched as a programmatic dependent of the previous kernel on the
+// stream, which must then be a pass of this kernel (it overlaps that pass's
+// tail: its coefficient prefetch runs before the dependency wait).
 void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
                  double* xout, const double* stream, const double* gst, double omega,
-                 double* partials, SolveState* st, int fin, int iter);
+                 double* partials, SolveState* st, int fin, int iter, bool pdl = false);
 void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b, double* stream);
 void launch_jacobi(cudaStream_t s, const KCtx& C, bool from_zero, bool dot, const double* xin,
                    double* xout, const double* A, const double* b, double omega,

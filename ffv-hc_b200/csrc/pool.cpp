@@ -705,21 +705,27 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   bytes += interior_bytes(P, 10);
   CK(cudaEventRecord(P->ev2, P->stream));
   int swept = 0;
+  // Each pass is a programmatic dependent of the pass before it (it
+  // prefetches coefficients during that pass's tail), except where a host
+  // poll or a timing event sits between them.
+  bool polled_last = true;
   for (int n = 2; n <= N; ++n) {
     launch_rbgs(P->stream, C, true, true, P->x[(c0 + n - 1) & 1], P->x[(c0 + n) & 1], P->coef,
-                nullptr, prm->omega, P->partials, P->st, FIN_RBGS, n - 1);
+                nullptr, prm->omega, P->partials, P->st, FIN_RBGS, n - 1, !polled_last);
+    polled_last = false;
     swept++;
     launches++;
     bytes += interior_bytes(P, 10);
     if (poll && (n % every) == 0) {
       bool done = false;
       if ((s = poll_done(P, &done))) return s;
+      polled_last = true;
       if (done) break;
     }
   }
   CK(cudaEventRecord(P->ev3, P->stream));
   launch_rbgs(P->stream, C, true, false, P->x[(c0 + N) & 1], nullptr, P->coef, nullptr,
-              prm->omega, P->partials, P->st, FIN_RBGS, N);
+              prm->omega, P->partials, P->st, FIN_RBGS, N, false);
   launches++;
   CK(cudaEventRecord(P->ev1, P->stream));
   CK(cudaGetLastError());

@@ -162,7 +162,6 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
                       double omega,
                       double* __restrict__ partials, SolveState* st, int fin, int iter) {
   using namespace pipe;
-  if (*((volatile const int32_t*)&st->done)) return;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem& S = *reinterpret_cast<Smem*>(smem_raw);
   const int tid = threadIdx.x;
@@ -183,44 +182,56 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
     S.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     fence_proxy_async();
+    // the next pass may start its prologue as soon as SMs free up
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   }
   __syncthreads();
+  const int myblocks = (blockIdx.x < nb) ? (nb - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int total_slots = myblocks * SLOTS;
 
   if (tid < GATHER0) {
     // ------------------------------------------------------------ producer
     if (tid == 0) {
-      uint32_t g = 0;            // chunks issued
+      uint32_t g = 0;            // slots issued
       uint32_t nx[2] = {0, 0};   // x copies issued per tile buffer
       bool ok = true;
-      int m = 0;
-      if (blockIdx.x < nb) {
+      // The coefficient stream does not depend on the previous pass: the
+      // first STAGES slots are issued before waiting for it.
+      auto issue_slot = [&](uint32_t gg) {
+        const int s = gg % STAGES;
+        const int blk = blockIdx.x + (int)(gg / SLOTS) * gridDim.x;
+        const int j = gg % SLOTS;
+        mbar_expect_tx(&S.full[s], SLOT_BYTES);
+        // slot j: stream chunks CPT*j .. CPT*j+CPT-1 (colour = j / (SLOTS/2))
+        bulk_g2s(S.ring[s], stream + (size_t)blk * STREAM_BLOCK + (size_t)j * CPT * STREAM_CHUNK,
+                 SLOT_BYTES, &S.full[s]);
+      };
+      for (; g < (uint32_t)STAGES && g < (uint32_t)total_slots; ++g) issue_slot(g);
+      asm volatile("griddepcontrol.wait;" ::: "memory");
+      const bool skip = *((volatile const int32_t*)&st->done) != 0;
+      if (!skip && myblocks > 0) {
         ++nx[0];
         mbar_expect_tx(&S.xfull[0], BLOCK_CELLS * 8);
         bulk_g2s(S.xt[0], xin + (size_t)blockIdx.x * BLOCK_CELLS, BLOCK_CELLS * 8, &S.xfull[0]);
       }
-      for (int blk = blockIdx.x; blk < nb && ok; blk += gridDim.x, ++m) {
-        const double* sb = stream + (size_t)blk * STREAM_BLOCK;
-        for (int j = 0; j < SLOTS && ok; ++j) {
-          const int s = g % STAGES;
-          const uint32_t u = g / STAGES;
-          if (!(ok = mbar_wait(&S.empty[s], (u & 1) ^ 1, abort_flag, ROLE_PRODUCER))) break;
-          ++g;
-          // slot j: stream chunks CPT*j .. CPT*j+CPT-1 (colour = j / (SLOTS/2)),
-          // contiguous in the stream
-          mbar_expect_tx(&S.full[s], SLOT_BYTES);
-          bulk_g2s(S.ring[s], sb + (size_t)j * CPT * STREAM_CHUNK, SLOT_BYTES, &S.full[s]);
-          if (j == X_ISSUE_AT && blk + (int)gridDim.x < nb) {
-            // x of block m+1 into the buffer block m-1 used (released by now:
-            // the consumers are in block m)
-            const int xb = (m + 1) & 1;
-            if (m >= 1 && !(ok = mbar_wait(&S.xempty[xb], ((m - 1) >> 1) & 1, abort_flag,
-                                           ROLE_PRODUCER)))
-              break;
-            ++nx[xb];
-            mbar_expect_tx(&S.xfull[xb], BLOCK_CELLS * 8);
-            bulk_g2s(S.xt[xb], xin + (size_t)(blk + gridDim.x) * BLOCK_CELLS, BLOCK_CELLS * 8,
-                     &S.xfull[xb]);
-          }
+      for (; !skip && ok && g < (uint32_t)total_slots; ++g) {
+        const int s = g % STAGES;
+        const uint32_t u = g / STAGES;
+        if (!(ok = mbar_wait(&S.empty[s], (u & 1) ^ 1, abort_flag, ROLE_PRODUCER))) break;
+        issue_slot(g);
+        const int m = g / SLOTS, j = g % SLOTS;
+        const int blk = blockIdx.x + m * gridDim.x;
+        if (j == X_ISSUE_AT && blk + (int)gridDim.x < nb) {
+          // x of block m+1 into the buffer block m-1 used (released by now:
+          // the consumers are in block m)
+          const int xb = (m + 1) & 1;
+          if (m >= 1 &&
+              !(ok = mbar_wait(&S.xempty[xb], ((m - 1) >> 1) & 1, abort_flag, ROLE_PRODUCER)))
+            break;
+          ++nx[xb];
+          mbar_expect_tx(&S.xfull[xb], BLOCK_CELLS * 8);
+          bulk_g2s(S.xt[xb], xin + (size_t)(blk + gridDim.x) * BLOCK_CELLS, BLOCK_CELLS * 8,
+                   &S.xfull[xb]);
         }
       }
       // Drain: the last armed phase of every barrier a copy completes on must
@@ -235,13 +246,17 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
         if (nx[b])
           for (uint32_t i = 0; i < DRAIN_LIMIT; ++i)
             if (mbar_try_wait(&S.xfull[b], (nx[b] - 1) & 1)) break;
+    } else {
+      asm volatile("griddepcontrol.wait;" ::: "memory");
     }
   } else if (tid < CONS0) {
     // ----------------------------------------------------------- gatherers
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int gt = tid - GATHER0;
     const int grp = gt >> 7, p0 = gt & 127, p1 = p0 + 128;
     int m = 0;
-    for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++m) {
+    const bool skip = *((volatile const int32_t*)&st->done) != 0;
+    for (int blk = blockIdx.x; !skip && blk < nb; blk += gridDim.x, ++m) {
       const int gb = m & 1;
       if (m >= 2 && !mbar_wait(&S.gempty[gb], ((m - 2) >> 1) & 1, abort_flag, ROLE_GATHER)) break;
       const double dx = C.dx[blk];
@@ -268,12 +283,14 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
     // Every consumer executes the same sequence of named barriers, warp
     // syncs and shuffles whatever happens; only the work is predicated on
     // 'live', which drops when a wait gives up.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int ct = tid - CONS0;
     const int lane = ct & 31, warp = ct >> 5;
     uint32_t g = 0;
     int m = 0;
     bool live = true;
-    for (int blk = blockIdx.x; blk < nb; blk += gridDim.x, ++m) {
+    const bool skip = *((volatile const int32_t*)&st->done) != 0;
+    for (int blk = blockIdx.x; !skip && blk < nb; blk += gridDim.x, ++m) {
       const int xb = m & 1;
       const uint32_t par = (m >> 1) & 1;
       live = live && mbar_wait(&S.xfull[xb], par, abort_flag, ROLE_CONSUMER);
@@ -361,6 +378,7 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
   }
 
   __syncthreads();
+  if (*((volatile const int32_t*)&st->done) != 0 && !*abort_flag) return;
   if (*abort_flag) {
     if (tid == 0) {
       atomicOr(&st->timeout_where, *abort_flag);
@@ -404,7 +422,7 @@ bool g_attr_set[4] = {false, false, false, false};
 template <bool R, bool W>
 void launch_one(cudaStream_t s, const KCtx& C, const double* xin, double* xout,
                 const double* stream, const double* gst, double omega, double* partials,
-                SolveState* st, int fin, int iter, int slot) {
+                SolveState* st, int fin, int iter, int slot, bool pdl) {
   const size_t smem = sizeof(pipe::Smem);
   if (!g_attr_set[slot]) {
     cudaFuncSetAttribute(rbgs_pipelined_kernel<R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -412,14 +430,24 @@ void launch_one(cudaStream_t s, const KCtx& C, const double* xin, double* xout,
     g_attr_set[slot] = true;
   }
   const int grid = C.nb < g_sm_count ? C.nb : g_sm_count;
-  rbgs_pipelined_kernel<R, W><<<grid, pipe::NTHREADS, smem, s>>>(C, xin, xout, stream, gst,
-                                                                 omega, partials, st, fin, iter);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(pipe::NTHREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = pdl ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, rbgs_pipelined_kernel<R, W>, C, xin, xout, stream, gst, omega, partials,
+                     st, fin, iter);
 }
 }  // namespace
 
 void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
                  double* xout, const double* stream, const double* gst, double omega,
-                 double* partials, SolveState* st, int fin, int iter) {
+                 double* partials, SolveState* st, int fin, int iter, bool pdl) {
   if (g_sm_count == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -427,11 +455,11 @@ void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const doub
     if (g_sm_count <= 0) g_sm_count = 1;
   }
   if (res && sweep)
-    launch_one<true, true>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 0);
+    launch_one<true, true>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 0, pdl);
   else if (sweep)
-    launch_one<false, true>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 1);
+    launch_one<false, true>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 1, pdl);
   else
-    launch_one<true, false>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 2);
+    launch_one<true, false>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 2, pdl);
 }
 
 size_t rbgs_pipelined_smem_bytes() { return sizeof(pipe::Smem); }
