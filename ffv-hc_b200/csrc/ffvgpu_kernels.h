@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "ffvgpu_layout.h"
@@ -54,5 +55,8 @@ void launch_assemble(cudaStream_t s, const KCtx& C, const double* ux, const doub
                      double* vface, double rhof, double dt, size_t field_stride);
 void launch_fold_bc(cudaStream_t s, const KCtx& C, double* A, double* b);
 void launch_fill(cudaStream_t s, int nb, double* x, size_t stride, double* g, double value);
+
+// Sets the message ffvgpu_last_error() returns on this thread.
+void set_last_error(const std::string& msg);
 
 }  // namespace ffvgpu

@@ -349,6 +349,8 @@ int64_t interior_bytes(const ffvgpu_pool* P, int words) {
 
 }  // namespace
 
+void ffvgpu::set_last_error(const std::string& msg) { g_last_error = msg; }
+
 extern "C" {
 
 int32_t ffvgpu_version(void) { return 1; }

@@ -34,7 +34,7 @@ EXPORTS = [
     "ffvgpu_solve_rbgs", "ffvgpu_solve_cg", "ffvgpu_rbgs_sweep", "ffvgpu_calc_r2",
     "ffvgpu_dot", "ffvgpu_version", "ffvgpu_last_error", "ffvgpu_sphere_grid_create",
     "ffvgpu_sphere_grid_destroy", "ffvgpu_sphere_grid_num_blocks",
-    "ffvgpu_sphere_grid_blocks", "ffvgpu_sphere_grid_fill",
+    "ffvgpu_sphere_grid_blocks", "ffvgpu_sphere_grid_fill", "ffvgpu_dot_noalloc",
 ]
 
 
@@ -115,6 +115,7 @@ def lib():
         L.ffvgpu_sphere_grid_blocks.argtypes = [vp, vp, vp]
         L.ffvgpu_sphere_grid_blocks.restype = None
         L.ffvgpu_sphere_grid_fill.argtypes = [vp, ctypes.c_uint64, dbl, i32, vp, vp, vp, vp, vp, vp]
+        L.ffvgpu_dot_noalloc.argtypes = [vp, vp, i32, vp, vp]
         _lib = L
     return _lib
 

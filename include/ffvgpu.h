@@ -187,6 +187,26 @@ ffvgpu_status ffvgpu_calc_r2(ffvgpu_pool* pool, double* rr);
 /* DOT (FFVILS.h:298-328) of two real fields. */
 ffvgpu_status ffvgpu_dot(ffvgpu_pool* pool, ffvgpu_field x, ffvgpu_field y, double* xy);
 
+/* Dot product of two device vectors that allocates nothing.  This entry
+ * point has no counterpart in the reference.  It is for callers that cannot
+ * call cudaMalloc: applications that hand the whole device memory to their
+ * own allocator at start-up, and loops that must not stall on the device
+ * synchronisation cudaMalloc/cudaFree bring.  x and y are caller-owned
+ * device arrays of num_blocks * 4096 doubles in the pool's device layout
+ * (per block, cells in the colour-split order of the pool, so the result is
+ * bit for bit what ffvgpu_dot returns for the same fields); result is a
+ * caller-owned device double; stream is a cudaStream_t (NULL = default).
+ * The per-block partial sums live in one fixed array compiled into the
+ * library, FFVGPU_NOALLOC_MAX_BLOCKS doubles per GPU, held until the process
+ * exits; larger num_blocks is rejected with FFVGPU_BAD_ARG.  The first call
+ * on a device looks the array up for that device, so make it before any
+ * stream capture.  Every call on a device shares the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The call is
+ * asynchronous on the stream. */
+#define FFVGPU_NOALLOC_MAX_BLOCKS 65536
+ffvgpu_status ffvgpu_dot_noalloc(const double* x, const double* y, int32_t num_blocks,
+                                 double* result, void* stream);
+
 /* Sums (CalcR2, DOT, the norms inside the solves) use one fixed reduction
  * tree, so every result is bit-reproducible run to run. */
 int32_t ffvgpu_version(void);
