@@ -267,6 +267,26 @@ __device__ __forceinline__ void finalize(SolveState* st, double total, int fin, 
       st->qp = total;
       st->alpha = st->rr1 / total;
       break;
+    case FIN_BI_RR1:
+      st->rr1 = total;
+      if (fabs(total) < (double)FLT_MIN) {  // FFVILS.h:847-851
+        st->residual = total;
+        st->count = 0;
+        st->done = 1;
+      } else {
+        st->beta = total / st->rr0 * st->alpha / st->gamma;
+      }
+      break;
+    case FIN_BI_QR0:
+      st->qp = total;
+      st->alpha = st->rr1 / total;
+      break;
+    case FIN_BI_TS:
+      st->ts = total;
+      break;
+    case FIN_BI_TT:
+      st->gamma = st->ts / total;
+      break;
   }
 }
 

@@ -36,6 +36,15 @@ void launch_p_update(cudaStream_t s, const KCtx& C, const double* z, double* p, 
                      SolveState* st);
 void launch_ax_dot(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
                    double* partials, SolveState* st);
+void launch_ax_dot_y(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
+                     const double* y, double* partials, SolveState* st, int fin);
+void launch_bicg_p(cudaStream_t s, const KCtx& C, const double* r, double* p, const double* q,
+                   int first, SolveState* st);
+void launch_axpyz(cudaStream_t s, const KCtx& C, double* z, const double* x, const double* y,
+                  SolveState* st);
+void launch_bicg_update(cudaStream_t s, const KCtx& C, double* x, const double* pz,
+                        const double* sz, double* r, const double* t, const double* sv,
+                        double* partials, SolveState* st, int iter);
 void launch_cg_update(cudaStream_t s, const KCtx& C, double* x, const double* p, double* r,
                       const double* q, double* partials, SolveState* st, int iter);
 void launch_dot(cudaStream_t s, const KCtx& C, const double* x, const double* y,

@@ -67,6 +67,7 @@ struct BCSet {
 struct SolveState {
   double bb, rr, residual;
   double rr0, rr1, alpha, beta, qp;
+  double gamma, ts;  // BiCGSTAB: gamma = t.s / t.t, and t.s
   double eps;
   int32_t count;     // reference loop-variable value at exit
   int32_t done;      // 1 once the solve has stopped; later kernels return at entry
@@ -91,7 +92,11 @@ enum Fin : int {
   FIN_RBGS,       // residual of RBGS iteration 'iter' (FFVILS.h:547-594)
   FIN_CG_RR1,     // rr1 = r.z; early exit if |rr1| < FLT_MIN (FFVILS.h:712-724)
   FIN_CG_QP,      // qp = q.p; alpha = rr1/qp (FFVILS.h:750-758)
-  FIN_CG_RR       // residual of CG iteration 'iter'; rr0 = rr1 (FFVILS.h:774-788)
+  FIN_CG_RR,      // residual of CG iteration 'iter'; rr0 = rr1 (FFVILS.h:774-788)
+  FIN_BI_RR1,     // BiCGSTAB rr1 = r.r0; early exit; beta = rr1/rr0*alpha/gamma (FFVILS.h:845-859)
+  FIN_BI_QR0,     // BiCGSTAB alpha = rr1 / (q_.r0) (FFVILS.h:890-896)
+  FIN_BI_TS,      // BiCGSTAB t_.s (FFVILS.h:923-929)
+  FIN_BI_TT       // BiCGSTAB gamma = t_s / (t_.t_) (FFVILS.h:930-936)
 };
 
 FFVGPU_HD inline int sidx(int i, int j, int k) {

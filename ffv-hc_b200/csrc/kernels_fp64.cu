@@ -214,10 +214,12 @@ p_update_kernel(const double* __restrict__ z, double* __restrict__ p, int first,
   }
 }
 
-// q = A p (calc_ax, bils.f90:162-206) and q.p (FFVILS.h:750-756 DOT(q, p)).
+// q = A p (calc_ax, bils.f90:162-206) and q.y (DOT(q, y), blas.f90:466-499):
+// y = p for CG (FFVILS.h:750-756), r0 or s for BiCGSTAB (FFVILS.h:890, 923).
 __global__ void __launch_bounds__(THREADS, 3)
 ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A,
-              double* __restrict__ q, double* __restrict__ partials, SolveState* st) {
+              double* __restrict__ q, const double* __restrict__ y,
+              double* __restrict__ partials, SolveState* st, int fin) {
   if (solve_done(st)) return;
   __shared__ double xs[TILE];
   const int blk = blockIdx.x, tid = threadIdx.x;
@@ -225,6 +227,7 @@ ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A
   __syncthreads();
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
   double* qo = q + (size_t)blk * BLOCK_CELLS;
+  const double* yb = y ? y + (size_t)blk * BLOCK_CELLS : nullptr;
   double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
@@ -239,10 +242,71 @@ ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A
                        __ldg(Ab + 20480 + s) * xs[t - TP] + __ldg(Ab + 24576 + s) * xs[t + TP] +
                        __ldg(Ab + s) * xs[t];
       qo[s] = v;
-      acc[c][m & 1] += v * xs[t];
+      acc[c][m & 1] += v * (yb ? __ldg(yb + s) : xs[t]);
     }
   }
-  reduce_finalize(acc, partials, st, FIN_CG_QP, 0);
+  reduce_finalize(acc, partials, st, fin, 0);
+}
+
+// BiCGSTAB p update (FFVILS.h:853-871): first iteration p = r (copy); after
+// it AXPY(p, q_, -gamma) then XPAY(p, r, beta), i.e. per cell
+// t = p + (-gamma)*q_ ; p = r + beta*t (blas.f90:329-395).
+__global__ void __launch_bounds__(THREADS)
+bicg_p_kernel(const double* __restrict__ r, double* __restrict__ p, const double* __restrict__ q,
+              int first, SolveState* st) {
+  if (solve_done(st)) return;
+  const double beta = st->beta, mgamma = -st->gamma;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+#pragma unroll 4
+  for (int m = 0; m < 16; ++m) {
+    const size_t s = base + threadIdx.x + THREADS * m;
+    if (first) {
+      p[s] = r[s];
+    } else {
+      const double t = p[s] + mgamma * q[s];
+      p[s] = r[s] + beta * t;
+    }
+  }
+}
+
+// AXPYZ (blas.f90:397-430): z = a*x + y with a = -alpha (FFVILS.h:898-903).
+__global__ void __launch_bounds__(THREADS)
+axpyz_kernel(double* __restrict__ z, const double* __restrict__ x, const double* __restrict__ y,
+             SolveState* st) {
+  if (solve_done(st)) return;
+  const double a = -st->alpha;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+#pragma unroll 4
+  for (int m = 0; m < 16; ++m) {
+    const size_t s = base + threadIdx.x + THREADS * m;
+    z[s] = a * x[s] + y[s];
+  }
+}
+
+// BiCGSTAB update (FFVILS.h:938-958): AXPBYPZ(x, p_, s_, alpha, gamma)
+// (x = alpha*p_ + gamma*s_ + x, blas.f90:432-464), AXPYZ(r, t_, s, -gamma)
+// (r = (-gamma)*t_ + s), and r.r for IsConverged.
+__global__ void __launch_bounds__(THREADS)
+bicg_update_kernel(double* __restrict__ x, const double* __restrict__ pz,
+                   const double* __restrict__ sz, double* __restrict__ r,
+                   const double* __restrict__ t, const double* __restrict__ s,
+                   double* __restrict__ partials, SolveState* st, int iter) {
+  if (solve_done(st)) return;
+  const double alpha = st->alpha, gamma = st->gamma, mgamma = -st->gamma;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll 4
+    for (int m = 0; m < 8; ++m) {
+      const size_t i = base + c * HALF_CELLS + threadIdx.x + THREADS * m;
+      x[i] = alpha * pz[i] + gamma * sz[i] + x[i];
+      const double rn = mgamma * t[i] + s[i];
+      r[i] = rn;
+      acc[c][m & 1] += rn * rn;
+    }
+  }
+  reduce_finalize(acc, partials, st, FIN_CG_RR, iter);
 }
 
 // x = x + alpha p; r = r + (-alpha) q (axpy, blas.f90:329-361); r.r.
@@ -556,7 +620,24 @@ void launch_p_update(cudaStream_t s, const KCtx& C, const double* z, double* p, 
 }
 void launch_ax_dot(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
                    double* partials, SolveState* st) {
-  ax_dot_kernel<<<C.nb, THREADS, 0, s>>>(C, p, A, q, partials, st);
+  ax_dot_kernel<<<C.nb, THREADS, 0, s>>>(C, p, A, q, nullptr, partials, st, FIN_CG_QP);
+}
+void launch_ax_dot_y(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
+                     const double* y, double* partials, SolveState* st, int fin) {
+  ax_dot_kernel<<<C.nb, THREADS, 0, s>>>(C, p, A, q, y, partials, st, fin);
+}
+void launch_bicg_p(cudaStream_t s, const KCtx& C, const double* r, double* p, const double* q,
+                   int first, SolveState* st) {
+  bicg_p_kernel<<<C.nb, THREADS, 0, s>>>(r, p, q, first, st);
+}
+void launch_axpyz(cudaStream_t s, const KCtx& C, double* z, const double* x, const double* y,
+                  SolveState* st) {
+  axpyz_kernel<<<C.nb, THREADS, 0, s>>>(z, x, y, st);
+}
+void launch_bicg_update(cudaStream_t s, const KCtx& C, double* x, const double* pz,
+                        const double* sz, double* r, const double* t, const double* sv,
+                        double* partials, SolveState* st, int iter) {
+  bicg_update_kernel<<<C.nb, THREADS, 0, s>>>(x, pz, sz, r, t, sv, partials, st, iter);
 }
 void launch_cg_update(cudaStream_t s, const KCtx& C, double* x, const double* p, double* r,
                       const double* q, double* partials, SolveState* st, int iter) {

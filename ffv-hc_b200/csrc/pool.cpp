@@ -82,6 +82,10 @@ struct ffvgpu_pool {
   double* p = nullptr;
   double* q = nullptr;
   double* z[2] = {nullptr, nullptr};
+  double* r0 = nullptr;            // BiCGSTAB shadow residual
+  double* sv = nullptr;            // BiCGSTAB s
+  double* tv = nullptr;            // BiCGSTAB t_
+  double* zb[2] = {nullptr, nullptr};  // BiCGSTAB s_ (Jacobi iterates)
   double* partials = nullptr;
   SolveState* st = nullptr;
   double* hist_d = nullptr;
@@ -197,6 +201,7 @@ ffvgpu_status reset_state(ffvgpu_pool* P, double eps, int count_max, double* his
   h.eps = eps;
   h.count_max = count_max;
   h.rr0 = 1.0;
+  h.gamma = 1.0;  // FFVILS.h:841-842: alpha = 0, gamma = 1 before the first iteration
   h.hist = hist;
   CK(cudaMemcpyAsync(P->st, &h, sizeof(h), cudaMemcpyHostToDevice, P->stream));
   return FFVGPU_OK;
@@ -438,7 +443,8 @@ void ffvgpu_pool_destroy(ffvgpu_pool* P) {
   if (P->own_stream) cudaStreamSynchronize(P->own_stream);
   void* ptrs[] = {P->x[0], P->x[1], P->gx, P->A, P->coef, P->b, P->u[0], P->u[1], P->u[2],
                   P->gu[0], P->gu[1], P->gu[2], P->cut, P->vface, P->flags, P->r,
-                  P->p, P->q, P->z[0], P->z[1], P->partials, P->st, P->hist_d,
+                  P->p, P->q, P->z[0], P->z[1], P->r0, P->sv, P->tv, P->zb[0], P->zb[1],
+                  P->partials, P->st, P->hist_d,
                   P->stage, P->nbr_d, P->dx_d};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -842,6 +848,119 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   CK(cudaGetLastError());
   if ((s = read_state(P, &h))) return s;
   launch_exchange(P->stream, C, x, P->gx);  // FFVILS.h:790
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(P->stream));
+  float ms = 0.f, sms = 0.f;
+  cudaEventElapsedTime(&ms, P->ev0, P->ev1);
+  cudaEventElapsedTime(&sms, P->ev2, P->ev3);
+  R.sweep_ms = sms;
+  R.sweep_launches = launches - launches_before;
+  R.count = h.done ? h.count : (N + 1);
+  R.residual = h.residual;
+  R.elapsed_ms = ms;
+  R.bytes_moved = bytes;
+  R.kernel_launches = launches + 1;
+  if (prm->history && N > 0) {
+    const int nh = (h.count >= 1 && h.count <= N) ? h.count : (h.count == 0 ? 0 : N);
+    if (nh > 0)
+      CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+  }
+  if (res) *res = R;
+  return solve_status(h, prm, N, R.count);
+}
+
+
+// Jacobi_PreConditioner (FFVILS.h:469-492) from z = 0 with right-hand side
+// rhs: K passes through the two buffers zz; returns the buffer holding the
+// result.  K = 0 leaves the zero field.
+static double* jacobi_pre(ffvgpu_pool* P, const KCtx& C, double* const zz[2], const double* rhs,
+                          int K, double omega, int64_t& bytes, int& launches) {
+  if (K <= 0) {
+    launch_fill(P->stream, P->nb, zz[0], BC, nullptr, 0.0);
+    bytes += interior_bytes(P, 1);
+    launches++;
+    return zz[0];
+  }
+  launch_jacobi(P->stream, C, true, false, nullptr, zz[0], P->A, rhs, omega, P->partials, P->st);
+  bytes += interior_bytes(P, 9);
+  launches++;
+  for (int k = 2; k <= K; ++k) {
+    launch_jacobi(P->stream, C, false, false, zz[(k - 2) & 1], zz[(k - 1) & 1], P->A, rhs, omega,
+                  P->partials, P->st);
+    bytes += interior_bytes(P, 10);
+    launches++;
+  }
+  return zz[(K - 1) & 1];
+}
+
+// FFVILS::BiCGSTAB (src/FFV/FFVILS.h:793-974), Jacobi-preconditioned: the
+// reference's default pressure solver.  As in CG, guide cells of p and s are
+// never read by a stencil (they are right-hand sides of the preconditioner
+// and operands of dots), so their exchanges are value-neutral and not run;
+// those of p_ and s_ are the gathers of the Jacobi and A*p kernels.
+ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
+                                    ffvgpu_result* res) {
+  if (!P || !prm) return bad("null argument");
+  cudaSetDevice(P->device);
+  ffvgpu_status s;
+  if ((s = require_system(P))) return s;
+  const size_t n = field_count(P);
+  if ((s = dalloc_t(P, &P->r, n)) || (s = dalloc_t(P, &P->r0, n)) || (s = dalloc_t(P, &P->p, n)) ||
+      (s = dalloc_t(P, &P->q, n)) || (s = dalloc_t(P, &P->sv, n)) || (s = dalloc_t(P, &P->tv, n)) ||
+      (s = dalloc_t(P, &P->z[0], n)) || (s = dalloc_t(P, &P->z[1], n)) ||
+      (s = dalloc_t(P, &P->zb[0], n)) || (s = dalloc_t(P, &P->zb[1], n)))
+    return s;
+  const int N = prm->count_max;
+  ffvgpu_result R;
+  std::memset(&R, 0, sizeof(R));
+  if ((s = ensure_hist(P, N > 0 ? N : 1))) return s;
+  if ((s = reset_state(P, prm->epsilon, N, P->hist_d))) return s;
+  const KCtx C = P->ctx(P->bc_p);
+  const int every = prm->check_every > 0 ? prm->check_every : 16;
+  const bool poll = prm->epsilon > 0.0;
+  double* x = P->x[P->xcur];
+  CK(cudaEventRecord(P->ev0, P->stream));
+  launch_dot(P->stream, C, P->b, P->b, P->partials, P->st, FIN_BB, 0);
+  int launches = 1;
+  int64_t bytes = interior_bytes(P, 2);
+  SolveState h;
+  if ((s = read_state(P, &h))) return s;
+  if (std::fabs(h.bb) < (double)FLT_MIN) {  // FFVILS.h:822-826
+    R.count = 0;
+    R.residual = 0.0;
+    if (res) *res = R;
+    return FFVGPU_OK;
+  }
+  launch_calc_r(P->stream, C, x, P->gx, P->A, P->b, P->r, P->st);  // FFVILS.h:828
+  CK(cudaMemcpyAsync(P->r0, P->r, n * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
+  launches++;
+  bytes += interior_bytes(P, 10 + 2);
+  const int K = prm->pre_count;
+  CK(cudaEventRecord(P->ev2, P->stream));
+  const int launches_before = launches;
+  for (int c = 1; c <= N; ++c) {
+    launch_dot(P->stream, C, P->r, P->r0, P->partials, P->st, FIN_BI_RR1, c);  // rr1
+    launch_bicg_p(P->stream, C, P->r, P->p, P->q, c == 1 ? 1 : 0, P->st);
+    const double* pz = jacobi_pre(P, C, P->z, P->p, K, prm->omega, bytes, launches);
+    launch_ax_dot_y(P->stream, C, pz, P->A, P->q, P->r0, P->partials, P->st, FIN_BI_QR0);
+    launch_axpyz(P->stream, C, P->sv, P->q, P->r, P->st);
+    const double* sz = jacobi_pre(P, C, P->zb, P->sv, K, prm->omega, bytes, launches);
+    launch_ax_dot_y(P->stream, C, sz, P->A, P->tv, P->sv, P->partials, P->st, FIN_BI_TS);
+    launch_dot(P->stream, C, P->tv, P->tv, P->partials, P->st, FIN_BI_TT, c);
+    launch_bicg_update(P->stream, C, x, pz, sz, P->r, P->tv, P->sv, P->partials, P->st, c);
+    launches += 7;
+    bytes += interior_bytes(P, 2 + (c == 1 ? 2 : 4) + 9 + 3 + 9 + 2 + 9);
+    if (poll && (c % every) == 0) {
+      bool done = false;
+      if ((s = poll_done(P, &done))) return s;
+      if (done) break;
+    }
+  }
+  CK(cudaEventRecord(P->ev3, P->stream));
+  CK(cudaEventRecord(P->ev1, P->stream));
+  CK(cudaGetLastError());
+  if ((s = read_state(P, &h))) return s;
+  launch_exchange(P->stream, C, x, P->gx);  // FFVILS.h:973
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(P->stream));
   float ms = 0.f, sms = 0.f;

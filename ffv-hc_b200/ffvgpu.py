@@ -31,7 +31,7 @@ EXPORTS = [
     "ffvgpu_pool_set_stream", "ffvgpu_fill", "ffvgpu_grid_neighbors",
     "ffvgpu_pool_neighbors", "ffvgpu_pool_device_bytes", "ffvgpu_pool_upload",
     "ffvgpu_pool_download", "ffvgpu_exchange", "ffvgpu_assemble_p", "ffvgpu_fold_bc",
-    "ffvgpu_solve_rbgs", "ffvgpu_solve_cg", "ffvgpu_rbgs_sweep", "ffvgpu_calc_r2",
+    "ffvgpu_solve_rbgs", "ffvgpu_solve_cg", "ffvgpu_solve_bicgstab", "ffvgpu_rbgs_sweep", "ffvgpu_calc_r2",
     "ffvgpu_dot", "ffvgpu_version", "ffvgpu_last_error", "ffvgpu_sphere_grid_create",
     "ffvgpu_sphere_grid_destroy", "ffvgpu_sphere_grid_num_blocks",
     "ffvgpu_sphere_grid_blocks", "ffvgpu_sphere_grid_fill", "ffvgpu_dot_noalloc",
@@ -105,6 +105,7 @@ def lib():
         L.ffvgpu_fold_bc.argtypes = [vp]
         L.ffvgpu_solve_rbgs.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
         L.ffvgpu_solve_cg.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
+        L.ffvgpu_solve_bicgstab.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
         L.ffvgpu_rbgs_sweep.argtypes = [vp, dbl]
         L.ffvgpu_calc_r2.argtypes = [vp, ctypes.POINTER(dbl)]
         L.ffvgpu_dot.argtypes = [vp, i32, i32, ctypes.POINTER(dbl)]
@@ -315,6 +316,11 @@ class Pool:
                  check_every=0):
         return self._solve(lib().ffvgpu_solve_cg, "solve_cg", omega, count_max, epsilon,
                            pre_count, history, check_every)
+
+    def solve_bicgstab(self, omega=1.0, pre_count=2, count_max=1000, epsilon=1e-10,
+                       history=True, check_every=0):
+        return self._solve(lib().ffvgpu_solve_bicgstab, "solve_bicgstab", omega, count_max,
+                           epsilon, pre_count, history, check_every)
 
     def set_stream(self, stream_handle):
         """Enqueue on a caller's CUDA stream (an int cudaStream_t, 0/None = own)."""

@@ -43,6 +43,16 @@ class FFVILSGpu {
     return finish(s, res, count, residual);
   }
 
+  // FFVILS::BiCGSTAB (FFVILS.h:793-974).
+  ffvgpu_status BiCGSTAB(ffvgpu_pool* pool, double omega, int countPreConditioner, int countMax,
+                         double epsilon, int& count, double& residual,
+                         double* history = nullptr) {
+    ffvgpu_iter_params prm = {omega, countMax, epsilon, countPreConditioner, 0, history};
+    ffvgpu_result res;
+    const ffvgpu_status s = ffvgpu_solve_bicgstab(pool, &prm, &res);
+    return finish(s, res, count, residual);
+  }
+
   // FFVILS::Fill (FFVILS.h:425-445).
   ffvgpu_status Fill(ffvgpu_pool* pool, ffvgpu_field field, double value) {
     return check(ffvgpu_fill(pool, field, value), "Fill");

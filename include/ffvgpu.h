@@ -178,6 +178,12 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* pool, const ffvgpu_iter_params* prm,
  * real field, guide cells included, set to value. */
 ffvgpu_status ffvgpu_fill(ffvgpu_pool* pool, ffvgpu_field field, double value);
 
+/* Jacobi-preconditioned BiCGSTAB on FIELD_X: FFVILS::BiCGSTAB
+ * (src/FFV/FFVILS.h:793-974), the reference's default pressure solver
+ * (src/FFV/Solver.cpp:5620-5676). */
+ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* pool, const ffvgpu_iter_params* prm,
+                                    ffvgpu_result* res);
+
 /* Single kernels of the path, for parity tests and for callers that drive
  * their own loop.  Each matches one FFVILS helper. */
 /* RBGS_Smoother (FFVILS.h:104-162): both colours on every block + exchange. */

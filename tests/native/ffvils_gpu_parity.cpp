@@ -4,7 +4,7 @@
 // oracle (linked for the comparison only).
 //
 // Steps: synthetic sphere grid -> exchange u (P02) -> bcut_calc_ab_p (P03)
-// -> fold outer BCs (P05) -> RBGS -> CG -> exchange p (P07).
+// -> fold outer BCs (P05) -> RBGS -> CG -> BiCGSTAB -> exchange p (P07).
 // Exit status 0 when every residual and every pressure value is identical.
 #include <cmath>
 #include <cstdint>
@@ -32,6 +32,8 @@ int orc_rbgs(Oracle*, double omega, int countMax, double eps, int* count, double
              double* hist);
 int orc_cg(Oracle*, double omega, int countPre, int countMax, double eps, int* count,
            double* residual, double* hist);
+int orc_bicgstab(Oracle*, double omega, int countPre, int countMax, double eps, int* count,
+                 double* residual, double* hist);
 }
 
 static int fail(const char* what) {
@@ -140,6 +142,13 @@ int main(int argc, char** argv) {
   if (count != ocount || residual != oresidual) bad++;
   const int nh = (count >= 1 && count <= cgmax) ? count : cgmax;
   for (int i = 0; i < nh; ++i) bad += cg_g[i] != cg_o[i];
+  // then the reference's default solver from the current x
+  std::vector<double> bi_g(cgmax), bi_o(cgmax);
+  ils.BiCGSTAB(pool, 1.0, 2, cgmax, 1e-12, count, residual, bi_g.data());
+  orc_bicgstab(O, 1.0, 2, cgmax, 1e-12, &ocount, &oresidual, bi_o.data());
+  if (count != ocount || residual != oresidual) bad++;
+  const int nb2 = (count >= 1 && count <= cgmax) ? count : cgmax;
+  for (int i = 0; i < nb2; ++i) bad += bi_g[i] != bi_o[i];
   std::vector<double> p(n);
   if (ffvgpu_pool_download(pool, FFVGPU_FIELD_X, p.data(), vc) != FFVGPU_OK) return fail("download");
   const double* po = orc_field(O, 0);

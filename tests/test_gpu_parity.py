@@ -234,3 +234,41 @@ def test_nan_rhs_is_reported_not_fatal():
     r = P.solve_rbgs(1.5, 5, 0.0)
     assert r["status"] == ffvgpu.OK
     P.close()
+
+
+@pytest.mark.parametrize("level,radius,count,eps", [(0, 0.5, 300, 1e-10), (2, 0.5, 60, 1e-10),
+                                                    (2, 0.5, 400, 1e-6)])
+def test_bicgstab_solve_bitwise(level, radius, count, eps):
+    """FFVILS::BiCGSTAB, the reference's default pressure solver."""
+    g, inp, O = problem(level, threads=THREADS, radius=radius)
+    P = device_problem(g, inp)
+    x0 = np.zeros((g.nb, 20, 20, 20))
+    O.field("X")[...] = x0
+    P.upload("X", x0, VC)
+    ro = O.solve_bicgstab(1.0, 2, count, eps)
+    rg = P.solve_bicgstab(1.0, 2, count, eps)
+    assert rg["count"] == ro["count"], (rg["count"], ro["count"])
+    assert_bitwise(rg["history"], ro["history"], "residual history")
+    assert_bitwise(interior(P.download("X", VC)), interior(O.field("X")), "pressure")
+    if eps >= 1e-6:
+        assert ro["residual"] <= eps  # converges on the refined, non-symmetric grid
+    P.close()
+
+
+def test_bicgstab_after_rbsor_and_edge_cases():
+    g, inp, O = problem(1, threads=THREADS)
+    P = device_problem(g, inp)
+    x0 = np.zeros((g.nb, 20, 20, 20))
+    O.field("X")[...] = x0
+    P.upload("X", x0, VC)
+    O.solve_rbgs(1.2, 10, 0.0)
+    P.solve_rbgs(1.2, 10, 0.0)
+    ro = O.solve_bicgstab(1.0, 3, 25, 1e-12)
+    rg = P.solve_bicgstab(1.0, 3, 25, 1e-12)
+    assert rg["count"] == ro["count"]
+    assert_bitwise(rg["history"], ro["history"], "history after RBSOR")
+    assert_bitwise(interior(P.download("X", VC)), interior(O.field("X")), "pressure")
+    # PreCount = 0: p_ = 0, alpha = rr1 / 0 -> NaN residual (the reference exits)
+    r = P.solve_bicgstab(1.0, 0, 5, 1e-10)
+    assert r["status"] == ffvgpu.NAN_DETECTED and r["count"] == 1
+    P.close()
