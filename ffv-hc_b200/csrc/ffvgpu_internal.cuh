@@ -24,13 +24,17 @@ __device__ __forceinline__ void intp_index(int i, int n, int& ic, double& r) {
   }
 }
 
-__device__ __forceinline__ double ld(const double* __restrict__ x, int blk, int i, int j, int k) {
-  return __ldg(x + (size_t)blk * BLOCK_CELLS + sidx(i, j, k));
+// Interior value of cell (i, j, k) of block blk, widened to double (exact
+// for float sources, whose guide cells are formed in double arithmetic).
+template <typename T>
+__device__ __forceinline__ double ld(const T* __restrict__ x, int blk, int i, int j, int k) {
+  return (double)__ldg(x + (size_t)blk * BLOCK_CELLS + sidx(i, j, k));
 }
 
 // Value of guide cell (layer L = 1 or 2) of face 'face' of block 'blk' at
 // transverse position (a, b) in [0,16)^2, computed from interior values of x.
-static __device__ __noinline__ double guide_value(const double* __restrict__ x, int blk, int face,
+template <typename T>
+static __device__ __noinline__ double guide_value(const T* __restrict__ x, int blk, int face,
                                            int a, int b, int L, const FaceNbr& nb,
                                            const BCSet& bc, double dx) {
   const int axis = face >> 1;
@@ -116,7 +120,8 @@ static __device__ __noinline__ double guide_value(const double* __restrict__ x, 
 // [0, 256) (p = v*16 + u), with every load of both issued before any is
 // used: the batched form of guide_value for the pipelined kernels.  Same
 // expressions, same evaluation order, same results as guide_value.
-__device__ __forceinline__ void guide_pair(const double* __restrict__ x, int blk, int face,
+template <typename T>
+__device__ __forceinline__ void guide_pair(const T* __restrict__ x, int blk, int face,
                                            int p0, int p1, const FaceNbr& nb, const BCSet& bc,
                                            double dx, double& v0, double& v1) {
   const int axis = face >> 1;
@@ -196,18 +201,21 @@ __device__ __forceinline__ void guide_pair(const double* __restrict__ x, int blk
 // the other colour's half O of a colour-split block (every face neighbour
 // has the other colour), or from the guide layer G ([face][v][u]) where the
 // neighbour lies outside the block.
-struct Nbrs {
-  double w, e, s, n, b, t;
+template <typename T>
+struct NbrsT {
+  T w, e, s, n, b, t;
 };
-__device__ __forceinline__ Nbrs split_neighbours(const double* __restrict__ O,
-                                           const double* __restrict__ G, int q, int c) {
+using Nbrs = NbrsT<double>;
+template <typename T>
+__device__ __forceinline__ NbrsT<T> split_neighbours(const T* __restrict__ O,
+                                               const T* __restrict__ G, int q, int c) {
   const int ih = q & 7, j = (q >> 3) & 15, k = q >> 7;
   const int p = (j + k + c) & 1;
   const int i = 2 * ih + p;
-  Nbrs r;
-  const double ow = O[max(q - 1 + p, 0)], oe = O[min(q + p, HALF_CELLS - 1)];
-  const double os = O[max(q - 8, 0)], on = O[min(q + 8, HALF_CELLS - 1)];
-  const double ob = O[max(q - 128, 0)], ot = O[min(q + 128, HALF_CELLS - 1)];
+  NbrsT<T> r;
+  const T ow = O[max(q - 1 + p, 0)], oe = O[min(q + p, HALF_CELLS - 1)];
+  const T os = O[max(q - 8, 0)], on = O[min(q + 8, HALF_CELLS - 1)];
+  const T ob = O[max(q - 128, 0)], ot = O[min(q + 128, HALF_CELLS - 1)];
   r.w = (i == 0) ? G[0 * FACE_CELLS + j + 16 * k] : ow;
   r.e = (i == 15) ? G[1 * FACE_CELLS + j + 16 * k] : oe;
   r.s = (j == 0) ? G[2 * FACE_CELLS + i + 16 * k] : os;

@@ -12,11 +12,14 @@ namespace ffvgpu {
 
 // Parameters every block kernel needs: neighbour table, cell sizes and the
 // outer BCs of the field being staged.
+// Kernels that take a block range (exchange, unpack, assembly, BC folding)
+// cover blocks [first, first + nb); the solver kernels run with first = 0.
 struct KCtx {
-  const FaceNbr* nbr;  // [nb][6]
-  const double* dx;    // [nb]
+  const FaceNbr* nbr;  // [blocks][6]
+  const double* dx;    // [blocks]
   BCSet bc;
   int nb;
+  int first;
 };
 
 // Fused residual + red-black sweep over the coefficient stream (rbgs_pipelined.cu).

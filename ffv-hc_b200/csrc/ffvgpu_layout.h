@@ -76,6 +76,19 @@ struct SolveState {
   uint32_t ticket;   // last-block-done counter of the current reduction
   int32_t timeout_where;  // roles whose bounded wait gave up (1 producer, 2 gatherer, 4 consumer)
   double* hist;      // device residual history [count_max] or null
+  int32_t iter;      // mixed form: number of the iteration under way (1-based)
+  int32_t pad_;
+};
+
+// Instances: independent problems that share one pool's blocks (a batch).
+// Each owns the contiguous block range [first, first + count) and its own
+// solver state; blocks of no instance carry -1.  A pool made from one grid
+// is one instance covering every block.
+struct InstTable {
+  const int32_t* blk_inst;  // [capacity]
+  const int32_t* first;     // [instances]
+  const int32_t* count;     // [instances]
+  SolveState* st;           // [instances]
 };
 
 // Sums over a block use one fixed tree of 512 virtual threads: virtual
@@ -96,7 +109,12 @@ enum Fin : int {
   FIN_BI_RR1,     // BiCGSTAB rr1 = r.r0; early exit; beta = rr1/rr0*alpha/gamma (FFVILS.h:845-859)
   FIN_BI_QR0,     // BiCGSTAB alpha = rr1 / (q_.r0) (FFVILS.h:890-896)
   FIN_BI_TS,      // BiCGSTAB t_.s (FFVILS.h:923-929)
-  FIN_BI_TT       // BiCGSTAB gamma = t_s / (t_.t_) (FFVILS.h:930-936)
+  FIN_BI_TT,      // BiCGSTAB gamma = t_s / (t_.t_) (FFVILS.h:930-936)
+  // mixed form, per instance (two sums where noted)
+  FIN_MX_INIT,    // b.b and r.r0: early exits of FFVILS.h:822-826 and 847-851
+  FIN_MX_ALPHA,   // alpha = rr1 / (q.r0)
+  FIN_MX_GAMMA,   // t.s and t.t: gamma = t.s / t.t
+  FIN_MX_UPDATE   // r.r and r.r0: residual, convergence, next rr1 and beta
 };
 
 FFVGPU_HD inline int sidx(int i, int j, int k) {

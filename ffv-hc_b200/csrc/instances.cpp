@@ -1,0 +1,697 @@
+// instances.cpp -- batches of independent pressure problems in one pool, and
+// the mixed-precision solve that runs them (include/ffvgpu.h).
+//
+// A batch pool reserves a block capacity on the device and admits
+// instances into free contiguous block ranges (first fit).  Every kernel of
+// the mixed solve covers the whole capacity; a block looks up its instance
+// and returns at once when the block is free or its instance is not
+// solving.  Each instance has its own solver state, its own reduction
+// ticket and its own sums, taken in block order over its range, so its
+// results do not depend on what else shares the pool.  One iteration of all
+// running instances is a fixed sequence of launches, captured once as a
+// CUDA graph and replayed; the host polls the per-instance states between
+// replays, and an instance admitted while others run joins at the next
+// replay.
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ffvgpu.h"
+#include "ffvgpu_gen.h"
+#include "ffvgpu_kernels.h"
+#include "ffvgpu_layout.h"
+#include "ffvgpu_mixed.h"
+#include "pool_internal.h"
+
+using namespace ffvgpu;
+using namespace ffvgpu::detail;
+
+namespace ffvgpu {
+namespace detail {
+
+void release_instances(ffvgpu_pool* P) {
+  if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
+  P->mgraph = nullptr;
+  void* ptrs[] = {P->blk_inst_d, P->inst_first_d, P->inst_count_d, P->blk_geo_d, P->mst,
+                  P->mpartials, P->mhist, P->mcoef, P->me[0], P->me[1], P->mv32, P->mph,
+                  P->msh};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (P->mst_h) cudaFreeHost(P->mst_h);
+  P->mst_h = nullptr;
+}
+
+}  // namespace detail
+}  // namespace ffvgpu
+
+namespace {
+
+int num_inst(const ffvgpu_pool* P) { return (int)P->inst.size(); }
+
+// Device copies of the instance tables (allocated once, sized by capacity).
+ffvgpu_status ensure_inst_device(ffvgpu_pool* P) {
+  ffvgpu_status s;
+  const int ni = num_inst(P);
+  if ((s = dalloc_t(P, &P->blk_inst_d, (size_t)P->nb)) ||
+      (s = dalloc_t(P, &P->inst_first_d, (size_t)ni)) ||
+      (s = dalloc_t(P, &P->inst_count_d, (size_t)ni)) ||
+      (s = dalloc_t(P, &P->blk_geo_d, (size_t)P->nb * 4)) ||
+      (s = dalloc_t(P, &P->mst, (size_t)ni)) || (s = dalloc_t(P, &P->mpartials, 2 * (size_t)P->nb)))
+    return s;
+  if (!P->mst_h) {
+    cudaError_t e = cudaMallocHost(&P->mst_h, sizeof(SolveState) * ni);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+    std::memset(P->mst_h, 0, sizeof(SolveState) * ni);
+    for (int i = 0; i < ni; ++i) P->mst_h[i].done = 1;  // idle until a solve begins
+    CK(cudaMemcpy(P->mst, P->mst_h, sizeof(SolveState) * ni, cudaMemcpyHostToDevice));
+  }
+  if (P->inst_dirty) {
+    std::vector<int32_t> first(ni), count(ni), geo((size_t)P->nb * 4);
+    for (int i = 0; i < ni; ++i) {
+      first[i] = P->inst[i].first;
+      count[i] = P->inst[i].count;
+    }
+    for (int b = 0; b < P->nb; ++b) {
+      geo[4 * b] = P->level[b];
+      for (int a = 0; a < 3; ++a) geo[4 * b + 1 + a] = P->index[3 * b + a];
+    }
+    CK(cudaMemcpy(P->blk_inst_d, P->blk_inst_h.data(), sizeof(int32_t) * P->nb,
+                  cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P->inst_first_d, first.data(), sizeof(int32_t) * ni, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P->inst_count_d, count.data(), sizeof(int32_t) * ni, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P->blk_geo_d, geo.data(), sizeof(int32_t) * 4 * P->nb, cudaMemcpyHostToDevice));
+    P->inst_dirty = false;
+  }
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P) {
+  ffvgpu_status s;
+  const size_t n = field_count(P);
+  if ((s = dalloc_t(P, &P->mcoef, 7 * n)) || (s = dalloc_t(P, &P->me[0], n)) ||
+      (s = dalloc_t(P, &P->me[1], n)) || (s = dalloc_t(P, &P->mv32, n)) ||
+      (s = dalloc_t(P, &P->mph, n)) || (s = dalloc_t(P, &P->msh, n)) ||
+      (s = dalloc_t(P, &P->r, n)) || (s = dalloc_t(P, &P->r0, n)) || (s = dalloc_t(P, &P->p, n)) ||
+      (s = dalloc_t(P, &P->q, n)) || (s = dalloc_t(P, &P->sv, n)) || (s = dalloc_t(P, &P->tv, n)))
+    return s;
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ensure_mhist(ffvgpu_pool* P, int n) {
+  if (n <= P->mhist_cap) return FFVGPU_OK;
+  if (P->mhist) {
+    for (const ffvgpu_instance& I : P->inst)
+      if (I.running) return bad("history length grows while solves run");
+    cudaFree(P->mhist);
+    P->bytes -= (int64_t)P->mhist_cap * num_inst(P) * 8;
+    P->mhist = nullptr;
+  }
+  P->mhist_cap = 0;
+  ffvgpu_status s = dalloc_t(P, &P->mhist, (size_t)n * num_inst(P));
+  if (s == FFVGPU_OK) P->mhist_cap = n;
+  return s;
+}
+
+MixCtx mix_ctx(const ffvgpu_pool* P) {
+  MixCtx C;
+  C.nbr = P->nbr_d;
+  C.dx = P->dx_d;
+  C.bc = P->bc_p;
+  C.inst.blk_inst = P->blk_inst_d;
+  C.inst.first = P->inst_first_d;
+  C.inst.count = P->inst_count_d;
+  C.inst.st = P->mst;
+  C.partials = P->mpartials;
+  C.capacity = P->nb;
+  C.first = 0;
+  return C;
+}
+
+KCtx range_ctx(const ffvgpu_pool* P, const BCSet& bc, const ffvgpu_instance& I) {
+  KCtx C = P->ctx(bc);
+  C.first = I.first;
+  C.nb = I.count;
+  return C;
+}
+
+ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
+  if (!prm) return bad("null parameters");
+  if (prm->sweeps < 1 || prm->sweeps_per_exchange < 1 ||
+      prm->sweeps % prm->sweeps_per_exchange != 0)
+    return bad("sweeps must be a positive multiple of sweeps_per_exchange");
+  if (prm->sweeps_per_exchange > 64) return bad("sweeps_per_exchange must be at most 64");
+  if (!(prm->omega > 0.0 && prm->omega < 2.0)) return bad("omega must lie in (0, 2)");
+  if (prm->count_max < 0) return bad("count_max must not be negative");
+  return FFVGPU_OK;
+}
+
+// Algorithmic HBM bytes of one iteration per cell: two preconditioner
+// applications, two A*x with dot products, the update.
+int64_t iteration_bytes_per_cell(int passes) {
+  const int64_t first_p = 28 + 8 + 16 + 8 + (passes > 1 ? 4 : 0) + 4;
+  const int64_t first_s = 28 + 16 + 8 + (passes > 1 ? 4 : 0) + 4;
+  const int64_t later = 28 + 4 + 4 + 4;
+  const int64_t matvec = 56 + 4 + 8 + 8;
+  const int64_t update = 4 + 4 + 8 + 8 + 8 + 8 + 8 + 8;
+  return first_p + first_s + 2 * (passes - 1) * later + 2 * matvec + update;
+}
+
+// One iteration of every running instance (all blocks of the pool).
+void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
+  const MixCtx C = mix_ctx(P);
+  const int nb = P->nb;
+  const int passes = P->m_sweeps / P->m_per_exchange;
+  const float om = (float)P->m_omega;
+  double* x = P->x[P->xcur];
+  for (int mode = 0; mode < 2; ++mode) {
+    double* rhs = mode == 0 ? P->p : P->sv;
+    float* hat = mode == 0 ? P->mph : P->msh;
+    for (int ps = 0; ps < passes; ++ps) {
+      const bool last = ps == passes - 1;
+      launch_mx_sweep(s, C, nb, mode, ps == 0, last, om, P->m_per_exchange, P->r, rhs, P->q,
+                      P->mcoef, P->mv32, ps > 0 ? P->me[(ps - 1) & 1] : nullptr,
+                      last ? hat : P->me[ps & 1]);
+    }
+    if (mode == 0)
+      launch_mx_matvec(s, C, nb, 1, P->mph, P->A, P->q, P->r0);
+    else
+      launch_mx_matvec(s, C, nb, 2, P->msh, P->A, P->tv, P->sv);
+  }
+  launch_mx_update(s, C, nb, x, P->mph, P->msh, P->r, P->tv, P->sv, P->r0);
+}
+
+int launches_per_iteration(const ffvgpu_pool* P) {
+  return 2 * (P->m_sweeps / P->m_per_exchange) + 3;
+}
+
+ffvgpu_status result_status(const ffvgpu_result& R, int status_code, double eps, int count_max) {
+  if (status_code == 2) {
+    g_last_error = "residual is NaN or Inf";
+    return FFVGPU_NAN_DETECTED;
+  }
+  if (eps > 0.0 && R.count > count_max) return FFVGPU_NOT_CONVERGED;
+  return FFVGPU_OK;
+}
+
+ffvgpu_status admit_range(ffvgpu_pool* P, const ffvgpu_grid_desc* d, int32_t* instance) {
+  if (!P->batch) return bad("instances are admitted into batch pools");
+  if (!d || !instance || !d->level || !d->block_index || d->num_blocks <= 0)
+    return bad("empty grid");
+  if (d->cells != 16) return bad("only 16^3 leaf blocks are supported");
+  if (d->root_length <= 0.0) return bad("root_length must be positive");
+  const int n = d->num_blocks;
+  for (int b = 0; b < n; ++b) {
+    if (d->level[b] < 0 || d->level[b] > 20) return bad("block level out of range");
+    for (int a = 0; a < 3; ++a) {
+      const long ext = (long)d->root_grid[a] << d->level[b];
+      if (d->block_index[3 * b + a] < 0 || d->block_index[3 * b + a] >= ext)
+        return bad("block index outside the root grid");
+    }
+  }
+  std::vector<FaceNbr> nbr;
+  ffvgpu_status s = derive_neighbors(n, d->level, d->block_index, d, nbr);
+  if (s != FFVGPU_OK) return s;
+  int slot = -1;
+  for (int i = 0; i < num_inst(P); ++i)
+    if (!P->inst[i].used) {
+      slot = i;
+      break;
+    }
+  if (slot < 0) {
+    g_last_error = "no free instance slot";
+    return FFVGPU_OOM;
+  }
+  int first = -1;
+  for (int b = 0, run = 0; b < P->nb; ++b) {
+    run = (P->blk_inst_h[b] < 0) ? run + 1 : 0;
+    if (run == n) {
+      first = b - n + 1;
+      break;
+    }
+  }
+  if (first < 0) {
+    g_last_error = "no free block range of " + std::to_string(n) + " blocks";
+    return FFVGPU_OOM;
+  }
+  if ((s = ensure_inst_device(P))) return s;
+  ffvgpu_instance& I = P->inst[slot];
+  I = ffvgpu_instance();
+  I.used = true;
+  I.first = first;
+  I.count = n;
+  I.level.assign(d->level, d->level + n);
+  I.index.assign(d->block_index, d->block_index + 3 * n);
+  I.desc = *d;
+  I.desc.level = I.level.data();
+  I.desc.block_index = I.index.data();
+  I.desc.neighbor_kind = nullptr;
+  I.desc.neighbor_ids = nullptr;
+  for (int b = 0; b < n; ++b) {
+    const int g = first + b;
+    P->blk_inst_h[g] = slot;
+    P->level[g] = d->level[b];
+    for (int a = 0; a < 3; ++a) P->index[3 * g + a] = d->block_index[3 * b + a];
+    P->dx_h[g] = d->root_length / (double)(1L << d->level[b]) / 16.0;
+    for (int f = 0; f < 6; ++f) {
+      FaceNbr F = nbr[(size_t)b * 6 + f];
+      for (int q = 0; q < 4; ++q)
+        if (F.id[q] >= 0) F.id[q] += first;
+      P->nbr_h[(size_t)g * 6 + f] = F;
+    }
+  }
+  // the instance's state stays idle (done) while its tables go live
+  SolveState idle;
+  std::memset(&idle, 0, sizeof(idle));
+  idle.done = 1;
+  CK(cudaMemcpy(P->mst + slot, &idle, sizeof(idle), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(P->nbr_d + (size_t)first * 6, P->nbr_h.data() + (size_t)first * 6,
+                sizeof(FaceNbr) * 6 * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(P->dx_d + first, P->dx_h.data() + first, sizeof(double) * n,
+                cudaMemcpyHostToDevice));
+  P->inst_dirty = true;
+  if ((s = ensure_inst_device(P))) return s;
+  *instance = slot;
+  return FFVGPU_OK;
+}
+
+ffvgpu_instance* get_inst(ffvgpu_pool* P, int32_t i) {
+  if (!P || i < 0 || i >= num_inst(P) || !P->inst[i].used) return nullptr;
+  return &P->inst[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+ffvgpu_status ffvgpu_batch_create(const ffvgpu_batch_desc* d, ffvgpu_pool** out) {
+  if (!d || !out) return bad("null argument");
+  *out = nullptr;
+  if (d->capacity_blocks <= 0) return bad("capacity_blocks must be positive");
+  if (d->max_instances <= 0 || d->max_instances > 65536)
+    return bad("max_instances must lie in [1, 65536]");
+  for (int f = 0; f < 6; ++f)
+    if (d->bc_type[f] != FFVGPU_BC_DIRICHLET && d->bc_type[f] != FFVGPU_BC_NEUMANN)
+      return bad("outer BC type must be Dirichlet or Neumann");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    g_last_error = "no CUDA device";
+    return FFVGPU_NO_DEVICE;
+  }
+  ffvgpu_pool* P = new ffvgpu_pool();
+  cudaGetDevice(&P->device);
+  P->batch = true;
+  P->nb = d->capacity_blocks;
+  P->level.assign(P->nb, 0);
+  P->index.assign((size_t)P->nb * 3, 0);
+  P->dx_h.assign(P->nb, 1.0);
+  FaceNbr outer;
+  std::memset(&outer, 0, sizeof(outer));
+  outer.kind = NB_OUTER;
+  for (int q = 0; q < 4; ++q) outer.id[q] = -1;
+  P->nbr_h.assign((size_t)P->nb * 6, outer);
+  for (int f = 0; f < 6; ++f) {
+    P->bc_p.type[f] = d->bc_type[f];
+    P->bc_p.value[f] = d->bc_value[f];
+    for (int c = 0; c < 3; ++c) {
+      P->bc_u[c].type[f] = FFVGPU_BC_NEUMANN;
+      P->bc_u[c].value[f] = 0.0;
+    }
+  }
+  P->inst.resize(d->max_instances);
+  P->blk_inst_h.assign(P->nb, -1);
+  ffvgpu_status s;
+  if ((s = pool_init_device(P)) || (s = ensure_inst_device(P))) {
+    ffvgpu_pool_destroy(P);
+    return s;
+  }
+  *out = P;
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_instance_admit(ffvgpu_pool* P, const ffvgpu_grid_desc* d,
+                                    int32_t* instance) {
+  if (!P) return bad("null pool");
+  cudaSetDevice(P->device);
+  return admit_range(P, d, instance);
+}
+
+ffvgpu_status ffvgpu_instance_admit_sphere(ffvgpu_pool* P, const ffvgpu_sphere_problem* prob,
+                                           int32_t* instance) {
+  if (!P || !prob || !instance) return bad("null argument");
+  if (!(prob->rhof > 0.0) || !(prob->dt > 0.0)) return bad("rhof and dt must be positive");
+  cudaSetDevice(P->device);
+  ffvgpu_sphere_grid* g = nullptr;
+  ffvgpu_status s = ffvgpu_sphere_grid_create(&prob->grid, &g);
+  if (s != FFVGPU_OK) return s == FFVGPU_BAD_ARG ? bad("bad sphere grid parameters") : s;
+  const int n = ffvgpu_sphere_grid_num_blocks(g);
+  std::vector<int32_t> lev(n), idx(3 * (size_t)n);
+  ffvgpu_sphere_grid_blocks(g, lev.data(), idx.data());
+  ffvgpu_sphere_grid_destroy(g);
+  ffvgpu_grid_desc d;
+  std::memset(&d, 0, sizeof(d));
+  d.num_blocks = n;
+  d.cells = 16;
+  d.level = lev.data();
+  d.block_index = idx.data();
+  for (int a = 0; a < 3; ++a) {
+    d.domain_origin[a] = prob->grid.domain_origin[a];
+    d.root_grid[a] = prob->grid.root_grid[a];
+  }
+  d.root_length = prob->grid.root_length;
+  int32_t slot = -1;
+  if ((s = admit_range(P, &d, &slot))) return s;
+  ffvgpu_instance& I = P->inst[slot];
+  // fields the generator and the assembly write (capacity-wide, allocated once)
+  double *ux, *uy, *uz, *c0, *xp, *dummy;
+  size_t stride;
+  if ((s = field_ptr(P, FFVGPU_FIELD_UX, true, &ux, &stride, &dummy)) ||
+      (s = field_ptr(P, FFVGPU_FIELD_UY, true, &uy, &stride, &dummy)) ||
+      (s = field_ptr(P, FFVGPU_FIELD_UZ, true, &uz, &stride, &dummy)) ||
+      (s = field_ptr(P, FFVGPU_FIELD_C0, true, &c0, &stride, &dummy)) ||
+      (s = field_ptr(P, FFVGPU_FIELD_X, true, &xp, &stride, &dummy)) ||
+      (s = dalloc_t(P, &P->flags, field_count(P))) ||
+      (s = dalloc_t(P, &P->A, 7 * field_count(P))) || (s = dalloc_t(P, &P->b, field_count(P)))) {
+    ffvgpu_instance_release(P, slot);
+    return s;
+  }
+  SphereGenParams G;
+  for (int a = 0; a < 3; ++a) {
+    G.domain_origin[a] = prob->grid.domain_origin[a];
+    G.center[a] = prob->grid.center[a];
+  }
+  G.root_length = prob->grid.root_length;
+  G.radius = prob->grid.radius;
+  G.seed = prob->seed;
+  G.sigma = prob->sigma;
+  launch_gen_sphere(P->stream, I.first, I.count, P->blk_geo_d, G, ux, uy, uz, c0, field_count(P),
+                    P->flags);
+  for (int c = 0; c < 3; ++c) {
+    BCSet bu;
+    for (int f = 0; f < 6; ++f) {
+      bu.type[f] = prob->u_bc_type[c][f];
+      bu.value[f] = prob->u_bc_value[c][f];
+    }
+    launch_exchange(P->stream, range_ctx(P, bu, I), P->u[c], P->gu[c]);
+  }
+  launch_assemble(P->stream, range_ctx(P, P->bc_p, I), P->u[0], P->u[1], P->u[2], P->gu[0],
+                  P->gu[1], P->gu[2], P->cut, P->flags, P->A, P->b, nullptr, prob->rhof,
+                  prob->dt, field_count(P));
+  launch_fold_bc(P->stream, range_ctx(P, P->bc_p, I), P->A, P->b);
+  launch_fill(P->stream, I.count, P->x[P->xcur] + (size_t)I.first * BC, BC,
+              P->gx + (size_t)I.first * 6 * FACE_CELLS, 0.0);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(P->stream));
+  *instance = slot;
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_instance_upload(ffvgpu_pool* P, int32_t inst, ffvgpu_field f,
+                                     const void* host, int32_t vc) {
+  ffvgpu_instance* I = get_inst(P, inst);
+  if (!I || !host) return bad("bad instance or null buffer");
+  if (I->running) return bad("instance is solving");
+  if (vc < 1 || vc > 4) return bad("vc must be in [1,4]");
+  cudaSetDevice(P->device);
+  const size_t w = 16 + 2 * (size_t)vc;
+  const size_t per = w * w * w;
+  ffvgpu_status s;
+  if (f >= FFVGPU_IFIELD_CID0 && f <= FFVGPU_IFIELD_PID) {
+    if ((s = dalloc_t(P, &P->flags, field_count(P)))) return s;
+    if ((s = ensure_stage(P, per * I->count * sizeof(int32_t)))) return s;
+    CK(cudaMemcpyAsync(P->stage, host, per * I->count * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       P->stream));
+    const int bit = (f == FFVGPU_IFIELD_PID) ? 7 : (f - FFVGPU_IFIELD_CID0);
+    launch_pack_flag(P->stream, I->count, (const int32_t*)P->stage, vc,
+                     P->flags + (size_t)I->first * BC, bit, f == FFVGPU_IFIELD_PID ? 1 : 0);
+  } else {
+    double *dst, *g;
+    size_t stride;
+    if ((s = field_ptr(P, f, true, &dst, &stride, &g))) return s;
+    if ((s = ensure_stage(P, per * I->count * sizeof(double)))) return s;
+    CK(cudaMemcpyAsync(P->stage, host, per * I->count * sizeof(double), cudaMemcpyHostToDevice,
+                       P->stream));
+    launch_pack(P->stream, I->count, (const double*)P->stage, vc, dst + (size_t)I->first * stride,
+                stride, g ? g + (size_t)I->first * 6 * FACE_CELLS : nullptr);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(P->stream));
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_instance_download(ffvgpu_pool* P, int32_t inst, ffvgpu_field f, void* host,
+                                       int32_t vc) {
+  ffvgpu_instance* I = get_inst(P, inst);
+  if (!I || !host) return bad("bad instance or null buffer");
+  if (vc < 1 || vc > 2) return bad("download supports vc = 1 or 2");
+  cudaSetDevice(P->device);
+  const size_t w = 16 + 2 * (size_t)vc;
+  const size_t per = w * w * w;
+  ffvgpu_status s;
+  if (f >= FFVGPU_IFIELD_CID0 && f <= FFVGPU_IFIELD_PID) {
+    if (!P->flags) return bad("integer fields have not been uploaded");
+    if ((s = ensure_stage(P, per * I->count * sizeof(int32_t)))) return s;
+    const int bit = (f == FFVGPU_IFIELD_PID) ? 7 : (f - FFVGPU_IFIELD_CID0);
+    launch_unpack_flag(P->stream, I->count, P->flags + (size_t)I->first * BC, vc,
+                       (int32_t*)P->stage, bit);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(host, P->stage, per * I->count * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       P->stream));
+    CK(cudaStreamSynchronize(P->stream));
+    return FFVGPU_OK;
+  }
+  double *src, *g;
+  size_t stride;
+  if ((s = field_ptr(P, f, false, &src, &stride, &g))) return s;
+  if ((s = ensure_stage(P, per * I->count * sizeof(double)))) return s;
+  const bool vec = (f == FFVGPU_FIELD_X) || (f >= FFVGPU_FIELD_UX && f <= FFVGPU_FIELD_UZ);
+  launch_unpack(P->stream, range_ctx(P, field_bc(P, f), *I), src, stride, vc, vec ? 1 : 0,
+                (double*)P->stage);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, P->stage, per * I->count * sizeof(double), cudaMemcpyDeviceToHost,
+                     P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_instance_release(ffvgpu_pool* P, int32_t inst) {
+  ffvgpu_instance* I = get_inst(P, inst);
+  if (!I) return bad("bad instance");
+  if (!P->batch) return bad("the instance of a one-grid pool is the pool");
+  if (I->running) return bad("instance is solving");
+  cudaSetDevice(P->device);
+  CK(cudaStreamSynchronize(P->stream));
+  for (int b = I->first; b < I->first + I->count; ++b) P->blk_inst_h[b] = -1;
+  CK(cudaMemcpy(P->blk_inst_d + I->first, P->blk_inst_h.data() + I->first,
+                sizeof(int32_t) * I->count, cudaMemcpyHostToDevice));
+  *I = ffvgpu_instance();
+  return FFVGPU_OK;
+}
+
+int32_t ffvgpu_instance_blocks(const ffvgpu_pool* P, int32_t inst) {
+  if (!P || inst < 0 || inst >= (int)P->inst.size() || !P->inst[inst].used) return 0;
+  return P->inst[inst].count;
+}
+
+ffvgpu_status ffvgpu_pool_free_blocks(const ffvgpu_pool* P, int32_t* free_blocks,
+                                      int32_t* largest_range) {
+  if (!P) return bad("null pool");
+  int32_t total = 0, best = 0, run = 0;
+  for (int b = 0; b < P->nb; ++b) {
+    if (P->blk_inst_h[b] < 0) {
+      ++total;
+      ++run;
+      if (run > best) best = run;
+    } else {
+      run = 0;
+    }
+  }
+  if (free_blocks) *free_blocks = total;
+  if (largest_range) *largest_range = best;
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixed_params* prm) {
+  ffvgpu_instance* I = get_inst(P, inst);
+  if (!I) return bad("bad instance");
+  if (I->running) return bad("instance is already solving");
+  ffvgpu_status s;
+  if ((s = check_mixed(prm))) return s;
+  if (!P->A || !P->b) return bad("A and b must be uploaded or assembled before a solve");
+  cudaSetDevice(P->device);
+  bool others = false;
+  for (const ffvgpu_instance& J : P->inst) others = others || J.running;
+  if (others && (prm->omega != P->m_omega || prm->sweeps != P->m_sweeps ||
+                 prm->sweeps_per_exchange != P->m_per_exchange))
+    return bad("running instances use other preconditioner settings");
+  double *xp, *g;
+  size_t stride;
+  if ((s = field_ptr(P, FFVGPU_FIELD_X, true, &xp, &stride, &g))) return s;
+  if ((s = ensure_inst_device(P)) || (s = ensure_mixed_buffers(P)) ||
+      (s = ensure_mhist(P, prm->count_max > 0 ? prm->count_max : 1)))
+    return s;
+  P->m_omega = prm->omega;
+  P->m_sweeps = prm->sweeps;
+  P->m_per_exchange = prm->sweeps_per_exchange;
+  I->count_max = prm->count_max;
+  I->epsilon = prm->epsilon;
+  I->result = ffvgpu_result();
+  SolveState& h = P->mst_h[inst];  // pinned staging of the state copy
+  std::memset(&h, 0, sizeof(h));
+  h.eps = prm->epsilon;
+  h.count_max = prm->count_max;
+  h.hist = P->mhist + (size_t)inst * P->mhist_cap;
+  h.done = 0;
+  if (prm->count_max <= 0) {  // for(count=1; count<=countMax; ...) runs no iteration
+    I->result.count = 1;
+    I->status = 0;
+    I->running = false;
+    return FFVGPU_OK;
+  }
+  // the instance's FP32 coefficients, its state, then b.b / r / r0 / r.r0
+  launch_mx_pack(P->stream, I->first, I->count, P->A, P->mcoef);
+  CK(cudaMemcpyAsync(P->mst + inst, &h, sizeof(h), cudaMemcpyHostToDevice, P->stream));
+  MixCtx C = mix_ctx(P);
+  C.first = I->first;
+  launch_mx_init(P->stream, C, I->count, P->x[P->xcur], P->gx, P->A, P->b, P->r, P->r0);
+  CK(cudaGetLastError());
+  P->m_launches += 2;
+  P->m_bytes += (int64_t)I->count * BC * (7 * 8 + 7 * 4 + 8 * 9 + 16);
+  I->running = true;
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
+  if (!P) return bad("null pool");
+  if (iterations <= 0) return FFVGPU_OK;
+  int running = 0;
+  int64_t cells = 0;
+  for (const ffvgpu_instance& I : P->inst)
+    if (I.running) {
+      ++running;
+      cells += (int64_t)I.count * BC;
+    }
+  if (!running) return FFVGPU_OK;
+  cudaSetDevice(P->device);
+  if (!P->mgraph || P->mgraph_iters != iterations || P->mgraph_omega != P->m_omega ||
+      P->mgraph_sweeps != P->m_sweeps || P->mgraph_per != P->m_per_exchange) {
+    if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
+    P->mgraph = nullptr;
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(P->own_stream, cudaStreamCaptureModeThreadLocal));
+    for (int it = 0; it < iterations; ++it) enqueue_iteration(P, P->own_stream);
+    CK(cudaStreamEndCapture(P->own_stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&P->mgraph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    P->mgraph_iters = iterations;
+    P->mgraph_omega = P->m_omega;
+    P->mgraph_sweeps = P->m_sweeps;
+    P->mgraph_per = P->m_per_exchange;
+  }
+  CK(cudaGraphLaunch(P->mgraph, P->stream));
+  P->m_launches += (int64_t)iterations * launches_per_iteration(P);
+  P->m_bytes += (int64_t)iterations * cells *
+                iteration_bytes_per_cell(P->m_sweeps / P->m_per_exchange);
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* P, int32_t* finished, int32_t capacity,
+                                int32_t* n_finished) {
+  if (!P) return bad("null pool");
+  if (n_finished) *n_finished = 0;
+  bool any = false;
+  for (const ffvgpu_instance& I : P->inst) any = any || I.running;
+  if (!any) return FFVGPU_OK;
+  cudaSetDevice(P->device);
+  const int ni = num_inst(P);
+  CK(cudaMemcpyAsync(P->mst_h, P->mst, sizeof(SolveState) * ni, cudaMemcpyDeviceToHost,
+                     P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  int nf = 0;
+  for (int i = 0; i < ni; ++i) {
+    ffvgpu_instance& I = P->inst[i];
+    if (!I.running || !P->mst_h[i].done) continue;
+    const SolveState& h = P->mst_h[i];
+    I.running = false;
+    I.result.count = h.count;
+    I.result.residual = h.residual;
+    I.status = h.status;
+    launch_exchange(P->stream, range_ctx(P, P->bc_p, I), P->x[P->xcur], P->gx);  // FFVILS.h:973
+    if (finished && nf < capacity) finished[nf] = i;
+    ++nf;
+  }
+  CK(cudaGetLastError());
+  if (nf) CK(cudaStreamSynchronize(P->stream));
+  if (n_finished) *n_finished = nf;
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* P, int32_t inst, ffvgpu_result* res,
+                                     double* history) {
+  if (!P || inst < 0 || inst >= (int)P->inst.size() || !P->inst[inst].used)
+    return bad("bad instance");
+  const ffvgpu_instance& I = P->inst[inst];
+  if (I.running) return bad("instance is solving");
+  if (res) *res = I.result;
+  if (history && I.count_max > 0 && P->mhist) {
+    const int c = I.result.count;
+    const int nh = (c >= 1 && c <= I.count_max) ? c : (c == 0 ? 0 : I.count_max);
+    if (nh > 0)
+      CK(cudaMemcpy(history, P->mhist + (size_t)inst * P->mhist_cap, sizeof(double) * nh,
+                    cudaMemcpyDeviceToHost));
+  }
+  return result_status(I.result, I.status, I.epsilon, I.count_max);
+}
+
+ffvgpu_status ffvgpu_solve_mixed(ffvgpu_pool* P, const ffvgpu_mixed_params* prm,
+                                 ffvgpu_result* res) {
+  if (!P) return bad("null pool");
+  ffvgpu_status s;
+  if ((s = check_mixed(prm))) return s;
+  cudaSetDevice(P->device);
+  for (const ffvgpu_instance& I : P->inst)
+    if (I.running) return bad("a stepped mixed solve is running on this pool");
+  const int64_t l0 = P->m_launches, b0 = P->m_bytes;
+  CK(cudaEventRecord(P->ev0, P->stream));
+  std::vector<int> mine;
+  for (int i = 0; i < num_inst(P); ++i) {
+    if (!P->inst[i].used) continue;
+    if ((s = ffvgpu_mixed_begin(P, i, prm))) return s;
+    mine.push_back(i);
+  }
+  CK(cudaEventRecord(P->ev2, P->stream));
+  const int every = prm->check_every > 0 ? prm->check_every : 8;
+  for (;;) {
+    int32_t nf = 0;
+    if ((s = ffvgpu_mixed_poll(P, nullptr, 0, &nf))) return s;
+    bool any = false;
+    for (int i : mine) any = any || P->inst[i].running;
+    if (!any) break;
+    if ((s = ffvgpu_mixed_advance(P, every))) return s;
+  }
+  CK(cudaEventRecord(P->ev1, P->stream));
+  CK(cudaEventSynchronize(P->ev1));
+  float ms = 0.f, sms = 0.f;
+  cudaEventElapsedTime(&ms, P->ev0, P->ev1);
+  cudaEventElapsedTime(&sms, P->ev2, P->ev1);
+  ffvgpu_status first_status = FFVGPU_OK;
+  bool first = true;
+  for (int i : mine) {
+    ffvgpu_instance& I = P->inst[i];
+    I.result.elapsed_ms = ms;
+    I.result.sweep_ms = sms;
+    I.result.sweep_launches = (int32_t)(P->m_launches - l0);
+    I.result.kernel_launches = (int32_t)(P->m_launches - l0);
+    I.result.bytes_moved = P->m_bytes - b0;
+    if (first) {
+      first = false;
+      first_status = ffvgpu_instance_result(P, i, res, prm->history);
+    }
+  }
+  return first_status;
+}
+
+}  // extern "C"

@@ -357,7 +357,7 @@ dot_kernel(const double* __restrict__ x, const double* __restrict__ y,
 // Writes layer-1 guide values of every face of every block into g.
 __global__ void __launch_bounds__(THREADS)
 exchange_kernel(KCtx C, const double* __restrict__ x, double* __restrict__ g) {
-  const int blk = blockIdx.x, tid = threadIdx.x;
+  const int blk = C.first + blockIdx.x, tid = threadIdx.x;
   const int a = tid & 15, b = tid >> 4;
   for (int f = 0; f < 6; ++f) {
     const FaceNbr nb = C.nbr[blk * 6 + f];
@@ -432,9 +432,9 @@ unpack_flag_kernel(const uint8_t* __restrict__ flags, int vc, int32_t* __restric
 __global__ void __launch_bounds__(THREADS)
 unpack_kernel(KCtx C, const double* __restrict__ src, size_t stride, int vc, int with_guides,
               double* __restrict__ stage) {
-  const int blk = blockIdx.x, tid = threadIdx.x;
+  const int blk = C.first + blockIdx.x, tid = threadIdx.x;
   const int w = 16 + 2 * vc;
-  double* sb = stage + (size_t)blk * w * w * w;
+  double* sb = stage + (size_t)blockIdx.x * w * w * w;
   for (int m = tid; m < w * w * w; m += THREADS) sb[m] = 0.0;
   __syncthreads();
   for (int m = 0; m < 16; ++m) {
@@ -480,7 +480,7 @@ assemble_kernel(KCtx C, const double* __restrict__ ux, const double* __restrict_
                 const uint8_t* __restrict__ flags, double* __restrict__ A,
                 double* __restrict__ bvec, double* __restrict__ vface /* [6][nb*4096] or null */,
                 double rhof, double dt, size_t field_stride) {
-  const int blk = blockIdx.x, tid = threadIdx.x;
+  const int blk = C.first + blockIdx.x, tid = threadIdx.x;
   const double dx = C.dx[blk];
   double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
   for (int m = 0; m < 16; ++m) {
@@ -537,7 +537,7 @@ assemble_kernel(KCtx C, const double* __restrict__ ux, const double* __restrict_
 // (BlockScalar3D.h:183-190) for every cell on an outer face.
 __global__ void __launch_bounds__(THREADS)
 fold_bc_kernel(KCtx C, double* __restrict__ A, double* __restrict__ bvec) {
-  const int blk = blockIdx.x, tid = threadIdx.x;
+  const int blk = C.first + blockIdx.x, tid = threadIdx.x;
   const double dx = C.dx[blk];
   int outer = 0;
   for (int f = 0; f < 6; ++f)

@@ -22,89 +22,13 @@
 #include "../../include/ffvgpu.h"
 #include "ffvgpu_kernels.h"
 #include "ffvgpu_layout.h"
+#include "pool_internal.h"
 
 using namespace ffvgpu;
+using namespace ffvgpu::detail;
 
-namespace {
-
-thread_local std::string g_last_error;
-
-ffvgpu_status cuda_fail(cudaError_t e, const char* what) {
-  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
-  return e == cudaErrorMemoryAllocation ? FFVGPU_OOM : FFVGPU_CUDA_ERROR;
-}
-
-#define CK(call)                                        \
-  do {                                                  \
-    cudaError_t e_ = (call);                            \
-    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
-  } while (0)
-
-ffvgpu_status bad(const char* why) {
-  g_last_error = why;
-  return FFVGPU_BAD_ARG;
-}
-
-constexpr size_t BC = BLOCK_CELLS;
-
-}  // namespace
-
-struct ffvgpu_pool {
-  int device = 0;
-  int nb = 0;
-  cudaStream_t stream = nullptr;      // where work is enqueued
-  cudaStream_t own_stream = nullptr;  // the pool's own stream
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
-  std::vector<int32_t> level, index;
-  std::vector<FaceNbr> nbr_h;
-  std::vector<double> dx_h;
-  FaceNbr* nbr_d = nullptr;
-  double* dx_d = nullptr;
-  BCSet bc_p;  // pressure BCs
-  BCSet bc_u[3];
-  int64_t bytes = 0;
-
-  // fields (device, colour-split interiors)
-  double* x[2] = {nullptr, nullptr};
-  int xcur = 0;
-  double* gx = nullptr;  // stored first guide layer of x
-  double* A = nullptr;   // [nb][7][4096]
-  double* coef = nullptr;         // sweep coefficient stream [nb][STREAM_BLOCK]
-  int64_t sys_version = 1;        // bumped whenever A or b change
-  int64_t stream_version = 0;     // sys_version the stream was packed from
-  double* b = nullptr;
-  double* u[3] = {nullptr, nullptr, nullptr};
-  double* gu[3] = {nullptr, nullptr, nullptr};
-  double* cut = nullptr;    // [6][nb*4096]
-  double* vface = nullptr;  // [6][nb*4096]
-  uint8_t* flags = nullptr; // bits 0..5 cut ids, bit 7 fluid
-  double* r = nullptr;
-  double* p = nullptr;
-  double* q = nullptr;
-  double* z[2] = {nullptr, nullptr};
-  double* r0 = nullptr;            // BiCGSTAB shadow residual
-  double* sv = nullptr;            // BiCGSTAB s
-  double* tv = nullptr;            // BiCGSTAB t_
-  double* zb[2] = {nullptr, nullptr};  // BiCGSTAB s_ (Jacobi iterates)
-  double* partials = nullptr;
-  SolveState* st = nullptr;
-  double* hist_d = nullptr;
-  int hist_cap = 0;
-  void* stage = nullptr;
-  size_t stage_bytes = 0;
-  int32_t* host_done = nullptr;  // pinned
-
-  KCtx ctx(const BCSet& bc) const {
-    KCtx C;
-    C.nbr = nbr_d;
-    C.dx = dx_d;
-    C.bc = bc;
-    C.nb = nb;
-    return C;
-  }
-};
-
-namespace {
+namespace ffvgpu {
+namespace detail {
 
 ffvgpu_status dalloc(ffvgpu_pool* P, void** ptr, size_t bytes) {
   if (*ptr) return FFVGPU_OK;
@@ -117,10 +41,6 @@ ffvgpu_status dalloc(ffvgpu_pool* P, void** ptr, size_t bytes) {
   return FFVGPU_OK;
 }
 
-template <class T>
-ffvgpu_status dalloc_t(ffvgpu_pool* P, T** ptr, size_t count) {
-  return dalloc(P, reinterpret_cast<void**>(ptr), count * sizeof(T));
-}
 
 ffvgpu_status ensure_stage(ffvgpu_pool* P, size_t bytes) {
   if (P->stage_bytes >= bytes) return FFVGPU_OK;
@@ -352,7 +272,28 @@ int64_t interior_bytes(const ffvgpu_pool* P, int words) {
   return (int64_t)P->nb * (int64_t)BC * 8 * words;
 }
 
-}  // namespace
+// Stream, events, neighbour table, cell sizes and the solver state of a
+// pool whose host tables are filled in.
+ffvgpu_status pool_init_device(ffvgpu_pool* P) {
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&P->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreate(&P->ev0)) != cudaSuccess ||
+      (e = cudaEventCreate(&P->ev1)) != cudaSuccess ||
+      (e = cudaEventCreate(&P->ev2)) != cudaSuccess ||
+      (e = cudaEventCreate(&P->ev3)) != cudaSuccess)
+    return cuda_fail(e, "stream/event create");
+  P->stream = P->own_stream;
+  ffvgpu_status s;
+  if ((s = dalloc_t(P, &P->nbr_d, P->nbr_h.size())) || (s = dalloc_t(P, &P->dx_d, P->dx_h.size())))
+    return s;
+  CK(cudaMemcpy(P->nbr_d, P->nbr_h.data(), P->nbr_h.size() * sizeof(FaceNbr),
+                cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(P->dx_d, P->dx_h.data(), P->dx_h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return ensure_solver(P);
+}
+
+}  // namespace detail
+}  // namespace ffvgpu
 
 void ffvgpu::set_last_error(const std::string& msg) { g_last_error = msg; }
 
@@ -412,23 +353,21 @@ ffvgpu_status ffvgpu_pool_create(const ffvgpu_grid_desc* d, ffvgpu_pool** out) {
     delete P;
     return s;
   }
-  cudaError_t e;
-  if ((e = cudaStreamCreateWithFlags(&P->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
-      (e = cudaEventCreate(&P->ev0)) != cudaSuccess ||
-      (e = cudaEventCreate(&P->ev1)) != cudaSuccess ||
-      (e = cudaEventCreate(&P->ev2)) != cudaSuccess ||
-      (e = cudaEventCreate(&P->ev3)) != cudaSuccess) {
-    ffvgpu_pool_destroy(P);
-    return cuda_fail(e, "stream/event create");
-  }
-  P->stream = P->own_stream;
-  if ((s = dalloc_t(P, &P->nbr_d, P->nbr_h.size())) || (s = dalloc_t(P, &P->dx_d, P->dx_h.size()))) {
-    ffvgpu_pool_destroy(P);
-    return s;
-  }
-  cudaMemcpy(P->nbr_d, P->nbr_h.data(), P->nbr_h.size() * sizeof(FaceNbr), cudaMemcpyHostToDevice);
-  cudaMemcpy(P->dx_d, P->dx_h.data(), P->dx_h.size() * sizeof(double), cudaMemcpyHostToDevice);
-  if ((s = ensure_solver(P)) != FFVGPU_OK) {
+  // the grid is instance 0 of its own pool
+  P->inst.resize(1);
+  ffvgpu_instance& I = P->inst[0];
+  I.used = true;
+  I.first = 0;
+  I.count = P->nb;
+  I.level = P->level;
+  I.index = P->index;
+  I.desc = *d;
+  I.desc.level = I.level.data();
+  I.desc.block_index = I.index.data();
+  I.desc.neighbor_kind = nullptr;
+  I.desc.neighbor_ids = nullptr;
+  P->blk_inst_h.assign(P->nb, 0);
+  if ((s = pool_init_device(P)) != FFVGPU_OK) {
     ffvgpu_pool_destroy(P);
     return s;
   }
@@ -441,6 +380,7 @@ void ffvgpu_pool_destroy(ffvgpu_pool* P) {
   cudaSetDevice(P->device);
   if (P->stream) cudaStreamSynchronize(P->stream);
   if (P->own_stream) cudaStreamSynchronize(P->own_stream);
+  release_instances(P);
   void* ptrs[] = {P->x[0], P->x[1], P->gx, P->A, P->coef, P->b, P->u[0], P->u[1], P->u[2],
                   P->gu[0], P->gu[1], P->gu[2], P->cut, P->vface, P->flags, P->r,
                   P->p, P->q, P->z[0], P->z[1], P->r0, P->sv, P->tv, P->zb[0], P->zb[1],
@@ -481,6 +421,7 @@ ffvgpu_status ffvgpu_grid_neighbors(const ffvgpu_grid_desc* d, int32_t* kind, in
 
 ffvgpu_status ffvgpu_fill(ffvgpu_pool* P, ffvgpu_field f, double value) {
   if (!P) return bad("null pool");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   cudaSetDevice(P->device);
   double *x, *g;
   size_t stride;
@@ -507,6 +448,7 @@ ffvgpu_status ffvgpu_pool_neighbors(const ffvgpu_pool* P, int32_t b, int32_t* ki
 
 ffvgpu_status ffvgpu_pool_upload(ffvgpu_pool* P, ffvgpu_field f, const void* host, int32_t vc) {
   if (!P || !host) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   if (vc < 1 || vc > 4) return bad("vc must be in [1,4]");
   cudaSetDevice(P->device);
   const size_t w = 16 + 2 * (size_t)vc;
@@ -540,6 +482,7 @@ ffvgpu_status ffvgpu_pool_upload(ffvgpu_pool* P, ffvgpu_field f, const void* hos
 
 ffvgpu_status ffvgpu_pool_download(ffvgpu_pool* P, ffvgpu_field f, void* host, int32_t vc) {
   if (!P || !host) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   if (vc < 1 || vc > 2) return bad("download supports vc = 1 or 2");
   cudaSetDevice(P->device);
   const size_t w = 16 + 2 * (size_t)vc;
@@ -574,6 +517,7 @@ ffvgpu_status ffvgpu_pool_download(ffvgpu_pool* P, ffvgpu_field f, void* host, i
 ffvgpu_status ffvgpu_exchange(ffvgpu_pool* P, ffvgpu_field f, const int32_t* bc_type6,
                               const double* bc_value6) {
   if (!P) return bad("null pool");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   cudaSetDevice(P->device);
   BCSet bc = P->bc_p;
   if (bc_type6 && bc_value6)
@@ -598,6 +542,7 @@ ffvgpu_status ffvgpu_exchange(ffvgpu_pool* P, ffvgpu_field f, const int32_t* bc_
 
 ffvgpu_status ffvgpu_assemble_p(ffvgpu_pool* P, double rhof, double dt) {
   if (!P) return bad("null pool");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   if (!(rhof > 0.0) || !(dt > 0.0)) return bad("rhof and dt must be positive");
   cudaSetDevice(P->device);
   for (int c = 0; c < 3; ++c)
@@ -618,6 +563,7 @@ ffvgpu_status ffvgpu_assemble_p(ffvgpu_pool* P, double rhof, double dt) {
 
 ffvgpu_status ffvgpu_fold_bc(ffvgpu_pool* P) {
   if (!P) return bad("null pool");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   if (!P->A || !P->b) return bad("A and b must exist before folding BCs");
   cudaSetDevice(P->device);
   launch_fold_bc(P->stream, P->ctx(P->bc_p), P->A, P->b);
@@ -629,6 +575,7 @@ ffvgpu_status ffvgpu_fold_bc(ffvgpu_pool* P) {
 
 ffvgpu_status ffvgpu_dot(ffvgpu_pool* P, ffvgpu_field fx, ffvgpu_field fy, double* xy) {
   if (!P || !xy) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   cudaSetDevice(P->device);
   double *x, *y, *g;
   size_t sx, sy;
@@ -647,6 +594,7 @@ ffvgpu_status ffvgpu_dot(ffvgpu_pool* P, ffvgpu_field fx, ffvgpu_field fy, doubl
 
 ffvgpu_status ffvgpu_calc_r2(ffvgpu_pool* P, double* rr) {
   if (!P || !rr) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   cudaSetDevice(P->device);
   ffvgpu_status s;
   if ((s = require_system(P))) return s;
@@ -664,6 +612,7 @@ ffvgpu_status ffvgpu_calc_r2(ffvgpu_pool* P, double* rr) {
 
 ffvgpu_status ffvgpu_rbgs_sweep(ffvgpu_pool* P, double omega) {
   if (!P) return bad("null pool");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   cudaSetDevice(P->device);
   ffvgpu_status s;
   if ((s = require_system(P))) return s;
@@ -685,6 +634,7 @@ ffvgpu_status ffvgpu_rbgs_sweep(ffvgpu_pool* P, double omega) {
 ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
                                 ffvgpu_result* res) {
   if (!P || !prm) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   cudaSetDevice(P->device);
   ffvgpu_status s;
   if ((s = require_system(P))) return s;
@@ -773,6 +723,7 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
 ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
                               ffvgpu_result* res) {
   if (!P || !prm) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   cudaSetDevice(P->device);
   ffvgpu_status s;
   if ((s = require_system(P))) return s;
@@ -901,6 +852,7 @@ static double* jacobi_pre(ffvgpu_pool* P, const KCtx& C, double* const zz[2], co
 ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
                                     ffvgpu_result* res) {
   if (!P || !prm) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
   cudaSetDevice(P->device);
   ffvgpu_status s;
   if ((s = require_system(P))) return s;

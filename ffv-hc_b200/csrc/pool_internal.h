@@ -1,0 +1,161 @@
+// pool_internal.h -- the device block pool shared by the host-side sources
+// of the library (pool.cpp: fields and the FFVILS-form solves; instances.cpp:
+// batches of independent problems and the mixed-precision form).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ffvgpu.h"
+#include "ffvgpu_kernels.h"
+#include "ffvgpu_layout.h"
+
+namespace ffvgpu {
+namespace detail {
+
+inline thread_local std::string g_last_error;
+
+inline ffvgpu_status cuda_fail(cudaError_t e, const char* what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? FFVGPU_OOM : FFVGPU_CUDA_ERROR;
+}
+
+inline ffvgpu_status bad(const char* why) {
+  g_last_error = why;
+  return FFVGPU_BAD_ARG;
+}
+
+constexpr size_t BC = BLOCK_CELLS;
+
+}  // namespace detail
+}  // namespace ffvgpu
+
+#define CK(call)                                                        \
+  do {                                                                  \
+    cudaError_t e_ = (call);                                            \
+    if (e_ != cudaSuccess) return ffvgpu::detail::cuda_fail(e_, #call); \
+  } while (0)
+
+// One admitted problem of a pool.
+struct ffvgpu_instance {
+  bool used = false;     // admitted
+  bool running = false;  // a mixed solve has begun and its end is not yet reported
+  int32_t first = 0, count = 0;
+  int32_t count_max = 0;
+  double epsilon = 0.0;
+  int32_t status = 0;  // of the last solve: 0 ok, 2 NaN/Inf residual
+  ffvgpu_result result{};
+  ffvgpu_grid_desc desc{};  // level / block_index point into the vectors below
+  std::vector<int32_t> level, index;
+};
+
+struct ffvgpu_pool {
+  int device = 0;
+  int nb = 0;  // blocks (a batch pool: its capacity)
+  cudaStream_t stream = nullptr;      // where work is enqueued
+  cudaStream_t own_stream = nullptr;  // the pool's own stream
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+  std::vector<int32_t> level, index;
+  std::vector<ffvgpu::FaceNbr> nbr_h;
+  std::vector<double> dx_h;
+  ffvgpu::FaceNbr* nbr_d = nullptr;
+  double* dx_d = nullptr;
+  ffvgpu::BCSet bc_p;  // pressure BCs
+  ffvgpu::BCSet bc_u[3];
+  int64_t bytes = 0;
+
+  // fields (device, colour-split interiors)
+  double* x[2] = {nullptr, nullptr};
+  int xcur = 0;
+  double* gx = nullptr;  // stored first guide layer of x
+  double* A = nullptr;   // [nb][7][4096]
+  double* coef = nullptr;         // sweep coefficient stream [nb][STREAM_BLOCK]
+  int64_t sys_version = 1;        // bumped whenever A or b change
+  int64_t stream_version = 0;     // sys_version the stream was packed from
+  double* b = nullptr;
+  double* u[3] = {nullptr, nullptr, nullptr};
+  double* gu[3] = {nullptr, nullptr, nullptr};
+  double* cut = nullptr;    // [6][nb*4096]
+  double* vface = nullptr;  // [6][nb*4096]
+  uint8_t* flags = nullptr; // bits 0..5 cut ids, bit 7 fluid
+  double* r = nullptr;
+  double* p = nullptr;
+  double* q = nullptr;
+  double* z[2] = {nullptr, nullptr};
+  double* r0 = nullptr;            // BiCGSTAB shadow residual
+  double* sv = nullptr;            // BiCGSTAB s
+  double* tv = nullptr;            // BiCGSTAB t_
+  double* zb[2] = {nullptr, nullptr};  // BiCGSTAB s_ (Jacobi iterates)
+  double* partials = nullptr;
+  ffvgpu::SolveState* st = nullptr;
+  double* hist_d = nullptr;
+  int hist_cap = 0;
+  void* stage = nullptr;
+  size_t stage_bytes = 0;
+  int32_t* host_done = nullptr;  // pinned
+
+  // instances: a pool made from one grid is instance 0 over every block; a
+  // batch pool admits and releases instances over its block capacity
+  bool batch = false;
+  std::vector<ffvgpu_instance> inst;
+  std::vector<int32_t> blk_inst_h;  // [nb], -1 for a free block
+  int32_t* blk_inst_d = nullptr;
+  int32_t* inst_first_d = nullptr;
+  int32_t* inst_count_d = nullptr;
+  int32_t* blk_geo_d = nullptr;      // [nb][4]: level, index x, y, z (device generator)
+  ffvgpu::SolveState* mst = nullptr;  // [instances]
+  ffvgpu::SolveState* mst_h = nullptr;  // pinned copy for polls
+  double* mpartials = nullptr;       // [2][nb]
+  double* mhist = nullptr;           // [instances][mhist_cap]
+  int mhist_cap = 0;
+  bool inst_dirty = true;            // host tables changed since the last upload
+
+  // mixed form
+  float* mcoef = nullptr;   // [nb][7][4096] FP32 sweep coefficients
+  float* me[2] = {nullptr, nullptr};
+  float* mv32 = nullptr;
+  float* mph = nullptr;     // preconditioned p (p_)
+  float* msh = nullptr;     // preconditioned s (s_)
+  int64_t mcoef_version = 0;  // sys_version the FP32 coefficients come from (one-grid pools)
+  double m_omega = 0.0;
+  int m_sweeps = 0, m_per_exchange = 0;
+  cudaGraphExec_t mgraph = nullptr;
+  int mgraph_iters = 0;
+  double mgraph_omega = 0.0;
+  int mgraph_sweeps = 0, mgraph_per = 0;
+  int64_t m_launches = 0;
+  int64_t m_bytes = 0;
+
+  ffvgpu::KCtx ctx(const ffvgpu::BCSet& bc) const {
+    ffvgpu::KCtx C;
+    C.nbr = nbr_d;
+    C.dx = dx_d;
+    C.bc = bc;
+    C.nb = nb;
+    C.first = 0;
+    return C;
+  }
+};
+
+namespace ffvgpu {
+namespace detail {
+
+ffvgpu_status dalloc(ffvgpu_pool* P, void** ptr, size_t bytes);
+template <class T>
+ffvgpu_status dalloc_t(ffvgpu_pool* P, T** ptr, size_t count) {
+  return dalloc(P, reinterpret_cast<void**>(ptr), count * sizeof(T));
+}
+ffvgpu_status ensure_stage(ffvgpu_pool* P, size_t bytes);
+size_t field_count(const ffvgpu_pool* P);
+ffvgpu_status field_ptr(ffvgpu_pool* P, int f, bool alloc, double** ptr, size_t* stride,
+                        double** guides);
+const BCSet& field_bc(const ffvgpu_pool* P, int f);
+ffvgpu_status derive_neighbors(int nb, const int32_t* level, const int32_t* index,
+                               const ffvgpu_grid_desc* d, std::vector<FaceNbr>& out);
+ffvgpu_status pool_init_device(ffvgpu_pool* P);
+void release_instances(ffvgpu_pool* P);
+
+}  // namespace detail
+}  // namespace ffvgpu

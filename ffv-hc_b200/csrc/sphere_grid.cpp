@@ -10,19 +10,10 @@
 // then refines further until every face neighbour differs by at most one
 // level (2:1 face balance).  Leaves are listed in depth-first Z order.
 //
-// Cut information per cell and direction f (0:-x 1:+x 2:-y 3:+y 4:-z 5:+z)
-// follows the meaning bcut_calc_ab_p gives it (src/FFV/bcut.f90:608-832):
-// cid_f != 0 when the segment from the cell centre to the neighbour centre
-// crosses the sphere, and c_f in (0,1] is the distance to the nearest
-// crossing in cell widths, rounded through float as Cutlib's CutPos32Array
-// stores it (src/FFV/Solver.cpp:618-637); uncut faces keep c_f = 1
-// (Solver::ClearCut, src/FFV/Solver.cpp:514-527).  A cell is fluid (pid 1)
-// when its centre lies outside the sphere.
-//
-// The intermediate velocity u* = (1,0,0) + N(0, sigma^2) draws one
-// Philox4x32-10 counter per (cell, component) (Salmon, Moraes, Dror, Shaw,
-// "Parallel random numbers: as easy as 1, 2, 3", SC'11) and a Box-Muller
-// transform, so any subset of cells can be regenerated independently.
+// Per-cell inputs (cut positions, fluid flags, u* = (1,0,0) + N(0, sigma^2))
+// come from sphere_gen.h, shared with the device generator; cell (i, j, k) of
+// the grid's block b draws from counter b*4096 + i + 16*(j + 16*k), so any
+// subset of cells can be regenerated independently.
 
 #include <cmath>
 #include <cstdint>
@@ -33,6 +24,7 @@
 #include <vector>
 
 #include "../../include/ffvgpu.h"
+#include "sphere_gen.h"
 
 struct ffvgpu_sphere_grid {
   ffvgpu_sphere_params prm;
@@ -134,31 +126,6 @@ struct Tree {
   }
 };
 
-inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
-  for (int r = 0; r < 10; ++r) {
-    const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
-    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
-    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
-    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
-    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-    c[0] = n0;
-    c[1] = lo1;
-    c[2] = n2;
-    c[3] = lo0;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
-  }
-}
-
-inline double normal_draw(uint64_t seed, uint64_t cell, uint32_t comp) {
-  uint32_t c[4] = {(uint32_t)cell, (uint32_t)(cell >> 32), comp, 0u};
-  philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-  const double two53 = 9007199254740992.0;
-  const double u1 = ((double)(c[0] >> 5) * 67108864.0 + (double)(c[1] >> 6) + 0.5) / two53;
-  const double u2 = ((double)(c[2] >> 5) * 67108864.0 + (double)(c[3] >> 6) + 0.5) / two53;
-  return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
-}
-
 }  // namespace
 
 extern "C" {
@@ -207,14 +174,11 @@ ffvgpu_status ffvgpu_sphere_grid_fill(const ffvgpu_sphere_grid* g, uint64_t seed
   const long w = n + 2 * vc;
   const long nc = w * w * w;
   const long nb = (long)g->level.size();
-  const double R = p.radius, R2 = R * R;
 #pragma omp parallel for schedule(dynamic, 4)
   for (long b = 0; b < nb; ++b) {
-    const int L = g->level[b];
-    const double bl = p.root_length / (double)(1L << L);
-    const double dx = bl / (double)n;
     double org[3];
-    for (int a = 0; a < 3; ++a) org[a] = p.domain_origin[a] + bl * (double)g->index[3 * b + a];
+    const double dx = ffvgpu::block_geometry(p.domain_origin, p.root_length, g->level[b],
+                                             &g->index[3 * b], org);
     const long base = b * nc;
     // guide cells are zero
     if (ux) std::memset(ux + base, 0, nc * sizeof(double));
@@ -231,34 +195,14 @@ ffvgpu_status ffvgpu_sphere_grid_fill(const ffvgpu_sphere_grid* g, uint64_t seed
         for (int i = 0; i < n; ++i) {
           const long m = base + (i + vc) + w * ((j + vc) + w * (k + vc));
           const uint64_t cell = (uint64_t)b * 4096u + (uint64_t)(i + 16 * (j + 16 * k));
-          if (ux) ux[m] = 1.0 + sigma * normal_draw(seed, cell, 0);
-          if (uy) uy[m] = sigma * normal_draw(seed, cell, 1);
-          if (uz) uz[m] = sigma * normal_draw(seed, cell, 2);
-          const double P[3] = {org[0] + ((double)i + 0.5) * dx,
-                               org[1] + ((double)j + 0.5) * dx,
-                               org[2] + ((double)k + 0.5) * dx};
-          double D[3], d2 = 0.0;
-          for (int a = 0; a < 3; ++a) {
-            D[a] = P[a] - p.center[a];
-            d2 += D[a] * D[a];
-          }
-          if (pid) pid[m] = (d2 >= R2) ? 1 : 0;
+          if (ux) ux[m] = 1.0 + sigma * ffvgpu::normal_draw(seed, cell, 0);
+          if (uy) uy[m] = sigma * ffvgpu::normal_draw(seed, cell, 1);
+          if (uz) uz[m] = sigma * ffvgpu::normal_draw(seed, cell, 2);
+          const ffvgpu::CellCut cc = ffvgpu::sphere_cell(org, dx, i, j, k, p.center, p.radius);
+          if (pid) pid[m] = cc.fluid;
           for (int f = 0; f < 6; ++f) {
-            const int a = f / 2;
-            const double s = (f & 1) ? 1.0 : -1.0;
-            const double bq = s * D[a];
-            const double disc = bq * bq - (d2 - R2);
-            if (disc < 0.0) continue;
-            const double sq = std::sqrt(disc);
-            const double t1 = -bq - sq, t2 = -bq + sq;
-            double t = -1.0;
-            if (t1 > 0.0 && t1 <= dx) t = t1;
-            else if (t2 > 0.0 && t2 <= dx) t = t2;
-            if (t <= 0.0) continue;
-            double d = (double)(float)(t / dx);
-            if (d <= 0.0) d = 1.0e-6;
-            if (d > 1.0) d = 1.0;
-            if (c6 && c6[f]) c6[f][m] = d;
+            if (!((cc.cid >> f) & 1)) continue;
+            if (c6 && c6[f]) c6[f][m] = cc.c[f];
             if (cid6 && cid6[f]) cid6[f][m] = 1;
           }
         }

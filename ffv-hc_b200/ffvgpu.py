@@ -35,6 +35,10 @@ EXPORTS = [
     "ffvgpu_dot", "ffvgpu_version", "ffvgpu_last_error", "ffvgpu_sphere_grid_create",
     "ffvgpu_sphere_grid_destroy", "ffvgpu_sphere_grid_num_blocks",
     "ffvgpu_sphere_grid_blocks", "ffvgpu_sphere_grid_fill", "ffvgpu_dot_noalloc",
+    "ffvgpu_solve_mixed", "ffvgpu_batch_create", "ffvgpu_instance_admit",
+    "ffvgpu_instance_admit_sphere", "ffvgpu_instance_upload", "ffvgpu_instance_download",
+    "ffvgpu_instance_release", "ffvgpu_instance_blocks", "ffvgpu_pool_free_blocks",
+    "ffvgpu_mixed_begin", "ffvgpu_mixed_advance", "ffvgpu_mixed_poll", "ffvgpu_instance_result",
 ]
 
 
@@ -72,6 +76,30 @@ class SphereParams(ctypes.Structure):
         ("root_length", ctypes.c_double), ("max_level", ctypes.c_int32),
         ("center", ctypes.c_double * 3), ("radius", ctypes.c_double),
         ("margin", ctypes.c_double),
+    ]
+
+
+class MixedParams(ctypes.Structure):
+    _fields_ = [
+        ("omega", ctypes.c_double), ("sweeps", ctypes.c_int32),
+        ("sweeps_per_exchange", ctypes.c_int32), ("count_max", ctypes.c_int32),
+        ("epsilon", ctypes.c_double), ("check_every", ctypes.c_int32),
+        ("history", ctypes.c_void_p),
+    ]
+
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [
+        ("capacity_blocks", ctypes.c_int32), ("max_instances", ctypes.c_int32),
+        ("bc_type", ctypes.c_int32 * 6), ("bc_value", ctypes.c_double * 6),
+    ]
+
+
+class SphereProblem(ctypes.Structure):
+    _fields_ = [
+        ("grid", SphereParams), ("seed", ctypes.c_uint64), ("sigma", ctypes.c_double),
+        ("rhof", ctypes.c_double), ("dt", ctypes.c_double),
+        ("u_bc_type", (ctypes.c_int32 * 6) * 3), ("u_bc_value", (ctypes.c_double * 6) * 3),
     ]
 
 
@@ -117,6 +145,20 @@ def lib():
         L.ffvgpu_sphere_grid_blocks.restype = None
         L.ffvgpu_sphere_grid_fill.argtypes = [vp, ctypes.c_uint64, dbl, i32, vp, vp, vp, vp, vp, vp]
         L.ffvgpu_dot_noalloc.argtypes = [vp, vp, i32, vp, vp]
+        MP, R = ctypes.POINTER(MixedParams), ctypes.POINTER(Result)
+        L.ffvgpu_solve_mixed.argtypes = [vp, MP, R]
+        L.ffvgpu_batch_create.argtypes = [ctypes.POINTER(BatchDesc), ctypes.POINTER(vp)]
+        L.ffvgpu_instance_admit.argtypes = [vp, ctypes.POINTER(GridDesc), vp]
+        L.ffvgpu_instance_admit_sphere.argtypes = [vp, ctypes.POINTER(SphereProblem), vp]
+        L.ffvgpu_instance_upload.argtypes = [vp, i32, i32, vp, i32]
+        L.ffvgpu_instance_download.argtypes = [vp, i32, i32, vp, i32]
+        L.ffvgpu_instance_release.argtypes = [vp, i32]
+        L.ffvgpu_instance_blocks.argtypes = [vp, i32]
+        L.ffvgpu_pool_free_blocks.argtypes = [vp, vp, vp]
+        L.ffvgpu_mixed_begin.argtypes = [vp, i32, MP]
+        L.ffvgpu_mixed_advance.argtypes = [vp, i32]
+        L.ffvgpu_mixed_poll.argtypes = [vp, vp, i32, vp]
+        L.ffvgpu_instance_result.argtypes = [vp, i32, R, vp]
         _lib = L
     return _lib
 
@@ -342,3 +384,142 @@ class Pool:
         v = ctypes.c_double()
         _check(lib().ffvgpu_dot(self._h, FIELD[fx], FIELD[fy], ctypes.byref(v)), "dot")
         return v.value
+
+    def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
+                    epsilon=1e-8, history=True, check_every=0):
+        """Mixed-precision solve (FP64 BiCGSTAB, FP32 RB-SOR preconditioner)."""
+        hist = np.zeros(max(count_max, 1), np.float64) if history else None
+        prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
+                          hist.ctypes.data if history else None)
+        res = Result()
+        st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
+        _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
+        out = dict(status=st, count=res.count, residual=res.residual, elapsed_ms=res.elapsed_ms,
+                   sweep_ms=res.sweep_ms, kernel_launches=res.kernel_launches,
+                   bytes_moved=res.bytes_moved)
+        if history:
+            n = res.count if 1 <= res.count <= count_max else (count_max if res.count > 0 else 0)
+            out["history"] = hist[:n].copy()
+        return out
+
+
+def sphere_problem(max_level, seed=1, sigma=0.01, dt=0.002, rhof=1.0, **grid_kw):
+    """ffvgpu_sphere_problem of the sphere-flow workload (grid keywords as SphereGrid)."""
+    p = dict(FLOW_PAST_SPHERE)
+    p.update(grid_kw)
+    sp = SphereParams(p["domain_origin"], p["root_grid"], p["root_length"], max_level,
+                      p["center"], p["radius"], p["margin"])
+    pr = SphereProblem()
+    pr.grid = sp
+    pr.seed = seed
+    pr.sigma = sigma
+    pr.rhof = rhof
+    pr.dt = dt
+    for c, u in enumerate(("UX", "UY", "UZ")):
+        for f in range(6):
+            pr.u_bc_type[c][f] = U_BC_TYPE[f]
+            pr.u_bc_value[c][f] = U_BC_VALUE[u][f]
+    return pr
+
+
+class Batch:
+    """A batch pool: independent pressure problems sharing one device pool."""
+
+    def __init__(self, capacity_blocks, max_instances=64, bc_type=P_BC_TYPE, bc_value=P_BC_VALUE):
+        d = BatchDesc(capacity_blocks, max_instances, tuple(bc_type), tuple(bc_value))
+        self._h = ctypes.c_void_p()
+        _check(lib().ffvgpu_batch_create(ctypes.byref(d), ctypes.byref(self._h)), "batch_create")
+        self.capacity = capacity_blocks
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None and self._h.value:
+            _lib.ffvgpu_pool_destroy(self._h)
+        self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def device_bytes(self):
+        return lib().ffvgpu_pool_device_bytes(self._h)
+
+    def admit_sphere(self, problem):
+        """Instance id, or None when no block range or slot is free (FFVGPU_OOM)."""
+        i = ctypes.c_int32()
+        st = lib().ffvgpu_instance_admit_sphere(self._h, ctypes.byref(problem), ctypes.byref(i))
+        if st == OOM:
+            return None
+        _check(st, "instance_admit_sphere")
+        return i.value
+
+    def admit(self, desc):
+        i = ctypes.c_int32()
+        st = lib().ffvgpu_instance_admit(self._h, ctypes.byref(desc), ctypes.byref(i))
+        if st == OOM:
+            return None
+        _check(st, "instance_admit")
+        return i.value
+
+    def blocks(self, inst):
+        return lib().ffvgpu_instance_blocks(self._h, inst)
+
+    def free_blocks(self):
+        t, r = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().ffvgpu_pool_free_blocks(self._h, ctypes.byref(t), ctypes.byref(r)),
+               "pool_free_blocks")
+        return t.value, r.value
+
+    def upload(self, inst, field, arr, vc=2):
+        fid = FIELD[field]
+        a = np.ascontiguousarray(arr, dtype=np.int32 if fid >= 100 else np.float64)
+        assert a.size == self.blocks(inst) * (16 + 2 * vc) ** 3
+        _check(lib().ffvgpu_instance_upload(self._h, inst, fid, _ptr(a), vc), f"upload {field}")
+
+    def download(self, inst, field, vc=2):
+        fid = FIELD[field]
+        w = 16 + 2 * vc
+        a = np.zeros((self.blocks(inst), w, w, w), np.int32 if fid >= 100 else np.float64)
+        _check(lib().ffvgpu_instance_download(self._h, inst, fid, _ptr(a), vc),
+               f"download {field}")
+        return a
+
+    def release(self, inst):
+        _check(lib().ffvgpu_instance_release(self._h, inst), "instance_release")
+
+    def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
+                    epsilon=1e-8, check_every=0):
+        """Solves every admitted instance; returns the first instance's result."""
+        prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
+                          None)
+        res = Result()
+        st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
+        _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
+        return dict(status=st, count=res.count, residual=res.residual, elapsed_ms=res.elapsed_ms,
+                    kernel_launches=res.kernel_launches, bytes_moved=res.bytes_moved)
+
+    def begin(self, inst, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
+              epsilon=1e-8):
+        prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, 0, None)
+        _check(lib().ffvgpu_mixed_begin(self._h, inst, ctypes.byref(prm)), "mixed_begin")
+
+    def advance(self, iterations):
+        _check(lib().ffvgpu_mixed_advance(self._h, iterations), "mixed_advance")
+
+    def poll(self, capacity=4096):
+        out = np.zeros(capacity, np.int32)
+        n = ctypes.c_int32()
+        _check(lib().ffvgpu_mixed_poll(self._h, _ptr(out), capacity, ctypes.byref(n)),
+               "mixed_poll")
+        return [int(v) for v in out[:n.value]]
+
+    def result(self, inst, count_max=None):
+        res = Result()
+        hist = np.zeros(max(count_max or 1, 1), np.float64)
+        st = lib().ffvgpu_instance_result(self._h, inst, ctypes.byref(res),
+                                          _ptr(hist) if count_max else None)
+        _check(st, "instance_result", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
+        out = dict(status=st, count=res.count, residual=res.residual)
+        if count_max:
+            n = res.count if 1 <= res.count <= count_max else (count_max if res.count > 0 else 0)
+            out["history"] = hist[:n].copy()
+        return out

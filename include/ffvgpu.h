@@ -259,6 +259,101 @@ ffvgpu_status ffvgpu_sphere_grid_fill(const ffvgpu_sphere_grid* g, uint64_t seed
                                       double* uy, double* uz, double* const* c6,
                                       int32_t* const* cid6, int32_t* pid);
 
+/* ---- mixed-precision form (no counterpart in the reference) -------------
+ * FFVILS::BiCGSTAB's recurrence (src/FFV/FFVILS.h:793-974) in FP64 --
+ * residuals, norms, dot products and the pressure update -- with the Jacobi
+ * preconditioner (FFVILS.h:469-492) replaced by FP32 red-black SOR sweeps
+ * from zero: 'sweeps' colour pairs per application, 'sweeps_per_exchange' of
+ * them between guide-cell exchanges (each block sweeps on chip against
+ * fixed guide values in between).  sweeps must be a multiple of
+ * sweeps_per_exchange.  Result fields as ffvgpu_solve_bicgstab; the solve
+ * stops when sqrt(r.r / b.b) <= epsilon or after count_max iterations. */
+typedef struct {
+  double omega;                /* FP32 SOR relaxation factor */
+  int32_t sweeps;              /* colour-pair sweeps per preconditioner application */
+  int32_t sweeps_per_exchange; /* sweeps between guide-cell exchanges */
+  int32_t count_max;
+  double epsilon;
+  int32_t check_every;         /* iterations between host polls (0: 8) */
+  double* history;             /* optional host array [count_max]: residual per iteration */
+} ffvgpu_mixed_params;
+
+/* Solves every admitted instance of the pool (a pool made from one grid is
+ * one instance); res receives instance 0's result when it is not NULL. */
+ffvgpu_status ffvgpu_solve_mixed(ffvgpu_pool* pool, const ffvgpu_mixed_params* prm,
+                                 ffvgpu_result* res);
+
+/* ---- batches: independent problems sharing one pool (no counterpart in the
+ * reference) ---------------------------------------------------------------
+ * A batch pool reserves capacity_blocks leaf blocks on the device and admits
+ * instances -- each a complete pressure problem on its own grid -- into
+ * free contiguous block ranges, up to max_instances at a time.  The
+ * instances share the pressure BCs of the batch.  The kernels of a batched
+ * solve run over all instances at once; every sum is taken per instance in
+ * the same order as for the instance alone, so each instance's results are
+ * bit-identical alone and in any mix.  The pool-wide entry points above
+ * (uploads, assembly, the FFVILS-form solves) refuse batch pools. */
+typedef struct {
+  int32_t capacity_blocks;
+  int32_t max_instances;
+  int32_t bc_type[6];  /* pressure BCs */
+  double bc_value[6];
+} ffvgpu_batch_desc;
+
+ffvgpu_status ffvgpu_batch_create(const ffvgpu_batch_desc* desc, ffvgpu_pool** out);
+
+/* Admits an instance on its own grid (desc's BC fields are ignored: the
+ * batch's apply).  A, b and x are then uploaded with ffvgpu_instance_upload.
+ * FFVGPU_OOM when no free block range or instance slot is large enough (the
+ * caller may retry after a release). */
+ffvgpu_status ffvgpu_instance_admit(ffvgpu_pool* pool, const ffvgpu_grid_desc* desc,
+                                   int32_t* instance);
+
+/* A sphere-flow pressure problem generated and assembled on the device: the
+ * grid of ffvgpu_sphere_grid_create, the inputs of ffvgpu_sphere_grid_fill
+ * (same seed, same values), then UpdateP's P02-P05 (velocity exchange with
+ * u_bc, bcut_calc_ab_p, BC folding) and x = 0. */
+typedef struct {
+  ffvgpu_sphere_params grid;
+  uint64_t seed;
+  double sigma;
+  double rhof;
+  double dt;
+  int32_t u_bc_type[3][6];
+  double u_bc_value[3][6];
+} ffvgpu_sphere_problem;
+
+ffvgpu_status ffvgpu_instance_admit_sphere(ffvgpu_pool* pool, const ffvgpu_sphere_problem* prob,
+                                           int32_t* instance);
+/* Per-instance transfers in the reference layout of ffvgpu_pool_upload /
+ * ffvgpu_pool_download (host buffers hold the instance's blocks only). */
+ffvgpu_status ffvgpu_instance_upload(ffvgpu_pool* pool, int32_t instance, ffvgpu_field field,
+                                     const void* host, int32_t vc);
+ffvgpu_status ffvgpu_instance_download(ffvgpu_pool* pool, int32_t instance, ffvgpu_field field,
+                                       void* host, int32_t vc);
+/* Frees the instance's blocks and slot; refused while its solve runs. */
+ffvgpu_status ffvgpu_instance_release(ffvgpu_pool* pool, int32_t instance);
+int32_t ffvgpu_instance_blocks(const ffvgpu_pool* pool, int32_t instance);
+/* Free blocks in total and in the largest free contiguous range. */
+ffvgpu_status ffvgpu_pool_free_blocks(const ffvgpu_pool* pool, int32_t* free_blocks,
+                                      int32_t* largest_range);
+
+/* Stepping form of the mixed solve, for request loops: begin starts an
+ * instance's solve (its count_max, epsilon and history come from prm; the
+ * preconditioner settings must equal those of instances already running);
+ * advance enqueues 'iterations' iterations of every running instance (one
+ * captured CUDA graph); poll returns the instances whose solves have ended
+ * since the last poll (their x guide layer is exchanged, as FFVILS.h:973
+ * does) and result reads one instance's outcome. */
+ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* pool, int32_t instance,
+                                 const ffvgpu_mixed_params* prm);
+ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* pool, int32_t iterations);
+ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* pool, int32_t* finished, int32_t capacity,
+                                int32_t* n_finished);
+/* history: optional host array receiving min(count, count_max) residuals. */
+ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* pool, int32_t instance,
+                                     ffvgpu_result* res, double* history);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1068,4 +1068,174 @@ int orc_bicgstab(Oracle* O, double omega, int countPre, int countMax,
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-precision form (no counterpart in the reference): orc_bicgstab's
+// recurrence (FFVILS.h:793-974) with Jacobi_PreConditioner replaced by FP32
+// red-black SOR sweeps from zero, 'per' sweeps between guide exchanges.
+// Restates ffv-hc_b200/csrc/kernels_mixed.cu:
+//   coefficients aw..at = (float)A*, dinv = (float)(1.0 / Ap); v = (float)rhs;
+//   per cell of colour c (colour 0 first, rbgs_smoother's order of terms):
+//     rc = fmaf(-aw, eW, v) ... fmaf(-at, eT, rc); xt = rc * dinv;
+//     e = fmaf(-omega, e - xt, e)
+//   guides of e: zero in the first group; later, the exchange of e (as
+//   double) with homogeneous Dirichlet outer faces, rounded to float.
+// The preconditioned vectors' guides come from the pressure-BC exchange
+// before CalcAx, and every dot product is DOT.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Coef32 {
+  std::vector<float> a[7];  // aw, ae, as, an, ab, at, dinv; reference layout
+};
+
+void mixed_coef(Oracle& O, Coef32& C) {
+  const long N = (long)O.G.nb * O.G.nc;
+  const int src[6] = {OF_AW, OF_AE, OF_AS, OF_AN, OF_AB, OF_AT};
+  for (int a = 0; a < 7; ++a) C.a[a].assign(N, 0.0f);
+  for (int bi = 0; bi < O.G.nb; ++bi)
+    for (long m = 0; m < O.G.nc; ++m) {
+      const long g = (long)bi * O.G.nc + m;
+      for (int a = 0; a < 6; ++a) C.a[a][g] = (float)O.F(src[a], bi)[m];
+      C.a[6][g] = (float)(1.0 / O.F(OF_AP, bi)[m]);
+    }
+}
+
+// out = M(v): FP32 sweeps, result widened to double (interior).
+void mixed_precondition(Oracle& O, const Coef32& C, int fv, int fout, float omega, int sweeps,
+                        int per) {
+  Grid& G = O.G;
+  const int n = G.n;
+  const long sy = n + 2 * G.g, sz = sy * sy;
+  const long N = (long)G.nb * G.nc;
+  std::vector<float> e(N, 0.0f), v(N, 0.0f);
+  for (int bi = 0; bi < G.nb; ++bi)
+    for (long m = 0; m < G.nc; ++m) v[(long)bi * G.nc + m] = (float)O.F(fv, bi)[m];
+  const int hom_t[6] = {BC_DIRICHLET, BC_DIRICHLET, BC_DIRICHLET,
+                        BC_DIRICHLET, BC_DIRICHLET, BC_DIRICHLET};
+  const double hom_v[6] = {0, 0, 0, 0, 0, 0};
+  for (int ps = 0; ps < sweeps / per; ++ps) {
+    if (ps > 0) {
+      // guide layer 1 of e through the exchange, in double
+      for (int bi = 0; bi < G.nb; ++bi) {
+        double* z = O.F(OF_Z, bi);
+        for (long m = 0; m < G.nc; ++m) z[m] = (double)e[(long)bi * G.nc + m];
+      }
+      impose_bc(O, OF_Z, hom_t, hom_v);
+      for (int bi = 0; bi < G.nb; ++bi) {
+        const double* z = O.F(OF_Z, bi);
+        float* eb = e.data() + (long)bi * G.nc;
+        for (int k = 0; k <= n + 1; ++k)
+          for (int j = 0; j <= n + 1; ++j)
+            for (int i = 0; i <= n + 1; ++i) {
+              const int out = (i == 0 || i == n + 1) + (j == 0 || j == n + 1) +
+                              (k == 0 || k == n + 1);
+              if (out != 1) continue;  // face guide cells of layer 1 only
+              const long m = IDX(G, i, j, k);
+              eb[m] = (float)z[m];
+            }
+      }
+    }
+    for (int it = 0; it < per; ++it)
+      for (int c = 0; c < 2; ++c) {
+#pragma omp parallel for num_threads(O.nthreads) schedule(static)
+        for (int bi = 0; bi < G.nb; ++bi) {
+          float* eb = e.data() + (long)bi * G.nc;
+          const float* vb = v.data() + (long)bi * G.nc;
+          const long o = (long)bi * G.nc;
+          for (int k = 1; k <= n; ++k)
+            for (int j = 1; j <= n; ++j)
+              for (int i = 1; i <= n; ++i) {
+                if ((((i - 1) + (j - 1) + (k - 1)) & 1) != c) continue;
+                const long m = IDX(G, i, j, k);
+                float rc = vb[m];
+                rc = std::fmaf(-C.a[0][o + m], eb[m - 1], rc);
+                rc = std::fmaf(-C.a[1][o + m], eb[m + 1], rc);
+                rc = std::fmaf(-C.a[2][o + m], eb[m - sy], rc);
+                rc = std::fmaf(-C.a[3][o + m], eb[m + sy], rc);
+                rc = std::fmaf(-C.a[4][o + m], eb[m - sz], rc);
+                rc = std::fmaf(-C.a[5][o + m], eb[m + sz], rc);
+                const float xt = rc * C.a[6][o + m];
+                const float ev = eb[m];
+                eb[m] = std::fmaf(-omega, ev - xt, ev);
+              }
+        }
+      }
+  }
+  for (int bi = 0; bi < G.nb; ++bi) {
+    double* out = O.F(fout, bi);
+    for (int k = 1; k <= n; ++k)
+      for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) {
+          const long m = IDX(G, i, j, k);
+          out[m] = (double)e[(long)bi * G.nc + m];
+        }
+  }
+}
+
+}  // namespace
+
+int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double epsilon,
+              int* count, double* residual, double* hist) {
+  Oracle& R = *O;
+  if (countMax <= 0) {
+    *count = 1;
+    *residual = 0.0;
+    return 0;
+  }
+  double bb = DOT(R, OF_B, OF_B);
+  if (std::fabs(bb) < FLT_MIN) {
+    *residual = 0.0;
+    *count = 0;
+    return 0;
+  }
+  Coef32 C;
+  mixed_coef(R, C);
+  const float om = (float)omega;
+  CalcR(R, OF_R, OF_X, OF_B);
+  COPY(R, OF_R0, OF_R);
+  double rr0 = 1.0, alpha = 0.0, gamma = 1.0;
+  int c;
+  for (c = 1; c <= countMax; ++c) {
+    double rr1 = DOT(R, OF_R, OF_R0);
+    if (std::fabs(rr1) < FLT_MIN) {
+      *residual = rr1;
+      c = 0;
+      break;
+    }
+    if (c == 1) {
+      COPY(R, OF_P, OF_R);
+    } else {
+      double beta = rr1 / rr0 * alpha / gamma;
+      AXPY(R, OF_P, OF_Q_, -gamma);
+      XPAY(R, OF_P, OF_R, beta);
+    }
+    mixed_precondition(R, C, OF_P, OF_P_, om, sweeps, per);
+    impose_bc_p(R, OF_P_);
+    CalcAx(R, OF_Q_, OF_P_);
+    double q_r0 = DOT(R, OF_Q_, OF_R0);
+    alpha = rr1 / q_r0;
+    AXPYZ(R, OF_S, OF_Q_, OF_R, -alpha);
+    mixed_precondition(R, C, OF_S, OF_S_, om, sweeps, per);
+    impose_bc_p(R, OF_S_);
+    CalcAx(R, OF_T_, OF_S_);
+    double t_s = DOT(R, OF_T_, OF_S);
+    double t_t_ = DOT(R, OF_T_, OF_T_);
+    gamma = t_s / t_t_;
+    AXPBYPZ(R, OF_X, OF_P_, OF_S_, alpha, gamma);
+    AXPYZ(R, OF_R, OF_T_, OF_S, -gamma);
+    double rr = DOT(R, OF_R, OF_R);
+    int st = is_converged(*residual, rr, bb, epsilon);
+    if (hist) hist[c - 1] = *residual;
+    if (st < 0) {
+      *count = c;
+      return 2;
+    }
+    if (st == 1) break;
+    rr0 = rr1;
+  }
+  impose_bc_p(R, OF_X);
+  *count = (c > countMax) ? countMax + 1 : c;
+  return 0;
+}
+
 }  // extern "C"

@@ -1,0 +1,201 @@
+"""Mixed-precision form, batches and the device generator, on the GPU.
+
+The mixed solve (FP64 BiCGSTAB recurrence, FP32 red-black SOR
+preconditioner) is checked bit for bit against the oracle's restatement
+(orc_mixed) for several sweep groupings; its converged pressure is compared
+with the FP64 solve of the same system (tolerance stated in the test).  A
+batch's instances are checked to give the same bits alone and in a mix,
+admitted together or while others run, and the device generator + assembly
+of an instance is checked against the host generator + oracle assembly.
+"""
+import numpy as np
+import pytest
+
+import ffvgpu
+from helpers import VC, assert_bitwise, device_problem, interior, problem
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("level,omega,sweeps,per,count", [
+    (1, 1.5, 8, 4, 12),
+    (1, 1.0, 4, 4, 10),
+    (2, 1.5, 8, 4, 8),
+    (2, 1.2, 6, 2, 6),
+    (1, 1.5, 3, 1, 6),
+])
+def test_mixed_solve_bitwise_against_oracle(level, omega, sweeps, per, count):
+    g, inp, O = problem(level)
+    P = device_problem(g, inp)
+    P.fill("X", 0.0)
+    O.field("X")[...] = 0.0
+    ro = O.solve_mixed(omega, sweeps, per, count, 0.0)
+    rg = P.solve_mixed(omega, sweeps, per, count, 0.0)
+    assert rg["count"] == ro["count"] == count + 1
+    assert_bitwise(rg["history"], ro["history"], "residual history")
+    assert_bitwise(interior(P.download("X", VC)), interior(O.field("X")), "pressure")
+    P.close()
+
+
+def test_mixed_converges_and_matches_fp64_solution():
+    g, inp, O = problem(2)
+    P = device_problem(g, inp)
+    P.fill("X", 0.0)
+    rm = P.solve_mixed(1.5, 8, 4, 500, 1e-8)
+    assert rm["status"] == ffvgpu.OK and rm["residual"] <= 1e-8, rm
+    pm = interior(P.download("X", VC)).copy()
+    # the oracle's converged mixed solve: same iteration count, same bits
+    O.field("X")[...] = 0.0
+    ro = O.solve_mixed(1.5, 8, 4, 500, 1e-8)
+    assert ro["count"] == rm["count"]
+    assert_bitwise(pm, interior(O.field("X")), "converged pressure")
+    # FP64 reference solution of the same system, far below the mixed tolerance
+    P.fill("X", 0.0)
+    rf = P.solve_bicgstab(1.0, 2, 3000, 1e-12)
+    assert rf["status"] == ffvgpu.OK
+    pf = interior(P.download("X", VC))
+    err = np.linalg.norm(pm - pf) / np.linalg.norm(pf)
+    # both solve A p = b; a 1e-8 relative residual bounds the relative error of
+    # p by the condition number times 1e-8 -- here it must stay below 1e-5
+    assert err < 1e-5, err
+    P.close()
+
+
+def test_mixed_edge_cases():
+    g, inp, O = problem(1)
+    P = device_problem(g, inp)
+    P.fill("X", 0.0)
+    r = P.solve_mixed(1.5, 8, 4, 0, 1e-8)          # countMax 0: no iteration
+    assert r["count"] == 1
+    with pytest.raises(ffvgpu.FFVGPUError):
+        P.solve_mixed(1.5, 6, 4, 10, 1e-8)          # sweeps not a multiple
+    with pytest.raises(ffvgpu.FFVGPUError):
+        P.solve_mixed(2.5, 8, 4, 10, 1e-8)          # omega outside (0, 2)
+    P.fill("B", 0.0)                                # b = 0: count 0, residual 0
+    r = P.solve_mixed(1.5, 8, 4, 10, 1e-8)
+    assert r["count"] == 0 and r["residual"] == 0.0
+    P.close()
+
+
+def sphere(level, seed, **kw):
+    return ffvgpu.sphere_problem(level, seed=seed, **kw)
+
+
+def test_device_generator_and_assembly_match_host_and_oracle():
+    B = ffvgpu.Batch(2000, 8)
+    kw = dict(center=(1.0, 0.5, -0.25), radius=0.4)
+    i = B.admit_sphere(sphere(2, 77, **kw))
+    g, inp, O = problem(2, seed=77, **kw)
+    assert B.blocks(i) == g.nb
+    for f in ("AP", "AW", "AE", "AS", "AN", "AB", "AT", "B"):
+        assert_bitwise(interior(B.download(i, f, VC)), interior(O.field(f)), f)
+    for u in ("UX", "UY", "UZ"):
+        assert_bitwise(interior(B.download(i, u, VC)), interior(inp[u]), u)
+    B.close()
+
+
+def solve_alone(level, seed, count, eps, kw):
+    B = ffvgpu.Batch(4000, 4)
+    i = B.admit_sphere(sphere(level, seed, **kw))
+    B.begin(i, count_max=count, epsilon=eps)
+    for _ in range(count):
+        B.advance(4)
+        if i in B.poll():
+            break
+    r = B.result(i, count_max=count)
+    x = interior(B.download(i, "X", VC)).copy()
+    B.close()
+    return r, x
+
+
+CASES = [(2, 5, dict()), (1, 9, dict(center=(2.0, 0.0, 0.0), radius=0.7)),
+         (2, 13, dict(center=(-1.0, 1.0, 0.5), radius=0.3))]
+
+
+def test_batch_instances_bitwise_alone_and_in_a_mix():
+    alone = [solve_alone(L, s, 40, 1e-8, kw) for (L, s, kw) in CASES]
+    B = ffvgpu.Batch(8000, 8)
+    ids = [B.admit_sphere(sphere(L, s, **kw)) for (L, s, kw) in CASES]
+    for i in ids:
+        B.begin(i, count_max=40, epsilon=1e-8)
+    left = set(ids)
+    for _ in range(100):
+        if not left:
+            break
+        B.advance(3)
+        left -= set(B.poll())
+    assert not left
+    for i, (ra, xa) in zip(ids, alone):
+        r = B.result(i, count_max=40)
+        assert r["count"] == ra["count"]
+        assert_bitwise(r["history"], ra["history"], "history in the mix")
+        assert_bitwise(interior(B.download(i, "X", VC)), xa, "pressure in the mix")
+    B.close()
+
+
+def test_batch_admission_while_others_run_and_release():
+    alone = [solve_alone(L, s, 40, 1e-8, kw) for (L, s, kw) in CASES]
+    B = ffvgpu.Batch(6000, 4)
+    name = {}  # instance slot -> case; a released slot is reused by the next admission
+    a = B.admit_sphere(sphere(*CASES[0][:2], **CASES[0][2]))
+    name[a] = 0
+    B.begin(a, count_max=40, epsilon=1e-8)
+    B.advance(5)
+    b = B.admit_sphere(sphere(*CASES[1][:2], **CASES[1][2]))   # joins mid-solve
+    name[b] = 1
+    B.begin(b, count_max=40, epsilon=1e-8)
+    done = {}
+    admitted_third = False
+    for _ in range(200):
+        if len(done) == 3:
+            break
+        B.advance(2)
+        for i in B.poll():
+            done[name.pop(i)] = (B.result(i, count_max=40),
+                                 interior(B.download(i, "X", VC)).copy())
+            B.release(i)
+            if not admitted_third:
+                admitted_third = True
+                c = B.admit_sphere(sphere(*CASES[2][:2], **CASES[2][2]))
+                name[c] = 2
+                B.begin(c, count_max=40, epsilon=1e-8)
+    assert len(done) == 3
+    for k, (ra, xa) in enumerate(alone):
+        r, x = done[k]
+        assert r["count"] == ra["count"]
+        assert_bitwise(r["history"], ra["history"], "history, staggered")
+        assert_bitwise(x, xa, "pressure, staggered")
+    assert B.free_blocks()[0] == 6000
+    B.close()
+
+
+def test_batch_instance_matches_one_grid_pool():
+    g, inp, O = problem(2, seed=21)
+    P = device_problem(g, inp)
+    P.fill("X", 0.0)
+    rp = P.solve_mixed(1.5, 8, 4, 30, 1e-8)
+    xp = interior(P.download("X", VC)).copy()
+    P.close()
+    B = ffvgpu.Batch(1000, 2)
+    i = B.admit_sphere(sphere(2, 21))
+    B.begin(i, count_max=30, epsilon=1e-8)
+    for _ in range(30):
+        if i in B.poll():
+            break
+        B.advance(4)
+    r = B.result(i, count_max=30)
+    assert r["count"] == rp["count"]
+    assert_bitwise(r["history"], rp["history"], "history")
+    assert_bitwise(interior(B.download(i, "X", VC)), xp, "pressure")
+    B.close()
+
+
+def test_batch_refuses_pool_wide_calls_and_full_capacity():
+    B = ffvgpu.Batch(190, 2)
+    i = B.admit_sphere(sphere(1, 3))                 # 72 blocks
+    assert B.admit_sphere(sphere(2, 4)) is None      # 128 blocks do not fit in the other 118
+    with pytest.raises(ffvgpu.FFVGPUError):
+        ffvgpu._check(ffvgpu.lib().ffvgpu_fold_bc(B._h), "fold_bc")
+    B.release(i)
+    assert B.admit_sphere(sphere(2, 4)) is not None
+    B.close()
