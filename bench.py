@@ -1,13 +1,13 @@
 #!/usr/bin/env python
-"""Benchmark: FP64 red-black SOR pressure solve on the level-3 sphere grid.
+"""Benchmark of the FP64 pressure-Poisson path on the sphere-flow grids.
 
-Workload (one "step"): FFVILS::RBGS on the FlowPastASphere-shaped grid of
-548 leaf blocks of 16^3 cells (2,244,608 cells; domain [-4,12]x[-4,4]x[-4,4],
-root grid 4x2x2, refined to level 3 within 0.5 of a unit-diameter sphere),
-A and b assembled from a seeded u* = (1,0,0) + N(0, 0.01^2) through the
-cut-cell assembly, omega = 1.5, 200 sweeps, a residual after every sweep,
-x reset to zero at the start of each step.  Metric: Gcell-sweeps/s =
-cells x sweeps / time.
+Default form (the headline line): FFVILS::RBGS on the level-5 FlowPastASphere
+grid -- 4692 leaf blocks of 16^3 cells (19,218,432 cells; domain
+[-4,12]x[-4,4]x[-4,4], root grid 4x2x2, refined to level 5 within 0.5 of a
+unit-diameter sphere) -- with A and b assembled from a seeded
+u* = (1,0,0) + N(0, 0.01^2) through the cut-cell assembly, omega = 1.5,
+200 sweeps, a residual after every sweep, x reset to zero at the start of
+each step.  Metric: Gcell-sweeps/s = cells x sweeps / time.
 
   value  device time (CUDA events on the pool's stream) of K steps with A, b
          resident in HBM;
@@ -18,6 +18,16 @@ cells x sweeps / time.
 --impl reference times the reference's CPU path on this machine's host
 cores: the C++ restatement in oracle/ (the reference itself cannot be built
 here), OpenMP over blocks, on a bounded sample of sweeps per step.
+
+Other forms (--form), each printing one JSON line of its own:
+  mixed  solves/s to a 1e-8 relative residual of the mixed-precision solve
+         (FP64 BiCGSTAB recurrence, FP32 RB-SOR preconditioner) against the
+         plain FP64 GPU solve (FFVILS::BiCGSTAB, Jacobi PreCount 2), with the
+         error of p and grad p against a converged FP64 solution;
+  batch  64 independent sphere instances (diameter U[0.5,2], centre in the
+         inner half of the domain, max level U{2..5}, seeds 0..63) solved to
+         1e-8 in one batch pool by the mixed solve under a captured CUDA
+         graph, against one-at-a-time plain FP64 GPU solves.
 """
 import argparse
 import json
@@ -42,7 +52,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ffvgpu", choices=["ffvgpu", "reference"])
-    ap.add_argument("--level", type=int, default=3)
+    ap.add_argument("--form", default="rbsor", choices=["rbsor", "mixed", "batch"])
+    ap.add_argument("--level", type=int, default=5)
+    ap.add_argument("--instances", type=int, default=64, help="batch form: instances")
+    ap.add_argument("--fp64-sample", type=int, default=64,
+                    help="batch form: instances solved one at a time in FP64 (a sample)")
     ap.add_argument("--sweeps", type=int, default=200)
     ap.add_argument("--omega", type=float, default=1.5)
     ap.add_argument("--seed", type=int, default=1)
@@ -61,18 +75,31 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the sweep kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "rbgs_sweep_level3_ncu.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.startswith("dram_bytes_per_launch_full_size:"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
-    return None
+def profile_traffic(level, cells):
+    """DRAM bytes per launch of the sweep kernel from the committed ncu summaries:
+    the capture of this level, else the level-3 capture scaled by cells (traffic
+    per cell is level-independent to first order), with its provenance."""
+    for lv in (level, 3):
+        path = os.path.join(ROOT, "profiles", f"rbgs_sweep_level{lv}_ncu.md")
+        if not os.path.exists(path):
+            continue
+        cap_cells = None
+        val = None
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                try:
+                    val = float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    val = None
+            if line.startswith("cells_per_launch:"):
+                cap_cells = float(line.split(":", 1)[1].split()[0])
+        if val is None:
+            continue
+        if lv == level:
+            return val, f"ncu, {os.path.basename(path)}"
+        if cap_cells:
+            return val * cells / cap_cells, f"ncu level-{lv} capture scaled by cells"
+    return None, None
 
 
 class ClockSampler:
@@ -139,18 +166,15 @@ def build_problem(level, seed):
     return g, inp
 
 
-def device_system(g, inp, stream):
-    """Pool with A, b assembled on the device (UpdateP P02-P05)."""
+def device_system(level, seed, stream):
+    """Pool with u*, cuts generated and A, b assembled on the device (UpdateP
+    P02-P05); the same values as the host generator + assembly."""
     import ffvgpu
+    g = ffvgpu.SphereGrid(level)
     P = ffvgpu.Pool(g.desc())
     P.set_stream(stream)
-    for k, v in inp.items():
-        P.upload(k, v, 2)
-    for u in ("UX", "UY", "UZ"):
-        P.exchange(u, ffvgpu.U_BC_TYPE, ffvgpu.U_BC_VALUE[u])
-    P.assemble_p(1.0, 0.002)
-    P.fold_bc()
-    return P
+    P.assemble_sphere(ffvgpu.sphere_problem(level, seed=seed, sigma=0.01))
+    return g, P
 
 
 def cpu_baseline(g, inp, sweeps_target, omega, budget_s):
@@ -250,6 +274,222 @@ def workload_config(g, args, extra=None):
     return c
 
 
+# ---------------------------------------------------------------------------
+# Other forms
+# ---------------------------------------------------------------------------
+MIXED = dict(omega=1.5, sweeps=8, sweeps_per_exchange=4)
+FP64_SOLVER = dict(omega=1.0, pre_count=2)  # FFV's pbicgstabP (sphere.tpp)
+
+
+def field_errors(pa, pb, level, root_length=4.0):
+    """Relative L2 and max errors of p and of its in-block face differences
+    (grad p, divided by each block's cell size) of interiors [nb][k][j][i]."""
+    dx = root_length / np.exp2(np.asarray(level, np.float64)) / 16.0
+    d = pa - pb
+    out = {"p_rel_l2": float(np.linalg.norm(d) / np.linalg.norm(pb)),
+           "p_max_rel": float(np.abs(d).max() / np.abs(pb).max())}
+    ga, gb = [], []
+    for ax in (1, 2, 3):
+        ga.append((np.diff(pa, axis=ax) / dx[:, None, None, None]).reshape(-1))
+        gb.append((np.diff(pb, axis=ax) / dx[:, None, None, None]).reshape(-1))
+    ga, gb = np.concatenate(ga), np.concatenate(gb)
+    out["gradp_rel_l2"] = float(np.linalg.norm(ga - gb) / np.linalg.norm(gb))
+    out["gradp_max_rel"] = float(np.abs(ga - gb).max() / np.abs(gb).max())
+    return out
+
+
+def timed(stream, fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    r = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return r, e0.elapsed_time(e1)
+
+
+def run_form(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    return run_mixed(args) if args.form == "mixed" else run_batch(args)
+
+
+def run_mixed(args):
+    import torch
+    import ffvgpu
+    stream = torch.cuda.current_stream()
+    g, P = device_system(args.level, args.seed, stream.cuda_stream)
+    peak, peak_kind = measured_peaks()
+
+    def fp64():
+        P.fill("X", 0.0)
+        return P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"], 50000, 1e-8,
+                                history=False)
+
+    def mixed():
+        P.fill("X", 0.0)
+        return P.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
+                             5000, 1e-8, history=False)
+
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        res = {}
+        for name, fn in (("fp64", fp64), ("mixed", mixed)):
+            for _ in range(max(1, args.warmup)):
+                fn()
+            ms, runs = [], []
+            for _ in range(args.steps):
+                r, t = timed(stream, fn)
+                ms.append(t)
+                runs.append(r)
+            res[name] = (runs[-1], float(np.mean(ms)), runs)
+    # errors against a converged FP64 solution of the same system
+    P.fill("X", 0.0)
+    rref = P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"], 50000, 1e-12,
+                            history=False)
+    pref = P.download("X", 2)[:, 2:18, 2:18, 2:18].copy()
+    mixed()
+    pm = P.download("X", 2)[:, 2:18, 2:18, 2:18].copy()
+    fp64()
+    pf = P.download("X", 2)[:, 2:18, 2:18, 2:18].copy()
+    P.close()
+    rf, tf, _ = res["fp64"]
+    rm, tm, _ = res["mixed"]
+    achieved = rm["bytes_moved"] / (tm * 1e-3) / 1e9
+    line = {
+        "form": "mixed", "metric": "solves/s to 1e-8 relative residual",
+        "value": 1e3 / tm, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tm, "higher_is_better": True,
+        "dtype": "f64 outer / f32 sweeps", "data": "synthetic",
+        "config": {"workload": f"mixed-vs-fp64-sphere-level{args.level}", "blocks": int(g.nb),
+                   "cells": int(g.cells), "epsilon": 1e-8, "mixed": MIXED,
+                   "fp64": dict(FP64_SOLVER, solver="BiCGSTAB (FFVILS.h:793-974)")},
+        "fp64": {"solves_per_s": 1e3 / tf, "ms": tf, "iterations": rf["count"],
+                 "residual": rf["residual"],
+                 "achieved_gbs": rf["bytes_moved"] / (tf * 1e-3) / 1e9},
+        "mixed": {"solves_per_s": 1e3 / tm, "ms": tm, "iterations": rm["count"],
+                  "residual": rm["residual"], "kernel_launches": rm["kernel_launches"]},
+        "speedup_vs_fp64": tf / tm,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "what": "algorithmic bytes of the whole mixed solve "
+                     "/ its device time", "peak_source": f"{peak_kind} hbm_gbs"},
+        "error_vs_fp64_converged": {"mixed": field_errors(pm, pref, g.level),
+                                    "fp64_at_1e-8": field_errors(pf, pref, g.level),
+                                    "reference_solution": f"FP64 BiCGSTAB to 1e-12 "
+                                                          f"({rref['count']} iterations)"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def batch_instances(n):
+    """Config-4 instances: diameter U[0.5,2], centre U([0,8]x[-2,2]x[-2,2]),
+    max level U{2..5}, seeds 0..n-1."""
+    out = []
+    for seed in range(n):
+        r = np.random.default_rng(seed)
+        d = r.uniform(0.5, 2.0)
+        c = r.uniform([0.0, -2.0, -2.0], [8.0, 2.0, 2.0])
+        L = int(r.integers(2, 6))
+        out.append((L, dict(center=tuple(float(v) for v in c), radius=d / 2.0), seed))
+    return out
+
+
+def run_batch(args):
+    import torch
+    import ffvgpu
+    stream = torch.cuda.current_stream()
+    insts = batch_instances(args.instances)
+    grids = [ffvgpu.SphereGrid(L, **kw) for (L, kw, _) in insts]
+    blocks = [gr.nb for gr in grids]
+    total = int(sum(blocks))
+    peak, peak_kind = measured_peaks()
+    B = ffvgpu.Batch(total, len(insts))
+    B.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    ids = [B.admit_sphere(ffvgpu.sphere_problem(L, seed=s, sigma=0.01, **kw))
+           for (L, kw, s) in insts]
+    torch.cuda.synchronize()
+    admit_s = time.perf_counter() - t0
+    assert all(i is not None for i in ids)
+
+    def batched():
+        for i in ids:
+            B.fill(i, "X", 0.0)
+        return B.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
+                             5000, 1e-8, check_every=8)
+
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for _ in range(max(1, args.warmup)):
+            batched()
+        ms, r = [], None
+        for _ in range(args.steps):
+            r, t = timed(stream, batched)
+            ms.append(t)
+    tb = float(np.mean(ms))
+    results = [B.result(i) for i in ids]
+    iters = [x["count"] for x in results]
+    worst = max(x["residual"] for x in results)
+    achieved = r["bytes_moved"] / (tb * 1e-3) / 1e9
+    dev_gb = B.device_bytes / 1e9
+    B.close()
+    # one-at-a-time plain FP64 GPU solves (and mixed, alone) of a sample
+    n_s = min(args.fp64_sample, len(insts))
+    sample = list(range(len(insts)))[:: max(1, len(insts) // n_s)][:n_s]
+    t64, tmix, it64 = 0.0, 0.0, []
+    for k in sample:
+        L, kw, s = insts[k]
+        P = ffvgpu.Pool(grids[k].desc())
+        P.set_stream(stream.cuda_stream)
+        P.assemble_sphere(ffvgpu.sphere_problem(L, seed=s, sigma=0.01, **kw))
+
+        def f64():
+            P.fill("X", 0.0)
+            return P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"], 50000, 1e-8,
+                                    history=False)
+
+        def mx():
+            P.fill("X", 0.0)
+            return P.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
+                                 5000, 1e-8, history=False)
+
+        f64()
+        rr, t = timed(stream, f64)
+        t64 += t
+        it64.append(rr["count"])
+        mx()
+        _, t = timed(stream, mx)
+        tmix += t
+        P.close()
+    fp64_sps = len(sample) / (t64 * 1e-3)
+    alone_sps = len(sample) / (tmix * 1e-3)
+    line = {
+        "form": "batch", "metric": "solves/s to 1e-8 relative residual", "value": 1e3 * len(ids) / tb,
+        "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tb, "higher_is_better": True, "dtype": "f64 outer / f32 sweeps",
+        "data": "synthetic",
+        "config": {"workload": f"batch-{len(ids)}-sphere-instances", "instances": len(ids),
+                   "blocks": total, "cells": total * CELLS_PER_BLOCK,
+                   "blocks_min_max": [int(min(blocks)), int(max(blocks))], "epsilon": 1e-8,
+                   "mixed": MIXED, "graph_iterations_per_replay": 8,
+                   "instances_rule": "diameter U[0.5,2], centre U([0,8]x[-2,2]x[-2,2]), "
+                                     "max level U{2..5}, seed = index"},
+        "iterations_min_max": [int(min(iters)), int(max(iters))], "worst_residual": worst,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "what": "algorithmic bytes of the batched solve / "
+                     "its device time", "peak_source": f"{peak_kind} hbm_gbs"},
+        "fp64_one_at_a_time": {"solves_per_s": fp64_sps, "sample": len(sample),
+                               "iterations_min_max": [int(min(it64)), int(max(it64))],
+                               "solver": "BiCGSTAB omega 1, PreCount 2"},
+        "mixed_one_at_a_time": {"solves_per_s": alone_sps, "sample": len(sample)},
+        "speedup_vs_fp64_one_at_a_time": (1e3 * len(ids) / tb) / fp64_sps,
+        "admission_s": admit_s, "device_gb": dev_gb, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -265,9 +505,12 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.form != "rbsor":
+        if world > 1:
+            raise SystemExit("--form mixed/batch run on one GPU")
+        return run_form(args)
     stream = torch.cuda.current_stream()
-    g, inp = build_problem(args.level, args.seed)
-    P = device_system(g, inp, stream.cuda_stream)
+    g, P = device_system(args.level, args.seed, stream.cuda_stream)
     cells = g.cells
 
     def barrier():
@@ -341,16 +584,17 @@ def main():
     alg_bytes = BYTES_PER_SWEEP_CELL * cells
     achieved = alg_bytes / (avg_launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profile_traffic()
+    traffic, traffic_src = profile_traffic(args.level, cells)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic,
-                "kernel": "rbgs_kernel<res,sweep> (fused residual + red-black sweep)",
+                "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
+                "kernel": "rbgs_pipelined_kernel<res,sweep> (fused residual + red-black sweep)",
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_launch_ms,
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(g, inp, args.sweeps, args.omega, args.cpu_seconds)
+        g2, inp = build_problem(args.level, args.seed)
+        cpu = cpu_baseline(g2, inp, args.sweeps, args.omega, args.cpu_seconds)
 
     if rank == 0:
         line = {

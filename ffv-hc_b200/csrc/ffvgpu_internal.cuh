@@ -248,6 +248,7 @@ __device__ __forceinline__ void finalize(SolveState* st, double total, int fin, 
       st->residual = res;
       if (st->hist) st->hist[iter - 1] = res;
       st->count = iter;
+      st->iter = iter;  // last iteration with a residual (history length on an early exit)
       if (res <= st->eps) {
         st->done = 1;
       } else if (isnan(res) || isinf(res)) {

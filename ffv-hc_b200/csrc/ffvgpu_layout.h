@@ -77,7 +77,9 @@ struct SolveState {
   int32_t timeout_where;  // roles whose bounded wait gave up (1 producer, 2 gatherer, 4 consumer)
   double* hist;      // device residual history [count_max] or null
   int32_t iter;      // mixed form: number of the iteration under way (1-based)
-  int32_t pad_;
+  int32_t cycle;     // mixed form: iteration within the current restart cycle (1: p = r)
+  double drop;       // mixed form: restart when the residual has dropped by this factor
+  double next_restart;  // mixed form: residual at which the next restart happens (< 0: none)
 };
 
 // Instances: independent problems that share one pool's blocks (a batch).

@@ -7,10 +7,14 @@
 
 namespace ffvgpu {
 
-// What every mixed-form kernel needs.  A launch covers the blocks
-// [first, first + count) of the pool; blocks of no instance, or of an
-// instance whose solve has stopped, return at entry.
+// What every mixed-form kernel needs.  The iteration kernels are persistent:
+// their CTAs walk the device list active[0, *n_active) of blocks of running
+// instances (a CUDA graph replays them while the list changes between
+// replays); the start-of-solve kernel covers blocks [first, first + count).
+// Blocks of an instance whose solve has stopped are skipped.
 struct MixCtx {
+  const int32_t* active;    // [capacity] block ids
+  const int32_t* n_active;  // device count of active entries
   const FaceNbr* nbr;  // [capacity][6]
   const double* dx;    // [capacity]
   BCSet bc;            // pressure BCs (outer guide cells of the FP64 stencils)
@@ -20,12 +24,16 @@ struct MixCtx {
   int first;
 };
 
+// CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel.
+void mx_grid_sizes(int* sweep, int* matvec, int* update);
 void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, float* coef);
 void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
                     const double* gx, const double* A, const double* b, double* r, double* r0);
+// The iteration launchers take 'count' = CTAs of the persistent grid.
 void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first, bool last,
-                     float omega, int nsweep, const double* r, double* pv, const double* q,
-                     const float* coef, float* v32, const float* ein, float* eout);
+                     float omega, int nsweep, const double* r, double* r0, double* pv,
+                     const double* q, const float* coef, float* v32, const float* ein,
+                     float* eout);
 void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, const float* x,
                       const double* A, double* y, const double* w0);
 void launch_mx_update(cudaStream_t s, const MixCtx& C, int count, double* x, const float* ph,

@@ -40,6 +40,11 @@ void release_instances(ffvgpu_pool* P) {
                   P->msh};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (P->act_d) cudaFree(P->act_d);
+  for (int k = 0; k < 2; ++k) {
+    if (P->act_h[k]) cudaFreeHost(P->act_h[k]);
+    if (P->act_ev[k]) cudaEventDestroy(P->act_ev[k]);
+  }
   if (P->mst_h) cudaFreeHost(P->mst_h);
   P->mst_h = nullptr;
 }
@@ -88,9 +93,38 @@ ffvgpu_status ensure_inst_device(ffvgpu_pool* P) {
   return FFVGPU_OK;
 }
 
+// Publishes the blocks of every running instance to the persistent kernels
+// (stream-ordered: work enqueued later sees the new list).  A staging buffer
+// is rewritten only after its previous copy has been consumed.
+ffvgpu_status publish_active(ffvgpu_pool* P) {
+  const int k = P->act_next;
+  P->act_next ^= 1;
+  CK(cudaEventSynchronize(P->act_ev[k]));
+  int32_t* h = P->act_h[k];
+  int n = 0;
+  for (const ffvgpu_instance& I : P->inst)
+    if (I.running)
+      for (int b = 0; b < I.count; ++b) h[1 + n++] = I.first + b;
+  h[0] = n;
+  CK(cudaMemcpyAsync(P->act_d, h, sizeof(int32_t) * (size_t)(n + 1), cudaMemcpyHostToDevice,
+                     P->stream));
+  CK(cudaEventRecord(P->act_ev[k], P->stream));
+  return FFVGPU_OK;
+}
+
 ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P) {
   ffvgpu_status s;
   const size_t n = field_count(P);
+  if (!P->act_d) {
+    if ((s = dalloc_t(P, &P->act_d, n / BC + 1))) return s;
+    CK(cudaMemset(P->act_d, 0, sizeof(int32_t)));
+    for (int k = 0; k < 2; ++k) {
+      CK(cudaMallocHost(&P->act_h[k], sizeof(int32_t) * (n / BC + 1)));
+      CK(cudaEventCreateWithFlags(&P->act_ev[k], cudaEventDisableTiming));
+      CK(cudaEventRecord(P->act_ev[k], P->stream));
+    }
+    mx_grid_sizes(&P->grid_sweep, &P->grid_matvec, &P->grid_update);
+  }
   if ((s = dalloc_t(P, &P->mcoef, 7 * n)) || (s = dalloc_t(P, &P->me[0], n)) ||
       (s = dalloc_t(P, &P->me[1], n)) || (s = dalloc_t(P, &P->mv32, n)) ||
       (s = dalloc_t(P, &P->mph, n)) || (s = dalloc_t(P, &P->msh, n)) ||
@@ -127,6 +161,8 @@ MixCtx mix_ctx(const ffvgpu_pool* P) {
   C.partials = P->mpartials;
   C.capacity = P->nb;
   C.first = 0;
+  C.n_active = P->act_d;
+  C.active = P->act_d + 1;
   return C;
 }
 
@@ -144,6 +180,8 @@ ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
     return bad("sweeps must be a positive multiple of sweeps_per_exchange");
   if (prm->sweeps_per_exchange > 64) return bad("sweeps_per_exchange must be at most 64");
   if (!(prm->omega > 0.0 && prm->omega < 2.0)) return bad("omega must lie in (0, 2)");
+  if (!(prm->restart_drop >= 0.0 && prm->restart_drop < 1.0))
+    return bad("restart_drop must lie in [0, 1)");
   if (prm->count_max < 0) return bad("count_max must not be negative");
   return FFVGPU_OK;
 }
@@ -162,7 +200,6 @@ int64_t iteration_bytes_per_cell(int passes) {
 // One iteration of every running instance (all blocks of the pool).
 void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
   const MixCtx C = mix_ctx(P);
-  const int nb = P->nb;
   const int passes = P->m_sweeps / P->m_per_exchange;
   const float om = (float)P->m_omega;
   double* x = P->x[P->xcur];
@@ -171,16 +208,18 @@ void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
     float* hat = mode == 0 ? P->mph : P->msh;
     for (int ps = 0; ps < passes; ++ps) {
       const bool last = ps == passes - 1;
-      launch_mx_sweep(s, C, nb, mode, ps == 0, last, om, P->m_per_exchange, P->r, rhs, P->q,
+      launch_mx_sweep(s, C, P->grid_sweep, mode, ps == 0, last, om, P->m_per_exchange, P->r,
+                      P->r0, rhs,
+                      P->q,
                       P->mcoef, P->mv32, ps > 0 ? P->me[(ps - 1) & 1] : nullptr,
                       last ? hat : P->me[ps & 1]);
     }
     if (mode == 0)
-      launch_mx_matvec(s, C, nb, 1, P->mph, P->A, P->q, P->r0);
+      launch_mx_matvec(s, C, P->grid_matvec, 1, P->mph, P->A, P->q, P->r0);
     else
-      launch_mx_matvec(s, C, nb, 2, P->msh, P->A, P->tv, P->sv);
+      launch_mx_matvec(s, C, P->grid_matvec, 2, P->msh, P->A, P->tv, P->sv);
   }
-  launch_mx_update(s, C, nb, x, P->mph, P->msh, P->r, P->tv, P->sv, P->r0);
+  launch_mx_update(s, C, P->grid_update, x, P->mph, P->msh, P->r, P->tv, P->sv, P->r0);
 }
 
 int launches_per_iteration(const ffvgpu_pool* P) {
@@ -277,6 +316,56 @@ ffvgpu_status admit_range(ffvgpu_pool* P, const ffvgpu_grid_desc* d, int32_t* in
   return FFVGPU_OK;
 }
 
+// UpdateP's P02-P05 for the blocks of instance I from device-generated
+// sphere-flow inputs: u*, cuts and flags (kernels_gen.cu), the velocity
+// exchange, bcut_calc_ab_p, the BC folding, and x = 0.
+ffvgpu_status generate_and_assemble(ffvgpu_pool* P, const ffvgpu_instance& I,
+                                    const ffvgpu_sphere_problem* prob) {
+  ffvgpu_status s;
+  if ((s = ensure_inst_device(P))) return s;
+  // fields the generator and the assembly write (pool-wide, allocated once)
+  double *ux, *uy, *uz, *c0, *xp, *dummy;
+  size_t stride;
+  if ((s = field_ptr(P, FFVGPU_FIELD_UX, true, &ux, &stride, &dummy)) ||
+      (s = field_ptr(P, FFVGPU_FIELD_UY, true, &uy, &stride, &dummy)) ||
+      (s = field_ptr(P, FFVGPU_FIELD_UZ, true, &uz, &stride, &dummy)) ||
+      (s = field_ptr(P, FFVGPU_FIELD_C0, true, &c0, &stride, &dummy)) ||
+      (s = field_ptr(P, FFVGPU_FIELD_X, true, &xp, &stride, &dummy)) ||
+      (s = dalloc_t(P, &P->flags, field_count(P))) ||
+      (s = dalloc_t(P, &P->A, 7 * field_count(P))) || (s = dalloc_t(P, &P->b, field_count(P))))
+    return s;
+  SphereGenParams G;
+  for (int a = 0; a < 3; ++a) {
+    G.domain_origin[a] = prob->grid.domain_origin[a];
+    G.center[a] = prob->grid.center[a];
+  }
+  G.root_length = prob->grid.root_length;
+  G.radius = prob->grid.radius;
+  G.seed = prob->seed;
+  G.sigma = prob->sigma;
+  launch_gen_sphere(P->stream, I.first, I.count, P->blk_geo_d, G, ux, uy, uz, c0, field_count(P),
+                    P->flags);
+  for (int c = 0; c < 3; ++c) {
+    BCSet bu;
+    for (int f = 0; f < 6; ++f) {
+      bu.type[f] = prob->u_bc_type[c][f];
+      bu.value[f] = prob->u_bc_value[c][f];
+    }
+    P->bc_u[c] = bu;
+    launch_exchange(P->stream, range_ctx(P, bu, I), P->u[c], P->gu[c]);
+  }
+  launch_assemble(P->stream, range_ctx(P, P->bc_p, I), P->u[0], P->u[1], P->u[2], P->gu[0],
+                  P->gu[1], P->gu[2], P->cut, P->flags, P->A, P->b, nullptr, prob->rhof,
+                  prob->dt, field_count(P));
+  launch_fold_bc(P->stream, range_ctx(P, P->bc_p, I), P->A, P->b);
+  launch_fill(P->stream, I.count, P->x[P->xcur] + (size_t)I.first * BC, BC,
+              P->gx + (size_t)I.first * 6 * FACE_CELLS, 0.0);
+  P->sys_version++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(P->stream));
+  return FFVGPU_OK;
+}
+
 ffvgpu_instance* get_inst(ffvgpu_pool* P, int32_t i) {
   if (!P || i < 0 || i >= num_inst(P) || !P->inst[i].used) return nullptr;
   return &P->inst[i];
@@ -363,49 +452,33 @@ ffvgpu_status ffvgpu_instance_admit_sphere(ffvgpu_pool* P, const ffvgpu_sphere_p
   d.root_length = prob->grid.root_length;
   int32_t slot = -1;
   if ((s = admit_range(P, &d, &slot))) return s;
-  ffvgpu_instance& I = P->inst[slot];
-  // fields the generator and the assembly write (capacity-wide, allocated once)
-  double *ux, *uy, *uz, *c0, *xp, *dummy;
-  size_t stride;
-  if ((s = field_ptr(P, FFVGPU_FIELD_UX, true, &ux, &stride, &dummy)) ||
-      (s = field_ptr(P, FFVGPU_FIELD_UY, true, &uy, &stride, &dummy)) ||
-      (s = field_ptr(P, FFVGPU_FIELD_UZ, true, &uz, &stride, &dummy)) ||
-      (s = field_ptr(P, FFVGPU_FIELD_C0, true, &c0, &stride, &dummy)) ||
-      (s = field_ptr(P, FFVGPU_FIELD_X, true, &xp, &stride, &dummy)) ||
-      (s = dalloc_t(P, &P->flags, field_count(P))) ||
-      (s = dalloc_t(P, &P->A, 7 * field_count(P))) || (s = dalloc_t(P, &P->b, field_count(P)))) {
+  if ((s = generate_and_assemble(P, P->inst[slot], prob))) {
     ffvgpu_instance_release(P, slot);
     return s;
   }
-  SphereGenParams G;
-  for (int a = 0; a < 3; ++a) {
-    G.domain_origin[a] = prob->grid.domain_origin[a];
-    G.center[a] = prob->grid.center[a];
-  }
-  G.root_length = prob->grid.root_length;
-  G.radius = prob->grid.radius;
-  G.seed = prob->seed;
-  G.sigma = prob->sigma;
-  launch_gen_sphere(P->stream, I.first, I.count, P->blk_geo_d, G, ux, uy, uz, c0, field_count(P),
-                    P->flags);
-  for (int c = 0; c < 3; ++c) {
-    BCSet bu;
-    for (int f = 0; f < 6; ++f) {
-      bu.type[f] = prob->u_bc_type[c][f];
-      bu.value[f] = prob->u_bc_value[c][f];
-    }
-    launch_exchange(P->stream, range_ctx(P, bu, I), P->u[c], P->gu[c]);
-  }
-  launch_assemble(P->stream, range_ctx(P, P->bc_p, I), P->u[0], P->u[1], P->u[2], P->gu[0],
-                  P->gu[1], P->gu[2], P->cut, P->flags, P->A, P->b, nullptr, prob->rhof,
-                  prob->dt, field_count(P));
-  launch_fold_bc(P->stream, range_ctx(P, P->bc_p, I), P->A, P->b);
-  launch_fill(P->stream, I.count, P->x[P->xcur] + (size_t)I.first * BC, BC,
-              P->gx + (size_t)I.first * 6 * FACE_CELLS, 0.0);
-  CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(P->stream));
   *instance = slot;
   return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_assemble_sphere(ffvgpu_pool* P, const ffvgpu_sphere_problem* prob) {
+  if (!P || !prob) return bad("null argument");
+  if (P->batch) return bad("a batch pool admits sphere problems with ffvgpu_instance_admit_sphere");
+  if (!(prob->rhof > 0.0) || !(prob->dt > 0.0)) return bad("rhof and dt must be positive");
+  cudaSetDevice(P->device);
+  // the pool's grid must be the problem's grid
+  ffvgpu_sphere_grid* g = nullptr;
+  ffvgpu_status s = ffvgpu_sphere_grid_create(&prob->grid, &g);
+  if (s != FFVGPU_OK) return bad("bad sphere grid parameters");
+  const int n = ffvgpu_sphere_grid_num_blocks(g);
+  std::vector<int32_t> lev(n), idx(3 * (size_t)n);
+  ffvgpu_sphere_grid_blocks(g, lev.data(), idx.data());
+  ffvgpu_sphere_grid_destroy(g);
+  if (n != P->nb || lev != P->level || idx != P->index)
+    return bad("the pool was not created from this sphere problem's grid");
+  for (int a = 0; a < 3; ++a)
+    if (P->inst[0].desc.domain_origin[a] != prob->grid.domain_origin[a])
+      return bad("the pool's domain origin differs from the problem's");
+  return generate_and_assemble(P, P->inst[0], prob);
 }
 
 ffvgpu_status ffvgpu_instance_upload(ffvgpu_pool* P, int32_t inst, ffvgpu_field f,
@@ -476,6 +549,23 @@ ffvgpu_status ffvgpu_instance_download(ffvgpu_pool* P, int32_t inst, ffvgpu_fiel
   return FFVGPU_OK;
 }
 
+ffvgpu_status ffvgpu_instance_fill(ffvgpu_pool* P, int32_t inst, ffvgpu_field f, double value) {
+  ffvgpu_instance* I = get_inst(P, inst);
+  if (!I) return bad("bad instance");
+  if (I->running) return bad("instance is solving");
+  cudaSetDevice(P->device);
+  double *x, *g;
+  size_t stride;
+  ffvgpu_status s;
+  if ((s = field_ptr(P, f, true, &x, &stride, &g))) return s;
+  launch_fill(P->stream, I->count, x + (size_t)I->first * stride, stride,
+              g ? g + (size_t)I->first * 6 * FACE_CELLS : nullptr, value);
+  if ((f >= FFVGPU_FIELD_AP && f <= FFVGPU_FIELD_AT) || f == FFVGPU_FIELD_B) P->sys_version++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(P->stream));
+  return FFVGPU_OK;
+}
+
 ffvgpu_status ffvgpu_instance_release(ffvgpu_pool* P, int32_t inst) {
   ffvgpu_instance* I = get_inst(P, inst);
   if (!I) return bad("bad instance");
@@ -542,6 +632,7 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
   std::memset(&h, 0, sizeof(h));
   h.eps = prm->epsilon;
   h.count_max = prm->count_max;
+  h.drop = prm->restart_drop;
   h.hist = P->mhist + (size_t)inst * P->mhist_cap;
   h.done = 0;
   if (prm->count_max <= 0) {  // for(count=1; count<=countMax; ...) runs no iteration
@@ -560,7 +651,7 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
   P->m_launches += 2;
   P->m_bytes += (int64_t)I->count * BC * (7 * 8 + 7 * 4 + 8 * 9 + 16);
   I->running = true;
-  return FFVGPU_OK;
+  return publish_active(P);
 }
 
 ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
@@ -619,12 +710,17 @@ ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* P, int32_t* finished, int32_t capac
     I.result.count = h.count;
     I.result.residual = h.residual;
     I.status = h.status;
+    I.last_iter = (h.count == 0) ? h.iter : 0;  // 0 when the exit came before iteration 1
     launch_exchange(P->stream, range_ctx(P, P->bc_p, I), P->x[P->xcur], P->gx);  // FFVILS.h:973
     if (finished && nf < capacity) finished[nf] = i;
     ++nf;
   }
   CK(cudaGetLastError());
-  if (nf) CK(cudaStreamSynchronize(P->stream));
+  if (nf) {
+    ffvgpu_status s = publish_active(P);
+    if (s != FFVGPU_OK) return s;
+    CK(cudaStreamSynchronize(P->stream));
+  }
   if (n_finished) *n_finished = nf;
   return FFVGPU_OK;
 }
@@ -638,7 +734,8 @@ ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* P, int32_t inst, ffvgpu_
   if (res) *res = I.result;
   if (history && I.count_max > 0 && P->mhist) {
     const int c = I.result.count;
-    const int nh = (c >= 1 && c <= I.count_max) ? c : (c == 0 ? 0 : I.count_max);
+    // an early exit (count 0) keeps the residuals of the iterations before it
+    const int nh = (c >= 1 && c <= I.count_max) ? c : (c == 0 ? I.last_iter : I.count_max);
     if (nh > 0)
       CK(cudaMemcpy(history, P->mhist + (size_t)inst * P->mhist_cap, sizeof(double) * nh,
                     cudaMemcpyDeviceToHost));

@@ -25,6 +25,7 @@
 //
 // Every sum is the canonical tree of the layout header taken over one
 // instance's blocks, so an instance gets the same bits alone or in a batch.
+#include <algorithm>
 #include <cfloat>
 #include <cuda_runtime.h>
 
@@ -68,6 +69,8 @@ __device__ void mx_finalize(SolveState* S, const double* t, int fin) {
       S->alpha = 0.0;
       S->gamma = 1.0;
       S->iter = 1;
+      S->cycle = 1;
+      S->next_restart = (S->drop > 0.0) ? resid_of(t[1], t[0]) * S->drop : -1.0;
       break;
     case FIN_MX_ALPHA:
       S->qp = t[0];
@@ -94,13 +97,25 @@ __device__ void mx_finalize(SolveState* S, const double* t, int fin) {
         S->count = S->count_max + 1;
       } else {
         S->rr0 = S->rr1;  // FFVILS.h:960
-        S->rr1 = t[1];    // next iteration's DOT(r, r0)
-        if (fabs(t[1]) < (double)FLT_MIN) {
-          S->residual = t[1];
+        S->cycle += 1;
+        double rr1 = t[1];  // next iteration's DOT(r, r0)
+        if (S->next_restart > 0.0 && res <= S->next_restart) {
+          // restart from the current r: r0 = r (written by the next
+          // iteration's first sweep pass), so DOT(r, r0) = r.r
+          S->next_restart = res * S->drop;
+          S->rr0 = 1.0;
+          S->alpha = 0.0;
+          S->gamma = 1.0;
+          S->cycle = 1;
+          rr1 = t[0];
+        }
+        S->rr1 = rr1;
+        if (fabs(rr1) < (double)FLT_MIN) {
+          S->residual = rr1;
           S->count = 0;
           S->done = 1;
         } else {
-          S->beta = t[1] / S->rr0 * S->alpha / S->gamma;
+          S->beta = rr1 / S->rr0 * S->alpha / S->gamma;
           S->iter = n + 1;
         }
       }
@@ -257,7 +272,8 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
 
 // ---------------------------------------------------------------------------
 // One pass of FP32 sweeps.  MODE 0: right-hand side p (FFVILS.h:853-871:
-// p = r at iteration 1, else p = r + beta*(p + (-gamma)*q)); MODE 1: right-
+// p = r at the first iteration of a cycle, which also sets r0 = r, else
+// p = r + beta*(p + (-gamma)*q)); MODE 1: right-
 // hand side s = (-alpha)*q + r (FFVILS.h:898-903).  FIRST: the pass that
 // forms the right-hand side (writes p or s in FP64, and its FP32 copy when
 // more passes follow) and starts from e = 0 with zero guides.  LAST: writes
@@ -266,98 +282,103 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
 template <int MODE, bool FIRST, bool LAST>
 __global__ void __launch_bounds__(PT, 1)
 mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
-                double* __restrict__ pv, const double* __restrict__ q,
+                double* __restrict__ r0, double* __restrict__ pv, const double* __restrict__ q,
                 const float* __restrict__ coef, float* __restrict__ v32,
                 const float* __restrict__ ein, float* __restrict__ eout) {
-  const int blk = C.first + blockIdx.x;
-  const int inst = active_instance(C, blk);
-  if (inst < 0) return;
   __shared__ float E[BLOCK_CELLS];
   __shared__ float G[6 * FACE_CELLS];
   const int tid = threadIdx.x;
-  const size_t base = (size_t)blk * BLOCK_CELLS;
-  // this thread's cells: storage slots tid + 512*m, colour m >> 2
-  float cf[8][7];
-  const float* cb = coef + (size_t)blk * 7 * BLOCK_CELLS;
-#pragma unroll
-  for (int m = 0; m < 8; ++m)
-#pragma unroll
-    for (int a = 0; a < 7; ++a) cf[m][a] = __ldg(cb + a * BLOCK_CELLS + tid + PT * m);
-  float v[8];
-  if (FIRST) {
-    const SolveState* S = C.inst.st + inst;
-    const bool copy = S->iter == 1;
-    const double mgamma = -S->gamma, beta = S->beta, malpha = -S->alpha;
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const size_t s = base + tid + PT * m;
-      double rhs;
-      if (MODE == 0) {
-        if (copy) {
-          rhs = r[s];
-        } else {
-          const double t = pv[s] + mgamma * q[s];
-          rhs = r[s] + beta * t;
-        }
-      } else {
-        rhs = malpha * q[s] + r[s];
-      }
-      pv[s] = rhs;
-      v[m] = (float)rhs;
-      if (!LAST) v32[s] = v[m];
-      E[tid + PT * m] = 0.0f;
-    }
-    for (int g = tid; g < 6 * FACE_CELLS; g += PT) G[g] = 0.0f;
-  } else {
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      v[m] = __ldg(v32 + base + tid + PT * m);
-      E[tid + PT * m] = __ldg(ein + base + tid + PT * m);
-    }
-    BCSet hom;
-    for (int f = 0; f < 6; ++f) {
-      hom.type[f] = BC_DIRICHLET;
-      hom.value[f] = 0.0;
-    }
-    const double dx = C.dx[blk];
-    if (tid < 3 * 128) {
-      const int f = 2 * (tid >> 7), p0 = tid & 127, p1 = p0 + 128;
-      for (int h = 0; h < 2; ++h) {
-        const FaceNbr nb = C.nbr[blk * 6 + f + h];
-        double g0, g1;
-        guide_pair(ein, blk, f + h, p0, p1, nb, hom, dx, g0, g1);
-        G[(f + h) * FACE_CELLS + p0] = (float)g0;
-        G[(f + h) * FACE_CELLS + p1] = (float)g1;
-      }
-    }
-  }
-  __syncthreads();
   const float mom = -omega;
-#pragma unroll 1
-  for (int it = 0; it < nsweep; ++it) {
+  const int n_act = *C.n_active;
+  for (int item = blockIdx.x; item < n_act; item += gridDim.x) {
+    const int blk = C.active[item];
+    const int inst = active_instance(C, blk);
+    if (inst < 0) continue;
+    const size_t base = (size_t)blk * BLOCK_CELLS;
+    // this thread's cells: storage slots tid + 512*m, colour m >> 2
+    float cf[8][7];
+    const float* cb = coef + (size_t)blk * 7 * BLOCK_CELLS;
 #pragma unroll
-    for (int c = 0; c < 2; ++c) {
+    for (int m = 0; m < 8; ++m)
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const int m = 4 * c + h;
-        const int qd = tid + PT * h;
-        const NbrsT<float> nb = split_neighbours(E + (1 - c) * HALF_CELLS, G, qd, c);
-        float rc = v[m];
-        rc = __fmaf_rn(-cf[m][0], nb.w, rc);
-        rc = __fmaf_rn(-cf[m][1], nb.e, rc);
-        rc = __fmaf_rn(-cf[m][2], nb.s, rc);
-        rc = __fmaf_rn(-cf[m][3], nb.n, rc);
-        rc = __fmaf_rn(-cf[m][4], nb.b, rc);
-        rc = __fmaf_rn(-cf[m][5], nb.t, rc);
-        const float xt = __fmul_rn(rc, cf[m][6]);
-        const float e = E[c * HALF_CELLS + qd];
-        E[c * HALF_CELLS + qd] = __fmaf_rn(mom, __fsub_rn(e, xt), e);
+      for (int a = 0; a < 7; ++a) cf[m][a] = __ldg(cb + a * BLOCK_CELLS + tid + PT * m);
+    float v[8];
+    if (FIRST) {
+      const SolveState* S = C.inst.st + inst;
+      const bool copy = S->cycle == 1;  // first iteration of a (re)start: p = r, r0 = r
+      const double mgamma = -S->gamma, beta = S->beta, malpha = -S->alpha;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const size_t s = base + tid + PT * m;
+        double rhs;
+        if (MODE == 0) {
+          if (copy) {
+            rhs = r[s];
+            r0[s] = rhs;
+          } else {
+            const double t = pv[s] + mgamma * q[s];
+            rhs = r[s] + beta * t;
+          }
+        } else {
+          rhs = malpha * q[s] + r[s];
+        }
+        pv[s] = rhs;
+        v[m] = (float)rhs;
+        if (!LAST) v32[s] = v[m];
+        E[tid + PT * m] = 0.0f;
       }
-      __syncthreads();
-    }
-  }
+      for (int g = tid; g < 6 * FACE_CELLS; g += PT) G[g] = 0.0f;
+    } else {
 #pragma unroll
-  for (int m = 0; m < 8; ++m) eout[base + tid + PT * m] = E[tid + PT * m];
+      for (int m = 0; m < 8; ++m) {
+        v[m] = __ldg(v32 + base + tid + PT * m);
+        E[tid + PT * m] = __ldg(ein + base + tid + PT * m);
+      }
+      BCSet hom;
+      for (int f = 0; f < 6; ++f) {
+        hom.type[f] = BC_DIRICHLET;
+        hom.value[f] = 0.0;
+      }
+      const double dx = C.dx[blk];
+      if (tid < 3 * 128) {
+        const int f = 2 * (tid >> 7), p0 = tid & 127, p1 = p0 + 128;
+        for (int h = 0; h < 2; ++h) {
+          const FaceNbr nb = C.nbr[blk * 6 + f + h];
+          double g0, g1;
+          guide_pair(ein, blk, f + h, p0, p1, nb, hom, dx, g0, g1);
+          G[(f + h) * FACE_CELLS + p0] = (float)g0;
+          G[(f + h) * FACE_CELLS + p1] = (float)g1;
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int it = 0; it < nsweep; ++it) {
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const int m = 4 * c + h;
+          const int qd = tid + PT * h;
+          const NbrsT<float> nb = split_neighbours(E + (1 - c) * HALF_CELLS, G, qd, c);
+          float rc = v[m];
+          rc = __fmaf_rn(-cf[m][0], nb.w, rc);
+          rc = __fmaf_rn(-cf[m][1], nb.e, rc);
+          rc = __fmaf_rn(-cf[m][2], nb.s, rc);
+          rc = __fmaf_rn(-cf[m][3], nb.n, rc);
+          rc = __fmaf_rn(-cf[m][4], nb.b, rc);
+          rc = __fmaf_rn(-cf[m][5], nb.t, rc);
+          const float xt = __fmul_rn(rc, cf[m][6]);
+          const float e = E[c * HALF_CELLS + qd];
+          E[c * HALF_CELLS + qd] = __fmaf_rn(mom, __fsub_rn(e, xt), e);
+        }
+        __syncthreads();
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 8; ++m) eout[base + tid + PT * m] = E[tid + PT * m];
+    __syncthreads();  // E and G are refilled for the next block
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -369,33 +390,37 @@ template <int NV>
 __global__ void __launch_bounds__(MT)
 mx_matvec_kernel(MixCtx C, const float* __restrict__ x, const double* __restrict__ A,
                  double* __restrict__ y, const double* __restrict__ w0) {
-  const int blk = C.first + blockIdx.x;
-  const int inst = active_instance(C, blk);
-  if (inst < 0) return;
   __shared__ double O[BLOCK_CELLS];
   __shared__ double G[6 * FACE_CELLS];
-  stage_f32_as_f64(O, G, x, blk, C);
-  __syncthreads();
   const int tid = threadIdx.x;
-  const size_t base = (size_t)blk * BLOCK_CELLS;
-  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
-  double acc[NV][2][2] = {};
+  const int n_act = *C.n_active;
+  for (int item = blockIdx.x; item < n_act; item += gridDim.x) {
+    const int blk = C.active[item];
+    const int inst = active_instance(C, blk);
+    if (inst < 0) continue;
+    stage_f32_as_f64(O, G, x, blk, C);
+    __syncthreads();
+    const size_t base = (size_t)blk * BLOCK_CELLS;
+    const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+    double acc[NV][2][2] = {};
 #pragma unroll
-  for (int c = 0; c < 2; ++c) {
+    for (int c = 0; c < 2; ++c) {
 #pragma unroll 2
-    for (int m = 0; m < 8; ++m) {
-      const int qd = tid + MT * m, s = c * HALF_CELLS + qd;
-      const Nbrs v = split_neighbours(O + (1 - c) * HALF_CELLS, G, qd, c);
-      const double yv = __ldg(Ab + 4096 + s) * v.w + __ldg(Ab + 8192 + s) * v.e +
-                        __ldg(Ab + 12288 + s) * v.s + __ldg(Ab + 16384 + s) * v.n +
-                        __ldg(Ab + 20480 + s) * v.b + __ldg(Ab + 24576 + s) * v.t +
-                        __ldg(Ab + s) * O[s];
-      y[base + s] = yv;
-      acc[0][c][m & 1] += yv * __ldg(w0 + base + s);
-      if (NV == 2) acc[NV - 1][c][m & 1] += yv * yv;
+      for (int m = 0; m < 8; ++m) {
+        const int qd = tid + MT * m, s = c * HALF_CELLS + qd;
+        const Nbrs v = split_neighbours(O + (1 - c) * HALF_CELLS, G, qd, c);
+        const double yv = __ldg(Ab + 4096 + s) * v.w + __ldg(Ab + 8192 + s) * v.e +
+                          __ldg(Ab + 12288 + s) * v.s + __ldg(Ab + 16384 + s) * v.n +
+                          __ldg(Ab + 20480 + s) * v.b + __ldg(Ab + 24576 + s) * v.t +
+                          __ldg(Ab + s) * O[s];
+        y[base + s] = yv;
+        acc[0][c][m & 1] += yv * __ldg(w0 + base + s);
+        if (NV == 2) acc[NV - 1][c][m & 1] += yv * yv;
+      }
     }
+    mx_reduce<NV>(acc, C, blk, inst, NV == 1 ? FIN_MX_ALPHA : FIN_MX_GAMMA);
+    __syncthreads();  // O and G are refilled for the next block
   }
-  mx_reduce<NV>(acc, C, blk, inst, NV == 1 ? FIN_MX_ALPHA : FIN_MX_GAMMA);
 }
 
 // ---------------------------------------------------------------------------
@@ -408,27 +433,31 @@ mx_update_kernel(MixCtx C, double* __restrict__ x, const float* __restrict__ ph,
                  const float* __restrict__ sh, double* __restrict__ r,
                  const double* __restrict__ t, const double* __restrict__ s,
                  const double* __restrict__ r0) {
-  const int blk = C.first + blockIdx.x;
-  const int inst = active_instance(C, blk);
-  if (inst < 0) return;
-  const SolveState* S = C.inst.st + inst;
-  const double alpha = S->alpha, gamma = S->gamma, mgamma = -S->gamma;
-  const size_t base = (size_t)blk * BLOCK_CELLS;
   const int tid = threadIdx.x;
-  double acc[2][2][2] = {};
+  const int n_act = *C.n_active;
+  for (int item = blockIdx.x; item < n_act; item += gridDim.x) {
+    const int blk = C.active[item];
+    const int inst = active_instance(C, blk);
+    if (inst < 0) continue;
+    const SolveState* S = C.inst.st + inst;
+    const double alpha = S->alpha, gamma = S->gamma, mgamma = -S->gamma;
+    const size_t base = (size_t)blk * BLOCK_CELLS;
+    double acc[2][2][2] = {};
 #pragma unroll
-  for (int c = 0; c < 2; ++c) {
+    for (int c = 0; c < 2; ++c) {
 #pragma unroll 4
-    for (int m = 0; m < 8; ++m) {
-      const size_t i = base + c * HALF_CELLS + tid + MT * m;
-      x[i] = alpha * (double)ph[i] + gamma * (double)sh[i] + x[i];
-      const double rn = mgamma * t[i] + s[i];
-      r[i] = rn;
-      acc[0][c][m & 1] += rn * rn;
-      acc[1][c][m & 1] += rn * __ldg(r0 + i);
+      for (int m = 0; m < 8; ++m) {
+        const size_t i = base + c * HALF_CELLS + tid + MT * m;
+        x[i] = alpha * (double)ph[i] + gamma * (double)sh[i] + x[i];
+        const double rn = mgamma * t[i] + s[i];
+        r[i] = rn;
+        acc[0][c][m & 1] += rn * rn;
+        acc[1][c][m & 1] += rn * __ldg(r0 + i);
+      }
     }
+    mx_reduce<2>(acc, C, blk, inst, FIN_MX_UPDATE);
+    __syncthreads();  // the reduction's shared words are reused for the next block
   }
-  mx_reduce<2>(acc, C, blk, inst, FIN_MX_UPDATE);
 }
 
 // ---------------------------------------------------------------------------
@@ -444,23 +473,37 @@ void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
 
 template <int MODE, bool FIRST, bool LAST>
 static void sweep_launch(cudaStream_t s, const MixCtx& C, int count, float omega, int nsweep,
-                         const double* r, double* pv, const double* q, const float* coef,
-                         float* v32, const float* ein, float* eout) {
+                         const double* r, double* r0, double* pv, const double* q,
+                         const float* coef, float* v32, const float* ein, float* eout) {
   mx_sweep_kernel<MODE, FIRST, LAST>
-      <<<count, PT, 0, s>>>(C, omega, nsweep, r, pv, q, coef, v32, ein, eout);
+      <<<count, PT, 0, s>>>(C, omega, nsweep, r, r0, pv, q, coef, v32, ein, eout);  // count: CTAs
 }
 
 void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first, bool last,
-                     float omega, int nsweep, const double* r, double* pv, const double* q,
-                     const float* coef, float* v32, const float* ein, float* eout) {
+                     float omega, int nsweep, const double* r, double* r0, double* pv,
+                     const double* q, const float* coef, float* v32, const float* ein,
+                     float* eout) {
 #define MX_CASE(M, F, L)                                                                   \
   if (mode == M && first == F && last == L) {                                              \
-    sweep_launch<M, F, L>(s, C, count, omega, nsweep, r, pv, q, coef, v32, ein, eout);     \
+    sweep_launch<M, F, L>(s, C, count, omega, nsweep, r, r0, pv, q, coef, v32, ein, eout); \
     return;                                                                                \
   }
   MX_CASE(0, true, true) MX_CASE(0, true, false) MX_CASE(0, false, true) MX_CASE(0, false, false)
   MX_CASE(1, true, true) MX_CASE(1, true, false) MX_CASE(1, false, true) MX_CASE(1, false, false)
 #undef MX_CASE
+}
+
+void mx_grid_sizes(int* sweep, int* matvec, int* update) {
+  int dev = 0, sms = 0, a = 0, b = 0, c = 0, d = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, true>, PT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, true>, PT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2>, MT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, mx_update_kernel, MT, 0);
+  *sweep = sms * std::max(1, std::min(a, b));
+  *matvec = sms * std::max(1, c);
+  *update = sms * std::max(1, d);
 }
 
 void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, const float* x,

@@ -742,6 +742,7 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   double* x = P->x[P->xcur];
   CK(cudaEventRecord(P->ev0, P->stream));
   launch_dot(P->stream, C, P->b, P->b, P->partials, P->st, FIN_BB, 0);
+  CK(cudaGetLastError());
   int launches = 1;
   int64_t bytes = interior_bytes(P, 2);
   SolveState h;
@@ -812,7 +813,7 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   R.bytes_moved = bytes;
   R.kernel_launches = launches + 1;
   if (prm->history && N > 0) {
-    const int nh = (h.count >= 1 && h.count <= N) ? h.count : (h.count == 0 ? 0 : N);
+    const int nh = (h.count >= 1 && h.count <= N) ? h.count : (h.count == 0 ? h.iter : N);
     if (nh > 0)
       CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
   }
@@ -873,6 +874,7 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
   double* x = P->x[P->xcur];
   CK(cudaEventRecord(P->ev0, P->stream));
   launch_dot(P->stream, C, P->b, P->b, P->partials, P->st, FIN_BB, 0);
+  CK(cudaGetLastError());
   int launches = 1;
   int64_t bytes = interior_bytes(P, 2);
   SolveState h;
@@ -926,7 +928,7 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
   R.bytes_moved = bytes;
   R.kernel_launches = launches + 1;
   if (prm->history && N > 0) {
-    const int nh = (h.count >= 1 && h.count <= N) ? h.count : (h.count == 0 ? 0 : N);
+    const int nh = (h.count >= 1 && h.count <= N) ? h.count : (h.count == 0 ? h.iter : N);
     if (nh > 0)
       CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
   }

@@ -46,6 +46,7 @@ struct ffvgpu_instance {
   int32_t count_max = 0;
   double epsilon = 0.0;
   int32_t status = 0;  // of the last solve: 0 ok, 2 NaN/Inf residual
+  int32_t last_iter = 0;  // iterations with a residual before an early exit
   ffvgpu_result result{};
   ffvgpu_grid_desc desc{};  // level / block_index point into the vectors below
   std::vector<int32_t> level, index;
@@ -127,6 +128,13 @@ struct ffvgpu_pool {
   int mgraph_sweeps = 0, mgraph_per = 0;
   int64_t m_launches = 0;
   int64_t m_bytes = 0;
+  // active-block list of the persistent kernels: device [1 + capacity]
+  // (count, then block ids), refilled from two pinned staging buffers
+  int32_t* act_d = nullptr;
+  int32_t* act_h[2] = {nullptr, nullptr};
+  cudaEvent_t act_ev[2] = {nullptr, nullptr};
+  int act_next = 0;
+  int grid_sweep = 0, grid_matvec = 0, grid_update = 0;
 
   ffvgpu::KCtx ctx(const ffvgpu::BCSet& bc) const {
     ffvgpu::KCtx C;

@@ -39,6 +39,7 @@ EXPORTS = [
     "ffvgpu_instance_admit_sphere", "ffvgpu_instance_upload", "ffvgpu_instance_download",
     "ffvgpu_instance_release", "ffvgpu_instance_blocks", "ffvgpu_pool_free_blocks",
     "ffvgpu_mixed_begin", "ffvgpu_mixed_advance", "ffvgpu_mixed_poll", "ffvgpu_instance_result",
+    "ffvgpu_assemble_sphere", "ffvgpu_instance_fill",
 ]
 
 
@@ -84,7 +85,7 @@ class MixedParams(ctypes.Structure):
         ("omega", ctypes.c_double), ("sweeps", ctypes.c_int32),
         ("sweeps_per_exchange", ctypes.c_int32), ("count_max", ctypes.c_int32),
         ("epsilon", ctypes.c_double), ("check_every", ctypes.c_int32),
-        ("history", ctypes.c_void_p),
+        ("history", ctypes.c_void_p), ("restart_drop", ctypes.c_double),
     ]
 
 
@@ -150,9 +151,11 @@ def lib():
         L.ffvgpu_batch_create.argtypes = [ctypes.POINTER(BatchDesc), ctypes.POINTER(vp)]
         L.ffvgpu_instance_admit.argtypes = [vp, ctypes.POINTER(GridDesc), vp]
         L.ffvgpu_instance_admit_sphere.argtypes = [vp, ctypes.POINTER(SphereProblem), vp]
+        L.ffvgpu_assemble_sphere.argtypes = [vp, ctypes.POINTER(SphereProblem)]
         L.ffvgpu_instance_upload.argtypes = [vp, i32, i32, vp, i32]
         L.ffvgpu_instance_download.argtypes = [vp, i32, i32, vp, i32]
         L.ffvgpu_instance_release.argtypes = [vp, i32]
+        L.ffvgpu_instance_fill.argtypes = [vp, i32, i32, dbl]
         L.ffvgpu_instance_blocks.argtypes = [vp, i32]
         L.ffvgpu_pool_free_blocks.argtypes = [vp, vp, vp]
         L.ffvgpu_mixed_begin.argtypes = [vp, i32, MP]
@@ -346,7 +349,10 @@ class Pool:
                    sweep_ms=res.sweep_ms, sweep_launches=res.sweep_launches,
                    bytes_moved=res.bytes_moved, kernel_launches=res.kernel_launches)
         if history:
-            n = res.count if 1 <= res.count <= count_max else (count_max if res.count > 0 else 0)
+            if res.count == 0:  # early exit: the residuals written before it
+                n = int(np.argmax(hist == 0)) if (hist == 0).any() else len(hist)
+            else:
+                n = res.count if 1 <= res.count <= count_max else count_max
             out["history"] = hist[:n].copy()
         return out
 
@@ -385,12 +391,16 @@ class Pool:
         _check(lib().ffvgpu_dot(self._h, FIELD[fx], FIELD[fy], ctypes.byref(v)), "dot")
         return v.value
 
+    def assemble_sphere(self, problem):
+        """Device-generated sphere-flow inputs + UpdateP P02-P05 (pool made from its grid)."""
+        _check(lib().ffvgpu_assemble_sphere(self._h, ctypes.byref(problem)), "assemble_sphere")
+
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-                    epsilon=1e-8, history=True, check_every=0):
+                    epsilon=1e-8, history=True, check_every=0, restart_drop=1e-3):
         """Mixed-precision solve (FP64 BiCGSTAB, FP32 RB-SOR preconditioner)."""
         hist = np.zeros(max(count_max, 1), np.float64) if history else None
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
-                          hist.ctypes.data if history else None)
+                          hist.ctypes.data if history else None, restart_drop)
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -486,11 +496,19 @@ class Batch:
     def release(self, inst):
         _check(lib().ffvgpu_instance_release(self._h, inst), "instance_release")
 
+    def fill(self, inst, field, value):
+        _check(lib().ffvgpu_instance_fill(self._h, inst, FIELD[field], float(value)),
+               "instance_fill")
+
+    def set_stream(self, stream_handle):
+        _check(lib().ffvgpu_pool_set_stream(self._h, ctypes.c_void_p(stream_handle or None)),
+               "pool_set_stream")
+
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-                    epsilon=1e-8, check_every=0):
+                    epsilon=1e-8, check_every=0, restart_drop=1e-3):
         """Solves every admitted instance; returns the first instance's result."""
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
-                          None)
+                          None, restart_drop)
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -498,8 +516,9 @@ class Batch:
                     kernel_launches=res.kernel_launches, bytes_moved=res.bytes_moved)
 
     def begin(self, inst, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-              epsilon=1e-8):
-        prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, 0, None)
+              epsilon=1e-8, restart_drop=1e-3):
+        prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, 0, None,
+                          restart_drop)
         _check(lib().ffvgpu_mixed_begin(self._h, inst, ctypes.byref(prm)), "mixed_begin")
 
     def advance(self, iterations):

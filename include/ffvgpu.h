@@ -267,7 +267,11 @@ ffvgpu_status ffvgpu_sphere_grid_fill(const ffvgpu_sphere_grid* g, uint64_t seed
  * them between guide-cell exchanges (each block sweeps on chip against
  * fixed guide values in between).  sweeps must be a multiple of
  * sweeps_per_exchange.  Result fields as ffvgpu_solve_bicgstab; the solve
- * stops when sqrt(r.r / b.b) <= epsilon or after count_max iterations. */
+ * stops when sqrt(r.r / b.b) <= epsilon or after count_max iterations.
+ * Rounding in FP32 makes the preconditioner slightly nonlinear, which
+ * BiCGSTAB's recurrence does not tolerate for long (it stalls, then
+ * diverges); restarts from the current residual every time it has fallen by
+ * restart_drop (1e-3 works on the sphere grids) keep it converging. */
 typedef struct {
   double omega;                /* FP32 SOR relaxation factor */
   int32_t sweeps;              /* colour-pair sweeps per preconditioner application */
@@ -276,6 +280,8 @@ typedef struct {
   double epsilon;
   int32_t check_every;         /* iterations between host polls (0: 8) */
   double* history;             /* optional host array [count_max]: residual per iteration */
+  double restart_drop;         /* restart the recurrence (r0 = r, p = r) each time the
+                                  residual has fallen by this factor; 0: never */
 } ffvgpu_mixed_params;
 
 /* Solves every admitted instance of the pool (a pool made from one grid is
@@ -325,12 +331,18 @@ typedef struct {
 
 ffvgpu_status ffvgpu_instance_admit_sphere(ffvgpu_pool* pool, const ffvgpu_sphere_problem* prob,
                                            int32_t* instance);
+/* The same generation and assembly for a pool made from the problem's own
+ * grid (ffvgpu_pool_create on the blocks of ffvgpu_sphere_grid_create). */
+ffvgpu_status ffvgpu_assemble_sphere(ffvgpu_pool* pool, const ffvgpu_sphere_problem* prob);
 /* Per-instance transfers in the reference layout of ffvgpu_pool_upload /
  * ffvgpu_pool_download (host buffers hold the instance's blocks only). */
 ffvgpu_status ffvgpu_instance_upload(ffvgpu_pool* pool, int32_t instance, ffvgpu_field field,
                                      const void* host, int32_t vc);
 ffvgpu_status ffvgpu_instance_download(ffvgpu_pool* pool, int32_t instance, ffvgpu_field field,
                                        void* host, int32_t vc);
+/* FFVILS::Fill on one instance's blocks (interior and stored guide layer). */
+ffvgpu_status ffvgpu_instance_fill(ffvgpu_pool* pool, int32_t instance, ffvgpu_field field,
+                                   double value);
 /* Frees the instance's blocks and slot; refused while its solve runs. */
 ffvgpu_status ffvgpu_instance_release(ffvgpu_pool* pool, int32_t instance);
 int32_t ffvgpu_instance_blocks(const ffvgpu_pool* pool, int32_t instance);

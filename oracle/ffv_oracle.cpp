@@ -1175,7 +1175,7 @@ void mixed_precondition(Oracle& O, const Coef32& C, int fv, int fout, float omeg
 }  // namespace
 
 int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double epsilon,
-              int* count, double* residual, double* hist) {
+              double restart_drop, int* count, double* residual, double* hist) {
   Oracle& R = *O;
   if (countMax <= 0) {
     *count = 1;
@@ -1194,6 +1194,10 @@ int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double
   CalcR(R, OF_R, OF_X, OF_B);
   COPY(R, OF_R0, OF_R);
   double rr0 = 1.0, alpha = 0.0, gamma = 1.0;
+  // restarts: when the residual has dropped by restart_drop since the last
+  // (re)start, the recurrence starts again from the current r (r0 = r, p = r)
+  double next_restart = -1.0;
+  int cycle = 1;
   int c;
   for (c = 1; c <= countMax; ++c) {
     double rr1 = DOT(R, OF_R, OF_R0);
@@ -1202,7 +1206,12 @@ int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double
       c = 0;
       break;
     }
-    if (c == 1) {
+    if (c == 1 && restart_drop > 0.0) {
+      double r_init;
+      is_converged(r_init, rr1, bb, 0.0);
+      next_restart = r_init * restart_drop;
+    }
+    if (cycle == 1) {
       COPY(R, OF_P, OF_R);
     } else {
       double beta = rr1 / rr0 * alpha / gamma;
@@ -1232,6 +1241,15 @@ int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double
     }
     if (st == 1) break;
     rr0 = rr1;
+    ++cycle;
+    if (next_restart > 0.0 && *residual <= next_restart && c < countMax) {
+      next_restart = *residual * restart_drop;
+      COPY(R, OF_R0, OF_R);
+      rr0 = 1.0;
+      alpha = 0.0;
+      gamma = 1.0;
+      cycle = 1;
+    }
   }
   impose_bc_p(R, OF_X);
   *count = (c > countMax) ? countMax + 1 : c;
