@@ -52,7 +52,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ffvgpu", choices=["ffvgpu", "reference"])
-    ap.add_argument("--form", default="rbsor", choices=["rbsor", "mixed", "batch"])
+    ap.add_argument("--form", default="rbsor", choices=["rbsor", "mixed", "batch", "serve"])
+    ap.add_argument("--requests", type=int, default=32, help="serve form: requests per rate")
+    ap.add_argument("--rates", default="10,20,50,100,200,500", help="serve form: req/s")
+    ap.add_argument("--capacity", type=int, default=40000, help="serve form: pool blocks")
+    ap.add_argument("--profile-iterations", type=int, default=0,
+                    help="mixed form: only run this many mixed iterations once (for ncu)")
     ap.add_argument("--level", type=int, default=5)
     ap.add_argument("--instances", type=int, default=64, help="batch form: instances")
     ap.add_argument("--fp64-sample", type=int, default=64,
@@ -312,7 +317,115 @@ def timed(stream, fn):
 def run_form(args):
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    return run_mixed(args) if args.form == "mixed" else run_batch(args)
+    return {"mixed": run_mixed, "batch": run_batch, "serve": run_serve}[args.form](args)
+
+
+def size_table():
+    """(level, radius) -> leaf blocks of the sphere grid centred at (4, 0, 0)."""
+    import ffvgpu
+    table = []
+    for L in range(2, 6):
+        for r in np.geomspace(0.1, 1.6, 20):
+            g = ffvgpu.SphereGrid(L, center=(4.0, 0.0, 0.0), radius=float(r))
+            table.append((g.nb, L, float(r)))
+    return table
+
+
+def serve_requests(n, seed, table):
+    """Config-5 requests: target block count log-uniform in [100, 8000], met by
+    the (max level, radius) of the table whose count is nearest; centre
+    uniform in the inner half of the domain; seeded RHS."""
+    r = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        target = float(np.exp(r.uniform(np.log(100.0), np.log(8000.0))))
+        nb, L, rad = min(table, key=lambda t: abs(np.log(t[0] / target)))
+        c = r.uniform([0.0, -2.0, -2.0], [8.0, 2.0, 2.0])
+        out.append((L, dict(center=tuple(float(v) for v in c), radius=rad), 1000 + k))
+    return out
+
+
+def fifo_latencies(arrivals, service):
+    """One server, first come first served: completion - arrival per request."""
+    t, lat = 0.0, []
+    for a, s_ in zip(arrivals, service):
+        t = max(t, a) + s_
+        lat.append(t - a)
+    return lat
+
+
+def run_serve(args):
+    import torch
+    import ffvgpu
+    stream = torch.cuda.current_stream()
+    table = size_table()
+    reqs = serve_requests(args.requests, args.seed, table)
+    probs = [ffvgpu.sphere_problem(L, seed=s, sigma=0.01, **kw) for (L, kw, s) in reqs]
+    blocks = [ffvgpu.SphereGrid(L, **kw).nb for (L, kw, _) in reqs]
+    rates = [float(v) for v in args.rates.split(",")]
+    B = ffvgpu.Batch(args.capacity, 64)
+    B.set_stream(stream.cuda_stream)
+    B.serve([0.0], probs[:1], iterations_per_step=8, count_max=5000)  # warm-up
+    per_rate = []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for rate in rates:
+            rng = np.random.default_rng(int(rate))
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(probs)))
+            arrivals -= arrivals[0]
+            out = B.serve(arrivals, probs, iterations_per_step=8, count_max=5000)
+            lat = np.array([o["finish_s"] - o["arrival_s"] for o in out])
+            span = max(o["finish_s"] for o in out)
+            per_rate.append({"rate": rate, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                             "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                             "solves_per_s": len(out) / span,
+                             "worst_residual": max(o["residual"] for o in out),
+                             "iterations_max": max(o["count"] for o in out)})
+    B.close()
+    # one-at-a-time plain FP64 GPU solves of the same requests: service times
+    service = []
+    for (L, kw, s), p in zip(reqs, probs):
+        t0 = time.perf_counter()
+        g = ffvgpu.SphereGrid(L, **kw)
+        P = ffvgpu.Pool(g.desc())
+        P.set_stream(stream.cuda_stream)
+        P.assemble_sphere(p)
+        r = P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"], 50000, 1e-8,
+                             history=False, restart_drop=1e-3)
+        P.download("X", 1)
+        torch.cuda.synchronize()
+        service.append(time.perf_counter() - t0)
+        P.close()
+    fp64 = []
+    for rate in rates:
+        rng = np.random.default_rng(int(rate))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(probs)))
+        arrivals -= arrivals[0]
+        lat = np.array(fifo_latencies(arrivals, service))
+        fp64.append({"rate": rate, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                     "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                     "solves_per_s": len(service) / float(max(arrivals[i] + lat[i]
+                                                              for i in range(len(lat))))})
+    top = per_rate[-1]
+    line = {
+        "form": "serve", "metric": "served solves/s and p50/p99 latency at 1e-8",
+        "value": top["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "f64 outer / f32 sweeps", "data": "synthetic",
+        "config": {"workload": f"serve-{len(probs)}-requests-per-rate", "rates": rates,
+                   "blocks_min_max": [int(min(blocks)), int(max(blocks))],
+                   "blocks_total": int(sum(blocks)), "capacity_blocks": args.capacity,
+                   "mixed": MIXED, "iterations_per_replay": 8, "epsilon": 1e-8,
+                   "requests_rule": "block count log-uniform [100, 8000] via (max level, "
+                                    "radius) table, centre U([0,8]x[-2,2]x[-2,2]), Poisson "
+                                    "arrivals per rate"},
+        "per_rate": per_rate,
+        "fp64_one_at_a_time": {"service_s_mean": float(np.mean(service)),
+                               "solves_per_s": len(service) / float(np.sum(service)),
+                               "solver": "BiCGSTAB omega 1, PreCount 2, restarts 1e-3",
+                               "per_rate_fifo": fp64},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_mixed(args):
@@ -321,11 +434,25 @@ def run_mixed(args):
     stream = torch.cuda.current_stream()
     g, P = device_system(args.level, args.seed, stream.cuda_stream)
     peak, peak_kind = measured_peaks()
+    if args.profile_iterations > 0:  # a fixed, short run for profilers
+        P.fill("X", 0.0)
+        r = P.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
+                          args.profile_iterations, 0.0, history=False,
+                          check_every=args.profile_iterations)
+        print(json.dumps({"form": "mixed-profile", "level": args.level, "blocks": int(g.nb),
+                          "iterations": args.profile_iterations, "ms": r["elapsed_ms"]}))
+        P.close()
+        return 0
 
-    def fp64():
+    def fp64_ref():  # the reference's recurrence, no restarts
+        P.fill("X", 0.0)
+        return P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"], 20000, 1e-8,
+                                history=False)
+
+    def fp64():  # with the restart option, so that it reaches 1e-8 where the above stalls
         P.fill("X", 0.0)
         return P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"], 50000, 1e-8,
-                                history=False)
+                                history=False, restart_drop=1e-3)
 
     def mixed():
         P.fill("X", 0.0)
@@ -334,7 +461,7 @@ def run_mixed(args):
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         res = {}
-        for name, fn in (("fp64", fp64), ("mixed", mixed)):
+        for name, fn in (("fp64_ref", fp64_ref), ("fp64", fp64), ("mixed", mixed)):
             for _ in range(max(1, args.warmup)):
                 fn()
             ms, runs = [], []
@@ -345,8 +472,8 @@ def run_mixed(args):
             res[name] = (runs[-1], float(np.mean(ms)), runs)
     # errors against a converged FP64 solution of the same system
     P.fill("X", 0.0)
-    rref = P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"], 50000, 1e-12,
-                            history=False)
+    rref = P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"], 50000, 1e-11,
+                            history=False, restart_drop=1e-3)
     pref = P.download("X", 2)[:, 2:18, 2:18, 2:18].copy()
     mixed()
     pm = P.download("X", 2)[:, 2:18, 2:18, 2:18].copy()
@@ -354,6 +481,7 @@ def run_mixed(args):
     pf = P.download("X", 2)[:, 2:18, 2:18, 2:18].copy()
     P.close()
     rf, tf, _ = res["fp64"]
+    rr_, tr_, _ = res["fp64_ref"]
     rm, tm, _ = res["mixed"]
     achieved = rm["bytes_moved"] / (tm * 1e-3) / 1e9
     line = {
@@ -365,8 +493,13 @@ def run_mixed(args):
                    "cells": int(g.cells), "epsilon": 1e-8, "mixed": MIXED,
                    "fp64": dict(FP64_SOLVER, solver="BiCGSTAB (FFVILS.h:793-974)")},
         "fp64": {"solves_per_s": 1e3 / tf, "ms": tf, "iterations": rf["count"],
-                 "residual": rf["residual"],
-                 "achieved_gbs": rf["bytes_moved"] / (tf * 1e-3) / 1e9},
+                 "residual": rf["residual"], "restart_drop": 1e-3},
+        "fp64_reference_recurrence": {
+            "ms": tr_, "iterations": rr_["count"], "residual": rr_["residual"],
+            "reached_1e-8": bool(rr_["status"] == 0 and rr_["count"] > 0 and
+                                 rr_["residual"] <= 1e-8),
+            "note": "FFVILS::BiCGSTAB as the reference runs it (no restarts); count 0 is its "
+                    "|r.r0| < FLT_MIN exit"},
         "mixed": {"solves_per_s": 1e3 / tm, "ms": tm, "iterations": rm["count"],
                   "residual": rm["residual"], "kernel_launches": rm["kernel_launches"]},
         "speedup_vs_fp64": tf / tm,
@@ -375,8 +508,9 @@ def run_mixed(args):
                      "/ its device time", "peak_source": f"{peak_kind} hbm_gbs"},
         "error_vs_fp64_converged": {"mixed": field_errors(pm, pref, g.level),
                                     "fp64_at_1e-8": field_errors(pf, pref, g.level),
-                                    "reference_solution": f"FP64 BiCGSTAB to 1e-12 "
-                                                          f"({rref['count']} iterations)"},
+                                    "reference_solution": f"FP64 BiCGSTAB with restarts to "
+                                                          f"1e-11 ({rref['count']} iterations, "
+                                                          f"residual {rref['residual']:.2e})"},
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -447,7 +581,7 @@ def run_batch(args):
         def f64():
             P.fill("X", 0.0)
             return P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"], 50000, 1e-8,
-                                    history=False)
+                                    history=False, restart_drop=1e-3)
 
         def mx():
             P.fill("X", 0.0)

@@ -242,7 +242,8 @@ __device__ __forceinline__ void finalize(SolveState* st, double total, int fin, 
       st->bb = total;
       break;
     case FIN_RBGS:
-    case FIN_CG_RR: {
+    case FIN_CG_RR:
+    case FIN_BI_RR: {
       const double res = resid_of(total, st->bb);
       st->rr = total;
       st->residual = res;
@@ -259,6 +260,17 @@ __device__ __forceinline__ void finalize(SolveState* st, double total, int fin, 
         st->count = st->count_max + 1;  // loop variable after the last pass
       } else if (fin == FIN_CG_RR) {
         st->rr0 = st->rr1;
+      } else if (fin == FIN_BI_RR) {
+        st->rr0 = st->rr1;  // FFVILS.h:960
+        st->cycle += 1;
+        if (st->next_restart > 0.0 && res <= st->next_restart) {
+          // restart from the current r: the next DOT(r, r0) first sets r0 = r
+          st->next_restart = res * st->drop;
+          st->rr0 = 1.0;
+          st->alpha = 0.0;
+          st->gamma = 1.0;
+          st->cycle = 1;
+        }
       }
       break;
     }
@@ -284,6 +296,8 @@ __device__ __forceinline__ void finalize(SolveState* st, double total, int fin, 
         st->done = 1;
       } else {
         st->beta = total / st->rr0 * st->alpha / st->gamma;
+        if (st->drop > 0.0 && st->next_restart < 0.0)  // first iteration: r0 = r
+          st->next_restart = resid_of(total, st->bb) * st->drop;
       }
       break;
     case FIN_BI_QR0:

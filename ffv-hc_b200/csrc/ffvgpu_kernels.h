@@ -41,8 +41,12 @@ void launch_ax_dot(cudaStream_t s, const KCtx& C, const double* p, const double*
                    double* partials, SolveState* st);
 void launch_ax_dot_y(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
                      const double* y, double* partials, SolveState* st, int fin);
+// p = r on the first iteration of a cycle (st->cycle == 1), else the update.
 void launch_bicg_p(cudaStream_t s, const KCtx& C, const double* r, double* p, const double* q,
-                   int first, SolveState* st);
+                   SolveState* st);
+// r.r0 (setting r0 = r first on the first iteration of a cycle).
+void launch_dot_rr0(cudaStream_t s, const KCtx& C, const double* r, double* r0, double* partials,
+                    SolveState* st, int fin, int iter);
 void launch_axpyz(cudaStream_t s, const KCtx& C, double* z, const double* x, const double* y,
                   SolveState* st);
 void launch_bicg_update(cudaStream_t s, const KCtx& C, double* x, const double* pz,

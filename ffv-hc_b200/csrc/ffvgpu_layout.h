@@ -80,6 +80,10 @@ struct SolveState {
   int32_t cycle;     // mixed form: iteration within the current restart cycle (1: p = r)
   double drop;       // mixed form: restart when the residual has dropped by this factor
   double next_restart;  // mixed form: residual at which the next restart happens (< 0: none)
+  double best;       // mixed form: smallest residual of the current cycle
+  double growth;     // mixed form: restart when the residual exceeds growth * best (0: never)
+  int32_t max_cycle; // mixed form: restart after this many iterations of a cycle (0: never)
+  int32_t pad2_;
 };
 
 // Instances: independent problems that share one pool's blocks (a batch).
@@ -112,6 +116,7 @@ enum Fin : int {
   FIN_BI_QR0,     // BiCGSTAB alpha = rr1 / (q_.r0) (FFVILS.h:890-896)
   FIN_BI_TS,      // BiCGSTAB t_.s (FFVILS.h:923-929)
   FIN_BI_TT,      // BiCGSTAB gamma = t_s / (t_.t_) (FFVILS.h:930-936)
+  FIN_BI_RR,      // BiCGSTAB residual of iteration 'iter' (FFVILS.h:952-960), optional restart
   // mixed form, per instance (two sums where noted)
   FIN_MX_INIT,    // b.b and r.r0: early exits of FFVILS.h:822-826 and 847-851
   FIN_MX_ALPHA,   // alpha = rr1 / (q.r0)

@@ -182,6 +182,9 @@ ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
   if (!(prm->omega > 0.0 && prm->omega < 2.0)) return bad("omega must lie in (0, 2)");
   if (!(prm->restart_drop >= 0.0 && prm->restart_drop < 1.0))
     return bad("restart_drop must lie in [0, 1)");
+  if (!(prm->restart_growth == 0.0 || prm->restart_growth > 1.0))
+    return bad("restart_growth must be 0 or greater than 1");
+  if (prm->restart_every < 0) return bad("restart_every must not be negative");
   if (prm->count_max < 0) return bad("count_max must not be negative");
   return FFVGPU_OK;
 }
@@ -633,6 +636,8 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
   h.eps = prm->epsilon;
   h.count_max = prm->count_max;
   h.drop = prm->restart_drop;
+  h.growth = prm->restart_growth;
+  h.max_cycle = prm->restart_every;
   h.hist = P->mhist + (size_t)inst * P->mhist_cap;
   h.done = 0;
   if (prm->count_max <= 0) {  // for(count=1; count<=countMax; ...) runs no iteration

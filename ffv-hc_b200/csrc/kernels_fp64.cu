@@ -253,9 +253,10 @@ ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A
 // t = p + (-gamma)*q_ ; p = r + beta*t (blas.f90:329-395).
 __global__ void __launch_bounds__(THREADS)
 bicg_p_kernel(const double* __restrict__ r, double* __restrict__ p, const double* __restrict__ q,
-              int first, SolveState* st) {
+              SolveState* st) {
   if (solve_done(st)) return;
   const double beta = st->beta, mgamma = -st->gamma;
+  const bool first = st->cycle == 1;  // iteration 1, or the first after a restart
   const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
 #pragma unroll 4
   for (int m = 0; m < 16; ++m) {
@@ -306,7 +307,7 @@ bicg_update_kernel(double* __restrict__ x, const double* __restrict__ pz,
       acc[c][m & 1] += rn * rn;
     }
   }
-  reduce_finalize(acc, partials, st, FIN_CG_RR, iter);
+  reduce_finalize(acc, partials, st, FIN_BI_RR, iter);
 }
 
 // x = x + alpha p; r = r + (-alpha) q (axpy, blas.f90:329-361); r.r.
@@ -345,6 +346,34 @@ dot_kernel(const double* __restrict__ x, const double* __restrict__ y,
     for (int m = 0; m < 8; ++m) {
       const size_t s = base + c * HALF_CELLS + threadIdx.x + THREADS * m;
       acc[c][m & 1] += __ldg(x + s) * __ldg(y + s);
+    }
+  }
+  reduce_finalize(acc, partials, st, fin, iter);
+}
+
+// BiCGSTAB's DOT(r, r0) (FFVILS.h:845-846); on the first iteration of a
+// cycle (iteration 1, or after a restart) r0 is first set to r.
+__global__ void __launch_bounds__(THREADS)
+dot_rr0_kernel(const double* __restrict__ r, double* __restrict__ r0, double* __restrict__ partials,
+               SolveState* st, int fin, int iter) {
+  if (solve_done(st)) return;
+  const bool copy = st->cycle == 1;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll 4
+    for (int m = 0; m < 8; ++m) {
+      const size_t s = base + c * HALF_CELLS + threadIdx.x + THREADS * m;
+      const double rv = r[s];
+      double yv;
+      if (copy) {
+        r0[s] = rv;
+        yv = rv;
+      } else {
+        yv = r0[s];
+      }
+      acc[c][m & 1] += rv * yv;
     }
   }
   reduce_finalize(acc, partials, st, fin, iter);
@@ -627,12 +656,16 @@ void launch_ax_dot_y(cudaStream_t s, const KCtx& C, const double* p, const doubl
   ax_dot_kernel<<<C.nb, THREADS, 0, s>>>(C, p, A, q, y, partials, st, fin);
 }
 void launch_bicg_p(cudaStream_t s, const KCtx& C, const double* r, double* p, const double* q,
-                   int first, SolveState* st) {
-  bicg_p_kernel<<<C.nb, THREADS, 0, s>>>(r, p, q, first, st);
+                   SolveState* st) {
+  bicg_p_kernel<<<C.nb, THREADS, 0, s>>>(r, p, q, st);
 }
 void launch_axpyz(cudaStream_t s, const KCtx& C, double* z, const double* x, const double* y,
                   SolveState* st) {
   axpyz_kernel<<<C.nb, THREADS, 0, s>>>(z, x, y, st);
+}
+void launch_dot_rr0(cudaStream_t s, const KCtx& C, const double* r, double* r0, double* partials,
+                    SolveState* st, int fin, int iter) {
+  dot_rr0_kernel<<<C.nb, THREADS, 0, s>>>(r, r0, partials, st, fin, iter);
 }
 void launch_bicg_update(cudaStream_t s, const KCtx& C, double* x, const double* pz,
                         const double* sz, double* r, const double* t, const double* sv,

@@ -14,11 +14,18 @@
 // coefficients in registers and its iterate in shared memory, and HBM sees
 // one read of the coefficients and one write of the result per group.
 //
-// FP32 sweep of one cell (colour order and neighbour terms as
-// rbgs_smoother, src/CGMfuncs/bils.f90:57-108), every step rounded once:
+// Sweep of one cell (colour order and neighbour terms as rbgs_smoother,
+// src/CGMfuncs/bils.f90:57-108) on FP32 data -- coefficients, right-hand
+// side and iterate are FP32 values -- with the update formed in FP64 and
+// rounded to FP32 once, when it is stored:
 //   rc = v; rc = fma(-aw, eW, rc); ... fma(-ab, eB, rc); fma(-at, eT, rc)
 //   xt = rc * dinv                       (dinv = (float)(1.0 / Ap))
-//   e  = fma(-omega, e - xt, e)          (e - omega (e - xt))
+//   e  = (float)fma(-omega, e - xt, e)   (e - omega (e - xt))
+// Forming rc in FP32 would cancel: once a block has nearly converged locally
+// rc is far smaller than its terms, and its FP32 rounding error (1e-5 and
+// more relative) makes the preconditioner visibly nonlinear, which the
+// BiCGSTAB recurrence does not survive; in FP64 the only nonlinearity left
+// is the final rounding of each stored value.
 // Guide cells of e: the exchange rules (same-level copy, 2:1 interpolation
 // and restriction, src/CGMfuncs/sup.f90) evaluated in FP64 on the FP32
 // values and rounded to FP32; outer faces take homogeneous Dirichlet values.
@@ -71,6 +78,7 @@ __device__ void mx_finalize(SolveState* S, const double* t, int fin) {
       S->iter = 1;
       S->cycle = 1;
       S->next_restart = (S->drop > 0.0) ? resid_of(t[1], t[0]) * S->drop : -1.0;
+      S->best = resid_of(t[1], t[0]);
       break;
     case FIN_MX_ALPHA:
       S->qp = t[0];
@@ -99,10 +107,15 @@ __device__ void mx_finalize(SolveState* S, const double* t, int fin) {
         S->rr0 = S->rr1;  // FFVILS.h:960
         S->cycle += 1;
         double rr1 = t[1];  // next iteration's DOT(r, r0)
-        if (S->next_restart > 0.0 && res <= S->next_restart) {
+        const bool dropped = S->next_restart > 0.0 && res <= S->next_restart;
+        const bool grew = S->growth > 0.0 && res > S->growth * S->best;
+        const bool aged = S->max_cycle > 0 && S->cycle > S->max_cycle;
+        if (res < S->best) S->best = res;
+        if (dropped || grew || aged) {
           // restart from the current r: r0 = r (written by the next
           // iteration's first sweep pass), so DOT(r, r0) = r.r
-          S->next_restart = res * S->drop;
+          if (S->drop > 0.0) S->next_restart = res * S->drop;
+          S->best = res;
           S->rr0 = 1.0;
           S->alpha = 0.0;
           S->gamma = 1.0;
@@ -288,7 +301,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
   __shared__ float E[BLOCK_CELLS];
   __shared__ float G[6 * FACE_CELLS];
   const int tid = threadIdx.x;
-  const float mom = -omega;
+  const double mom = -(double)omega;
   const int n_act = *C.n_active;
   for (int item = blockIdx.x; item < n_act; item += gridDim.x) {
     const int blk = C.active[item];
@@ -361,16 +374,16 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
           const int m = 4 * c + h;
           const int qd = tid + PT * h;
           const NbrsT<float> nb = split_neighbours(E + (1 - c) * HALF_CELLS, G, qd, c);
-          float rc = v[m];
-          rc = __fmaf_rn(-cf[m][0], nb.w, rc);
-          rc = __fmaf_rn(-cf[m][1], nb.e, rc);
-          rc = __fmaf_rn(-cf[m][2], nb.s, rc);
-          rc = __fmaf_rn(-cf[m][3], nb.n, rc);
-          rc = __fmaf_rn(-cf[m][4], nb.b, rc);
-          rc = __fmaf_rn(-cf[m][5], nb.t, rc);
-          const float xt = __fmul_rn(rc, cf[m][6]);
-          const float e = E[c * HALF_CELLS + qd];
-          E[c * HALF_CELLS + qd] = __fmaf_rn(mom, __fsub_rn(e, xt), e);
+          double rc = (double)v[m];
+          rc = __fma_rn(-(double)cf[m][0], (double)nb.w, rc);
+          rc = __fma_rn(-(double)cf[m][1], (double)nb.e, rc);
+          rc = __fma_rn(-(double)cf[m][2], (double)nb.s, rc);
+          rc = __fma_rn(-(double)cf[m][3], (double)nb.n, rc);
+          rc = __fma_rn(-(double)cf[m][4], (double)nb.b, rc);
+          rc = __fma_rn(-(double)cf[m][5], (double)nb.t, rc);
+          const double xt = __dmul_rn(rc, (double)cf[m][6]);
+          const double e = (double)E[c * HALF_CELLS + qd];
+          E[c * HALF_CELLS + qd] = __double2float_rn(__fma_rn(mom, __dsub_rn(e, xt), e));
         }
         __syncthreads();
       }

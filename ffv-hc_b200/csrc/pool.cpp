@@ -115,7 +115,8 @@ ffvgpu_status ensure_solver(ffvgpu_pool* P) {
   return FFVGPU_OK;
 }
 
-ffvgpu_status reset_state(ffvgpu_pool* P, double eps, int count_max, double* hist) {
+ffvgpu_status reset_state(ffvgpu_pool* P, double eps, int count_max, double* hist,
+                          double drop = 0.0) {
   SolveState h;
   std::memset(&h, 0, sizeof(h));
   h.eps = eps;
@@ -123,6 +124,9 @@ ffvgpu_status reset_state(ffvgpu_pool* P, double eps, int count_max, double* his
   h.rr0 = 1.0;
   h.gamma = 1.0;  // FFVILS.h:841-842: alpha = 0, gamma = 1 before the first iteration
   h.hist = hist;
+  h.cycle = 1;
+  h.drop = drop;
+  h.next_restart = -1.0;
   CK(cudaMemcpyAsync(P->st, &h, sizeof(h), cudaMemcpyHostToDevice, P->stream));
   return FFVGPU_OK;
 }
@@ -867,7 +871,9 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
   ffvgpu_result R;
   std::memset(&R, 0, sizeof(R));
   if ((s = ensure_hist(P, N > 0 ? N : 1))) return s;
-  if ((s = reset_state(P, prm->epsilon, N, P->hist_d))) return s;
+  if (!(prm->restart_drop >= 0.0 && prm->restart_drop < 1.0))
+    return bad("restart_drop must lie in [0, 1)");
+  if ((s = reset_state(P, prm->epsilon, N, P->hist_d, prm->restart_drop))) return s;
   const KCtx C = P->ctx(P->bc_p);
   const int every = prm->check_every > 0 ? prm->check_every : 16;
   const bool poll = prm->epsilon > 0.0;
@@ -886,15 +892,15 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
     return FFVGPU_OK;
   }
   launch_calc_r(P->stream, C, x, P->gx, P->A, P->b, P->r, P->st);  // FFVILS.h:828
-  CK(cudaMemcpyAsync(P->r0, P->r, n * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
+  // r0 = r (FFVILS.h:830-833) is made by the first DOT(r, r0) of the loop
   launches++;
   bytes += interior_bytes(P, 10 + 2);
   const int K = prm->pre_count;
   CK(cudaEventRecord(P->ev2, P->stream));
   const int launches_before = launches;
   for (int c = 1; c <= N; ++c) {
-    launch_dot(P->stream, C, P->r, P->r0, P->partials, P->st, FIN_BI_RR1, c);  // rr1
-    launch_bicg_p(P->stream, C, P->r, P->p, P->q, c == 1 ? 1 : 0, P->st);
+    launch_dot_rr0(P->stream, C, P->r, P->r0, P->partials, P->st, FIN_BI_RR1, c);  // rr1
+    launch_bicg_p(P->stream, C, P->r, P->p, P->q, P->st);
     const double* pz = jacobi_pre(P, C, P->z, P->p, K, prm->omega, bytes, launches);
     launch_ax_dot_y(P->stream, C, pz, P->A, P->q, P->r0, P->partials, P->st, FIN_BI_QR0);
     launch_axpyz(P->stream, C, P->sv, P->q, P->r, P->st);

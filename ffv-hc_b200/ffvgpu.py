@@ -39,7 +39,7 @@ EXPORTS = [
     "ffvgpu_instance_admit_sphere", "ffvgpu_instance_upload", "ffvgpu_instance_download",
     "ffvgpu_instance_release", "ffvgpu_instance_blocks", "ffvgpu_pool_free_blocks",
     "ffvgpu_mixed_begin", "ffvgpu_mixed_advance", "ffvgpu_mixed_poll", "ffvgpu_instance_result",
-    "ffvgpu_assemble_sphere", "ffvgpu_instance_fill",
+    "ffvgpu_assemble_sphere", "ffvgpu_instance_fill", "ffvgpu_serve",
 ]
 
 
@@ -59,6 +59,7 @@ class IterParams(ctypes.Structure):
         ("omega", ctypes.c_double), ("count_max", ctypes.c_int32),
         ("epsilon", ctypes.c_double), ("pre_count", ctypes.c_int32),
         ("check_every", ctypes.c_int32), ("history", ctypes.c_void_p),
+        ("restart_drop", ctypes.c_double),
     ]
 
 
@@ -86,7 +87,12 @@ class MixedParams(ctypes.Structure):
         ("sweeps_per_exchange", ctypes.c_int32), ("count_max", ctypes.c_int32),
         ("epsilon", ctypes.c_double), ("check_every", ctypes.c_int32),
         ("history", ctypes.c_void_p), ("restart_drop", ctypes.c_double),
+        ("restart_growth", ctypes.c_double), ("restart_every", ctypes.c_int32),
     ]
+
+
+# Restart settings of the mixed form used by default (see ffvgpu_mixed_params).
+RESTART = dict(restart_drop=1e-3, restart_growth=0.0, restart_every=0)
 
 
 class BatchDesc(ctypes.Structure):
@@ -101,6 +107,18 @@ class SphereProblem(ctypes.Structure):
         ("grid", SphereParams), ("seed", ctypes.c_uint64), ("sigma", ctypes.c_double),
         ("rhof", ctypes.c_double), ("dt", ctypes.c_double),
         ("u_bc_type", (ctypes.c_int32 * 6) * 3), ("u_bc_value", (ctypes.c_double * 6) * 3),
+    ]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("arrival_s", ctypes.c_double), ("problem", SphereProblem)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [
+        ("admit_s", ctypes.c_double), ("finish_s", ctypes.c_double),
+        ("count", ctypes.c_int32), ("residual", ctypes.c_double),
+        ("status", ctypes.c_int32), ("blocks", ctypes.c_int32),
     ]
 
 
@@ -156,6 +174,8 @@ def lib():
         L.ffvgpu_instance_download.argtypes = [vp, i32, i32, vp, i32]
         L.ffvgpu_instance_release.argtypes = [vp, i32]
         L.ffvgpu_instance_fill.argtypes = [vp, i32, i32, dbl]
+        L.ffvgpu_serve.argtypes = [vp, MP, i32, ctypes.POINTER(Request), i32,
+                                   ctypes.POINTER(RequestResult)]
         L.ffvgpu_instance_blocks.argtypes = [vp, i32]
         L.ffvgpu_pool_free_blocks.argtypes = [vp, vp, vp]
         L.ffvgpu_mixed_begin.argtypes = [vp, i32, MP]
@@ -338,10 +358,11 @@ class Pool:
     def fold_bc(self):
         _check(lib().ffvgpu_fold_bc(self._h), "fold_bc")
 
-    def _solve(self, fn, what, omega, count_max, epsilon, pre_count, history, check_every):
+    def _solve(self, fn, what, omega, count_max, epsilon, pre_count, history, check_every,
+               restart_drop=0.0):
         hist = np.zeros(max(count_max, 1), np.float64) if history else None
         prm = IterParams(omega, count_max, epsilon, pre_count, check_every,
-                         hist.ctypes.data if history else None)
+                         hist.ctypes.data if history else None, restart_drop)
         res = Result()
         st = fn(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, what, allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -366,9 +387,9 @@ class Pool:
                            pre_count, history, check_every)
 
     def solve_bicgstab(self, omega=1.0, pre_count=2, count_max=1000, epsilon=1e-10,
-                       history=True, check_every=0):
+                       history=True, check_every=0, restart_drop=0.0):
         return self._solve(lib().ffvgpu_solve_bicgstab, "solve_bicgstab", omega, count_max,
-                           epsilon, pre_count, history, check_every)
+                           epsilon, pre_count, history, check_every, restart_drop)
 
     def set_stream(self, stream_handle):
         """Enqueue on a caller's CUDA stream (an int cudaStream_t, 0/None = own)."""
@@ -396,11 +417,13 @@ class Pool:
         _check(lib().ffvgpu_assemble_sphere(self._h, ctypes.byref(problem)), "assemble_sphere")
 
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-                    epsilon=1e-8, history=True, check_every=0, restart_drop=1e-3):
+                    epsilon=1e-8, history=True, check_every=0, restart_drop=None,
+                    restart_growth=None, restart_every=None):
         """Mixed-precision solve (FP64 BiCGSTAB, FP32 RB-SOR preconditioner)."""
         hist = np.zeros(max(count_max, 1), np.float64) if history else None
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
-                          hist.ctypes.data if history else None, restart_drop)
+                          hist.ctypes.data if history else None,
+                          *_restart(restart_drop, restart_growth, restart_every))
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -411,6 +434,12 @@ class Pool:
             n = res.count if 1 <= res.count <= count_max else (count_max if res.count > 0 else 0)
             out["history"] = hist[:n].copy()
         return out
+
+
+def _restart(drop, growth, every):
+    return (RESTART["restart_drop"] if drop is None else drop,
+            RESTART["restart_growth"] if growth is None else growth,
+            RESTART["restart_every"] if every is None else every)
 
 
 def sphere_problem(max_level, seed=1, sigma=0.01, dt=0.002, rhof=1.0, **grid_kw):
@@ -505,20 +534,40 @@ class Batch:
                "pool_set_stream")
 
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-                    epsilon=1e-8, check_every=0, restart_drop=1e-3):
+                    epsilon=1e-8, check_every=0, restart_drop=None, restart_growth=None,
+                    restart_every=None):
         """Solves every admitted instance; returns the first instance's result."""
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
-                          None, restart_drop)
+                          None, *_restart(restart_drop, restart_growth, restart_every))
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
         return dict(status=st, count=res.count, residual=res.residual, elapsed_ms=res.elapsed_ms,
                     kernel_launches=res.kernel_launches, bytes_moved=res.bytes_moved)
 
-    def begin(self, inst, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-              epsilon=1e-8, restart_drop=1e-3):
+    def serve(self, arrivals, problems, iterations_per_step=8, omega=1.5, sweeps=8,
+              sweeps_per_exchange=4, count_max=5000, epsilon=1e-8, restart_drop=None,
+              restart_growth=None, restart_every=None):
+        """Request loop (ffvgpu_serve): per request admit/finish times, iterations,
+        residual, status, blocks."""
+        n = len(problems)
+        req = (Request * n)()
+        for i, (t, p) in enumerate(zip(arrivals, problems)):
+            req[i].arrival_s = float(t)
+            req[i].problem = p
+        out = (RequestResult * n)()
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, 0, None,
-                          restart_drop)
+                          *_restart(restart_drop, restart_growth, restart_every))
+        _check(lib().ffvgpu_serve(self._h, ctypes.byref(prm), n, req, iterations_per_step, out),
+               "serve")
+        return [dict(arrival_s=float(arrivals[i]), admit_s=out[i].admit_s,
+                     finish_s=out[i].finish_s, count=out[i].count, residual=out[i].residual,
+                     status=out[i].status, blocks=out[i].blocks) for i in range(n)]
+
+    def begin(self, inst, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
+              epsilon=1e-8, restart_drop=None, restart_growth=None, restart_every=None):
+        prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, 0, None,
+                          *_restart(restart_drop, restart_growth, restart_every))
         _check(lib().ffvgpu_mixed_begin(self._h, inst, ctypes.byref(prm)), "mixed_begin")
 
     def advance(self, iterations):

@@ -103,6 +103,9 @@ typedef struct {
   int32_t check_every;   /* host polls convergence every this many iterations
                             (0 = default); does not change results */
   double* history;       /* optional host array [count_max]: residual per iteration */
+  double restart_drop;   /* BiCGSTAB only, no counterpart in the reference: restart the
+                            recurrence (r0 = r, p = r) each time the residual has fallen by
+                            this factor; 0 (the default) keeps the reference's recurrence */
 } ffvgpu_iter_params;
 
 typedef struct {
@@ -282,6 +285,9 @@ typedef struct {
   double* history;             /* optional host array [count_max]: residual per iteration */
   double restart_drop;         /* restart the recurrence (r0 = r, p = r) each time the
                                   residual has fallen by this factor; 0: never */
+  double restart_growth;       /* also restart when the residual exceeds this factor times
+                                  the cycle's smallest; 0: never */
+  int32_t restart_every;       /* also restart after this many iterations of a cycle; 0: never */
 } ffvgpu_mixed_params;
 
 /* Solves every admitted instance of the pool (a pool made from one grid is
@@ -365,6 +371,35 @@ ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* pool, int32_t* finished, int32_t ca
 /* history: optional host array receiving min(count, count_max) residuals. */
 ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* pool, int32_t instance,
                                      ffvgpu_result* res, double* history);
+
+/* ---- serving (no counterpart in the reference) ---------------------------
+ * A request loop with continuous batching on a batch pool: requests (sorted
+ * by arrival time, seconds from the start of the call) are admitted in
+ * arrival order as block ranges and instance slots free up -- one that does
+ * not fit waits while later, smaller ones may pass it -- and join the
+ * running solves at the next graph replay; every replay advances all running
+ * solves by iterations_per_step iterations; a solve that ends has its
+ * pressure copied to the host and its blocks released.  out[i] receives
+ * request i's admission and completion times (same clock), iterations,
+ * residual, status and block count.  On an error the pool may still hold
+ * admitted instances: destroy it. */
+typedef struct {
+  double arrival_s;
+  ffvgpu_sphere_problem problem;
+} ffvgpu_request;
+
+typedef struct {
+  double admit_s;
+  double finish_s;
+  int32_t count;
+  double residual;
+  int32_t status;
+  int32_t blocks;
+} ffvgpu_request_result;
+
+ffvgpu_status ffvgpu_serve(ffvgpu_pool* batch, const ffvgpu_mixed_params* prm, int32_t n,
+                           const ffvgpu_request* requests, int32_t iterations_per_step,
+                           ffvgpu_request_result* out);
 
 #ifdef __cplusplus
 }

@@ -1010,8 +1010,19 @@ int orc_cg(Oracle* O, double omega, int countPre, int countMax, double epsilon,
 }
 
 // FFVILS.h:793-974 BiCGSTAB (Jacobi-preconditioned).  Returns 0 ok, 2 NaN/Inf.
+int orc_bicgstab_restart(Oracle* O, double omega, int countPre, int countMax, double epsilon,
+                         double restart_drop, int* count, double* residual, double* hist);
+
 int orc_bicgstab(Oracle* O, double omega, int countPre, int countMax,
                  double epsilon, int* count, double* residual, double* hist) {
+  return orc_bicgstab_restart(O, omega, countPre, countMax, epsilon, 0.0, count, residual, hist);
+}
+
+// FFVILS::BiCGSTAB; restart_drop > 0 (no counterpart in the reference)
+// restarts the recurrence (r0 = r, p = r) each time the residual has fallen
+// by that factor since the last (re)start, as the GPU's restart option does.
+int orc_bicgstab_restart(Oracle* O, double omega, int countPre, int countMax, double epsilon,
+                         double restart_drop, int* count, double* residual, double* hist) {
   Oracle& R = *O;
   double bb = DOT(R, OF_B, OF_B);
   if (std::fabs(bb) < FLT_MIN) {
@@ -1022,6 +1033,8 @@ int orc_bicgstab(Oracle* O, double omega, int countPre, int countMax,
   CalcR(R, OF_R, OF_X, OF_B);
   COPY(R, OF_R0, OF_R);
   double rr0 = 1.0, alpha = 0.0, gamma = 1.0;
+  double next_restart = -1.0;
+  int cycle = 1;
   int c;
   for (c = 1; c <= countMax; ++c) {
     double rr1 = DOT(R, OF_R, OF_R0);
@@ -1030,7 +1043,12 @@ int orc_bicgstab(Oracle* O, double omega, int countPre, int countMax,
       c = 0;
       break;
     }
-    if (c == 1) {
+    if (c == 1 && restart_drop > 0.0) {
+      double r_init;
+      is_converged(r_init, rr1, bb, 0.0);
+      next_restart = r_init * restart_drop;
+    }
+    if (cycle == 1) {
       COPY(R, OF_P, OF_R);
     } else {
       double beta = rr1 / rr0 * alpha / gamma;
@@ -1062,6 +1080,15 @@ int orc_bicgstab(Oracle* O, double omega, int countPre, int countMax,
     }
     if (st == 1) break;
     rr0 = rr1;
+    ++cycle;
+    if (next_restart > 0.0 && *residual <= next_restart && c < countMax) {
+      next_restart = *residual * restart_drop;
+      COPY(R, OF_R0, OF_R);
+      rr0 = 1.0;
+      alpha = 0.0;
+      gamma = 1.0;
+      cycle = 1;
+    }
   }
   impose_bc_p(R, OF_X);
   *count = (c > countMax) ? countMax + 1 : c;
@@ -1074,9 +1101,10 @@ int orc_bicgstab(Oracle* O, double omega, int countPre, int countMax,
 // red-black SOR sweeps from zero, 'per' sweeps between guide exchanges.
 // Restates ffv-hc_b200/csrc/kernels_mixed.cu:
 //   coefficients aw..at = (float)A*, dinv = (float)(1.0 / Ap); v = (float)rhs;
-//   per cell of colour c (colour 0 first, rbgs_smoother's order of terms):
-//     rc = fmaf(-aw, eW, v) ... fmaf(-at, eT, rc); xt = rc * dinv;
-//     e = fmaf(-omega, e - xt, e)
+//   per cell of colour c (colour 0 first, rbgs_smoother's order of terms),
+//   on those FP32 values in double arithmetic, rounded to float when stored:
+//     rc = fma(-aw, eW, v) ... fma(-at, eT, rc); xt = rc * dinv;
+//     e = (float)fma(-omega, e - xt, e)
 //   guides of e: zero in the first group; later, the exchange of e (as
 //   double) with homogeneous Dirichlet outer faces, rounded to float.
 // The preconditioned vectors' guides come from the pressure-BC exchange
@@ -1147,16 +1175,16 @@ void mixed_precondition(Oracle& O, const Coef32& C, int fv, int fout, float omeg
               for (int i = 1; i <= n; ++i) {
                 if ((((i - 1) + (j - 1) + (k - 1)) & 1) != c) continue;
                 const long m = IDX(G, i, j, k);
-                float rc = vb[m];
-                rc = std::fmaf(-C.a[0][o + m], eb[m - 1], rc);
-                rc = std::fmaf(-C.a[1][o + m], eb[m + 1], rc);
-                rc = std::fmaf(-C.a[2][o + m], eb[m - sy], rc);
-                rc = std::fmaf(-C.a[3][o + m], eb[m + sy], rc);
-                rc = std::fmaf(-C.a[4][o + m], eb[m - sz], rc);
-                rc = std::fmaf(-C.a[5][o + m], eb[m + sz], rc);
-                const float xt = rc * C.a[6][o + m];
-                const float ev = eb[m];
-                eb[m] = std::fmaf(-omega, ev - xt, ev);
+                double rc = (double)vb[m];
+                rc = std::fma(-(double)C.a[0][o + m], (double)eb[m - 1], rc);
+                rc = std::fma(-(double)C.a[1][o + m], (double)eb[m + 1], rc);
+                rc = std::fma(-(double)C.a[2][o + m], (double)eb[m - sy], rc);
+                rc = std::fma(-(double)C.a[3][o + m], (double)eb[m + sy], rc);
+                rc = std::fma(-(double)C.a[4][o + m], (double)eb[m - sz], rc);
+                rc = std::fma(-(double)C.a[5][o + m], (double)eb[m + sz], rc);
+                const double xt = rc * (double)C.a[6][o + m];
+                const double ev = (double)eb[m];
+                eb[m] = (float)std::fma(-(double)omega, ev - xt, ev);
               }
         }
       }
@@ -1175,7 +1203,8 @@ void mixed_precondition(Oracle& O, const Coef32& C, int fv, int fout, float omeg
 }  // namespace
 
 int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double epsilon,
-              double restart_drop, int* count, double* residual, double* hist) {
+              double restart_drop, double restart_growth, int restart_every, int* count,
+              double* residual, double* hist) {
   Oracle& R = *O;
   if (countMax <= 0) {
     *count = 1;
@@ -1196,7 +1225,7 @@ int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double
   double rr0 = 1.0, alpha = 0.0, gamma = 1.0;
   // restarts: when the residual has dropped by restart_drop since the last
   // (re)start, the recurrence starts again from the current r (r0 = r, p = r)
-  double next_restart = -1.0;
+  double next_restart = -1.0, best = 0.0;
   int cycle = 1;
   int c;
   for (c = 1; c <= countMax; ++c) {
@@ -1206,10 +1235,11 @@ int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double
       c = 0;
       break;
     }
-    if (c == 1 && restart_drop > 0.0) {
+    if (c == 1) {
       double r_init;
       is_converged(r_init, rr1, bb, 0.0);
-      next_restart = r_init * restart_drop;
+      if (restart_drop > 0.0) next_restart = r_init * restart_drop;
+      best = r_init;
     }
     if (cycle == 1) {
       COPY(R, OF_P, OF_R);
@@ -1242,8 +1272,13 @@ int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double
     if (st == 1) break;
     rr0 = rr1;
     ++cycle;
-    if (next_restart > 0.0 && *residual <= next_restart && c < countMax) {
-      next_restart = *residual * restart_drop;
+    const bool dropped = next_restart > 0.0 && *residual <= next_restart;
+    const bool grew = restart_growth > 0.0 && *residual > restart_growth * best;
+    const bool aged = restart_every > 0 && cycle > restart_every;
+    if (*residual < best) best = *residual;
+    if ((dropped || grew || aged) && c < countMax) {
+      if (restart_drop > 0.0) next_restart = *residual * restart_drop;
+      best = *residual;
       COPY(R, OF_R0, OF_R);
       rr0 = 1.0;
       alpha = 0.0;

@@ -66,7 +66,8 @@ def lib():
             fn.argtypes = [vp, dbl, i32, dbl, vp, vp, vp]
         for fn in (L.orc_cg, L.orc_bicgstab):
             fn.argtypes = [vp, dbl, i32, i32, dbl, vp, vp, vp]
-        L.orc_mixed.argtypes = [vp, dbl, i32, i32, i32, dbl, dbl, vp, vp, vp]
+        L.orc_bicgstab_restart.argtypes = [vp, dbl, i32, i32, dbl, dbl, vp, vp, vp]
+        L.orc_mixed.argtypes = [vp, dbl, i32, i32, i32, dbl, dbl, dbl, i32, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -176,13 +177,22 @@ class Oracle:
                                           float(epsilon)), count_max)
 
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-                    epsilon=1e-8, restart_drop=1e-3):
+                    epsilon=1e-8, restart_drop=1e-3, restart_growth=0.0, restart_every=0):
         """Mixed-precision form: BiCGSTAB with FP32 RB-SOR preconditioning."""
         return self._solve(lib().orc_mixed, (float(omega), int(sweeps), int(sweeps_per_exchange),
-                                             int(count_max), float(epsilon),
-                                             float(restart_drop)), count_max)
+                                             int(count_max), float(epsilon), float(restart_drop),
+                                             float(restart_growth), int(restart_every)),
+                           count_max)
 
-    def solve_bicgstab(self, omega=1.0, pre_count=2, count_max=1000, epsilon=1e-10):
+    def solve_bicgstab(self, omega=1.0, pre_count=2, count_max=1000, epsilon=1e-10,
+                       restart_drop=0.0):
+        if restart_drop > 0.0:
+            return self._solve(lib().orc_bicgstab_restart,
+                               (float(omega), int(pre_count), int(count_max), float(epsilon),
+                                float(restart_drop)), count_max)
+        return self._solve_plain_bicgstab(omega, pre_count, count_max, epsilon)
+
+    def _solve_plain_bicgstab(self, omega, pre_count, count_max, epsilon):
         return self._solve(lib().orc_bicgstab, (float(omega), int(pre_count), int(count_max),
                                                 float(epsilon)), count_max)
 

@@ -199,3 +199,20 @@ def test_batch_refuses_pool_wide_calls_and_full_capacity():
     B.release(i)
     assert B.admit_sphere(sphere(2, 4)) is not None
     B.close()
+
+
+def test_serve_continuous_batching_results_equal_alone():
+    """ffvgpu_serve: requests arriving while others run are admitted as blocks
+    free up; each result equals the same request solved alone."""
+    cases = CASES + [(1, 17, dict(center=(5.0, -1.0, 1.0), radius=0.6))]
+    alone = [solve_alone(L, s, 60, 1e-8, kw)[0] for (L, s, kw) in cases]
+    B = ffvgpu.Batch(300, 4)            # room for two of these requests at a time
+    arrivals = [0.0, 0.0, 0.002, 0.004]
+    probs = [sphere(L, s, **kw) for (L, s, kw) in cases]
+    out = B.serve(arrivals, probs, iterations_per_step=4, count_max=60)
+    for o, ra in zip(out, alone):
+        assert o["finish_s"] >= o["admit_s"] >= o["arrival_s"] - 1e-9
+        assert o["count"] == ra["count"]
+        assert o["residual"] == ra["residual"]
+    assert B.free_blocks()[0] == 300
+    B.close()

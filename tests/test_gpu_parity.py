@@ -255,6 +255,22 @@ def test_bicgstab_solve_bitwise(level, radius, count, eps):
     P.close()
 
 
+@pytest.mark.parametrize("level,drop,count,eps", [(2, 1e-3, 300, 1e-10), (3, 1e-2, 40, 0.0)])
+def test_bicgstab_with_restarts_bitwise(level, drop, count, eps):
+    """The FP64 BiCGSTAB's restart option (no counterpart in the reference):
+    the same restarts, iterations and bits as the oracle's."""
+    g, inp, O = problem(level, threads=THREADS)
+    P = device_problem(g, inp)
+    P.fill("X", 0.0)
+    O.field("X")[...] = 0.0
+    ro = O.solve_bicgstab(1.0, 2, count, eps, restart_drop=drop)
+    rg = P.solve_bicgstab(1.0, 2, count, eps, restart_drop=drop)
+    assert rg["count"] == ro["count"], (rg["count"], ro["count"])
+    assert_bitwise(rg["history"], ro["history"], "residual history")
+    assert_bitwise(interior(P.download("X", VC)), interior(O.field("X")), "pressure")
+    P.close()
+
+
 def test_bicgstab_after_rbsor_and_edge_cases():
     g, inp, O = problem(1, threads=THREADS)
     P = device_problem(g, inp)
