@@ -310,6 +310,9 @@ __device__ __forceinline__ void finalize(SolveState* st, double total, int fin, 
     case FIN_BI_TT:
       st->gamma = st->ts / total;
       break;
+    case FIN_FA_SHIFT:
+      st->alpha = -total / st->scale;
+      break;
   }
 }
 

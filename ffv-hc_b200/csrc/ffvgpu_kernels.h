@@ -44,6 +44,10 @@ void launch_ax_dot_y(cudaStream_t s, const KCtx& C, const double* p, const doubl
 // p = r on the first iteration of a cycle (st->cycle == 1), else the update.
 void launch_bicg_p(cudaStream_t s, const KCtx& C, const double* r, double* p, const double* q,
                    SolveState* st);
+// Sum of x over the interior (finaliser fin); x += st->alpha.
+void launch_sum(cudaStream_t s, const KCtx& C, const double* x, double* partials, SolveState* st,
+                int fin);
+void launch_shift(cudaStream_t s, const KCtx& C, double* x, SolveState* st);
 // r.r0 (setting r0 = r first on the first iteration of a cycle).
 void launch_dot_rr0(cudaStream_t s, const KCtx& C, const double* r, double* r0, double* partials,
                     SolveState* st, int fin, int iter);

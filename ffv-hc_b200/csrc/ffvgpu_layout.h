@@ -82,6 +82,7 @@ struct SolveState {
   double next_restart;  // mixed form: residual at which the next restart happens (< 0: none)
   double best;       // mixed form: smallest residual of the current cycle
   double growth;     // mixed form: restart when the residual exceeds growth * best (0: never)
+  double scale;      // RBGS_WithFixedAverage: the cell count the sum is divided by
   int32_t max_cycle; // mixed form: restart after this many iterations of a cycle (0: never)
   int32_t pad2_;
 };
@@ -117,6 +118,7 @@ enum Fin : int {
   FIN_BI_TS,      // BiCGSTAB t_.s (FFVILS.h:923-929)
   FIN_BI_TT,      // BiCGSTAB gamma = t_s / (t_.t_) (FFVILS.h:930-936)
   FIN_BI_RR,      // BiCGSTAB residual of iteration 'iter' (FFVILS.h:952-960), optional restart
+  FIN_FA_SHIFT,   // RBGS_WithFixedAverage: alpha = -sum(x) / scale (FFVILS.h:636-639)
   // mixed form, per instance (two sums where noted)
   FIN_MX_INIT,    // b.b and r.r0: early exits of FFVILS.h:822-826 and 847-851
   FIN_MX_ALPHA,   // alpha = rr1 / (q.r0)

@@ -379,6 +379,36 @@ dot_rr0_kernel(const double* __restrict__ r, double* __restrict__ r0, double* __
   reduce_finalize(acc, partials, st, fin, iter);
 }
 
+// LocalScalar3D::CalcSum (LocalScalar3D.h:130-157, sf3d_calc_sum,
+// src/CGMfuncs/bsf3d.f90:35-67): the sum of x over all interior cells.
+__global__ void __launch_bounds__(THREADS)
+sum_kernel(const double* __restrict__ x, double* __restrict__ partials, SolveState* st, int fin) {
+  if (solve_done(st)) return;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+#pragma unroll 4
+    for (int m = 0; m < 8; ++m)
+      acc[c][m & 1] += __ldg(x + base + c * HALF_CELLS + threadIdx.x + THREADS * m);
+  }
+  reduce_finalize(acc, partials, st, fin, 0);
+}
+
+// LocalScalar3D::ShiftByA (LocalScalar3D.h:159-178, adda, blas.f90:162-193):
+// x = x + a on the interior with a = st->alpha.
+__global__ void __launch_bounds__(THREADS)
+shift_kernel(double* __restrict__ x, SolveState* st) {
+  if (solve_done(st)) return;
+  const double a = st->alpha;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+#pragma unroll 4
+  for (int m = 0; m < 16; ++m) {
+    const size_t s = base + threadIdx.x + THREADS * m;
+    x[s] = x[s] + a;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Exchange into a stored guide layer, layout conversion and set-up kernels.
 // ---------------------------------------------------------------------------
@@ -662,6 +692,13 @@ void launch_bicg_p(cudaStream_t s, const KCtx& C, const double* r, double* p, co
 void launch_axpyz(cudaStream_t s, const KCtx& C, double* z, const double* x, const double* y,
                   SolveState* st) {
   axpyz_kernel<<<C.nb, THREADS, 0, s>>>(z, x, y, st);
+}
+void launch_sum(cudaStream_t s, const KCtx& C, const double* x, double* partials, SolveState* st,
+                int fin) {
+  sum_kernel<<<C.nb, THREADS, 0, s>>>(x, partials, st, fin);
+}
+void launch_shift(cudaStream_t s, const KCtx& C, double* x, SolveState* st) {
+  shift_kernel<<<C.nb, THREADS, 0, s>>>(x, st);
 }
 void launch_dot_rr0(cudaStream_t s, const KCtx& C, const double* r, double* r0, double* partials,
                     SolveState* st, int fin, int iter) {

@@ -720,6 +720,88 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   return solve_status(h, prm, N, R.count);
 }
 
+// FFVILS::RBGS_WithFixedAverage (src/FFV/FFVILS.h:596-659): each iteration an
+// RB sweep (stored guides the first time, the in-kernel exchange after), the
+// shift x += -sum(x)/ncells (CalcSum / ShiftByA, LocalScalar3D.h:130-178,
+// then the exchange, made by the next kernel's gathers), and the residual of
+// the shifted x.  The reference's xave argument is unused by the reference.
+ffvgpu_status ffvgpu_solve_rbgs_fixed_average(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
+                                              int64_t ncells, ffvgpu_result* res) {
+  if (!P || !prm) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
+  if (ncells <= 0) return bad("ncells must be positive");
+  cudaSetDevice(P->device);
+  ffvgpu_status s;
+  if ((s = require_system(P))) return s;
+  const int N = prm->count_max;
+  ffvgpu_result R;
+  std::memset(&R, 0, sizeof(R));
+  if (N <= 0) {
+    R.count = 1;
+    if (res) *res = R;
+    return FFVGPU_OK;
+  }
+  if ((s = ensure_hist(P, N)) || (s = ensure_stream(P))) return s;
+  SolveState h0;
+  std::memset(&h0, 0, sizeof(h0));
+  h0.eps = prm->epsilon;
+  h0.count_max = N;
+  h0.rr0 = 1.0;
+  h0.gamma = 1.0;
+  h0.hist = P->hist_d;
+  h0.scale = (double)ncells;
+  CK(cudaMemcpyAsync(P->st, &h0, sizeof(h0), cudaMemcpyHostToDevice, P->stream));
+  const KCtx C = P->ctx(P->bc_p);
+  const int every = prm->check_every > 0 ? prm->check_every : 32;
+  const bool poll = prm->epsilon > 0.0;
+  CK(cudaEventRecord(P->ev0, P->stream));
+  launch_dot(P->stream, C, P->b, P->b, P->partials, P->st, FIN_BB, 0);
+  int launches = 1;
+  int64_t bytes = interior_bytes(P, 2);
+  const int c0 = P->xcur;
+  int cur = c0;
+  for (int n = 1; n <= N; ++n) {
+    // once the solve has stopped these kernels return at entry: the iterate
+    // kept is the one of the stopping iteration (below)
+    launch_rbgs(P->stream, C, false, true, P->x[cur], P->x[1 - cur], P->coef,
+                n == 1 ? P->gx : nullptr, prm->omega, P->partials, P->st, FIN_STORE, n);
+    cur = 1 - cur;
+    launch_sum(P->stream, C, P->x[cur], P->partials, P->st, FIN_FA_SHIFT);
+    launch_shift(P->stream, C, P->x[cur], P->st);
+    launch_rbgs(P->stream, C, true, false, P->x[cur], nullptr, P->coef, nullptr, prm->omega,
+                P->partials, P->st, FIN_RBGS, n);
+    launches += 4;
+    bytes += interior_bytes(P, 10 + 1 + 2 + 9);
+    if (poll && (n % every) == 0) {
+      bool done = false;
+      if ((s = poll_done(P, &done))) return s;
+      if (done) break;
+    }
+  }
+  CK(cudaEventRecord(P->ev1, P->stream));
+  CK(cudaGetLastError());
+  SolveState h;
+  if ((s = read_state(P, &h))) return s;
+  const int kept = (h.count >= 1 && h.count <= N) ? h.count : N;
+  P->xcur = (c0 + kept) & 1;
+  launch_exchange(P->stream, C, P->x[P->xcur], P->gx);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(P->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, P->ev0, P->ev1);
+  R.count = h.count;
+  R.residual = h.residual;
+  R.elapsed_ms = ms;
+  R.bytes_moved = bytes;
+  R.kernel_launches = launches + 1;
+  if (prm->history) {
+    const int nh = (h.count >= 1 && h.count <= N) ? h.count : N;
+    CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+  }
+  if (res) *res = R;
+  return solve_status(h, prm, N, R.count);
+}
+
 // FFVILS::CG (src/FFV/FFVILS.h:661-791) with Jacobi_PreConditioner
 // (FFVILS.h:469-492).  Guide cells of r are never read by a stencil in the
 // reference's CG, so its exchanges of r are value-neutral and not run; those

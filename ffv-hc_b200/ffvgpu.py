@@ -40,6 +40,7 @@ EXPORTS = [
     "ffvgpu_instance_release", "ffvgpu_instance_blocks", "ffvgpu_pool_free_blocks",
     "ffvgpu_mixed_begin", "ffvgpu_mixed_advance", "ffvgpu_mixed_poll", "ffvgpu_instance_result",
     "ffvgpu_assemble_sphere", "ffvgpu_instance_fill", "ffvgpu_serve",
+    "ffvgpu_solve_rbgs_fixed_average",
 ]
 
 
@@ -153,6 +154,8 @@ def lib():
         L.ffvgpu_solve_rbgs.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
         L.ffvgpu_solve_cg.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
         L.ffvgpu_solve_bicgstab.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
+        L.ffvgpu_solve_rbgs_fixed_average.argtypes = [vp, ctypes.POINTER(IterParams),
+                                                      ctypes.c_int64, ctypes.POINTER(Result)]
         L.ffvgpu_rbgs_sweep.argtypes = [vp, dbl]
         L.ffvgpu_calc_r2.argtypes = [vp, ctypes.POINTER(dbl)]
         L.ffvgpu_dot.argtypes = [vp, i32, i32, ctypes.POINTER(dbl)]
@@ -380,6 +383,22 @@ class Pool:
     def solve_rbgs(self, omega=1.5, count_max=200, epsilon=0.0, history=True, check_every=0):
         return self._solve(lib().ffvgpu_solve_rbgs, "solve_rbgs", omega, count_max, epsilon, 0,
                            history, check_every)
+
+    def solve_rbgs_fixed_average(self, omega=1.0, ncells=None, count_max=200, epsilon=0.0,
+                                 history=True, check_every=0):
+        n = self.nb * 4096 if ncells is None else ncells
+        hist = np.zeros(max(count_max, 1), np.float64) if history else None
+        prm = IterParams(omega, count_max, epsilon, 0, check_every,
+                         hist.ctypes.data if history else None, 0.0)
+        res = Result()
+        st = lib().ffvgpu_solve_rbgs_fixed_average(self._h, ctypes.byref(prm), n,
+                                                   ctypes.byref(res))
+        _check(st, "solve_rbgs_fixed_average", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
+        out = dict(status=st, count=res.count, residual=res.residual, elapsed_ms=res.elapsed_ms)
+        if history:
+            nh = res.count if 1 <= res.count <= count_max else count_max
+            out["history"] = hist[:nh].copy()
+        return out
 
     def solve_cg(self, omega=1.0, pre_count=2, count_max=10000, epsilon=1e-10, history=True,
                  check_every=0):

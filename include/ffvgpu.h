@@ -181,6 +181,15 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* pool, const ffvgpu_iter_params* prm,
  * real field, guide cells included, set to value. */
 ffvgpu_status ffvgpu_fill(ffvgpu_pool* pool, ffvgpu_field field, double value);
 
+/* FFVILS::RBGS_WithFixedAverage (src/FFV/FFVILS.h:596-659), the pressure
+ * solver FFV uses for all-Neumann problems: each iteration an RB sweep, the
+ * shift x += -sum(x)/ncells (LocalScalar3D::CalcSum / ShiftByA) and the
+ * residual of the shifted x.  ncells: FFV passes numTotalCells, every
+ * interior cell of every leaf block (Solver.cpp:1486-1490, 5601).  The
+ * reference's xave argument is unused there and has no counterpart here. */
+ffvgpu_status ffvgpu_solve_rbgs_fixed_average(ffvgpu_pool* pool, const ffvgpu_iter_params* prm,
+                                              int64_t ncells, ffvgpu_result* res);
+
 /* Jacobi-preconditioned BiCGSTAB on FIELD_X: FFVILS::BiCGSTAB
  * (src/FFV/FFVILS.h:793-974), the reference's default pressure solver
  * (src/FFV/Solver.cpp:5620-5676). */

@@ -623,6 +623,38 @@ double DOT(Oracle& O, int fx, int fy) {
   return canonical_blocks(part);
 }
 
+// LocalScalar3D.h:130-157 CalcSum: per block sf3d_calc_sum (bsf3d.f90:35-67,
+// serial in i, j, k), blocks summed serially in block order (no OpenMP there).
+double SUM(Oracle& O, int fx) {
+  Grid& G = O.G;
+  const int n = G.n;
+  if (O.red_mode == RED_REFERENCE) {
+    double sum_l = 0.0;
+    for (int bi = 0; bi < G.nb; ++bi) {
+      const double* x = O.F(fx, bi);
+      double dsum = 0.0;
+      for (int k = 1; k <= n; ++k)
+        for (int j = 1; j <= n; ++j)
+          for (int i = 1; i <= n; ++i) dsum = dsum + x[IDX(G, i, j, k)];
+      sum_l += dsum;
+    }
+    return sum_l;
+  }
+  std::vector<double> part(G.nb);
+#pragma omp parallel for num_threads(O.nthreads) schedule(static)
+  for (int bi = 0; bi < G.nb; ++bi) {
+    const double* x = O.F(fx, bi);
+    double v[4096];
+    for (int s = 0; s < 4096; ++s) {
+      int i, j, k;
+      cell_of_storage(s, i, j, k);
+      v[s] = x[IDX(G, i + 1, j + 1, k + 1)];
+    }
+    part[bi] = canonical_block(v);
+  }
+  return canonical_blocks(part);
+}
+
 // FFVILS.h:247-296 CalcR2
 double CalcR2(Oracle& O, int fx) {
   Grid& G = O.G;
@@ -1012,6 +1044,39 @@ int orc_cg(Oracle* O, double omega, int countPre, int countMax, double epsilon,
 // FFVILS.h:793-974 BiCGSTAB (Jacobi-preconditioned).  Returns 0 ok, 2 NaN/Inf.
 int orc_bicgstab_restart(Oracle* O, double omega, int countPre, int countMax, double epsilon,
                          double restart_drop, int* count, double* residual, double* hist);
+
+// FFVILS.h:596-659 RBGS_WithFixedAverage (the reference's xave is unused).
+int orc_rbgs_fixed_average(Oracle* O, double omega, long ncells, int countMax, double epsilon,
+                           int* count, double* residual, double* hist) {
+  Oracle& R = *O;
+  const double bb = DOT(R, OF_B, OF_B);
+  int c;
+  for (c = 1; c <= countMax; ++c) {
+    RBGS_Smoother(R, OF_X, omega);
+    const double sum_x1 = SUM(R, OF_X);
+    const double a = -sum_x1 / (double)ncells;
+    for (int bi = 0; bi < R.G.nb; ++bi) {  // adda, blas.f90:162-193
+      double* x = R.F(OF_X, bi);
+      for (int k = 1; k <= R.G.n; ++k)
+        for (int j = 1; j <= R.G.n; ++j)
+          for (int i = 1; i <= R.G.n; ++i) {
+            const long m = IDX(R.G, i, j, k);
+            x[m] = x[m] + a;
+          }
+    }
+    impose_bc_p(R, OF_X);
+    const double rr = CalcR2(R, OF_X);
+    const int st = is_converged(*residual, rr, bb, epsilon);
+    if (hist) hist[c - 1] = *residual;
+    if (st < 0) {
+      *count = c;
+      return 2;
+    }
+    if (st == 1) break;
+  }
+  *count = (c > countMax) ? countMax + 1 : c;
+  return 0;
+}
 
 int orc_bicgstab(Oracle* O, double omega, int countPre, int countMax,
                  double epsilon, int* count, double* residual, double* hist) {

@@ -66,6 +66,7 @@ def lib():
             fn.argtypes = [vp, dbl, i32, dbl, vp, vp, vp]
         for fn in (L.orc_cg, L.orc_bicgstab):
             fn.argtypes = [vp, dbl, i32, i32, dbl, vp, vp, vp]
+        L.orc_rbgs_fixed_average.argtypes = [vp, dbl, ctypes.c_long, i32, dbl, vp, vp, vp]
         L.orc_bicgstab_restart.argtypes = [vp, dbl, i32, i32, dbl, dbl, vp, vp, vp]
         L.orc_mixed.argtypes = [vp, dbl, i32, i32, i32, dbl, dbl, dbl, i32, vp, vp, vp]
         _lib = L
@@ -171,6 +172,11 @@ class Oracle:
 
     def solve_rbgs(self, omega=1.5, count_max=200, epsilon=0.0):
         return self._solve(lib().orc_rbgs, (float(omega), int(count_max), float(epsilon)), count_max)
+
+    def solve_rbgs_fixed_average(self, omega=1.0, ncells=None, count_max=200, epsilon=0.0):
+        n = self.nb * 4096 if ncells is None else ncells
+        return self._solve(lib().orc_rbgs_fixed_average, (float(omega), int(n), int(count_max),
+                                                          float(epsilon)), count_max)
 
     def solve_cg(self, omega=1.0, pre_count=2, count_max=10000, epsilon=1e-10):
         return self._solve(lib().orc_cg, (float(omega), int(pre_count), int(count_max),

@@ -288,3 +288,32 @@ def test_bicgstab_after_rbsor_and_edge_cases():
     r = P.solve_bicgstab(1.0, 0, 5, 1e-10)
     assert r["status"] == ffvgpu.NAN_DETECTED and r["count"] == 1
     P.close()
+
+
+ALL_NEUMANN = ((ffvgpu.BC_NEUMANN,) * 6, (0.0,) * 6)
+
+
+@pytest.mark.parametrize("level,omega,count,eps", [(1, 1.0, 40, 0.0), (2, 1.2, 60, 0.0),
+                                                   (0, 1.0, 400, 2e-2)])
+def test_rbgs_fixed_average_bitwise(level, omega, count, eps):
+    """FFVILS::RBGS_WithFixedAverage on an all-Neumann problem: every
+    iteration's residual, the pressure and its guide layers bit-equal."""
+    g, inp, O = problem(level, threads=THREADS, bc_type=ALL_NEUMANN[0], bc_value=ALL_NEUMANN[1])
+    P = device_problem(g, inp, bc_type=ALL_NEUMANN[0], bc_value=ALL_NEUMANN[1])
+    x0 = np.zeros((g.nb, 20, 20, 20))
+    O.field("X")[...] = x0
+    P.upload("X", x0, VC)
+    ro = O.solve_rbgs_fixed_average(omega, None, count, eps)
+    rg = P.solve_rbgs_fixed_average(omega, None, count, eps, check_every=7)
+    assert rg["count"] == ro["count"], (rg["count"], ro["count"])
+    assert_bitwise(rg["history"], ro["history"], "residual history")
+    got = P.download("X", VC)
+    assert_bitwise(interior(got), interior(O.field("X")), "pressure")
+    gg, rgd = fo.face_guides(got, VC, 1), fo.face_guides(O.field("X"), VC, 1)
+    for f in range(6):
+        assert_bitwise(gg[f], rgd[f], f"guides face {f}")
+    if eps > 0:
+        assert 1 < ro["count"] <= count
+    # the shifted pressure has zero mean up to rounding
+    assert abs(interior(got).mean()) < 1e-12 * (np.abs(interior(got)).max() + 1.0)
+    P.close()
