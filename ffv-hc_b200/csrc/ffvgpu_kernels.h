@@ -74,6 +74,11 @@ void launch_assemble(cudaStream_t s, const KCtx& C, const double* ux, const doub
                      const double* cut, const uint8_t* flags, double* A, double* b,
                      double* vface, double rhof, double dt, size_t field_stride);
 void launch_fold_bc(cudaStream_t s, const KCtx& C, double* A, double* b);
+// bcut_remove_p (corr false) or bcut_corr_u (corr true) on every block.
+void launch_projection(cudaStream_t s, const KCtx& C, bool corr, const double* p,
+                       const double* gp, const double* cut, const uint8_t* flags, double* ux,
+                       double* uy, double* uz, double* vface, double* lapp, double rhof,
+                       double dt, size_t field_stride);
 void launch_fill(cudaStream_t s, int nb, double* x, size_t stride, double* g, double value);
 
 // Sets the message ffvgpu_last_error() returns on this thread.

@@ -592,6 +592,76 @@ assemble_kernel(KCtx C, const double* __restrict__ ux, const double* __restrict_
   }
 }
 
+// bcut_remove_p (bcut.f90:3879-4061, CORR false) and bcut_corr_u
+// (bcut.f90:4063-4297, CORR true), one cell per thread-iteration, p staged
+// with its stored guide layer.  Each expression in the reference's order.
+template <bool CORR>
+__global__ void __launch_bounds__(THREADS)
+projection_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ gp,
+                  const double* __restrict__ cut, const uint8_t* __restrict__ flags,
+                  double* __restrict__ ux, double* __restrict__ uy, double* __restrict__ uz,
+                  double* __restrict__ vface, double* __restrict__ lapp, double rhof, double dt,
+                  size_t fs) {
+  __shared__ double xs[TILE];
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  stage_tile(xs, p, blk, C, gp);
+  __syncthreads();
+  const double dx = C.dx[blk];
+  for (int m = 0; m < 16; ++m) {
+    const int s = tid + THREADS * m;
+    int i, j, k;
+    cell_of(s, i, j, k);
+    const int t = tix(i, j, k);
+    const size_t gs = (size_t)blk * BLOCK_CELLS + s;
+    const double r0 = 1.0 / rhof, r1 = 1.0 / rhof, r2 = 1.0 / rhof;
+    const double r3 = 1.0 / rhof, r4 = 1.0 / rhof, r5 = 1.0 / rhof;
+    double dpx0 = (xs[t] - xs[t - 1]) / dx;
+    double dpx1 = (xs[t + 1] - xs[t]) / dx;
+    double dpy2 = (xs[t] - xs[t - TW]) / dx;
+    double dpy3 = (xs[t + TW] - xs[t]) / dx;
+    double dpz4 = (xs[t] - xs[t - TP]) / dx;
+    double dpz5 = (xs[t + TP] - xs[t]) / dx;
+    double rdpx0 = r0 * dpx0, rdpx1 = r1 * dpx1, rdpy2 = r2 * dpy2;
+    double rdpy3 = r3 * dpy3, rdpz4 = r4 * dpz4, rdpz5 = r5 * dpz5;
+    const double d0 = __ldg(cut + gs), d1 = __ldg(cut + fs + gs), d2 = __ldg(cut + 2 * fs + gs);
+    const double d3 = __ldg(cut + 3 * fs + gs), d4 = __ldg(cut + 4 * fs + gs);
+    const double d5 = __ldg(cut + 5 * fs + gs);
+    const unsigned fl = flags[gs];
+    const bool c0 = fl & 1, c1 = fl & 2, c2 = fl & 4, c3 = fl & 8, c4 = fl & 16, c5 = fl & 32;
+    const bool fluid = fl & 128;
+    if (c0) { rdpx0 = rdpx1 * (d0 - 0.5) / (d0 + 0.5); dpx0 = dpx1 * (d0 - 0.5) / (d0 + 0.5); }
+    if (c1) { rdpx1 = rdpx0 * (d1 - 0.5) / (d1 + 0.5); dpx1 = dpx0 * (d1 - 0.5) / (d1 + 0.5); }
+    if (c2) { rdpy2 = rdpy3 * (d2 - 0.5) / (d2 + 0.5); dpy2 = dpy3 * (d2 - 0.5) / (d2 + 0.5); }
+    if (c3) { rdpy3 = rdpy2 * (d3 - 0.5) / (d3 + 0.5); dpy3 = dpy2 * (d3 - 0.5) / (d3 + 0.5); }
+    if (c4) { rdpz4 = rdpz5 * (d4 - 0.5) / (d4 + 0.5); dpz4 = dpz5 * (d4 - 0.5) / (d4 + 0.5); }
+    if (c5) { rdpz5 = rdpz4 * (d5 - 0.5) / (d5 + 0.5); dpz5 = dpz4 * (d5 - 0.5) / (d5 + 0.5); }
+    if (c0 && c1) { rdpx0 = 0.0; rdpx1 = 0.0; }
+    if (c2 && c3) { rdpy2 = 0.0; rdpy3 = 0.0; }
+    if (c4 && c5) { rdpz4 = 0.0; rdpz5 = 0.0; }
+    const double rdpx = 0.5 * (rdpx0 + rdpx1);
+    const double rdpy = 0.5 * (rdpy2 + rdpy3);
+    const double rdpz = 0.5 * (rdpz4 + rdpz5);
+    if (!CORR) {
+      ux[gs] = fluid ? ux[gs] + rdpx * dt : 0.0;
+      uy[gs] = fluid ? uy[gs] + rdpy * dt : 0.0;
+      uz[gs] = fluid ? uz[gs] + rdpz * dt : 0.0;
+    } else {
+      ux[gs] = fluid ? ux[gs] - rdpx * dt : 0.0;
+      uy[gs] = fluid ? uy[gs] - rdpy * dt : 0.0;
+      uz[gs] = fluid ? uz[gs] - rdpz * dt : 0.0;
+      vface[gs] = fluid ? vface[gs] - rdpx0 * dt : 0.0;
+      vface[fs + gs] = fluid ? vface[fs + gs] - rdpx1 * dt : 0.0;
+      vface[2 * fs + gs] = fluid ? vface[2 * fs + gs] - rdpy2 * dt : 0.0;
+      vface[3 * fs + gs] = fluid ? vface[3 * fs + gs] - rdpy3 * dt : 0.0;
+      vface[4 * fs + gs] = fluid ? vface[4 * fs + gs] - rdpz4 * dt : 0.0;
+      vface[5 * fs + gs] = fluid ? vface[5 * fs + gs] - rdpz5 * dt : 0.0;
+      const double lp = (xs[t + 1] + xs[t - 1] + xs[t + TW] + xs[t - TW] + xs[t + TP] +
+                         xs[t - TP] - 6.0 * xs[t]) / (dx * dx);
+      lapp[gs] = (!fluid || (fl & 63)) ? 0.0 : lp;
+    }
+  }
+}
+
 // Outer-BC folding (bca.f90:5-388) in the order w, e, s, n, b, t
 // (BlockScalar3D.h:183-190) for every cell on an outer face.
 __global__ void __launch_bounds__(THREADS)
@@ -748,6 +818,17 @@ void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b
 }
 void launch_fill(cudaStream_t s, int nb, double* x, size_t stride, double* g, double value) {
   fill_kernel<<<nb, THREADS, 0, s>>>(x, stride, g, value);
+}
+void launch_projection(cudaStream_t s, const KCtx& C, bool corr, const double* p,
+                       const double* gp, const double* cut, const uint8_t* flags, double* ux,
+                       double* uy, double* uz, double* vface, double* lapp, double rhof,
+                       double dt, size_t field_stride) {
+  if (corr)
+    projection_kernel<true><<<C.nb, THREADS, 0, s>>>(C, p, gp, cut, flags, ux, uy, uz, vface,
+                                                     lapp, rhof, dt, field_stride);
+  else
+    projection_kernel<false><<<C.nb, THREADS, 0, s>>>(C, p, gp, cut, flags, ux, uy, uz, vface,
+                                                      lapp, rhof, dt, field_stride);
 }
 void launch_fold_bc(cudaStream_t s, const KCtx& C, double* A, double* b) {
   fold_bc_kernel<<<C.nb, THREADS, 0, s>>>(C, A, b);

@@ -92,6 +92,9 @@ ffvgpu_status field_ptr(ffvgpu_pool* P, int f, bool alloc, double** ptr, size_t*
   } else if (f >= FFVGPU_FIELD_VW && f <= FFVGPU_FIELD_VT) {
     if (alloc && (s = dalloc_t(P, &P->vface, 6 * n))) return s;
     *ptr = P->vface ? P->vface + (size_t)(f - FFVGPU_FIELD_VW) * n : nullptr;
+  } else if (f == FFVGPU_FIELD_LAPP) {
+    if (alloc && (s = dalloc_t(P, &P->lapp, n))) return s;
+    *ptr = P->lapp;
   } else {
     return bad("unknown real field");
   }
@@ -386,7 +389,7 @@ void ffvgpu_pool_destroy(ffvgpu_pool* P) {
   if (P->own_stream) cudaStreamSynchronize(P->own_stream);
   release_instances(P);
   void* ptrs[] = {P->x[0], P->x[1], P->gx, P->A, P->coef, P->b, P->u[0], P->u[1], P->u[2],
-                  P->gu[0], P->gu[1], P->gu[2], P->cut, P->vface, P->flags, P->r,
+                  P->gu[0], P->gu[1], P->gu[2], P->cut, P->vface, P->lapp, P->flags, P->r,
                   P->p, P->q, P->z[0], P->z[1], P->r0, P->sv, P->tv, P->zb[0], P->zb[1],
                   P->partials, P->st, P->hist_d,
                   P->stage, P->nbr_d, P->dx_d};
@@ -563,6 +566,34 @@ ffvgpu_status ffvgpu_assemble_p(ffvgpu_pool* P, double rhof, double dt) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(P->stream));
   return FFVGPU_OK;
+}
+
+static ffvgpu_status projection(ffvgpu_pool* P, double rhof, double dt, bool corr) {
+  if (!P) return bad("null pool");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
+  if (!(rhof > 0.0) || !(dt > 0.0)) return bad("rhof and dt must be positive");
+  cudaSetDevice(P->device);
+  for (int c = 0; c < 3; ++c)
+    if (!P->u[c]) return bad("UX, UY, UZ must exist");
+  if (!P->cut || !P->flags) return bad("cut fields C0..C5, CID0..5 and PID must be uploaded");
+  if (!P->x[P->xcur]) return bad("the pressure must exist");
+  ffvgpu_status s;
+  const size_t n = field_count(P);
+  if (corr && ((s = dalloc_t(P, &P->vface, 6 * n)) || (s = dalloc_t(P, &P->lapp, n)))) return s;
+  launch_projection(P->stream, P->ctx(P->bc_p), corr, P->x[P->xcur], P->gx, P->cut, P->flags,
+                    P->u[0], P->u[1], P->u[2], corr ? P->vface : nullptr,
+                    corr ? P->lapp : nullptr, rhof, dt, n);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(P->stream));
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_remove_p(ffvgpu_pool* P, double rhof, double dt) {
+  return projection(P, rhof, dt, false);
+}
+
+ffvgpu_status ffvgpu_corr_u(ffvgpu_pool* P, double rhof, double dt) {
+  return projection(P, rhof, dt, true);
 }
 
 ffvgpu_status ffvgpu_fold_bc(ffvgpu_pool* P) {

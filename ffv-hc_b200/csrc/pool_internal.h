@@ -80,6 +80,7 @@ struct ffvgpu_pool {
   double* gu[3] = {nullptr, nullptr, nullptr};
   double* cut = nullptr;    // [6][nb*4096]
   double* vface = nullptr;  // [6][nb*4096]
+  double* lapp = nullptr;   // Laplacian of p (bcut_corr_u)
   uint8_t* flags = nullptr; // bits 0..5 cut ids, bit 7 fluid
   double* r = nullptr;
   double* p = nullptr;

@@ -20,7 +20,7 @@ FIELD = {
     "X": 0, "AP": 1, "AW": 2, "AE": 3, "AS": 4, "AN": 5, "AB": 6, "AT": 7, "B": 8,
     "UX": 9, "UY": 10, "UZ": 11,
     "C0": 12, "C1": 13, "C2": 14, "C3": 15, "C4": 16, "C5": 17,
-    "VW": 18, "VE": 19, "VS": 20, "VN": 21, "VB": 22, "VT": 23,
+    "VW": 18, "VE": 19, "VS": 20, "VN": 21, "VB": 22, "VT": 23, "LAPP": 24,
     "CID0": 100, "CID1": 101, "CID2": 102, "CID3": 103, "CID4": 104, "CID5": 105,
     "PID": 106,
 }
@@ -40,7 +40,8 @@ EXPORTS = [
     "ffvgpu_instance_release", "ffvgpu_instance_blocks", "ffvgpu_pool_free_blocks",
     "ffvgpu_mixed_begin", "ffvgpu_mixed_advance", "ffvgpu_mixed_poll", "ffvgpu_instance_result",
     "ffvgpu_assemble_sphere", "ffvgpu_instance_fill", "ffvgpu_serve",
-    "ffvgpu_solve_rbgs_fixed_average",
+    "ffvgpu_solve_rbgs_fixed_average", "ffvgpu_dump2", "ffvgpu_load2",
+    "ffvgpu_restart_filename", "ffvgpu_remove_p", "ffvgpu_corr_u",
 ]
 
 
@@ -154,6 +155,12 @@ def lib():
         L.ffvgpu_solve_rbgs.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
         L.ffvgpu_solve_cg.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
         L.ffvgpu_solve_bicgstab.argtypes = [vp, ctypes.POINTER(IterParams), ctypes.POINTER(Result)]
+        L.ffvgpu_remove_p.argtypes = [vp, dbl, dbl]
+        L.ffvgpu_corr_u.argtypes = [vp, dbl, dbl]
+        L.ffvgpu_dump2.argtypes = [vp, i32, i32, ctypes.c_char_p]
+        L.ffvgpu_load2.argtypes = [vp, i32, i32, ctypes.c_char_p]
+        L.ffvgpu_restart_filename.argtypes = [ctypes.c_char_p, i32, ctypes.c_char_p,
+                                              ctypes.c_char_p, ctypes.c_char_p, i32, i32]
         L.ffvgpu_solve_rbgs_fixed_average.argtypes = [vp, ctypes.POINTER(IterParams),
                                                       ctypes.c_int64, ctypes.POINTER(Result)]
         L.ffvgpu_rbgs_sweep.argtypes = [vp, dbl]
@@ -187,6 +194,16 @@ def lib():
         L.ffvgpu_instance_result.argtypes = [vp, i32, R, vp]
         _lib = L
     return _lib
+
+
+def restart_filename(path, prefix, label, rank, step):
+    """The reference's Dump2/Load2 file name (ffvgpu_restart_filename)."""
+    buf = ctypes.create_string_buffer(4096)
+    n = lib().ffvgpu_restart_filename(buf, 4096, path.encode(), prefix.encode(), label.encode(),
+                                      rank, step)
+    if n < 0:
+        raise ValueError("file name too long")
+    return buf.value.decode()
 
 
 class FFVGPUError(RuntimeError):
@@ -409,6 +426,18 @@ class Pool:
                        history=True, check_every=0, restart_drop=0.0):
         return self._solve(lib().ffvgpu_solve_bicgstab, "solve_bicgstab", omega, count_max,
                            epsilon, pre_count, history, check_every, restart_drop)
+
+    def remove_p(self, rhof=1.0, dt=0.002):
+        _check(lib().ffvgpu_remove_p(self._h, rhof, dt), "remove_p")
+
+    def corr_u(self, rhof=1.0, dt=0.002):
+        _check(lib().ffvgpu_corr_u(self._h, rhof, dt), "corr_u")
+
+    def dump2(self, field, filename, vc=2):
+        _check(lib().ffvgpu_dump2(self._h, FIELD[field], vc, filename.encode()), "dump2")
+
+    def load2(self, field, filename, vc=2):
+        _check(lib().ffvgpu_load2(self._h, FIELD[field], vc, filename.encode()), "load2")
 
     def set_stream(self, stream_handle):
         """Enqueue on a caller's CUDA stream (an int cudaStream_t, 0/None = own)."""

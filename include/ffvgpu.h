@@ -60,6 +60,7 @@ typedef enum {
   FFVGPU_FIELD_C4, FFVGPU_FIELD_C5,
   FFVGPU_FIELD_VW, FFVGPU_FIELD_VE, FFVGPU_FIELD_VS, FFVGPU_FIELD_VN,
   FFVGPU_FIELD_VB, FFVGPU_FIELD_VT,
+  FFVGPU_FIELD_LAPP, /* Laplacian of p written by ffvgpu_corr_u (bcut_corr_u's lapp) */
   FFVGPU_FIELD_NUM_REAL,
   /* integer fields */
   FFVGPU_IFIELD_CID0 = 100, FFVGPU_IFIELD_CID1, FFVGPU_IFIELD_CID2,
@@ -270,6 +271,35 @@ ffvgpu_status ffvgpu_sphere_grid_fill(const ffvgpu_sphere_grid* g, uint64_t seed
                                       double sigma, int32_t vc, double* ux,
                                       double* uy, double* uz, double* const* c6,
                                       int32_t* const* cid6, int32_t* pid);
+
+/* ---- the projection either side of the solve ------------------------------
+ * bcut_remove_p (src/FFV/bcut.f90:3879-4061; Solver.cpp:5378-5386, P01):
+ * u* += dt grad(p)/rho on UX, UY, UZ with the cut-cell gradient rules, 0 in
+ * solid cells.  bcut_corr_u (bcut.f90:4063-4297; Solver.cpp:5738-5748):
+ * u -= dt grad(p)/rho on UX, UY, UZ and the face velocities VW..VT, LAPP = the
+ * 7-point Laplacian of p (0 in solid and cut cells).  Both read p's stored
+ * guide layer (what FIELD_X holds after its last exchange) and the cut fields;
+ * the caller exchanges u afterwards, as UpdateP/UpdateU do. */
+ffvgpu_status ffvgpu_remove_p(ffvgpu_pool* pool, double rhof, double dt);
+ffvgpu_status ffvgpu_corr_u(ffvgpu_pool* pool, double rhof, double dt);
+
+/* ---- restart files: LocalScalar3D::Dump2 / Load2 -------------------------
+ * (src/FFV/LocalScalar3D.cpp:216-354).  The file holds six native int32
+ * (cells per block x, y, z = 16, guide width vc, 1, number of blocks) and then
+ * every block's (16+2vc)^3 doubles in block order, guide cells included.
+ * Dump2 exchanges the field first and writes it; Load2 reads a file of the
+ * same shape, or of 8^3 blocks whose cells each fill 2x2x2 cells
+ * (sf3d_copy_x2, src/CGMfuncs/bsf3d.f90:5-33), and exchanges the field.
+ * Fields X, UX, UY, UZ.  A file that matches neither shape is refused
+ * (the reference exits). */
+ffvgpu_status ffvgpu_dump2(ffvgpu_pool* pool, ffvgpu_field field, int32_t vc,
+                           const char* filename);
+ffvgpu_status ffvgpu_load2(ffvgpu_pool* pool, ffvgpu_field field, int32_t vc,
+                           const char* filename);
+/* The reference's file name, path/prefix label-RRRRR-SSSSSSSSSS.bin
+ * (LocalScalar3D.cpp:224-243); returns its length, or -1 when cap is too small. */
+int32_t ffvgpu_restart_filename(char* out, int32_t cap, const char* path, const char* prefix,
+                                const char* label, int32_t rank, int32_t step);
 
 /* ---- mixed-precision form (no counterpart in the reference) -------------
  * FFVILS::BiCGSTAB's recurrence (src/FFV/FFVILS.h:793-974) in FP64 --

@@ -514,7 +514,7 @@ enum OracleField {
   OF_UX, OF_UY, OF_UZ,
   OF_C0, OF_C1, OF_C2, OF_C3, OF_C4, OF_C5,
   OF_VW, OF_VE, OF_VS, OF_VN, OF_VB, OF_VT,
-  OF_R, OF_P, OF_Q, OF_Z, OF_X0, OF_R0, OF_P_, OF_Q_, OF_S, OF_S_, OF_T_,
+  OF_R, OF_P, OF_Q, OF_Z, OF_X0, OF_R0, OF_P_, OF_Q_, OF_S, OF_S_, OF_T_, OF_LAPP,
   OF_NUM
 };
 enum OracleIField { OI_CID0 = 0, OI_CID1, OI_CID2, OI_CID3, OI_CID4, OI_CID5, OI_PID, OI_NUM };
@@ -1044,6 +1044,93 @@ int orc_cg(Oracle* O, double omega, int countPre, int countMax, double epsilon,
 // FFVILS.h:793-974 BiCGSTAB (Jacobi-preconditioned).  Returns 0 ok, 2 NaN/Inf.
 int orc_bicgstab_restart(Oracle* O, double omega, int countPre, int countMax, double epsilon,
                          double restart_drop, int* count, double* residual, double* hist);
+
+// bcut.f90:3879-4061 bcut_remove_p (corr = 0) and bcut.f90:4063-4297
+// bcut_corr_u (corr = 1), per block in i, j, k order, on the reference
+// layout: p = X with the guide values it holds.
+void orc_projection(Oracle* O, int corr, double rhof, double dt) {
+  Oracle& R = *O;
+  Grid& G = R.G;
+  const int n = G.n;
+  const long sy = n + 2 * G.g, sz = sy * sy;
+#pragma omp parallel for num_threads(R.nthreads) schedule(static)
+  for (int bi = 0; bi < G.nb; ++bi) {
+    const double dx = G.blocks[bi].dx;
+    const double* p = R.F(OF_X, bi);
+    double* ux = R.F(OF_UX, bi);
+    double* uy = R.F(OF_UY, bi);
+    double* uz = R.F(OF_UZ, bi);
+    double* vw = R.F(OF_VW, bi);
+    double* ve = R.F(OF_VE, bi);
+    double* vs = R.F(OF_VS, bi);
+    double* vn = R.F(OF_VN, bi);
+    double* vb = R.F(OF_VB, bi);
+    double* vt = R.F(OF_VT, bi);
+    double* lapp = R.F(OF_LAPP, bi);
+    const double* c[6] = {R.F(OF_C0, bi), R.F(OF_C1, bi), R.F(OF_C2, bi),
+                          R.F(OF_C3, bi), R.F(OF_C4, bi), R.F(OF_C5, bi)};
+    const int* cid[6];
+    for (int f = 0; f < 6; ++f) cid[f] = R.fi[OI_CID0 + f].data() + (long)bi * G.nc;
+    const int* pid = R.fi[OI_PID].data() + (long)bi * G.nc;
+    for (int k = 1; k <= n; ++k)
+      for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) {
+          const long m = IDX(G, i, j, k);
+          const double r0 = 1.0 / rhof, r1 = 1.0 / rhof, r2 = 1.0 / rhof;
+          const double r3 = 1.0 / rhof, r4 = 1.0 / rhof, r5 = 1.0 / rhof;
+          double dpx0 = (p[m] - p[m - 1]) / dx;
+          double dpx1 = (p[m + 1] - p[m]) / dx;
+          double dpy2 = (p[m] - p[m - sy]) / dx;
+          double dpy3 = (p[m + sy] - p[m]) / dx;
+          double dpz4 = (p[m] - p[m - sz]) / dx;
+          double dpz5 = (p[m + sz] - p[m]) / dx;
+          double rdpx0 = r0 * dpx0, rdpx1 = r1 * dpx1, rdpy2 = r2 * dpy2;
+          double rdpy3 = r3 * dpy3, rdpz4 = r4 * dpz4, rdpz5 = r5 * dpz5;
+          const double d0 = c[0][m], d1 = c[1][m], d2 = c[2][m];
+          const double d3 = c[3][m], d4 = c[4][m], d5 = c[5][m];
+          const int cp0 = cid[0][m], cp1 = cid[1][m], cp2 = cid[2][m];
+          const int cp3 = cid[3][m], cp4 = cid[4][m], cp5 = cid[5][m];
+          if (cp0 != 0) { rdpx0 = rdpx1 * (d0 - 0.5) / (d0 + 0.5); dpx0 = dpx1 * (d0 - 0.5) / (d0 + 0.5); }
+          if (cp1 != 0) { rdpx1 = rdpx0 * (d1 - 0.5) / (d1 + 0.5); dpx1 = dpx0 * (d1 - 0.5) / (d1 + 0.5); }
+          if (cp2 != 0) { rdpy2 = rdpy3 * (d2 - 0.5) / (d2 + 0.5); dpy2 = dpy3 * (d2 - 0.5) / (d2 + 0.5); }
+          if (cp3 != 0) { rdpy3 = rdpy2 * (d3 - 0.5) / (d3 + 0.5); dpy3 = dpy2 * (d3 - 0.5) / (d3 + 0.5); }
+          if (cp4 != 0) { rdpz4 = rdpz5 * (d4 - 0.5) / (d4 + 0.5); dpz4 = dpz5 * (d4 - 0.5) / (d4 + 0.5); }
+          if (cp5 != 0) { rdpz5 = rdpz4 * (d5 - 0.5) / (d5 + 0.5); dpz5 = dpz4 * (d5 - 0.5) / (d5 + 0.5); }
+          if (cp0 != 0 && cp1 != 0) { rdpx0 = 0.0; rdpx1 = 0.0; }
+          if (cp2 != 0 && cp3 != 0) { rdpy2 = 0.0; rdpy3 = 0.0; }
+          if (cp4 != 0 && cp5 != 0) { rdpz4 = 0.0; rdpz5 = 0.0; }
+          const double rdpx = 0.5 * (rdpx0 + rdpx1);
+          const double rdpy = 0.5 * (rdpy2 + rdpy3);
+          const double rdpz = 0.5 * (rdpz4 + rdpz5);
+          (void)dpx0; (void)dpx1; (void)dpy2; (void)dpy3; (void)dpz4; (void)dpz5;
+          if (!corr) {
+            ux[m] = ux[m] + rdpx * dt;
+            uy[m] = uy[m] + rdpy * dt;
+            uz[m] = uz[m] + rdpz * dt;
+            if (pid[m] != 1) ux[m] = uy[m] = uz[m] = 0.0;
+          } else {
+            ux[m] = ux[m] - rdpx * dt;
+            uy[m] = uy[m] - rdpy * dt;
+            uz[m] = uz[m] - rdpz * dt;
+            vw[m] = vw[m] - rdpx0 * dt;
+            ve[m] = ve[m] - rdpx1 * dt;
+            vs[m] = vs[m] - rdpy2 * dt;
+            vn[m] = vn[m] - rdpy3 * dt;
+            vb[m] = vb[m] - rdpz4 * dt;
+            vt[m] = vt[m] - rdpz5 * dt;
+            lapp[m] = (p[m + 1] + p[m - 1] + p[m + sy] + p[m - sy] + p[m + sz] + p[m - sz] -
+                       6.0 * p[m]) / (dx * dx);
+            if (pid[m] != 1) {
+              ux[m] = uy[m] = uz[m] = 0.0;
+              vw[m] = ve[m] = vs[m] = vn[m] = vb[m] = vt[m] = 0.0;
+              lapp[m] = 0.0;
+            }
+            if (cp0 != 0 || cp1 != 0 || cp2 != 0 || cp3 != 0 || cp4 != 0 || cp5 != 0)
+              lapp[m] = 0.0;
+          }
+        }
+  }
+}
 
 // FFVILS.h:596-659 RBGS_WithFixedAverage (the reference's xave is unused).
 int orc_rbgs_fixed_average(Oracle* O, double omega, long ncells, int countMax, double epsilon,

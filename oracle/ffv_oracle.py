@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(_HERE, "libffvoracle.so")
 
 F = dict(X=0, AP=1, AW=2, AE=3, AS=4, AN=5, AB=6, AT=7, B=8, UX=9, UY=10, UZ=11,
          C0=12, C1=13, C2=14, C3=15, C4=16, C5=17, VW=18, VE=19, VS=20, VN=21, VB=22, VT=23,
-         R=24, P=25, Q=26, Z=27, X0=28, R0=29, P_=30, Q_=31, S=32, S_=33, T_=34)
+         R=24, P=25, Q=26, Z=27, X0=28, R0=29, P_=30, Q_=31, S=32, S_=33, T_=34, LAPP=35)
 FI = dict(CID0=0, CID1=1, CID2=2, CID3=3, CID4=4, CID5=5, PID=6)
 RED_REFERENCE, RED_CANONICAL = 0, 1
 
@@ -66,6 +66,8 @@ def lib():
             fn.argtypes = [vp, dbl, i32, dbl, vp, vp, vp]
         for fn in (L.orc_cg, L.orc_bicgstab):
             fn.argtypes = [vp, dbl, i32, i32, dbl, vp, vp, vp]
+        L.orc_projection.argtypes = [vp, i32, dbl, dbl]
+        L.orc_projection.restype = None
         L.orc_rbgs_fixed_average.argtypes = [vp, dbl, ctypes.c_long, i32, dbl, vp, vp, vp]
         L.orc_bicgstab_restart.argtypes = [vp, dbl, i32, i32, dbl, dbl, vp, vp, vp]
         L.orc_mixed.argtypes = [vp, dbl, i32, i32, i32, dbl, dbl, dbl, i32, vp, vp, vp]
@@ -152,6 +154,12 @@ class Oracle:
 
     def fold_bc(self):
         lib().orc_fold_bc(self._h)
+
+    def remove_p(self, rhof=1.0, dt=0.002):
+        lib().orc_projection(self._h, 0, rhof, dt)
+
+    def corr_u(self, rhof=1.0, dt=0.002):
+        lib().orc_projection(self._h, 1, rhof, dt)
 
     def rbgs_sweep(self, omega):
         lib().orc_rbgs_sweep(self._h, omega)

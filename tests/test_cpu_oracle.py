@@ -503,3 +503,10 @@ def test_bicgstab_converges_on_refined_sphere_grid():
     O.field("X")[...] = 0.0
     r = O.solve_bicgstab(1.0, 2, 600, 1e-8)
     assert r["status"] == 0 and r["residual"] <= 1e-8
+
+
+def test_restart_filename_follows_the_reference_pattern():
+    """LocalScalar3D.cpp:224-243: path/prefix label-rank(5)-step(10).bin."""
+    import ffvgpu
+    assert (ffvgpu.restart_filename("out", "ffv_", "p", 3, 1200)
+            == "out/ffv_p-00003-0000001200.bin")

@@ -317,3 +317,60 @@ def test_rbgs_fixed_average_bitwise(level, omega, count, eps):
     # the shifted pressure has zero mean up to rounding
     assert abs(interior(got).mean()) < 1e-12 * (np.abs(interior(got)).max() + 1.0)
     P.close()
+
+
+def test_dump2_load2_roundtrip_and_half_resolution(tmp_path):
+    """LocalScalar3D::Dump2 / Load2: the file layout, a round trip through
+    another pool, and a half-resolution file spread 2x2x2 (sf3d_copy_x2)."""
+    g, inp, O = problem(1, threads=THREADS)
+    P = device_problem(g, inp)
+    x = random_field(g, 31)
+    P.upload("X", x, VC)
+    fn = str(tmp_path / ffvgpu.restart_filename(".", "ffv_", "p", 0, 7).lstrip("./"))
+    P.dump2("X", fn, VC)
+    raw = np.fromfile(fn, dtype=np.int32, count=6)
+    assert list(raw) == [16, 16, 16, VC, 1, g.nb]
+    body = np.fromfile(fn, dtype=np.float64, offset=24).reshape(g.nb, 20, 20, 20)
+    P.exchange("X")
+    assert_bitwise(body, P.download("X", VC), "file body = exchanged field")
+    Q = ffvgpu.Pool(g.desc())
+    Q.load2("X", fn, VC)
+    assert_bitwise(interior(Q.download("X", VC)), interior(body), "loaded interior")
+    # a file of 8^3 blocks
+    rng = np.random.default_rng(3)
+    coarse = rng.standard_normal((g.nb, 12, 12, 12))
+    fc = str(tmp_path / "coarse.bin")
+    with open(fc, "wb") as f:
+        np.array([8, 8, 8, VC, 1, g.nb], np.int32).tofile(f)
+        coarse.tofile(f)
+    Q.load2("X", fc, VC)
+    want = np.repeat(np.repeat(np.repeat(coarse[:, 2:10, 2:10, 2:10], 2, 1), 2, 2), 2, 3)
+    assert_bitwise(interior(Q.download("X", VC)), want, "x2 spread interior")
+    bad_file = str(tmp_path / "bad.bin")
+    with open(bad_file, "wb") as f:
+        np.array([16, 16, 16, VC, 1, g.nb + 1], np.int32).tofile(f)
+    with pytest.raises(ffvgpu.FFVGPUError):
+        Q.load2("X", bad_file, VC)
+    P.close()
+    Q.close()
+
+
+def test_projection_remove_p_and_corr_u_bitwise():
+    """bcut_remove_p and bcut_corr_u around the solve: u, the face velocities
+    and the Laplacian of p bit-equal to the oracle on a cut-cell grid."""
+    g, inp, O = problem(2, threads=THREADS)
+    P = device_problem(g, inp)
+    x = random_field(g, 41) * 1e-3
+    O.field("X")[...] = x
+    O.exchange("X", ffvgpu.P_BC_TYPE, ffvgpu.P_BC_VALUE)
+    P.upload("X", O.field("X").copy(), VC)
+    O.remove_p(1.0, 0.002)
+    P.remove_p(1.0, 0.002)
+    for u in ("UX", "UY", "UZ"):
+        assert_bitwise(interior(P.download(u, VC)), interior(O.field(u)), f"remove_p {u}")
+    O.corr_u(1.0, 0.002)
+    P.corr_u(1.0, 0.002)
+    for f in ("UX", "UY", "UZ", "VW", "VE", "VS", "VN", "VB", "VT", "LAPP"):
+        assert_bitwise(interior(P.download(f, VC)), interior(O.field(f)), f"corr_u {f}")
+    assert np.abs(interior(O.field("LAPP"))).max() > 0
+    P.close()
