@@ -266,6 +266,22 @@ def run_reference(args):
     return 0
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time (ms): every rank's device-timed region, max-reduced."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, ms):
+    """Whole-job throughput in G units/s: every rank processes units_per_rank
+    (weak scaling), all within the slowest rank's time."""
+    return world * units_per_rank / (ms * 1e-3) / 1e9
+
+
 def workload_config(g, args, extra=None):
     c = {"workload": f"rbsor-fp64-sphere-level{args.level}", "blocks": int(g.nb),
          "cells": int(g.cells), "sweeps": args.sweeps, "omega": args.omega,
@@ -670,11 +686,8 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
     t_ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-    value = world * cells * args.sweeps * args.steps / (t_ms * 1e-3) / 1e9
+    t_ms = max_over_ranks(t_ms, dist, "cuda")
+    value = whole_job_rate(world, cells * args.sweeps * args.steps, t_ms)
 
     # ---- end-to-end through the C ABI with host buffers ---------------------
     w = 20
@@ -707,11 +720,8 @@ def main():
     ev1.record(stream)
     torch.cuda.synchronize()
     te_ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([te_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        te_ms = float(t.item())
-    e2e_value = world * cells * args.sweeps * args.steps / (te_ms * 1e-3) / 1e9
+    te_ms = max_over_ranks(te_ms, dist, "cuda")
+    e2e_value = whole_job_rate(world, cells * args.sweeps * args.steps, te_ms)
 
     # ---- roofline of the dominant kernel (fused residual + RB sweep) ---------
     avg_launch_ms = float(np.sum(sweep_ms) / max(1, np.sum(sweep_n)))
