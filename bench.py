@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--requests", type=int, default=32, help="serve form: requests per rate")
     ap.add_argument("--rates", default="10,20,50,100,200,500", help="serve form: req/s")
     ap.add_argument("--capacity", type=int, default=40000, help="serve form: pool blocks")
+    ap.add_argument("--tune", action="store_true",
+                    help="batch form: pick the mixed settings with the autotuner first")
+    ap.add_argument("--tune-sample", type=int, default=8,
+                    help="batch form: instances the autotuner times each candidate on")
     ap.add_argument("--profile-iterations", type=int, default=0,
                     help="mixed form: only run this many mixed iterations once (for ncu)")
     ap.add_argument("--level", type=int, default=5)
@@ -564,11 +568,35 @@ def run_batch(args):
     admit_s = time.perf_counter() - t0
     assert all(i is not None for i in ids)
 
+    setting = dict(MIXED, iterations_per_replay=8)
+    tune = None
+    if args.tune:
+        # a sample spread over the instance sizes (every k-th by block count)
+        order = sorted(range(len(ids)), key=lambda k: blocks[k])
+        step = max(1, len(order) // max(1, args.tune_sample))
+        sample = [ids[k] for k in order[::step][:args.tune_sample]]
+        t0 = time.perf_counter()
+        recs, best = B.autotune(sample)
+        tune = {"sample_instances": len(sample),
+                "sample_blocks": int(sum(B.blocks(i) for i in sample)),
+                "candidates": len(recs), "seconds": time.perf_counter() - t0,
+                "converged_candidates": sum(r["converged"] for r in recs),
+                "best": recs[best] if best >= 0 else None,
+                "default": next((r for r in recs if r["omega"] == MIXED["omega"] and
+                                 r["sweeps"] == MIXED["sweeps"] and
+                                 r["sweeps_per_exchange"] == MIXED["sweeps_per_exchange"] and
+                                 r["iterations_per_replay"] == 8), None)}
+        if best >= 0:
+            b = recs[best]
+            setting = dict(omega=b["omega"], sweeps=b["sweeps"],
+                           sweeps_per_exchange=b["sweeps_per_exchange"],
+                           iterations_per_replay=b["iterations_per_replay"])
+
     def batched():
         for i in ids:
             B.fill(i, "X", 0.0)
-        return B.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
-                             5000, 1e-8, check_every=8)
+        return B.solve_mixed(setting["omega"], setting["sweeps"], setting["sweeps_per_exchange"],
+                             5000, 1e-8, check_every=setting["iterations_per_replay"])
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         for _ in range(max(1, args.warmup)):
@@ -622,7 +650,7 @@ def run_batch(args):
         "config": {"workload": f"batch-{len(ids)}-sphere-instances", "instances": len(ids),
                    "blocks": total, "cells": total * CELLS_PER_BLOCK,
                    "blocks_min_max": [int(min(blocks)), int(max(blocks))], "epsilon": 1e-8,
-                   "mixed": MIXED, "graph_iterations_per_replay": 8,
+                   "mixed": setting, "autotuned": bool(args.tune),
                    "instances_rule": "diameter U[0.5,2], centre U([0,8]x[-2,2]x[-2,2]), "
                                      "max level U{2..5}, seed = index"},
         "iterations_min_max": [int(min(iters)), int(max(iters))], "worst_residual": worst,
@@ -634,7 +662,7 @@ def run_batch(args):
                                "solver": "BiCGSTAB omega 1, PreCount 2"},
         "mixed_one_at_a_time": {"solves_per_s": alone_sps, "sample": len(sample)},
         "speedup_vs_fp64_one_at_a_time": (1e3 * len(ids) / tb) / fp64_sps,
-        "admission_s": admit_s, "device_gb": dev_gb, "clocks": clk.summary(),
+        "admission_s": admit_s, "device_gb": dev_gb, "autotune": tune, "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     return 0

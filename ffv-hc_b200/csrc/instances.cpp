@@ -796,4 +796,73 @@ ffvgpu_status ffvgpu_solve_mixed(ffvgpu_pool* P, const ffvgpu_mixed_params* prm,
   return first_status;
 }
 
+// Times the mixed solve of the given instances, from x = 0, for each
+// candidate setting in records (omega, sweeps, sweeps_per_exchange,
+// iterations per graph replay), with base's count_max, epsilon and restart
+// settings; fills in each record's time, largest iteration count and whether
+// every instance converged, and returns in *best the fastest candidate that
+// converged them all (-1 if none did).  The instances end with x = 0.
+ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* P, const int32_t* instances, int32_t n,
+                                    const ffvgpu_mixed_params* base, ffvgpu_tune_record* rec,
+                                    int32_t n_rec, int32_t* best) {
+  if (!P || !instances || n <= 0 || !base || !rec || n_rec <= 0 || !best)
+    return bad("null or empty argument");
+  cudaSetDevice(P->device);
+  for (const ffvgpu_instance& I : P->inst)
+    if (I.running) return bad("a stepped mixed solve is running on this pool");
+  for (int i = 0; i < n; ++i)
+    if (!get_inst(P, instances[i])) return bad("bad instance");
+  ffvgpu_status s;
+  *best = -1;
+  double best_ms = 0.0;
+  for (int c = 0; c < n_rec; ++c) {
+    ffvgpu_tune_record& R = rec[c];
+    ffvgpu_mixed_params prm = *base;
+    prm.omega = R.omega;
+    prm.sweeps = R.sweeps;
+    prm.sweeps_per_exchange = R.sweeps_per_exchange;
+    prm.history = nullptr;
+    R.ms = 0.0;
+    R.max_count = 0;
+    R.converged = 0;
+    if ((s = check_mixed(&prm))) return s;
+    if (R.iterations_per_replay <= 0) return bad("iterations_per_replay must be positive");
+    for (int i = 0; i < n; ++i)
+      if ((s = ffvgpu_instance_fill(P, instances[i], FFVGPU_FIELD_X, 0.0))) return s;
+    CK(cudaEventRecord(P->ev0, P->stream));
+    for (int i = 0; i < n; ++i)
+      if ((s = ffvgpu_mixed_begin(P, instances[i], &prm))) return s;
+    for (;;) {
+      int32_t nf = 0;
+      if ((s = ffvgpu_mixed_poll(P, nullptr, 0, &nf))) return s;
+      bool any = false;
+      for (int i = 0; i < n; ++i) any = any || P->inst[instances[i]].running;
+      if (!any) break;
+      if ((s = ffvgpu_mixed_advance(P, R.iterations_per_replay))) return s;
+    }
+    CK(cudaEventRecord(P->ev1, P->stream));
+    CK(cudaEventSynchronize(P->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, P->ev0, P->ev1);
+    R.ms = ms;
+    bool all = true;
+    for (int i = 0; i < n; ++i) {
+      const ffvgpu_instance& I = P->inst[instances[i]];
+      const int cnt = I.result.count;
+      if (cnt > R.max_count) R.max_count = cnt;
+      const bool ok = I.status == 0 && cnt >= 1 && cnt <= prm.count_max &&
+                      I.result.residual <= prm.epsilon;
+      all = all && ok;
+    }
+    R.converged = all ? 1 : 0;
+    if (all && (*best < 0 || R.ms < best_ms)) {
+      *best = c;
+      best_ms = R.ms;
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    if ((s = ffvgpu_instance_fill(P, instances[i], FFVGPU_FIELD_X, 0.0))) return s;
+  return FFVGPU_OK;
+}
+
 }  // extern "C"

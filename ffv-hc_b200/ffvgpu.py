@@ -41,7 +41,7 @@ EXPORTS = [
     "ffvgpu_mixed_begin", "ffvgpu_mixed_advance", "ffvgpu_mixed_poll", "ffvgpu_instance_result",
     "ffvgpu_assemble_sphere", "ffvgpu_instance_fill", "ffvgpu_serve",
     "ffvgpu_solve_rbgs_fixed_average", "ffvgpu_dump2", "ffvgpu_load2",
-    "ffvgpu_restart_filename", "ffvgpu_remove_p", "ffvgpu_corr_u",
+    "ffvgpu_restart_filename", "ffvgpu_remove_p", "ffvgpu_corr_u", "ffvgpu_mixed_autotune",
 ]
 
 
@@ -110,6 +110,21 @@ class SphereProblem(ctypes.Structure):
         ("rhof", ctypes.c_double), ("dt", ctypes.c_double),
         ("u_bc_type", (ctypes.c_int32 * 6) * 3), ("u_bc_value", (ctypes.c_double * 6) * 3),
     ]
+
+
+class TuneRecord(ctypes.Structure):
+    _fields_ = [
+        ("omega", ctypes.c_double), ("sweeps", ctypes.c_int32),
+        ("sweeps_per_exchange", ctypes.c_int32), ("iterations_per_replay", ctypes.c_int32),
+        ("ms", ctypes.c_double), ("max_count", ctypes.c_int32), ("converged", ctypes.c_int32),
+    ]
+
+
+# Candidate settings the batch autotuner sweeps: sweeps per exchange 1, 2, 4,
+# 8 (8 sweeps per application, and 4), omega 1.2 and 1.5, 4 / 8 / 16 graph
+# iterations per replay.
+TUNE_SPACE = [(om, sw, per, it) for om in (1.5, 1.2) for (sw, per) in
+              ((8, 4), (8, 8), (8, 2), (8, 1), (4, 4), (4, 2)) for it in (4, 8, 16)]
 
 
 class Request(ctypes.Structure):
@@ -184,6 +199,8 @@ def lib():
         L.ffvgpu_instance_download.argtypes = [vp, i32, i32, vp, i32]
         L.ffvgpu_instance_release.argtypes = [vp, i32]
         L.ffvgpu_instance_fill.argtypes = [vp, i32, i32, dbl]
+        L.ffvgpu_mixed_autotune.argtypes = [vp, vp, i32, MP, ctypes.POINTER(TuneRecord), i32,
+                                             vp]
         L.ffvgpu_serve.argtypes = [vp, MP, i32, ctypes.POINTER(Request), i32,
                                    ctypes.POINTER(RequestResult)]
         L.ffvgpu_instance_blocks.argtypes = [vp, i32]
@@ -611,6 +628,24 @@ class Batch:
         return [dict(arrival_s=float(arrivals[i]), admit_s=out[i].admit_s,
                      finish_s=out[i].finish_s, count=out[i].count, residual=out[i].residual,
                      status=out[i].status, blocks=out[i].blocks) for i in range(n)]
+
+    def autotune(self, instances, space=None, count_max=1500, epsilon=1e-8):
+        """ffvgpu_mixed_autotune over space (omega, sweeps, per-exchange, replay
+        iterations): (records as dicts, index of the best or -1)."""
+        space = space or TUNE_SPACE
+        recs = (TuneRecord * len(space))()
+        for k, (om, sw, per, it) in enumerate(space):
+            recs[k].omega, recs[k].sweeps = om, sw
+            recs[k].sweeps_per_exchange, recs[k].iterations_per_replay = per, it
+        ids = np.ascontiguousarray(instances, np.int32)
+        prm = MixedParams(1.5, 8, 4, count_max, epsilon, 0, None, *_restart(None, None, None))
+        best = ctypes.c_int32()
+        _check(lib().ffvgpu_mixed_autotune(self._h, _ptr(ids), len(ids), ctypes.byref(prm),
+                                           recs, len(space), ctypes.byref(best)), "autotune")
+        out = [dict(omega=r.omega, sweeps=r.sweeps, sweeps_per_exchange=r.sweeps_per_exchange,
+                    iterations_per_replay=r.iterations_per_replay, ms=r.ms,
+                    max_count=r.max_count, converged=bool(r.converged)) for r in recs]
+        return out, best.value
 
     def begin(self, inst, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
               epsilon=1e-8, restart_drop=None, restart_growth=None, restart_every=None):

@@ -411,6 +411,28 @@ ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* pool, int32_t* finished, int32_t ca
 ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* pool, int32_t instance,
                                      ffvgpu_result* res, double* history);
 
+/* The autotuner (no counterpart in the reference): times the mixed solve of
+ * the given admitted instances from x = 0 for each candidate setting --
+ * omega, sweeps, sweeps_per_exchange, and iterations per captured-graph
+ * replay -- with base's count_max, epsilon and restart settings, fills in
+ * each record's device time (ms), its largest iteration count and whether
+ * every instance reached epsilon, and sets *best to the fastest candidate
+ * that converged them all (-1 if none did).  The instances end with x = 0. */
+typedef struct {
+  double omega;
+  int32_t sweeps;
+  int32_t sweeps_per_exchange;
+  int32_t iterations_per_replay;
+  double ms;          /* out */
+  int32_t max_count;  /* out */
+  int32_t converged;  /* out: 1 when every instance reached epsilon */
+} ffvgpu_tune_record;
+
+ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* pool, const int32_t* instances,
+                                    int32_t n_instances, const ffvgpu_mixed_params* base,
+                                    ffvgpu_tune_record* records, int32_t n_records,
+                                    int32_t* best);
+
 /* ---- serving (no counterpart in the reference) ---------------------------
  * A request loop with continuous batching on a batch pool: requests (sorted
  * by arrival time, seconds from the start of the call) are admitted in

@@ -216,3 +216,27 @@ def test_serve_continuous_batching_results_equal_alone():
         assert o["residual"] == ra["residual"]
     assert B.free_blocks()[0] == 300
     B.close()
+
+
+def test_autotuner_times_candidates_and_leaves_x_zero():
+    B = ffvgpu.Batch(600, 4)
+    ids = [B.admit_sphere(sphere(1, 3)), B.admit_sphere(sphere(1, 4, center=(3.0, 1.0, 0.0)))]
+    space = [(1.5, 8, 4, 8), (1.2, 4, 4, 4), (1.5, 8, 8, 16)]
+    recs, best = B.autotune(ids, space=space, count_max=400)
+    assert len(recs) == 3 and all(r["ms"] > 0 and r["max_count"] >= 1 for r in recs)
+    assert best == -1 or recs[best]["converged"]
+    if best >= 0:
+        assert recs[best]["ms"] == min(r["ms"] for r in recs if r["converged"])
+    for i in ids:
+        assert not np.any(interior(B.download(i, "X", VC)))
+    # the tuned setting reproduces the solve it timed
+    if best >= 0:
+        r = recs[best]
+        B.begin(ids[0], omega=r["omega"], sweeps=r["sweeps"],
+                sweeps_per_exchange=r["sweeps_per_exchange"], count_max=400)
+        for _ in range(400):
+            B.advance(r["iterations_per_replay"])
+            if ids[0] in B.poll():
+                break
+        assert B.result(ids[0])["count"] <= r["max_count"]
+    B.close()
