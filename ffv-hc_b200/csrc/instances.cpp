@@ -36,7 +36,7 @@ void release_instances(ffvgpu_pool* P) {
   if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
   P->mgraph = nullptr;
   void* ptrs[] = {P->blk_inst_d, P->inst_first_d, P->inst_count_d, P->blk_geo_d, P->mst,
-                  P->mpartials, P->mhist, P->mcoef, P->me[0], P->me[1], P->mv32, P->mph,
+                  P->mpartials, P->mhist, P->mcoef, P->me[0], P->me[1], P->mph,
                   P->msh};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -126,8 +126,8 @@ ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P) {
     mx_grid_sizes(&P->grid_sweep, &P->grid_matvec, &P->grid_update);
   }
   if ((s = dalloc_t(P, &P->mcoef, 7 * n)) || (s = dalloc_t(P, &P->me[0], n)) ||
-      (s = dalloc_t(P, &P->me[1], n)) || (s = dalloc_t(P, &P->mv32, n)) ||
-      (s = dalloc_t(P, &P->mph, n)) || (s = dalloc_t(P, &P->msh, n)) ||
+      (s = dalloc_t(P, &P->me[1], n)) || (s = dalloc_t(P, &P->mph, n)) ||
+      (s = dalloc_t(P, &P->msh, n)) ||
       (s = dalloc_t(P, &P->r, n)) || (s = dalloc_t(P, &P->r0, n)) || (s = dalloc_t(P, &P->p, n)) ||
       (s = dalloc_t(P, &P->q, n)) || (s = dalloc_t(P, &P->sv, n)) || (s = dalloc_t(P, &P->tv, n)))
     return s;
@@ -192,9 +192,9 @@ ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
 // Algorithmic HBM bytes of one iteration per cell: two preconditioner
 // applications, two A*x with dot products, the update.
 int64_t iteration_bytes_per_cell(int passes) {
-  const int64_t first_p = 28 + 8 + 16 + 8 + (passes > 1 ? 4 : 0) + 4;
-  const int64_t first_s = 28 + 16 + 8 + (passes > 1 ? 4 : 0) + 4;
-  const int64_t later = 28 + 4 + 4 + 4;
+  const int64_t first_p = 28 + 8 + 16 + 8 + 4;  // coefficients, r, p and q, p, e
+  const int64_t first_s = 28 + 16 + 8 + 4;       // coefficients, q and r, s, e
+  const int64_t later = 28 + 8 + 4 + 4;          // coefficients, p or s, e in, e out
   const int64_t matvec = 56 + 4 + 8 + 8;
   const int64_t update = 4 + 4 + 8 + 8 + 8 + 8 + 8 + 8;
   return first_p + first_s + 2 * (passes - 1) * later + 2 * matvec + update;
@@ -211,10 +211,8 @@ void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
     float* hat = mode == 0 ? P->mph : P->msh;
     for (int ps = 0; ps < passes; ++ps) {
       const bool last = ps == passes - 1;
-      launch_mx_sweep(s, C, P->grid_sweep, mode, ps == 0, last, om, P->m_per_exchange, P->r,
-                      P->r0, rhs,
-                      P->q,
-                      P->mcoef, P->mv32, ps > 0 ? P->me[(ps - 1) & 1] : nullptr,
+      launch_mx_sweep(s, C, P->grid_sweep, mode, ps == 0, om, P->m_per_exchange, P->r, P->r0,
+                      rhs, P->q, P->mcoef, ps > 0 ? P->me[(ps - 1) & 1] : nullptr,
                       last ? hat : P->me[ps & 1]);
     }
     if (mode == 0)

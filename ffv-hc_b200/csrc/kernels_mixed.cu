@@ -7,28 +7,33 @@
 // keep the reference's per-cell expressions and are compiled with
 // --fmad=false.  Its preconditioner -- FFVILS's Jacobi_PreConditioner
 // (FFVILS.h:469-492) in the reference -- is replaced by red-black SOR sweeps
-// in FP32 that solve A e = v approximately from e = 0: 'sweeps' colour pairs
-// per application, grouped 'per_exchange' at a time between guide-cell
-// exchanges.  Inside a group a block sweeps against fixed guide values, so
-// the whole group runs on chip: one CTA per block keeps the block's FP32
-// coefficients in registers and its iterate in shared memory, and HBM sees
-// one read of the coefficients and one write of the result per group.
+// on 32-bit data that solve A e = v approximately from e = 0: 'sweeps'
+// colour pairs per application, grouped 'per_exchange' at a time between
+// guide-cell exchanges (one pass of the sweep kernel per group).  Inside a
+// pass a block sweeps against fixed guide values, so the whole pass runs on
+// chip: one CTA per block keeps the block's coefficients in registers and
+// its iterate in shared memory, and HBM sees one read of the coefficients
+// and the right-hand side and one FP32 write of the iterate per pass.
 //
-// Sweep of one cell (colour order and neighbour terms as rbgs_smoother,
-// src/CGMfuncs/bils.f90:57-108) on FP32 data -- coefficients, right-hand
-// side and iterate are FP32 values -- with the update formed in FP64 and
-// rounded to FP32 once, when it is stored:
+// Data in HBM: the coefficients aw..at and dinv = 1 / Ap as 32-bit words
+// (each FP64 value rounded to 20 fraction bits, kept as the high word of an
+// FP64 number, so widening it is a register move), the iterate between
+// passes and the preconditioned vectors in FP32, the right-hand side in
+// FP64.  Arithmetic: FP64 throughout a pass, on an FP64 iterate (the tile);
+// the iterate is rounded to FP32 once, at the end of the pass.  Sweep of
+// one cell (colour order and neighbour terms as rbgs_smoother,
+// src/CGMfuncs/bils.f90:57-108):
 //   rc = v; rc = fma(-aw, eW, rc); ... fma(-ab, eB, rc); fma(-at, eT, rc)
-//   xt = rc * dinv                       (dinv = (float)(1.0 / Ap))
-//   e  = (float)fma(-omega, e - xt, e)   (e - omega (e - xt))
+//   xt = rc * dinv;  e = fma(-omega, e - xt, e)   (e - omega (e - xt))
 // Forming rc in FP32 would cancel: once a block has nearly converged locally
-// rc is far smaller than its terms, and its FP32 rounding error (1e-5 and
-// more relative) makes the preconditioner visibly nonlinear, which the
-// BiCGSTAB recurrence does not survive; in FP64 the only nonlinearity left
-// is the final rounding of each stored value.
-// Guide cells of e: the exchange rules (same-level copy, 2:1 interpolation
-// and restriction, src/CGMfuncs/sup.f90) evaluated in FP64 on the FP32
-// values and rounded to FP32; outer faces take homogeneous Dirichlet values.
+// rc is far smaller than its terms, and its FP32 rounding error makes the
+// preconditioner visibly nonlinear, which the BiCGSTAB recurrence does not
+// survive; here the only nonlinearity left is the rounding of each pass's
+// result.
+// Guide cells of e: zero in the first pass; later, the exchange rules
+// (same-level copy, 2:1 interpolation and restriction, src/CGMfuncs/sup.f90)
+// evaluated in FP64 on the previous pass's FP32 values, with homogeneous
+// Dirichlet values on outer faces.
 //
 // Every sum is the canonical tree of the layout header taken over one
 // instance's blocks, so an instance gets the same bits alone or in a batch.
@@ -36,6 +41,7 @@
 #include <cfloat>
 #include <cuda_runtime.h>
 
+#include "ffvgpu_async.cuh"
 #include "ffvgpu_internal.cuh"
 #include "ffvgpu_mixed.h"
 
@@ -44,7 +50,28 @@ namespace ffvgpu {
 namespace {
 
 constexpr int MT = 256;  // FP64 kernels: 16 cells per thread
-constexpr int PT = 512;  // FP32 sweep kernel: 8 cells per thread
+constexpr int PT = 512;  // sweep kernel: 8 cells per thread
+
+// Shared-memory tile of the sweep kernel: per colour a padded
+// [k + 1][j + 1][ii] array of FP64 iterate values, k, j in -1..16 and
+// ii = (i + 2) >> 1 for i in -1..16, with row pitch SP and plane pitch SQ;
+// the first guide layer sits in the padding, in the half of its own colour
+// (colour = (i + j + k) & 1).  With SQ = 2 mod 4 the two 8-cell groups of a
+// half-warp's 64-bit accesses (k groups 4 planes apart: 4 SQ = 8 mod 16
+// doubles) fall into disjoint banks.
+constexpr int SP = 10, SQ = 190, SH = 18 * SQ;
+constexpr int TILE = 2 * SH;
+constexpr int COEF_WORDS = 7 * 8 * PT;  // coefficient words of one block
+constexpr int SWEEP_SMEM = COEF_WORDS * 4 + TILE * 8 + 8 * PT * 8 + 16;
+
+__device__ __forceinline__ int tile_at(int i, int j, int k) {
+  return (k + 1) * SQ + (j + 1) * SP + ((i + 2) >> 1);
+}
+// Storage slot of sweep thread t's cell m (colour m >> 2, z plane 4 kg + (m & 3)).
+__host__ __device__ __forceinline__ int sweep_cell(int t, int m) {
+  const int ih = t & 7, kg = (t >> 3) & 3, j = t >> 5, c = m >> 2, h = m & 3;
+  return c * HALF_CELLS + ((4 * kg + h) * 16 + j) * 8 + ih;
+}
 
 __device__ __forceinline__ int active_instance(const MixCtx& C, int blk) {
   const int i = C.inst.blk_inst[blk];
@@ -223,20 +250,37 @@ __device__ __forceinline__ void stage_f32_as_f64(double* __restrict__ O, double*
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// FP32 coefficients of the sweeps: [blk][7][4096] = aw, ae, as, an, ab, at,
-// dinv, colour-split like every field.
+// 32-bit coefficients of the sweeps.  Each is the FP64 value rounded to 20
+// fraction bits (to nearest, ties away from zero) and stored as the high
+// word of that FP64 number, so widening it back is a register move:
+// aw, ae, as, an, ab, at and dinv = 1 / Ap (FP64 division, then rounded).
+// Per block the words are laid out in the sweep kernel's thread order,
+// [a][m][t] (coefficient a, the thread's cell m, thread t), 112 KB that one
+// bulk copy moves into shared memory.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t hi_round(double x) {
+  return (uint32_t)(((unsigned long long)__double_as_longlong(x) + 0x80000000ull) >> 32);
+}
+__device__ __forceinline__ double widen(uint32_t w) { return __hiloint2double((int)w, 0); }
+// The same inside the sweep loop, kept there: hoisting the 56 widened
+// coefficients out of the loop would need 112 registers.
+__device__ __forceinline__ double widen_here(uint32_t w) {
+  uint32_t v;
+  asm volatile("mov.b32 %0, %1;" : "=r"(v) : "r"(w));
+  return __hiloint2double((int)v, 0);
+}
+
 __global__ void __launch_bounds__(MT)
-mx_pack_kernel(int first, const double* __restrict__ A, float* __restrict__ coef) {
+mx_pack_kernel(int first, const double* __restrict__ A, uint32_t* __restrict__ coef) {
   const int blk = first + blockIdx.x;
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
-  float* cb = coef + (size_t)blk * 7 * BLOCK_CELLS;
-#pragma unroll 2
-  for (int m = 0; m < 16; ++m) {
-    const int s = threadIdx.x + MT * m;
+  uint32_t* cb = coef + (size_t)blk * COEF_WORDS;
+  for (int w = threadIdx.x; w < 8 * PT; w += MT) {
+    const int m = w / PT, t = w % PT;
+    const int s = sweep_cell(t, m);
 #pragma unroll
-    for (int a = 0; a < 6; ++a) cb[a * BLOCK_CELLS + s] = (float)Ab[(1 + a) * BLOCK_CELLS + s];
-    cb[6 * BLOCK_CELLS + s] = (float)(1.0 / Ab[s]);
+    for (int a = 0; a < 6; ++a) cb[(a * 8 + m) * PT + t] = hi_round(Ab[(1 + a) * BLOCK_CELLS + s]);
+    cb[(6 * 8 + m) * PT + t] = hi_round(1.0 / Ab[s]);
   }
 }
 
@@ -284,74 +328,157 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
 }
 
 // ---------------------------------------------------------------------------
-// One pass of FP32 sweeps.  MODE 0: right-hand side p (FFVILS.h:853-871:
-// p = r at the first iteration of a cycle, which also sets r0 = r, else
-// p = r + beta*(p + (-gamma)*q)); MODE 1: right-
-// hand side s = (-alpha)*q + r (FFVILS.h:898-903).  FIRST: the pass that
-// forms the right-hand side (writes p or s in FP64, and its FP32 copy when
-// more passes follow) and starts from e = 0 with zero guides.  LAST: writes
-// the preconditioned vector; otherwise the pass's iterate for the next.
+// One pass of sweeps.  MODE 0: right-hand side p (FFVILS.h:853-871: p = r
+// at the first iteration of a cycle, which also sets r0 = r, else
+// p = r + beta*(p + (-gamma)*q)); MODE 1: right-hand side s = (-alpha)*q + r
+// (FFVILS.h:898-903).  FIRST: the pass that forms the right-hand side
+// (written to pv in FP64) and starts from e = 0 with zero guides; later
+// passes read the right-hand side back from pv and start from ein with its
+// exchanged guide layer.  Every pass writes its iterate to eout in FP32.
+//
+// Thread t owns the k-column (ih, j, 4 kg .. 4 kg + 3) of both colours
+// (ih = t & 7, kg = (t >> 3) & 3, j = t >> 5): eight cells whose iterate
+// and coefficients stay in registers for the whole pass (the right-hand
+// side sits in shared memory in thread order).
+// Of a cell's six neighbours (all of the other colour) the one at the same
+// (ih, j) -- west or east by the row's parity -- and the z neighbours inside
+// the column are this thread's own registers; the rest come from the tile.
+// The next block's coefficients arrive by one bulk copy while this block
+// sweeps, and its vectors are prefetched into L2.
 // ---------------------------------------------------------------------------
-template <int MODE, bool FIRST, bool LAST>
+// T and V are written by other threads between the barriers: no __restrict__
+// on them, which would let the compiler move tile loads across
+// __syncthreads().
+__device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, int p0,
+                                           double (&E)[2][4],
+                                           const uint32_t (&cw)[8][7], double mom, int nsweep) {
+#pragma unroll 1
+  for (int it = 0; it < nsweep; ++it) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const int m = 4 * c + h;
+        const int par = p0 ^ ((h + c) & 1);  // x parity of the cell: i = 2 ih + par
+        const double* O = T + o0 + (1 - c) * SH + h * SQ;  // same (ih, j, k), other colour
+        // the x neighbour at the same ih is this thread's own; the other one is
+        // east (par 1) or west (par 0) of it in the tile
+        const double xo = O[par ? 1 : -1];
+        const double nw = par ? E[1 - c][h] : xo;
+        const double ne = par ? xo : E[1 - c][h];
+        const double ns = O[-SP], nn = O[SP];
+        const double nb = h > 0 ? E[1 - c][h - 1] : O[-SQ];
+        const double nt = h < 3 ? E[1 - c][h + 1] : O[SQ];
+        double rc = V[m * PT];
+        rc = __fma_rn(-widen_here(cw[m][0]), nw, rc);
+        rc = __fma_rn(-widen_here(cw[m][1]), ne, rc);
+        rc = __fma_rn(-widen_here(cw[m][2]), ns, rc);
+        rc = __fma_rn(-widen_here(cw[m][3]), nn, rc);
+        rc = __fma_rn(-widen_here(cw[m][4]), nb, rc);
+        rc = __fma_rn(-widen_here(cw[m][5]), nt, rc);
+        const double xt = __dmul_rn(rc, widen_here(cw[m][6]));
+        const double e = E[c][h];
+        const double en = __fma_rn(mom, __dsub_rn(e, xt), e);
+        E[c][h] = en;
+        T[o0 + c * SH + h * SQ] = en;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Tile address of the guide cell at position p (u + 16 v) of a face.
+__device__ __forceinline__ int guide_slot(int face, int p) {
+  const int u = p & 15, v = p >> 4, out = (face & 1) ? 16 : -1;
+  const int axis = face >> 1;
+  const int i = axis == 0 ? out : u;
+  const int j = axis == 0 ? u : (axis == 1 ? out : v);
+  const int k = axis == 2 ? out : v;
+  return ((i + j + k) & 1) * SH + tile_at(i, j, k);
+}
+
+constexpr int ROLE_SWEEP = 8;  // SolveState::timeout_where bit of this kernel's waits
+
+template <int MODE, bool FIRST>
 __global__ void __launch_bounds__(PT, 1)
 mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
                 double* __restrict__ r0, double* __restrict__ pv, const double* __restrict__ q,
-                const float* __restrict__ coef, float* __restrict__ v32,
-                const float* __restrict__ ein, float* __restrict__ eout) {
-  __shared__ float E[BLOCK_CELLS];
-  __shared__ float G[6 * FACE_CELLS];
+                const uint32_t* __restrict__ coef, const float* __restrict__ ein,
+                float* __restrict__ eout) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem);
+  double* T = reinterpret_cast<double*>(smem + COEF_WORDS * 4);
+  double* V = reinterpret_cast<double*>(smem + COEF_WORDS * 4 + TILE * 8);  // [m][t] rhs
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + COEF_WORDS * 4 + TILE * 8 + 8 * PT * 8);
+  __shared__ int abort_flag, s_inst;
   const int tid = threadIdx.x;
+  const int ih = tid & 7, kg = (tid >> 3) & 3, j = tid >> 5;
+  const int o0 = (4 * kg + 1) * SQ + (j + 1) * SP + ih + 1;  // tile slot of cell (c 0, h 0)
+  const int s0 = sweep_cell(tid, 0);                          // its storage slot
   const double mom = -(double)omega;
   const int n_act = *C.n_active;
-  for (int item = blockIdx.x; item < n_act; item += gridDim.x) {
+  BCSet hom;
+  for (int f = 0; f < 6; ++f) {
+    hom.type[f] = BC_DIRICHLET;
+    hom.value[f] = 0.0;
+  }
+  if (tid == 0) {
+    async::mbar_init(bar, 1);
+    async::fence_mbar_init();
+    abort_flag = 0;
+  }
+  if (FIRST)
+    for (int g = tid; g < TILE; g += PT) T[g] = 0.0;  // guides of e stay 0 in a first pass
+  __syncthreads();
+  int item = blockIdx.x;
+  if (tid == 0 && item < n_act) {
+    async::mbar_expect_tx(bar, COEF_WORDS * 4);
+    async::bulk_g2s(slot, coef + (size_t)C.active[item] * COEF_WORDS, COEF_WORDS * 4, bar);
+  }
+  uint32_t phase = 0;
+  for (; item < n_act; item += gridDim.x, phase ^= 1u) {
     const int blk = C.active[item];
-    const int inst = active_instance(C, blk);
-    if (inst < 0) continue;
-    const size_t base = (size_t)blk * BLOCK_CELLS;
-    // this thread's cells: storage slots tid + 512*m, colour m >> 2
-    float cf[8][7];
-    const float* cb = coef + (size_t)blk * 7 * BLOCK_CELLS;
-#pragma unroll
-    for (int m = 0; m < 8; ++m)
-#pragma unroll
-      for (int a = 0; a < 7; ++a) cf[m][a] = __ldg(cb + a * BLOCK_CELLS + tid + PT * m);
-    float v[8];
-    if (FIRST) {
+    if (tid == 0) s_inst = active_instance(C, blk);
+    __syncthreads();
+    const int inst = s_inst;  // one reading of the done flag for the whole CTA
+    const size_t base = (size_t)blk * BLOCK_CELLS + s0;
+    double E[2][4] = {};
+    if (inst >= 0 && FIRST) {
       const SolveState* S = C.inst.st + inst;
       const bool copy = S->cycle == 1;  // first iteration of a (re)start: p = r, r0 = r
       const double mgamma = -S->gamma, beta = S->beta, malpha = -S->alpha;
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const size_t s = base + tid + PT * m;
-        double rhs;
-        if (MODE == 0) {
-          if (copy) {
-            rhs = r[s];
-            r0[s] = rhs;
-          } else {
-            const double t = pv[s] + mgamma * q[s];
-            rhs = r[s] + beta * t;
-          }
-        } else {
-          rhs = malpha * q[s] + r[s];
-        }
-        pv[s] = rhs;
-        v[m] = (float)rhs;
-        if (!LAST) v32[s] = v[m];
-        E[tid + PT * m] = 0.0f;
-      }
-      for (int g = tid; g < 6 * FACE_CELLS; g += PT) G[g] = 0.0f;
-    } else {
+      for (int c = 0; c < 2; ++c)
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        v[m] = __ldg(v32 + base + tid + PT * m);
-        E[tid + PT * m] = __ldg(ein + base + tid + PT * m);
-      }
-      BCSet hom;
-      for (int f = 0; f < 6; ++f) {
-        hom.type[f] = BC_DIRICHLET;
-        hom.value[f] = 0.0;
-      }
+        for (int h = 0; h < 4; ++h) {
+          const size_t s = base + c * HALF_CELLS + h * 128;
+          double rhs;
+          if (MODE == 0) {
+            if (copy) {
+              rhs = r[s];
+              r0[s] = rhs;
+            } else {
+              const double t = pv[s] + mgamma * q[s];
+              rhs = r[s] + beta * t;
+            }
+          } else {
+            rhs = malpha * q[s] + r[s];
+          }
+          pv[s] = rhs;
+          V[(4 * c + h) * PT + tid] = rhs;
+          E[c][h] = 0.0;
+          T[o0 + c * SH + h * SQ] = 0.0;
+        }
+    } else if (inst >= 0) {
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const size_t s = base + c * HALF_CELLS + h * 128;
+          V[(4 * c + h) * PT + tid] = pv[s];
+          E[c][h] = (double)__ldg(ein + s);
+          T[o0 + c * SH + h * SQ] = E[c][h];
+        }
       const double dx = C.dx[blk];
       if (tid < 3 * 128) {
         const int f = 2 * (tid >> 7), p0 = tid & 127, p1 = p0 + 128;
@@ -359,38 +486,61 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
           const FaceNbr nb = C.nbr[blk * 6 + f + h];
           double g0, g1;
           guide_pair(ein, blk, f + h, p0, p1, nb, hom, dx, g0, g1);
-          G[(f + h) * FACE_CELLS + p0] = (float)g0;
-          G[(f + h) * FACE_CELLS + p1] = (float)g1;
+          T[guide_slot(f + h, p0)] = g0;
+          T[guide_slot(f + h, p1)] = g1;
         }
       }
     }
+    // this block's coefficients (the copy issued a block ago), then the next block's copy
+    async::mbar_wait(bar, phase, &abort_flag, ROLE_SWEEP);
+    uint32_t cw[8][7];
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+#pragma unroll
+      for (int a = 0; a < 7; ++a) cw[m][a] = slot[(a * 8 + m) * PT + tid];
+    async::fence_proxy_async();
     __syncthreads();
-#pragma unroll 1
-    for (int it = 0; it < nsweep; ++it) {
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          const int m = 4 * c + h;
-          const int qd = tid + PT * h;
-          const NbrsT<float> nb = split_neighbours(E + (1 - c) * HALF_CELLS, G, qd, c);
-          double rc = (double)v[m];
-          rc = __fma_rn(-(double)cf[m][0], (double)nb.w, rc);
-          rc = __fma_rn(-(double)cf[m][1], (double)nb.e, rc);
-          rc = __fma_rn(-(double)cf[m][2], (double)nb.s, rc);
-          rc = __fma_rn(-(double)cf[m][3], (double)nb.n, rc);
-          rc = __fma_rn(-(double)cf[m][4], (double)nb.b, rc);
-          rc = __fma_rn(-(double)cf[m][5], (double)nb.t, rc);
-          const double xt = __dmul_rn(rc, (double)cf[m][6]);
-          const double e = (double)E[c * HALF_CELLS + qd];
-          E[c * HALF_CELLS + qd] = __double2float_rn(__fma_rn(mom, __dsub_rn(e, xt), e));
+    if (abort_flag) {
+      // the copy never landed: stop every instance this CTA still had to
+      // sweep, give the copy a bounded time to drain, and leave
+      if (tid == 0) {
+        for (int it2 = item; it2 < n_act; it2 += gridDim.x) {
+          const int i2 = C.inst.blk_inst[C.active[it2]];
+          if (i2 < 0) continue;
+          atomicOr(&C.inst.st[i2].timeout_where, ROLE_SWEEP);
+          atomicExch(&C.inst.st[i2].status, 3);
+          atomicExch(&C.inst.st[i2].done, 1);
         }
-        __syncthreads();
+        for (uint32_t n = 0; n < (1u << 24) && !async::mbar_try_wait(bar, phase); ++n) {
+        }
+      }
+      return;
+    }
+    const int nxt = item + gridDim.x;
+    if (tid == 0 && nxt < n_act) {
+      const int nbk = C.active[nxt];
+      async::mbar_expect_tx(bar, COEF_WORDS * 4);
+      async::bulk_g2s(slot, coef + (size_t)nbk * COEF_WORDS, COEF_WORDS * 4, bar);
+      const size_t nbase = (size_t)nbk * BLOCK_CELLS;
+      if (FIRST) {
+        const int ni = C.inst.blk_inst[nbk];
+        const bool copy = MODE == 0 && ni >= 0 && C.inst.st[ni].cycle == 1;
+        async::prefetch_l2(r + nbase, BLOCK_CELLS * 8);
+        if (!copy) async::prefetch_l2(q + nbase, BLOCK_CELLS * 8);
+        if (MODE == 0 && !copy) async::prefetch_l2(pv + nbase, BLOCK_CELLS * 8);
+      } else {
+        async::prefetch_l2(pv + nbase, BLOCK_CELLS * 8);
+        async::prefetch_l2(ein + nbase, BLOCK_CELLS * 4);
       }
     }
+    if (inst < 0) continue;
+    __syncthreads();
+    run_sweeps(T, V + tid, o0, j & 1, E, cw, mom, nsweep);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) eout[base + tid + PT * m] = E[tid + PT * m];
-    __syncthreads();  // E and G are refilled for the next block
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+      for (int h = 0; h < 4; ++h)
+        eout[base + c * HALF_CELLS + h * 128] = __double2float_rn(E[c][h]);
   }
 }
 
@@ -476,7 +626,7 @@ mx_update_kernel(MixCtx C, double* __restrict__ x, const float* __restrict__ ph,
 // ---------------------------------------------------------------------------
 // Launchers.
 // ---------------------------------------------------------------------------
-void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, float* coef) {
+void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint32_t* coef) {
   mx_pack_kernel<<<count, MT, 0, s>>>(first, A, coef);
 }
 void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
@@ -484,34 +634,38 @@ void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
   mx_init_kernel<<<count, MT, 0, s>>>(C, x, gx, A, b, r, r0);
 }
 
-template <int MODE, bool FIRST, bool LAST>
+template <int MODE, bool FIRST>
 static void sweep_launch(cudaStream_t s, const MixCtx& C, int count, float omega, int nsweep,
                          const double* r, double* r0, double* pv, const double* q,
-                         const float* coef, float* v32, const float* ein, float* eout) {
-  mx_sweep_kernel<MODE, FIRST, LAST>
-      <<<count, PT, 0, s>>>(C, omega, nsweep, r, r0, pv, q, coef, v32, ein, eout);  // count: CTAs
+                         const uint32_t* coef, const float* ein, float* eout) {
+  mx_sweep_kernel<MODE, FIRST>
+      <<<count, PT, SWEEP_SMEM, s>>>(C, omega, nsweep, r, r0, pv, q, coef, ein, eout);
 }
 
-void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first, bool last,
+void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first,
                      float omega, int nsweep, const double* r, double* r0, double* pv,
-                     const double* q, const float* coef, float* v32, const float* ein,
-                     float* eout) {
-#define MX_CASE(M, F, L)                                                                   \
-  if (mode == M && first == F && last == L) {                                              \
-    sweep_launch<M, F, L>(s, C, count, omega, nsweep, r, r0, pv, q, coef, v32, ein, eout); \
-    return;                                                                                \
-  }
-  MX_CASE(0, true, true) MX_CASE(0, true, false) MX_CASE(0, false, true) MX_CASE(0, false, false)
-  MX_CASE(1, true, true) MX_CASE(1, true, false) MX_CASE(1, false, true) MX_CASE(1, false, false)
-#undef MX_CASE
+                     const double* q, const uint32_t* coef, const float* ein, float* eout) {
+  if (mode == 0 && first) sweep_launch<0, true>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, eout);
+  if (mode == 0 && !first) sweep_launch<0, false>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, eout);
+  if (mode == 1 && first) sweep_launch<1, true>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, eout);
+  if (mode == 1 && !first) sweep_launch<1, false>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, eout);
 }
 
 void mx_grid_sizes(int* sweep, int* matvec, int* update) {
   int dev = 0, sms = 0, a = 0, b = 0, c = 0, d = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, true>, PT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, true>, PT, 0);
+  // the sweep kernels' shared memory, on the calling device (before any launch)
+  cudaFuncSetAttribute(mx_sweep_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       SWEEP_SMEM);
+  cudaFuncSetAttribute(mx_sweep_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       SWEEP_SMEM);
+  cudaFuncSetAttribute(mx_sweep_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       SWEEP_SMEM);
+  cudaFuncSetAttribute(mx_sweep_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       SWEEP_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true>, PT, SWEEP_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false>, PT, SWEEP_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2>, MT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, mx_update_kernel, MT, 0);
   *sweep = sms * std::max(1, std::min(a, b));

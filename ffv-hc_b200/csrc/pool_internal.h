@@ -115,12 +115,11 @@ struct ffvgpu_pool {
   bool inst_dirty = true;            // host tables changed since the last upload
 
   // mixed form
-  float* mcoef = nullptr;   // [nb][7][4096] FP32 sweep coefficients
+  uint32_t* mcoef = nullptr;  // [nb][7][4096] 32-bit sweep coefficients (FP64 high words)
   float* me[2] = {nullptr, nullptr};
-  float* mv32 = nullptr;
   float* mph = nullptr;     // preconditioned p (p_)
   float* msh = nullptr;     // preconditioned s (s_)
-  int64_t mcoef_version = 0;  // sys_version the FP32 coefficients come from (one-grid pools)
+  int64_t mcoef_version = 0;  // sys_version the sweep coefficients come from (one-grid pools)
   double m_omega = 0.0;
   int m_sweeps = 0, m_per_exchange = 0;
   cudaGraphExec_t mgraph = nullptr;

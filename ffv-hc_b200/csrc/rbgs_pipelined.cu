@@ -35,6 +35,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "ffvgpu_async.cuh"
 #include "ffvgpu_internal.cuh"
 #include "ffvgpu_kernels.h"
 
@@ -55,7 +56,6 @@ constexpr int CONS0 = GATHER0 + 32 * GATHER_WARPS;
 constexpr int NTHREADS = CONS0 + 32 * CONSUMER_WARPS;  // 800
 constexpr int NCONS = 32 * CONSUMER_WARPS;            // one cell per consumer per slot
 constexpr int NGATHER = 32 * GATHER_WARPS;
-constexpr uint64_t WAIT_NS = 4000000000ull;  // a wait gives up after 4 s
 constexpr uint32_t DRAIN_LIMIT = 1u << 24;    // polls while draining copies in flight
 enum { ROLE_PRODUCER = 1, ROLE_GATHER = 2, ROLE_CONSUMER = 4 };
 
@@ -71,62 +71,8 @@ struct __align__(128) Smem {
   int last;
 };
 
-__device__ __forceinline__ uint32_t sa(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa(b)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sa(b)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(sa(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ uint64_t now_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-// Bounded wait; false when it gave up (recording its role) or another role aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag,
-                                          int role) {
-  if (mbar_try_wait(b, parity)) return true;
-  const uint64_t t0 = now_ns();
-  for (;;) {
-    if (mbar_try_wait(b, parity)) return true;
-    if (*abort_flag) return false;
-    if (now_ns() - t0 > WAIT_NS) {
-      atomicOr((int*)abort_flag, role);
-      return false;
-    }
-  }
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          sa(dst)),
-      "l"(src), "r"(bytes), "r"(sa(bar))
-      : "memory");
-}
-// Orders this thread's reads of shared memory before later async-proxy
-// (TMA) writes to it.  Buffers refilled by TMA must be released only after
-// it: without it a refill can overwrite data a lane is still reading.
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
+using namespace async;
+
 // The coefficients of one cell, read from a ring slot.
 struct Coef {
   double ap, aw, ae, as, an, ab, at, b;

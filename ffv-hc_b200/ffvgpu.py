@@ -94,7 +94,7 @@ class MixedParams(ctypes.Structure):
 
 
 # Restart settings of the mixed form used by default (see ffvgpu_mixed_params).
-RESTART = dict(restart_drop=1e-3, restart_growth=0.0, restart_every=0)
+RESTART = dict(restart_drop=1e-3, restart_growth=100.0, restart_every=0)
 
 
 class BatchDesc(ctypes.Structure):

@@ -304,18 +304,22 @@ int32_t ffvgpu_restart_filename(char* out, int32_t cap, const char* path, const 
 /* ---- mixed-precision form (no counterpart in the reference) -------------
  * FFVILS::BiCGSTAB's recurrence (src/FFV/FFVILS.h:793-974) in FP64 --
  * residuals, norms, dot products and the pressure update -- with the Jacobi
- * preconditioner (FFVILS.h:469-492) replaced by FP32 red-black SOR sweeps
- * from zero: 'sweeps' colour pairs per application, 'sweeps_per_exchange' of
- * them between guide-cell exchanges (each block sweeps on chip against
- * fixed guide values in between).  sweeps must be a multiple of
+ * preconditioner (FFVILS.h:469-492) replaced by red-black SOR sweeps on
+ * 32-bit data from zero: 'sweeps' colour pairs per application,
+ * 'sweeps_per_exchange' of them between guide-cell exchanges (each block
+ * sweeps on chip, in FP64 arithmetic, against fixed guide values in
+ * between; the coefficients are kept as 32-bit words and the iterate is
+ * stored in FP32 between exchanges).  sweeps must be a multiple of
  * sweeps_per_exchange.  Result fields as ffvgpu_solve_bicgstab; the solve
  * stops when sqrt(r.r / b.b) <= epsilon or after count_max iterations.
- * Rounding in FP32 makes the preconditioner slightly nonlinear, which
- * BiCGSTAB's recurrence does not tolerate for long (it stalls, then
- * diverges); restarts from the current residual every time it has fallen by
- * restart_drop (1e-3 works on the sphere grids) keep it converging. */
+ * BiCGSTAB's recurrence stalls on the sphere grids (the reference's own FP64
+ * BiCGSTAB stops by its breakdown test there) and the FP32 rounding of the
+ * preconditioned vectors adds to it; restarts from the current residual each
+ * time it has fallen by restart_drop (1e-3), and whenever it exceeds
+ * restart_growth (100) times the smallest since the last restart, keep it
+ * converging. */
 typedef struct {
-  double omega;                /* FP32 SOR relaxation factor */
+  double omega;                /* SOR relaxation factor of the sweeps */
   int32_t sweeps;              /* colour-pair sweeps per preconditioner application */
   int32_t sweeps_per_exchange; /* sweeps between guide-cell exchanges */
   int32_t count_max;

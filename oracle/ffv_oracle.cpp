@@ -1249,97 +1249,103 @@ int orc_bicgstab_restart(Oracle* O, double omega, int countPre, int countMax, do
 
 // ---------------------------------------------------------------------------
 // Mixed-precision form (no counterpart in the reference): orc_bicgstab's
-// recurrence (FFVILS.h:793-974) with Jacobi_PreConditioner replaced by FP32
-// red-black SOR sweeps from zero, 'per' sweeps between guide exchanges.
-// Restates ffv-hc_b200/csrc/kernels_mixed.cu:
-//   coefficients aw..at = (float)A*, dinv = (float)(1.0 / Ap); v = (float)rhs;
+// recurrence (FFVILS.h:793-974) with Jacobi_PreConditioner replaced by
+// red-black SOR sweeps from zero on 32-bit data, 'per' sweeps between guide
+// exchanges.  Restates ffv-hc_b200/csrc/kernels_mixed.cu:
+//   coefficients aw..at and dinv = 1.0 / Ap, each rounded to 20 fraction
+//   bits (the FP64 bit pattern plus 2^31, low word cleared) -- the 32-bit
+//   words the kernel keeps;
+//   per pass, the iterate in FP64: zero (interior and guides) in the first
+//   pass; later, the FP32 iterate of the previous pass widened and its
+//   first guide layer by the exchange (homogeneous Dirichlet outer faces),
+//   in FP64;
 //   per cell of colour c (colour 0 first, rbgs_smoother's order of terms),
-//   on those FP32 values in double arithmetic, rounded to float when stored:
+//   with the FP64 right-hand side v:
 //     rc = fma(-aw, eW, v) ... fma(-at, eT, rc); xt = rc * dinv;
-//     e = (float)fma(-omega, e - xt, e)
-//   guides of e: zero in the first group; later, the exchange of e (as
-//   double) with homogeneous Dirichlet outer faces, rounded to float.
+//     e = fma(-omega, e - xt, e)
+//   at the end of a pass the iterate is rounded to FP32.
 // The preconditioned vectors' guides come from the pressure-BC exchange
 // before CalcAx, and every dot product is DOT.
 // ---------------------------------------------------------------------------
 namespace {
 
 struct Coef32 {
-  std::vector<float> a[7];  // aw, ae, as, an, ab, at, dinv; reference layout
+  std::vector<double> a[7];  // aw, ae, as, an, ab, at, dinv (rounded); reference layout
 };
+
+double round_hi(double x) {
+  uint64_t u;
+  std::memcpy(&u, &x, 8);
+  u = (u + 0x80000000ull) & 0xFFFFFFFF00000000ull;
+  double d;
+  std::memcpy(&d, &u, 8);
+  return d;
+}
 
 void mixed_coef(Oracle& O, Coef32& C) {
   const long N = (long)O.G.nb * O.G.nc;
   const int src[6] = {OF_AW, OF_AE, OF_AS, OF_AN, OF_AB, OF_AT};
-  for (int a = 0; a < 7; ++a) C.a[a].assign(N, 0.0f);
+  for (int a = 0; a < 7; ++a) C.a[a].assign(N, 0.0);
   for (int bi = 0; bi < O.G.nb; ++bi)
     for (long m = 0; m < O.G.nc; ++m) {
       const long g = (long)bi * O.G.nc + m;
-      for (int a = 0; a < 6; ++a) C.a[a][g] = (float)O.F(src[a], bi)[m];
-      C.a[6][g] = (float)(1.0 / O.F(OF_AP, bi)[m]);
+      for (int a = 0; a < 6; ++a) C.a[a][g] = round_hi(O.F(src[a], bi)[m]);
+      C.a[6][g] = round_hi(1.0 / O.F(OF_AP, bi)[m]);
     }
 }
 
-// out = M(v): FP32 sweeps, result widened to double (interior).
+// out = M(v), widened to double (interior).  The pass's FP64 iterate with
+// its guide layer lives in the scratch field Z.
 void mixed_precondition(Oracle& O, const Coef32& C, int fv, int fout, float omega, int sweeps,
                         int per) {
   Grid& G = O.G;
   const int n = G.n;
   const long sy = n + 2 * G.g, sz = sy * sy;
   const long N = (long)G.nb * G.nc;
-  std::vector<float> e(N, 0.0f), v(N, 0.0f);
-  for (int bi = 0; bi < G.nb; ++bi)
-    for (long m = 0; m < G.nc; ++m) v[(long)bi * G.nc + m] = (float)O.F(fv, bi)[m];
+  std::vector<float> e(N, 0.0f);  // the iterate between passes (interior)
   const int hom_t[6] = {BC_DIRICHLET, BC_DIRICHLET, BC_DIRICHLET,
                         BC_DIRICHLET, BC_DIRICHLET, BC_DIRICHLET};
   const double hom_v[6] = {0, 0, 0, 0, 0, 0};
   for (int ps = 0; ps < sweeps / per; ++ps) {
-    if (ps > 0) {
-      // guide layer 1 of e through the exchange, in double
-      for (int bi = 0; bi < G.nb; ++bi) {
-        double* z = O.F(OF_Z, bi);
-        for (long m = 0; m < G.nc; ++m) z[m] = (double)e[(long)bi * G.nc + m];
-      }
-      impose_bc(O, OF_Z, hom_t, hom_v);
-      for (int bi = 0; bi < G.nb; ++bi) {
-        const double* z = O.F(OF_Z, bi);
-        float* eb = e.data() + (long)bi * G.nc;
-        for (int k = 0; k <= n + 1; ++k)
-          for (int j = 0; j <= n + 1; ++j)
-            for (int i = 0; i <= n + 1; ++i) {
-              const int out = (i == 0 || i == n + 1) + (j == 0 || j == n + 1) +
-                              (k == 0 || k == n + 1);
-              if (out != 1) continue;  // face guide cells of layer 1 only
-              const long m = IDX(G, i, j, k);
-              eb[m] = (float)z[m];
-            }
-      }
+    for (int bi = 0; bi < G.nb; ++bi) {
+      double* z = O.F(OF_Z, bi);
+      for (long m = 0; m < G.nc; ++m) z[m] = (ps == 0) ? 0.0 : (double)e[(long)bi * G.nc + m];
     }
+    if (ps > 0) impose_bc(O, OF_Z, hom_t, hom_v);  // guide layer 1 of the iterate, in double
     for (int it = 0; it < per; ++it)
       for (int c = 0; c < 2; ++c) {
 #pragma omp parallel for num_threads(O.nthreads) schedule(static)
         for (int bi = 0; bi < G.nb; ++bi) {
-          float* eb = e.data() + (long)bi * G.nc;
-          const float* vb = v.data() + (long)bi * G.nc;
+          double* eb = O.F(OF_Z, bi);
+          const double* vb = O.F(fv, bi);
           const long o = (long)bi * G.nc;
           for (int k = 1; k <= n; ++k)
             for (int j = 1; j <= n; ++j)
               for (int i = 1; i <= n; ++i) {
                 if ((((i - 1) + (j - 1) + (k - 1)) & 1) != c) continue;
                 const long m = IDX(G, i, j, k);
-                double rc = (double)vb[m];
-                rc = std::fma(-(double)C.a[0][o + m], (double)eb[m - 1], rc);
-                rc = std::fma(-(double)C.a[1][o + m], (double)eb[m + 1], rc);
-                rc = std::fma(-(double)C.a[2][o + m], (double)eb[m - sy], rc);
-                rc = std::fma(-(double)C.a[3][o + m], (double)eb[m + sy], rc);
-                rc = std::fma(-(double)C.a[4][o + m], (double)eb[m - sz], rc);
-                rc = std::fma(-(double)C.a[5][o + m], (double)eb[m + sz], rc);
-                const double xt = rc * (double)C.a[6][o + m];
-                const double ev = (double)eb[m];
-                eb[m] = (float)std::fma(-(double)omega, ev - xt, ev);
+                double rc = vb[m];
+                rc = std::fma(-C.a[0][o + m], eb[m - 1], rc);
+                rc = std::fma(-C.a[1][o + m], eb[m + 1], rc);
+                rc = std::fma(-C.a[2][o + m], eb[m - sy], rc);
+                rc = std::fma(-C.a[3][o + m], eb[m + sy], rc);
+                rc = std::fma(-C.a[4][o + m], eb[m - sz], rc);
+                rc = std::fma(-C.a[5][o + m], eb[m + sz], rc);
+                const double xt = rc * C.a[6][o + m];
+                const double ev = eb[m];
+                eb[m] = std::fma(-(double)omega, ev - xt, ev);
               }
         }
       }
+    for (int bi = 0; bi < G.nb; ++bi) {
+      const double* z = O.F(OF_Z, bi);
+      for (int k = 1; k <= n; ++k)
+        for (int j = 1; j <= n; ++j)
+          for (int i = 1; i <= n; ++i) {
+            const long m = IDX(G, i, j, k);
+            e[(long)bi * G.nc + m] = (float)z[m];
+          }
+    }
   }
   for (int bi = 0; bi < G.nb; ++bi) {
     double* out = O.F(fout, bi);

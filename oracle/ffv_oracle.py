@@ -191,8 +191,8 @@ class Oracle:
                                           float(epsilon)), count_max)
 
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-                    epsilon=1e-8, restart_drop=1e-3, restart_growth=0.0, restart_every=0):
-        """Mixed-precision form: BiCGSTAB with FP32 RB-SOR preconditioning."""
+                    epsilon=1e-8, restart_drop=1e-3, restart_growth=100.0, restart_every=0):
+        """Mixed-precision form: BiCGSTAB with RB-SOR preconditioning on 32-bit data."""
         return self._solve(lib().orc_mixed, (float(omega), int(sweeps), int(sweeps_per_exchange),
                                              int(count_max), float(epsilon), float(restart_drop),
                                              float(restart_growth), int(restart_every)),

@@ -23,6 +23,8 @@ pytestmark = pytest.mark.gpu
     (2, 1.5, 8, 4, 8),
     (2, 1.2, 6, 2, 6),
     (1, 1.5, 3, 1, 6),
+    (3, 1.5, 8, 4, 3),   # 548 blocks: several blocks per CTA (coefficient copy pipeline)
+    (3, 1.2, 6, 2, 2),
 ])
 def test_mixed_solve_bitwise_against_oracle(level, omega, sweeps, per, count):
     g, inp, O = problem(level)
