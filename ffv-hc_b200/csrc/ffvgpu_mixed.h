@@ -25,7 +25,7 @@ struct MixCtx {
 };
 
 // CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel.
-void mx_grid_sizes(int* sweep, int* matvec, int* update);
+void mx_grid_sizes(int* sweep, int* matvec, int* update, int* guides);
 // 32-bit sweep coefficients of blocks [first, first + count): [blk][7][8][512]
 // words (FP64 high words, rounded), MIXED_COEF_WORDS per block.
 constexpr int MIXED_COEF_WORDS = 7 * 8 * 512;
@@ -33,9 +33,15 @@ void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint3
 void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
                     const double* gx, const double* A, const double* b, double* r, double* r0);
 // The iteration launchers take 'count' = CTAs of the persistent grid.
+// One pass of sweeps; a later pass (first false) takes ein and its guide
+// layer, written by launch_mx_guides.
 void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first,
                      float omega, int nsweep, const double* r, double* r0, double* pv,
-                     const double* q, const uint32_t* coef, const float* ein, float* eout);
+                     const double* q, const uint32_t* coef, const float* ein,
+                     const double* guides, float* eout);
+// Guide layer [blk][6][256] (FP64) of the FP32 iterate e for the next pass.
+void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const float* e,
+                      double* guides);
 void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, const float* x,
                       const double* A, double* y, const double* w0);
 void launch_mx_update(cudaStream_t s, const MixCtx& C, int count, double* x, const float* ph,

@@ -36,7 +36,7 @@ void release_instances(ffvgpu_pool* P) {
   if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
   P->mgraph = nullptr;
   void* ptrs[] = {P->blk_inst_d, P->inst_first_d, P->inst_count_d, P->blk_geo_d, P->mst,
-                  P->mpartials, P->mhist, P->mcoef, P->me[0], P->me[1], P->mph,
+                  P->mpartials, P->mhist, P->mcoef, P->mguide, P->me[0], P->me[1], P->mph,
                   P->msh};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -123,9 +123,10 @@ ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P) {
       CK(cudaEventCreateWithFlags(&P->act_ev[k], cudaEventDisableTiming));
       CK(cudaEventRecord(P->act_ev[k], P->stream));
     }
-    mx_grid_sizes(&P->grid_sweep, &P->grid_matvec, &P->grid_update);
+    mx_grid_sizes(&P->grid_sweep, &P->grid_matvec, &P->grid_update, &P->grid_guides);
   }
-  if ((s = dalloc_t(P, &P->mcoef, 7 * n)) || (s = dalloc_t(P, &P->me[0], n)) ||
+  if ((s = dalloc_t(P, &P->mcoef, 7 * n)) || (s = dalloc_t(P, &P->mguide, n / BC * 6 * 256)) ||
+      (s = dalloc_t(P, &P->me[0], n)) ||
       (s = dalloc_t(P, &P->me[1], n)) || (s = dalloc_t(P, &P->mph, n)) ||
       (s = dalloc_t(P, &P->msh, n)) ||
       (s = dalloc_t(P, &P->r, n)) || (s = dalloc_t(P, &P->r0, n)) || (s = dalloc_t(P, &P->p, n)) ||
@@ -211,9 +212,10 @@ void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
     float* hat = mode == 0 ? P->mph : P->msh;
     for (int ps = 0; ps < passes; ++ps) {
       const bool last = ps == passes - 1;
+      const float* ein = ps > 0 ? P->me[(ps - 1) & 1] : nullptr;
+      if (ps > 0) launch_mx_guides(s, C, P->grid_guides, ein, P->mguide);
       launch_mx_sweep(s, C, P->grid_sweep, mode, ps == 0, om, P->m_per_exchange, P->r, P->r0,
-                      rhs, P->q, P->mcoef, ps > 0 ? P->me[(ps - 1) & 1] : nullptr,
-                      last ? hat : P->me[ps & 1]);
+                      rhs, P->q, P->mcoef, ein, P->mguide, last ? hat : P->me[ps & 1]);
     }
     if (mode == 0)
       launch_mx_matvec(s, C, P->grid_matvec, 1, P->mph, P->A, P->q, P->r0);
@@ -224,7 +226,8 @@ void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
 }
 
 int launches_per_iteration(const ffvgpu_pool* P) {
-  return 2 * (P->m_sweeps / P->m_per_exchange) + 3;
+  const int passes = P->m_sweeps / P->m_per_exchange;
+  return 2 * passes + 2 * (passes - 1) + 3;  // sweeps, guide layers, A*x (2), update
 }
 
 ffvgpu_status result_status(const ffvgpu_result& R, int status_code, double eps, int count_max) {

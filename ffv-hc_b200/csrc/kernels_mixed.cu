@@ -62,8 +62,13 @@ constexpr int PT = 512;  // sweep kernel: 8 cells per thread
 constexpr int SP = 10, SQ = 190, SH = 18 * SQ;
 constexpr int TILE = 2 * SH;
 constexpr int COEF_WORDS = 7 * 8 * PT;  // coefficient words of one block
-constexpr int SWEEP_SMEM = COEF_WORDS * 4 + TILE * 8 + 8 * PT * 8 + 16;
+constexpr int GUIDES = 6 * FACE_CELLS;  // guide values of one block (FP64)
+constexpr int SWEEP_SMEM = COEF_WORDS * 4 + TILE * 8 + 8 * PT * 8 + GUIDES * 8 + 16;
 
+// Word of coefficient a of sweep thread t's cell m within a block.
+__device__ __forceinline__ int coef_word(int a, int m, int t) {
+  return ((a * 2 + (m >> 2)) * PT + t) * 4 + (m & 3);
+}
 __device__ __forceinline__ int tile_at(int i, int j, int k) {
   return (k + 1) * SQ + (j + 1) * SP + ((i + 2) >> 1);
 }
@@ -255,8 +260,9 @@ __device__ __forceinline__ void stage_f32_as_f64(double* __restrict__ O, double*
 // word of that FP64 number, so widening it back is a register move:
 // aw, ae, as, an, ab, at and dinv = 1 / Ap (FP64 division, then rounded).
 // Per block the words are laid out in the sweep kernel's thread order,
-// [a][m][t] (coefficient a, the thread's cell m, thread t), 112 KB that one
-// bulk copy moves into shared memory.
+// [a][m / 4][t][m % 4] (coefficient a, the thread's cell m, thread t): 112 KB
+// that one bulk copy moves into shared memory, where each thread reads its
+// words as 14 16-byte vectors.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t hi_round(double x) {
   return (uint32_t)(((unsigned long long)__double_as_longlong(x) + 0x80000000ull) >> 32);
@@ -279,8 +285,8 @@ mx_pack_kernel(int first, const double* __restrict__ A, uint32_t* __restrict__ c
     const int m = w / PT, t = w % PT;
     const int s = sweep_cell(t, m);
 #pragma unroll
-    for (int a = 0; a < 6; ++a) cb[(a * 8 + m) * PT + t] = hi_round(Ab[(1 + a) * BLOCK_CELLS + s]);
-    cb[(6 * 8 + m) * PT + t] = hi_round(1.0 / Ab[s]);
+    for (int a = 0; a < 6; ++a) cb[coef_word(a, m, t)] = hi_round(Ab[(1 + a) * BLOCK_CELLS + s]);
+    cb[coef_word(6, m, t)] = hi_round(1.0 / Ab[s]);
   }
 }
 
@@ -356,27 +362,41 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
   for (int it = 0; it < nsweep; ++it) {
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
+      // the four cells of this colour advance term by term, so their
+      // dependent FP64 chains overlap (each chain keeps its own order)
+      const double* O = T + o0 + (1 - c) * SH;  // cell h: O + h SQ, same (ih, j, k), other colour
+      double rc[4], xo[4];
 #pragma unroll
       for (int h = 0; h < 4; ++h) {
-        const int m = 4 * c + h;
         const int par = p0 ^ ((h + c) & 1);  // x parity of the cell: i = 2 ih + par
-        const double* O = T + o0 + (1 - c) * SH + h * SQ;  // same (ih, j, k), other colour
-        // the x neighbour at the same ih is this thread's own; the other one is
-        // east (par 1) or west (par 0) of it in the tile
-        const double xo = O[par ? 1 : -1];
-        const double nw = par ? E[1 - c][h] : xo;
-        const double ne = par ? xo : E[1 - c][h];
-        const double ns = O[-SP], nn = O[SP];
-        const double nb = h > 0 ? E[1 - c][h - 1] : O[-SQ];
-        const double nt = h < 3 ? E[1 - c][h + 1] : O[SQ];
-        double rc = V[m * PT];
-        rc = __fma_rn(-widen_here(cw[m][0]), nw, rc);
-        rc = __fma_rn(-widen_here(cw[m][1]), ne, rc);
-        rc = __fma_rn(-widen_here(cw[m][2]), ns, rc);
-        rc = __fma_rn(-widen_here(cw[m][3]), nn, rc);
-        rc = __fma_rn(-widen_here(cw[m][4]), nb, rc);
-        rc = __fma_rn(-widen_here(cw[m][5]), nt, rc);
-        const double xt = __dmul_rn(rc, widen_here(cw[m][6]));
+        // the x neighbour at the same ih is this thread's own; the other one
+        // is east (par 1) or west (par 0) of it in the tile
+        xo[h] = O[h * SQ + (par ? 1 : -1)];
+        rc[h] = V[(4 * c + h) * PT];
+      }
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const int par = p0 ^ ((h + c) & 1);
+        rc[h] = __fma_rn(-widen_here(cw[4 * c + h][0]), par ? E[1 - c][h] : xo[h], rc[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const int par = p0 ^ ((h + c) & 1);
+        rc[h] = __fma_rn(-widen_here(cw[4 * c + h][1]), par ? xo[h] : E[1 - c][h], rc[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < 4; ++h) rc[h] = __fma_rn(-widen_here(cw[4 * c + h][2]), O[h * SQ - SP], rc[h]);
+#pragma unroll
+      for (int h = 0; h < 4; ++h) rc[h] = __fma_rn(-widen_here(cw[4 * c + h][3]), O[h * SQ + SP], rc[h]);
+#pragma unroll
+      for (int h = 0; h < 4; ++h)
+        rc[h] = __fma_rn(-widen_here(cw[4 * c + h][4]), h > 0 ? E[1 - c][h - 1] : O[-SQ], rc[h]);
+#pragma unroll
+      for (int h = 0; h < 4; ++h)
+        rc[h] = __fma_rn(-widen_here(cw[4 * c + h][5]), h < 3 ? E[1 - c][h + 1] : O[4 * SQ], rc[h]);
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const double xt = __dmul_rn(rc[h], widen_here(cw[4 * c + h][6]));
         const double e = E[c][h];
         const double en = __fma_rn(mom, __dsub_rn(e, xt), e);
         E[c][h] = en;
@@ -399,29 +419,39 @@ __device__ __forceinline__ int guide_slot(int face, int p) {
 
 constexpr int ROLE_SWEEP = 8;  // SolveState::timeout_where bit of this kernel's waits
 
+// Called by a whole warp: the first item from, from + gridDim.x, ... (below
+// n_act) whose block belongs to an instance still solving, or n_act; 32
+// candidates per round.
+__device__ __forceinline__ int next_live(const MixCtx& C, int from, int n_act, int lane) {
+  for (int b = from; b < n_act; b += 32 * gridDim.x) {
+    const int it = b + lane * gridDim.x;
+    const bool live = it < n_act && active_instance(C, C.active[it]) >= 0;
+    const unsigned m = __ballot_sync(0xffffffffu, live);
+    if (m) return b + (__ffs(m) - 1) * gridDim.x;
+  }
+  return n_act;
+}
+
 template <int MODE, bool FIRST>
 __global__ void __launch_bounds__(PT, 1)
 mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
                 double* __restrict__ r0, double* __restrict__ pv, const double* __restrict__ q,
                 const uint32_t* __restrict__ coef, const float* __restrict__ ein,
-                float* __restrict__ eout) {
+                const double* __restrict__ guides, float* __restrict__ eout) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t* slot = reinterpret_cast<uint32_t*>(smem);
   double* T = reinterpret_cast<double*>(smem + COEF_WORDS * 4);
   double* V = reinterpret_cast<double*>(smem + COEF_WORDS * 4 + TILE * 8);  // [m][t] rhs
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + COEF_WORDS * 4 + TILE * 8 + 8 * PT * 8);
-  __shared__ int abort_flag, s_inst;
+  double* GB = V + 8 * PT;  // [face][p] guides of the block, copied with its coefficients
+  uint64_t* bar = reinterpret_cast<uint64_t*>(GB + GUIDES);
+  constexpr uint32_t COPY_BYTES = COEF_WORDS * 4 + (FIRST ? 0 : GUIDES * 8);
+  __shared__ int abort_flag, s_item[2], s_blk[2], s_inst[2];  // [copy parity]
   const int tid = threadIdx.x;
   const int ih = tid & 7, kg = (tid >> 3) & 3, j = tid >> 5;
   const int o0 = (4 * kg + 1) * SQ + (j + 1) * SP + ih + 1;  // tile slot of cell (c 0, h 0)
   const int s0 = sweep_cell(tid, 0);                          // its storage slot
   const double mom = -(double)omega;
   const int n_act = *C.n_active;
-  BCSet hom;
-  for (int f = 0; f < 6; ++f) {
-    hom.type[f] = BC_DIRICHLET;
-    hom.value[f] = 0.0;
-  }
   if (tid == 0) {
     async::mbar_init(bar, 1);
     async::fence_mbar_init();
@@ -430,17 +460,33 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
   if (FIRST)
     for (int g = tid; g < TILE; g += PT) T[g] = 0.0;  // guides of e stay 0 in a first pass
   __syncthreads();
-  int item = blockIdx.x;
-  if (tid == 0 && item < n_act) {
-    async::mbar_expect_tx(bar, COEF_WORDS * 4);
-    async::bulk_g2s(slot, coef + (size_t)C.active[item] * COEF_WORDS, COEF_WORDS * 4, bar);
+  // The CTA visits the live items blockIdx.x + n gridDim.x of the active
+  // list (blocks of instances still solving); warp 0 finds the next one a
+  // block ahead and issues its coefficient copy, so blocks of instances that
+  // have stopped cost neither a copy nor a wait.
+  if (tid < 32) {
+    const int it0 = next_live(C, blockIdx.x, n_act, tid);
+    if (tid == 0) {
+      s_item[0] = it0;
+      if (it0 < n_act) {
+        const int b0 = C.active[it0];
+        async::mbar_expect_tx(bar, COPY_BYTES);
+        async::bulk_g2s(slot, coef + (size_t)b0 * COEF_WORDS, COEF_WORDS * 4, bar);
+        if (!FIRST) async::bulk_g2s(GB, guides + (size_t)b0 * GUIDES, GUIDES * 8, bar);
+        s_blk[0] = b0;
+        s_inst[0] = active_instance(C, b0);
+      }
+    }
   }
-  uint32_t phase = 0;
-  for (; item < n_act; item += gridDim.x, phase ^= 1u) {
-    const int blk = C.active[item];
-    if (tid == 0) s_inst = active_instance(C, blk);
+  uint32_t phase = 0;  // parity of the copy the current item waits on
+  for (;; phase ^= 1u) {
+    // item, block and instance were found a block ahead (when its copy was
+    // issued): one reading of the done flag for the whole CTA, off the
+    // block's critical path (the flag changes between launches only)
     __syncthreads();
-    const int inst = s_inst;  // one reading of the done flag for the whole CTA
+    const int item = s_item[phase];
+    if (item >= n_act) break;
+    const int blk = s_blk[phase], inst = s_inst[phase];
     const size_t base = (size_t)blk * BLOCK_CELLS + s0;
     double E[2][4] = {};
     if (inst >= 0 && FIRST) {
@@ -479,25 +525,24 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
           E[c][h] = (double)__ldg(ein + s);
           T[o0 + c * SH + h * SQ] = E[c][h];
         }
-      const double dx = C.dx[blk];
-      if (tid < 3 * 128) {
-        const int f = 2 * (tid >> 7), p0 = tid & 127, p1 = p0 + 128;
-        for (int h = 0; h < 2; ++h) {
-          const FaceNbr nb = C.nbr[blk * 6 + f + h];
-          double g0, g1;
-          guide_pair(ein, blk, f + h, p0, p1, nb, hom, dx, g0, g1);
-          T[guide_slot(f + h, p0)] = g0;
-          T[guide_slot(f + h, p1)] = g1;
-        }
-      }
     }
-    // this block's coefficients (the copy issued a block ago), then the next block's copy
+    // this block's coefficients and guides (the copy issued a block ago),
+    // then the next block's copy
     async::mbar_wait(bar, phase, &abort_flag, ROLE_SWEEP);
+    if (!FIRST && inst >= 0)
+#pragma unroll
+      for (int g = tid; g < GUIDES; g += PT) T[guide_slot(g >> 8, g & 255)] = GB[g];
     uint32_t cw[8][7];
 #pragma unroll
-    for (int m = 0; m < 8; ++m)
+    for (int a = 0; a < 7; ++a)
 #pragma unroll
-      for (int a = 0; a < 7; ++a) cw[m][a] = slot[(a * 8 + m) * PT + tid];
+      for (int hq = 0; hq < 2; ++hq) {
+        const uint4 w = reinterpret_cast<const uint4*>(slot)[(a * 2 + hq) * PT + tid];
+        cw[4 * hq + 0][a] = w.x;
+        cw[4 * hq + 1][a] = w.y;
+        cw[4 * hq + 2][a] = w.z;
+        cw[4 * hq + 3][a] = w.w;
+      }
     async::fence_proxy_async();
     __syncthreads();
     if (abort_flag) {
@@ -516,11 +561,15 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       }
       return;
     }
-    const int nxt = item + gridDim.x;
+    const int nxt = tid < 32 ? next_live(C, item + gridDim.x, n_act, tid) : n_act;
+    if (tid == 0) s_item[phase ^ 1u] = nxt;
     if (tid == 0 && nxt < n_act) {
       const int nbk = C.active[nxt];
-      async::mbar_expect_tx(bar, COEF_WORDS * 4);
+      async::mbar_expect_tx(bar, COPY_BYTES);
       async::bulk_g2s(slot, coef + (size_t)nbk * COEF_WORDS, COEF_WORDS * 4, bar);
+      if (!FIRST) async::bulk_g2s(GB, guides + (size_t)nbk * GUIDES, GUIDES * 8, bar);
+      s_blk[phase ^ 1u] = nbk;
+      s_inst[phase ^ 1u] = active_instance(C, nbk);
       const size_t nbase = (size_t)nbk * BLOCK_CELLS;
       if (FIRST) {
         const int ni = C.inst.blk_inst[nbk];
@@ -534,13 +583,46 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       }
     }
     if (inst < 0) continue;
-    __syncthreads();
     run_sweeps(T, V + tid, o0, j & 1, E, cw, mom, nsweep);
 #pragma unroll
     for (int c = 0; c < 2; ++c)
 #pragma unroll
       for (int h = 0; h < 4; ++h)
         eout[base + c * HALF_CELLS + h * 128] = __double2float_rn(E[c][h]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Guide layer of an FP32 iterate for the next sweep pass: per live block the
+// first guide layer by the exchange rules (same-level copy, 2:1
+// interpolation and restriction, src/CGMfuncs/sup.f90) evaluated in FP64,
+// homogeneous Dirichlet values on outer faces; [blk][face][p] FP64, which
+// the sweep kernel bulk-copies with the block's coefficients.
+// ---------------------------------------------------------------------------
+constexpr int GT = MT;  // guides kernel: three pairs (face, p, p + 128) per thread
+
+__global__ void __launch_bounds__(GT)
+mx_guides_kernel(MixCtx C, const float* __restrict__ e, double* __restrict__ guides) {
+  BCSet hom;
+  for (int f = 0; f < 6; ++f) {
+    hom.type[f] = BC_DIRICHLET;
+    hom.value[f] = 0.0;
+  }
+  const int n_act = *C.n_active;
+  for (int item = blockIdx.x; item < n_act; item += gridDim.x) {
+    const int blk = C.active[item];
+    if (active_instance(C, blk) < 0) continue;
+    const double dx = C.dx[blk];
+    double* gb = guides + (size_t)blk * GUIDES;
+#pragma unroll 1
+    for (int w = threadIdx.x; w < 3 * FACE_CELLS; w += GT) {
+      const int f = w >> 7, p0 = w & 127, p1 = p0 + 128;
+      const FaceNbr nb = C.nbr[blk * 6 + f];
+      double g0, g1;
+      guide_pair(e, blk, f, p0, p1, nb, hom, dx, g0, g1);
+      gb[f * FACE_CELLS + p0] = g0;
+      gb[f * FACE_CELLS + p1] = g1;
+    }
   }
 }
 
@@ -637,21 +719,30 @@ void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
 template <int MODE, bool FIRST>
 static void sweep_launch(cudaStream_t s, const MixCtx& C, int count, float omega, int nsweep,
                          const double* r, double* r0, double* pv, const double* q,
-                         const uint32_t* coef, const float* ein, float* eout) {
+                         const uint32_t* coef, const float* ein, const double* guides,
+                         float* eout) {
   mx_sweep_kernel<MODE, FIRST>
-      <<<count, PT, SWEEP_SMEM, s>>>(C, omega, nsweep, r, r0, pv, q, coef, ein, eout);
+      <<<count, PT, SWEEP_SMEM, s>>>(C, omega, nsweep, r, r0, pv, q, coef, ein, guides, eout);
 }
 
 void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first,
                      float omega, int nsweep, const double* r, double* r0, double* pv,
-                     const double* q, const uint32_t* coef, const float* ein, float* eout) {
-  if (mode == 0 && first) sweep_launch<0, true>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, eout);
-  if (mode == 0 && !first) sweep_launch<0, false>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, eout);
-  if (mode == 1 && first) sweep_launch<1, true>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, eout);
-  if (mode == 1 && !first) sweep_launch<1, false>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, eout);
+                     const double* q, const uint32_t* coef, const float* ein,
+                     const double* guides, float* eout) {
+#define MX_SWEEP(M, F) sweep_launch<M, F>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, guides, eout)
+  if (mode == 0 && first) MX_SWEEP(0, true);
+  if (mode == 0 && !first) MX_SWEEP(0, false);
+  if (mode == 1 && first) MX_SWEEP(1, true);
+  if (mode == 1 && !first) MX_SWEEP(1, false);
+#undef MX_SWEEP
 }
 
-void mx_grid_sizes(int* sweep, int* matvec, int* update) {
+void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const float* e,
+                      double* guides) {
+  mx_guides_kernel<<<count, GT, 0, s>>>(C, e, guides);
+}
+
+void mx_grid_sizes(int* sweep, int* matvec, int* update, int* guides) {
   int dev = 0, sms = 0, a = 0, b = 0, c = 0, d = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -669,6 +760,9 @@ void mx_grid_sizes(int* sweep, int* matvec, int* update) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2>, MT, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, mx_update_kernel, MT, 0);
   *sweep = sms * std::max(1, std::min(a, b));
+  int g = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, mx_guides_kernel, GT, 0);
+  *guides = sms * std::max(1, g);
   *matvec = sms * std::max(1, c);
   *update = sms * std::max(1, d);
 }

@@ -116,6 +116,7 @@ struct ffvgpu_pool {
 
   // mixed form
   uint32_t* mcoef = nullptr;  // [nb][7][4096] 32-bit sweep coefficients (FP64 high words)
+  double* mguide = nullptr;   // [nb][6][256] guide layer of the sweep iterate between passes
   float* me[2] = {nullptr, nullptr};
   float* mph = nullptr;     // preconditioned p (p_)
   float* msh = nullptr;     // preconditioned s (s_)
@@ -134,7 +135,7 @@ struct ffvgpu_pool {
   int32_t* act_h[2] = {nullptr, nullptr};
   cudaEvent_t act_ev[2] = {nullptr, nullptr};
   int act_next = 0;
-  int grid_sweep = 0, grid_matvec = 0, grid_update = 0;
+  int grid_sweep = 0, grid_matvec = 0, grid_update = 0, grid_guides = 0;
 
   ffvgpu::KCtx ctx(const ffvgpu::BCSet& bc) const {
     ffvgpu::KCtx C;
