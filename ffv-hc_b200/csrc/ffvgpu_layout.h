@@ -84,7 +84,7 @@ struct SolveState {
   double growth;     // mixed form: restart when the residual exceeds growth * best (0: never)
   double scale;      // RBGS_WithFixedAverage: the cell count the sum is divided by
   int32_t max_cycle; // mixed form: restart after this many iterations of a cycle (0: never)
-  int32_t pad2_;
+  int32_t ublocks;   // mixed form: blocks whose seven coefficients are the same in every cell
 };
 
 // Instances: independent problems that share one pool's blocks (a batch).

@@ -20,6 +20,10 @@ struct MixCtx {
   BCSet bc;            // pressure BCs (outer guide cells of the FP64 stencils)
   InstTable inst;
   double* partials;    // [2][capacity] per-block sums
+  // [capacity][8]: ap, aw, ae, as, an, ab, at of cell 0 and a flag (1.0) when
+  // every cell of the block has those seven coefficients; the sweep and A*x
+  // kernels then take them from here instead of streaming the per-cell arrays
+  const double* ucoef;
   int capacity;
   int first;
 };
@@ -29,7 +33,10 @@ void mx_grid_sizes(int* sweep, int* matvec, int* update, int* guides);
 // 32-bit sweep coefficients of blocks [first, first + count): [blk][7][8][512]
 // words (FP64 high words, rounded), MIXED_COEF_WORDS per block.
 constexpr int MIXED_COEF_WORDS = 7 * 8 * 512;
-void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint32_t* coef);
+// Also writes each block's ucoef record and adds the instance's uniform
+// blocks to st->ublocks.
+void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint32_t* coef,
+                    double* ucoef, SolveState* st);
 void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
                     const double* gx, const double* A, const double* b, double* r, double* r0);
 // The iteration launchers take 'count' = CTAs of the persistent grid.

@@ -36,7 +36,7 @@ void release_instances(ffvgpu_pool* P) {
   if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
   P->mgraph = nullptr;
   void* ptrs[] = {P->blk_inst_d, P->inst_first_d, P->inst_count_d, P->blk_geo_d, P->mst,
-                  P->mpartials, P->mhist, P->mcoef, P->mguide, P->me[0], P->me[1], P->mph,
+                  P->mpartials, P->mhist, P->mcoef, P->mguide, P->mucoef, P->me[0], P->me[1], P->mph,
                   P->msh};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -126,6 +126,7 @@ ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P) {
     mx_grid_sizes(&P->grid_sweep, &P->grid_matvec, &P->grid_update, &P->grid_guides);
   }
   if ((s = dalloc_t(P, &P->mcoef, 7 * n)) || (s = dalloc_t(P, &P->mguide, n / BC * 6 * 256)) ||
+      (s = dalloc_t(P, &P->mucoef, n / BC * 8)) ||
       (s = dalloc_t(P, &P->me[0], n)) ||
       (s = dalloc_t(P, &P->me[1], n)) || (s = dalloc_t(P, &P->mph, n)) ||
       (s = dalloc_t(P, &P->msh, n)) ||
@@ -160,6 +161,7 @@ MixCtx mix_ctx(const ffvgpu_pool* P) {
   C.inst.count = P->inst_count_d;
   C.inst.st = P->mst;
   C.partials = P->mpartials;
+  C.ucoef = P->mucoef;
   C.capacity = P->nb;
   C.first = 0;
   C.n_active = P->act_d;
@@ -192,6 +194,10 @@ ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
 
 // Algorithmic HBM bytes of one iteration per cell: two preconditioner
 // applications, two A*x with dot products, the update.
+// Of those, the per-cell coefficient bytes that a uniform block does not move
+// (its seven values come from one per-block record).
+int64_t uniform_saving_per_cell(int passes) { return 2 * passes * 28 + 2 * 56; }
+
 int64_t iteration_bytes_per_cell(int passes) {
   const int64_t first_p = 28 + 8 + 16 + 8 + 4;  // coefficients, r, p and q, p, e
   const int64_t first_s = 28 + 16 + 8 + 4;       // coefficients, q and r, s, e
@@ -647,9 +653,11 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
     I->running = false;
     return FFVGPU_OK;
   }
-  // the instance's FP32 coefficients, its state, then b.b / r / r0 / r.r0
-  launch_mx_pack(P->stream, I->first, I->count, P->A, P->mcoef);
+  // the instance's state, its 32-bit coefficients and uniform-block records
+  // (counted into the state), then b.b / r / r0 / r.r0
+  I->ublocks = 0;
   CK(cudaMemcpyAsync(P->mst + inst, &h, sizeof(h), cudaMemcpyHostToDevice, P->stream));
+  launch_mx_pack(P->stream, I->first, I->count, P->A, P->mcoef, P->mucoef, P->mst + inst);
   MixCtx C = mix_ctx(P);
   C.first = I->first;
   launch_mx_init(P->stream, C, I->count, P->x[P->xcur], P->gx, P->A, P->b, P->r, P->r0);
@@ -664,11 +672,12 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
   if (!P) return bad("null pool");
   if (iterations <= 0) return FFVGPU_OK;
   int running = 0;
-  int64_t cells = 0;
+  int64_t cells = 0, ucells = 0;
   for (const ffvgpu_instance& I : P->inst)
     if (I.running) {
       ++running;
       cells += (int64_t)I.count * BC;
+      ucells += (int64_t)I.ublocks * BC;
     }
   if (!running) return FFVGPU_OK;
   cudaSetDevice(P->device);
@@ -690,8 +699,9 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
   }
   CK(cudaGraphLaunch(P->mgraph, P->stream));
   P->m_launches += (int64_t)iterations * launches_per_iteration(P);
-  P->m_bytes += (int64_t)iterations * cells *
-                iteration_bytes_per_cell(P->m_sweeps / P->m_per_exchange);
+  const int passes = P->m_sweeps / P->m_per_exchange;
+  P->m_bytes += (int64_t)iterations * (cells * iteration_bytes_per_cell(passes) -
+                                       ucells * uniform_saving_per_cell(passes));
   return FFVGPU_OK;
 }
 
@@ -710,6 +720,7 @@ ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* P, int32_t* finished, int32_t capac
   int nf = 0;
   for (int i = 0; i < ni; ++i) {
     ffvgpu_instance& I = P->inst[i];
+    if (I.running) I.ublocks = I.result.uniform_blocks = P->mst_h[i].ublocks;  // from the packing
     if (!I.running || !P->mst_h[i].done) continue;
     const SolveState& h = P->mst_h[i];
     I.running = false;

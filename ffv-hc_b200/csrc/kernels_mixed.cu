@@ -277,7 +277,8 @@ __device__ __forceinline__ double widen_here(uint32_t w) {
 }
 
 __global__ void __launch_bounds__(MT)
-mx_pack_kernel(int first, const double* __restrict__ A, uint32_t* __restrict__ coef) {
+mx_pack_kernel(int first, const double* __restrict__ A, uint32_t* __restrict__ coef,
+               double* __restrict__ ucoef, SolveState* st) {
   const int blk = first + blockIdx.x;
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
   uint32_t* cb = coef + (size_t)blk * COEF_WORDS;
@@ -288,6 +289,18 @@ mx_pack_kernel(int first, const double* __restrict__ A, uint32_t* __restrict__ c
     for (int a = 0; a < 6; ++a) cb[coef_word(a, m, t)] = hi_round(Ab[(1 + a) * BLOCK_CELLS + s]);
     cb[coef_word(6, m, t)] = hi_round(1.0 / Ab[s]);
   }
+  // uniform block: all seven coefficients bitwise equal to cell 0's everywhere
+  bool same = true;
+  for (int s = threadIdx.x; s < BLOCK_CELLS; s += MT)
+#pragma unroll
+    for (int a = 0; a < 7; ++a)
+      same = same && __double_as_longlong(Ab[a * BLOCK_CELLS + s]) ==
+                         __double_as_longlong(Ab[a * BLOCK_CELLS]);
+  same = __syncthreads_and(same);
+  if (threadIdx.x < 8)
+    ucoef[(size_t)blk * 8 + threadIdx.x] =
+        threadIdx.x < 7 ? Ab[threadIdx.x * BLOCK_CELLS] : (same ? 1.0 : 0.0);
+  if (threadIdx.x == 0 && same) atomicAdd(&st->ublocks, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -444,8 +457,28 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
   double* V = reinterpret_cast<double*>(smem + COEF_WORDS * 4 + TILE * 8);  // [m][t] rhs
   double* GB = V + 8 * PT;  // [face][p] guides of the block, copied with its coefficients
   uint64_t* bar = reinterpret_cast<uint64_t*>(GB + GUIDES);
-  constexpr uint32_t COPY_BYTES = COEF_WORDS * 4 + (FIRST ? 0 : GUIDES * 8);
-  __shared__ int abort_flag, s_item[2], s_blk[2], s_inst[2];  // [copy parity]
+  __shared__ int abort_flag, s_item[2], s_blk[2], s_inst[2], s_uni[2];  // [copy parity]
+  __shared__ uint32_t s_uw[2][7];  // a uniform block's seven coefficient words
+  // the copy of one block: its coefficient words unless the block is
+  // uniform, and its guide layer in a later pass; with neither, the arrival
+  // alone completes the phase.  Run by thread 0 for item 'it', copy parity p.
+  auto issue = [&](int it, uint32_t p) {
+    const int b = C.active[it];
+    const double* U = C.ucoef + (size_t)b * 8;
+    const bool uni = U[7] != 0.0;
+    if (uni) {
+#pragma unroll
+      for (int a = 0; a < 6; ++a) s_uw[p][a] = hi_round(U[1 + a]);
+      s_uw[p][6] = hi_round(1.0 / U[0]);
+    }
+    async::mbar_expect_tx(bar, (uni ? 0u : COEF_WORDS * 4u) + (FIRST ? 0u : GUIDES * 8u));
+    if (!uni) async::bulk_g2s(slot, coef + (size_t)b * COEF_WORDS, COEF_WORDS * 4, bar);
+    if (!FIRST) async::bulk_g2s(GB, guides + (size_t)b * GUIDES, GUIDES * 8, bar);
+    s_uni[p] = uni;
+    s_blk[p] = b;
+    s_inst[p] = active_instance(C, b);
+    return b;
+  };
   const int tid = threadIdx.x;
   const int ih = tid & 7, kg = (tid >> 3) & 3, j = tid >> 5;
   const int o0 = (4 * kg + 1) * SQ + (j + 1) * SP + ih + 1;  // tile slot of cell (c 0, h 0)
@@ -468,14 +501,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     const int it0 = next_live(C, blockIdx.x, n_act, tid);
     if (tid == 0) {
       s_item[0] = it0;
-      if (it0 < n_act) {
-        const int b0 = C.active[it0];
-        async::mbar_expect_tx(bar, COPY_BYTES);
-        async::bulk_g2s(slot, coef + (size_t)b0 * COEF_WORDS, COEF_WORDS * 4, bar);
-        if (!FIRST) async::bulk_g2s(GB, guides + (size_t)b0 * GUIDES, GUIDES * 8, bar);
-        s_blk[0] = b0;
-        s_inst[0] = active_instance(C, b0);
-      }
+      if (it0 < n_act) issue(it0, 0);
     }
   }
   uint32_t phase = 0;  // parity of the copy the current item waits on
@@ -533,16 +559,25 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
 #pragma unroll
       for (int g = tid; g < GUIDES; g += PT) T[guide_slot(g >> 8, g & 255)] = GB[g];
     uint32_t cw[8][7];
+    if (s_uni[phase]) {
 #pragma unroll
-    for (int a = 0; a < 7; ++a)
+      for (int a = 0; a < 7; ++a) {
+        const uint32_t w = s_uw[phase][a];
 #pragma unroll
-      for (int hq = 0; hq < 2; ++hq) {
-        const uint4 w = reinterpret_cast<const uint4*>(slot)[(a * 2 + hq) * PT + tid];
-        cw[4 * hq + 0][a] = w.x;
-        cw[4 * hq + 1][a] = w.y;
-        cw[4 * hq + 2][a] = w.z;
-        cw[4 * hq + 3][a] = w.w;
+        for (int m = 0; m < 8; ++m) cw[m][a] = w;
       }
+    } else {
+#pragma unroll
+      for (int a = 0; a < 7; ++a)
+#pragma unroll
+        for (int hq = 0; hq < 2; ++hq) {
+          const uint4 w = reinterpret_cast<const uint4*>(slot)[(a * 2 + hq) * PT + tid];
+          cw[4 * hq + 0][a] = w.x;
+          cw[4 * hq + 1][a] = w.y;
+          cw[4 * hq + 2][a] = w.z;
+          cw[4 * hq + 3][a] = w.w;
+        }
+    }
     async::fence_proxy_async();
     __syncthreads();
     if (abort_flag) {
@@ -564,12 +599,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     const int nxt = tid < 32 ? next_live(C, item + gridDim.x, n_act, tid) : n_act;
     if (tid == 0) s_item[phase ^ 1u] = nxt;
     if (tid == 0 && nxt < n_act) {
-      const int nbk = C.active[nxt];
-      async::mbar_expect_tx(bar, COPY_BYTES);
-      async::bulk_g2s(slot, coef + (size_t)nbk * COEF_WORDS, COEF_WORDS * 4, bar);
-      if (!FIRST) async::bulk_g2s(GB, guides + (size_t)nbk * GUIDES, GUIDES * 8, bar);
-      s_blk[phase ^ 1u] = nbk;
-      s_inst[phase ^ 1u] = active_instance(C, nbk);
+      const int nbk = issue(nxt, phase ^ 1u);
       const size_t nbase = (size_t)nbk * BLOCK_CELLS;
       if (FIRST) {
         const int ni = C.inst.blk_inst[nbk];
@@ -647,6 +677,11 @@ mx_matvec_kernel(MixCtx C, const float* __restrict__ x, const double* __restrict
     __syncthreads();
     const size_t base = (size_t)blk * BLOCK_CELLS;
     const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+    const double* U = C.ucoef + (size_t)blk * 8;
+    const bool uni = U[7] != 0.0;  // the same seven coefficients in every cell
+    double u[7];
+#pragma unroll
+    for (int a = 0; a < 7; ++a) u[a] = uni ? U[a] : 0.0;
     double acc[NV][2][2] = {};
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
@@ -654,10 +689,13 @@ mx_matvec_kernel(MixCtx C, const float* __restrict__ x, const double* __restrict
       for (int m = 0; m < 8; ++m) {
         const int qd = tid + MT * m, s = c * HALF_CELLS + qd;
         const Nbrs v = split_neighbours(O + (1 - c) * HALF_CELLS, G, qd, c);
-        const double yv = __ldg(Ab + 4096 + s) * v.w + __ldg(Ab + 8192 + s) * v.e +
-                          __ldg(Ab + 12288 + s) * v.s + __ldg(Ab + 16384 + s) * v.n +
-                          __ldg(Ab + 20480 + s) * v.b + __ldg(Ab + 24576 + s) * v.t +
-                          __ldg(Ab + s) * O[s];
+        const double yv =
+            uni ? u[1] * v.w + u[2] * v.e + u[3] * v.s + u[4] * v.n + u[5] * v.b + u[6] * v.t +
+                      u[0] * O[s]
+                : __ldg(Ab + 4096 + s) * v.w + __ldg(Ab + 8192 + s) * v.e +
+                      __ldg(Ab + 12288 + s) * v.s + __ldg(Ab + 16384 + s) * v.n +
+                      __ldg(Ab + 20480 + s) * v.b + __ldg(Ab + 24576 + s) * v.t +
+                      __ldg(Ab + s) * O[s];
         y[base + s] = yv;
         acc[0][c][m & 1] += yv * __ldg(w0 + base + s);
         if (NV == 2) acc[NV - 1][c][m & 1] += yv * yv;
@@ -708,8 +746,9 @@ mx_update_kernel(MixCtx C, double* __restrict__ x, const float* __restrict__ ph,
 // ---------------------------------------------------------------------------
 // Launchers.
 // ---------------------------------------------------------------------------
-void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint32_t* coef) {
-  mx_pack_kernel<<<count, MT, 0, s>>>(first, A, coef);
+void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint32_t* coef,
+                    double* ucoef, SolveState* st) {
+  mx_pack_kernel<<<count, MT, 0, s>>>(first, A, coef, ucoef, st);
 }
 void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
                     const double* gx, const double* A, const double* b, double* r, double* r0) {

@@ -47,6 +47,7 @@ struct ffvgpu_instance {
   double epsilon = 0.0;
   int32_t status = 0;  // of the last solve: 0 ok, 2 NaN/Inf residual
   int32_t last_iter = 0;  // iterations with a residual before an early exit
+  int32_t ublocks = 0;    // blocks with the same coefficients in every cell (known after a poll)
   ffvgpu_result result{};
   ffvgpu_grid_desc desc{};  // level / block_index point into the vectors below
   std::vector<int32_t> level, index;
@@ -117,6 +118,7 @@ struct ffvgpu_pool {
   // mixed form
   uint32_t* mcoef = nullptr;  // [nb][7][4096] 32-bit sweep coefficients (FP64 high words)
   double* mguide = nullptr;   // [nb][6][256] guide layer of the sweep iterate between passes
+  double* mucoef = nullptr;   // [nb][8] per-block coefficients of uniform blocks (MixCtx::ucoef)
   float* me[2] = {nullptr, nullptr};
   float* mph = nullptr;     // preconditioned p (p_)
   float* msh = nullptr;     // preconditioned s (s_)

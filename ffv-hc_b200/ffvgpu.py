@@ -70,7 +70,7 @@ class Result(ctypes.Structure):
         ("count", ctypes.c_int32), ("residual", ctypes.c_double),
         ("elapsed_ms", ctypes.c_double), ("sweep_ms", ctypes.c_double),
         ("sweep_launches", ctypes.c_int32), ("bytes_moved", ctypes.c_int64),
-        ("kernel_launches", ctypes.c_int32),
+        ("kernel_launches", ctypes.c_int32), ("uniform_blocks", ctypes.c_int32),
     ]
 
 
@@ -494,7 +494,7 @@ class Pool:
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
         out = dict(status=st, count=res.count, residual=res.residual, elapsed_ms=res.elapsed_ms,
                    sweep_ms=res.sweep_ms, kernel_launches=res.kernel_launches,
-                   bytes_moved=res.bytes_moved)
+                   bytes_moved=res.bytes_moved, uniform_blocks=res.uniform_blocks)
         if history:
             n = res.count if 1 <= res.count <= count_max else (count_max if res.count > 0 else 0)
             out["history"] = hist[:n].copy()

@@ -117,6 +117,8 @@ typedef struct {
   int32_t sweep_launches;/* number of launches sweep_ms covers */
   int64_t bytes_moved;   /* algorithmic HBM bytes of the solve */
   int32_t kernel_launches;
+  int32_t uniform_blocks;/* mixed form: blocks whose seven coefficients are the same in every
+                            cell, which its kernels read once per block; 0 otherwise */
 } ffvgpu_result;
 
 /* ---- pool lifetime ------------------------------------------------------ */

@@ -45,6 +45,12 @@ def test_mixed_converges_and_matches_fp64_solution():
     P.fill("X", 0.0)
     rm = P.solve_mixed(1.5, 8, 4, 500, 1e-8)
     assert rm["status"] == ffvgpu.OK and rm["residual"] <= 1e-8, rm
+    # blocks whose seven coefficients are bitwise the same in every cell are
+    # read once per block by the mixed kernels: the count matches the oracle's A
+    A = np.stack([interior(O.field(f)).reshape(g.nb, -1)
+                  for f in ("AP", "AW", "AE", "AS", "AN", "AB", "AT")]).view(np.int64)
+    n_uniform = int(np.all(A == A[:, :, :1], axis=(0, 2)).sum())
+    assert 0 < n_uniform < g.nb and rm["uniform_blocks"] == n_uniform, (rm["uniform_blocks"], n_uniform)
     pm = interior(P.download("X", VC)).copy()
     # the oracle's converged mixed solve: same iteration count, same bits
     O.field("X")[...] = 0.0
