@@ -71,7 +71,8 @@ ffvgpu_status ensure_inst_device(ffvgpu_pool* P) {
     if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
     std::memset(P->mst_h, 0, sizeof(SolveState) * ni);
     for (int i = 0; i < ni; ++i) P->mst_h[i].done = 1;  // idle until a solve begins
-    CK(cudaMemcpy(P->mst, P->mst_h, sizeof(SolveState) * ni, cudaMemcpyHostToDevice));
+    CK(upload(P, P->mst, P->mst_h, sizeof(SolveState) * ni));
+    CK(cudaStreamSynchronize(P->stream));  // mst_h is pinned: rewritten only after the copy
   }
   if (P->inst_dirty) {
     std::vector<int32_t> first(ni), count(ni), geo((size_t)P->nb * 4);
@@ -83,11 +84,10 @@ ffvgpu_status ensure_inst_device(ffvgpu_pool* P) {
       geo[4 * b] = P->level[b];
       for (int a = 0; a < 3; ++a) geo[4 * b + 1 + a] = P->index[3 * b + a];
     }
-    CK(cudaMemcpy(P->blk_inst_d, P->blk_inst_h.data(), sizeof(int32_t) * P->nb,
-                  cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(P->inst_first_d, first.data(), sizeof(int32_t) * ni, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(P->inst_count_d, count.data(), sizeof(int32_t) * ni, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(P->blk_geo_d, geo.data(), sizeof(int32_t) * 4 * P->nb, cudaMemcpyHostToDevice));
+    CK(upload(P, P->blk_inst_d, P->blk_inst_h.data(), sizeof(int32_t) * P->nb));
+    CK(upload(P, P->inst_first_d, first.data(), sizeof(int32_t) * ni));
+    CK(upload(P, P->inst_count_d, count.data(), sizeof(int32_t) * ni));
+    CK(upload(P, P->blk_geo_d, geo.data(), sizeof(int32_t) * 4 * P->nb));
     P->inst_dirty = false;
   }
   return FFVGPU_OK;
@@ -117,7 +117,7 @@ ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P) {
   const size_t n = field_count(P);
   if (!P->act_d) {
     if ((s = dalloc_t(P, &P->act_d, n / BC + 1))) return s;
-    CK(cudaMemset(P->act_d, 0, sizeof(int32_t)));
+    CK(cudaMemsetAsync(P->act_d, 0, sizeof(int32_t), P->stream));
     for (int k = 0; k < 2; ++k) {
       CK(cudaMallocHost(&P->act_h[k], sizeof(int32_t) * (n / BC + 1)));
       CK(cudaEventCreateWithFlags(&P->act_ev[k], cudaEventDisableTiming));
@@ -315,11 +315,10 @@ ffvgpu_status admit_range(ffvgpu_pool* P, const ffvgpu_grid_desc* d, int32_t* in
   SolveState idle;
   std::memset(&idle, 0, sizeof(idle));
   idle.done = 1;
-  CK(cudaMemcpy(P->mst + slot, &idle, sizeof(idle), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(P->nbr_d + (size_t)first * 6, P->nbr_h.data() + (size_t)first * 6,
-                sizeof(FaceNbr) * 6 * n, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(P->dx_d + first, P->dx_h.data() + first, sizeof(double) * n,
-                cudaMemcpyHostToDevice));
+  CK(upload(P, P->mst + slot, &idle, sizeof(idle)));
+  CK(upload(P, P->nbr_d + (size_t)first * 6, P->nbr_h.data() + (size_t)first * 6,
+            sizeof(FaceNbr) * 6 * n));
+  CK(upload(P, P->dx_d + first, P->dx_h.data() + first, sizeof(double) * n));
   P->inst_dirty = true;
   if ((s = ensure_inst_device(P))) return s;
   *instance = slot;
@@ -584,8 +583,8 @@ ffvgpu_status ffvgpu_instance_release(ffvgpu_pool* P, int32_t inst) {
   cudaSetDevice(P->device);
   CK(cudaStreamSynchronize(P->stream));
   for (int b = I->first; b < I->first + I->count; ++b) P->blk_inst_h[b] = -1;
-  CK(cudaMemcpy(P->blk_inst_d + I->first, P->blk_inst_h.data() + I->first,
-                sizeof(int32_t) * I->count, cudaMemcpyHostToDevice));
+  CK(upload(P, P->blk_inst_d + I->first, P->blk_inst_h.data() + I->first,
+            sizeof(int32_t) * I->count));
   *I = ffvgpu_instance();
   return FFVGPU_OK;
 }
@@ -754,8 +753,8 @@ ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* P, int32_t inst, ffvgpu_
     // an early exit (count 0) keeps the residuals of the iterations before it
     const int nh = (c >= 1 && c <= I.count_max) ? c : (c == 0 ? I.last_iter : I.count_max);
     if (nh > 0)
-      CK(cudaMemcpy(history, P->mhist + (size_t)inst * P->mhist_cap, sizeof(double) * nh,
-                    cudaMemcpyDeviceToHost));
+      CK(download_sync(const_cast<ffvgpu_pool*>(P), history,
+                       P->mhist + (size_t)inst * P->mhist_cap, sizeof(double) * nh));
   }
   return result_status(I.result, I.status, I.epsilon, I.count_max);
 }

@@ -293,9 +293,8 @@ ffvgpu_status pool_init_device(ffvgpu_pool* P) {
   ffvgpu_status s;
   if ((s = dalloc_t(P, &P->nbr_d, P->nbr_h.size())) || (s = dalloc_t(P, &P->dx_d, P->dx_h.size())))
     return s;
-  CK(cudaMemcpy(P->nbr_d, P->nbr_h.data(), P->nbr_h.size() * sizeof(FaceNbr),
-                cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(P->dx_d, P->dx_h.data(), P->dx_h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(upload(P, P->nbr_d, P->nbr_h.data(), P->nbr_h.size() * sizeof(FaceNbr)));
+  CK(upload(P, P->dx_d, P->dx_h.data(), P->dx_h.size() * sizeof(double)));
   return ensure_solver(P);
 }
 
@@ -745,7 +744,7 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   R.kernel_launches = launches + 1;
   if (prm->history) {
     const int nh = (h.count >= 1 && h.count <= N) ? h.count : N;
-    CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+    CK(download_sync(P, prm->history, P->hist_d, sizeof(double) * nh));
   }
   if (res) *res = R;
   return solve_status(h, prm, N, R.count);
@@ -827,7 +826,7 @@ ffvgpu_status ffvgpu_solve_rbgs_fixed_average(ffvgpu_pool* P, const ffvgpu_iter_
   R.kernel_launches = launches + 1;
   if (prm->history) {
     const int nh = (h.count >= 1 && h.count <= N) ? h.count : N;
-    CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+    CK(download_sync(P, prm->history, P->hist_d, sizeof(double) * nh));
   }
   if (res) *res = R;
   return solve_status(h, prm, N, R.count);
@@ -932,7 +931,7 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   if (prm->history && N > 0) {
     const int nh = (h.count >= 1 && h.count <= N) ? h.count : (h.count == 0 ? h.iter : N);
     if (nh > 0)
-      CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+      CK(download_sync(P, prm->history, P->hist_d, sizeof(double) * nh));
   }
   if (res) *res = R;
   return solve_status(h, prm, N, R.count);
@@ -1049,7 +1048,7 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
   if (prm->history && N > 0) {
     const int nh = (h.count >= 1 && h.count <= N) ? h.count : (h.count == 0 ? h.iter : N);
     if (nh > 0)
-      CK(cudaMemcpy(prm->history, P->hist_d, sizeof(double) * nh, cudaMemcpyDeviceToHost));
+      CK(download_sync(P, prm->history, P->hist_d, sizeof(double) * nh));
   }
   if (res) *res = R;
   return solve_status(h, prm, N, R.count);

@@ -154,6 +154,19 @@ namespace ffvgpu {
 namespace detail {
 
 ffvgpu_status dalloc(ffvgpu_pool* P, void** ptr, size_t bytes);
+// Copies between host and device ordered on the pool's stream.  The pool's
+// stream is non-blocking, so it does not wait for the legacy default stream:
+// a plain cudaMemcpy from pageable memory may return before its data reaches
+// the device, and a kernel enqueued next on the pool's stream could read the
+// old contents.  Pageable sources are staged before upload() returns.
+inline cudaError_t upload(ffvgpu_pool* P, void* dst, const void* src, size_t bytes) {
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, P->stream);
+}
+// Waits for the pool's stream, so the copy sees all work enqueued before it.
+inline cudaError_t download_sync(ffvgpu_pool* P, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, P->stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(P->stream);
+}
 template <class T>
 ffvgpu_status dalloc_t(ffvgpu_pool* P, T** ptr, size_t count) {
   return dalloc(P, reinterpret_cast<void**>(ptr), count * sizeof(T));
