@@ -233,20 +233,22 @@ __device__ void mx_reduce(double (&acc)[NV][2][2], const MixCtx& C, int blk, int
 // Stages block blk of an FP32 vector as FP64: the colour-split interior in
 // O[4096] and the first guide layer in G[6][256], guides by the exchange
 // rules in FP64 (outer faces by the field's BCs).
+// nb: the block's six face records, already in shared memory (so each
+// guide needs one round of global loads, not a dependent second).
 __device__ __forceinline__ void stage_f32_as_f64(double* __restrict__ O, double* __restrict__ G,
                                                  const float* __restrict__ x, int blk,
+                                                 const FaceNbr* nb, double dx,
                                                  const MixCtx& C) {
   const int tid = threadIdx.x;
   const float* xb = x + (size_t)blk * BLOCK_CELLS;
 #pragma unroll 4
   for (int m = 0; m < 16; ++m) O[tid + MT * m] = (double)__ldg(xb + tid + MT * m);
-  const double dx = C.dx[blk];
-#pragma unroll 1
-  for (int it = 0; it < 3; ++it) {
+#pragma unroll
+  for (int it = 0; it < 3; ++it) {  // the three pairs' loads in flight together
     const int f = 2 * it + (tid >> 7), p0 = tid & 127, p1 = p0 + 128;
-    const FaceNbr nb = C.nbr[blk * 6 + f];
+    const FaceNbr nf = nb[f];
     double v0, v1;
-    guide_pair(x, blk, f, p0, p1, nb, C.bc, dx, v0, v1);
+    guide_pair(x, blk, f, p0, p1, nf, C.bc, dx, v0, v1);
     G[f * FACE_CELLS + p0] = v0;
     G[f * FACE_CELLS + p1] = v1;
   }
@@ -368,9 +370,21 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
 // T and V are written by other threads between the barriers: no __restrict__
 // on them, which would let the compiler move tile loads across
 // __syncthreads().
+// UNI: a uniform block -- the seven coefficients ku (widened once) serve
+// every cell and cw is not read; otherwise each cell's words cw[m] are
+// widened at use.  The values, and so the results, are the same either way.
+template <bool UNI>
 __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, int p0,
-                                           double (&E)[2][4],
-                                           const uint32_t (&cw)[8][7], double mom, int nsweep) {
+                                           double (&E)[2][4], const uint32_t (&cw)[8][7],
+                                           const double (&ku)[7], double mom, int nsweep) {
+#define MX_COEF(m, a) (UNI ? ku[a] : widen_here(cw[m][a]))
+  // a uniform block has the registers to keep its right-hand side too (one
+  // shared-memory read less per update)
+  double vr[2][4];
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int h = 0; h < 4; ++h) vr[c][h] = UNI ? V[(4 * c + h) * PT] : 0.0;
 #pragma unroll 1
   for (int it = 0; it < nsweep; ++it) {
 #pragma unroll
@@ -385,31 +399,31 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
         // the x neighbour at the same ih is this thread's own; the other one
         // is east (par 1) or west (par 0) of it in the tile
         xo[h] = O[h * SQ + (par ? 1 : -1)];
-        rc[h] = V[(4 * c + h) * PT];
+        rc[h] = UNI ? vr[c][h] : V[(4 * c + h) * PT];
       }
 #pragma unroll
       for (int h = 0; h < 4; ++h) {
         const int par = p0 ^ ((h + c) & 1);
-        rc[h] = __fma_rn(-widen_here(cw[4 * c + h][0]), par ? E[1 - c][h] : xo[h], rc[h]);
+        rc[h] = __fma_rn(-MX_COEF(4 * c + h, 0), par ? E[1 - c][h] : xo[h], rc[h]);
       }
 #pragma unroll
       for (int h = 0; h < 4; ++h) {
         const int par = p0 ^ ((h + c) & 1);
-        rc[h] = __fma_rn(-widen_here(cw[4 * c + h][1]), par ? xo[h] : E[1 - c][h], rc[h]);
+        rc[h] = __fma_rn(-MX_COEF(4 * c + h, 1), par ? xo[h] : E[1 - c][h], rc[h]);
       }
 #pragma unroll
-      for (int h = 0; h < 4; ++h) rc[h] = __fma_rn(-widen_here(cw[4 * c + h][2]), O[h * SQ - SP], rc[h]);
+      for (int h = 0; h < 4; ++h) rc[h] = __fma_rn(-MX_COEF(4 * c + h, 2), O[h * SQ - SP], rc[h]);
 #pragma unroll
-      for (int h = 0; h < 4; ++h) rc[h] = __fma_rn(-widen_here(cw[4 * c + h][3]), O[h * SQ + SP], rc[h]);
-#pragma unroll
-      for (int h = 0; h < 4; ++h)
-        rc[h] = __fma_rn(-widen_here(cw[4 * c + h][4]), h > 0 ? E[1 - c][h - 1] : O[-SQ], rc[h]);
+      for (int h = 0; h < 4; ++h) rc[h] = __fma_rn(-MX_COEF(4 * c + h, 3), O[h * SQ + SP], rc[h]);
 #pragma unroll
       for (int h = 0; h < 4; ++h)
-        rc[h] = __fma_rn(-widen_here(cw[4 * c + h][5]), h < 3 ? E[1 - c][h + 1] : O[4 * SQ], rc[h]);
+        rc[h] = __fma_rn(-MX_COEF(4 * c + h, 4), h > 0 ? E[1 - c][h - 1] : O[-SQ], rc[h]);
+#pragma unroll
+      for (int h = 0; h < 4; ++h)
+        rc[h] = __fma_rn(-MX_COEF(4 * c + h, 5), h < 3 ? E[1 - c][h + 1] : O[4 * SQ], rc[h]);
 #pragma unroll
       for (int h = 0; h < 4; ++h) {
-        const double xt = __dmul_rn(rc[h], widen_here(cw[4 * c + h][6]));
+        const double xt = __dmul_rn(rc[h], MX_COEF(4 * c + h, 6));
         const double e = E[c][h];
         const double en = __fma_rn(mom, __dsub_rn(e, xt), e);
         E[c][h] = en;
@@ -419,6 +433,7 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
     }
   }
 }
+#undef MX_COEF
 
 // Tile address of the guide cell at position p (u + 16 v) of a face.
 __device__ __forceinline__ int guide_slot(int face, int p) {
@@ -559,13 +574,11 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
 #pragma unroll
       for (int g = tid; g < GUIDES; g += PT) T[guide_slot(g >> 8, g & 255)] = GB[g];
     uint32_t cw[8][7];
-    if (s_uni[phase]) {
+    double ku[7];
+    const bool uni = s_uni[phase];
+    if (uni) {
 #pragma unroll
-      for (int a = 0; a < 7; ++a) {
-        const uint32_t w = s_uw[phase][a];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) cw[m][a] = w;
-      }
+      for (int a = 0; a < 7; ++a) ku[a] = widen(s_uw[phase][a]);
     } else {
 #pragma unroll
       for (int a = 0; a < 7; ++a)
@@ -613,7 +626,10 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       }
     }
     if (inst < 0) continue;
-    run_sweeps(T, V + tid, o0, j & 1, E, cw, mom, nsweep);
+    if (uni)
+      run_sweeps<true>(T, V + tid, o0, j & 1, E, cw, ku, mom, nsweep);
+    else
+      run_sweeps<false>(T, V + tid, o0, j & 1, E, cw, ku, mom, nsweep);
 #pragma unroll
     for (int c = 0; c < 2; ++c)
 #pragma unroll
@@ -638,21 +654,31 @@ mx_guides_kernel(MixCtx C, const float* __restrict__ e, double* __restrict__ gui
     hom.type[f] = BC_DIRICHLET;
     hom.value[f] = 0.0;
   }
+  __shared__ FaceNbr snb[6];
+  __shared__ double sdx;
+  __shared__ int live;
   const int n_act = *C.n_active;
   for (int item = blockIdx.x; item < n_act; item += gridDim.x) {
     const int blk = C.active[item];
-    if (active_instance(C, blk) < 0) continue;
-    const double dx = C.dx[blk];
-    double* gb = guides + (size_t)blk * GUIDES;
-#pragma unroll 1
-    for (int w = threadIdx.x; w < 3 * FACE_CELLS; w += GT) {
-      const int f = w >> 7, p0 = w & 127, p1 = p0 + 128;
-      const FaceNbr nb = C.nbr[blk * 6 + f];
-      double g0, g1;
-      guide_pair(e, blk, f, p0, p1, nb, hom, dx, g0, g1);
-      gb[f * FACE_CELLS + p0] = g0;
-      gb[f * FACE_CELLS + p1] = g1;
+    if (threadIdx.x < 6) snb[threadIdx.x] = C.nbr[blk * 6 + threadIdx.x];
+    if (threadIdx.x == 0) {
+      live = active_instance(C, blk) >= 0;
+      sdx = C.dx[blk];
     }
+    __syncthreads();
+    if (live) {
+      double* gb = guides + (size_t)blk * GUIDES;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {  // the three pairs' loads in flight together
+        const int w = threadIdx.x + GT * r, f = w >> 7, p0 = w & 127, p1 = p0 + 128;
+        const FaceNbr nf = snb[f];
+        double g0, g1;
+        guide_pair(e, blk, f, p0, p1, nf, hom, sdx, g0, g1);
+        gb[f * FACE_CELLS + p0] = g0;
+        gb[f * FACE_CELLS + p1] = g1;
+      }
+    }
+    __syncthreads();  // snb, sdx and live are refilled for the next block
   }
 }
 
@@ -662,18 +688,21 @@ mx_guides_kernel(MixCtx C, const float* __restrict__ e, double* __restrict__ gui
 // (t_.s and t_.t_, FFVILS.h:923-936).
 // ---------------------------------------------------------------------------
 template <int NV>
-__global__ void __launch_bounds__(MT)
+__global__ void __launch_bounds__(MT, 4)
 mx_matvec_kernel(MixCtx C, const float* __restrict__ x, const double* __restrict__ A,
                  double* __restrict__ y, const double* __restrict__ w0) {
   __shared__ double O[BLOCK_CELLS];
   __shared__ double G[6 * FACE_CELLS];
+  __shared__ FaceNbr snb[6];
   const int tid = threadIdx.x;
   const int n_act = *C.n_active;
   for (int item = blockIdx.x; item < n_act; item += gridDim.x) {
     const int blk = C.active[item];
     const int inst = active_instance(C, blk);
     if (inst < 0) continue;
-    stage_f32_as_f64(O, G, x, blk, C);
+    if (tid < 6) snb[tid] = C.nbr[blk * 6 + tid];
+    __syncthreads();
+    stage_f32_as_f64(O, G, x, blk, snb, C.dx[blk], C);
     __syncthreads();
     const size_t base = (size_t)blk * BLOCK_CELLS;
     const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
