@@ -477,21 +477,43 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
   // the copy of one block: its coefficient words unless the block is
   // uniform, and its guide layer in a later pass; with neither, the arrival
   // alone completes the phase.  Run by thread 0 for item 'it', copy parity p.
+  // A uniform block needs no coefficient words, so in a first pass its copy
+  // brings the block's vectors into the slot instead and its staging reads
+  // shared memory: r (slot doubles [0, 4096)), q ([4096, 8192)) and p
+  // ([8192, 12288)) as far as it reads them.  (A later pass reads p and the
+  // FP32 iterate from global memory, prefetched into L2 a block ahead: that
+  // measured faster than copying them.)
   auto issue = [&](int it, uint32_t p) {
     const int b = C.active[it];
+    const int ib = active_instance(C, b);
     const double* U = C.ucoef + (size_t)b * 8;
     const bool uni = U[7] != 0.0;
+    const size_t gb = (size_t)b * BLOCK_CELLS;
+    constexpr uint32_t VB = BLOCK_CELLS * 8;  // bytes of one FP64 vector block
+    double* sd = reinterpret_cast<double*>(slot);
     if (uni) {
 #pragma unroll
       for (int a = 0; a < 6; ++a) s_uw[p][a] = hi_round(U[1 + a]);
       s_uw[p][6] = hi_round(1.0 / U[0]);
+      if (FIRST) {
+        const bool copy = MODE == 0 && ib >= 0 && C.inst.st[ib].cycle == 1;
+        const bool needq = !copy, needp = MODE == 0 && !copy;
+        async::mbar_expect_tx(bar, VB + (needq ? VB : 0u) + (needp ? VB : 0u));
+        async::bulk_g2s(sd, r + gb, VB, bar);
+        if (needq) async::bulk_g2s(sd + BLOCK_CELLS, q + gb, VB, bar);
+        if (needp) async::bulk_g2s(sd + 2 * BLOCK_CELLS, pv + gb, VB, bar);
+      } else {
+        async::mbar_expect_tx(bar, GUIDES * 8u);
+        async::bulk_g2s(GB, guides + (size_t)b * GUIDES, GUIDES * 8, bar);
+      }
+    } else {
+      async::mbar_expect_tx(bar, COEF_WORDS * 4u + (FIRST ? 0u : GUIDES * 8u));
+      async::bulk_g2s(slot, coef + (size_t)b * COEF_WORDS, COEF_WORDS * 4, bar);
+      if (!FIRST) async::bulk_g2s(GB, guides + (size_t)b * GUIDES, GUIDES * 8, bar);
     }
-    async::mbar_expect_tx(bar, (uni ? 0u : COEF_WORDS * 4u) + (FIRST ? 0u : GUIDES * 8u));
-    if (!uni) async::bulk_g2s(slot, coef + (size_t)b * COEF_WORDS, COEF_WORDS * 4, bar);
-    if (!FIRST) async::bulk_g2s(GB, guides + (size_t)b * GUIDES, GUIDES * 8, bar);
     s_uni[p] = uni;
     s_blk[p] = b;
-    s_inst[p] = active_instance(C, b);
+    s_inst[p] = ib;
     return b;
   };
   const int tid = threadIdx.x;
@@ -530,26 +552,36 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     const int blk = s_blk[phase], inst = s_inst[phase];
     const size_t base = (size_t)blk * BLOCK_CELLS + s0;
     double E[2][4] = {};
+    // this block's copy (issued a block ago): coefficients and guides, or
+    // for a uniform block its vectors and guides
+    async::mbar_wait(bar, phase, &abort_flag, ROLE_SWEEP);
+    const bool uni = s_uni[phase];
+    const double* sd = reinterpret_cast<const double*>(slot);
+    const size_t gbase = (size_t)blk * BLOCK_CELLS;
     if (inst >= 0 && FIRST) {
       const SolveState* S = C.inst.st + inst;
       const bool copy = S->cycle == 1;  // first iteration of a (re)start: p = r, r0 = r
       const double mgamma = -S->gamma, beta = S->beta, malpha = -S->alpha;
+      const double* rs = uni ? sd : r + gbase;
+      const double* qs = uni ? sd + BLOCK_CELLS : q + gbase;
+      const double* ps = uni ? sd + 2 * BLOCK_CELLS : pv + gbase;
 #pragma unroll
       for (int c = 0; c < 2; ++c)
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
-          const size_t s = base + c * HALF_CELLS + h * 128;
+          const int sl = s0 + c * HALF_CELLS + h * 128;
+          const size_t s = gbase + sl;
           double rhs;
           if (MODE == 0) {
             if (copy) {
-              rhs = r[s];
+              rhs = rs[sl];
               r0[s] = rhs;
             } else {
-              const double t = pv[s] + mgamma * q[s];
-              rhs = r[s] + beta * t;
+              const double t = ps[sl] + mgamma * qs[sl];
+              rhs = rs[sl] + beta * t;
             }
           } else {
-            rhs = malpha * q[s] + r[s];
+            rhs = malpha * qs[sl] + rs[sl];
           }
           pv[s] = rhs;
           V[(4 * c + h) * PT + tid] = rhs;
@@ -567,15 +599,11 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
           T[o0 + c * SH + h * SQ] = E[c][h];
         }
     }
-    // this block's coefficients and guides (the copy issued a block ago),
-    // then the next block's copy
-    async::mbar_wait(bar, phase, &abort_flag, ROLE_SWEEP);
     if (!FIRST && inst >= 0)
 #pragma unroll
       for (int g = tid; g < GUIDES; g += PT) T[guide_slot(g >> 8, g & 255)] = GB[g];
     uint32_t cw[8][7];
     double ku[7];
-    const bool uni = s_uni[phase];
     if (uni) {
 #pragma unroll
       for (int a = 0; a < 7; ++a) ku[a] = widen(s_uw[phase][a]);
@@ -614,7 +642,9 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     if (tid == 0 && nxt < n_act) {
       const int nbk = issue(nxt, phase ^ 1u);
       const size_t nbase = (size_t)nbk * BLOCK_CELLS;
-      if (FIRST) {
+      if (FIRST && s_uni[phase ^ 1u]) {
+        // its vectors come with the copy
+      } else if (FIRST) {
         const int ni = C.inst.blk_inst[nbk];
         const bool copy = MODE == 0 && ni >= 0 && C.inst.st[ni].cycle == 1;
         async::prefetch_l2(r + nbase, BLOCK_CELLS * 8);
