@@ -364,8 +364,10 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
 // Of a cell's six neighbours (all of the other colour) the one at the same
 // (ih, j) -- west or east by the row's parity -- and the z neighbours inside
 // the column are this thread's own registers; the rest come from the tile.
-// The next block's coefficients arrive by one bulk copy while this block
-// sweeps, and its vectors are prefetched into L2.
+// While this block sweeps, one bulk copy brings the next block's coefficient
+// words (or, for a uniform block in a first pass, its right-hand-side vectors)
+// and, in a later pass, its guide layer; vectors not copied are prefetched
+// into L2.
 // ---------------------------------------------------------------------------
 // T and V are written by other threads between the barriers: no __restrict__
 // on them, which would let the compiler move tile loads across
