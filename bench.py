@@ -21,7 +21,7 @@ here), OpenMP over blocks, on a bounded sample of sweeps per step.
 
 Other forms (--form), each printing one JSON line of its own:
   mixed  solves/s to a 1e-8 relative residual of the mixed-precision solve
-         (FP64 BiCGSTAB recurrence, FP32 RB-SOR preconditioner) against the
+         (FP64 BiCGSTAB recurrence, RB-SOR preconditioner on 32-bit data) against the
          plain FP64 GPU solve (FFVILS::BiCGSTAB, Jacobi PreCount 2), with the
          error of p and grad p against a converged FP64 solution;
   batch  64 independent sphere instances (diameter U[0.5,2], centre in the
@@ -429,7 +429,7 @@ def run_serve(args):
     line = {
         "form": "serve", "metric": "served solves/s and p50/p99 latency at 1e-8",
         "value": top["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
-        "higher_is_better": True, "dtype": "f64 outer / f32 sweeps", "data": "synthetic",
+        "higher_is_better": True, "dtype": "f64 arithmetic, 32-bit sweep data", "data": "synthetic",
         "config": {"workload": f"serve-{len(probs)}-requests-per-rate", "rates": rates,
                    "blocks_min_max": [int(min(blocks)), int(max(blocks))],
                    "blocks_total": int(sum(blocks)), "capacity_blocks": args.capacity,
@@ -508,7 +508,7 @@ def run_mixed(args):
         "form": "mixed", "metric": "solves/s to 1e-8 relative residual",
         "value": 1e3 / tm, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tm, "higher_is_better": True,
-        "dtype": "f64 outer / f32 sweeps", "data": "synthetic",
+        "dtype": "f64 arithmetic, 32-bit sweep data", "data": "synthetic",
         "config": {"workload": f"mixed-vs-fp64-sphere-level{args.level}", "blocks": int(g.nb),
                    "cells": int(g.cells), "epsilon": 1e-8, "mixed": MIXED,
                    "fp64": dict(FP64_SOLVER, solver="BiCGSTAB (FFVILS.h:793-974)")},
@@ -645,7 +645,7 @@ def run_batch(args):
     line = {
         "form": "batch", "metric": "solves/s to 1e-8 relative residual", "value": 1e3 * len(ids) / tb,
         "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": tb, "higher_is_better": True, "dtype": "f64 outer / f32 sweeps",
+        "ms_per_step": tb, "higher_is_better": True, "dtype": "f64 arithmetic, 32-bit sweep data",
         "data": "synthetic",
         "config": {"workload": f"batch-{len(ids)}-sphere-instances", "instances": len(ids),
                    "blocks": total, "cells": total * CELLS_PER_BLOCK,

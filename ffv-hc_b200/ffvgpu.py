@@ -484,7 +484,7 @@ class Pool:
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
                     epsilon=1e-8, history=True, check_every=0, restart_drop=None,
                     restart_growth=None, restart_every=None):
-        """Mixed-precision solve (FP64 BiCGSTAB, FP32 RB-SOR preconditioner)."""
+        """Mixed-precision solve (FP64 BiCGSTAB; RB-SOR preconditioner on 32-bit data)."""
         hist = np.zeros(max(count_max, 1), np.float64) if history else None
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
                           hist.ctypes.data if history else None,
