@@ -1,8 +1,9 @@
 """Mixed-precision form, batches and the device generator, on the GPU.
 
-The mixed solve (FP64 BiCGSTAB recurrence, FP32 red-black SOR
-preconditioner) is checked bit for bit against the oracle's restatement
-(orc_mixed) for several sweep groupings; its converged pressure is compared
+The mixed solve (FP64 BiCGSTAB recurrence, red-black SOR preconditioner on
+32-bit coefficients with FP64 arithmetic) is checked bit for bit against the
+oracle's restatement (orc_mixed) for several sweep groupings, on grids with
+fewer blocks than CTAs and with several blocks per CTA; its converged pressure is compared
 with the FP64 solve of the same system (tolerance stated in the test).  A
 batch's instances are checked to give the same bits alone and in a mix,
 admitted together or while others run, and the device generator + assembly
