@@ -505,6 +505,26 @@ def test_bicgstab_converges_on_refined_sphere_grid():
     assert r["status"] == 0 and r["residual"] <= 1e-8
 
 
+def test_mixed_oracle_converges_to_the_fp64_solution():
+    """The oracle's restatement of the mixed form (FP64 BiCGSTAB recurrence,
+    red-black SOR preconditioner on 32-bit coefficients, restarts on a drop of
+    1e-3 or a growth of 100) reaches 1e-8 on a refined grid, and its pressure
+    agrees with the FP64 BiCGSTAB solution of the same system: a 1e-8 relative
+    residual bounds the relative error by the condition number times 1e-8,
+    below 1e-5 here."""
+    from helpers import interior, problem
+    g, inp, O = problem(1)
+    O.field("X")[...] = 0.0
+    rm = O.solve_mixed(1.5, 8, 4, 400, 1e-8)
+    assert rm["status"] == 0 and rm["residual"] <= 1e-8 and 1 <= rm["count"] <= 400, rm
+    pm = interior(O.field("X")).copy()
+    O.field("X")[...] = 0.0
+    rf = O.solve_bicgstab(1.0, 2, 3000, 1e-12, restart_drop=1e-3)
+    assert rf["status"] == 0
+    pf = interior(O.field("X"))
+    assert np.linalg.norm(pm - pf) / np.linalg.norm(pf) < 1e-5
+
+
 def test_restart_filename_follows_the_reference_pattern():
     """LocalScalar3D.cpp:224-243: path/prefix label-rank(5)-step(10).bin."""
     import ffvgpu
