@@ -18,7 +18,7 @@ from helpers import VC, assert_bitwise, device_problem, interior, problem, rel_e
 pytestmark = pytest.mark.gpu
 THREADS = os.cpu_count() or 8
 # Relative tolerance of the FP64 path against the reference-order oracle
-# (sums in a different order): the north-star bar.
+# (sums in a different order): residual histories agree to 1e-12.
 TOL_REFERENCE_ORDER = 1e-12
 
 
