@@ -17,6 +17,12 @@
 // it and must be serialised by the caller.  The counter is cleared by each
 // call before its reduction starts.
 //
+// The array's device address is looked up once per device and kept for the
+// life of the process: it assumes that device's primary context lives as
+// long as the process does (after cudaDeviceReset the module may load
+// elsewhere, so the cached address would be stale).  The stream passed must
+// belong to the device that is current at the call.
+//
 // The sum uses the same fixed tree as ffvgpu_dot, so the result is bit for
 // bit the one the pool-based entry point returns for the same vectors.
 #include <cstdio>

@@ -1,17 +1,27 @@
 // ffvgpu_async.cuh -- shared-memory mbarriers and bulk copies (global ->
 // shared, and global -> L2 prefetch) for the persistent kernels, sm_100a.
 //
-// Every wait is bounded in time: mbar_wait gives up after WAIT_NS, records
-// the caller's role in an abort word and returns false, so a kernel whose
-// copy never lands reports an error instead of spinning.
+// Every wait is bounded in time: mbar_wait gives up after the caller's limit
+// (a pool setting, DEFAULT_WAIT_NS unless changed), records the caller's role
+// in an abort word and returns false, so a kernel whose copy never lands
+// reports an error instead of spinning.  After an abort, mbar_drain waits for
+// copies already issued into the CTA's shared memory; its bound (DRAIN_NS)
+// does not depend on the pool setting, so a short wait limit never lets a
+// CTA exit while a copy is still landing in its shared memory.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "ffvgpu_layout.h"
+
 namespace ffvgpu {
 namespace async {
 
-constexpr uint64_t WAIT_NS = 4000000000ull;  // a wait gives up after 4 s
+constexpr uint64_t DRAIN_NS = 2000000000ull;         // a post-abort drain gives up after 2 s
+// SolveState::timeout_where bit of a drain that gave up: a copy was still in
+// flight when the CTA left (never seen: copies from device memory complete
+// in microseconds)
+constexpr int ROLE_DRAIN = 16;
 
 __device__ __forceinline__ uint32_t sa(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -48,16 +58,27 @@ __device__ __forceinline__ uint64_t now_ns() {
 }
 // Bounded wait; false when it gave up (recording its role) or another role aborted.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag,
-                                          int role) {
+                                          int role, uint64_t limit_ns) {
   if (mbar_try_wait(b, parity)) return true;
   const uint64_t t0 = now_ns();
   for (;;) {
     if (mbar_try_wait(b, parity)) return true;
     if (*abort_flag) return false;
-    if (now_ns() - t0 > WAIT_NS) {
+    if (now_ns() - t0 > limit_ns) {
       atomicOr((int*)abort_flag, role);
       return false;
     }
+  }
+}
+// Waits, bounded by DRAIN_NS and regardless of any abort, until the phase
+// with the given parity has completed (every copy armed on it has landed);
+// false if it gave up.
+__device__ __forceinline__ bool mbar_drain(uint64_t* b, uint32_t parity) {
+  if (mbar_try_wait(b, parity)) return true;
+  const uint64_t t0 = now_ns();
+  for (;;) {
+    if (mbar_try_wait(b, parity)) return true;
+    if (now_ns() - t0 > DRAIN_NS) return false;
   }
 }
 // dst, src 16-byte aligned; bytes a multiple of 16.

@@ -20,6 +20,7 @@ struct KCtx {
   BCSet bc;
   int nb;
   int first;
+  uint64_t wait_ns;    // limit of every bounded device wait (ffvgpu_pool_set_wait_limit)
 };
 
 // Fused residual + red-black sweep over the coefficient stream (rbgs_pipelined.cu).

@@ -37,6 +37,10 @@ constexpr int THREADS = 256;      // threads per CTA of every block kernel
 // of its 256 cells back to back (16 KB), so one bulk copy moves a chunk.
 constexpr int STREAM_CHUNK = 8 * 256;
 constexpr int STREAM_BLOCK = 16 * STREAM_CHUNK;
+// Default limit of every bounded device wait (a pool setting,
+// ffvgpu_pool_set_wait_limit): a wait that has not completed after it gives
+// up and the solve reports a timeout.
+constexpr uint64_t DEFAULT_WAIT_NS = 4000000000ull;
 
 enum { X_M = 0, X_P, Y_M, Y_P, Z_M, Z_P };
 enum { BC_DIRICHLET = 0, BC_NEUMANN = 1 };

@@ -26,6 +26,7 @@ struct MixCtx {
   const double* ucoef;
   int capacity;
   int first;
+  uint64_t wait_ns;    // limit of every bounded device wait (ffvgpu_pool_set_wait_limit)
 };
 
 // CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel.

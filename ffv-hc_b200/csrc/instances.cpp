@@ -13,6 +13,7 @@
 // replays, and an instance admitted while others run joins at the next
 // replay.
 #include <cfloat>
+#include <cstddef>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -166,6 +167,7 @@ MixCtx mix_ctx(const ffvgpu_pool* P) {
   C.first = 0;
   C.n_active = P->act_d;
   C.active = P->act_d + 1;
+  C.wait_ns = P->wait_ns;
   return C;
 }
 
@@ -236,7 +238,16 @@ int launches_per_iteration(const ffvgpu_pool* P) {
   return 2 * passes + 2 * (passes - 1) + 3;  // sweeps, guide layers, A*x (2), update
 }
 
-ffvgpu_status result_status(const ffvgpu_result& R, int status_code, double eps, int count_max) {
+ffvgpu_status result_status(const ffvgpu_result& R, int status_code, double eps, int count_max,
+                            int timeout_where) {
+  if (status_code == 3) {
+    g_last_error = timeout_message(timeout_where);
+    return FFVGPU_TIMEOUT;
+  }
+  if (status_code == 4) {
+    g_last_error = "the solve was cancelled";
+    return FFVGPU_CANCELLED;
+  }
   if (status_code == 2) {
     g_last_error = "residual is NaN or Inf";
     return FFVGPU_NAN_DETECTED;
@@ -680,8 +691,10 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
     }
   if (!running) return FFVGPU_OK;
   cudaSetDevice(P->device);
+  // kernel arguments (the wait limit among them) are fixed at capture
   if (!P->mgraph || P->mgraph_iters != iterations || P->mgraph_omega != P->m_omega ||
-      P->mgraph_sweeps != P->m_sweeps || P->mgraph_per != P->m_per_exchange) {
+      P->mgraph_sweeps != P->m_sweeps || P->mgraph_per != P->m_per_exchange ||
+      P->mgraph_wait_ns != P->wait_ns) {
     if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
     P->mgraph = nullptr;
     cudaGraph_t graph;
@@ -695,6 +708,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
     P->mgraph_omega = P->m_omega;
     P->mgraph_sweeps = P->m_sweeps;
     P->mgraph_per = P->m_per_exchange;
+    P->mgraph_wait_ns = P->wait_ns;
   }
   CK(cudaGraphLaunch(P->mgraph, P->stream));
   P->m_launches += (int64_t)iterations * launches_per_iteration(P);
@@ -726,6 +740,7 @@ ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* P, int32_t* finished, int32_t capac
     I.result.count = h.count;
     I.result.residual = h.residual;
     I.status = h.status;
+    I.timeout_where = h.timeout_where;
     I.last_iter = (h.count == 0) ? h.iter : 0;  // 0 when the exit came before iteration 1
     launch_exchange(P->stream, range_ctx(P, P->bc_p, I), P->x[P->xcur], P->gx);  // FFVILS.h:973
     if (finished && nf < capacity) finished[nf] = i;
@@ -739,6 +754,35 @@ ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* P, int32_t* finished, int32_t capac
   }
   if (n_finished) *n_finished = nf;
   return FFVGPU_OK;
+}
+
+// Stops one running instance: its device state is marked done (status 4,
+// stream-ordered, so the next replay skips its blocks), its blocks leave the
+// active list, and its result records the iterations completed so far.
+ffvgpu_status ffvgpu_mixed_cancel(ffvgpu_pool* P, int32_t inst) {
+  ffvgpu_instance* I = get_inst(P, inst);
+  if (!I) return bad("bad instance");
+  if (!I->running) return bad("instance is not solving");
+  cudaSetDevice(P->device);
+  // done and status are adjacent int32 fields of SolveState
+  static_assert(offsetof(SolveState, status) == offsetof(SolveState, done) + 4,
+                "SolveState layout");
+  int32_t* flags = reinterpret_cast<int32_t*>(P->host_done);  // pinned
+  flags[0] = 1;
+  flags[1] = 4;
+  CK(cudaMemcpyAsync(&P->mst[inst].done, flags, 2 * sizeof(int32_t), cudaMemcpyHostToDevice,
+                     P->stream));
+  CK(cudaMemcpyAsync(P->mst_h + inst, P->mst + inst, sizeof(SolveState), cudaMemcpyDeviceToHost,
+                     P->stream));
+  CK(cudaStreamSynchronize(P->stream));
+  const SolveState& h = P->mst_h[inst];
+  I->running = false;
+  I->status = 4;
+  I->timeout_where = 0;
+  I->result.count = h.iter > 1 ? h.iter - 1 : 0;  // iterations with a residual
+  I->result.residual = h.residual;
+  I->last_iter = I->result.count;
+  return publish_active(P);
 }
 
 ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* P, int32_t inst, ffvgpu_result* res,
@@ -756,7 +800,7 @@ ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* P, int32_t inst, ffvgpu_
       CK(download_sync(const_cast<ffvgpu_pool*>(P), history,
                        P->mhist + (size_t)inst * P->mhist_cap, sizeof(double) * nh));
   }
-  return result_status(I.result, I.status, I.epsilon, I.count_max);
+  return result_status(I.result, I.status, I.epsilon, I.count_max, I.timeout_where);
 }
 
 ffvgpu_status ffvgpu_solve_mixed(ffvgpu_pool* P, const ffvgpu_mixed_params* prm,

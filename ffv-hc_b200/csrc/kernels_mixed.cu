@@ -556,7 +556,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     double E[2][4] = {};
     // this block's copy (issued a block ago): coefficients and guides, or
     // for a uniform block its vectors and guides
-    async::mbar_wait(bar, phase, &abort_flag, ROLE_SWEEP);
+    async::mbar_wait(bar, phase, &abort_flag, ROLE_SWEEP, C.wait_ns);
     const bool uni = s_uni[phase];
     const double* sd = reinterpret_cast<const double*>(slot);
     const size_t gbase = (size_t)blk * BLOCK_CELLS;
@@ -624,17 +624,20 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     async::fence_proxy_async();
     __syncthreads();
     if (abort_flag) {
-      // the copy never landed: stop every instance this CTA still had to
-      // sweep, give the copy a bounded time to drain, and leave
+      // the copy did not land in time: wait (bounded by DRAIN_NS, whatever
+      // the wait limit) until it has, so that the CTA never exits with a
+      // copy into its shared memory in flight, stop every instance this CTA
+      // still had to sweep, and leave.  Only one copy is ever in flight: the
+      // next block's is issued after this check.
       if (tid == 0) {
+        const bool drained = async::mbar_drain(bar, phase);
+        const int where = ROLE_SWEEP | (drained ? 0 : async::ROLE_DRAIN);
         for (int it2 = item; it2 < n_act; it2 += gridDim.x) {
           const int i2 = C.inst.blk_inst[C.active[it2]];
           if (i2 < 0) continue;
-          atomicOr(&C.inst.st[i2].timeout_where, ROLE_SWEEP);
+          atomicOr(&C.inst.st[i2].timeout_where, where);
           atomicExch(&C.inst.st[i2].status, 3);
           atomicExch(&C.inst.st[i2].done, 1);
-        }
-        for (uint32_t n = 0; n < (1u << 24) && !async::mbar_try_wait(bar, phase); ++n) {
         }
       }
       return;

@@ -264,7 +264,7 @@ ffvgpu_status explicit_neighbors(ffvgpu_pool* P, const ffvgpu_grid_desc* d) {
 
 ffvgpu_status solve_status(const SolveState& h, const ffvgpu_iter_params* prm, int N, int count) {
   if (h.status == 3) {
-    g_last_error = "a bounded device wait gave up (roles " + std::to_string(h.timeout_where) + ")";
+    g_last_error = timeout_message(h.timeout_where);
     return FFVGPU_TIMEOUT;
   }
   if (h.status == 2) {
@@ -317,13 +317,9 @@ ffvgpu_status ffvgpu_pool_create(const ffvgpu_grid_desc* d, ffvgpu_pool** out) {
   for (int f = 0; f < 6; ++f)
     if (d->bc_type[f] != FFVGPU_BC_DIRICHLET && d->bc_type[f] != FFVGPU_BC_NEUMANN)
       return bad("outer BC type must be Dirichlet or Neumann");
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    g_last_error = "no CUDA device";
-    return FFVGPU_NO_DEVICE;
-  }
+  // every check of the description runs on the host, before the device is
+  // touched, so a malformed grid is BAD_ARG whether or not a device is there
   ffvgpu_pool* P = new ffvgpu_pool();
-  cudaGetDevice(&P->device);
   P->nb = d->num_blocks;
   P->level.assign(d->level, d->level + P->nb);
   P->index.assign(d->block_index, d->block_index + 3 * P->nb);
@@ -359,6 +355,13 @@ ffvgpu_status ffvgpu_pool_create(const ffvgpu_grid_desc* d, ffvgpu_pool** out) {
     delete P;
     return s;
   }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    delete P;
+    g_last_error = "no CUDA device";
+    return FFVGPU_NO_DEVICE;
+  }
+  cudaGetDevice(&P->device);
   // the grid is instance 0 of its own pool
   P->inst.resize(1);
   ffvgpu_instance& I = P->inst[0];
@@ -409,6 +412,13 @@ ffvgpu_status ffvgpu_pool_set_stream(ffvgpu_pool* P, void* stream) {
   cudaSetDevice(P->device);
   CK(cudaStreamSynchronize(P->stream));
   P->stream = stream ? (cudaStream_t)stream : P->own_stream;
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_pool_set_wait_limit(ffvgpu_pool* P, double seconds) {
+  if (!P) return bad("null pool");
+  if (!(seconds >= 0.0 && seconds <= 3600.0)) return bad("wait limit must lie in [0, 3600] s");
+  P->wait_ns = (uint64_t)(seconds * 1e9);
   return FFVGPU_OK;
 }
 
@@ -640,7 +650,10 @@ ffvgpu_status ffvgpu_calc_r2(ffvgpu_pool* P, double* rr) {
   SolveState h;
   if ((s = read_state(P, &h))) return s;
   *rr = h.rr;
-  if (h.status == 3) return bad("a bounded device wait gave up");
+  if (h.status == 3) {
+    g_last_error = timeout_message(h.timeout_where);
+    return FFVGPU_TIMEOUT;
+  }
   return FFVGPU_OK;
 }
 
@@ -657,7 +670,12 @@ ffvgpu_status ffvgpu_rbgs_sweep(ffvgpu_pool* P, double omega) {
   P->xcur = 1 - P->xcur;
   launch_exchange(P->stream, P->ctx(P->bc_p), P->x[P->xcur], P->gx);
   CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(P->stream));
+  SolveState h;
+  if ((s = read_state(P, &h))) return s;
+  if (h.status == 3) {
+    g_last_error = timeout_message(h.timeout_where);
+    return FFVGPU_TIMEOUT;
+  }
   return FFVGPU_OK;
 }
 
@@ -724,7 +742,9 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   SolveState h;
   if ((s = read_state(P, &h))) return s;
   const bool early = h.count >= 1 && h.count < N;  // stopped before the last pass
-  const int m = early ? h.count : ((h.count == N) ? N : N);  // iterate kept
+  // iterate kept: the stopping iteration's after an early stop; otherwise
+  // (the solve ran to countMax, or converged on its last residual) iterate N
+  const int m = early ? h.count : N;
   // passes that ran: sweeps 1..min(m+1, N), residual-only pass only at the end
   bytes = interior_bytes(P, 2) + interior_bytes(P, 10) * (early ? (m + 1) : N) +
           (early ? 0 : interior_bytes(P, 9));

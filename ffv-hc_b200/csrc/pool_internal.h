@@ -27,6 +27,23 @@ inline ffvgpu_status bad(const char* why) {
   return FFVGPU_BAD_ARG;
 }
 
+// Message of a solve that a bounded device wait ended: which roles gave up
+// (SolveState::timeout_where bits).
+inline std::string timeout_message(int where) {
+  std::string m = "a bounded device wait gave up (";
+  const char* names[] = {"producer", "gatherer", "consumer", "sweep", "drain"};
+  bool any = false;
+  for (int b = 0; b < 5; ++b)
+    if (where & (1 << b)) {
+      m += any ? ", " : "";
+      m += names[b];
+      any = true;
+    }
+  m += any ? ")" : "no role recorded)";
+  if (where & 16) m += "; a copy into shared memory was still in flight when its CTA exited";
+  return m;
+}
+
 constexpr size_t BC = BLOCK_CELLS;
 
 }  // namespace detail
@@ -45,7 +62,8 @@ struct ffvgpu_instance {
   int32_t first = 0, count = 0;
   int32_t count_max = 0;
   double epsilon = 0.0;
-  int32_t status = 0;  // of the last solve: 0 ok, 2 NaN/Inf residual
+  int32_t status = 0;  // of the last solve: 0 ok, 2 NaN/Inf residual, 3 a device wait gave up
+  int32_t timeout_where = 0;  // roles whose wait gave up (SolveState::timeout_where)
   int32_t last_iter = 0;  // iterations with a residual before an early exit
   int32_t ublocks = 0;    // blocks with the same coefficients in every cell (known after a poll)
   ffvgpu_result result{};
@@ -67,6 +85,7 @@ struct ffvgpu_pool {
   ffvgpu::BCSet bc_p;  // pressure BCs
   ffvgpu::BCSet bc_u[3];
   int64_t bytes = 0;
+  uint64_t wait_ns = ffvgpu::DEFAULT_WAIT_NS;  // limit of every bounded device wait
 
   // fields (device, colour-split interiors)
   double* x[2] = {nullptr, nullptr};
@@ -129,6 +148,7 @@ struct ffvgpu_pool {
   int mgraph_iters = 0;
   double mgraph_omega = 0.0;
   int mgraph_sweeps = 0, mgraph_per = 0;
+  uint64_t mgraph_wait_ns = 0;
   int64_t m_launches = 0;
   int64_t m_bytes = 0;
   // active-block list of the persistent kernels: device [1 + capacity]
@@ -146,6 +166,7 @@ struct ffvgpu_pool {
     C.bc = bc;
     C.nb = nb;
     C.first = 0;
+    C.wait_ns = wait_ns;
     return C;
   }
 };

@@ -28,11 +28,14 @@
 // Stencil neighbours are read straight from the colour-split tile: every
 // neighbour of a cell of one colour lies in the other colour's half, and
 // cells on the block surface take the guide buffer instead.
-// Every wait on an mbarrier is bounded in time; a wait that gives up raises
-// the CTA's abort flag, every role leaves its loop, the producer drains the
-// copies it has in flight, and the solver state reports TIMEOUT.
+// Every wait on an mbarrier is bounded in time (KCtx::wait_ns); a wait that
+// gives up raises the CTA's abort flag, every role leaves its loop, the
+// producer waits for the copies it has in flight to land (bounded by
+// DRAIN_NS, independently of the wait limit; a drain that gives up is
+// reported as ROLE_DRAIN), and the solver state reports TIMEOUT.
 #include <cfloat>
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "ffvgpu_async.cuh"
@@ -56,7 +59,6 @@ constexpr int CONS0 = GATHER0 + 32 * GATHER_WARPS;
 constexpr int NTHREADS = CONS0 + 32 * CONSUMER_WARPS;  // 800
 constexpr int NCONS = 32 * CONSUMER_WARPS;            // one cell per consumer per slot
 constexpr int NGATHER = 32 * GATHER_WARPS;
-constexpr uint32_t DRAIN_LIMIT = 1u << 24;    // polls while draining copies in flight
 enum { ROLE_PRODUCER = 1, ROLE_GATHER = 2, ROLE_CONSUMER = 4 };
 
 struct __align__(128) Smem {
@@ -163,7 +165,8 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       for (; !skip && ok && g < (uint32_t)total_slots; ++g) {
         const int s = g % STAGES;
         const uint32_t u = g / STAGES;
-        if (!(ok = mbar_wait(&S.empty[s], (u & 1) ^ 1, abort_flag, ROLE_PRODUCER))) break;
+        if (!(ok = mbar_wait(&S.empty[s], (u & 1) ^ 1, abort_flag, ROLE_PRODUCER, C.wait_ns)))
+          break;
         issue_slot(g);
         const int m = g / SLOTS, j = g % SLOTS;
         const int blk = blockIdx.x + m * gridDim.x;
@@ -172,7 +175,8 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
           // the consumers are in block m)
           const int xb = (m + 1) & 1;
           if (m >= 1 &&
-              !(ok = mbar_wait(&S.xempty[xb], ((m - 1) >> 1) & 1, abort_flag, ROLE_PRODUCER)))
+              !(ok = mbar_wait(&S.xempty[xb], ((m - 1) >> 1) & 1, abort_flag, ROLE_PRODUCER,
+                               C.wait_ns)))
             break;
           ++nx[xb];
           mbar_expect_tx(&S.xfull[xb], BLOCK_CELLS * 8);
@@ -182,16 +186,18 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       }
       // Drain: the last armed phase of every barrier a copy completes on must
       // complete before the CTA may exit (copies land in its shared memory).
+      // Each barrier has at most one copy in flight (a slot or tile buffer is
+      // refilled only after the consumers released it, which they do after
+      // its copy landed), so the last armed phase completing means every
+      // copy on it has landed.
+      bool drained = true;
       for (int s = 0; s < STAGES; ++s) {
         const uint32_t issued = (g > (uint32_t)s) ? (g - 1 - s) / STAGES + 1 : 0;
-        if (issued)
-          for (uint32_t i = 0; i < DRAIN_LIMIT; ++i)
-            if (mbar_try_wait(&S.full[s], (issued - 1) & 1)) break;
+        if (issued) drained = mbar_drain(&S.full[s], (issued - 1) & 1) && drained;
       }
       for (int b = 0; b < 2; ++b)
-        if (nx[b])
-          for (uint32_t i = 0; i < DRAIN_LIMIT; ++i)
-            if (mbar_try_wait(&S.xfull[b], (nx[b] - 1) & 1)) break;
+        if (nx[b]) drained = mbar_drain(&S.xfull[b], (nx[b] - 1) & 1) && drained;
+      if (!drained) atomicOr((int*)abort_flag, ROLE_DRAIN);
     } else {
       asm volatile("griddepcontrol.wait;" ::: "memory");
     }
@@ -204,7 +210,9 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
     const bool skip = *((volatile const int32_t*)&st->done) != 0;
     for (int blk = blockIdx.x; !skip && blk < nb; blk += gridDim.x, ++m) {
       const int gb = m & 1;
-      if (m >= 2 && !mbar_wait(&S.gempty[gb], ((m - 2) >> 1) & 1, abort_flag, ROLE_GATHER)) break;
+      if (m >= 2 &&
+          !mbar_wait(&S.gempty[gb], ((m - 2) >> 1) & 1, abort_flag, ROLE_GATHER, C.wait_ns))
+        break;
       const double dx = C.dx[blk];
       // two groups of 128 threads take alternate faces; each thread resolves
       // two positions of its face with all their loads in flight
@@ -239,8 +247,8 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
     for (int blk = blockIdx.x; !skip && blk < nb; blk += gridDim.x, ++m) {
       const int xb = m & 1;
       const uint32_t par = (m >> 1) & 1;
-      live = live && mbar_wait(&S.xfull[xb], par, abort_flag, ROLE_CONSUMER);
-      live = live && mbar_wait(&S.gfull[xb], par, abort_flag, ROLE_CONSUMER);
+      live = live && mbar_wait(&S.xfull[xb], par, abort_flag, ROLE_CONSUMER, C.wait_ns);
+      live = live && mbar_wait(&S.gfull[xb], par, abort_flag, ROLE_CONSUMER, C.wait_ns);
       const double* T = S.xt[xb];
       const double* G = S.gbuf[xb];
       double* xo = xout + (size_t)blk * BLOCK_CELLS;
@@ -250,7 +258,8 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       const int h = ct >> 8, t = ct & 255;
       for (int mm = 0; mm < SLOTS / 2; ++mm, ++g) {
         const int s = g % STAGES;
-        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
+        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER,
+                                 C.wait_ns);
         Coef c = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         if (live) c = load_coef(S.ring[s][h], t);
         hold(c);
@@ -276,7 +285,8 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       // colour 1: residual against the old colour-0 values, update against the new
       for (int mm = 0; mm < SLOTS / 2; ++mm, ++g) {
         const int s = g % STAGES;
-        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER);
+        live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER,
+                                 C.wait_ns);
         Coef c = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         if (live) c = load_coef(S.ring[s][h], t);
         hold(c);
@@ -362,20 +372,41 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
 }
 
 namespace {
-int g_sm_count = 0;
-bool g_attr_set[4] = {false, false, false, false};
+// Per-device launch data: SM count (grid size) and whether the dynamic
+// shared-memory limit of each instantiation has been raised on that device
+// (cudaFuncSetAttribute applies to the current device only).
+constexpr int MAX_DEVICES = 64;
+struct DeviceCache {
+  int sm_count = 0;
+  bool attr_set[3] = {false, false, false};
+};
+std::mutex g_cache_mu;
+DeviceCache g_cache[MAX_DEVICES];
 
 template <bool R, bool W>
 void launch_one(cudaStream_t s, const KCtx& C, const double* xin, double* xout,
                 const double* stream, const double* gst, double omega, double* partials,
                 SolveState* st, int fin, int iter, int slot, bool pdl) {
   const size_t smem = sizeof(pipe::Smem);
-  if (!g_attr_set[slot]) {
-    cudaFuncSetAttribute(rbgs_pipelined_kernel<R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    g_attr_set[slot] = true;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int sms = 0;
+  {
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    DeviceCache local;
+    DeviceCache& D = (dev >= 0 && dev < MAX_DEVICES) ? g_cache[dev] : local;
+    if (D.sm_count == 0) {
+      cudaDeviceGetAttribute(&D.sm_count, cudaDevAttrMultiProcessorCount, dev);
+      if (D.sm_count <= 0) D.sm_count = 1;
+    }
+    if (!D.attr_set[slot]) {
+      cudaFuncSetAttribute(rbgs_pipelined_kernel<R, W>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      D.attr_set[slot] = true;
+    }
+    sms = D.sm_count;
   }
-  const int grid = C.nb < g_sm_count ? C.nb : g_sm_count;
+  const int grid = C.nb < sms ? C.nb : sms;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(pipe::NTHREADS);
@@ -394,12 +425,6 @@ void launch_one(cudaStream_t s, const KCtx& C, const double* xin, double* xout,
 void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
                  double* xout, const double* stream, const double* gst, double omega,
                  double* partials, SolveState* st, int fin, int iter, bool pdl) {
-  if (g_sm_count == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sm_count <= 0) g_sm_count = 1;
-  }
   if (res && sweep)
     launch_one<true, true>(s, C, xin, xout, stream, gst, omega, partials, st, fin, iter, 0, pdl);
   else if (sweep)

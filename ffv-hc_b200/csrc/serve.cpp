@@ -49,9 +49,39 @@ ffvgpu_status ffvgpu_serve(ffvgpu_pool* P, const ffvgpu_mixed_params* prm, int32
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   };
   std::vector<int32_t> done(P->inst.size());
+  auto cancelled = [&](int k, double t) { return req[k].cancel_s > 0.0 && req[k].cancel_s <= t; };
   while (finished < n && status == FFVGPU_OK) {
     const double t = now();
     while (next < n && req[next].arrival_s <= t) waiting.push_back(next++);
+    // withdraw what has passed its cancel time: waiting requests are dropped,
+    // running solves stopped and their blocks released
+    for (auto it = waiting.begin(); it != waiting.end();) {
+      if (!cancelled(*it, t)) {
+        ++it;
+        continue;
+      }
+      out[*it].finish_s = now();
+      out[*it].status = FFVGPU_CANCELLED;
+      ++finished;
+      it = waiting.erase(it);
+    }
+    for (int inst = 0; inst < (int)slot_req.size() && status == FFVGPU_OK; ++inst) {
+      const int k = slot_req[inst];
+      if (k < 0 || !cancelled(k, t)) continue;
+      if ((status = ffvgpu_mixed_cancel(P, inst)) != FFVGPU_OK) break;
+      ffvgpu_result r;
+      ffvgpu_instance_result(P, inst, &r, nullptr);
+      out[k].finish_s = now();
+      out[k].count = r.count;
+      out[k].residual = r.residual;
+      out[k].status = FFVGPU_CANCELLED;
+      slot_req[inst] = -1;
+      --running;
+      ++finished;
+      status = ffvgpu_instance_release(P, inst);
+    }
+    if (status != FFVGPU_OK) break;
+    if (finished >= n) break;
     // admit in arrival order; a request that does not fit waits
     for (auto it = waiting.begin(); it != waiting.end();) {
       const int k = *it;

@@ -12,7 +12,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libffvhc_b200.so")
 
-OK, NOT_CONVERGED, NAN_DETECTED, TIMEOUT, OOM, BAD_ARG, CUDA_ERROR, NO_DEVICE = range(8)
+OK, NOT_CONVERGED, NAN_DETECTED, TIMEOUT, OOM, BAD_ARG, CUDA_ERROR, NO_DEVICE, CANCELLED = range(9)
 BC_DIRICHLET, BC_NEUMANN = 0, 1
 NB_OUTER, NB_SAME, NB_COARSE, NB_FINE = range(4)
 
@@ -42,6 +42,7 @@ EXPORTS = [
     "ffvgpu_assemble_sphere", "ffvgpu_instance_fill", "ffvgpu_serve",
     "ffvgpu_solve_rbgs_fixed_average", "ffvgpu_dump2", "ffvgpu_load2",
     "ffvgpu_restart_filename", "ffvgpu_remove_p", "ffvgpu_corr_u", "ffvgpu_mixed_autotune",
+    "ffvgpu_pool_set_wait_limit", "ffvgpu_mixed_cancel",
 ]
 
 
@@ -128,7 +129,8 @@ TUNE_SPACE = [(om, sw, per, it) for om in (1.5, 1.2) for (sw, per) in
 
 
 class Request(ctypes.Structure):
-    _fields_ = [("arrival_s", ctypes.c_double), ("problem", SphereProblem)]
+    _fields_ = [("arrival_s", ctypes.c_double), ("cancel_s", ctypes.c_double),
+                ("problem", SphereProblem)]
 
 
 class RequestResult(ctypes.Structure):
@@ -160,6 +162,7 @@ def lib():
         L.ffvgpu_pool_device_bytes.restype = ctypes.c_int64
         L.ffvgpu_pool_neighbors.argtypes = [vp, i32, vp, vp]
         L.ffvgpu_pool_set_stream.argtypes = [vp, vp]
+        L.ffvgpu_pool_set_wait_limit.argtypes = [vp, dbl]
         L.ffvgpu_fill.argtypes = [vp, i32, dbl]
         L.ffvgpu_grid_neighbors.argtypes = [ctypes.POINTER(GridDesc), vp, vp]
         L.ffvgpu_pool_upload.argtypes = [vp, i32, vp, i32]
@@ -208,6 +211,7 @@ def lib():
         L.ffvgpu_mixed_begin.argtypes = [vp, i32, MP]
         L.ffvgpu_mixed_advance.argtypes = [vp, i32]
         L.ffvgpu_mixed_poll.argtypes = [vp, vp, i32, vp]
+        L.ffvgpu_mixed_cancel.argtypes = [vp, i32]
         L.ffvgpu_instance_result.argtypes = [vp, i32, R, vp]
         _lib = L
     return _lib
@@ -461,6 +465,10 @@ class Pool:
         _check(lib().ffvgpu_pool_set_stream(self._h, ctypes.c_void_p(stream_handle or None)),
                "pool_set_stream")
 
+    def set_wait_limit(self, seconds):
+        """Time limit of every bounded device wait (ffvgpu_pool_set_wait_limit)."""
+        _check(lib().ffvgpu_pool_set_wait_limit(self._h, float(seconds)), "pool_set_wait_limit")
+
     def fill(self, field, value):
         _check(lib().ffvgpu_fill(self._h, FIELD[field], float(value)), "fill")
 
@@ -598,6 +606,9 @@ class Batch:
         _check(lib().ffvgpu_pool_set_stream(self._h, ctypes.c_void_p(stream_handle or None)),
                "pool_set_stream")
 
+    def set_wait_limit(self, seconds):
+        _check(lib().ffvgpu_pool_set_wait_limit(self._h, float(seconds)), "pool_set_wait_limit")
+
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
                     epsilon=1e-8, check_every=0, restart_drop=None, restart_growth=None,
                     restart_every=None):
@@ -612,13 +623,14 @@ class Batch:
 
     def serve(self, arrivals, problems, iterations_per_step=8, omega=1.5, sweeps=8,
               sweeps_per_exchange=4, count_max=5000, epsilon=1e-8, restart_drop=None,
-              restart_growth=None, restart_every=None):
+              restart_growth=None, restart_every=None, cancels=None):
         """Request loop (ffvgpu_serve): per request admit/finish times, iterations,
-        residual, status, blocks."""
+        residual, status, blocks.  cancels: optional per-request cancel times (0: never)."""
         n = len(problems)
         req = (Request * n)()
         for i, (t, p) in enumerate(zip(arrivals, problems)):
             req[i].arrival_s = float(t)
+            req[i].cancel_s = float(cancels[i]) if cancels is not None else 0.0
             req[i].problem = p
         out = (RequestResult * n)()
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, 0, None,
@@ -653,6 +665,9 @@ class Batch:
                           *_restart(restart_drop, restart_growth, restart_every))
         _check(lib().ffvgpu_mixed_begin(self._h, inst, ctypes.byref(prm)), "mixed_begin")
 
+    def cancel(self, inst):
+        _check(lib().ffvgpu_mixed_cancel(self._h, inst), "mixed_cancel")
+
     def advance(self, iterations):
         _check(lib().ffvgpu_mixed_advance(self._h, iterations), "mixed_advance")
 
@@ -668,7 +683,7 @@ class Batch:
         hist = np.zeros(max(count_max or 1, 1), np.float64)
         st = lib().ffvgpu_instance_result(self._h, inst, ctypes.byref(res),
                                           _ptr(hist) if count_max else None)
-        _check(st, "instance_result", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
+        _check(st, "instance_result", allow=(OK, NOT_CONVERGED, NAN_DETECTED, CANCELLED))
         out = dict(status=st, count=res.count, residual=res.residual)
         if count_max:
             n = res.count if 1 <= res.count <= count_max else (count_max if res.count > 0 else 0)

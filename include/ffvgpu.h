@@ -35,7 +35,9 @@ typedef enum {
   FFVGPU_OOM = 4,           /* device allocation failed */
   FFVGPU_BAD_ARG = 5,       /* invalid argument or grid description */
   FFVGPU_CUDA_ERROR = 6,    /* a CUDA runtime call failed */
-  FFVGPU_NO_DEVICE = 7      /* no CUDA device visible */
+  FFVGPU_NO_DEVICE = 7,     /* no CUDA device visible */
+  FFVGPU_CANCELLED = 8      /* the solve was stopped by ffvgpu_mixed_cancel or a serve
+                               request's cancel time (no counterpart in the reference) */
 } ffvgpu_status;
 
 /* Outer boundary types, src/FFV/FFVBC.h:6-14. */
@@ -132,6 +134,13 @@ int32_t ffvgpu_pool_num_blocks(const ffvgpu_pool* pool);
 /* Runs the pool's work on the caller's CUDA stream (cudaStream_t passed as
  * void*; NULL = the pool's own stream).  All later calls enqueue there. */
 ffvgpu_status ffvgpu_pool_set_stream(ffvgpu_pool* pool, void* stream);
+/* Time limit, in seconds, of every bounded wait inside the pool's kernels
+ * (default 4; 0 to 3600).  A wait that runs out ends the solve with
+ * FFVGPU_TIMEOUT (ffvgpu_last_error names the roles that gave up) and leaves
+ * the pool usable; copies already in flight are waited for before a kernel
+ * exits, whatever the limit.  The reference has no device waits: its
+ * counterpart is the MPI runtime's own timeouts. */
+ffvgpu_status ffvgpu_pool_set_wait_limit(ffvgpu_pool* pool, double seconds);
 /* Neighbour table as derived (kind [6], ids [6][4]); for tests. */
 ffvgpu_status ffvgpu_pool_neighbors(const ffvgpu_pool* pool, int32_t block,
                                     int32_t* kind6, int32_t* ids24);
@@ -221,9 +230,12 @@ ffvgpu_status ffvgpu_dot(ffvgpu_pool* pool, ffvgpu_field x, ffvgpu_field y, doub
  * library, FFVGPU_NOALLOC_MAX_BLOCKS doubles per GPU, held until the process
  * exits; larger num_blocks is rejected with FFVGPU_BAD_ARG.  The first call
  * on a device looks the array up for that device, so make it before any
- * stream capture.  Every call on a device shares the array: calls that
- * overlap on the GPU race and must be serialised by the caller.  The call is
- * asynchronous on the stream. */
+ * stream capture; the address is kept for the life of the process, which
+ * assumes the device's primary context is never reset (no cudaDeviceReset
+ * between calls).  stream must belong to the device current at the call.
+ * Every call on a device shares the array: calls that overlap on the GPU
+ * race and must be serialised by the caller.  The call is asynchronous on
+ * the stream. */
 #define FFVGPU_NOALLOC_MAX_BLOCKS 65536
 ffvgpu_status ffvgpu_dot_noalloc(const double* x, const double* y, int32_t num_blocks,
                                  double* result, void* stream);
@@ -413,6 +425,11 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* pool, int32_t instance,
 ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* pool, int32_t iterations);
 ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* pool, int32_t* finished, int32_t capacity,
                                 int32_t* n_finished);
+/* Stops one running instance before its next replay: its solve ends with
+ * FFVGPU_CANCELLED, its result holds the iterations completed and the last
+ * residual, its x is the iterate of the last completed iteration, and it can
+ * be released or begun again. */
+ffvgpu_status ffvgpu_mixed_cancel(ffvgpu_pool* pool, int32_t instance);
 /* history: optional host array receiving min(count, count_max) residuals. */
 ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* pool, int32_t instance,
                                      ffvgpu_result* res, double* history);
@@ -446,12 +463,16 @@ ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* pool, const int32_t* instances,
  * not fit waits while later, smaller ones may pass it -- and join the
  * running solves at the next graph replay; every replay advances all running
  * solves by iterations_per_step iterations; a solve that ends has its
- * pressure copied to the host and its blocks released.  out[i] receives
- * request i's admission and completion times (same clock), iterations,
- * residual, status and block count.  On an error the pool may still hold
+ * pressure copied to the host and its blocks released; a request whose
+ * cancel time passes first is dropped or stopped instead.  out[i] receives
+ * request i's admission and completion (or cancellation) times (same clock),
+ * iterations, residual, status and block count.  On an error the pool may still hold
  * admitted instances: destroy it. */
 typedef struct {
   double arrival_s;
+  double cancel_s;  /* withdrawn at this time (same clock) if not finished by then:
+                       dropped while waiting, stopped while solving (its blocks are
+                       released); status FFVGPU_CANCELLED.  0: never */
   ffvgpu_sphere_problem problem;
 } ffvgpu_request;
 

@@ -26,9 +26,10 @@
 //
 // Reductions.  The reference sums each block serially (i fastest) and then
 // sums blocks under an OpenMP reduction, whose order is not deterministic.
-// RED_REFERENCE follows the per-block serial order and adds blocks in id
-// order (one OpenMP thread).  RED_CANONICAL reproduces the fixed two-level
-// tree the CUDA path uses, so that Krylov scalars can be compared bit for bit.
+// RED_REFERENCE follows the per-block serial order and adds the block sums
+// in id order (block sums taken on all threads, added by one).
+// RED_CANONICAL reproduces the fixed two-level tree the CUDA path uses, so
+// that Krylov scalars can be compared bit for bit.
 
 #include <cmath>
 #include <cfloat>
@@ -591,7 +592,10 @@ double DOT(Oracle& O, int fx, int fy) {
   Grid& G = O.G;
   const int n = G.n;
   if (O.red_mode == RED_REFERENCE) {
-    double xy_local = 0.0;
+    // per-block sums on all threads, then added in block order: the same
+    // bits as one thread doing both
+    std::vector<double> part(G.nb);
+#pragma omp parallel for num_threads(O.nthreads) schedule(static)
     for (int bi = 0; bi < G.nb; ++bi) {
       const double* x = O.F(fx, bi);
       const double* y = O.F(fy, bi);
@@ -602,8 +606,10 @@ double DOT(Oracle& O, int fx, int fy) {
             const long m = IDX(G, i, j, k);
             xy = xy + x[m] * y[m];
           }
-      xy_local += xy;
+      part[bi] = xy;
     }
+    double xy_local = 0.0;
+    for (int bi = 0; bi < G.nb; ++bi) xy_local += part[bi];
     return xy_local;
   }
   std::vector<double> part(G.nb);
@@ -629,15 +635,18 @@ double SUM(Oracle& O, int fx) {
   Grid& G = O.G;
   const int n = G.n;
   if (O.red_mode == RED_REFERENCE) {
-    double sum_l = 0.0;
+    std::vector<double> part(G.nb);
+#pragma omp parallel for num_threads(O.nthreads) schedule(static)
     for (int bi = 0; bi < G.nb; ++bi) {
       const double* x = O.F(fx, bi);
       double dsum = 0.0;
       for (int k = 1; k <= n; ++k)
         for (int j = 1; j <= n; ++j)
           for (int i = 1; i <= n; ++i) dsum = dsum + x[IDX(G, i, j, k)];
-      sum_l += dsum;
+      part[bi] = dsum;
     }
+    double sum_l = 0.0;
+    for (int bi = 0; bi < G.nb; ++bi) sum_l += part[bi];
     return sum_l;
   }
   std::vector<double> part(G.nb);
@@ -663,7 +672,8 @@ double CalcR2(Oracle& O, int fx) {
   const double *Ap = nullptr;
   (void)Ap;
   if (O.red_mode == RED_REFERENCE) {
-    double rr_local = 0.0;
+    std::vector<double> part(G.nb);
+#pragma omp parallel for num_threads(O.nthreads) schedule(static)
     for (int bi = 0; bi < G.nb; ++bi) {
       const double* x = O.F(fx, bi);
       double rr = 0.0;  // bils.f90:256-304 calc_r2
@@ -676,8 +686,10 @@ double CalcR2(Oracle& O, int fx) {
                                     O.F(OF_AT, bi), x, O.F(OF_B, bi), m, sy, sz);
             rr = rr + r * r;
           }
-      rr_local += rr;
+      part[bi] = rr;
     }
+    double rr_local = 0.0;
+    for (int bi = 0; bi < G.nb; ++bi) rr_local += part[bi];
     return rr_local;
   }
   std::vector<double> part(G.nb);

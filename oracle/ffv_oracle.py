@@ -71,8 +71,112 @@ def lib():
         L.orc_rbgs_fixed_average.argtypes = [vp, dbl, ctypes.c_long, i32, dbl, vp, vp, vp]
         L.orc_bicgstab_restart.argtypes = [vp, dbl, i32, i32, dbl, dbl, vp, vp, vp]
         L.orc_mixed.argtypes = [vp, dbl, i32, i32, i32, dbl, dbl, dbl, i32, vp, vp, vp]
+        # the host sphere-grid generator compiled into this library
+        L.ffvgpu_sphere_grid_create.argtypes = [ctypes.POINTER(_SphereParams),
+                                                ctypes.POINTER(vp)]
+        L.ffvgpu_sphere_grid_destroy.argtypes = [vp]
+        L.ffvgpu_sphere_grid_destroy.restype = None
+        L.ffvgpu_sphere_grid_num_blocks.argtypes = [vp]
+        L.ffvgpu_sphere_grid_blocks.argtypes = [vp, vp, vp]
+        L.ffvgpu_sphere_grid_blocks.restype = None
+        L.ffvgpu_sphere_grid_fill.argtypes = [vp, ctypes.c_uint64, dbl, i32, vp, vp, vp, vp, vp,
+                                              vp]
         _lib = L
     return _lib
+
+
+# ---------------------------------------------------------------------------
+# Inputs of the sphere-flow workload, built with the generator compiled into
+# this library (the same source as the device library's host generator), so
+# that CPU-only runs never load the device library.
+# ---------------------------------------------------------------------------
+BC_DIRICHLET, BC_NEUMANN = 0, 1
+# Pressure BCs of the sphere example (examples/FlowPastASphere/sphere.tpp):
+# Neumann 0 at the inlet (X_M) and side walls, Dirichlet 0 at the outlet (X_P).
+P_BC_TYPE = (BC_NEUMANN, BC_DIRICHLET, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN)
+P_BC_VALUE = (0.0,) * 6
+# Velocity BCs: inlet Dirichlet (1,0,0); outlet and walls Neumann 0.
+U_BC_TYPE = (BC_DIRICHLET, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN)
+U_BC_VALUE = {"UX": (1.0, 0, 0, 0, 0, 0), "UY": (0.0,) * 6, "UZ": (0.0,) * 6}
+FLOW_PAST_SPHERE = dict(domain_origin=(-4.0, -4.0, -4.0), root_grid=(4, 2, 2), root_length=4.0,
+                        center=(0.0, 0.0, 0.0), radius=0.5, margin=0.5)
+
+
+class _SphereParams(ctypes.Structure):
+    _fields_ = [
+        ("domain_origin", ctypes.c_double * 3), ("root_grid", ctypes.c_int32 * 3),
+        ("root_length", ctypes.c_double), ("max_level", ctypes.c_int32),
+        ("center", ctypes.c_double * 3), ("radius", ctypes.c_double),
+        ("margin", ctypes.c_double),
+    ]
+
+
+class SphereGrid:
+    """2:1-balanced octree of 16^3 leaf blocks refined around a sphere, and its
+    per-cell inputs in the reference layout (the device library's SphereGrid,
+    from this library's copy of the generator)."""
+
+    def __init__(self, max_level, **kw):
+        p = dict(FLOW_PAST_SPHERE)
+        p.update(kw)
+        self.params = p
+        self.max_level = max_level
+        sp = _SphereParams(p["domain_origin"], p["root_grid"], p["root_length"], max_level,
+                           p["center"], p["radius"], p["margin"])
+        self._h = ctypes.c_void_p()
+        if lib().ffvgpu_sphere_grid_create(ctypes.byref(sp), ctypes.byref(self._h)) != 0:
+            raise ValueError("sphere grid parameters rejected")
+        self.nb = lib().ffvgpu_sphere_grid_num_blocks(self._h)
+        self.level = np.zeros(self.nb, np.int32)
+        self.index = np.zeros((self.nb, 3), np.int32)
+        lib().ffvgpu_sphere_grid_blocks(self._h, self.level.ctypes.data, self.index.ctypes.data)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.ffvgpu_sphere_grid_destroy(self._h)
+            self._h = None
+
+    @property
+    def cells(self):
+        return self.nb * 4096
+
+    def fill(self, seed=0, sigma=0.01, vc=2):
+        """Per-cell inputs in the reference layout: dict of numpy arrays."""
+        w = 16 + 2 * vc
+        shape = (self.nb, w, w, w)
+        out = {k: np.zeros(shape, np.float64) for k in ("UX", "UY", "UZ")}
+        for f in range(6):
+            out[f"C{f}"] = np.zeros(shape, np.float64)
+            out[f"CID{f}"] = np.zeros(shape, np.int32)
+        out["PID"] = np.zeros(shape, np.int32)
+        c6 = (ctypes.c_void_p * 6)(*[out[f"C{f}"].ctypes.data for f in range(6)])
+        i6 = (ctypes.c_void_p * 6)(*[out[f"CID{f}"].ctypes.data for f in range(6)])
+        st = lib().ffvgpu_sphere_grid_fill(self._h, seed, sigma, vc, out["UX"].ctypes.data,
+                                           out["UY"].ctypes.data, out["UZ"].ctypes.data,
+                                           ctypes.cast(c6, ctypes.c_void_p),
+                                           ctypes.cast(i6, ctypes.c_void_p),
+                                           out["PID"].ctypes.data)
+        if st != 0:
+            raise ValueError("sphere_grid_fill failed")
+        return out
+
+
+def sphere_problem(max_level, seed=1, sigma=0.01, rhof=1.0, dt=0.002, threads=1,
+                   reduction=RED_REFERENCE, **grid_kw):
+    """The sphere-flow pressure problem on the CPU: grid, inputs, oracle with
+    u exchanged, A and b assembled and the BCs folded (UpdateP P02-P05)."""
+    g = SphereGrid(max_level, **grid_kw)
+    inp = g.fill(seed=seed, sigma=sigma, vc=2)
+    O = Oracle.from_grid(g, vc=2, bc_type=P_BC_TYPE, bc_value=P_BC_VALUE, threads=threads,
+                         reduction=reduction)
+    for k, v in inp.items():
+        O.field(k)[...] = v
+    del inp
+    for u in ("UX", "UY", "UZ"):
+        O.exchange(u, U_BC_TYPE, U_BC_VALUE[u])
+    O.assemble_p(rhof, dt)
+    O.fold_bc()
+    return g, O
 
 
 class Oracle:

@@ -15,12 +15,15 @@ def pytest_configure(config):
 
 
 def _ensure_built():
-    lib = os.path.join(ROOT, "ffv-hc_b200", "libffvhc_b200.so")
-    if not os.path.exists(lib):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "ffv-hc_b200")], check=True)
-    orc = os.path.join(ROOT, "oracle", "libffvoracle.so")
-    if not os.path.exists(orc):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    """make is idempotent: it rebuilds only what is older than its sources and
+    headers, so the tests never run against a stale library.  Where the source
+    tree travels without its build tools (a GPU host that runs the prebuilt
+    libraries), a library that exists is used as it is."""
+    for sub, lib in (("ffv-hc_b200", "libffvhc_b200.so"), ("oracle", "libffvoracle.so")):
+        d = os.path.join(ROOT, sub)
+        r = subprocess.run(["make", "-s", "-C", d], capture_output=True, text=True)
+        if r.returncode != 0 and not os.path.exists(os.path.join(d, lib)):
+            raise RuntimeError(f"building {sub} failed:\n{r.stdout}{r.stderr}")
 
 
 _ensure_built()

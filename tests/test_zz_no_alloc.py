@@ -5,10 +5,10 @@ all device memory to its own allocator, or a loop that must not stall on the
 synchronisation cudaMalloc/cudaFree bring): the caller passes device vectors
 and a device result, and the partial sums live in a fixed array compiled
 into the library.  Checked through the C ABI against the pool-based
-ffvgpu_dot on the same vectors (the same sum tree: bit equality), on two
-calls in a row, since every call reuses the same array.  This file is
-collected last so that a run stopping at the first failure has run every
-other test first.
+ffvgpu_dot and against the CPU oracle's dot in the same fixed sum order, on
+the same vectors (bit equality), on two calls in a row, since every call
+reuses the same array.  This file is collected last so that a run stopping
+at the first failure has run every other test first.
 """
 import ctypes
 
@@ -16,6 +16,7 @@ import numpy as np
 import pytest
 
 import ffvgpu
+import ffv_oracle as fo
 
 pytestmark = pytest.mark.gpu
 
@@ -37,6 +38,7 @@ def test_dot_noalloc_matches_pool_dot_on_consecutive_calls():
     torch.cuda.init()
     g = ffvgpu.SphereGrid(2)
     P = ffvgpu.Pool(g.desc())
+    O = fo.Oracle.from_grid(g, vc=2, reduction=fo.RED_CANONICAL)
     rng = np.random.default_rng(2024)
     w = 20
     perm = colour_split_order()
@@ -49,6 +51,9 @@ def test_dot_noalloc_matches_pool_dot_on_consecutive_calls():
         P.upload("X", x, 2)
         P.upload("B", b, 2)
         expected = P.dot("X", "B")
+        O.field("X")[...] = x
+        O.field("B")[...] = b
+        assert O.dot("X", "B") == expected, call
         xi = x[:, 2:18, 2:18, 2:18].reshape(g.nb, 4096)[:, perm]
         bi = b[:, 2:18, 2:18, 2:18].reshape(g.nb, 4096)[:, perm]
         xd = torch.from_numpy(np.ascontiguousarray(xi)).cuda()
@@ -61,6 +66,7 @@ def test_dot_noalloc_matches_pool_dot_on_consecutive_calls():
         got = float(result.item())
         assert got == expected, (call, got, expected)
     P.close()
+    O.close()
 
 
 def test_dot_noalloc_rejects_sizes_beyond_its_array():
