@@ -27,6 +27,7 @@ struct MixCtx {
   int capacity;
   int first;
   uint64_t wait_ns;    // limit of every bounded device wait (ffvgpu_pool_set_wait_limit)
+  int stall;           // test hook: the sweep issues no copy, so its first wait runs out
 };
 
 // CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel.

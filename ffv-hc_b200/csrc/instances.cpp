@@ -168,6 +168,7 @@ MixCtx mix_ctx(const ffvgpu_pool* P) {
   C.n_active = P->act_d;
   C.active = P->act_d + 1;
   C.wait_ns = P->wait_ns;
+  C.stall = P->stall_sweep;
   return C;
 }
 
@@ -694,7 +695,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
   // kernel arguments (the wait limit among them) are fixed at capture
   if (!P->mgraph || P->mgraph_iters != iterations || P->mgraph_omega != P->m_omega ||
       P->mgraph_sweeps != P->m_sweeps || P->mgraph_per != P->m_per_exchange ||
-      P->mgraph_wait_ns != P->wait_ns) {
+      P->mgraph_wait_ns != P->wait_ns || P->mgraph_stall != P->stall_sweep) {
     if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
     P->mgraph = nullptr;
     cudaGraph_t graph;
@@ -709,6 +710,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
     P->mgraph_sweeps = P->m_sweeps;
     P->mgraph_per = P->m_per_exchange;
     P->mgraph_wait_ns = P->wait_ns;
+    P->mgraph_stall = P->stall_sweep;
   }
   CK(cudaGraphLaunch(P->mgraph, P->stream));
   P->m_launches += (int64_t)iterations * launches_per_iteration(P);
@@ -741,6 +743,7 @@ ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* P, int32_t* finished, int32_t capac
     I.result.residual = h.residual;
     I.status = h.status;
     I.timeout_where = h.timeout_where;
+    P->stall_sweep = 0;  // the test hook covers one solve
     I.last_iter = (h.count == 0) ? h.iter : 0;  // 0 when the exit came before iteration 1
     launch_exchange(P->stream, range_ctx(P, P->bc_p, I), P->x[P->xcur], P->gx);  // FFVILS.h:973
     if (finished && nf < capacity) finished[nf] = i;
@@ -753,6 +756,15 @@ ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* P, int32_t* finished, int32_t capac
     CK(cudaStreamSynchronize(P->stream));
   }
   if (n_finished) *n_finished = nf;
+  return FFVGPU_OK;
+}
+
+// Test hook: the next mixed solve's sweep kernel waits for a copy it never
+// issues, so the wait runs out after the pool's wait limit and the solve ends
+// with FFVGPU_TIMEOUT; nothing is in flight, so nothing is drained.
+ffvgpu_status ffvgpu_pool_stall_next_solve(ffvgpu_pool* P) {
+  if (!P) return bad("null pool");
+  P->stall_sweep = 1;
   return FFVGPU_OK;
 }
 

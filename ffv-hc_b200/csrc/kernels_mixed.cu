@@ -475,6 +475,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
   double* GB = V + 8 * PT;  // [face][p] guides of the block, copied with its coefficients
   uint64_t* bar = reinterpret_cast<uint64_t*>(GB + GUIDES);
   __shared__ int abort_flag, s_item[2], s_blk[2], s_inst[2], s_uni[2];  // [copy parity]
+  __shared__ int s_copied[2];  // a copy was issued on the barrier for this parity
   __shared__ uint32_t s_uw[2][7];  // a uniform block's seven coefficient words
   // the copy of one block: its coefficient words unless the block is
   // uniform, and its guide layer in a later pass; with neither, the arrival
@@ -490,6 +491,13 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     const int ib = active_instance(C, b);
     const double* U = C.ucoef + (size_t)b * 8;
     const bool uni = U[7] != 0.0;
+    s_uni[p] = uni;
+    s_blk[p] = b;
+    s_inst[p] = ib;
+    // test hook (MixCtx::stall): nothing arrives on the barrier, so the wait
+    // for this block runs out after the wait limit
+    s_copied[p] = !C.stall;
+    if (C.stall) return b;
     const size_t gb = (size_t)b * BLOCK_CELLS;
     constexpr uint32_t VB = BLOCK_CELLS * 8;  // bytes of one FP64 vector block
     double* sd = reinterpret_cast<double*>(slot);
@@ -513,9 +521,6 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       async::bulk_g2s(slot, coef + (size_t)b * COEF_WORDS, COEF_WORDS * 4, bar);
       if (!FIRST) async::bulk_g2s(GB, guides + (size_t)b * GUIDES, GUIDES * 8, bar);
     }
-    s_uni[p] = uni;
-    s_blk[p] = b;
-    s_inst[p] = ib;
     return b;
   };
   const int tid = threadIdx.x;
@@ -630,7 +635,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       // still had to sweep, and leave.  Only one copy is ever in flight: the
       // next block's is issued after this check.
       if (tid == 0) {
-        const bool drained = async::mbar_drain(bar, phase);
+        const bool drained = !s_copied[phase] || async::mbar_drain(bar, phase);
         const int where = ROLE_SWEEP | (drained ? 0 : async::ROLE_DRAIN);
         for (int it2 = item; it2 < n_act; it2 += gridDim.x) {
           const int i2 = C.inst.blk_inst[C.active[it2]];

@@ -149,6 +149,8 @@ struct ffvgpu_pool {
   double mgraph_omega = 0.0;
   int mgraph_sweeps = 0, mgraph_per = 0;
   uint64_t mgraph_wait_ns = 0;
+  int mgraph_stall = 0;
+  int stall_sweep = 0;  // test hook (ffvgpu_pool_stall_next_solve), cleared when a solve ends
   int64_t m_launches = 0;
   int64_t m_bytes = 0;
   // active-block list of the persistent kernels: device [1 + capacity]

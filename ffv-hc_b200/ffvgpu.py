@@ -42,7 +42,7 @@ EXPORTS = [
     "ffvgpu_assemble_sphere", "ffvgpu_instance_fill", "ffvgpu_serve",
     "ffvgpu_solve_rbgs_fixed_average", "ffvgpu_dump2", "ffvgpu_load2",
     "ffvgpu_restart_filename", "ffvgpu_remove_p", "ffvgpu_corr_u", "ffvgpu_mixed_autotune",
-    "ffvgpu_pool_set_wait_limit", "ffvgpu_mixed_cancel",
+    "ffvgpu_pool_set_wait_limit", "ffvgpu_mixed_cancel", "ffvgpu_pool_stall_next_solve",
 ]
 
 
@@ -163,6 +163,7 @@ def lib():
         L.ffvgpu_pool_neighbors.argtypes = [vp, i32, vp, vp]
         L.ffvgpu_pool_set_stream.argtypes = [vp, vp]
         L.ffvgpu_pool_set_wait_limit.argtypes = [vp, dbl]
+        L.ffvgpu_pool_stall_next_solve.argtypes = [vp]
         L.ffvgpu_fill.argtypes = [vp, i32, dbl]
         L.ffvgpu_grid_neighbors.argtypes = [ctypes.POINTER(GridDesc), vp, vp]
         L.ffvgpu_pool_upload.argtypes = [vp, i32, vp, i32]
@@ -468,6 +469,10 @@ class Pool:
     def set_wait_limit(self, seconds):
         """Time limit of every bounded device wait (ffvgpu_pool_set_wait_limit)."""
         _check(lib().ffvgpu_pool_set_wait_limit(self._h, float(seconds)), "pool_set_wait_limit")
+
+    def stall_next_solve(self):
+        """Test hook: the next mixed solve's sweep waits for a copy never issued."""
+        _check(lib().ffvgpu_pool_stall_next_solve(self._h), "pool_stall_next_solve")
 
     def fill(self, field, value):
         _check(lib().ffvgpu_fill(self._h, FIELD[field], float(value)), "fill")

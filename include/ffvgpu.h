@@ -141,6 +141,11 @@ ffvgpu_status ffvgpu_pool_set_stream(ffvgpu_pool* pool, void* stream);
  * exits, whatever the limit.  The reference has no device waits: its
  * counterpart is the MPI runtime's own timeouts. */
 ffvgpu_status ffvgpu_pool_set_wait_limit(ffvgpu_pool* pool, double seconds);
+/* Test hook for the timeout path (no counterpart in the reference): the next
+ * mixed-form solve on the pool waits in its sweep kernel for a copy that is
+ * never issued, so that wait runs out after the wait limit and the solve ends
+ * with FFVGPU_TIMEOUT.  The hook covers that one solve. */
+ffvgpu_status ffvgpu_pool_stall_next_solve(ffvgpu_pool* pool);
 /* Neighbour table as derived (kind [6], ids [6][4]); for tests. */
 ffvgpu_status ffvgpu_pool_neighbors(const ffvgpu_pool* pool, int32_t block,
                                     int32_t* kind6, int32_t* ids24);

@@ -1,8 +1,10 @@
 """Failure handling on the GPU, without faulting it.
 
 * A bounded device wait that runs out.  The wait limit is a pool setting;
-  set to 0, any wait that does not complete at once gives up (the copies it
-  waits for take microseconds), so the solve must end with FFVGPU_TIMEOUT --
+  set to 0, the sweep kernel's waits on work of its other roles give up (the
+  copies they wait for take microseconds), and a test hook makes the mixed
+  sweep wait for a copy it never issues; the solve must end with
+  FFVGPU_TIMEOUT --
   the kernel's roles leave their loops, copies in flight are waited for, the
   state reports the roles that gave up -- and, with the limit restored, the
   same pool must solve again bit for bit as the oracle does.
@@ -49,10 +51,14 @@ def test_rbgs_wait_limit_runs_out_and_pool_stays_usable():
 
 
 def test_mixed_wait_limit_runs_out_and_pool_stays_usable():
+    """The mixed sweep's one wait is for the block copy it issued itself, which
+    lands within the wait instruction's own suspend time even with a zero
+    limit; the test hook makes the sweep wait for a copy it never issues."""
     g, inp, O = problem(2)
     P = device_problem(g, inp)
     P.fill("X", 0.0)
-    P.set_wait_limit(0.0)
+    P.set_wait_limit(0.05)
+    P.stall_next_solve()
     with pytest.raises(ffvgpu.FFVGPUError) as e:
         P.solve_mixed(1.5, 8, 4, 6, 0.0)
     assert e.value.status == ffvgpu.TIMEOUT
@@ -110,7 +116,7 @@ def test_cancel_a_running_instance_leaves_the_others_unchanged():
         if cancel:
             B.cancel(b)
         done = set(B.poll())
-        while a not in done:
+        while a not in done or (not cancel and b not in done):
             B.advance(4)
             done |= set(B.poll())
         ra, xa = B.result(a, count_max=300), interior(B.download(a, "X", VC)).copy()
