@@ -14,6 +14,9 @@ each step.  Metric: Gcell-sweeps/s = cells x sweeps / time.
   e2e    the same solve through the C ABI with host buffers: upload of
          A (7 fields), b, x from pinned host memory in the reference layout
          (vc = 2), the solve, download of x; copies inside the timed region.
+  forms  (one GPU) the three forms below in compact form, measured after the
+         headline: the level-5 mixed solve, the 64-instance batch and a
+         served run of 100 requests at 50 and 500 req/s (--no-forms skips it).
 
 --impl reference times the reference's CPU path on this machine's host
 cores: the C++ restatement in oracle/ (the reference itself cannot be built
@@ -53,7 +56,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ffvgpu", choices=["ffvgpu", "reference"])
-    ap.add_argument("--form", default="rbsor", choices=["rbsor", "mixed", "batch", "serve"])
+    ap.add_argument("--form", default="rbsor",
+                    choices=["rbsor", "mixed", "batch", "serve", "steps"])
+    ap.add_argument("--time-steps", type=int, default=20, help="steps form: time steps")
+    ap.add_argument("--agree-iterations", type=int, default=3,
+                    help="steps form: BiCGSTAB iterations per step of the oracle comparison")
+    ap.add_argument("--sigma", type=float, default=0.05, help="steps form: noise of u*")
+    ap.add_argument("--agree-steps", type=int, default=0,
+                    help="steps form: steps compared with the oracle (0: all)")
     ap.add_argument("--requests", type=int, default=32, help="serve form: requests per rate")
     ap.add_argument("--rates", default="10,20,50,100,200,500", help="serve form: req/s")
     ap.add_argument("--capacity", type=int, default=40000, help="serve form: pool blocks")
@@ -62,7 +72,9 @@ def parse():
     ap.add_argument("--tune-sample", type=int, default=8,
                     help="batch form: instances the autotuner times each candidate on")
     ap.add_argument("--profile-iterations", type=int, default=0,
-                    help="mixed form: only run this many mixed iterations once (for ncu)")
+                    help="mixed form: only run this many iterations once (for ncu)")
+    ap.add_argument("--profile-solver", default="mixed", choices=["mixed", "bicgstab"],
+                    help="mixed form with --profile-iterations: the solve to run")
     ap.add_argument("--level", type=int, default=5)
     ap.add_argument("--instances", type=int, default=64, help="batch form: instances")
     ap.add_argument("--fp64-sample", type=int, default=64,
@@ -73,6 +85,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="target CPU work of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="headline line without the compact mixed/batch/serve figures")
+    ap.add_argument("--form-requests", type=int, default=100,
+                    help="served requests per rate in the headline line's forms")
+    ap.add_argument("--form-rates", default="50,500",
+                    help="arrival rates (req/s) of the headline line's served run")
     return ap.parse_args()
 
 
@@ -347,7 +365,10 @@ def timed(stream, fn):
 def run_form(args):
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    return {"mixed": run_mixed, "batch": run_batch, "serve": run_serve}[args.form](args)
+    line = {"mixed": run_mixed, "batch": run_batch, "serve": run_serve,
+            "steps": run_steps}[args.form](args)
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def size_table():
@@ -454,8 +475,7 @@ def run_serve(args):
                                "per_rate_fifo": fp64},
         "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_mixed(args):
@@ -466,13 +486,17 @@ def run_mixed(args):
     peak, peak_kind = measured_peaks()
     if args.profile_iterations > 0:  # a fixed, short run for profilers
         P.fill("X", 0.0)
-        r = P.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
-                          args.profile_iterations, 0.0, history=False,
-                          check_every=args.profile_iterations)
-        print(json.dumps({"form": "mixed-profile", "level": args.level, "blocks": int(g.nb),
-                          "iterations": args.profile_iterations, "ms": r["elapsed_ms"]}))
+        if args.profile_solver == "bicgstab":
+            r = P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"],
+                                 args.profile_iterations, 0.0, history=False)
+        else:
+            r = P.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
+                              args.profile_iterations, 0.0, history=False,
+                              check_every=args.profile_iterations)
         P.close()
-        return 0
+        return {"form": f"{args.profile_solver}-profile", "level": args.level,
+                "blocks": int(g.nb), "iterations": args.profile_iterations,
+                "ms": r["elapsed_ms"], "bytes_moved": r["bytes_moved"]}
 
     def fp64_ref():  # the reference's recurrence, no restarts
         P.fill("X", 0.0)
@@ -489,9 +513,15 @@ def run_mixed(args):
         return P.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
                              5000, 1e-8, history=False)
 
+    def rbsor64():  # the same preconditioner on FP64 data: what the 32-bit data buy
+        P.fill("X", 0.0)
+        return P.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
+                             5000, 1e-8, history=False, fp64_data=True)
+
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         res = {}
-        for name, fn in (("fp64_ref", fp64_ref), ("fp64", fp64), ("mixed", mixed)):
+        for name, fn in (("fp64_ref", fp64_ref), ("fp64", fp64), ("rbsor64", rbsor64),
+                         ("mixed", mixed)):
             for _ in range(max(1, args.warmup)):
                 fn()
             ms, runs = [], []
@@ -513,6 +543,7 @@ def run_mixed(args):
     rf, tf, _ = res["fp64"]
     rr_, tr_, _ = res["fp64_ref"]
     rm, tm, _ = res["mixed"]
+    rd, td, _ = res["rbsor64"]
     achieved = rm["bytes_moved"] / (tm * 1e-3) / 1e9
     line = {
         "form": "mixed", "metric": "solves/s to 1e-8 relative residual",
@@ -533,6 +564,12 @@ def run_mixed(args):
         "mixed": {"solves_per_s": 1e3 / tm, "ms": tm, "iterations": rm["count"],
                   "residual": rm["residual"], "kernel_launches": rm["kernel_launches"]},
         "speedup_vs_fp64": tf / tm,
+        "fp64_bicgstab_rbsor": {"solves_per_s": 1e3 / td, "ms": td, "iterations": rd["count"],
+                                "residual": rd["residual"],
+                                "what": "the same BiCGSTAB and RB-SOR preconditioner with FP64 "
+                                        "coefficients, iterate and preconditioned vectors",
+                                "achieved_gbs": rd["bytes_moved"] / (td * 1e-3) / 1e9},
+        "speedup_vs_fp64_bicgstab_rbsor": td / tm,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "what": "algorithmic bytes of the whole mixed solve "
                      "/ its device time", "peak_source": f"{peak_kind} hbm_gbs"},
@@ -543,8 +580,107 @@ def run_mixed(args):
                                                           f"residual {rref['residual']:.2e})"},
         "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
+
+
+def run_steps(args):
+    """The at-scale workload's time-step loop: --time-steps fractional steps on
+    the level-args.level sphere grid, each the pressure part of a step on the
+    device in Solver::UpdateP / UpdateU's order (ffvgpu_update_p /
+    ffvgpu_update_u: remove_p with the previous pressure, u exchange,
+    assembly, BC folding, FP64 BiCGSTAB from the previous pressure to 1e-8,
+    p exchange, corr_u, u and p exchanges), with u* = (1,0,0) + N(0, sigma^2)
+    regenerated on the device from a per-step seed (the reference's
+    convection/diffusion, which would produce u*, is not on this path).
+    Then the same steps with --agree-iterations BiCGSTAB iterations per step
+    on the device and on the oracle (the reference's CPU path restated, same
+    sums), with the per-step pressure agreement."""
+    import torch
+    import ffvgpu
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ffv_oracle as fo
+    stream = torch.cuda.current_stream()
+    level, nsteps, sigma = args.level, args.time_steps, args.sigma
+    g = ffvgpu.SphereGrid(level)
+    peak, peak_kind = measured_peaks()
+
+    def device_pool():
+        P = ffvgpu.Pool(g.desc())
+        P.set_stream(stream.cuda_stream)
+        P.assemble_sphere(ffvgpu.sphere_problem(level, seed=args.seed, sigma=sigma))
+        P.fill("X", 0.0)
+        return P
+
+    def step(P, n, count_max, eps, restart):
+        P.generate_sphere(ffvgpu.sphere_problem(level, seed=args.seed + n, sigma=sigma))
+        r = P.update_p(ffvgpu.SOLVER_BICGSTAB, omega=FP64_SOLVER["omega"],
+                       pre_count=FP64_SOLVER["pre_count"], count_max=count_max, epsilon=eps,
+                       restart_drop=restart)
+        P.update_u()
+        return r
+
+    # ---- timed: every step solved to 1e-8 --------------------------------
+    P = device_pool()
+    for n in range(max(1, args.warmup)):  # warm-up steps on a separate history
+        step(P, 1000 + n, 50000, 1e-8, 1e-3)
+    P.close()
+    P = device_pool()
+    per_step = []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for n in range(nsteps):
+            r, t = timed(stream, lambda: step(P, n, 50000, 1e-8, 1e-3))
+            per_step.append({"step": n, "ms": t, "solve_ms": r["elapsed_ms"],
+                             "iterations": r["count"], "residual": r["residual"],
+                             "solve_gbs": r["bytes_moved"] / (r["elapsed_ms"] * 1e-3) / 1e9})
+    P.close()
+    tot = float(sum(x["ms"] for x in per_step))
+    solve_gbs = [x["solve_gbs"] for x in per_step]
+
+    # ---- agreement with the oracle, a bounded solve per step ---------------
+    K = args.agree_iterations
+    P = device_pool()
+    O = fo.sphere_problem(level, seed=args.seed, sigma=sigma, threads=host_info()["threads_available"],
+                          reduction=fo.RED_CANONICAL)[1]
+    O.field("X")[...] = 0.0
+    go = fo.SphereGrid(level)
+    agree = []
+    t0 = time.perf_counter()
+    for n in range(args.agree_steps if args.agree_steps > 0 else nsteps):
+        rg = step(P, n, K, 0.0, 0.0)
+        ro = fo.time_step(O, go.fill_u(seed=args.seed + n, sigma=sigma, vc=2),
+                          lambda o: o.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"],
+                                                     K, 0.0))
+        pg = P.download("X", 2)[:, 2:18, 2:18, 2:18]
+        po = O.field("X")[:, 2:18, 2:18, 2:18]
+        d = float(np.abs(pg - po).max() / max(np.abs(po).max(), 1e-300))
+        agree.append({"step": n, "p_max_rel_diff": d, "bitwise": bool(np.array_equal(pg, po)),
+                      "residual_gpu": rg["residual"], "residual_oracle": ro["residual"]})
+    oracle_s = time.perf_counter() - t0
+    P.close()
+    O.close()
+    line = {
+        "form": "steps", "metric": "fractional steps/s (pressure part, FP64 BiCGSTAB to 1e-8)",
+        "value": 1e3 * nsteps / tot, "unit": "steps/s", "n_gpus": 1, "steps": nsteps,
+        "warmup": max(1, args.warmup), "ms_per_step": tot / nsteps, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"time-steps-sphere-level{level}", "blocks": int(g.nb),
+                   "cells": int(g.cells), "sigma": sigma, "seeds": [args.seed, args.seed + nsteps - 1],
+                   "dt": 0.002, "rhof": 1.0,
+                   "solver": dict(FP64_SOLVER, solver="BiCGSTAB", epsilon=1e-8, restart_drop=1e-3),
+                   "sequence": "generate u*; remove_p; exchange u; assemble; fold BCs; solve; "
+                               "exchange p; corr_u; exchange u; exchange p"},
+        "per_step": per_step,
+        "solve_hbm": {"achieved_gbs_median": float(np.median(solve_gbs)), "peak": peak,
+                      "frac_median": float(np.median(solve_gbs)) / peak,
+                      "peak_source": f"{peak_kind} hbm_gbs"},
+        "oracle_agreement": {"iterations_per_step": K, "steps": agree,
+                             "all_bitwise": all(a["bitwise"] for a in agree),
+                             "max_p_rel_diff": max(a["p_max_rel_diff"] for a in agree),
+                             "oracle_seconds": oracle_s,
+                             "oracle": "reference CPU path restated (oracle/), canonical sums"},
+        "clocks": clk.summary(),
+    }
+    return line
 
 
 def batch_instances(n):
@@ -578,7 +714,7 @@ def run_batch(args):
     admit_s = time.perf_counter() - t0
     assert all(i is not None for i in ids)
 
-    setting = dict(MIXED, iterations_per_replay=8)
+    setting = dict(MIXED, iterations_per_replay=8, threads_per_block=256, stage_depth=1)
     tune = None
     if args.tune:
         # a sample spread over the instance sizes (every k-th by block count)
@@ -595,18 +731,23 @@ def run_batch(args):
                 "default": next((r for r in recs if r["omega"] == MIXED["omega"] and
                                  r["sweeps"] == MIXED["sweeps"] and
                                  r["sweeps_per_exchange"] == MIXED["sweeps_per_exchange"] and
-                                 r["iterations_per_replay"] == 8), None)}
+                                 r["iterations_per_replay"] == 8 and
+                                 r["threads_per_block"] == 256 and r["stage_depth"] == 1), None)}
         if best >= 0:
             b = recs[best]
             setting = dict(omega=b["omega"], sweeps=b["sweeps"],
                            sweeps_per_exchange=b["sweeps_per_exchange"],
-                           iterations_per_replay=b["iterations_per_replay"])
+                           iterations_per_replay=b["iterations_per_replay"],
+                           threads_per_block=b["threads_per_block"],
+                           stage_depth=b["stage_depth"])
 
     def batched():
         for i in ids:
             B.fill(i, "X", 0.0)
         return B.solve_mixed(setting["omega"], setting["sweeps"], setting["sweeps_per_exchange"],
-                             5000, 1e-8, check_every=setting["iterations_per_replay"])
+                             5000, 1e-8, check_every=setting["iterations_per_replay"],
+                             threads_per_block=setting["threads_per_block"],
+                             stage_depth=setting["stage_depth"])
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         for _ in range(max(1, args.warmup)):
@@ -620,6 +761,22 @@ def run_batch(args):
     iters = [x["count"] for x in results]
     worst = max(x["residual"] for x in results)
     achieved = r["bytes_moved"] / (tb * 1e-3) / 1e9
+    # the same batched solve with the preconditioner on FP64 data: what the
+    # 32-bit data buy, on the same instances, batch and graph
+    for i in ids:
+        B.fill(i, "X", 0.0)
+    r64, t64b = timed(stream, lambda: B.solve_mixed(
+        setting["omega"], setting["sweeps"], setting["sweeps_per_exchange"], 5000, 1e-8,
+        check_every=setting["iterations_per_replay"], fp64_data=True,
+        threads_per_block=setting["threads_per_block"], stage_depth=setting["stage_depth"]))
+    res64 = [B.result(i) for i in ids]
+    rbsor64 = {"solves_per_s": 1e3 * len(ids) / t64b, "ms": t64b,
+               "iterations_min_max": [int(min(x["count"] for x in res64)),
+                                      int(max(x["count"] for x in res64))],
+               "worst_residual": max(x["residual"] for x in res64),
+               "achieved_gbs": r64["bytes_moved"] / (t64b * 1e-3) / 1e9,
+               "what": "the same batched BiCGSTAB and RB-SOR preconditioner with FP64 "
+                       "coefficients, iterate and preconditioned vectors"}
     dev_gb = B.device_bytes / 1e9
     B.close()
     # one-at-a-time plain FP64 GPU solves (and mixed, alone) of a sample
@@ -672,10 +829,88 @@ def run_batch(args):
                                "solver": "BiCGSTAB omega 1, PreCount 2"},
         "mixed_one_at_a_time": {"solves_per_s": alone_sps, "sample": len(sample)},
         "speedup_vs_fp64_one_at_a_time": (1e3 * len(ids) / tb) / fp64_sps,
+        "fp64_rbsor_batched": rbsor64,
+        "speedup_vs_fp64_rbsor_batched": t64b / tb,
         "admission_s": admit_s, "device_gb": dev_gb, "autotune": tune, "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
+
+
+def forms_summary(args):
+    """The three forms in compact form for the headline line (one GPU, rank 0):
+    the level-5 mixed solve against the plain FP64 GPU solve, the 64-instance
+    batch, and a served run of args.form_requests requests at two arrival
+    rates.  Each entry keeps the figures of its own --form line; a form that
+    fails records its error instead of stopping the line."""
+    import copy
+    out = {}
+    t_all = time.perf_counter()
+    plans = (
+        ("mixed_level5", run_mixed, dict(level=5, steps=2, warmup=1, profile_iterations=0)),
+        ("batch64", run_batch, dict(instances=64, steps=1, warmup=1, tune=False, fp64_sample=64)),
+        ("serve", run_serve, dict(requests=args.form_requests, rates=args.form_rates,
+                                  capacity=40000)),
+        ("steps_level5", run_steps, dict(level=5, time_steps=20, warmup=1, agree_steps=3,
+                                         agree_iterations=3, sigma=0.05)),
+    )
+    for name, fn, over in plans:
+        a = copy.copy(args)
+        for k, v in over.items():
+            setattr(a, k, v)
+        t0 = time.perf_counter()
+        try:
+            ln = fn(a)
+        except Exception as e:  # recorded, the headline stands
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+            continue
+        sec = time.perf_counter() - t0
+        if name == "mixed_level5":
+            out[name] = {
+                "solves_per_s": ln["value"], "ms": ln["ms_per_step"],
+                "iterations": ln["mixed"]["iterations"], "residual": ln["mixed"]["residual"],
+                "fp64_bicgstab_jacobi": {k: ln["fp64"][k] for k in ("solves_per_s", "ms",
+                                                                     "iterations")},
+                "speedup_vs_fp64_bicgstab_jacobi": ln["speedup_vs_fp64"],
+                "hbm_frac": ln["roofline"]["frac"], "achieved_gbs": ln["roofline"]["achieved"],
+                "error_vs_fp64_converged": ln["error_vs_fp64_converged"]["mixed"],
+                "clocks": ln["clocks"], "seconds": sec}
+            for k in ("fp64_bicgstab_rbsor", "speedup_vs_fp64_bicgstab_rbsor"):
+                if k in ln:
+                    out[name][k] = ln[k]
+        elif name == "batch64":
+            out[name] = {
+                "solves_per_s": ln["value"], "ms": ln["ms_per_step"],
+                "blocks": ln["config"]["blocks"], "iterations_min_max": ln["iterations_min_max"],
+                "worst_residual": ln["worst_residual"], "hbm_frac": ln["roofline"]["frac"],
+                "achieved_gbs": ln["roofline"]["achieved"],
+                "fp64_one_at_a_time": ln["fp64_one_at_a_time"],
+                "speedup_vs_fp64_one_at_a_time": ln["speedup_vs_fp64_one_at_a_time"],
+                "clocks": ln["clocks"], "seconds": sec}
+            for k in ("fp64_rbsor_batched", "speedup_vs_fp64_rbsor_batched"):
+                if k in ln:
+                    out[name][k] = ln[k]
+        elif name == "steps_level5":
+            out[name] = {
+                "steps_per_s": ln["value"], "ms_per_step": ln["ms_per_step"],
+                "iterations_per_step": [x["iterations"] for x in ln["per_step"]],
+                "solve_hbm_frac_median": ln["solve_hbm"]["frac_median"],
+                "solve_gbs_median": ln["solve_hbm"]["achieved_gbs_median"],
+                "oracle_agreement": {k: ln["oracle_agreement"][k] for k in
+                                     ("iterations_per_step", "all_bitwise", "max_p_rel_diff")},
+                "oracle_steps_compared": len(ln["oracle_agreement"]["steps"]),
+                "clocks": ln["clocks"], "seconds": sec}
+        else:
+            out[name] = {
+                "requests_per_rate": args.form_requests,
+                "blocks_min_max": ln["config"]["blocks_min_max"],
+                "per_rate": [{k: r[k] for k in ("rate", "p50_ms", "p99_ms", "solves_per_s")}
+                             for r in ln["per_rate"]],
+                "fp64_one_at_a_time_fifo": [{k: r[k] for k in ("rate", "p50_ms", "p99_ms")}
+                                            for r in ln["fp64_one_at_a_time"]["per_rate_fifo"]],
+                "fp64_one_at_a_time_solves_per_s": ln["fp64_one_at_a_time"]["solves_per_s"],
+                "clocks": ln["clocks"], "seconds": sec}
+    out["seconds"] = time.perf_counter() - t_all
+    return out
 
 
 def main():
@@ -777,6 +1012,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.level, args.seed, args.sweeps, args.omega, args.cpu_seconds)
 
+    P.close()
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms = forms_summary(args)
+
     if rank == 0:
         line = {
             "metric": "Gcell-sweeps/s", "value": value, "unit": "Gcell-sweeps/s", "n_gpus": world,
@@ -788,8 +1028,9 @@ def main():
                     "d2h_bytes_per_step": d2h, "ms_per_step": te_ms / args.steps},
             "clocks": clk.summary(), "gpu_launches": launches,
         }
+        if forms is not None:
+            line["forms"] = forms
         print(json.dumps(line), flush=True)
-    P.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

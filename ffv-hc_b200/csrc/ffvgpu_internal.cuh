@@ -226,6 +226,80 @@ __device__ __forceinline__ NbrsT<T> split_neighbours(const T* __restrict__ O,
 }
 
 // ---------------------------------------------------------------------------
+// Coarse-fine flux conservation (no counterpart in the reference).  The
+// reference's 2:1 exchange interpolates (src/CGMfuncs/sup.f90:54-179), so the
+// flux a coarse cell sees through a face shared with four fine cells,
+// A_f (g - x_P) with g the restriction of eight fine cells, differs from the
+// sum of what the four fine cells see through their quarter faces.  The
+// correction replaces the coarse side's term by that sum: per coarse cell P
+// on a face f whose neighbours are finer,
+//   F = 0.125 * sum_{dv, du} A_fo(phi) * (x_phi - g_phi)
+// over the four fine cells phi that touch P's face (du along the face's first
+// transverse axis inner, dv outer, summed from 0.0 in that order), fo the
+// opposite face, A_fo(phi) the fine cell's coefficient toward P and g_phi its
+// guide value across fo (the 2:1 prolongation); 0.125 is the fine-to-coarse
+// volume ratio.  The corrected operator adds delta = F - A_f(P) * (g - x_P)
+// to (A x)_P for each such face, in face order 0..5.
+// ---------------------------------------------------------------------------
+// F of the coarse cell at transverse position (a, b) of face 'face' of block
+// blk (kind NB_FINE, record nb).  gx: the stored first guide layer
+// [block][face][p] of x, or null to evaluate the fine guides by the exchange
+// rules from x.
+template <typename T>
+__device__ __noinline__ double cf_fine_flux(const T* __restrict__ x, const double* __restrict__ gx,
+                                            const double* __restrict__ A,
+                                            const FaceNbr* __restrict__ nbr,
+                                            const double* __restrict__ dxs, const BCSet& bc,
+                                            int face, int a, int b, const FaceNbr& nb) {
+  const int axis = face >> 1, fo = face ^ 1;
+  const bool plus = face & 1;
+  const int ta = (axis == 0) ? 1 : 0, tb = (axis == 2) ? 1 : 2;
+  const int fb = nb.id[(a >> 3) + 2 * (b >> 3)];
+  double F = 0.0;
+  for (int dv = 0; dv < 2; ++dv)
+    for (int du = 0; du < 2; ++du) {
+      const int fu = 2 * (a & 7) + du, fv = 2 * (b & 7) + dv;
+      int c[3];
+      c[ta] = fu;
+      c[tb] = fv;
+      c[axis] = plus ? 0 : 15;
+      const int s = sidx(c[0], c[1], c[2]);
+      const double xf = (double)x[(size_t)fb * BLOCK_CELLS + s];
+      const double gf =
+          gx ? gx[((size_t)fb * 6 + fo) * FACE_CELLS + fu + 16 * fv]
+             : guide_value(x, fb, fo, fu, fv, 1, nbr[(size_t)fb * 6 + fo], bc, dxs[fb]);
+      const double af = A[((size_t)fb * 7 + 1 + fo) * BLOCK_CELLS + s];
+      F = F + af * (xf - gf);
+    }
+  return 0.125 * F;
+}
+
+// y plus (SUB: minus) the correction delta of each face of cell s (storage
+// slot) whose neighbours are finer, in face order; y unchanged when it has
+// none.  x_P and its guide layer G ([face][p]) as the stencil used them, its
+// face coefficients af(f).
+template <bool SUB, typename T, typename AF>
+__device__ __forceinline__ double cf_delta(const T* __restrict__ x, const double* __restrict__ gx,
+                                           const double* __restrict__ A,
+                                           const FaceNbr* __restrict__ nbr,
+                                           const double* __restrict__ dxs, const BCSet& bc,
+                                           const FaceNbr* snb, const double* G, double xp,
+                                           int s, double y, AF af) {
+  int cc[3];
+  cell_of(s, cc[0], cc[1], cc[2]);
+#pragma unroll 1
+  for (int f = 0; f < 6; ++f) {
+    const int axis = f >> 1;
+    if (cc[axis] != ((f & 1) ? 15 : 0) || snb[f].kind != NB_FINE) continue;
+    const int a = cc[(axis == 0) ? 1 : 0], b = cc[(axis == 2) ? 1 : 2];
+    const double F = cf_fine_flux(x, gx, A, nbr, dxs, bc, f, a, b, snb[f]);
+    const double d = F - af(f) * (G[f * FACE_CELLS + a + 16 * b] - xp);
+    y = SUB ? y - d : y + d;
+  }
+  return y;
+}
+
+// ---------------------------------------------------------------------------
 // Convergence bookkeeping run by the last CTA of a reduction.
 // ---------------------------------------------------------------------------
 // FFVILS.h:24-47 IsConverged residual

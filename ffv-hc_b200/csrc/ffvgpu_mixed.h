@@ -28,33 +28,44 @@ struct MixCtx {
   int first;
   uint64_t wait_ns;    // limit of every bounded device wait (ffvgpu_pool_set_wait_limit)
   int stall;           // test hook: the sweep issues no copy, so its first wait runs out
+  int cf;              // coarse-fine flux correction in the FP64 residual and A*x
+  int depth;           // sweep kernel: L2 prefetch distance in blocks (staging depth, >= 1)
 };
 
-// CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel.
-void mx_grid_sizes(int* sweep, int* matvec, int* update, int* guides);
-// 32-bit sweep coefficients of blocks [first, first + count): [blk][7][8][512]
-// words (FP64 high words, rounded), MIXED_COEF_WORDS per block.
+// CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel,
+// with 'threads' (128, 256 or 512) per CTA of the A*x and update kernels.
+void mx_grid_sizes(int threads, int* sweep, int* matvec, int* update, int* guides);
+// Sweep coefficients of blocks [first, first + count), MIXED_COEF_WORDS per
+// block: 32-bit words [blk][7][8][512] (FP64 high words, rounded) into coef,
+// or with d64 (the FP64-data variant) the FP64 values [blk][7][8][512] into
+// coef64.  Also writes each block's ucoef record and adds the instance's
+// uniform blocks to st->ublocks.
 constexpr int MIXED_COEF_WORDS = 7 * 8 * 512;
-// Also writes each block's ucoef record and adds the instance's uniform
-// blocks to st->ublocks.
 void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint32_t* coef,
-                    double* ucoef, SolveState* st);
+                    double* coef64, double* ucoef, SolveState* st, bool d64);
 void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
                     const double* gx, const double* A, const double* b, double* r, double* r0);
-// The iteration launchers take 'count' = CTAs of the persistent grid.
+// The iteration launchers take 'count' = CTAs of the persistent grid.  The
+// iterate between passes and the preconditioned vectors (void* below) are
+// float, or double with d64.
 // One pass of sweeps; a later pass (first false) takes ein and its guide
 // layer, written by launch_mx_guides.
 void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first,
                      float omega, int nsweep, const double* r, double* r0, double* pv,
-                     const double* q, const uint32_t* coef, const float* ein,
-                     const double* guides, float* eout);
-// Guide layer [blk][6][256] (FP64) of the FP32 iterate e for the next pass.
-void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const float* e,
-                      double* guides);
-void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, const float* x,
-                      const double* A, double* y, const double* w0);
-void launch_mx_update(cudaStream_t s, const MixCtx& C, int count, double* x, const float* ph,
-                      const float* sh, double* r, const double* t, const double* sv,
-                      const double* r0);
+                     const double* q, const uint32_t* coef, const double* coef64,
+                     const void* ein, const double* guides, void* eout, bool d64);
+// Guide layer [blk][6][256] (FP64) of the iterate e for the next pass.
+void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const void* e, double* guides,
+                      bool d64);
+void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads,
+                      const void* x, const double* A, double* y, const double* w0, bool d64);
+// Coarse-fine flux mismatch per face cell of the (block, face) pairs
+// [npairs][2] of kind NB_FINE: out [npairs][256][2] = (delta, F).
+void launch_cf_mismatch(cudaStream_t s, int npairs, const double* x, const double* gx,
+                        const double* A, const FaceNbr* nbr, const double* dx, const BCSet& bc,
+                        const int32_t* pairs, double* out);
+void launch_mx_update(cudaStream_t s, const MixCtx& C, int count, int threads, double* x,
+                      const void* ph, const void* sh, double* r, const double* t,
+                      const double* sv, const double* r0, bool d64);
 
 }  // namespace ffvgpu

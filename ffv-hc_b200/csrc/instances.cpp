@@ -38,7 +38,7 @@ void release_instances(ffvgpu_pool* P) {
   P->mgraph = nullptr;
   void* ptrs[] = {P->blk_inst_d, P->inst_first_d, P->inst_count_d, P->blk_geo_d, P->mst,
                   P->mpartials, P->mhist, P->mcoef, P->mguide, P->mucoef, P->me[0], P->me[1], P->mph,
-                  P->msh};
+                  P->msh, P->mcoef64, P->me64[0], P->me64[1], P->mph64, P->msh64};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (P->act_d) cudaFree(P->act_d);
@@ -113,7 +113,7 @@ ffvgpu_status publish_active(ffvgpu_pool* P) {
   return FFVGPU_OK;
 }
 
-ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P) {
+ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P, bool d64) {
   ffvgpu_status s;
   const size_t n = field_count(P);
   if (!P->act_d) {
@@ -124,7 +124,9 @@ ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P) {
       CK(cudaEventCreateWithFlags(&P->act_ev[k], cudaEventDisableTiming));
       CK(cudaEventRecord(P->act_ev[k], P->stream));
     }
-    mx_grid_sizes(&P->grid_sweep, &P->grid_matvec, &P->grid_update, &P->grid_guides);
+    mx_grid_sizes(P->m_threads, &P->grid_sweep, &P->grid_matvec, &P->grid_update,
+                  &P->grid_guides);
+    P->grid_threads = P->m_threads;
   }
   if ((s = dalloc_t(P, &P->mcoef, 7 * n)) || (s = dalloc_t(P, &P->mguide, n / BC * 6 * 256)) ||
       (s = dalloc_t(P, &P->mucoef, n / BC * 8)) ||
@@ -133,6 +135,10 @@ ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P) {
       (s = dalloc_t(P, &P->msh, n)) ||
       (s = dalloc_t(P, &P->r, n)) || (s = dalloc_t(P, &P->r0, n)) || (s = dalloc_t(P, &P->p, n)) ||
       (s = dalloc_t(P, &P->q, n)) || (s = dalloc_t(P, &P->sv, n)) || (s = dalloc_t(P, &P->tv, n)))
+    return s;
+  if (d64 && ((s = dalloc_t(P, &P->mcoef64, 7 * n)) || (s = dalloc_t(P, &P->me64[0], n)) ||
+              (s = dalloc_t(P, &P->me64[1], n)) || (s = dalloc_t(P, &P->mph64, n)) ||
+              (s = dalloc_t(P, &P->msh64, n))))
     return s;
   return FFVGPU_OK;
 }
@@ -169,6 +175,8 @@ MixCtx mix_ctx(const ffvgpu_pool* P) {
   C.active = P->act_d + 1;
   C.wait_ns = P->wait_ns;
   C.stall = P->stall_sweep;
+  C.cf = P->m_cf;
+  C.depth = P->m_depth;
   return C;
 }
 
@@ -177,6 +185,13 @@ KCtx range_ctx(const ffvgpu_pool* P, const BCSet& bc, const ffvgpu_instance& I) 
   C.first = I.first;
   C.nb = I.count;
   return C;
+}
+
+int stage_depth_of(const ffvgpu_mixed_params* prm) {
+  return prm->stage_depth > 0 ? prm->stage_depth : 1;
+}
+int threads_of(const ffvgpu_mixed_params* prm) {
+  return prm->threads_per_block > 0 ? prm->threads_per_block : 256;
 }
 
 ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
@@ -192,21 +207,30 @@ ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
     return bad("restart_growth must be 0 or greater than 1");
   if (prm->restart_every < 0) return bad("restart_every must not be negative");
   if (prm->count_max < 0) return bad("count_max must not be negative");
+  if (prm->stage_depth < 0 || prm->stage_depth > 3) return bad("stage_depth must lie in 0..3");
+  if (prm->threads_per_block != 0 && prm->threads_per_block != 128 &&
+      prm->threads_per_block != 256 && prm->threads_per_block != 512)
+    return bad("threads_per_block must be 0, 128, 256 or 512");
   return FFVGPU_OK;
 }
 
 // Algorithmic HBM bytes of one iteration per cell: two preconditioner
-// applications, two A*x with dot products, the update.
+// applications, two A*x with dot products, the update.  cw: coefficient bytes
+// of a cell in a sweep pass (28 as 32-bit words, 56 in FP64), ew: bytes of one
+// iterate or preconditioned-vector value (4 in FP32, 8 in FP64).
 // Of those, the per-cell coefficient bytes that a uniform block does not move
 // (its seven values come from one per-block record).
-int64_t uniform_saving_per_cell(int passes) { return 2 * passes * 28 + 2 * 56; }
+int64_t uniform_saving_per_cell(int passes, bool d64) {
+  return 2 * passes * (d64 ? 56 : 28) + 2 * 56;
+}
 
-int64_t iteration_bytes_per_cell(int passes) {
-  const int64_t first_p = 28 + 8 + 16 + 8 + 4;  // coefficients, r, p and q, p, e
-  const int64_t first_s = 28 + 16 + 8 + 4;       // coefficients, q and r, s, e
-  const int64_t later = 28 + 8 + 4 + 4;          // coefficients, p or s, e in, e out
-  const int64_t matvec = 56 + 4 + 8 + 8;
-  const int64_t update = 4 + 4 + 8 + 8 + 8 + 8 + 8 + 8;
+int64_t iteration_bytes_per_cell(int passes, bool d64) {
+  const int64_t cw = d64 ? 56 : 28, ew = d64 ? 8 : 4;
+  const int64_t first_p = cw + 8 + 16 + 8 + ew;  // coefficients, r, p and q, p, e
+  const int64_t first_s = cw + 16 + 8 + ew;      // coefficients, q and r, s, e
+  const int64_t later = cw + 8 + ew + ew;        // coefficients, p or s, e in, e out
+  const int64_t matvec = 56 + ew + 8 + 8;
+  const int64_t update = ew + ew + 8 + 8 + 8 + 8 + 8 + 8;
   return first_p + first_s + 2 * (passes - 1) * later + 2 * matvec + update;
 }
 
@@ -215,23 +239,30 @@ void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
   const MixCtx C = mix_ctx(P);
   const int passes = P->m_sweeps / P->m_per_exchange;
   const float om = (float)P->m_omega;
+  const bool d64 = P->m_d64 != 0;
   double* x = P->x[P->xcur];
+  void* e[2] = {d64 ? (void*)P->me64[0] : (void*)P->me[0],
+                d64 ? (void*)P->me64[1] : (void*)P->me[1]};
+  void* ph = d64 ? (void*)P->mph64 : (void*)P->mph;
+  void* sh = d64 ? (void*)P->msh64 : (void*)P->msh;
   for (int mode = 0; mode < 2; ++mode) {
     double* rhs = mode == 0 ? P->p : P->sv;
-    float* hat = mode == 0 ? P->mph : P->msh;
+    void* hat = mode == 0 ? ph : sh;
     for (int ps = 0; ps < passes; ++ps) {
       const bool last = ps == passes - 1;
-      const float* ein = ps > 0 ? P->me[(ps - 1) & 1] : nullptr;
-      if (ps > 0) launch_mx_guides(s, C, P->grid_guides, ein, P->mguide);
+      const void* ein = ps > 0 ? e[(ps - 1) & 1] : nullptr;
+      if (ps > 0) launch_mx_guides(s, C, P->grid_guides, ein, P->mguide, d64);
       launch_mx_sweep(s, C, P->grid_sweep, mode, ps == 0, om, P->m_per_exchange, P->r, P->r0,
-                      rhs, P->q, P->mcoef, ein, P->mguide, last ? hat : P->me[ps & 1]);
+                      rhs, P->q, P->mcoef, P->mcoef64, ein, P->mguide, last ? hat : e[ps & 1],
+                      d64);
     }
     if (mode == 0)
-      launch_mx_matvec(s, C, P->grid_matvec, 1, P->mph, P->A, P->q, P->r0);
+      launch_mx_matvec(s, C, P->grid_matvec, 1, P->m_threads, ph, P->A, P->q, P->r0, d64);
     else
-      launch_mx_matvec(s, C, P->grid_matvec, 2, P->msh, P->A, P->tv, P->sv);
+      launch_mx_matvec(s, C, P->grid_matvec, 2, P->m_threads, sh, P->A, P->tv, P->sv, d64);
   }
-  launch_mx_update(s, C, P->grid_update, x, P->mph, P->msh, P->r, P->tv, P->sv, P->r0);
+  launch_mx_update(s, C, P->grid_update, P->m_threads, x, ph, sh, P->r, P->tv, P->sv, P->r0,
+                   d64);
 }
 
 int launches_per_iteration(const ffvgpu_pool* P) {
@@ -340,8 +371,9 @@ ffvgpu_status admit_range(ffvgpu_pool* P, const ffvgpu_grid_desc* d, int32_t* in
 // UpdateP's P02-P05 for the blocks of instance I from device-generated
 // sphere-flow inputs: u*, cuts and flags (kernels_gen.cu), the velocity
 // exchange, bcut_calc_ab_p, the BC folding, and x = 0.
+// assemble false: only u*, the cut fields and the flags (and the u BCs).
 ffvgpu_status generate_and_assemble(ffvgpu_pool* P, const ffvgpu_instance& I,
-                                    const ffvgpu_sphere_problem* prob) {
+                                    const ffvgpu_sphere_problem* prob, bool assemble = true) {
   ffvgpu_status s;
   if ((s = ensure_inst_device(P))) return s;
   // fields the generator and the assembly write (pool-wide, allocated once)
@@ -373,7 +405,12 @@ ffvgpu_status generate_and_assemble(ffvgpu_pool* P, const ffvgpu_instance& I,
       bu.value[f] = prob->u_bc_value[c][f];
     }
     P->bc_u[c] = bu;
-    launch_exchange(P->stream, range_ctx(P, bu, I), P->u[c], P->gu[c]);
+    if (assemble) launch_exchange(P->stream, range_ctx(P, bu, I), P->u[c], P->gu[c]);
+  }
+  if (!assemble) {
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(P->stream));
+    return FFVGPU_OK;
   }
   launch_assemble(P->stream, range_ctx(P, P->bc_p, I), P->u[0], P->u[1], P->u[2], P->gu[0],
                   P->gu[1], P->gu[2], P->cut, P->flags, P->A, P->b, nullptr, prob->rhof,
@@ -481,7 +518,19 @@ ffvgpu_status ffvgpu_instance_admit_sphere(ffvgpu_pool* P, const ffvgpu_sphere_p
   return FFVGPU_OK;
 }
 
+static ffvgpu_status sphere_on_pool(ffvgpu_pool* P, const ffvgpu_sphere_problem* prob,
+                                    bool assemble);
+
 ffvgpu_status ffvgpu_assemble_sphere(ffvgpu_pool* P, const ffvgpu_sphere_problem* prob) {
+  return sphere_on_pool(P, prob, true);
+}
+
+ffvgpu_status ffvgpu_generate_sphere(ffvgpu_pool* P, const ffvgpu_sphere_problem* prob) {
+  return sphere_on_pool(P, prob, false);
+}
+
+static ffvgpu_status sphere_on_pool(ffvgpu_pool* P, const ffvgpu_sphere_problem* prob,
+                                    bool assemble) {
   if (!P || !prob) return bad("null argument");
   if (P->batch) return bad("a batch pool admits sphere problems with ffvgpu_instance_admit_sphere");
   if (!(prob->rhof > 0.0) || !(prob->dt > 0.0)) return bad("rhof and dt must be positive");
@@ -499,7 +548,7 @@ ffvgpu_status ffvgpu_assemble_sphere(ffvgpu_pool* P, const ffvgpu_sphere_problem
   for (int a = 0; a < 3; ++a)
     if (P->inst[0].desc.domain_origin[a] != prob->grid.domain_origin[a])
       return bad("the pool's domain origin differs from the problem's");
-  return generate_and_assemble(P, P->inst[0], prob);
+  return generate_and_assemble(P, P->inst[0], prob, assemble);
 }
 
 ffvgpu_status ffvgpu_instance_upload(ffvgpu_pool* P, int32_t inst, ffvgpu_field f,
@@ -635,17 +684,29 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
   bool others = false;
   for (const ffvgpu_instance& J : P->inst) others = others || J.running;
   if (others && (prm->omega != P->m_omega || prm->sweeps != P->m_sweeps ||
-                 prm->sweeps_per_exchange != P->m_per_exchange))
+                 prm->sweeps_per_exchange != P->m_per_exchange ||
+                 (prm->flux_correction != 0) != (P->m_cf != 0) ||
+                 (prm->fp64_data != 0) != (P->m_d64 != 0) ||
+                 stage_depth_of(prm) != P->m_depth || threads_of(prm) != P->m_threads))
     return bad("running instances use other preconditioner settings");
   double *xp, *g;
   size_t stride;
   if ((s = field_ptr(P, FFVGPU_FIELD_X, true, &xp, &stride, &g))) return s;
-  if ((s = ensure_inst_device(P)) || (s = ensure_mixed_buffers(P)) ||
+  if ((s = ensure_inst_device(P)) || (s = ensure_mixed_buffers(P, prm->fp64_data != 0)) ||
       (s = ensure_mhist(P, prm->count_max > 0 ? prm->count_max : 1)))
     return s;
   P->m_omega = prm->omega;
   P->m_sweeps = prm->sweeps;
   P->m_per_exchange = prm->sweeps_per_exchange;
+  P->m_cf = prm->flux_correction != 0;
+  P->m_d64 = prm->fp64_data != 0;
+  P->m_depth = stage_depth_of(prm);
+  P->m_threads = threads_of(prm);
+  if (P->grid_threads != P->m_threads) {  // the persistent grids of this CTA size
+    mx_grid_sizes(P->m_threads, &P->grid_sweep, &P->grid_matvec, &P->grid_update,
+                  &P->grid_guides);
+    P->grid_threads = P->m_threads;
+  }
   I->count_max = prm->count_max;
   I->epsilon = prm->epsilon;
   I->result = ffvgpu_result();
@@ -668,13 +729,14 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
   // (counted into the state), then b.b / r / r0 / r.r0
   I->ublocks = 0;
   CK(cudaMemcpyAsync(P->mst + inst, &h, sizeof(h), cudaMemcpyHostToDevice, P->stream));
-  launch_mx_pack(P->stream, I->first, I->count, P->A, P->mcoef, P->mucoef, P->mst + inst);
+  launch_mx_pack(P->stream, I->first, I->count, P->A, P->mcoef, P->mcoef64, P->mucoef,
+                 P->mst + inst, P->m_d64 != 0);
   MixCtx C = mix_ctx(P);
   C.first = I->first;
   launch_mx_init(P->stream, C, I->count, P->x[P->xcur], P->gx, P->A, P->b, P->r, P->r0);
   CK(cudaGetLastError());
   P->m_launches += 2;
-  P->m_bytes += (int64_t)I->count * BC * (7 * 8 + 7 * 4 + 8 * 9 + 16);
+  P->m_bytes += (int64_t)I->count * BC * (7 * 8 + 7 * (P->m_d64 ? 8 : 4) + 8 * 9 + 16);
   I->running = true;
   return publish_active(P);
 }
@@ -695,7 +757,9 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
   // kernel arguments (the wait limit among them) are fixed at capture
   if (!P->mgraph || P->mgraph_iters != iterations || P->mgraph_omega != P->m_omega ||
       P->mgraph_sweeps != P->m_sweeps || P->mgraph_per != P->m_per_exchange ||
-      P->mgraph_wait_ns != P->wait_ns || P->mgraph_stall != P->stall_sweep) {
+      P->mgraph_wait_ns != P->wait_ns || P->mgraph_stall != P->stall_sweep ||
+      P->mgraph_cf != P->m_cf || P->mgraph_d64 != P->m_d64 ||
+      P->mgraph_depth != P->m_depth || P->mgraph_threads != P->m_threads) {
     if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
     P->mgraph = nullptr;
     cudaGraph_t graph;
@@ -711,12 +775,17 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
     P->mgraph_per = P->m_per_exchange;
     P->mgraph_wait_ns = P->wait_ns;
     P->mgraph_stall = P->stall_sweep;
+    P->mgraph_cf = P->m_cf;
+    P->mgraph_d64 = P->m_d64;
+    P->mgraph_depth = P->m_depth;
+    P->mgraph_threads = P->m_threads;
   }
   CK(cudaGraphLaunch(P->mgraph, P->stream));
   P->m_launches += (int64_t)iterations * launches_per_iteration(P);
   const int passes = P->m_sweeps / P->m_per_exchange;
-  P->m_bytes += (int64_t)iterations * (cells * iteration_bytes_per_cell(passes) -
-                                       ucells * uniform_saving_per_cell(passes));
+  P->m_bytes += (int64_t)iterations *
+                (cells * iteration_bytes_per_cell(passes, P->m_d64 != 0) -
+                 ucells * uniform_saving_per_cell(passes, P->m_d64 != 0));
   return FFVGPU_OK;
 }
 
@@ -888,6 +957,8 @@ ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* P, const int32_t* instances, in
     prm.omega = R.omega;
     prm.sweeps = R.sweeps;
     prm.sweeps_per_exchange = R.sweeps_per_exchange;
+    prm.threads_per_block = R.threads_per_block;
+    prm.stage_depth = R.stage_depth;
     prm.history = nullptr;
     R.ms = 0.0;
     R.max_count = 0;
@@ -933,3 +1004,62 @@ ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* P, const int32_t* instances, in
 }
 
 }  // extern "C"
+
+// Coarse-fine flux mismatch of FIELD_X (interior and stored guide layer):
+// per coarse cell on a face whose neighbours are finer, the fine-side flux F
+// and delta = F - A_f (g - x_P); sums of V_P |delta| and V_P |F| in (block,
+// face, position) order.
+ffvgpu_status ffvgpu_cf_flux_mismatch(ffvgpu_pool* P, double* mismatch, double* flux,
+                                      int32_t* n_cells, double* per_cell, int32_t capacity) {
+  if (!P || !mismatch || !flux || !n_cells) return bad("null argument");
+  if (!P->A) return bad("A must be uploaded or assembled first");
+  cudaSetDevice(P->device);
+  double *xp, *g;
+  size_t stride;
+  ffvgpu_status s;
+  if ((s = field_ptr(P, FFVGPU_FIELD_X, false, &xp, &stride, &g))) return s;
+  if (!xp || !g) return bad("pressure field not allocated");
+  std::vector<int32_t> pairs;
+  for (int b = 0; b < P->nb; ++b) {
+    if (b < (int)P->blk_inst_h.size() && P->blk_inst_h[b] < 0) continue;
+    for (int f = 0; f < 6; ++f)
+      if (P->nbr_h[(size_t)b * 6 + f].kind == NB_FINE) {
+        pairs.push_back(b);
+        pairs.push_back(f);
+      }
+  }
+  const int np = (int)pairs.size() / 2;
+  const int64_t nc = (int64_t)np * FACE_CELLS;
+  *n_cells = (int32_t)nc;
+  *mismatch = 0.0;
+  *flux = 0.0;
+  if (per_cell && capacity < nc) return bad("per_cell capacity below the number of cells");
+  if (np == 0) return FFVGPU_OK;
+  int32_t* pd = nullptr;
+  double* od = nullptr;
+  cudaError_t e = cudaMalloc(&pd, sizeof(int32_t) * pairs.size());
+  if (e == cudaSuccess) e = cudaMalloc(&od, sizeof(double) * 2 * nc);
+  std::vector<double> out(2 * nc);
+  if (e == cudaSuccess) e = upload(P, pd, pairs.data(), sizeof(int32_t) * pairs.size());
+  if (e == cudaSuccess) {
+    launch_cf_mismatch(P->stream, np, xp, g, P->A, P->nbr_d, P->dx_d, P->bc_p, pd, od);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = download_sync(P, out.data(), od, sizeof(double) * 2 * nc);
+  cudaFree(pd);
+  cudaFree(od);
+  if (e != cudaSuccess) return cuda_fail(e, "cf_flux_mismatch");
+  double m = 0.0, fl = 0.0;
+  for (int i = 0; i < np; ++i) {
+    const double dx = P->dx_h[pairs[2 * i]], vol = dx * dx * dx;
+    for (int p = 0; p < FACE_CELLS; ++p) {
+      const size_t c = (size_t)i * FACE_CELLS + p;
+      m += vol * std::fabs(out[2 * c]);
+      fl += vol * std::fabs(out[2 * c + 1]);
+    }
+  }
+  if (per_cell) std::memcpy(per_cell, out.data(), sizeof(double) * 2 * nc);
+  *mismatch = m;
+  *flux = fl;
+  return FFVGPU_OK;
+}

@@ -169,27 +169,29 @@ __device__ void mx_finalize(SolveState* S, const double* t, int fin) {
   }
 }
 
-// Canonical block sums of NV values (acc[v][colour][virtual thread r or
-// r + 256]), per-instance ticket, and the last CTA's cross-block sums over
-// the instance's blocks in block order.
-template <int NV>
-__device__ void mx_reduce(double (&acc)[NV][2][2], const MixCtx& C, int blk, int inst, int fin) {
+// Canonical block sums of NV values and the last CTA's cross-block sums over
+// the instance's blocks in block order, for CTAs of NT threads (128, 256 or
+// 512).  Thread tid carries the sums of virtual threads tid + NT k of the
+// block's 512-thread tree (acc[v][colour][k], k < 512 / NT), so the tree --
+// and every result -- is the same for every NT; likewise the 256 lanes of
+// the cross-block stage are threads tid + NT k below 256.
+template <int NV, int NT>
+__device__ void mx_reduce(double (&acc)[NV][2][512 / NT], const MixCtx& C, int blk, int inst,
+                          int fin) {
+  constexpr int VPT = 512 / NT, NW = NT / 32;
+  constexpr int LPT = NT >= 256 ? 1 : 256 / NT;  // cross-block lanes per thread
   __shared__ double ws[NV][16];
   __shared__ int amlast;
   const int tid = threadIdx.x;
 #pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    double v0 = acc[v][0][0] + acc[v][1][0], v1 = acc[v][0][1] + acc[v][1][1];
+  for (int v = 0; v < NV; ++v)
 #pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) {
-      v0 += __shfl_xor_sync(0xffffffffu, v0, off);
-      v1 += __shfl_xor_sync(0xffffffffu, v1, off);
+    for (int k = 0; k < VPT; ++k) {
+      double x = acc[v][0][k] + acc[v][1][k];
+#pragma unroll
+      for (int off = 16; off >= 1; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+      if ((tid & 31) == 0) ws[v][(tid >> 5) + NW * k] = x;
     }
-    if ((tid & 31) == 0) {
-      ws[v][tid >> 5] = v0;
-      ws[v][8 + (tid >> 5)] = v1;
-    }
-  }
   __syncthreads();
   SolveState* S = C.inst.st + inst;
   const int first = C.inst.first[inst], cnt = C.inst.count[inst];
@@ -211,12 +213,23 @@ __device__ void mx_reduce(double (&acc)[NV][2][2], const MixCtx& C, int blk, int
   double tot[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    double s = 0.0;
-    for (int b = tid; b < cnt; b += MT) s += __ldcg(C.partials + (size_t)v * C.capacity + first + b);
+    double lv[LPT];
 #pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    for (int k = 0; k < LPT; ++k) {
+      const int lane = tid + NT * k;
+      double s = 0.0;
+      if (lane < 256)
+        for (int b = lane; b < cnt; b += 256)
+          s += __ldcg(C.partials + (size_t)v * C.capacity + first + b);
+#pragma unroll
+      for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+      lv[k] = s;
+    }
     __syncthreads();
-    if ((tid & 31) == 0) ws[0][tid >> 5] = s;
+    if ((tid & 31) == 0)
+#pragma unroll
+      for (int k = 0; k < LPT; ++k)
+        if (tid + NT * k < 256) ws[0][(tid + NT * k) >> 5] = lv[k];
     __syncthreads();
     double total = 0.0;
 #pragma unroll
@@ -230,22 +243,28 @@ __device__ void mx_reduce(double (&acc)[NV][2][2], const MixCtx& C, int blk, int
   }
 }
 
-// Stages block blk of an FP32 vector as FP64: the colour-split interior in
+// Stages block blk of an FP32 (or FP64) vector as FP64: the colour-split interior in
 // O[4096] and the first guide layer in G[6][256], guides by the exchange
 // rules in FP64 (outer faces by the field's BCs).
 // nb: the block's six face records, already in shared memory (so each
 // guide needs one round of global loads, not a dependent second).
+template <int NT, typename ET>
 __device__ __forceinline__ void stage_f32_as_f64(double* __restrict__ O, double* __restrict__ G,
-                                                 const float* __restrict__ x, int blk,
+                                                 const ET* __restrict__ x, int blk,
                                                  const FaceNbr* nb, double dx,
                                                  const MixCtx& C) {
   const int tid = threadIdx.x;
-  const float* xb = x + (size_t)blk * BLOCK_CELLS;
+  const ET* xb = x + (size_t)blk * BLOCK_CELLS;
 #pragma unroll 4
-  for (int m = 0; m < 16; ++m) O[tid + MT * m] = (double)__ldg(xb + tid + MT * m);
+  for (int m = 0; m < BLOCK_CELLS / NT; ++m) O[tid + NT * m] = (double)__ldg(xb + tid + NT * m);
+  // the guide pairs (face, p, p + 128), 768 of them, NT at a time: all the
+  // pairs' loads in flight together
+  constexpr int NP = (6 * 128 + NT - 1) / NT;
 #pragma unroll
-  for (int it = 0; it < 3; ++it) {  // the three pairs' loads in flight together
-    const int f = 2 * it + (tid >> 7), p0 = tid & 127, p1 = p0 + 128;
+  for (int it = 0; it < NP; ++it) {
+    const int w = tid + NT * it;
+    if (NP * NT > 6 * 128 && w >= 6 * 128) break;
+    const int f = w >> 7, p0 = w & 127, p1 = p0 + 128;
     const FaceNbr nf = nb[f];
     double v0, v1;
     guide_pair(x, blk, f, p0, p1, nf, C.bc, dx, v0, v1);
@@ -278,18 +297,29 @@ __device__ __forceinline__ double widen_here(uint32_t w) {
   return __hiloint2double((int)v, 0);
 }
 
+// D64 (the FP64-data variant): coef64 [blk][a][m][t] holds the FP64 values
+// themselves (dinv = 1 / Ap in FP64), read at use by the sweep kernel.
+template <bool D64>
 __global__ void __launch_bounds__(MT)
 mx_pack_kernel(int first, const double* __restrict__ A, uint32_t* __restrict__ coef,
-               double* __restrict__ ucoef, SolveState* st) {
+               double* __restrict__ coef64, double* __restrict__ ucoef, SolveState* st) {
   const int blk = first + blockIdx.x;
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
-  uint32_t* cb = coef + (size_t)blk * COEF_WORDS;
+  uint32_t* cb = D64 ? nullptr : coef + (size_t)blk * COEF_WORDS;
+  double* cd = D64 ? coef64 + (size_t)blk * COEF_WORDS : nullptr;
   for (int w = threadIdx.x; w < 8 * PT; w += MT) {
     const int m = w / PT, t = w % PT;
     const int s = sweep_cell(t, m);
+    if (D64) {
 #pragma unroll
-    for (int a = 0; a < 6; ++a) cb[coef_word(a, m, t)] = hi_round(Ab[(1 + a) * BLOCK_CELLS + s]);
-    cb[coef_word(6, m, t)] = hi_round(1.0 / Ab[s]);
+      for (int a = 0; a < 6; ++a) cd[(a * 8 + m) * PT + t] = Ab[(1 + a) * BLOCK_CELLS + s];
+      cd[(6 * 8 + m) * PT + t] = 1.0 / Ab[s];
+    } else {
+#pragma unroll
+      for (int a = 0; a < 6; ++a)
+        cb[coef_word(a, m, t)] = hi_round(Ab[(1 + a) * BLOCK_CELLS + s]);
+      cb[coef_word(6, m, t)] = hi_round(1.0 / Ab[s]);
+    }
   }
   // uniform block: all seven coefficients bitwise equal to cell 0's everywhere
   bool same = true;
@@ -318,8 +348,10 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
   if (inst < 0) return;
   __shared__ double O[BLOCK_CELLS];
   __shared__ double G[6 * FACE_CELLS];
+  __shared__ FaceNbr snb[6];
   const int tid = threadIdx.x;
   const size_t base = (size_t)blk * BLOCK_CELLS;
+  if (tid < 6) snb[tid] = C.nbr[blk * 6 + tid];
 #pragma unroll 4
   for (int m = 0; m < 16; ++m) O[tid + MT * m] = __ldg(x + base + tid + MT * m);
 #pragma unroll
@@ -334,10 +366,13 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
     for (int m = 0; m < 8; ++m) {
       const int q = tid + MT * m, s = c * HALF_CELLS + q;
       const Nbrs v = split_neighbours(O + (1 - c) * HALF_CELLS, G, q, c);
-      const double rv = __ldg(bvec + base + s) - __ldg(Ab + 4096 + s) * v.w -
+      double rv = __ldg(bvec + base + s) - __ldg(Ab + 4096 + s) * v.w -
                         __ldg(Ab + 8192 + s) * v.e - __ldg(Ab + 12288 + s) * v.s -
                         __ldg(Ab + 16384 + s) * v.n - __ldg(Ab + 20480 + s) * v.b -
                         __ldg(Ab + 24576 + s) * v.t - __ldg(Ab + s) * O[s];
+      if (C.cf)  // coarse-fine flux correction: r = b - (A x + delta)
+        rv = cf_delta<true>(x, gx, A, C.nbr, C.dx, C.bc, snb, G, O[s], s, rv,
+                            [&](int f) { return __ldg(Ab + (1 + f) * BLOCK_CELLS + s); });
       r[base + s] = rv;
       r0[base + s] = rv;
       const double bv = __ldg(bvec + base + s);
@@ -345,7 +380,7 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
       acc[1][c][m & 1] += rv * rv;
     }
   }
-  mx_reduce<2>(acc, C, blk, inst, FIN_MX_INIT);
+  mx_reduce<2, MT>(acc, C, blk, inst, FIN_MX_INIT);
 }
 
 // ---------------------------------------------------------------------------
@@ -372,14 +407,25 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
 // T and V are written by other threads between the barriers: no __restrict__
 // on them, which would let the compiler move tile loads across
 // __syncthreads().
-// UNI: a uniform block -- the seven coefficients ku (widened once) serve
-// every cell and cw is not read; otherwise each cell's words cw[m] are
-// widened at use.  The values, and so the results, are the same either way.
-template <bool UNI>
+// Where a cell's coefficients come from.  CS_UNI: a uniform block -- the
+// seven coefficients ku (widened once) serve every cell.  CS_W32: each cell's
+// 32-bit words cw[m] are widened at use.  CS_G64 (the FP64-data variant):
+// each cell's FP64 coefficients are read at use from c64, the block's
+// coefficients in thread order ([a][m][thread], c64 already offset to this
+// thread).  For one data format the values, and so the results, do not
+// depend on the source.
+enum { CS_UNI = 0, CS_W32 = 1, CS_G64 = 2 };
+template <int CS>
 __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, int p0,
                                            double (&E)[2][4], const uint32_t (&cw)[8][7],
-                                           const double (&ku)[7], double mom, int nsweep) {
-#define MX_COEF(m, a) (UNI ? ku[a] : widen_here(cw[m][a]))
+                                           const double (&ku)[7],
+                                           const double* __restrict__ c64, double mom,
+                                           int nsweep) {
+  constexpr bool UNI = CS == CS_UNI;
+#define MX_COEF(m, a)                                          \
+  (CS == CS_UNI ? ku[a]                                        \
+   : CS == CS_W32 ? widen_here(cw[m][a])                       \
+                  : __ldg(c64 + ((a) * 8 + (m)) * PT))
   // a uniform block has the registers to keep its right-hand side too (one
   // shared-memory read less per update)
   double vr[2][4];
@@ -449,69 +495,118 @@ __device__ __forceinline__ int guide_slot(int face, int p) {
 
 constexpr int ROLE_SWEEP = 8;  // SolveState::timeout_where bit of this kernel's waits
 
-// Called by a whole warp: the first item from, from + gridDim.x, ... (below
-// n_act) whose block belongs to an instance still solving, or n_act; 32
-// candidates per round.
-__device__ __forceinline__ int next_live(const MixCtx& C, int from, int n_act, int lane) {
-  for (int b = from; b < n_act; b += 32 * gridDim.x) {
-    const int it = b + lane * gridDim.x;
-    const bool live = it < n_act && active_instance(C, C.active[it]) >= 0;
+// A CTA's live items, found once per chunk instead of a block ahead: entry
+// (block, instance | flags) of the items blockIdx.x + k gridDim.x whose
+// instance is still solving (the done flags change between launches only).
+constexpr int LIST_CAP = 1024;           // entries per chunk (8 KB of shared memory)
+constexpr int LF_UNI = 1 << 30;          // the block is uniform (MixCtx::ucoef)
+constexpr int LF_COPY = 1 << 29;         // its instance starts a cycle (p = r, r0 = r)
+constexpr int LF_INST = LF_COPY - 1;
+
+// Called by every thread: fills list[0, *n) from the candidates from, from +
+// gridDim.x, ... (LIST_CAP of them, in item order) and sets *next to the
+// first candidate after them.
+template <int MODE, bool FIRST>
+__device__ void build_live_list(const MixCtx& C, int from, int n_act, int2* list, int* n,
+                                int* next, int* wcount) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int base = 0;
+  for (int r = 0; r < LIST_CAP / PT; ++r) {
+    const int it = from + (r * PT + tid) * gridDim.x;
+    int b = -1, e = 0;
+    bool live = false;
+    if (it < n_act) {
+      b = C.active[it];
+      const int i = C.inst.blk_inst[b];
+      live = i >= 0 && !*((volatile const int32_t*)&C.inst.st[i].done);
+      if (live) {
+        e = i;
+        if (C.ucoef[(size_t)b * 8 + 7] != 0.0) e |= LF_UNI;
+        if (FIRST && MODE == 0 && C.inst.st[i].cycle == 1) e |= LF_COPY;
+      }
+    }
     const unsigned m = __ballot_sync(0xffffffffu, live);
-    if (m) return b + (__ffs(m) - 1) * gridDim.x;
+    if (lane == 0) wcount[warp] = __popc(m);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < warp; ++w) off += wcount[w];
+    if (live) list[off + __popc(m & ((1u << lane) - 1u))] = make_int2(b, e);
+    int tot = 0;
+    for (int w = 0; w < PT / 32; ++w) tot += wcount[w];
+    base += tot;
+    __syncthreads();  // wcount is refilled by the next round
   }
-  return n_act;
+  if (tid == 0) {
+    *n = base;
+    *next = from + LIST_CAP * gridDim.x;
+  }
+  __syncthreads();
 }
 
-template <int MODE, bool FIRST>
+// ET: the iterate between passes, float (the mixed form) or double (the
+// FP64-data variant, whose coefficients are FP64 too and read at use).
+template <int MODE, bool FIRST, typename ET>
 __global__ void __launch_bounds__(PT, 1)
 mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
                 double* __restrict__ r0, double* __restrict__ pv, const double* __restrict__ q,
-                const uint32_t* __restrict__ coef, const float* __restrict__ ein,
-                const double* __restrict__ guides, float* __restrict__ eout) {
+                const uint32_t* __restrict__ coef, const double* __restrict__ coef64,
+                const ET* __restrict__ ein, const double* __restrict__ guides,
+                ET* __restrict__ eout, int depth) {
+  constexpr bool D64 = sizeof(ET) == 8;
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t* slot = reinterpret_cast<uint32_t*>(smem);
   double* T = reinterpret_cast<double*>(smem + COEF_WORDS * 4);
   double* V = reinterpret_cast<double*>(smem + COEF_WORDS * 4 + TILE * 8);  // [m][t] rhs
   double* GB = V + 8 * PT;  // [face][p] guides of the block, copied with its coefficients
   uint64_t* bar = reinterpret_cast<uint64_t*>(GB + GUIDES);
-  __shared__ int abort_flag, s_item[2], s_blk[2], s_inst[2], s_uni[2];  // [copy parity]
+  __shared__ int2 s_list[LIST_CAP];
+  __shared__ int s_nlist, s_next_from, s_wcount[PT / 32];
+  __shared__ int abort_flag;
   __shared__ int s_copied[2];  // a copy was issued on the barrier for this parity
-  __shared__ uint32_t s_uw[2][7];  // a uniform block's seven coefficient words
+  // a uniform block's coefficient record (MixCtx::ucoef), copied with the block
+  __shared__ __align__(16) double s_urec[2][8];
   // the copy of one block: its coefficient words unless the block is
-  // uniform, and its guide layer in a later pass; with neither, the arrival
-  // alone completes the phase.  Run by thread 0 for item 'it', copy parity p.
-  // A uniform block needs no coefficient words, so in a first pass its copy
-  // brings the block's vectors into the slot instead and its staging reads
-  // shared memory: r (slot doubles [0, 4096)), q ([4096, 8192)) and p
-  // ([8192, 12288)) as far as it reads them.  (A later pass reads p and the
-  // FP32 iterate from global memory, prefetched into L2 a block ahead: that
-  // measured faster than copying them.)
-  auto issue = [&](int it, uint32_t p) {
-    const int b = C.active[it];
-    const int ib = active_instance(C, b);
-    const double* U = C.ucoef + (size_t)b * 8;
-    const bool uni = U[7] != 0.0;
-    s_uni[p] = uni;
-    s_blk[p] = b;
-    s_inst[p] = ib;
+  // uniform (then its coefficient record), and its guide layer in a later
+  // pass; with none of them, the arrival alone completes the phase.  Run by
+  // thread 0 for list entry e, copy parity p.  A uniform block needs no
+  // coefficient words, so in a first pass its copy brings the block's
+  // vectors into the slot instead and its staging reads shared memory: r
+  // (slot doubles [0, 4096)), q ([4096, 8192)) and p ([8192, 12288)) as far
+  // as it reads them.  (A later pass reads p and the FP32 iterate from global
+  // memory, prefetched into L2 a block ahead: that measured faster than
+  // copying them.)  Nothing here waits on a global load.
+  auto issue = [&](int2 e, uint32_t p) {
+    const int b = e.x;
+    const bool uni = e.y & LF_UNI;
     // test hook (MixCtx::stall): nothing arrives on the barrier, so the wait
     // for this block runs out after the wait limit
     s_copied[p] = !C.stall;
-    if (C.stall) return b;
+    if (C.stall) return;
     const size_t gb = (size_t)b * BLOCK_CELLS;
     constexpr uint32_t VB = BLOCK_CELLS * 8;  // bytes of one FP64 vector block
+    constexpr uint32_t UB = 8 * 8;            // bytes of a coefficient record
     double* sd = reinterpret_cast<double*>(slot);
     if (uni) {
-#pragma unroll
-      for (int a = 0; a < 6; ++a) s_uw[p][a] = hi_round(U[1 + a]);
-      s_uw[p][6] = hi_round(1.0 / U[0]);
       if (FIRST) {
-        const bool copy = MODE == 0 && ib >= 0 && C.inst.st[ib].cycle == 1;
+        const bool copy = e.y & LF_COPY;
         const bool needq = !copy, needp = MODE == 0 && !copy;
-        async::mbar_expect_tx(bar, VB + (needq ? VB : 0u) + (needp ? VB : 0u));
+        async::mbar_expect_tx(bar, UB + VB + (needq ? VB : 0u) + (needp ? VB : 0u));
+        async::bulk_g2s(s_urec[p], C.ucoef + (size_t)b * 8, UB, bar);
         async::bulk_g2s(sd, r + gb, VB, bar);
         if (needq) async::bulk_g2s(sd + BLOCK_CELLS, q + gb, VB, bar);
         if (needp) async::bulk_g2s(sd + 2 * BLOCK_CELLS, pv + gb, VB, bar);
+      } else {
+        async::mbar_expect_tx(bar, UB + GUIDES * 8u);
+        async::bulk_g2s(s_urec[p], C.ucoef + (size_t)b * 8, UB, bar);
+        async::bulk_g2s(GB, guides + (size_t)b * GUIDES, GUIDES * 8, bar);
+      }
+      return;
+    }
+    if (D64) {
+      // FP64 coefficients are read at use (prefetched into L2); the copy
+      // brings the guide layer only
+      if (FIRST) {
+        async::mbar_arrive(bar);
       } else {
         async::mbar_expect_tx(bar, GUIDES * 8u);
         async::bulk_g2s(GB, guides + (size_t)b * GUIDES, GUIDES * 8, bar);
@@ -521,7 +616,30 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       async::bulk_g2s(slot, coef + (size_t)b * COEF_WORDS, COEF_WORDS * 4, bar);
       if (!FIRST) async::bulk_g2s(GB, guides + (size_t)b * GUIDES, GUIDES * 8, bar);
     }
-    return b;
+  };
+  // Brings into L2 what the copy and the staging of list entry e will read:
+  // run for the entry 'depth' blocks ahead of the one being swept (depth 1:
+  // the next block, whose copy is issued now).
+  auto prefetch = [&](int2 e) {
+    const int b = e.x;
+    const bool uni = e.y & LF_UNI, copy = e.y & LF_COPY;
+    const size_t gb = (size_t)b * BLOCK_CELLS;
+    constexpr uint32_t VB = BLOCK_CELLS * 8;
+    if (!uni) {
+      if (D64)
+        async::prefetch_l2(coef64 + (size_t)b * COEF_WORDS, COEF_WORDS * 8u);
+      else if (depth > 1)
+        async::prefetch_l2(coef + (size_t)b * COEF_WORDS, COEF_WORDS * 4u);
+    }
+    if (FIRST) {
+      async::prefetch_l2(r + gb, VB);
+      if (!copy) async::prefetch_l2(q + gb, VB);
+      if (MODE == 0 && !copy) async::prefetch_l2(pv + gb, VB);
+    } else {
+      if (depth > 1) async::prefetch_l2(guides + (size_t)b * GUIDES, GUIDES * 8u);
+      async::prefetch_l2(pv + gb, VB);
+      async::prefetch_l2(ein + gb, BLOCK_CELLS * (uint32_t)sizeof(ET));
+    }
   };
   const int tid = threadIdx.x;
   const int ih = tid & 7, kg = (tid >> 3) & 3, j = tid >> 5;
@@ -536,38 +654,36 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
   }
   if (FIRST)
     for (int g = tid; g < TILE; g += PT) T[g] = 0.0;  // guides of e stay 0 in a first pass
-  __syncthreads();
   // The CTA visits the live items blockIdx.x + n gridDim.x of the active
-  // list (blocks of instances still solving); warp 0 finds the next one a
-  // block ahead and issues its coefficient copy, so blocks of instances that
-  // have stopped cost neither a copy nor a wait.
-  if (tid < 32) {
-    const int it0 = next_live(C, blockIdx.x, n_act, tid);
-    if (tid == 0) {
-      s_item[0] = it0;
-      if (it0 < n_act) issue(it0, 0);
-    }
+  // list (blocks of instances still solving), found a chunk at a time, and
+  // issues each block's copy while the block before it sweeps, so blocks of
+  // instances that have stopped cost neither a copy nor a wait.
+  build_live_list<MODE, FIRST>(C, blockIdx.x, n_act, s_list, &s_nlist, &s_next_from, s_wcount);
+  while (s_nlist == 0 && s_next_from < n_act)  // a chunk with no live item
+    build_live_list<MODE, FIRST>(C, s_next_from, n_act, s_list, &s_nlist, &s_next_from,
+                                 s_wcount);
+  if (tid == 0 && s_nlist > 0) {
+    issue(s_list[0], 0);
+    for (int k = 0; k < depth && k < s_nlist; ++k) prefetch(s_list[k]);
   }
-  uint32_t phase = 0;  // parity of the copy the current item waits on
+  int pos = 0;         // list position of the current block
+  uint32_t phase = 0;  // parity of the copy the current block waits on
   for (;; phase ^= 1u) {
-    // item, block and instance were found a block ahead (when its copy was
-    // issued): one reading of the done flag for the whole CTA, off the
-    // block's critical path (the flag changes between launches only)
     __syncthreads();
-    const int item = s_item[phase];
-    if (item >= n_act) break;
-    const int blk = s_blk[phase], inst = s_inst[phase];
+    if (pos >= s_nlist) break;
+    const int2 ent = s_list[pos];
+    const int blk = ent.x, inst = ent.y & LF_INST;
+    const bool uni = ent.y & LF_UNI;
     const size_t base = (size_t)blk * BLOCK_CELLS + s0;
     double E[2][4] = {};
     // this block's copy (issued a block ago): coefficients and guides, or
-    // for a uniform block its vectors and guides
+    // for a uniform block its record, vectors or guides
     async::mbar_wait(bar, phase, &abort_flag, ROLE_SWEEP, C.wait_ns);
-    const bool uni = s_uni[phase];
     const double* sd = reinterpret_cast<const double*>(slot);
     const size_t gbase = (size_t)blk * BLOCK_CELLS;
-    if (inst >= 0 && FIRST) {
+    if (FIRST) {
       const SolveState* S = C.inst.st + inst;
-      const bool copy = S->cycle == 1;  // first iteration of a (re)start: p = r, r0 = r
+      const bool copy = ent.y & LF_COPY;  // first iteration of a (re)start: p = r, r0 = r
       const double mgamma = -S->gamma, beta = S->beta, malpha = -S->alpha;
       const double* rs = uni ? sd : r + gbase;
       const double* qs = uni ? sd + BLOCK_CELLS : q + gbase;
@@ -595,7 +711,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
           E[c][h] = 0.0;
           T[o0 + c * SH + h * SQ] = 0.0;
         }
-    } else if (inst >= 0) {
+    } else {
 #pragma unroll
       for (int c = 0; c < 2; ++c)
 #pragma unroll
@@ -605,16 +721,23 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
           E[c][h] = (double)__ldg(ein + s);
           T[o0 + c * SH + h * SQ] = E[c][h];
         }
-    }
-    if (!FIRST && inst >= 0)
 #pragma unroll
       for (int g = tid; g < GUIDES; g += PT) T[guide_slot(g >> 8, g & 255)] = GB[g];
+    }
     uint32_t cw[8][7];
     double ku[7];
     if (uni) {
+      const double* U = s_urec[phase];
+      if (D64) {
 #pragma unroll
-      for (int a = 0; a < 7; ++a) ku[a] = widen(s_uw[phase][a]);
-    } else {
+        for (int a = 0; a < 6; ++a) ku[a] = U[1 + a];
+        ku[6] = 1.0 / U[0];
+      } else {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) ku[a] = widen(hi_round(U[1 + a]));
+        ku[6] = widen(hi_round(1.0 / U[0]));
+      }
+    } else if (!D64) {
 #pragma unroll
       for (int a = 0; a < 7; ++a)
 #pragma unroll
@@ -637,44 +760,46 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       if (tid == 0) {
         const bool drained = !s_copied[phase] || async::mbar_drain(bar, phase);
         const int where = ROLE_SWEEP | (drained ? 0 : async::ROLE_DRAIN);
-        for (int it2 = item; it2 < n_act; it2 += gridDim.x) {
-          const int i2 = C.inst.blk_inst[C.active[it2]];
-          if (i2 < 0) continue;
+        auto stop = [&](int i2) {
           atomicOr(&C.inst.st[i2].timeout_where, where);
           atomicExch(&C.inst.st[i2].status, 3);
           atomicExch(&C.inst.st[i2].done, 1);
+        };
+        for (int k = pos; k < s_nlist; ++k) stop(s_list[k].y & LF_INST);
+        for (int it2 = s_next_from; it2 < n_act; it2 += gridDim.x) {
+          const int i2 = C.inst.blk_inst[C.active[it2]];
+          if (i2 >= 0) stop(i2);
         }
       }
       return;
     }
-    const int nxt = tid < 32 ? next_live(C, item + gridDim.x, n_act, tid) : n_act;
-    if (tid == 0) s_item[phase ^ 1u] = nxt;
-    if (tid == 0 && nxt < n_act) {
-      const int nbk = issue(nxt, phase ^ 1u);
-      const size_t nbase = (size_t)nbk * BLOCK_CELLS;
-      if (FIRST && s_uni[phase ^ 1u]) {
-        // its vectors come with the copy
-      } else if (FIRST) {
-        const int ni = C.inst.blk_inst[nbk];
-        const bool copy = MODE == 0 && ni >= 0 && C.inst.st[ni].cycle == 1;
-        async::prefetch_l2(r + nbase, BLOCK_CELLS * 8);
-        if (!copy) async::prefetch_l2(q + nbase, BLOCK_CELLS * 8);
-        if (MODE == 0 && !copy) async::prefetch_l2(pv + nbase, BLOCK_CELLS * 8);
-      } else {
-        async::prefetch_l2(pv + nbase, BLOCK_CELLS * 8);
-        async::prefetch_l2(ein + nbase, BLOCK_CELLS * 4);
-      }
+    // the next block: from this chunk, or from the next one (built by every
+    // thread; this block's entry is already in registers)
+    int npos = pos + 1;
+    if (npos >= s_nlist && s_next_from < n_act) {
+      do
+        build_live_list<MODE, FIRST>(C, s_next_from, n_act, s_list, &s_nlist, &s_next_from,
+                                     s_wcount);
+      while (s_nlist == 0 && s_next_from < n_act);
+      npos = 0;
     }
-    if (inst < 0) continue;
+    if (tid == 0 && npos < s_nlist) {
+      issue(s_list[npos], phase ^ 1u);
+      if (npos + depth - 1 < s_nlist) prefetch(s_list[npos + depth - 1]);
+    }
+    pos = npos;
+    const double* c64 = D64 ? coef64 + (size_t)blk * COEF_WORDS + tid : nullptr;
     if (uni)
-      run_sweeps<true>(T, V + tid, o0, j & 1, E, cw, ku, mom, nsweep);
+      run_sweeps<CS_UNI>(T, V + tid, o0, j & 1, E, cw, ku, c64, mom, nsweep);
+    else if constexpr (D64)
+      run_sweeps<CS_G64>(T, V + tid, o0, j & 1, E, cw, ku, c64, mom, nsweep);
     else
-      run_sweeps<false>(T, V + tid, o0, j & 1, E, cw, ku, mom, nsweep);
+      run_sweeps<CS_W32>(T, V + tid, o0, j & 1, E, cw, ku, c64, mom, nsweep);
 #pragma unroll
     for (int c = 0; c < 2; ++c)
 #pragma unroll
       for (int h = 0; h < 4; ++h)
-        eout[base + c * HALF_CELLS + h * 128] = __double2float_rn(E[c][h]);
+        eout[base + c * HALF_CELLS + h * 128] = (ET)E[c][h];
   }
 }
 
@@ -687,8 +812,9 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
 // ---------------------------------------------------------------------------
 constexpr int GT = MT;  // guides kernel: three pairs (face, p, p + 128) per thread
 
+template <typename ET>
 __global__ void __launch_bounds__(GT)
-mx_guides_kernel(MixCtx C, const float* __restrict__ e, double* __restrict__ guides) {
+mx_guides_kernel(MixCtx C, const ET* __restrict__ e, double* __restrict__ guides) {
   BCSet hom;
   for (int f = 0; f < 6; ++f) {
     hom.type[f] = BC_DIRICHLET;
@@ -727,9 +853,9 @@ mx_guides_kernel(MixCtx C, const float* __restrict__ e, double* __restrict__ gui
 // products.  NV = 1: y.w0 (q_.r0, FFVILS.h:890-896).  NV = 2: y.w0 and y.y
 // (t_.s and t_.t_, FFVILS.h:923-936).
 // ---------------------------------------------------------------------------
-template <int NV>
-__global__ void __launch_bounds__(MT, 4)
-mx_matvec_kernel(MixCtx C, const float* __restrict__ x, const double* __restrict__ A,
+template <int NV, bool CF, typename ET, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT)
+mx_matvec_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ A,
                  double* __restrict__ y, const double* __restrict__ w0) {
   __shared__ double O[BLOCK_CELLS];
   __shared__ double G[6 * FACE_CELLS];
@@ -742,7 +868,7 @@ mx_matvec_kernel(MixCtx C, const float* __restrict__ x, const double* __restrict
     if (inst < 0) continue;
     if (tid < 6) snb[tid] = C.nbr[blk * 6 + tid];
     __syncthreads();
-    stage_f32_as_f64(O, G, x, blk, snb, C.dx[blk], C);
+    stage_f32_as_f64<NT>(O, G, x, blk, snb, C.dx[blk], C);
     __syncthreads();
     const size_t base = (size_t)blk * BLOCK_CELLS;
     const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
@@ -751,26 +877,32 @@ mx_matvec_kernel(MixCtx C, const float* __restrict__ x, const double* __restrict
     double u[7];
 #pragma unroll
     for (int a = 0; a < 7; ++a) u[a] = uni ? U[a] : 0.0;
-    double acc[NV][2][2] = {};
+    constexpr int VPT = 512 / NT;
+    double acc[NV][2][VPT] = {};
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
 #pragma unroll 2
-      for (int m = 0; m < 8; ++m) {
-        const int qd = tid + MT * m, s = c * HALF_CELLS + qd;
+      for (int m = 0; m < HALF_CELLS / NT; ++m) {
+        const int qd = tid + NT * m, s = c * HALF_CELLS + qd;
         const Nbrs v = split_neighbours(O + (1 - c) * HALF_CELLS, G, qd, c);
-        const double yv =
+        double yv =
             uni ? u[1] * v.w + u[2] * v.e + u[3] * v.s + u[4] * v.n + u[5] * v.b + u[6] * v.t +
                       u[0] * O[s]
                 : __ldg(Ab + 4096 + s) * v.w + __ldg(Ab + 8192 + s) * v.e +
                       __ldg(Ab + 12288 + s) * v.s + __ldg(Ab + 16384 + s) * v.n +
                       __ldg(Ab + 20480 + s) * v.b + __ldg(Ab + 24576 + s) * v.t +
                       __ldg(Ab + s) * O[s];
+        if (CF)  // coarse-fine flux correction: y = A x + delta
+          yv = cf_delta<false>(x, (const double*)nullptr, A, C.nbr, C.dx, C.bc, snb, G, O[s], s,
+                               yv, [&](int f) {
+                                 return uni ? u[1 + f] : __ldg(Ab + (1 + f) * BLOCK_CELLS + s);
+                               });
         y[base + s] = yv;
-        acc[0][c][m & 1] += yv * __ldg(w0 + base + s);
-        if (NV == 2) acc[NV - 1][c][m & 1] += yv * yv;
+        acc[0][c][m % VPT] += yv * __ldg(w0 + base + s);
+        if (NV == 2) acc[NV - 1][c][m % VPT] += yv * yv;
       }
     }
-    mx_reduce<NV>(acc, C, blk, inst, NV == 1 ? FIN_MX_ALPHA : FIN_MX_GAMMA);
+    mx_reduce<NV, NT>(acc, C, blk, inst, NV == 1 ? FIN_MX_ALPHA : FIN_MX_GAMMA);
     __syncthreads();  // O and G are refilled for the next block
   }
 }
@@ -780,9 +912,10 @@ mx_matvec_kernel(MixCtx C, const float* __restrict__ x, const double* __restrict
 // r = (-gamma)*t_ + s (axpyz, blas.f90:397-429, FFVILS.h:945-950); r.r and
 // the next iteration's r.r0.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(MT)
-mx_update_kernel(MixCtx C, double* __restrict__ x, const float* __restrict__ ph,
-                 const float* __restrict__ sh, double* __restrict__ r,
+template <typename ET, int NT>
+__global__ void __launch_bounds__(NT)
+mx_update_kernel(MixCtx C, double* __restrict__ x, const ET* __restrict__ ph,
+                 const ET* __restrict__ sh, double* __restrict__ r,
                  const double* __restrict__ t, const double* __restrict__ s,
                  const double* __restrict__ r0) {
   const int tid = threadIdx.x;
@@ -794,99 +927,209 @@ mx_update_kernel(MixCtx C, double* __restrict__ x, const float* __restrict__ ph,
     const SolveState* S = C.inst.st + inst;
     const double alpha = S->alpha, gamma = S->gamma, mgamma = -S->gamma;
     const size_t base = (size_t)blk * BLOCK_CELLS;
-    double acc[2][2][2] = {};
+    constexpr int VPT = 512 / NT;
+    double acc[2][2][VPT] = {};
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
 #pragma unroll 4
-      for (int m = 0; m < 8; ++m) {
-        const size_t i = base + c * HALF_CELLS + tid + MT * m;
+      for (int m = 0; m < HALF_CELLS / NT; ++m) {
+        const size_t i = base + c * HALF_CELLS + tid + NT * m;
         x[i] = alpha * (double)ph[i] + gamma * (double)sh[i] + x[i];
         const double rn = mgamma * t[i] + s[i];
         r[i] = rn;
-        acc[0][c][m & 1] += rn * rn;
-        acc[1][c][m & 1] += rn * __ldg(r0 + i);
+        acc[0][c][m % VPT] += rn * rn;
+        acc[1][c][m % VPT] += rn * __ldg(r0 + i);
       }
     }
-    mx_reduce<2>(acc, C, blk, inst, FIN_MX_UPDATE);
+    mx_reduce<2, NT>(acc, C, blk, inst, FIN_MX_UPDATE);
     __syncthreads();  // the reduction's shared words are reused for the next block
   }
+}
+
+// ---------------------------------------------------------------------------
+// Coarse-fine flux mismatch of an FP64 field with its stored guide layer:
+// per (block, face) pair of kind NB_FINE and face position p = a + 16 b, the
+// fine-side flux F of the coarse cell there and delta = F - A_f (g - x_P),
+// out[(pair * 256 + p) * 2 + {0, 1}] = delta, F.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(FACE_CELLS)
+cf_mismatch_kernel(const double* __restrict__ x, const double* __restrict__ gx,
+                   const double* __restrict__ A, const FaceNbr* __restrict__ nbr,
+                   const double* __restrict__ dx, BCSet bc, const int32_t* __restrict__ pairs,
+                   double* __restrict__ out) {
+  const int blk = pairs[2 * blockIdx.x], f = pairs[2 * blockIdx.x + 1];
+  const int p = threadIdx.x, a = p & 15, b = p >> 4;
+  const int axis = f >> 1, ta = (axis == 0) ? 1 : 0, tb = (axis == 2) ? 1 : 2;
+  int c[3];
+  c[ta] = a;
+  c[tb] = b;
+  c[axis] = (f & 1) ? 15 : 0;
+  const int s = sidx(c[0], c[1], c[2]);
+  const FaceNbr nb = nbr[(size_t)blk * 6 + f];
+  const double F = cf_fine_flux(x, gx, A, nbr, dx, bc, f, a, b, nb);
+  const double xp = x[(size_t)blk * BLOCK_CELLS + s];
+  const double g = gx[((size_t)blk * 6 + f) * FACE_CELLS + p];
+  const double af = A[((size_t)blk * 7 + 1 + f) * BLOCK_CELLS + s];
+  const double d = F - af * (g - xp);
+  out[((size_t)blockIdx.x * FACE_CELLS + p) * 2] = d;
+  out[((size_t)blockIdx.x * FACE_CELLS + p) * 2 + 1] = F;
+}
+
+void launch_cf_mismatch(cudaStream_t s, int npairs, const double* x, const double* gx,
+                        const double* A, const FaceNbr* nbr, const double* dx, const BCSet& bc,
+                        const int32_t* pairs, double* out) {
+  if (npairs > 0) cf_mismatch_kernel<<<npairs, FACE_CELLS, 0, s>>>(x, gx, A, nbr, dx, bc, pairs, out);
 }
 
 // ---------------------------------------------------------------------------
 // Launchers.
 // ---------------------------------------------------------------------------
 void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint32_t* coef,
-                    double* ucoef, SolveState* st) {
-  mx_pack_kernel<<<count, MT, 0, s>>>(first, A, coef, ucoef, st);
+                    double* coef64, double* ucoef, SolveState* st, bool d64) {
+  if (d64)
+    mx_pack_kernel<true><<<count, MT, 0, s>>>(first, A, coef, coef64, ucoef, st);
+  else
+    mx_pack_kernel<false><<<count, MT, 0, s>>>(first, A, coef, coef64, ucoef, st);
 }
 void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
                     const double* gx, const double* A, const double* b, double* r, double* r0) {
   mx_init_kernel<<<count, MT, 0, s>>>(C, x, gx, A, b, r, r0);
 }
 
-template <int MODE, bool FIRST>
+template <int MODE, bool FIRST, typename ET>
 static void sweep_launch(cudaStream_t s, const MixCtx& C, int count, float omega, int nsweep,
                          const double* r, double* r0, double* pv, const double* q,
-                         const uint32_t* coef, const float* ein, const double* guides,
-                         float* eout) {
-  mx_sweep_kernel<MODE, FIRST>
-      <<<count, PT, SWEEP_SMEM, s>>>(C, omega, nsweep, r, r0, pv, q, coef, ein, guides, eout);
+                         const uint32_t* coef, const double* coef64, const void* ein,
+                         const double* guides, void* eout) {
+  mx_sweep_kernel<MODE, FIRST, ET><<<count, PT, SWEEP_SMEM, s>>>(
+      C, omega, nsweep, r, r0, pv, q, coef, coef64, static_cast<const ET*>(ein), guides,
+      static_cast<ET*>(eout), C.depth);
 }
 
 void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first,
                      float omega, int nsweep, const double* r, double* r0, double* pv,
-                     const double* q, const uint32_t* coef, const float* ein,
-                     const double* guides, float* eout) {
-#define MX_SWEEP(M, F) sweep_launch<M, F>(s, C, count, omega, nsweep, r, r0, pv, q, coef, ein, guides, eout)
-  if (mode == 0 && first) MX_SWEEP(0, true);
-  if (mode == 0 && !first) MX_SWEEP(0, false);
-  if (mode == 1 && first) MX_SWEEP(1, true);
-  if (mode == 1 && !first) MX_SWEEP(1, false);
+                     const double* q, const uint32_t* coef, const double* coef64,
+                     const void* ein, const double* guides, void* eout, bool d64) {
+#define MX_SWEEP(M, F, T) \
+  sweep_launch<M, F, T>(s, C, count, omega, nsweep, r, r0, pv, q, coef, coef64, ein, guides, eout)
+  if (!d64) {
+    if (mode == 0 && first) MX_SWEEP(0, true, float);
+    if (mode == 0 && !first) MX_SWEEP(0, false, float);
+    if (mode == 1 && first) MX_SWEEP(1, true, float);
+    if (mode == 1 && !first) MX_SWEEP(1, false, float);
+  } else {
+    if (mode == 0 && first) MX_SWEEP(0, true, double);
+    if (mode == 0 && !first) MX_SWEEP(0, false, double);
+    if (mode == 1 && first) MX_SWEEP(1, true, double);
+    if (mode == 1 && !first) MX_SWEEP(1, false, double);
+  }
 #undef MX_SWEEP
 }
 
-void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const float* e,
-                      double* guides) {
-  mx_guides_kernel<<<count, GT, 0, s>>>(C, e, guides);
+void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const void* e, double* guides,
+                      bool d64) {
+  if (d64)
+    mx_guides_kernel<double><<<count, GT, 0, s>>>(C, static_cast<const double*>(e), guides);
+  else
+    mx_guides_kernel<float><<<count, GT, 0, s>>>(C, static_cast<const float*>(e), guides);
 }
 
-void mx_grid_sizes(int* sweep, int* matvec, int* update, int* guides) {
+template <typename K>
+static void allow_sweep_smem(K kernel) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SWEEP_SMEM);
+}
+
+void mx_grid_sizes(int threads, int* sweep, int* matvec, int* update, int* guides) {
   int dev = 0, sms = 0, a = 0, b = 0, c = 0, d = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // the sweep kernels' shared memory, on the calling device (before any launch)
-  cudaFuncSetAttribute(mx_sweep_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       SWEEP_SMEM);
-  cudaFuncSetAttribute(mx_sweep_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       SWEEP_SMEM);
-  cudaFuncSetAttribute(mx_sweep_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       SWEEP_SMEM);
-  cudaFuncSetAttribute(mx_sweep_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       SWEEP_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true>, PT, SWEEP_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false>, PT, SWEEP_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2>, MT, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, mx_update_kernel, MT, 0);
+  allow_sweep_smem(mx_sweep_kernel<0, true, float>);
+  allow_sweep_smem(mx_sweep_kernel<0, false, float>);
+  allow_sweep_smem(mx_sweep_kernel<1, true, float>);
+  allow_sweep_smem(mx_sweep_kernel<1, false, float>);
+  allow_sweep_smem(mx_sweep_kernel<0, true, double>);
+  allow_sweep_smem(mx_sweep_kernel<0, false, double>);
+  allow_sweep_smem(mx_sweep_kernel<1, true, double>);
+  allow_sweep_smem(mx_sweep_kernel<1, false, double>);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, float>, PT,
+                                                SWEEP_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, float>, PT,
+                                                SWEEP_SMEM);
+  if (threads == 128) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2, false, float, 128>,
+                                                  128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, mx_update_kernel<float, 128>, 128, 0);
+  } else if (threads == 512) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2, false, float, 512>,
+                                                  512, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, mx_update_kernel<float, 512>, 512, 0);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2, false, float, 256>,
+                                                  256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, mx_update_kernel<float, 256>, 256, 0);
+  }
   *sweep = sms * std::max(1, std::min(a, b));
   int g = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, mx_guides_kernel, GT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, mx_guides_kernel<float>, GT, 0);
   *guides = sms * std::max(1, g);
   *matvec = sms * std::max(1, c);
   *update = sms * std::max(1, d);
 }
 
-void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, const float* x,
-                      const double* A, double* y, const double* w0) {
-  if (ndot == 1)
-    mx_matvec_kernel<1><<<count, MT, 0, s>>>(C, x, A, y, w0);
+template <typename ET, int NT>
+static void matvec_launch(cudaStream_t s, const MixCtx& C, int count, int ndot, const ET* x,
+                          const double* A, double* y, const double* w0) {
+  if (ndot == 1 && !C.cf)
+    mx_matvec_kernel<1, false, ET, NT><<<count, NT, 0, s>>>(C, x, A, y, w0);
+  else if (!C.cf)
+    mx_matvec_kernel<2, false, ET, NT><<<count, NT, 0, s>>>(C, x, A, y, w0);
+  else if (ndot == 1)
+    mx_matvec_kernel<1, true, ET, NT><<<count, NT, 0, s>>>(C, x, A, y, w0);
   else
-    mx_matvec_kernel<2><<<count, MT, 0, s>>>(C, x, A, y, w0);
+    mx_matvec_kernel<2, true, ET, NT><<<count, NT, 0, s>>>(C, x, A, y, w0);
 }
 
-void launch_mx_update(cudaStream_t s, const MixCtx& C, int count, double* x, const float* ph,
-                      const float* sh, double* r, const double* t, const double* sv,
+template <typename ET>
+static void matvec_nt(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads,
+                      const ET* x, const double* A, double* y, const double* w0) {
+  if (threads == 128)
+    matvec_launch<ET, 128>(s, C, count, ndot, x, A, y, w0);
+  else if (threads == 512)
+    matvec_launch<ET, 512>(s, C, count, ndot, x, A, y, w0);
+  else
+    matvec_launch<ET, 256>(s, C, count, ndot, x, A, y, w0);
+}
+
+void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads,
+                      const void* x, const double* A, double* y, const double* w0, bool d64) {
+  if (d64)
+    matvec_nt(s, C, count, ndot, threads, static_cast<const double*>(x), A, y, w0);
+  else
+    matvec_nt(s, C, count, ndot, threads, static_cast<const float*>(x), A, y, w0);
+}
+
+template <typename ET>
+static void update_nt(cudaStream_t s, const MixCtx& C, int count, int threads, double* x,
+                      const ET* ph, const ET* sh, double* r, const double* t, const double* sv,
                       const double* r0) {
-  mx_update_kernel<<<count, MT, 0, s>>>(C, x, ph, sh, r, t, sv, r0);
+  if (threads == 128)
+    mx_update_kernel<ET, 128><<<count, 128, 0, s>>>(C, x, ph, sh, r, t, sv, r0);
+  else if (threads == 512)
+    mx_update_kernel<ET, 512><<<count, 512, 0, s>>>(C, x, ph, sh, r, t, sv, r0);
+  else
+    mx_update_kernel<ET, 256><<<count, 256, 0, s>>>(C, x, ph, sh, r, t, sv, r0);
+}
+
+void launch_mx_update(cudaStream_t s, const MixCtx& C, int count, int threads, double* x,
+                      const void* ph, const void* sh, double* r, const double* t,
+                      const double* sv, const double* r0, bool d64) {
+  if (d64)
+    update_nt(s, C, count, threads, x, static_cast<const double*>(ph),
+              static_cast<const double*>(sh), r, t, sv, r0);
+  else
+    update_nt(s, C, count, threads, x, static_cast<const float*>(ph),
+              static_cast<const float*>(sh), r, t, sv, r0);
 }
 
 }  // namespace ffvgpu

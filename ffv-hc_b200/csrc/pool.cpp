@@ -617,6 +617,47 @@ ffvgpu_status ffvgpu_fold_bc(ffvgpu_pool* P) {
   return FFVGPU_OK;
 }
 
+// Solver::UpdateP's pressure sequence (Solver.cpp:5294-5688): P01, P02, P03,
+// P05, P06, P07.
+ffvgpu_status ffvgpu_update_p(ffvgpu_pool* P, const ffvgpu_step_params* prm,
+                              const ffvgpu_mixed_params* mixed, ffvgpu_result* res) {
+  if (!P || !prm) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
+  if (prm->solver == FFVGPU_SOLVER_MIXED && !mixed) return bad("mixed settings missing");
+  if (prm->solver < FFVGPU_SOLVER_RBGS || prm->solver > FFVGPU_SOLVER_MIXED)
+    return bad("unknown solver");
+  ffvgpu_status s;
+  if ((s = ffvgpu_remove_p(P, prm->rhof, prm->dt))) return s;  // P01
+  for (int c = 0; c < 3; ++c)                                    // P02
+    if ((s = ffvgpu_exchange(P, (ffvgpu_field)(FFVGPU_FIELD_UX + c), prm->u_bc_type[c],
+                             prm->u_bc_value[c])))
+      return s;
+  if ((s = ffvgpu_assemble_p(P, prm->rhof, prm->dt))) return s;  // P03
+  if ((s = ffvgpu_fold_bc(P))) return s;                           // P05
+  ffvgpu_status solved;                                            // P06
+  if (prm->solver == FFVGPU_SOLVER_RBGS)
+    solved = ffvgpu_solve_rbgs(P, &prm->iter, res);
+  else if (prm->solver == FFVGPU_SOLVER_BICGSTAB)
+    solved = ffvgpu_solve_bicgstab(P, &prm->iter, res);
+  else
+    solved = ffvgpu_solve_mixed(P, mixed, res);
+  if (solved != FFVGPU_OK && solved != FFVGPU_NOT_CONVERGED) return solved;
+  if ((s = ffvgpu_exchange(P, FFVGPU_FIELD_X, nullptr, nullptr))) return s;  // P07
+  return solved;
+}
+
+// Solver::UpdateU (Solver.cpp:5690-5771): U01, U02, U03 (p only).
+ffvgpu_status ffvgpu_update_u(ffvgpu_pool* P, const ffvgpu_step_params* prm) {
+  if (!P || !prm) return bad("null argument");
+  ffvgpu_status s;
+  if ((s = ffvgpu_corr_u(P, prm->rhof, prm->dt))) return s;  // U01
+  for (int c = 0; c < 3; ++c)                                 // U02
+    if ((s = ffvgpu_exchange(P, (ffvgpu_field)(FFVGPU_FIELD_UX + c), prm->u_bc_type[c],
+                             prm->u_bc_value[c])))
+      return s;
+  return ffvgpu_exchange(P, FFVGPU_FIELD_X, nullptr, nullptr);  // U03
+}
+
 ffvgpu_status ffvgpu_dot(ffvgpu_pool* P, ffvgpu_field fx, ffvgpu_field fy, double* xy) {
   if (!P || !xy) return bad("null argument");
   if (P->batch) return bad("a batch pool is used through the instance entry points");
@@ -1075,3 +1116,71 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
 }
 
 }  // extern "C"
+
+// ---- pieces of a sharded solve (ffvgpu_shard_*): one pass over a shard's
+// own blocks, per-block partial sums, the device address of the iterate ----
+
+ffvgpu_status ffvgpu_rbgs_pass(ffvgpu_pool* P, int32_t blocks, int32_t residual, int32_t sweep,
+                               int32_t stored, double omega, double* partials) {
+  if (!P) return bad("null pool");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
+  if (blocks < 1 || blocks > P->nb) return bad("blocks must lie in [1, pool blocks]");
+  const bool res = residual != 0, swp = sweep != 0, st = stored != 0;
+  if (!((!res && swp && st) || (res && swp && !st) || (res && !swp && !st)))
+    return bad("pass kinds: first sweep (stored guides), residual + sweep, residual");
+  if (res && !partials) return bad("null partials");
+  cudaSetDevice(P->device);
+  ffvgpu_status s;
+  if ((s = require_system(P))) return s;
+  if ((s = ensure_stream(P))) return s;
+  if ((s = reset_state(P, 0.0, 0, nullptr))) return s;
+  KCtx C = P->ctx(P->bc_p);
+  C.nb = blocks;
+  const int c = P->xcur;
+  launch_rbgs(P->stream, C, res, swp, P->x[c], swp ? P->x[1 - c] : nullptr, P->coef,
+              st ? P->gx : nullptr, omega, P->partials, P->st, FIN_STORE, 0);
+  CK(cudaGetLastError());
+  if (swp) P->xcur = 1 - c;
+  SolveState h;
+  if ((s = read_state(P, &h))) return s;
+  if (h.status == 3) {
+    g_last_error = timeout_message(h.timeout_where);
+    return FFVGPU_TIMEOUT;
+  }
+  if (res) CK(download_sync(P, partials, P->partials, sizeof(double) * blocks));
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_block_dots(ffvgpu_pool* P, ffvgpu_field fx, ffvgpu_field fy, int32_t blocks,
+                                double* partials) {
+  if (!P || !partials) return bad("null argument");
+  if (P->batch) return bad("a batch pool is used through the instance entry points");
+  if (blocks < 1 || blocks > P->nb) return bad("blocks must lie in [1, pool blocks]");
+  cudaSetDevice(P->device);
+  double *x, *y, *g;
+  size_t sx, sy;
+  ffvgpu_status s;
+  if ((s = field_ptr(P, fx, false, &x, &sx, &g)) || (s = field_ptr(P, fy, false, &y, &sy, &g)))
+    return s;
+  if (sx != BC || sy != BC) return bad("dot of matrix fields is not supported");
+  if ((s = reset_state(P, 0.0, 0, nullptr))) return s;
+  KCtx C = P->ctx(P->bc_p);
+  C.nb = blocks;
+  launch_dot(P->stream, C, x, y, P->partials, P->st, FIN_STORE, 0);
+  CK(cudaGetLastError());
+  return download_sync(P, partials, P->partials, sizeof(double) * blocks) == cudaSuccess
+             ? FFVGPU_OK
+             : cuda_fail(cudaGetLastError(), "block_dots");
+}
+
+ffvgpu_status ffvgpu_pool_field_device(ffvgpu_pool* P, ffvgpu_field f, void** ptr) {
+  if (!P || !ptr) return bad("null argument");
+  if (f != FFVGPU_FIELD_X && f != FFVGPU_FIELD_B) return bad("only X and B are exposed");
+  double *x, *g;
+  size_t stride;
+  ffvgpu_status s;
+  if ((s = field_ptr(P, f, false, &x, &stride, &g))) return s;
+  if (!x) return bad("field not allocated");
+  *ptr = x;
+  return FFVGPU_OK;
+}

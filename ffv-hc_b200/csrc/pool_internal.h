@@ -141,15 +141,28 @@ struct ffvgpu_pool {
   float* me[2] = {nullptr, nullptr};
   float* mph = nullptr;     // preconditioned p (p_)
   float* msh = nullptr;     // preconditioned s (s_)
+  // the FP64-data variant (ffvgpu_mixed_params.fp64_data): FP64 coefficients
+  // in the sweep's thread order, FP64 iterate and preconditioned vectors
+  double* mcoef64 = nullptr;  // [nb][7][4096]
+  double* me64[2] = {nullptr, nullptr};
+  double* mph64 = nullptr;
+  double* msh64 = nullptr;
   int64_t mcoef_version = 0;  // sys_version the sweep coefficients come from (one-grid pools)
   double m_omega = 0.0;
   int m_sweeps = 0, m_per_exchange = 0;
+  int m_cf = 0;   // coarse-fine flux correction of the running solves
+  int m_d64 = 0;  // the running solves use the FP64-data variant
+  int m_depth = 1;  // sweep kernel staging depth (L2 prefetch distance in blocks)
+  int m_threads = 256;  // CTA size of the A*x and update kernels
   cudaGraphExec_t mgraph = nullptr;
   int mgraph_iters = 0;
   double mgraph_omega = 0.0;
   int mgraph_sweeps = 0, mgraph_per = 0;
   uint64_t mgraph_wait_ns = 0;
   int mgraph_stall = 0;
+  int mgraph_cf = 0;
+  int mgraph_d64 = 0;
+  int mgraph_depth = 0, mgraph_threads = 0;
   int stall_sweep = 0;  // test hook (ffvgpu_pool_stall_next_solve), cleared when a solve ends
   int64_t m_launches = 0;
   int64_t m_bytes = 0;
@@ -160,6 +173,7 @@ struct ffvgpu_pool {
   cudaEvent_t act_ev[2] = {nullptr, nullptr};
   int act_next = 0;
   int grid_sweep = 0, grid_matvec = 0, grid_update = 0, grid_guides = 0;
+  int grid_threads = 0;  // m_threads the grid sizes were computed for
 
   ffvgpu::KCtx ctx(const ffvgpu::BCSet& bc) const {
     ffvgpu::KCtx C;

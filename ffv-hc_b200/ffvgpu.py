@@ -35,7 +35,11 @@ EXPORTS = [
     "ffvgpu_dot", "ffvgpu_version", "ffvgpu_last_error", "ffvgpu_sphere_grid_create",
     "ffvgpu_sphere_grid_destroy", "ffvgpu_sphere_grid_num_blocks",
     "ffvgpu_sphere_grid_blocks", "ffvgpu_sphere_grid_fill", "ffvgpu_dot_noalloc",
-    "ffvgpu_solve_mixed", "ffvgpu_batch_create", "ffvgpu_instance_admit",
+    "ffvgpu_solve_mixed", "ffvgpu_cf_flux_mismatch", "ffvgpu_update_p", "ffvgpu_update_u",
+    "ffvgpu_generate_sphere", "ffvgpu_shard_create", "ffvgpu_shard_destroy", "ffvgpu_shard_info",
+    "ffvgpu_shard_local_blocks", "ffvgpu_shard_zorder", "ffvgpu_shard_local_desc",
+    "ffvgpu_shard_peer", "ffvgpu_rbgs_pass", "ffvgpu_block_dots", "ffvgpu_pool_field_device",
+    "ffvgpu_canonical_sum", "ffvgpu_batch_create", "ffvgpu_instance_admit",
     "ffvgpu_instance_admit_sphere", "ffvgpu_instance_upload", "ffvgpu_instance_download",
     "ffvgpu_instance_release", "ffvgpu_instance_blocks", "ffvgpu_pool_free_blocks",
     "ffvgpu_mixed_begin", "ffvgpu_mixed_advance", "ffvgpu_mixed_poll", "ffvgpu_instance_result",
@@ -66,6 +70,17 @@ class IterParams(ctypes.Structure):
     ]
 
 
+class StepParams(ctypes.Structure):
+    _fields_ = [
+        ("rhof", ctypes.c_double), ("dt", ctypes.c_double),
+        ("u_bc_type", (ctypes.c_int32 * 6) * 3), ("u_bc_value", (ctypes.c_double * 6) * 3),
+        ("solver", ctypes.c_int32), ("iter", IterParams),
+    ]
+
+
+SOLVER_RBGS, SOLVER_BICGSTAB, SOLVER_MIXED = 0, 1, 2
+
+
 class Result(ctypes.Structure):
     _fields_ = [
         ("count", ctypes.c_int32), ("residual", ctypes.c_double),
@@ -91,6 +106,8 @@ class MixedParams(ctypes.Structure):
         ("epsilon", ctypes.c_double), ("check_every", ctypes.c_int32),
         ("history", ctypes.c_void_p), ("restart_drop", ctypes.c_double),
         ("restart_growth", ctypes.c_double), ("restart_every", ctypes.c_int32),
+        ("flux_correction", ctypes.c_int32), ("fp64_data", ctypes.c_int32),
+        ("threads_per_block", ctypes.c_int32), ("stage_depth", ctypes.c_int32),
     ]
 
 
@@ -118,6 +135,7 @@ class TuneRecord(ctypes.Structure):
         ("omega", ctypes.c_double), ("sweeps", ctypes.c_int32),
         ("sweeps_per_exchange", ctypes.c_int32), ("iterations_per_replay", ctypes.c_int32),
         ("ms", ctypes.c_double), ("max_count", ctypes.c_int32), ("converged", ctypes.c_int32),
+        ("threads_per_block", ctypes.c_int32), ("stage_depth", ctypes.c_int32),
     ]
 
 
@@ -126,6 +144,9 @@ class TuneRecord(ctypes.Structure):
 # iterations per replay.
 TUNE_SPACE = [(om, sw, per, it) for om in (1.5, 1.2) for (sw, per) in
               ((8, 4), (8, 8), (8, 2), (8, 1), (4, 4), (4, 2)) for it in (4, 8, 16)]
+# Then, for the fastest of those: threads per block of the A*x and update
+# kernels 128 / 256 / 512 and the sweep kernel's staging depth 1 / 2 / 3.
+TUNE_LAUNCH = [(nt, dp) for nt in (128, 256, 512) for dp in (1, 2, 3)]
 
 
 class Request(ctypes.Structure):
@@ -195,6 +216,23 @@ def lib():
         L.ffvgpu_dot_noalloc.argtypes = [vp, vp, i32, vp, vp]
         MP, R = ctypes.POINTER(MixedParams), ctypes.POINTER(Result)
         L.ffvgpu_solve_mixed.argtypes = [vp, MP, R]
+        L.ffvgpu_cf_flux_mismatch.argtypes = [vp, vp, vp, vp, vp, i32]
+        L.ffvgpu_update_p.argtypes = [vp, ctypes.POINTER(StepParams), vp, R]
+        L.ffvgpu_shard_create.argtypes = [ctypes.POINTER(GridDesc), i32, i32, ctypes.POINTER(vp)]
+        L.ffvgpu_shard_destroy.argtypes = [vp]
+        L.ffvgpu_shard_destroy.restype = None
+        L.ffvgpu_shard_info.argtypes = [vp, vp, vp]
+        L.ffvgpu_shard_local_blocks.argtypes = [vp, vp]
+        L.ffvgpu_shard_zorder.argtypes = [vp, vp, vp]
+        L.ffvgpu_shard_local_desc.argtypes = [vp]
+        L.ffvgpu_shard_local_desc.restype = ctypes.POINTER(GridDesc)
+        L.ffvgpu_shard_peer.argtypes = [vp, i32, vp, vp, vp, vp]
+        L.ffvgpu_rbgs_pass.argtypes = [vp, i32, i32, i32, i32, dbl, vp]
+        L.ffvgpu_block_dots.argtypes = [vp, i32, i32, i32, vp]
+        L.ffvgpu_pool_field_device.argtypes = [vp, i32, ctypes.POINTER(vp)]
+        L.ffvgpu_canonical_sum.argtypes = [vp, i32, vp]
+        L.ffvgpu_update_u.argtypes = [vp, ctypes.POINTER(StepParams)]
+        L.ffvgpu_generate_sphere.argtypes = [vp, ctypes.POINTER(SphereProblem)]
         L.ffvgpu_batch_create.argtypes = [ctypes.POINTER(BatchDesc), ctypes.POINTER(vp)]
         L.ffvgpu_instance_admit.argtypes = [vp, ctypes.POINTER(GridDesc), vp]
         L.ffvgpu_instance_admit_sphere.argtypes = [vp, ctypes.POINTER(SphereProblem), vp]
@@ -452,6 +490,70 @@ class Pool:
     def remove_p(self, rhof=1.0, dt=0.002):
         _check(lib().ffvgpu_remove_p(self._h, rhof, dt), "remove_p")
 
+    @staticmethod
+    def _step_params(rhof, dt, solver, omega, pre_count, count_max, epsilon, restart_drop):
+        sp = StepParams()
+        sp.rhof, sp.dt, sp.solver = rhof, dt, solver
+        for c, u in enumerate(("UX", "UY", "UZ")):
+            for f in range(6):
+                sp.u_bc_type[c][f] = U_BC_TYPE[f]
+                sp.u_bc_value[c][f] = U_BC_VALUE[u][f]
+        sp.iter = IterParams(omega, count_max, epsilon, pre_count, 0, None, restart_drop)
+        return sp
+
+    def update_p(self, solver=SOLVER_BICGSTAB, omega=1.0, pre_count=2, count_max=1000,
+                 epsilon=1e-8, restart_drop=0.0, rhof=1.0, dt=0.002, mixed=None):
+        """Solver::UpdateP's pressure sequence (ffvgpu_update_p) with the sphere
+        example's velocity BCs; mixed: dict of solve_mixed settings for SOLVER_MIXED."""
+        sp = self._step_params(rhof, dt, solver, omega, pre_count, count_max, epsilon,
+                               restart_drop)
+        mp = None
+        if solver == SOLVER_MIXED:
+            m = dict(omega=1.5, sweeps=8, sweeps_per_exchange=4, flux_correction=False)
+            m.update(mixed or {})
+            mp = MixedParams(m["omega"], m["sweeps"], m["sweeps_per_exchange"], count_max,
+                             epsilon, 0, None, *_restart(None, None, None))
+            mp.flux_correction = int(bool(m["flux_correction"]))
+        res = Result()
+        st = lib().ffvgpu_update_p(self._h, ctypes.byref(sp),
+                                   ctypes.byref(mp) if mp is not None else None,
+                                   ctypes.byref(res))
+        _check(st, "update_p", allow=(OK, NOT_CONVERGED))
+        return dict(status=st, count=res.count, residual=res.residual, elapsed_ms=res.elapsed_ms,
+                    bytes_moved=res.bytes_moved, kernel_launches=res.kernel_launches)
+
+    def update_u(self, rhof=1.0, dt=0.002):
+        """Solver::UpdateU (ffvgpu_update_u) with the sphere example's velocity BCs."""
+        sp = self._step_params(rhof, dt, SOLVER_BICGSTAB, 1.0, 0, 0, 0.0, 0.0)
+        _check(lib().ffvgpu_update_u(self._h, ctypes.byref(sp)), "update_u")
+
+    # ---- pieces of a sharded solve -------------------------------------
+    def rbgs_pass(self, blocks, residual, sweep, stored, omega):
+        """One red-black pass over the first 'blocks' blocks (ffvgpu_rbgs_pass);
+        returns the per-block residual partials when residual is set."""
+        part = np.zeros(max(blocks, 1), np.float64) if residual else None
+        _check(lib().ffvgpu_rbgs_pass(self._h, blocks, int(residual), int(sweep), int(stored),
+                                      float(omega), _ptr(part) if residual else None),
+               "rbgs_pass")
+        return part
+
+    def block_dots(self, fx, fy, blocks):
+        part = np.zeros(max(blocks, 1), np.float64)
+        _check(lib().ffvgpu_block_dots(self._h, FIELD[fx], FIELD[fy], blocks, _ptr(part)),
+               "block_dots")
+        return part
+
+    def field_device(self, field="X"):
+        """Device address of the current iterate (X) or of b (B): blocks x 4096 doubles."""
+        v = ctypes.c_void_p()
+        _check(lib().ffvgpu_pool_field_device(self._h, FIELD[field], ctypes.byref(v)),
+               "pool_field_device")
+        return v.value
+
+    def generate_sphere(self, problem):
+        """Device-generated u*, cut fields and flags only (ffvgpu_generate_sphere)."""
+        _check(lib().ffvgpu_generate_sphere(self._h, ctypes.byref(problem)), "generate_sphere")
+
     def corr_u(self, rhof=1.0, dt=0.002):
         _check(lib().ffvgpu_corr_u(self._h, rhof, dt), "corr_u")
 
@@ -490,18 +592,41 @@ class Pool:
         _check(lib().ffvgpu_dot(self._h, FIELD[fx], FIELD[fy], ctypes.byref(v)), "dot")
         return v.value
 
+    def cf_flux_mismatch(self, per_cell=False):
+        """Coarse-fine flux mismatch of X (ffvgpu_cf_flux_mismatch): dict with
+        mismatch = sum V|delta|, flux = sum V|F|, cells, and with per_cell an
+        array [cells][2] of (delta, F) in (block, face, position) order."""
+        m, fl, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int32()
+        _check(lib().ffvgpu_cf_flux_mismatch(self._h, ctypes.byref(m), ctypes.byref(fl),
+                                             ctypes.byref(n), None, 0), "cf_flux_mismatch")
+        out = dict(mismatch=m.value, flux=fl.value, cells=n.value)
+        if per_cell:
+            arr = np.zeros((max(n.value, 1), 2), np.float64)
+            _check(lib().ffvgpu_cf_flux_mismatch(self._h, ctypes.byref(m), ctypes.byref(fl),
+                                                 ctypes.byref(n), arr.ctypes.data, n.value),
+                   "cf_flux_mismatch")
+            out["per_cell"] = arr[:n.value]
+        return out
+
     def assemble_sphere(self, problem):
         """Device-generated sphere-flow inputs + UpdateP P02-P05 (pool made from its grid)."""
         _check(lib().ffvgpu_assemble_sphere(self._h, ctypes.byref(problem)), "assemble_sphere")
 
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
                     epsilon=1e-8, history=True, check_every=0, restart_drop=None,
-                    restart_growth=None, restart_every=None):
-        """Mixed-precision solve (FP64 BiCGSTAB; RB-SOR preconditioner on 32-bit data)."""
+                    restart_growth=None, restart_every=None, flux_correction=False,
+                    fp64_data=False, threads_per_block=0, stage_depth=0):
+        """Mixed-precision solve (FP64 BiCGSTAB; RB-SOR preconditioner on 32-bit data).
+        flux_correction: the FP64 residual and A*x use the coarse-fine
+        flux-conserving operator; fp64_data: the same preconditioner on FP64 data;
+        threads_per_block, stage_depth: launch settings (0: defaults)."""
         hist = np.zeros(max(count_max, 1), np.float64) if history else None
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
                           hist.ctypes.data if history else None,
                           *_restart(restart_drop, restart_growth, restart_every))
+        prm.flux_correction = int(bool(flux_correction))
+        prm.fp64_data = int(bool(fp64_data))
+        prm.threads_per_block, prm.stage_depth = int(threads_per_block), int(stage_depth)
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -512,6 +637,128 @@ class Pool:
             n = res.count if 1 <= res.count <= count_max else (count_max if res.count > 0 else 0)
             out["history"] = hist[:n].copy()
         return out
+
+
+def canonical_sum(partials):
+    """The pool's cross-block reduction over per-block partials in block order."""
+    a = np.ascontiguousarray(partials, np.float64)
+    t = ctypes.c_double()
+    _check(lib().ffvgpu_canonical_sum(_ptr(a), len(a), ctypes.byref(t)), "canonical_sum")
+    return t.value
+
+
+class Shard:
+    """One rank's part of a grid sharded across ranks (ffvgpu_shard_*): its own
+    blocks (local 0 .. owned-1), halo blocks, and the exchange lists per peer."""
+
+    def __init__(self, desc, num_ranks, rank):
+        self._h = ctypes.c_void_p()
+        self._desc = desc
+        _check(lib().ffvgpu_shard_create(ctypes.byref(desc), num_ranks, rank,
+                                         ctypes.byref(self._h)), "shard_create")
+        o, h = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().ffvgpu_shard_info(self._h, ctypes.byref(o), ctypes.byref(h)), "shard_info")
+        self.ranks, self.rank = num_ranks, rank
+        self.owned, self.halo = o.value, h.value
+        self.local = np.zeros(self.owned + self.halo, np.int32)
+        _check(lib().ffvgpu_shard_local_blocks(self._h, _ptr(self.local)), "shard_local_blocks")
+        n = desc.num_blocks
+        self.zorder = np.zeros(n, np.int32)
+        self.owner = np.zeros(n, np.int32)
+        _check(lib().ffvgpu_shard_zorder(self._h, _ptr(self.zorder), _ptr(self.owner)),
+               "shard_zorder")
+        self.send, self.recv = {}, {}
+        for p in range(num_ranks):
+            if p == rank:
+                continue
+            ns, nr = ctypes.c_int32(), ctypes.c_int32()
+            _check(lib().ffvgpu_shard_peer(self._h, p, ctypes.byref(ns), None, ctypes.byref(nr),
+                                           None), "shard_peer")
+            sl = np.zeros(max(ns.value, 1), np.int32)
+            rl = np.zeros(max(nr.value, 1), np.int32)
+            _check(lib().ffvgpu_shard_peer(self._h, p, ctypes.byref(ns), _ptr(sl),
+                                           ctypes.byref(nr), _ptr(rl)), "shard_peer")
+            self.send[p] = sl[:ns.value]
+            self.recv[p] = rl[:nr.value]
+
+    def desc(self):
+        """The local grid description (pointers valid while this object lives)."""
+        return lib().ffvgpu_shard_local_desc(self._h).contents
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None and self._h.value:
+            _lib.ffvgpu_shard_destroy(self._h)
+        self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+
+class _DeviceArray:
+    """A device array for torch.as_tensor (__cuda_array_interface__, no copy)."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8",
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None}
+
+
+def pool_iterate(pool, blocks):
+    """torch view [blocks][4096] of the pool's current iterate (device memory, no copy)."""
+    import torch
+    return torch.as_tensor(_DeviceArray(pool.field_device("X"), (blocks, 4096)), device="cuda")
+
+
+def halo_exchange(dist, shard, x):
+    """One exchange of a shard's halo blocks over torch.distributed: x is the
+    rank's [local blocks][4096] iterate (a device view of the pool, or a host
+    tensor); every rank sends each peer the blocks shard.send lists and
+    stores what the peer sends into the blocks shard.recv lists, in list
+    order.  Point-to-point only, the same steps on every rank."""
+    import torch
+    ops, recvs = [], []
+    for p in sorted(set(shard.send) | set(shard.recv)):
+        snd, rcv = shard.send.get(p, ()), shard.recv.get(p, ())
+        if len(snd):
+            idx = torch.as_tensor(np.asarray(snd, np.int64), device=x.device)
+            ops.append(dist.P2POp(dist.isend, x.index_select(0, idx).contiguous(), p))
+        if len(rcv):
+            buf = torch.empty((len(rcv), x.shape[1]), dtype=x.dtype, device=x.device)
+            ops.append(dist.P2POp(dist.irecv, buf, p))
+            recvs.append((rcv, buf))
+    if ops:
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
+    for rcv, buf in recvs:
+        x.index_copy_(0, torch.as_tensor(np.asarray(rcv, np.int64), device=x.device), buf)
+
+
+def sharded_rbgs(parts, omega, count, exchange, gather):
+    """FFVILS::RBGS (ffvgpu_solve_rbgs's passes, epsilon 0) on a sharded grid.
+    parts: the [(pool, shard)] this process drives (one per GPU: one part per
+    rank over torch.distributed, or every part on one device); exchange():
+    refreshes every part's halo blocks of the current iterate from their
+    owners (halo_exchange); gather(list of per-block partials, one array per
+    part, own blocks in local order): the per-block partials of every block
+    of the grid in global block order.  Returns the residual history, bit for
+    bit the unsharded pool's: same passes, same per-block sums, same
+    cross-block tree."""
+    tiny = float(np.finfo(np.float32).tiny)
+    bb = canonical_sum(gather([P.block_dots("B", "B", S.owned) for P, S in parts]))
+
+    def resid(partials):
+        rr = canonical_sum(gather(partials))
+        return float(np.sqrt(abs(rr) / abs(bb))) if abs(bb) > tiny else float(np.sqrt(abs(rr)))
+
+    for P, S in parts:
+        P.rbgs_pass(S.owned, 0, 1, 1, omega)
+    hist = []
+    for _ in range(2, count + 1):
+        exchange()
+        hist.append(resid([P.rbgs_pass(S.owned, 1, 1, 0, omega) for P, S in parts]))
+    exchange()
+    hist.append(resid([P.rbgs_pass(S.owned, 1, 0, 0, omega) for P, S in parts]))
+    return np.array(hist)
 
 
 def _restart(drop, growth, every):
@@ -616,10 +863,14 @@ class Batch:
 
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
                     epsilon=1e-8, check_every=0, restart_drop=None, restart_growth=None,
-                    restart_every=None):
+                    restart_every=None, flux_correction=False, fp64_data=False,
+                    threads_per_block=0, stage_depth=0):
         """Solves every admitted instance; returns the first instance's result."""
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
                           None, *_restart(restart_drop, restart_growth, restart_every))
+        prm.flux_correction = int(bool(flux_correction))
+        prm.fp64_data = int(bool(fp64_data))
+        prm.threads_per_block, prm.stage_depth = int(threads_per_block), int(stage_depth)
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -646,28 +897,50 @@ class Batch:
                      finish_s=out[i].finish_s, count=out[i].count, residual=out[i].residual,
                      status=out[i].status, blocks=out[i].blocks) for i in range(n)]
 
-    def autotune(self, instances, space=None, count_max=1500, epsilon=1e-8):
-        """ffvgpu_mixed_autotune over space (omega, sweeps, per-exchange, replay
-        iterations): (records as dicts, index of the best or -1)."""
-        space = space or TUNE_SPACE
-        recs = (TuneRecord * len(space))()
-        for k, (om, sw, per, it) in enumerate(space):
+    def _tune(self, ids, cands, count_max, epsilon):
+        recs = (TuneRecord * len(cands))()
+        for k, (om, sw, per, it, nt, dp) in enumerate(cands):
             recs[k].omega, recs[k].sweeps = om, sw
             recs[k].sweeps_per_exchange, recs[k].iterations_per_replay = per, it
-        ids = np.ascontiguousarray(instances, np.int32)
+            recs[k].threads_per_block, recs[k].stage_depth = nt, dp
         prm = MixedParams(1.5, 8, 4, count_max, epsilon, 0, None, *_restart(None, None, None))
         best = ctypes.c_int32()
         _check(lib().ffvgpu_mixed_autotune(self._h, _ptr(ids), len(ids), ctypes.byref(prm),
-                                           recs, len(space), ctypes.byref(best)), "autotune")
+                                           recs, len(cands), ctypes.byref(best)), "autotune")
         out = [dict(omega=r.omega, sweeps=r.sweeps, sweeps_per_exchange=r.sweeps_per_exchange,
-                    iterations_per_replay=r.iterations_per_replay, ms=r.ms,
-                    max_count=r.max_count, converged=bool(r.converged)) for r in recs]
+                    iterations_per_replay=r.iterations_per_replay,
+                    threads_per_block=r.threads_per_block or 256, stage_depth=r.stage_depth or 1,
+                    ms=r.ms, max_count=r.max_count, converged=bool(r.converged)) for r in recs]
         return out, best.value
 
+    def autotune(self, instances, space=None, launch=None, count_max=1500, epsilon=1e-8):
+        """ffvgpu_mixed_autotune in two stages: the numerical settings of space
+        (omega, sweeps, per-exchange, replay iterations) at 256 threads and
+        staging depth 1, then the fastest of them over launch (threads per
+        block, staging depth).  Returns (records as dicts, index of the best
+        or -1)."""
+        ids = np.ascontiguousarray(instances, np.int32)
+        space = space or TUNE_SPACE
+        launch = launch or TUNE_LAUNCH
+        recs, best = self._tune(ids, [(om, sw, per, it, 256, 1) for (om, sw, per, it) in space],
+                                count_max, epsilon)
+        if best < 0:
+            return recs, best
+        b = recs[best]
+        head = (b["omega"], b["sweeps"], b["sweeps_per_exchange"], b["iterations_per_replay"])
+        more, best2 = self._tune(ids, [head + (nt, dp) for (nt, dp) in launch
+                                       if (nt, dp) != (256, 1)], count_max, epsilon)
+        recs2 = recs + more
+        if best2 >= 0 and more[best2]["ms"] < b["ms"]:
+            best = len(recs) + best2
+        return recs2, best
+
     def begin(self, inst, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-              epsilon=1e-8, restart_drop=None, restart_growth=None, restart_every=None):
+              epsilon=1e-8, restart_drop=None, restart_growth=None, restart_every=None,
+              threads_per_block=0, stage_depth=0):
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, 0, None,
                           *_restart(restart_drop, restart_growth, restart_every))
+        prm.threads_per_block, prm.stage_depth = int(threads_per_block), int(stage_depth)
         _check(lib().ffvgpu_mixed_begin(self._h, inst, ctypes.byref(prm)), "mixed_begin")
 
     def cancel(self, inst):

@@ -302,6 +302,58 @@ ffvgpu_status ffvgpu_sphere_grid_fill(const ffvgpu_sphere_grid* g, uint64_t seed
 ffvgpu_status ffvgpu_remove_p(ffvgpu_pool* pool, double rhof, double dt);
 ffvgpu_status ffvgpu_corr_u(ffvgpu_pool* pool, double rhof, double dt);
 
+/* ---- block sharding across GPUs (one process per GPU) ---------------------
+ * The reference spreads its leaf blocks over MPI ranks as contiguous ranges
+ * of its ordered leaf list (Solver::InitTree / InitBlocks,
+ * src/FFV/Solver.cpp:306-381) and exchanges guide faces between ranks.  A
+ * shard plan puts the leaves in Z order (root blocks x fastest, then the
+ * Morton order of each leaf's position in its root block at the finest
+ * level), gives rank r the r-th of num_ranks contiguous ranges (sizes differ
+ * by at most one) and describes r's local grid: its own blocks (local ids
+ * 0 .. owned-1, in Z order), then halo blocks -- copies of other ranks'
+ * blocks that its blocks' guide cells are computed from -- grouped by owner
+ * rank, Z order within a group.  The local description carries an explicit
+ * neighbour table (halo blocks have outer faces: they are never solved), so
+ * ffvgpu_pool_create on it gives the shard's pool.  Before every pass that
+ * reads neighbours, rank r sends peer p the interiors (ffvgpu_pool_field_device
+ * layout, 4096 doubles per block) of the local blocks ffvgpu_shard_peer lists
+ * under send, and stores what p sends into the blocks listed under recv, in
+ * list order; the in-kernel exchange then gives the unsharded grid's guide
+ * values.  Sums stay those of the unsharded pool when every rank's per-block
+ * partials (ffvgpu_rbgs_pass, ffvgpu_block_dots) are gathered into global
+ * block order and added by ffvgpu_canonical_sum. */
+typedef struct ffvgpu_shard ffvgpu_shard;
+ffvgpu_status ffvgpu_shard_create(const ffvgpu_grid_desc* global, int32_t num_ranks,
+                                  int32_t rank, ffvgpu_shard** out);
+void ffvgpu_shard_destroy(ffvgpu_shard* shard);
+ffvgpu_status ffvgpu_shard_info(const ffvgpu_shard* shard, int32_t* owned, int32_t* halo);
+/* global id of every local block, [owned + halo] */
+ffvgpu_status ffvgpu_shard_local_blocks(const ffvgpu_shard* shard, int32_t* global_ids);
+/* global ids in Z order [num_blocks] and the owner rank of every block [num_blocks] */
+ffvgpu_status ffvgpu_shard_zorder(const ffvgpu_shard* shard, int32_t* order, int32_t* owner);
+/* the local grid description (valid while the shard lives) */
+const ffvgpu_grid_desc* ffvgpu_shard_local_desc(const ffvgpu_shard* shard);
+/* exchange lists with one peer: local ids to send, local ids to receive into */
+ffvgpu_status ffvgpu_shard_peer(const ffvgpu_shard* shard, int32_t peer, int32_t* n_send,
+                                int32_t* send_local, int32_t* n_recv, int32_t* recv_local);
+/* One pass of the red-black kernel over the pool's first 'blocks' blocks (a
+ * shard's own blocks), the passes of ffvgpu_solve_rbgs: first sweep
+ * (residual 0, sweep 1, stored 1: the guide layer stored with x), residual of
+ * the current iterate + sweep (1, 1, 0), last residual (1, 0, 0).  A sweep
+ * makes its result the current iterate; a residual writes each block's sum
+ * of (b - A x)^2 (the pool's per-block tree) into partials[blocks]. */
+ffvgpu_status ffvgpu_rbgs_pass(ffvgpu_pool* pool, int32_t blocks, int32_t residual,
+                               int32_t sweep, int32_t stored, double omega, double* partials);
+/* Per-block sums x.y (the pool's per-block tree) of the first 'blocks' blocks. */
+ffvgpu_status ffvgpu_block_dots(ffvgpu_pool* pool, ffvgpu_field x, ffvgpu_field y,
+                                int32_t blocks, double* partials);
+/* Device address of the current iterate (FIELD_X) or of b (FIELD_B):
+ * per block 4096 doubles in the pool's colour-split cell order. */
+ffvgpu_status ffvgpu_pool_field_device(ffvgpu_pool* pool, ffvgpu_field field, void** ptr);
+/* The cross-block stage of the pool's reduction tree over per-block partials
+ * in block order (host only): the same bits as the pool's own sums. */
+ffvgpu_status ffvgpu_canonical_sum(const double* partials, int32_t n, double* total);
+
 /* ---- restart files: LocalScalar3D::Dump2 / Load2 -------------------------
  * (src/FFV/LocalScalar3D.cpp:216-354).  The file holds six native int32
  * (cells per block x, y, z = 16, guide width vc, 1, number of blocks) and then
@@ -350,12 +402,70 @@ typedef struct {
   double restart_growth;       /* also restart when the residual exceeds this factor times
                                   the cycle's smallest; 0: never */
   int32_t restart_every;       /* also restart after this many iterations of a cycle; 0: never */
+  int32_t flux_correction;     /* 1: the FP64 residual and A*x products use the coarse-fine
+                                  flux-conserving operator (ffvgpu_cf_flux_mismatch describes
+                                  it); the sweeps keep the interpolating one.  0: the
+                                  reference's operator */
+  int32_t fp64_data;           /* 1: the same preconditioner on FP64 data -- coefficients and
+                                  the iterate between exchanges in FP64, the preconditioned
+                                  vectors in FP64 -- so that a comparison with the default
+                                  (32-bit data) isolates what the 32-bit data buy */
+  int32_t threads_per_block;   /* CTA size of the A*x and update kernels: 128, 256 or 512
+                                  (0: 256); results do not depend on it */
+  int32_t stage_depth;         /* sweep kernel: how many blocks ahead a block's data are
+                                  brought into L2 (1..3; 0: 1); results do not depend on it */
 } ffvgpu_mixed_params;
 
 /* Solves every admitted instance of the pool (a pool made from one grid is
  * one instance); res receives instance 0's result when it is not NULL. */
 ffvgpu_status ffvgpu_solve_mixed(ffvgpu_pool* pool, const ffvgpu_mixed_params* prm,
                                  ffvgpu_result* res);
+
+/* Coarse-fine flux conservation (no counterpart in the reference, whose 2:1
+ * exchange interpolates, src/CGMfuncs/sup.f90:54-179, and so does not
+ * conserve flux across coarse-fine faces).  For every coarse cell P on a
+ * face f whose neighbours are four finer blocks: the flux through f as the
+ * four fine cells phi touching it see it, in P's equation,
+ *   F = 0.125 * sum_{dv, du} A_fo(phi) * (x_phi - g_phi)
+ * (fo the opposite face, g_phi phi's guide value across fo, the
+ * prolongation; du inner, dv outer, summed from 0), and
+ *   delta = F - A_f(P) * (g - x_P),
+ * the difference from the coarse side's own term (g: P's guide value across
+ * f, the restriction).  The flux-conserving operator of
+ * ffvgpu_mixed_params.flux_correction adds delta to (A x)_P per such face in
+ * face order.  This call evaluates both on FIELD_X (interior and stored
+ * guide layer, as a solve leaves it) and returns mismatch = sum V_P |delta|
+ * and flux = sum V_P |F| (V_P = dx^3), in FP64, over the n_cells such cells
+ * in (block, face, position u + 16 v) order; per_cell (optional, capacity
+ * pairs) receives (delta, F) per cell in that order. */
+ffvgpu_status ffvgpu_cf_flux_mismatch(ffvgpu_pool* pool, double* mismatch, double* flux,
+                                      int32_t* n_cells, double* per_cell, int32_t capacity);
+
+/* ---- the pressure part of a fractional time step ---------------------------
+ * Solver::UpdateP (src/FFV/Solver.cpp:5294-5688) and Solver::UpdateU
+ * (Solver.cpp:5690-5771) on the device, in the reference's order:
+ * update_p: P01 bcut_remove_p (the previous pressure), P02 exchange of UX,
+ * UY, UZ with u_bc, P03 bcut_calc_ab_p, P05 BC folding, P06 the solve (x
+ * starts from the previous pressure), P07 exchange of p;
+ * update_u: U01 bcut_corr_u, U02 exchange of UX, UY, UZ, U03 exchange of p.
+ * P04 (the reference-pressure pin, only active for all-Neumann problems,
+ * Solver.cpp:5495-5566) and gravity/forcing (bcut_add_g, bcut_add_f) are not
+ * part of this path; LapP's exchange in U03 is left out (no kernel of the
+ * path reads its guide cells).  res receives the solve's result. */
+enum { FFVGPU_SOLVER_RBGS = 0, FFVGPU_SOLVER_BICGSTAB = 1, FFVGPU_SOLVER_MIXED = 2 };
+typedef struct {
+  double rhof;
+  double dt;
+  int32_t u_bc_type[3][6];   /* per velocity component and face */
+  double u_bc_value[3][6];
+  int32_t solver;            /* FFVGPU_SOLVER_* */
+  ffvgpu_iter_params iter;   /* RBGS, BiCGSTAB */
+} ffvgpu_step_params;
+
+/* mixed: the mixed-form settings when solver is FFVGPU_SOLVER_MIXED (else NULL). */
+ffvgpu_status ffvgpu_update_p(ffvgpu_pool* pool, const ffvgpu_step_params* prm,
+                              const ffvgpu_mixed_params* mixed, ffvgpu_result* res);
+ffvgpu_status ffvgpu_update_u(ffvgpu_pool* pool, const ffvgpu_step_params* prm);
 
 /* ---- batches: independent problems sharing one pool (no counterpart in the
  * reference) ---------------------------------------------------------------
@@ -402,6 +512,10 @@ ffvgpu_status ffvgpu_instance_admit_sphere(ffvgpu_pool* pool, const ffvgpu_spher
 /* The same generation and assembly for a pool made from the problem's own
  * grid (ffvgpu_pool_create on the blocks of ffvgpu_sphere_grid_create). */
 ffvgpu_status ffvgpu_assemble_sphere(ffvgpu_pool* pool, const ffvgpu_sphere_problem* prob);
+/* Only the generation: u* (UX, UY, UZ interiors), the cut fields and the
+ * phase flags of the problem, and the u BCs; no exchange, no assembly, the
+ * pressure untouched.  The time-step loop below regenerates u* with it. */
+ffvgpu_status ffvgpu_generate_sphere(ffvgpu_pool* pool, const ffvgpu_sphere_problem* prob);
 /* Per-instance transfers in the reference layout of ffvgpu_pool_upload /
  * ffvgpu_pool_download (host buffers hold the instance's blocks only). */
 ffvgpu_status ffvgpu_instance_upload(ffvgpu_pool* pool, int32_t instance, ffvgpu_field field,
@@ -441,8 +555,9 @@ ffvgpu_status ffvgpu_instance_result(const ffvgpu_pool* pool, int32_t instance,
 
 /* The autotuner (no counterpart in the reference): times the mixed solve of
  * the given admitted instances from x = 0 for each candidate setting --
- * omega, sweeps, sweeps_per_exchange, and iterations per captured-graph
- * replay -- with base's count_max, epsilon and restart settings, fills in
+ * omega, sweeps, sweeps_per_exchange, iterations per captured-graph replay,
+ * threads per block of the A*x and update kernels and the sweep kernel's
+ * staging depth -- with base's count_max, epsilon and restart settings, fills in
  * each record's device time (ms), its largest iteration count and whether
  * every instance reached epsilon, and sets *best to the fastest candidate
  * that converged them all (-1 if none did).  The instances end with x = 0. */
@@ -454,6 +569,8 @@ typedef struct {
   double ms;          /* out */
   int32_t max_count;  /* out */
   int32_t converged;  /* out: 1 when every instance reached epsilon */
+  int32_t threads_per_block;  /* as ffvgpu_mixed_params (0: 256) */
+  int32_t stage_depth;        /* as ffvgpu_mixed_params (0: 1) */
 } ffvgpu_tune_record;
 
 ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* pool, const int32_t* instances,

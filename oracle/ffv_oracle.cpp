@@ -1277,7 +1277,10 @@ int orc_bicgstab_restart(Oracle* O, double omega, int countPre, int countMax, do
 //     e = fma(-omega, e - xt, e)
 //   at the end of a pass the iterate is rounded to FP32.
 // The preconditioned vectors' guides come from the pressure-BC exchange
-// before CalcAx, and every dot product is DOT.
+// before CalcAx, and every dot product is DOT.  The FP64-data variant
+// (data64) keeps the coefficients unrounded and the iterate in FP64 between
+// passes; the arithmetic is the same.  With cf, the FP64 residual and both
+// A*x products add the coarse-fine flux correction (cf_apply).
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1294,34 +1297,38 @@ double round_hi(double x) {
   return d;
 }
 
-void mixed_coef(Oracle& O, Coef32& C) {
+// data64 (the FP64-data variant): the FP64 values themselves, unrounded.
+void mixed_coef(Oracle& O, Coef32& C, bool data64) {
   const long N = (long)O.G.nb * O.G.nc;
   const int src[6] = {OF_AW, OF_AE, OF_AS, OF_AN, OF_AB, OF_AT};
+  auto rnd = [data64](double v) { return data64 ? v : round_hi(v); };
   for (int a = 0; a < 7; ++a) C.a[a].assign(N, 0.0);
   for (int bi = 0; bi < O.G.nb; ++bi)
     for (long m = 0; m < O.G.nc; ++m) {
       const long g = (long)bi * O.G.nc + m;
-      for (int a = 0; a < 6; ++a) C.a[a][g] = round_hi(O.F(src[a], bi)[m]);
-      C.a[6][g] = round_hi(1.0 / O.F(OF_AP, bi)[m]);
+      for (int a = 0; a < 6; ++a) C.a[a][g] = rnd(O.F(src[a], bi)[m]);
+      C.a[6][g] = rnd(1.0 / O.F(OF_AP, bi)[m]);
     }
 }
 
 // out = M(v), widened to double (interior).  The pass's FP64 iterate with
-// its guide layer lives in the scratch field Z.
+// its guide layer lives in the scratch field Z.  Between passes the iterate
+// is rounded to FP32 (data64: kept in FP64).
 void mixed_precondition(Oracle& O, const Coef32& C, int fv, int fout, float omega, int sweeps,
-                        int per) {
+                        int per, bool data64) {
   Grid& G = O.G;
   const int n = G.n;
   const long sy = n + 2 * G.g, sz = sy * sy;
   const long N = (long)G.nb * G.nc;
-  std::vector<float> e(N, 0.0f);  // the iterate between passes (interior)
+  std::vector<double> e(N, 0.0);  // the iterate between passes (interior)
+  auto store = [data64](double v) { return data64 ? v : (double)(float)v; };
   const int hom_t[6] = {BC_DIRICHLET, BC_DIRICHLET, BC_DIRICHLET,
                         BC_DIRICHLET, BC_DIRICHLET, BC_DIRICHLET};
   const double hom_v[6] = {0, 0, 0, 0, 0, 0};
   for (int ps = 0; ps < sweeps / per; ++ps) {
     for (int bi = 0; bi < G.nb; ++bi) {
       double* z = O.F(OF_Z, bi);
-      for (long m = 0; m < G.nc; ++m) z[m] = (ps == 0) ? 0.0 : (double)e[(long)bi * G.nc + m];
+      for (long m = 0; m < G.nc; ++m) z[m] = (ps == 0) ? 0.0 : e[(long)bi * G.nc + m];
     }
     if (ps > 0) impose_bc(O, OF_Z, hom_t, hom_v);  // guide layer 1 of the iterate, in double
     for (int it = 0; it < per; ++it)
@@ -1355,7 +1362,7 @@ void mixed_precondition(Oracle& O, const Coef32& C, int fv, int fout, float omeg
         for (int j = 1; j <= n; ++j)
           for (int i = 1; i <= n; ++i) {
             const long m = IDX(G, i, j, k);
-            e[(long)bi * G.nc + m] = (float)z[m];
+            e[(long)bi * G.nc + m] = store(z[m]);
           }
     }
   }
@@ -1365,16 +1372,109 @@ void mixed_precondition(Oracle& O, const Coef32& C, int fv, int fout, float omeg
       for (int j = 1; j <= n; ++j)
         for (int i = 1; i <= n; ++i) {
           const long m = IDX(G, i, j, k);
-          out[m] = (double)e[(long)bi * G.nc + m];
+          out[m] = e[(long)bi * G.nc + m];
         }
   }
 }
 
+// Coarse-fine flux correction (no counterpart in the reference; restates
+// ffv-hc_b200/csrc/ffvgpu_internal.cuh cf_fine_flux and cf_delta).  For the
+// coarse cell at 0-based transverse position (a, b) of face f of block bi,
+// whose neighbours across f are finer: F = 0.125 * sum over the four fine
+// cells phi touching the face (du inner, dv outer, from 0.0) of
+// A_fo(phi) * (x_phi - g_phi), g_phi phi's guide cell across the opposite
+// face fo; delta = F - A_f(P) * (g - x_P).  Guide cells as field fx holds them.
+void cf_cell(Oracle& O, int fx, int bi, int f, int a, int b, double& delta, double& F) {
+  const Grid& G = O.G;
+  const Block& B = G.blocks[bi];
+  const int coef_of[6] = {OF_AW, OF_AE, OF_AS, OF_AN, OF_AB, OF_AT};
+  const int axis = f >> 1, fo = f ^ 1;
+  const bool plus = f & 1;
+  const int ta = (axis == 0) ? 1 : 0, tb = (axis == 2) ? 1 : 2;
+  // subface of the quarter (a >> 3, b >> 3) as the reference's updater
+  // numbers them (so0 + 2 so1, Scalar3DUpdater1.cpp:430-520): so0 along the
+  // face's first transverse axis, except on Y faces, where so0 runs along z
+  const int qa = a >> 3, qb = b >> 3;
+  const int fb = B.nbr[f][axis == 1 ? qb + 2 * qa : qa + 2 * qb];
+  const int gstep = (fo & 1) ? 1 : -1;  // the fine cell's guide across fo
+  double Fs = 0.0;
+  for (int dv = 0; dv < 2; ++dv)
+    for (int du = 0; du < 2; ++du) {
+      int c[3];
+      c[ta] = 2 * (a & 7) + du;
+      c[tb] = 2 * (b & 7) + dv;
+      c[axis] = plus ? 0 : 15;
+      const long m = IDX(G, c[0] + 1, c[1] + 1, c[2] + 1);
+      c[axis] += gstep;
+      const long gm = IDX(G, c[0] + 1, c[1] + 1, c[2] + 1);
+      const double* xf = O.F(fx, fb);
+      Fs = Fs + O.F(coef_of[fo], fb)[m] * (xf[m] - xf[gm]);
+    }
+  F = 0.125 * Fs;
+  int c[3];
+  c[ta] = a;
+  c[tb] = b;
+  c[axis] = plus ? 15 : 0;
+  const long m = IDX(G, c[0] + 1, c[1] + 1, c[2] + 1);
+  c[axis] += plus ? 1 : -1;
+  const long gm = IDX(G, c[0] + 1, c[1] + 1, c[2] + 1);
+  const double* x = O.F(fx, bi);
+  delta = F - O.F(coef_of[f], bi)[m] * (x[gm] - x[m]);
+}
+
+// y +/- delta (sign > 0: A x + delta; sign < 0: b - A x - delta) on every
+// coarse cell at a face with finer neighbours, faces in order 0..5.
+void cf_apply(Oracle& O, int fy, int fx, int sign) {
+  const Grid& G = O.G;
+  for (int bi = 0; bi < G.nb; ++bi)
+    for (int f = 0; f < 6; ++f) {
+      if (G.blocks[bi].kind[f] != NB_FINE) continue;
+      const int axis = f >> 1, ta = (axis == 0) ? 1 : 0, tb = (axis == 2) ? 1 : 2;
+      for (int b = 0; b < 16; ++b)
+        for (int a = 0; a < 16; ++a) {
+          double d, F;
+          cf_cell(O, fx, bi, f, a, b, d, F);
+          int c[3];
+          c[ta] = a;
+          c[tb] = b;
+          c[axis] = (f & 1) ? 15 : 0;
+          double& y = O.F(fy, bi)[IDX(G, c[0] + 1, c[1] + 1, c[2] + 1)];
+          y = sign > 0 ? y + d : y - d;
+        }
+    }
+}
+
 }  // namespace
 
+// y = y + delta (sign > 0) or y - delta (sign < 0) of field fx on every
+// coarse cell at a face with finer neighbours (the flux-conserving operator
+// applied after orc_calc_ax / orc_calc_r).
+void orc_cf_apply(Oracle* O, int fy, int fx, int sign) { cf_apply(*O, fy, fx, sign); }
+
+// Per coarse cell at a face with finer neighbours, in (block, face,
+// position a + 16 b) order: (delta, F) of field fx into out[2 * n] (when
+// out and capacity allow); returns the number of such cells.
+long orc_cf_cells(Oracle* O, int fx, double* out, long capacity) {
+  const Grid& G = O->G;
+  long n = 0;
+  for (int bi = 0; bi < G.nb; ++bi)
+    for (int f = 0; f < 6; ++f) {
+      if (G.blocks[bi].kind[f] != NB_FINE) continue;
+      for (int p = 0; p < 256; ++p, ++n) {
+        double d, F;
+        cf_cell(*O, fx, bi, f, p & 15, p >> 4, d, F);
+        if (out && n < capacity) {
+          out[2 * n] = d;
+          out[2 * n + 1] = F;
+        }
+      }
+    }
+  return n;
+}
+
 int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double epsilon,
-              double restart_drop, double restart_growth, int restart_every, int* count,
-              double* residual, double* hist) {
+              double restart_drop, double restart_growth, int restart_every, int cf,
+              int data64, int* count, double* residual, double* hist) {
   Oracle& R = *O;
   if (countMax <= 0) {
     *count = 1;
@@ -1388,9 +1488,10 @@ int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double
     return 0;
   }
   Coef32 C;
-  mixed_coef(R, C);
+  mixed_coef(R, C, data64 != 0);
   const float om = (float)omega;
   CalcR(R, OF_R, OF_X, OF_B);
+  if (cf) cf_apply(R, OF_R, OF_X, -1);
   COPY(R, OF_R0, OF_R);
   double rr0 = 1.0, alpha = 0.0, gamma = 1.0;
   // restarts: when the residual has dropped by restart_drop since the last
@@ -1418,15 +1519,17 @@ int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double
       AXPY(R, OF_P, OF_Q_, -gamma);
       XPAY(R, OF_P, OF_R, beta);
     }
-    mixed_precondition(R, C, OF_P, OF_P_, om, sweeps, per);
+    mixed_precondition(R, C, OF_P, OF_P_, om, sweeps, per, data64 != 0);
     impose_bc_p(R, OF_P_);
     CalcAx(R, OF_Q_, OF_P_);
+    if (cf) cf_apply(R, OF_Q_, OF_P_, 1);
     double q_r0 = DOT(R, OF_Q_, OF_R0);
     alpha = rr1 / q_r0;
     AXPYZ(R, OF_S, OF_Q_, OF_R, -alpha);
-    mixed_precondition(R, C, OF_S, OF_S_, om, sweeps, per);
+    mixed_precondition(R, C, OF_S, OF_S_, om, sweeps, per, data64 != 0);
     impose_bc_p(R, OF_S_);
     CalcAx(R, OF_T_, OF_S_);
+    if (cf) cf_apply(R, OF_T_, OF_S_, 1);
     double t_s = DOT(R, OF_T_, OF_S);
     double t_t_ = DOT(R, OF_T_, OF_T_);
     gamma = t_s / t_t_;

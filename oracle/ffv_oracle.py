@@ -70,7 +70,11 @@ def lib():
         L.orc_projection.restype = None
         L.orc_rbgs_fixed_average.argtypes = [vp, dbl, ctypes.c_long, i32, dbl, vp, vp, vp]
         L.orc_bicgstab_restart.argtypes = [vp, dbl, i32, i32, dbl, dbl, vp, vp, vp]
-        L.orc_mixed.argtypes = [vp, dbl, i32, i32, i32, dbl, dbl, dbl, i32, vp, vp, vp]
+        L.orc_mixed.argtypes = [vp, dbl, i32, i32, i32, dbl, dbl, dbl, i32, i32, i32, vp, vp, vp]
+        L.orc_cf_apply.argtypes = [vp, i32, i32, i32]
+        L.orc_cf_apply.restype = None
+        L.orc_cf_cells.restype = ctypes.c_long
+        L.orc_cf_cells.argtypes = [vp, i32, vp, ctypes.c_long]
         # the host sphere-grid generator compiled into this library
         L.ffvgpu_sphere_grid_create.argtypes = [ctypes.POINTER(_SphereParams),
                                                 ctypes.POINTER(vp)]
@@ -139,6 +143,18 @@ class SphereGrid:
     @property
     def cells(self):
         return self.nb * 4096
+
+    def fill_u(self, seed=0, sigma=0.01, vc=2):
+        """Only u* = (1,0,0) + N(0, sigma^2) in the reference layout (guides 0)."""
+        w = 16 + 2 * vc
+        shape = (self.nb, w, w, w)
+        out = {k: np.zeros(shape, np.float64) for k in ("UX", "UY", "UZ")}
+        st = lib().ffvgpu_sphere_grid_fill(self._h, seed, sigma, vc, out["UX"].ctypes.data,
+                                           out["UY"].ctypes.data, out["UZ"].ctypes.data,
+                                           None, None, None)
+        if st != 0:
+            raise ValueError("sphere_grid_fill failed")
+        return out
 
     def fill(self, seed=0, sigma=0.01, vc=2):
         """Per-cell inputs in the reference layout: dict of numpy arrays."""
@@ -295,12 +311,32 @@ class Oracle:
                                           float(epsilon)), count_max)
 
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
-                    epsilon=1e-8, restart_drop=1e-3, restart_growth=100.0, restart_every=0):
-        """Mixed-precision form: BiCGSTAB with RB-SOR preconditioning on 32-bit data."""
+                    epsilon=1e-8, restart_drop=1e-3, restart_growth=100.0, restart_every=0,
+                    flux_correction=False, fp64_data=False):
+        """Mixed-precision form: BiCGSTAB with RB-SOR preconditioning on 32-bit data;
+        flux_correction: the FP64 residual and A*x use the coarse-fine
+        flux-conserving operator; fp64_data: the same preconditioner on FP64 data."""
         return self._solve(lib().orc_mixed, (float(omega), int(sweeps), int(sweeps_per_exchange),
                                              int(count_max), float(epsilon), float(restart_drop),
-                                             float(restart_growth), int(restart_every)),
+                                             float(restart_growth), int(restart_every),
+                                             int(bool(flux_correction)), int(bool(fp64_data))),
                            count_max)
+
+    def calc_ax(self, out, x, flux_correction=False):
+        """out = A x (CalcAx, FFVILS.h:164-202), with flux_correction the
+        coarse-fine flux-conserving operator; x's guide cells as held."""
+        lib().orc_calc_ax(self._h, F[out], F[x])
+        if flux_correction:
+            lib().orc_cf_apply(self._h, F[out], F[x], 1)
+
+    def cf_cells(self, name="X"):
+        """Per coarse cell at a face with finer neighbours, in (block, face,
+        position) order: array [n][2] of (delta, F) of the field as it is held
+        (guide cells included)."""
+        n = lib().orc_cf_cells(self._h, F[name], None, 0)
+        out = np.zeros((max(n, 1), 2), np.float64)
+        lib().orc_cf_cells(self._h, F[name], out.ctypes.data, n)
+        return out[:n]
 
     def solve_bicgstab(self, omega=1.0, pre_count=2, count_max=1000, epsilon=1e-10,
                        restart_drop=0.0):
@@ -313,6 +349,30 @@ class Oracle:
     def _solve_plain_bicgstab(self, omega, pre_count, count_max, epsilon):
         return self._solve(lib().orc_bicgstab, (float(omega), int(pre_count), int(count_max),
                                                 float(epsilon)), count_max)
+
+
+def time_step(O, u_star, solve, rhof=1.0, dt=0.002):
+    """The pressure part of one fractional step on the oracle, in
+    Solver::UpdateP / UpdateU's order (src/FFV/Solver.cpp:5294-5771): u* set
+    from u_star (dict UX, UY, UZ in the reference layout), P01 bcut_remove_p
+    with the previous pressure, P02 exchange of u, P03 bcut_calc_ab_p, P05 BC
+    folding, P06 solve(O) (x from the previous pressure), P07 exchange of p,
+    U01 bcut_corr_u, U02 exchange of u, U03 exchange of p.  Returns solve's
+    result."""
+    for k in ("UX", "UY", "UZ"):
+        O.field(k)[...] = u_star[k]
+    O.remove_p(rhof, dt)
+    for k in ("UX", "UY", "UZ"):
+        O.exchange(k, U_BC_TYPE, U_BC_VALUE[k])
+    O.assemble_p(rhof, dt)
+    O.fold_bc()
+    r = solve(O)
+    O.exchange("X", P_BC_TYPE, P_BC_VALUE)
+    O.corr_u(rhof, dt)
+    for k in ("UX", "UY", "UZ"):
+        O.exchange(k, U_BC_TYPE, U_BC_VALUE[k])
+    O.exchange("X", P_BC_TYPE, P_BC_VALUE)
+    return r
 
 
 def interior(a, vc=2):

@@ -40,6 +40,47 @@ def test_mixed_solve_bitwise_against_oracle(level, omega, sweeps, per, count):
     P.close()
 
 
+@pytest.mark.parametrize("level,omega,sweeps,per,count", [
+    (1, 1.5, 8, 4, 8),
+    (2, 1.2, 6, 2, 5),
+    (3, 1.5, 8, 4, 2),   # several blocks per CTA, uniform and non-uniform blocks
+])
+def test_fp64_data_variant_bitwise_against_oracle(level, omega, sweeps, per, count):
+    """The same preconditioner on FP64 data (coefficients unrounded, FP64
+    iterate between exchanges): bit for bit the oracle's restatement."""
+    g, inp, O = problem(level)
+    P = device_problem(g, inp)
+    P.fill("X", 0.0)
+    O.field("X")[...] = 0.0
+    ro = O.solve_mixed(omega, sweeps, per, count, 0.0, fp64_data=True)
+    rg = P.solve_mixed(omega, sweeps, per, count, 0.0, fp64_data=True)
+    assert rg["count"] == ro["count"] == count + 1
+    assert_bitwise(rg["history"], ro["history"], "residual history")
+    assert_bitwise(interior(P.download("X", VC)), interior(O.field("X")), "pressure")
+    # and it is a different computation from the 32-bit data form
+    P.fill("X", 0.0)
+    r32 = P.solve_mixed(omega, sweeps, per, count, 0.0)
+    assert not np.array_equal(r32["history"], rg["history"])
+    P.close()
+
+
+@pytest.mark.parametrize("threads,depth", [(128, 1), (512, 3), (256, 2)])
+def test_launch_settings_do_not_change_results(threads, depth):
+    """CTA size of the A*x and update kernels and the sweep kernel's staging
+    depth are tuning knobs only: the same bits as the defaults (the 512-lane
+    block tree and the 256-lane cross-block tree do not depend on them)."""
+    g, inp, O = problem(3)
+    P = device_problem(g, inp)
+    P.fill("X", 0.0)
+    ref = P.solve_mixed(1.5, 8, 4, 4, 0.0)
+    xr = interior(P.download("X", VC)).copy()
+    P.fill("X", 0.0)
+    r = P.solve_mixed(1.5, 8, 4, 4, 0.0, threads_per_block=threads, stage_depth=depth)
+    assert_bitwise(r["history"], ref["history"], "residual history")
+    assert_bitwise(interior(P.download("X", VC)), xr, "pressure")
+    P.close()
+
+
 def test_mixed_converges_and_matches_fp64_solution():
     g, inp, O = problem(2)
     P = device_problem(g, inp)
@@ -232,7 +273,12 @@ def test_autotuner_times_candidates_and_leaves_x_zero():
     ids = [B.admit_sphere(sphere(1, 3)), B.admit_sphere(sphere(1, 4, center=(3.0, 1.0, 0.0)))]
     space = [(1.5, 8, 4, 8), (1.2, 4, 4, 4), (1.5, 8, 8, 16)]
     recs, best = B.autotune(ids, space=space, count_max=400)
-    assert len(recs) == 3 and all(r["ms"] > 0 and r["max_count"] >= 1 for r in recs)
+    # stage 1: the three numerical settings; stage 2 (when one converged): the
+    # fastest of them at the eight other (threads per block, staging depth) pairs
+    assert len(recs) in (3, 11) and all(r["ms"] > 0 and r["max_count"] >= 1 for r in recs)
+    if len(recs) == 11:
+        assert {(r["threads_per_block"], r["stage_depth"]) for r in recs[3:]} == \
+            {(nt, dp) for nt in (128, 256, 512) for dp in (1, 2, 3)} - {(256, 1)}
     assert best == -1 or recs[best]["converged"]
     if best >= 0:
         assert recs[best]["ms"] == min(r["ms"] for r in recs if r["converged"])
@@ -242,7 +288,8 @@ def test_autotuner_times_candidates_and_leaves_x_zero():
     if best >= 0:
         r = recs[best]
         B.begin(ids[0], omega=r["omega"], sweeps=r["sweeps"],
-                sweeps_per_exchange=r["sweeps_per_exchange"], count_max=400)
+                sweeps_per_exchange=r["sweeps_per_exchange"], count_max=400,
+                threads_per_block=r["threads_per_block"], stage_depth=r["stage_depth"])
         for _ in range(400):
             B.advance(r["iterations_per_replay"])
             if ids[0] in B.poll():
