@@ -714,7 +714,8 @@ def run_batch(args):
     admit_s = time.perf_counter() - t0
     assert all(i is not None for i in ids)
 
-    setting = dict(MIXED, iterations_per_replay=8, threads_per_block=256, stage_depth=1)
+    setting = dict(MIXED, iterations_per_replay=8, threads_per_block=256, stage_depth=1,
+                   sweep_threads=512)
     tune = None
     if args.tune:
         # a sample spread over the instance sizes (every k-th by block count)
@@ -732,14 +733,15 @@ def run_batch(args):
                                  r["sweeps"] == MIXED["sweeps"] and
                                  r["sweeps_per_exchange"] == MIXED["sweeps_per_exchange"] and
                                  r["iterations_per_replay"] == 8 and
-                                 r["threads_per_block"] == 256 and r["stage_depth"] == 1), None)}
+                                 r["threads_per_block"] == 256 and r["stage_depth"] == 1 and
+                                 r["sweep_threads"] == 512), None)}
         if best >= 0:
             b = recs[best]
             setting = dict(omega=b["omega"], sweeps=b["sweeps"],
                            sweeps_per_exchange=b["sweeps_per_exchange"],
                            iterations_per_replay=b["iterations_per_replay"],
                            threads_per_block=b["threads_per_block"],
-                           stage_depth=b["stage_depth"])
+                           stage_depth=b["stage_depth"], sweep_threads=b["sweep_threads"])
 
     def batched():
         for i in ids:
@@ -747,7 +749,8 @@ def run_batch(args):
         return B.solve_mixed(setting["omega"], setting["sweeps"], setting["sweeps_per_exchange"],
                              5000, 1e-8, check_every=setting["iterations_per_replay"],
                              threads_per_block=setting["threads_per_block"],
-                             stage_depth=setting["stage_depth"])
+                             stage_depth=setting["stage_depth"],
+                             sweep_threads=setting["sweep_threads"])
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         for _ in range(max(1, args.warmup)):
@@ -768,7 +771,8 @@ def run_batch(args):
     r64, t64b = timed(stream, lambda: B.solve_mixed(
         setting["omega"], setting["sweeps"], setting["sweeps_per_exchange"], 5000, 1e-8,
         check_every=setting["iterations_per_replay"], fp64_data=True,
-        threads_per_block=setting["threads_per_block"], stage_depth=setting["stage_depth"]))
+        threads_per_block=setting["threads_per_block"], stage_depth=setting["stage_depth"],
+        sweep_threads=setting["sweep_threads"]))
     res64 = [B.result(i) for i in ids]
     rbsor64 = {"solves_per_s": 1e3 * len(ids) / t64b, "ms": t64b,
                "iterations_min_max": [int(min(x["count"] for x in res64)),

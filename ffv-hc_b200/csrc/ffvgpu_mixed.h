@@ -30,19 +30,20 @@ struct MixCtx {
   int stall;           // test hook: the sweep issues no copy, so its first wait runs out
   int cf;              // coarse-fine flux correction in the FP64 residual and A*x
   int depth;           // sweep kernel: L2 prefetch distance in blocks (staging depth, >= 1)
+  int sweep_threads;   // sweep kernel: 512 (a row per thread) or 256 (two rows per thread)
 };
 
 // CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel,
 // with 'threads' (128, 256 or 512) per CTA of the A*x and update kernels.
 void mx_grid_sizes(int threads, int* sweep, int* matvec, int* update, int* guides);
 // Sweep coefficients of blocks [first, first + count), MIXED_COEF_WORDS per
-// block: 32-bit words [blk][7][8][512] (FP64 high words, rounded) into coef,
-// or with d64 (the FP64-data variant) the FP64 values [blk][7][8][512] into
-// coef64.  Also writes each block's ucoef record and adds the instance's
+// block, in the thread order of a sweep kernel of sweep_threads threads:
+// 32-bit words (FP64 high words, rounded) into coef, or with d64 (the
+// FP64-data variant) the FP64 values into coef64.  Also writes each block's ucoef record and adds the instance's
 // uniform blocks to st->ublocks.
-constexpr int MIXED_COEF_WORDS = 7 * 8 * 512;
+constexpr int MIXED_COEF_WORDS = 7 * 4096;
 void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint32_t* coef,
-                    double* coef64, double* ucoef, SolveState* st, bool d64);
+                    double* coef64, double* ucoef, SolveState* st, bool d64, int sweep_threads);
 void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
                     const double* gx, const double* A, const double* b, double* r, double* r0);
 // The iteration launchers take 'count' = CTAs of the persistent grid.  The

@@ -177,6 +177,7 @@ MixCtx mix_ctx(const ffvgpu_pool* P) {
   C.stall = P->stall_sweep;
   C.cf = P->m_cf;
   C.depth = P->m_depth;
+  C.sweep_threads = P->m_sweep_threads;
   return C;
 }
 
@@ -193,6 +194,9 @@ int stage_depth_of(const ffvgpu_mixed_params* prm) {
 int threads_of(const ffvgpu_mixed_params* prm) {
   return prm->threads_per_block > 0 ? prm->threads_per_block : 256;
 }
+int sweep_threads_of(const ffvgpu_mixed_params* prm) {
+  return prm->sweep_threads > 0 ? prm->sweep_threads : 512;
+}
 
 ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
   if (!prm) return bad("null parameters");
@@ -208,6 +212,8 @@ ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
   if (prm->restart_every < 0) return bad("restart_every must not be negative");
   if (prm->count_max < 0) return bad("count_max must not be negative");
   if (prm->stage_depth < 0 || prm->stage_depth > 3) return bad("stage_depth must lie in 0..3");
+  if (prm->sweep_threads != 0 && prm->sweep_threads != 256 && prm->sweep_threads != 512)
+    return bad("sweep_threads must be 0, 256 or 512");
   if (prm->threads_per_block != 0 && prm->threads_per_block != 128 &&
       prm->threads_per_block != 256 && prm->threads_per_block != 512)
     return bad("threads_per_block must be 0, 128, 256 or 512");
@@ -687,7 +693,8 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
                  prm->sweeps_per_exchange != P->m_per_exchange ||
                  (prm->flux_correction != 0) != (P->m_cf != 0) ||
                  (prm->fp64_data != 0) != (P->m_d64 != 0) ||
-                 stage_depth_of(prm) != P->m_depth || threads_of(prm) != P->m_threads))
+                 stage_depth_of(prm) != P->m_depth || threads_of(prm) != P->m_threads ||
+                 sweep_threads_of(prm) != P->m_sweep_threads))
     return bad("running instances use other preconditioner settings");
   double *xp, *g;
   size_t stride;
@@ -702,6 +709,7 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
   P->m_d64 = prm->fp64_data != 0;
   P->m_depth = stage_depth_of(prm);
   P->m_threads = threads_of(prm);
+  P->m_sweep_threads = sweep_threads_of(prm);
   if (P->grid_threads != P->m_threads) {  // the persistent grids of this CTA size
     mx_grid_sizes(P->m_threads, &P->grid_sweep, &P->grid_matvec, &P->grid_update,
                   &P->grid_guides);
@@ -730,7 +738,7 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
   I->ublocks = 0;
   CK(cudaMemcpyAsync(P->mst + inst, &h, sizeof(h), cudaMemcpyHostToDevice, P->stream));
   launch_mx_pack(P->stream, I->first, I->count, P->A, P->mcoef, P->mcoef64, P->mucoef,
-                 P->mst + inst, P->m_d64 != 0);
+                 P->mst + inst, P->m_d64 != 0, P->m_sweep_threads);
   MixCtx C = mix_ctx(P);
   C.first = I->first;
   launch_mx_init(P->stream, C, I->count, P->x[P->xcur], P->gx, P->A, P->b, P->r, P->r0);
@@ -759,7 +767,8 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
       P->mgraph_sweeps != P->m_sweeps || P->mgraph_per != P->m_per_exchange ||
       P->mgraph_wait_ns != P->wait_ns || P->mgraph_stall != P->stall_sweep ||
       P->mgraph_cf != P->m_cf || P->mgraph_d64 != P->m_d64 ||
-      P->mgraph_depth != P->m_depth || P->mgraph_threads != P->m_threads) {
+      P->mgraph_depth != P->m_depth || P->mgraph_threads != P->m_threads ||
+      P->mgraph_sweep_threads != P->m_sweep_threads) {
     if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
     P->mgraph = nullptr;
     cudaGraph_t graph;
@@ -779,6 +788,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
     P->mgraph_d64 = P->m_d64;
     P->mgraph_depth = P->m_depth;
     P->mgraph_threads = P->m_threads;
+    P->mgraph_sweep_threads = P->m_sweep_threads;
   }
   CK(cudaGraphLaunch(P->mgraph, P->stream));
   P->m_launches += (int64_t)iterations * launches_per_iteration(P);
@@ -959,6 +969,7 @@ ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* P, const int32_t* instances, in
     prm.sweeps_per_exchange = R.sweeps_per_exchange;
     prm.threads_per_block = R.threads_per_block;
     prm.stage_depth = R.stage_depth;
+    prm.sweep_threads = R.sweep_threads;
     prm.history = nullptr;
     R.ms = 0.0;
     R.max_count = 0;

@@ -50,7 +50,7 @@ namespace ffvgpu {
 namespace {
 
 constexpr int MT = 256;  // FP64 kernels: 16 cells per thread
-constexpr int PT = 512;  // sweep kernel: 8 cells per thread
+constexpr int PT = 512;  // sweep kernel, default: 8 cells per thread (256 threads: 16)
 
 // Shared-memory tile of the sweep kernel: per colour a padded
 // [k + 1][j + 1][ii] array of FP64 iterate values, k, j in -1..16 and
@@ -61,21 +61,35 @@ constexpr int PT = 512;  // sweep kernel: 8 cells per thread
 // doubles) fall into disjoint banks.
 constexpr int SP = 10, SQ = 190, SH = 18 * SQ;
 constexpr int TILE = 2 * SH;
-constexpr int COEF_WORDS = 7 * 8 * PT;  // coefficient words of one block
+constexpr int COEF_WORDS = 7 * BLOCK_CELLS;  // coefficient words of one block
 constexpr int GUIDES = 6 * FACE_CELLS;  // guide values of one block (FP64)
-constexpr int SWEEP_SMEM = COEF_WORDS * 4 + TILE * 8 + 8 * PT * 8 + GUIDES * 8 + 16;
+constexpr int SWEEP_SMEM = COEF_WORDS * 4 + TILE * 8 + BLOCK_CELLS * 8 + GUIDES * 8 + 16;
 
+// Sweep-kernel geometry for PTS threads per CTA (512 or 256).  Thread t owns
+// the cells (i, j, k) with i in {2 ih, 2 ih + 1}, j = JJ jp + jj (jj < JJ
+// rows), k = 4 kg + h (h < 4), both colours: ih = t & 7, kg = (t >> 3) & 3,
+// jp = t >> 5.  Its cell m < CPT is (colour c, row jj, plane h) with
+// m = (c JJ + jj) 4 + h.
+template <int PTS>
+struct SweepGeom {
+  static constexpr int JJ = 512 / PTS;  // rows per thread
+  static constexpr int CPT = 8 * JJ;    // cells per thread
+};
 // Word of coefficient a of sweep thread t's cell m within a block.
+template <int PTS>
 __device__ __forceinline__ int coef_word(int a, int m, int t) {
-  return ((a * 2 + (m >> 2)) * PT + t) * 4 + (m & 3);
+  return ((a * (SweepGeom<PTS>::CPT / 4) + (m >> 2)) * PTS + t) * 4 + (m & 3);
 }
 __device__ __forceinline__ int tile_at(int i, int j, int k) {
   return (k + 1) * SQ + (j + 1) * SP + ((i + 2) >> 1);
 }
-// Storage slot of sweep thread t's cell m (colour m >> 2, z plane 4 kg + (m & 3)).
+// Storage slot of sweep thread t's cell m.
+template <int PTS>
 __host__ __device__ __forceinline__ int sweep_cell(int t, int m) {
-  const int ih = t & 7, kg = (t >> 3) & 3, j = t >> 5, c = m >> 2, h = m & 3;
-  return c * HALF_CELLS + ((4 * kg + h) * 16 + j) * 8 + ih;
+  constexpr int JJ = SweepGeom<PTS>::JJ;
+  const int ih = t & 7, kg = (t >> 3) & 3, jp = t >> 5;
+  const int h = m & 3, jj = (m >> 2) % JJ, c = (m >> 2) / JJ;
+  return c * HALF_CELLS + ((4 * kg + h) * 16 + JJ * jp + jj) * 8 + ih;
 }
 
 __device__ __forceinline__ int active_instance(const MixCtx& C, int blk) {
@@ -299,26 +313,27 @@ __device__ __forceinline__ double widen_here(uint32_t w) {
 
 // D64 (the FP64-data variant): coef64 [blk][a][m][t] holds the FP64 values
 // themselves (dinv = 1 / Ap in FP64), read at use by the sweep kernel.
-template <bool D64>
+template <bool D64, int PTS>
 __global__ void __launch_bounds__(MT)
 mx_pack_kernel(int first, const double* __restrict__ A, uint32_t* __restrict__ coef,
                double* __restrict__ coef64, double* __restrict__ ucoef, SolveState* st) {
+  constexpr int CPT = SweepGeom<PTS>::CPT;
   const int blk = first + blockIdx.x;
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
   uint32_t* cb = D64 ? nullptr : coef + (size_t)blk * COEF_WORDS;
   double* cd = D64 ? coef64 + (size_t)blk * COEF_WORDS : nullptr;
-  for (int w = threadIdx.x; w < 8 * PT; w += MT) {
-    const int m = w / PT, t = w % PT;
-    const int s = sweep_cell(t, m);
+  for (int w = threadIdx.x; w < BLOCK_CELLS; w += MT) {
+    const int m = w / PTS, t = w % PTS;
+    const int s = sweep_cell<PTS>(t, m);
     if (D64) {
 #pragma unroll
-      for (int a = 0; a < 6; ++a) cd[(a * 8 + m) * PT + t] = Ab[(1 + a) * BLOCK_CELLS + s];
-      cd[(6 * 8 + m) * PT + t] = 1.0 / Ab[s];
+      for (int a = 0; a < 6; ++a) cd[(a * CPT + m) * PTS + t] = Ab[(1 + a) * BLOCK_CELLS + s];
+      cd[(6 * CPT + m) * PTS + t] = 1.0 / Ab[s];
     } else {
 #pragma unroll
       for (int a = 0; a < 6; ++a)
-        cb[coef_word(a, m, t)] = hi_round(Ab[(1 + a) * BLOCK_CELLS + s]);
-      cb[coef_word(6, m, t)] = hi_round(1.0 / Ab[s]);
+        cb[coef_word<PTS>(a, m, t)] = hi_round(Ab[(1 + a) * BLOCK_CELLS + s]);
+      cb[coef_word<PTS>(6, m, t)] = hi_round(1.0 / Ab[s]);
     }
   }
   // uniform block: all seven coefficients bitwise equal to cell 0's everywhere
@@ -415,68 +430,105 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
 // thread).  For one data format the values, and so the results, do not
 // depend on the source.
 enum { CS_UNI = 0, CS_W32 = 1, CS_G64 = 2 };
-template <int CS>
+// PTS threads: the cells m = (c JJ + jj) 4 + h of a thread (SweepGeom).  Of a
+// cell's six neighbours (all of the other colour) the x neighbour at the same
+// ih, the z neighbours inside the 4-cell column and, with two rows per thread
+// (PTS 256), the y neighbour in the thread's other row are its own registers;
+// the rest come from the tile.  The terms keep rbgs_smoother's order (w, e,
+// s, n, b, t) whatever their source, so every PTS gives the same bits.
+template <int CS, int PTS>
 __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, int p0,
-                                           double (&E)[2][4], const uint32_t (&cw)[8][7],
+                                           double (&E)[2][SweepGeom<PTS>::JJ][4],
+                                           const uint32_t (&cw)[SweepGeom<PTS>::CPT][7],
                                            const double (&ku)[7],
                                            const double* __restrict__ c64, double mom,
                                            int nsweep) {
   constexpr bool UNI = CS == CS_UNI;
+  constexpr int JJ = SweepGeom<PTS>::JJ, CPT = SweepGeom<PTS>::CPT;
 #define MX_COEF(m, a)                                          \
   (CS == CS_UNI ? ku[a]                                        \
    : CS == CS_W32 ? widen_here(cw[m][a])                       \
-                  : __ldg(c64 + ((a) * 8 + (m)) * PT))
+                  : __ldg(c64 + ((a) * CPT + (m)) * PTS))
   // a uniform block has the registers to keep its right-hand side too (one
   // shared-memory read less per update)
-  double vr[2][4];
+  double vr[2][JJ][4];
 #pragma unroll
   for (int c = 0; c < 2; ++c)
 #pragma unroll
-    for (int h = 0; h < 4; ++h) vr[c][h] = UNI ? V[(4 * c + h) * PT] : 0.0;
+    for (int jj = 0; jj < JJ; ++jj)
+#pragma unroll
+      for (int h = 0; h < 4; ++h) vr[c][jj][h] = UNI ? V[((c * JJ + jj) * 4 + h) * PTS] : 0.0;
 #pragma unroll 1
   for (int it = 0; it < nsweep; ++it) {
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-      // the four cells of this colour advance term by term, so their
-      // dependent FP64 chains overlap (each chain keeps its own order)
-      const double* O = T + o0 + (1 - c) * SH;  // cell h: O + h SQ, same (ih, j, k), other colour
-      double rc[4], xo[4];
+      // the cells of this colour advance term by term, so their dependent
+      // FP64 chains overlap (each chain keeps its own order)
+      const double* O = T + o0 + (1 - c) * SH;  // cell (jj, h): O + jj SP + h SQ, other colour
+      double rc[JJ][4], xo[JJ][4];
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const int par = p0 ^ ((h + c) & 1);  // x parity of the cell: i = 2 ih + par
-        // the x neighbour at the same ih is this thread's own; the other one
-        // is east (par 1) or west (par 0) of it in the tile
-        xo[h] = O[h * SQ + (par ? 1 : -1)];
-        rc[h] = UNI ? vr[c][h] : V[(4 * c + h) * PT];
-      }
+      for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const int par = p0 ^ ((h + c) & 1);
-        rc[h] = __fma_rn(-MX_COEF(4 * c + h, 0), par ? E[1 - c][h] : xo[h], rc[h]);
-      }
+        for (int h = 0; h < 4; ++h) {
+          const int par = p0 ^ ((jj + h + c) & 1);  // x parity of the cell: i = 2 ih + par
+          // the x neighbour at the same ih is this thread's own; the other one
+          // is east (par 1) or west (par 0) of it in the tile
+          xo[jj][h] = O[jj * SP + h * SQ + (par ? 1 : -1)];
+          rc[jj][h] = UNI ? vr[c][jj][h] : V[((c * JJ + jj) * 4 + h) * PTS];
+        }
+#define MX_M(jj, h) ((c * JJ + (jj)) * 4 + (h))
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const int par = p0 ^ ((h + c) & 1);
-        rc[h] = __fma_rn(-MX_COEF(4 * c + h, 1), par ? xo[h] : E[1 - c][h], rc[h]);
-      }
+      for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
-      for (int h = 0; h < 4; ++h) rc[h] = __fma_rn(-MX_COEF(4 * c + h, 2), O[h * SQ - SP], rc[h]);
+        for (int h = 0; h < 4; ++h) {
+          const int par = p0 ^ ((jj + h + c) & 1);
+          rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 0), par ? E[1 - c][jj][h] : xo[jj][h],
+                               rc[jj][h]);
+        }
 #pragma unroll
-      for (int h = 0; h < 4; ++h) rc[h] = __fma_rn(-MX_COEF(4 * c + h, 3), O[h * SQ + SP], rc[h]);
+      for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
-      for (int h = 0; h < 4; ++h)
-        rc[h] = __fma_rn(-MX_COEF(4 * c + h, 4), h > 0 ? E[1 - c][h - 1] : O[-SQ], rc[h]);
+        for (int h = 0; h < 4; ++h) {
+          const int par = p0 ^ ((jj + h + c) & 1);
+          rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 1), par ? xo[jj][h] : E[1 - c][jj][h],
+                               rc[jj][h]);
+        }
 #pragma unroll
-      for (int h = 0; h < 4; ++h)
-        rc[h] = __fma_rn(-MX_COEF(4 * c + h, 5), h < 3 ? E[1 - c][h + 1] : O[4 * SQ], rc[h]);
+      for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const double xt = __dmul_rn(rc[h], MX_COEF(4 * c + h, 6));
-        const double e = E[c][h];
-        const double en = __fma_rn(mom, __dsub_rn(e, xt), e);
-        E[c][h] = en;
-        T[o0 + c * SH + h * SQ] = en;
-      }
+        for (int h = 0; h < 4; ++h)
+          rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 2),
+                               jj > 0 ? E[1 - c][jj - 1][h] : O[jj * SP + h * SQ - SP], rc[jj][h]);
+#pragma unroll
+      for (int jj = 0; jj < JJ; ++jj)
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+          rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 3),
+                               jj < JJ - 1 ? E[1 - c][jj + 1][h] : O[jj * SP + h * SQ + SP],
+                               rc[jj][h]);
+#pragma unroll
+      for (int jj = 0; jj < JJ; ++jj)
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+          rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 4),
+                               h > 0 ? E[1 - c][jj][h - 1] : O[jj * SP - SQ], rc[jj][h]);
+#pragma unroll
+      for (int jj = 0; jj < JJ; ++jj)
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+          rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 5),
+                               h < 3 ? E[1 - c][jj][h + 1] : O[jj * SP + 4 * SQ], rc[jj][h]);
+#pragma unroll
+      for (int jj = 0; jj < JJ; ++jj)
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const double xt = __dmul_rn(rc[jj][h], MX_COEF(MX_M(jj, h), 6));
+          const double e = E[c][jj][h];
+          const double en = __fma_rn(mom, __dsub_rn(e, xt), e);
+          E[c][jj][h] = en;
+          T[o0 + c * SH + jj * SP + h * SQ] = en;
+        }
+#undef MX_M
       __syncthreads();
     }
   }
@@ -506,13 +558,13 @@ constexpr int LF_INST = LF_COPY - 1;
 // Called by every thread: fills list[0, *n) from the candidates from, from +
 // gridDim.x, ... (LIST_CAP of them, in item order) and sets *next to the
 // first candidate after them.
-template <int MODE, bool FIRST>
+template <int MODE, bool FIRST, int PTS>
 __device__ void build_live_list(const MixCtx& C, int from, int n_act, int2* list, int* n,
                                 int* next, int* wcount) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int base = 0;
-  for (int r = 0; r < LIST_CAP / PT; ++r) {
-    const int it = from + (r * PT + tid) * gridDim.x;
+  for (int r = 0; r < LIST_CAP / PTS; ++r) {
+    const int it = from + (r * PTS + tid) * gridDim.x;
     int b = -1, e = 0;
     bool live = false;
     if (it < n_act) {
@@ -532,7 +584,7 @@ __device__ void build_live_list(const MixCtx& C, int from, int n_act, int2* list
     for (int w = 0; w < warp; ++w) off += wcount[w];
     if (live) list[off + __popc(m & ((1u << lane) - 1u))] = make_int2(b, e);
     int tot = 0;
-    for (int w = 0; w < PT / 32; ++w) tot += wcount[w];
+    for (int w = 0; w < PTS / 32; ++w) tot += wcount[w];
     base += tot;
     __syncthreads();  // wcount is refilled by the next round
   }
@@ -545,22 +597,23 @@ __device__ void build_live_list(const MixCtx& C, int from, int n_act, int2* list
 
 // ET: the iterate between passes, float (the mixed form) or double (the
 // FP64-data variant, whose coefficients are FP64 too and read at use).
-template <int MODE, bool FIRST, typename ET>
-__global__ void __launch_bounds__(PT, 1)
+template <int MODE, bool FIRST, typename ET, int PTS>
+__global__ void __launch_bounds__(PTS, 1)
 mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
                 double* __restrict__ r0, double* __restrict__ pv, const double* __restrict__ q,
                 const uint32_t* __restrict__ coef, const double* __restrict__ coef64,
                 const ET* __restrict__ ein, const double* __restrict__ guides,
                 ET* __restrict__ eout, int depth) {
   constexpr bool D64 = sizeof(ET) == 8;
+  constexpr int JJ = SweepGeom<PTS>::JJ, CPT = SweepGeom<PTS>::CPT;
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t* slot = reinterpret_cast<uint32_t*>(smem);
   double* T = reinterpret_cast<double*>(smem + COEF_WORDS * 4);
   double* V = reinterpret_cast<double*>(smem + COEF_WORDS * 4 + TILE * 8);  // [m][t] rhs
-  double* GB = V + 8 * PT;  // [face][p] guides of the block, copied with its coefficients
+  double* GB = V + BLOCK_CELLS;  // [face][p] guides of the block, copied with its coefficients
   uint64_t* bar = reinterpret_cast<uint64_t*>(GB + GUIDES);
   __shared__ int2 s_list[LIST_CAP];
-  __shared__ int s_nlist, s_next_from, s_wcount[PT / 32];
+  __shared__ int s_nlist, s_next_from, s_wcount[PTS / 32];
   __shared__ int abort_flag;
   __shared__ int s_copied[2];  // a copy was issued on the barrier for this parity
   // a uniform block's coefficient record (MixCtx::ucoef), copied with the block
@@ -642,9 +695,9 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     }
   };
   const int tid = threadIdx.x;
-  const int ih = tid & 7, kg = (tid >> 3) & 3, j = tid >> 5;
-  const int o0 = (4 * kg + 1) * SQ + (j + 1) * SP + ih + 1;  // tile slot of cell (c 0, h 0)
-  const int s0 = sweep_cell(tid, 0);                          // its storage slot
+  const int ih = tid & 7, kg = (tid >> 3) & 3, j0 = JJ * (tid >> 5);
+  const int o0 = (4 * kg + 1) * SQ + (j0 + 1) * SP + ih + 1;  // tile slot of cell m = 0
+  const int s0 = sweep_cell<PTS>(tid, 0);                      // its storage slot
   const double mom = -(double)omega;
   const int n_act = *C.n_active;
   if (tid == 0) {
@@ -653,15 +706,16 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     abort_flag = 0;
   }
   if (FIRST)
-    for (int g = tid; g < TILE; g += PT) T[g] = 0.0;  // guides of e stay 0 in a first pass
+    for (int g = tid; g < TILE; g += PTS) T[g] = 0.0;  // guides of e stay 0 in a first pass
   // The CTA visits the live items blockIdx.x + n gridDim.x of the active
   // list (blocks of instances still solving), found a chunk at a time, and
   // issues each block's copy while the block before it sweeps, so blocks of
   // instances that have stopped cost neither a copy nor a wait.
-  build_live_list<MODE, FIRST>(C, blockIdx.x, n_act, s_list, &s_nlist, &s_next_from, s_wcount);
+  build_live_list<MODE, FIRST, PTS>(C, blockIdx.x, n_act, s_list, &s_nlist, &s_next_from,
+                                    s_wcount);
   while (s_nlist == 0 && s_next_from < n_act)  // a chunk with no live item
-    build_live_list<MODE, FIRST>(C, s_next_from, n_act, s_list, &s_nlist, &s_next_from,
-                                 s_wcount);
+    build_live_list<MODE, FIRST, PTS>(C, s_next_from, n_act, s_list, &s_nlist, &s_next_from,
+                                      s_wcount);
   if (tid == 0 && s_nlist > 0) {
     issue(s_list[0], 0);
     for (int k = 0; k < depth && k < s_nlist; ++k) prefetch(s_list[k]);
@@ -675,7 +729,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     const int blk = ent.x, inst = ent.y & LF_INST;
     const bool uni = ent.y & LF_UNI;
     const size_t base = (size_t)blk * BLOCK_CELLS + s0;
-    double E[2][4] = {};
+    double E[2][JJ][4] = {};
     // this block's copy (issued a block ago): coefficients and guides, or
     // for a uniform block its record, vectors or guides
     async::mbar_wait(bar, phase, &abort_flag, ROLE_SWEEP, C.wait_ns);
@@ -691,8 +745,10 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
 #pragma unroll
       for (int c = 0; c < 2; ++c)
 #pragma unroll
+        for (int jj = 0; jj < JJ; ++jj)
+#pragma unroll
         for (int h = 0; h < 4; ++h) {
-          const int sl = s0 + c * HALF_CELLS + h * 128;
+          const int sl = s0 + c * HALF_CELLS + jj * 8 + h * 128;
           const size_t s = gbase + sl;
           double rhs;
           if (MODE == 0) {
@@ -707,24 +763,26 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
             rhs = malpha * qs[sl] + rs[sl];
           }
           pv[s] = rhs;
-          V[(4 * c + h) * PT + tid] = rhs;
-          E[c][h] = 0.0;
-          T[o0 + c * SH + h * SQ] = 0.0;
+          V[((c * JJ + jj) * 4 + h) * PTS + tid] = rhs;
+          E[c][jj][h] = 0.0;
+          T[o0 + c * SH + jj * SP + h * SQ] = 0.0;
         }
     } else {
 #pragma unroll
       for (int c = 0; c < 2; ++c)
 #pragma unroll
+        for (int jj = 0; jj < JJ; ++jj)
+#pragma unroll
         for (int h = 0; h < 4; ++h) {
-          const size_t s = base + c * HALF_CELLS + h * 128;
-          V[(4 * c + h) * PT + tid] = pv[s];
-          E[c][h] = (double)__ldg(ein + s);
-          T[o0 + c * SH + h * SQ] = E[c][h];
+          const size_t s = base + c * HALF_CELLS + jj * 8 + h * 128;
+          V[((c * JJ + jj) * 4 + h) * PTS + tid] = pv[s];
+          E[c][jj][h] = (double)__ldg(ein + s);
+          T[o0 + c * SH + jj * SP + h * SQ] = E[c][jj][h];
         }
 #pragma unroll
-      for (int g = tid; g < GUIDES; g += PT) T[guide_slot(g >> 8, g & 255)] = GB[g];
+      for (int g = tid; g < GUIDES; g += PTS) T[guide_slot(g >> 8, g & 255)] = GB[g];
     }
-    uint32_t cw[8][7];
+    uint32_t cw[CPT][7];
     double ku[7];
     if (uni) {
       const double* U = s_urec[phase];
@@ -741,8 +799,8 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
 #pragma unroll
       for (int a = 0; a < 7; ++a)
 #pragma unroll
-        for (int hq = 0; hq < 2; ++hq) {
-          const uint4 w = reinterpret_cast<const uint4*>(slot)[(a * 2 + hq) * PT + tid];
+        for (int hq = 0; hq < CPT / 4; ++hq) {
+          const uint4 w = reinterpret_cast<const uint4*>(slot)[(a * (CPT / 4) + hq) * PTS + tid];
           cw[4 * hq + 0][a] = w.x;
           cw[4 * hq + 1][a] = w.y;
           cw[4 * hq + 2][a] = w.z;
@@ -778,8 +836,8 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     int npos = pos + 1;
     if (npos >= s_nlist && s_next_from < n_act) {
       do
-        build_live_list<MODE, FIRST>(C, s_next_from, n_act, s_list, &s_nlist, &s_next_from,
-                                     s_wcount);
+        build_live_list<MODE, FIRST, PTS>(C, s_next_from, n_act, s_list, &s_nlist,
+                                          &s_next_from, s_wcount);
       while (s_nlist == 0 && s_next_from < n_act);
       npos = 0;
     }
@@ -790,16 +848,18 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     pos = npos;
     const double* c64 = D64 ? coef64 + (size_t)blk * COEF_WORDS + tid : nullptr;
     if (uni)
-      run_sweeps<CS_UNI>(T, V + tid, o0, j & 1, E, cw, ku, c64, mom, nsweep);
+      run_sweeps<CS_UNI, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, mom, nsweep);
     else if constexpr (D64)
-      run_sweeps<CS_G64>(T, V + tid, o0, j & 1, E, cw, ku, c64, mom, nsweep);
+      run_sweeps<CS_G64, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, mom, nsweep);
     else
-      run_sweeps<CS_W32>(T, V + tid, o0, j & 1, E, cw, ku, c64, mom, nsweep);
+      run_sweeps<CS_W32, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, mom, nsweep);
 #pragma unroll
     for (int c = 0; c < 2; ++c)
 #pragma unroll
-      for (int h = 0; h < 4; ++h)
-        eout[base + c * HALF_CELLS + h * 128] = (ET)E[c][h];
+      for (int jj = 0; jj < JJ; ++jj)
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+          eout[base + c * HALF_CELLS + jj * 8 + h * 128] = (ET)E[c][jj][h];
   }
 }
 
@@ -985,11 +1045,15 @@ void launch_cf_mismatch(cudaStream_t s, int npairs, const double* x, const doubl
 // Launchers.
 // ---------------------------------------------------------------------------
 void launch_mx_pack(cudaStream_t s, int first, int count, const double* A, uint32_t* coef,
-                    double* coef64, double* ucoef, SolveState* st, bool d64) {
-  if (d64)
-    mx_pack_kernel<true><<<count, MT, 0, s>>>(first, A, coef, coef64, ucoef, st);
+                    double* coef64, double* ucoef, SolveState* st, bool d64, int sweep_threads) {
+  if (d64 && sweep_threads == 256)
+    mx_pack_kernel<true, 256><<<count, MT, 0, s>>>(first, A, coef, coef64, ucoef, st);
+  else if (d64)
+    mx_pack_kernel<true, 512><<<count, MT, 0, s>>>(first, A, coef, coef64, ucoef, st);
+  else if (sweep_threads == 256)
+    mx_pack_kernel<false, 256><<<count, MT, 0, s>>>(first, A, coef, coef64, ucoef, st);
   else
-    mx_pack_kernel<false><<<count, MT, 0, s>>>(first, A, coef, coef64, ucoef, st);
+    mx_pack_kernel<false, 512><<<count, MT, 0, s>>>(first, A, coef, coef64, ucoef, st);
 }
 void launch_mx_init(cudaStream_t s, const MixCtx& C, int count, const double* x,
                     const double* gx, const double* A, const double* b, double* r, double* r0) {
@@ -1001,9 +1065,14 @@ static void sweep_launch(cudaStream_t s, const MixCtx& C, int count, float omega
                          const double* r, double* r0, double* pv, const double* q,
                          const uint32_t* coef, const double* coef64, const void* ein,
                          const double* guides, void* eout) {
-  mx_sweep_kernel<MODE, FIRST, ET><<<count, PT, SWEEP_SMEM, s>>>(
-      C, omega, nsweep, r, r0, pv, q, coef, coef64, static_cast<const ET*>(ein), guides,
-      static_cast<ET*>(eout), C.depth);
+  if (C.sweep_threads == 256)
+    mx_sweep_kernel<MODE, FIRST, ET, 256><<<count, 256, SWEEP_SMEM, s>>>(
+        C, omega, nsweep, r, r0, pv, q, coef, coef64, static_cast<const ET*>(ein), guides,
+        static_cast<ET*>(eout), C.depth);
+  else
+    mx_sweep_kernel<MODE, FIRST, ET, 512><<<count, 512, SWEEP_SMEM, s>>>(
+        C, omega, nsweep, r, r0, pv, q, coef, coef64, static_cast<const ET*>(ein), guides,
+        static_cast<ET*>(eout), C.depth);
 }
 
 void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first,
@@ -1044,17 +1113,22 @@ void mx_grid_sizes(int threads, int* sweep, int* matvec, int* update, int* guide
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // the sweep kernels' shared memory, on the calling device (before any launch)
-  allow_sweep_smem(mx_sweep_kernel<0, true, float>);
-  allow_sweep_smem(mx_sweep_kernel<0, false, float>);
-  allow_sweep_smem(mx_sweep_kernel<1, true, float>);
-  allow_sweep_smem(mx_sweep_kernel<1, false, float>);
-  allow_sweep_smem(mx_sweep_kernel<0, true, double>);
-  allow_sweep_smem(mx_sweep_kernel<0, false, double>);
-  allow_sweep_smem(mx_sweep_kernel<1, true, double>);
-  allow_sweep_smem(mx_sweep_kernel<1, false, double>);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, float>, PT,
+#define MX_ALLOW(PTS)                                    \
+  allow_sweep_smem(mx_sweep_kernel<0, true, float, PTS>);  \
+  allow_sweep_smem(mx_sweep_kernel<0, false, float, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<1, true, float, PTS>);  \
+  allow_sweep_smem(mx_sweep_kernel<1, false, float, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<0, true, double, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<0, false, double, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<1, true, double, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<1, false, double, PTS>);
+  MX_ALLOW(512)
+  MX_ALLOW(256)
+#undef MX_ALLOW
+  // one CTA per SM for either thread count (its shared memory)
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, float, 512>, 512,
                                                 SWEEP_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, float>, PT,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, float, 256>, 256,
                                                 SWEEP_SMEM);
   if (threads == 128) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2, false, float, 128>,

@@ -154,6 +154,7 @@ struct ffvgpu_pool {
   int m_d64 = 0;  // the running solves use the FP64-data variant
   int m_depth = 1;  // sweep kernel staging depth (L2 prefetch distance in blocks)
   int m_threads = 256;  // CTA size of the A*x and update kernels
+  int m_sweep_threads = 512;  // CTA size of the sweep kernel
   cudaGraphExec_t mgraph = nullptr;
   int mgraph_iters = 0;
   double mgraph_omega = 0.0;
@@ -162,7 +163,7 @@ struct ffvgpu_pool {
   int mgraph_stall = 0;
   int mgraph_cf = 0;
   int mgraph_d64 = 0;
-  int mgraph_depth = 0, mgraph_threads = 0;
+  int mgraph_depth = 0, mgraph_threads = 0, mgraph_sweep_threads = 0;
   int stall_sweep = 0;  // test hook (ffvgpu_pool_stall_next_solve), cleared when a solve ends
   int64_t m_launches = 0;
   int64_t m_bytes = 0;

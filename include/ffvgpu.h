@@ -414,6 +414,9 @@ typedef struct {
                                   (0: 256); results do not depend on it */
   int32_t stage_depth;         /* sweep kernel: how many blocks ahead a block's data are
                                   brought into L2 (1..3; 0: 1); results do not depend on it */
+  int32_t sweep_threads;       /* CTA size of the sweep kernel: 512 (each thread a 4-cell
+                                  column of one row) or 256 (of two rows); 0: 512; results
+                                  do not depend on it */
 } ffvgpu_mixed_params;
 
 /* Solves every admitted instance of the pool (a pool made from one grid is
@@ -571,6 +574,7 @@ typedef struct {
   int32_t converged;  /* out: 1 when every instance reached epsilon */
   int32_t threads_per_block;  /* as ffvgpu_mixed_params (0: 256) */
   int32_t stage_depth;        /* as ffvgpu_mixed_params (0: 1) */
+  int32_t sweep_threads;      /* as ffvgpu_mixed_params (0: 512) */
 } ffvgpu_tune_record;
 
 ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* pool, const int32_t* instances,
