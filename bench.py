@@ -48,6 +48,9 @@ sys.path.insert(0, os.path.join(ROOT, "ffv-hc_b200"))
 
 CELLS_PER_BLOCK = 4096
 BYTES_PER_SWEEP_CELL = 80  # 7 coefficients + b + x read, x written (FP64)
+# the same for a uniform block, whose seven coefficients are one record: b + x
+# read, x written
+BYTES_PER_SWEEP_CELL_UNIFORM = 24
 
 
 def parse():
@@ -1002,7 +1005,12 @@ def main():
 
     # ---- roofline of the dominant kernel (fused residual + RB sweep) ---------
     avg_launch_ms = float(np.sum(sweep_ms) / max(1, np.sum(sweep_n)))
-    alg_bytes = BYTES_PER_SWEEP_CELL * cells
+    # bytes of one pass in the pool's format: per-cell coefficients for the
+    # blocks that need them, one record for the uniform ones
+    ublocks = int(r.get("uniform_blocks", 0))
+    alg_bytes = CELLS_PER_BLOCK * ((g.nb - ublocks) * BYTES_PER_SWEEP_CELL +
+                                   ublocks * BYTES_PER_SWEEP_CELL_UNIFORM)
+    ref_bytes = BYTES_PER_SWEEP_CELL * cells
     achieved = alg_bytes / (avg_launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic, traffic_src = profile_traffic(args.level, cells)
@@ -1010,6 +1018,11 @@ def main():
                 "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                 "kernel": "rbgs_pipelined_kernel<res,sweep> (fused residual + red-black sweep)",
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_launch_ms,
+                "uniform_blocks": ublocks,
+                "bytes_per_cell": f"{BYTES_PER_SWEEP_CELL} (per-cell coefficients), "
+                                  f"{BYTES_PER_SWEEP_CELL_UNIFORM} (uniform block)",
+                "reference_format_bytes_per_launch": ref_bytes,
+                "reference_format_gbs": ref_bytes / (avg_launch_ms * 1e-3) / 1e9,
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"}
 
     cpu = None

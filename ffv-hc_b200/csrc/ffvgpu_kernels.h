@@ -21,6 +21,9 @@ struct KCtx {
   int nb;
   int first;
   uint64_t wait_ns;    // limit of every bounded device wait (ffvgpu_pool_set_wait_limit)
+  // [blocks][8] uniform records of the sweep's coefficient stream
+  // (launch_pack_stream), or null: every block streams all its coefficients
+  const double* urec;
 };
 
 // Fused residual + red-black sweep over the coefficient stream (rbgs_pipelined.cu).
@@ -30,7 +33,11 @@ struct KCtx {
 void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const double* xin,
                  double* xout, const double* stream, const double* gst, double omega,
                  double* partials, SolveState* st, int fin, int iter, bool pdl = false);
-void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b, double* stream);
+// Packs A and b into the sweep's coefficient stream and writes each block's
+// uniform record urec[blk][8] (Ap..At of cell 0, then 1.0 when every cell has
+// those seven coefficients, else 0.0), adding the uniform blocks to *ucount.
+void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b, double* stream,
+                        double* urec, int32_t* ucount);
 void launch_jacobi(cudaStream_t s, const KCtx& C, bool from_zero, bool dot, const double* xin,
                    double* xout, const double* A, const double* b, double omega,
                    double* partials, SolveState* st);

@@ -31,11 +31,14 @@ struct MixCtx {
   int cf;              // coarse-fine flux correction in the FP64 residual and A*x
   int depth;           // sweep kernel: L2 prefetch distance in blocks (staging depth, >= 1)
   int sweep_threads;   // sweep kernel: 512 (a row per thread) or 256 (two rows per thread)
+  int sweep_ctas;      // sweep kernel: 1 CTA per SM (coefficient slot) or 2 (words read at use)
 };
 
 // CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel,
-// with 'threads' (128, 256 or 512) per CTA of the A*x and update kernels.
-void mx_grid_sizes(int threads, int* sweep, int* matvec, int* update, int* guides);
+// with 'threads' (128, 256 or 512) per CTA of the A*x and update kernels and
+// sweep_ctas (1 or 2) sweep CTAs per SM.
+void mx_grid_sizes(int threads, int sweep_ctas, int* sweep, int* matvec, int* update,
+                   int* guides);
 // Sweep coefficients of blocks [first, first + count), MIXED_COEF_WORDS per
 // block, in the thread order of a sweep kernel of sweep_threads threads:
 // 32-bit words (FP64 high words, rounded) into coef, or with d64 (the

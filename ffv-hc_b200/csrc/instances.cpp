@@ -124,9 +124,10 @@ ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P, bool d64) {
       CK(cudaEventCreateWithFlags(&P->act_ev[k], cudaEventDisableTiming));
       CK(cudaEventRecord(P->act_ev[k], P->stream));
     }
-    mx_grid_sizes(P->m_threads, &P->grid_sweep, &P->grid_matvec, &P->grid_update,
-                  &P->grid_guides);
+    mx_grid_sizes(P->m_threads, P->m_sweep_ctas, &P->grid_sweep, &P->grid_matvec,
+                  &P->grid_update, &P->grid_guides);
     P->grid_threads = P->m_threads;
+    P->grid_sweep_ctas = P->m_sweep_ctas;
   }
   if ((s = dalloc_t(P, &P->mcoef, 7 * n)) || (s = dalloc_t(P, &P->mguide, n / BC * 6 * 256)) ||
       (s = dalloc_t(P, &P->mucoef, n / BC * 8)) ||
@@ -178,6 +179,7 @@ MixCtx mix_ctx(const ffvgpu_pool* P) {
   C.cf = P->m_cf;
   C.depth = P->m_depth;
   C.sweep_threads = P->m_sweep_threads;
+  C.sweep_ctas = P->m_sweep_ctas;
   return C;
 }
 
@@ -214,6 +216,7 @@ ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
   if (prm->stage_depth < 0 || prm->stage_depth > 3) return bad("stage_depth must lie in 0..3");
   if (prm->sweep_threads != 0 && prm->sweep_threads != 256 && prm->sweep_threads != 512)
     return bad("sweep_threads must be 0, 256 or 512");
+  if (prm->sweep_ctas < 0 || prm->sweep_ctas > 2) return bad("sweep_ctas must be 0, 1 or 2");
   if (prm->threads_per_block != 0 && prm->threads_per_block != 128 &&
       prm->threads_per_block != 256 && prm->threads_per_block != 512)
     return bad("threads_per_block must be 0, 128, 256 or 512");
@@ -694,7 +697,8 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
                  (prm->flux_correction != 0) != (P->m_cf != 0) ||
                  (prm->fp64_data != 0) != (P->m_d64 != 0) ||
                  stage_depth_of(prm) != P->m_depth || threads_of(prm) != P->m_threads ||
-                 sweep_threads_of(prm) != P->m_sweep_threads))
+                 sweep_threads_of(prm) != P->m_sweep_threads ||
+                 (prm->sweep_ctas == 2 ? 2 : 1) != P->m_sweep_ctas))
     return bad("running instances use other preconditioner settings");
   double *xp, *g;
   size_t stride;
@@ -710,10 +714,13 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
   P->m_depth = stage_depth_of(prm);
   P->m_threads = threads_of(prm);
   P->m_sweep_threads = sweep_threads_of(prm);
-  if (P->grid_threads != P->m_threads) {  // the persistent grids of this CTA size
-    mx_grid_sizes(P->m_threads, &P->grid_sweep, &P->grid_matvec, &P->grid_update,
-                  &P->grid_guides);
+  P->m_sweep_ctas = prm->sweep_ctas == 2 ? 2 : 1;
+  if (P->grid_threads != P->m_threads || P->grid_sweep_ctas != P->m_sweep_ctas) {
+    // the persistent grids of these CTA sizes
+    mx_grid_sizes(P->m_threads, P->m_sweep_ctas, &P->grid_sweep, &P->grid_matvec,
+                  &P->grid_update, &P->grid_guides);
     P->grid_threads = P->m_threads;
+    P->grid_sweep_ctas = P->m_sweep_ctas;
   }
   I->count_max = prm->count_max;
   I->epsilon = prm->epsilon;
@@ -768,7 +775,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
       P->mgraph_wait_ns != P->wait_ns || P->mgraph_stall != P->stall_sweep ||
       P->mgraph_cf != P->m_cf || P->mgraph_d64 != P->m_d64 ||
       P->mgraph_depth != P->m_depth || P->mgraph_threads != P->m_threads ||
-      P->mgraph_sweep_threads != P->m_sweep_threads) {
+      P->mgraph_sweep_threads != P->m_sweep_threads || P->mgraph_sweep_ctas != P->m_sweep_ctas) {
     if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
     P->mgraph = nullptr;
     cudaGraph_t graph;
@@ -789,6 +796,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
     P->mgraph_depth = P->m_depth;
     P->mgraph_threads = P->m_threads;
     P->mgraph_sweep_threads = P->m_sweep_threads;
+    P->mgraph_sweep_ctas = P->m_sweep_ctas;
   }
   CK(cudaGraphLaunch(P->mgraph, P->stream));
   P->m_launches += (int64_t)iterations * launches_per_iteration(P);
@@ -970,6 +978,7 @@ ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* P, const int32_t* instances, in
     prm.threads_per_block = R.threads_per_block;
     prm.stage_depth = R.stage_depth;
     prm.sweep_threads = R.sweep_threads;
+    prm.sweep_ctas = R.sweep_ctas;
     prm.history = nullptr;
     R.ms = 0.0;
     R.max_count = 0;

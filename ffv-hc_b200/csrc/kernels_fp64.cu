@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cuda_runtime.h>
 
+#include "ffvgpu_async.cuh"
 #include "ffvgpu_internal.cuh"
 #include "ffvgpu_kernels.h"
 
@@ -47,28 +48,47 @@ __device__ __forceinline__ int guide_tix(int f, int a, int b) {
   }
 }
 
-// Stage block 'blk' of x in the shared tile, guide layer included.
+// Brings 'arrays' consecutive block-sized arrays of block blk (stride
+// BLOCK_CELLS doubles, the first at base) into L2 from thread 0: issued at a
+// kernel's entry, so the loads of the compute loop find them there.
+__device__ __forceinline__ void prefetch_block(const double* base, int blk, int arrays,
+                                               size_t stride) {
+  if (threadIdx.x == 0)
+    for (int a = 0; a < arrays; ++a)
+      async::prefetch_l2(base + (size_t)blk * stride + (size_t)a * BLOCK_CELLS,
+                         BLOCK_CELLS * 8u);
+}
+
+// Stage block 'blk' of x in the shared tile, guide layer included.  The
+// interior's sixteen loads per thread are issued together, and the guide
+// layer as pairs of positions of a face (guide_pair: the same values as
+// guide_value) with the three pairs' loads in flight together.
 __device__ __forceinline__ void stage_tile(double* __restrict__ xs, const double* __restrict__ x,
                                            int blk, const KCtx& C, const double* __restrict__ gst) {
   const int tid = threadIdx.x;
   const double* xb = x + (size_t)blk * BLOCK_CELLS;
-#pragma unroll 4
+  double v[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) v[m] = __ldg(xb + tid + THREADS * m);
+#pragma unroll
   for (int m = 0; m < 16; ++m) {
-    const int s = tid + THREADS * m;
     int i, j, k;
-    cell_of(s, i, j, k);
-    xs[tix(i, j, k)] = __ldg(xb + s);
+    cell_of(tid + THREADS * m, i, j, k);
+    xs[tix(i, j, k)] = v[m];
   }
-  const int a = tid & 15, b = tid >> 4;
-  for (int f = 0; f < 6; ++f) {
-    double v;
+#pragma unroll
+  for (int it = 0; it < 3; ++it) {
+    const int f = 2 * it + (tid >> 7), p0 = tid & 127, p1 = p0 + 128;
+    double g0, g1;
     if (gst) {
-      v = __ldg(gst + ((size_t)blk * 6 + f) * FACE_CELLS + b * 16 + a);
+      g0 = __ldg(gst + ((size_t)blk * 6 + f) * FACE_CELLS + p0);
+      g1 = __ldg(gst + ((size_t)blk * 6 + f) * FACE_CELLS + p1);
     } else {
       const FaceNbr nb = C.nbr[blk * 6 + f];
-      v = guide_value(x, blk, f, a, b, 1, nb, C.bc, C.dx[blk]);
+      guide_pair(x, blk, f, p0, p1, nb, C.bc, C.dx[blk], g0, g1);
     }
-    xs[guide_tix(f, a, b)] = v;
+    xs[guide_tix(f, p0 & 15, p0 >> 4)] = g0;
+    xs[guide_tix(f, p1 & 15, p1 >> 4)] = g1;
   }
 }
 
@@ -135,6 +155,8 @@ jacobi_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
   if (solve_done(st)) return;
   __shared__ double xs[FROM_ZERO ? 1 : TILE];
   const int blk = blockIdx.x, tid = threadIdx.x;
+  prefetch_block(A, blk, 7, 7 * (size_t)BLOCK_CELLS);
+  prefetch_block(bvec, blk, 1, BLOCK_CELLS);
   if (!FROM_ZERO) {
     stage_tile(xs, xin, blk, C, nullptr);
     __syncthreads();
@@ -183,6 +205,8 @@ calc_r_kernel(KCtx C, const double* __restrict__ x, const double* __restrict__ g
   if (st && solve_done(st)) return;
   __shared__ double xs[TILE];
   const int blk = blockIdx.x, tid = threadIdx.x;
+  prefetch_block(A, blk, 7, 7 * (size_t)BLOCK_CELLS);
+  prefetch_block(bvec, blk, 1, BLOCK_CELLS);
   stage_tile(xs, x, blk, C, gst);
   __syncthreads();
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
@@ -223,6 +247,8 @@ ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A
   if (solve_done(st)) return;
   __shared__ double xs[TILE];
   const int blk = blockIdx.x, tid = threadIdx.x;
+  prefetch_block(A, blk, 7, 7 * (size_t)BLOCK_CELLS);
+  if (y) prefetch_block(y, blk, 1, BLOCK_CELLS);
   stage_tile(xs, p, blk, C, nullptr);
   __syncthreads();
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
@@ -701,16 +727,27 @@ fold_bc_kernel(KCtx C, double* __restrict__ A, double* __restrict__ bvec) {
 // A (7 arrays) and b -> the sweep's coefficient stream (STREAM_BLOCK per block).
 __global__ void __launch_bounds__(THREADS)
 pack_stream_kernel(const double* __restrict__ A, const double* __restrict__ b,
-                   double* __restrict__ stream) {
+                   double* __restrict__ stream, double* __restrict__ urec,
+                   int32_t* __restrict__ ucount) {
   const int blk = blockIdx.x, tid = threadIdx.x;
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
   double* sb = stream + (size_t)blk * STREAM_BLOCK;
+  bool same = true;
   for (int m = 0; m < 16; ++m) {
     const int s = tid + THREADS * m;  // chunk m, cell tid
     double* dst = sb + (size_t)m * STREAM_CHUNK + tid;
-    for (int a = 0; a < 7; ++a) dst[a * 256] = Ab[(size_t)a * BLOCK_CELLS + s];
+    for (int a = 0; a < 7; ++a) {
+      const double v = Ab[(size_t)a * BLOCK_CELLS + s];
+      dst[a * 256] = v;
+      same = same && __double_as_longlong(v) == __double_as_longlong(Ab[(size_t)a * BLOCK_CELLS]);
+    }
     dst[7 * 256] = b[(size_t)blk * BLOCK_CELLS + s];
   }
+  // a uniform block (all seven coefficients bitwise equal to cell 0's): the
+  // sweep kernel copies only b of its stream and takes Ap..At from here
+  same = __syncthreads_and(same);
+  if (tid < 8) urec[(size_t)blk * 8 + tid] = tid < 7 ? Ab[(size_t)tid * BLOCK_CELLS] : (same ? 1.0 : 0.0);
+  if (tid == 0 && same) atomicAdd(ucount, 1);
 }
 
 // FFVILS::Fill (blas.f90:5-33): interior and stored guide layer.
@@ -813,8 +850,9 @@ void launch_assemble(cudaStream_t s, const KCtx& C, const double* ux, const doub
   assemble_kernel<<<C.nb, THREADS, 0, s>>>(C, ux, uy, uz, gux, guy, guz, cut, flags, A, b, vface,
                                            rhof, dt, field_stride);
 }
-void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b, double* stream) {
-  pack_stream_kernel<<<nb, THREADS, 0, s>>>(A, b, stream);
+void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b, double* stream,
+                        double* urec, int32_t* ucount) {
+  pack_stream_kernel<<<nb, THREADS, 0, s>>>(A, b, stream, urec, ucount);
 }
 void launch_fill(cudaStream_t s, int nb, double* x, size_t stride, double* g, double value) {
   fill_kernel<<<nb, THREADS, 0, s>>>(x, stride, g, value);

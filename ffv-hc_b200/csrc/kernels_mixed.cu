@@ -64,6 +64,9 @@ constexpr int TILE = 2 * SH;
 constexpr int COEF_WORDS = 7 * BLOCK_CELLS;  // coefficient words of one block
 constexpr int GUIDES = 6 * FACE_CELLS;  // guide values of one block (FP64)
 constexpr int SWEEP_SMEM = COEF_WORDS * 4 + TILE * 8 + BLOCK_CELLS * 8 + GUIDES * 8 + 16;
+// Two CTAs per SM (DUAL): no coefficient slot; a block's 32-bit words are
+// read at use from global memory (L2) and a first pass reads its vectors there.
+constexpr int SWEEP_SMEM_DUAL = TILE * 8 + BLOCK_CELLS * 8 + GUIDES * 8 + 16;
 
 // Sweep-kernel geometry for PTS threads per CTA (512 or 256).  Thread t owns
 // the cells (i, j, k) with i in {2 ih, 2 ih + 1}, j = JJ jp + jj (jj < JJ
@@ -269,7 +272,7 @@ __device__ __forceinline__ void stage_f32_as_f64(double* __restrict__ O, double*
                                                  const MixCtx& C) {
   const int tid = threadIdx.x;
   const ET* xb = x + (size_t)blk * BLOCK_CELLS;
-#pragma unroll 4
+#pragma unroll
   for (int m = 0; m < BLOCK_CELLS / NT; ++m) O[tid + NT * m] = (double)__ldg(xb + tid + NT * m);
   // the guide pairs (face, p, p + 128), 768 of them, NT at a time: all the
   // pairs' loads in flight together
@@ -429,26 +432,43 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
 // coefficients in thread order ([a][m][thread], c64 already offset to this
 // thread).  For one data format the values, and so the results, do not
 // depend on the source.
-enum { CS_UNI = 0, CS_W32 = 1, CS_G64 = 2 };
+enum { CS_UNI = 0, CS_W32 = 1, CS_G64 = 2, CS_G32 = 3 };
+__device__ __forceinline__ uint32_t quad_word(const uint4& q, int h) {
+  return h == 0 ? q.x : (h == 1 ? q.y : (h == 2 ? q.z : q.w));
+}
 // PTS threads: the cells m = (c JJ + jj) 4 + h of a thread (SweepGeom).  Of a
 // cell's six neighbours (all of the other colour) the x neighbour at the same
 // ih, the z neighbours inside the 4-cell column and, with two rows per thread
 // (PTS 256), the y neighbour in the thread's other row are its own registers;
 // the rest come from the tile.  The terms keep rbgs_smoother's order (w, e,
 // s, n, b, t) whatever their source, so every PTS gives the same bits.
-template <int CS, int PTS>
+// CS_G32 (two CTAs per SM, no slot): the cell's 32-bit words are read at use
+// from global memory, the four cells (h) of a row as one 16-byte vector per
+// coefficient (c32q: the block's words as vectors, offset to this thread).
+// RREG: a uniform block keeps its right-hand side in registers (off where
+// the registers are short: two CTAs per SM).
+template <int CS, int PTS, bool RREG = true>
 __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, int p0,
                                            double (&E)[2][SweepGeom<PTS>::JJ][4],
                                            const uint32_t (&cw)[SweepGeom<PTS>::CPT][7],
                                            const double (&ku)[7],
-                                           const double* __restrict__ c64, double mom,
+                                           const double* __restrict__ c64,
+                                           const uint4* __restrict__ c32q, double mom,
                                            int nsweep) {
-  constexpr bool UNI = CS == CS_UNI;
+  constexpr bool UNI = CS == CS_UNI && RREG;
   constexpr int JJ = SweepGeom<PTS>::JJ, CPT = SweepGeom<PTS>::CPT;
+  uint4 cq[JJ];
 #define MX_COEF(m, a)                                          \
   (CS == CS_UNI ? ku[a]                                        \
    : CS == CS_W32 ? widen_here(cw[m][a])                       \
-                  : __ldg(c64 + ((a) * CPT + (m)) * PTS))
+   : CS == CS_G64 ? __ldg(c64 + ((a) * CPT + (m)) * PTS)        \
+                  : widen(quad_word(cq[((m) >> 2) % JJ], (m) & 3)))
+  // the vectors of coefficient a of this colour's rows (CS_G32)
+#define MX_LOADQ(a)                                                               \
+  if (CS == CS_G32) {                                                             \
+    _Pragma("unroll") for (int jq = 0; jq < JJ; ++jq)                             \
+      cq[jq] = __ldg(c32q + ((a) * (CPT / 4) + c * JJ + jq) * PTS);               \
+  }
   // a uniform block has the registers to keep its right-hand side too (one
   // shared-memory read less per update)
   double vr[2][JJ][4];
@@ -477,6 +497,7 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
           rc[jj][h] = UNI ? vr[c][jj][h] : V[((c * JJ + jj) * 4 + h) * PTS];
         }
 #define MX_M(jj, h) ((c * JJ + (jj)) * 4 + (h))
+      MX_LOADQ(0)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
@@ -485,6 +506,7 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 0), par ? E[1 - c][jj][h] : xo[jj][h],
                                rc[jj][h]);
         }
+      MX_LOADQ(1)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
@@ -493,12 +515,14 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 1), par ? xo[jj][h] : E[1 - c][jj][h],
                                rc[jj][h]);
         }
+      MX_LOADQ(2)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
         for (int h = 0; h < 4; ++h)
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 2),
                                jj > 0 ? E[1 - c][jj - 1][h] : O[jj * SP + h * SQ - SP], rc[jj][h]);
+      MX_LOADQ(3)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
@@ -506,18 +530,21 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 3),
                                jj < JJ - 1 ? E[1 - c][jj + 1][h] : O[jj * SP + h * SQ + SP],
                                rc[jj][h]);
+      MX_LOADQ(4)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
         for (int h = 0; h < 4; ++h)
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 4),
                                h > 0 ? E[1 - c][jj][h - 1] : O[jj * SP - SQ], rc[jj][h]);
+      MX_LOADQ(5)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
         for (int h = 0; h < 4; ++h)
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 5),
                                h < 3 ? E[1 - c][jj][h + 1] : O[jj * SP + 4 * SQ], rc[jj][h]);
+      MX_LOADQ(6)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
@@ -534,6 +561,7 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
   }
 }
 #undef MX_COEF
+#undef MX_LOADQ
 
 // Tile address of the guide cell at position p (u + 16 v) of a face.
 __device__ __forceinline__ int guide_slot(int face, int p) {
@@ -597,8 +625,11 @@ __device__ void build_live_list(const MixCtx& C, int from, int n_act, int2* list
 
 // ET: the iterate between passes, float (the mixed form) or double (the
 // FP64-data variant, whose coefficients are FP64 too and read at use).
-template <int MODE, bool FIRST, typename ET, int PTS>
-__global__ void __launch_bounds__(PTS, 1)
+// DUAL: two CTAs per SM (no coefficient slot: a block's words are read at
+// use and a first pass reads its vectors from global memory, prefetched into
+// L2), so one CTA's staging and barriers overlap the other's sweeps.
+template <int MODE, bool FIRST, typename ET, int PTS, bool DUAL>
+__global__ void __launch_bounds__(PTS, DUAL ? 2 : 1)
 mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
                 double* __restrict__ r0, double* __restrict__ pv, const double* __restrict__ q,
                 const uint32_t* __restrict__ coef, const double* __restrict__ coef64,
@@ -607,9 +638,10 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
   constexpr bool D64 = sizeof(ET) == 8;
   constexpr int JJ = SweepGeom<PTS>::JJ, CPT = SweepGeom<PTS>::CPT;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint32_t* slot = reinterpret_cast<uint32_t*>(smem);
-  double* T = reinterpret_cast<double*>(smem + COEF_WORDS * 4);
-  double* V = reinterpret_cast<double*>(smem + COEF_WORDS * 4 + TILE * 8);  // [m][t] rhs
+  constexpr int SLOT_BYTES = DUAL ? 0 : COEF_WORDS * 4;
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem);  // not used with DUAL
+  double* T = reinterpret_cast<double*>(smem + SLOT_BYTES);
+  double* V = reinterpret_cast<double*>(smem + SLOT_BYTES + TILE * 8);  // [m][t] rhs
   double* GB = V + BLOCK_CELLS;  // [face][p] guides of the block, copied with its coefficients
   uint64_t* bar = reinterpret_cast<uint64_t*>(GB + GUIDES);
   __shared__ int2 s_list[LIST_CAP];
@@ -640,7 +672,10 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     constexpr uint32_t UB = 8 * 8;            // bytes of a coefficient record
     double* sd = reinterpret_cast<double*>(slot);
     if (uni) {
-      if (FIRST) {
+      if (FIRST && DUAL) {  // its vectors are read from global memory
+        async::mbar_expect_tx(bar, UB);
+        async::bulk_g2s(s_urec[p], C.ucoef + (size_t)b * 8, UB, bar);
+      } else if (FIRST) {
         const bool copy = e.y & LF_COPY;
         const bool needq = !copy, needp = MODE == 0 && !copy;
         async::mbar_expect_tx(bar, UB + VB + (needq ? VB : 0u) + (needp ? VB : 0u));
@@ -655,8 +690,8 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       }
       return;
     }
-    if (D64) {
-      // FP64 coefficients are read at use (prefetched into L2); the copy
+    if (D64 || DUAL) {
+      // the coefficients are read at use (prefetched into L2); the copy
       // brings the guide layer only
       if (FIRST) {
         async::mbar_arrive(bar);
@@ -681,7 +716,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     if (!uni) {
       if (D64)
         async::prefetch_l2(coef64 + (size_t)b * COEF_WORDS, COEF_WORDS * 8u);
-      else if (depth > 1)
+      else if (DUAL || depth > 1)
         async::prefetch_l2(coef + (size_t)b * COEF_WORDS, COEF_WORDS * 4u);
     }
     if (FIRST) {
@@ -739,9 +774,10 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       const SolveState* S = C.inst.st + inst;
       const bool copy = ent.y & LF_COPY;  // first iteration of a (re)start: p = r, r0 = r
       const double mgamma = -S->gamma, beta = S->beta, malpha = -S->alpha;
-      const double* rs = uni ? sd : r + gbase;
-      const double* qs = uni ? sd + BLOCK_CELLS : q + gbase;
-      const double* ps = uni ? sd + 2 * BLOCK_CELLS : pv + gbase;
+      const bool slotted = uni && !DUAL;  // its vectors came with its copy
+      const double* rs = slotted ? sd : r + gbase;
+      const double* qs = slotted ? sd + BLOCK_CELLS : q + gbase;
+      const double* ps = slotted ? sd + 2 * BLOCK_CELLS : pv + gbase;
 #pragma unroll
       for (int c = 0; c < 2; ++c)
 #pragma unroll
@@ -795,7 +831,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
         for (int a = 0; a < 6; ++a) ku[a] = widen(hi_round(U[1 + a]));
         ku[6] = widen(hi_round(1.0 / U[0]));
       }
-    } else if (!D64) {
+    } else if (!D64 && !DUAL) {
 #pragma unroll
       for (int a = 0; a < 7; ++a)
 #pragma unroll
@@ -847,12 +883,16 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     }
     pos = npos;
     const double* c64 = D64 ? coef64 + (size_t)blk * COEF_WORDS + tid : nullptr;
+    const uint4* c32q =
+        reinterpret_cast<const uint4*>(coef + (size_t)blk * COEF_WORDS) + tid;
     if (uni)
-      run_sweeps<CS_UNI, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, mom, nsweep);
+      run_sweeps<CS_UNI, PTS, !DUAL>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, c32q, mom, nsweep);
     else if constexpr (D64)
-      run_sweeps<CS_G64, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, mom, nsweep);
+      run_sweeps<CS_G64, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, c32q, mom, nsweep);
+    else if constexpr (DUAL)
+      run_sweeps<CS_G32, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, c32q, mom, nsweep);
     else
-      run_sweeps<CS_W32, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, mom, nsweep);
+      run_sweeps<CS_W32, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, c32q, mom, nsweep);
 #pragma unroll
     for (int c = 0; c < 2; ++c)
 #pragma unroll
@@ -926,17 +966,40 @@ mx_matvec_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ 
     const int blk = C.active[item];
     const int inst = active_instance(C, blk);
     if (inst < 0) continue;
+    if (tid == 0 && item + (int)gridDim.x < n_act) {
+      // the next block's vectors into L2 while this one is staged and summed
+      const size_t nb = (size_t)C.active[item + gridDim.x] * BLOCK_CELLS;
+      async::prefetch_l2(x + nb, BLOCK_CELLS * (uint32_t)sizeof(ET));
+      async::prefetch_l2(w0 + nb, BLOCK_CELLS * 8u);
+    }
     if (tid < 6) snb[tid] = C.nbr[blk * 6 + tid];
+    const size_t base = (size_t)blk * BLOCK_CELLS;
+    // with 8 cells per thread (NT 512) the registers hold the block's dot
+    // partners and coefficient record, loaded before the staging so that
+    // their latency overlaps it; with more cells per thread they are read
+    // in the loop
+    constexpr bool HOIST = NT >= 512;
+    constexpr int CPC = HALF_CELLS / NT;  // cells per colour of a thread
+    double wv[2][HOIST ? CPC : 1];
+    double ur[8];
+    if (HOIST) {
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int m = 0; m < (HOIST ? CPC : 1); ++m)
+          wv[c][m] = __ldg(w0 + base + c * HALF_CELLS + tid + NT * m);
+#pragma unroll
+      for (int a = 0; a < 8; ++a) ur[a] = __ldg(C.ucoef + (size_t)blk * 8 + a);
+    }
     __syncthreads();
     stage_f32_as_f64<NT>(O, G, x, blk, snb, C.dx[blk], C);
     __syncthreads();
-    const size_t base = (size_t)blk * BLOCK_CELLS;
     const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
     const double* U = C.ucoef + (size_t)blk * 8;
-    const bool uni = U[7] != 0.0;  // the same seven coefficients in every cell
+    const bool uni = (HOIST ? ur[7] : U[7]) != 0.0;  // the same seven coefficients in every cell
     double u[7];
 #pragma unroll
-    for (int a = 0; a < 7; ++a) u[a] = uni ? U[a] : 0.0;
+    for (int a = 0; a < 7; ++a) u[a] = uni ? (HOIST ? ur[a] : U[a]) : 0.0;
     constexpr int VPT = 512 / NT;
     double acc[NV][2][VPT] = {};
 #pragma unroll
@@ -958,7 +1021,7 @@ mx_matvec_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ 
                                  return uni ? u[1 + f] : __ldg(Ab + (1 + f) * BLOCK_CELLS + s);
                                });
         y[base + s] = yv;
-        acc[0][c][m % VPT] += yv * __ldg(w0 + base + s);
+        acc[0][c][m % VPT] += yv * (HOIST ? wv[c][HOIST ? m : 0] : __ldg(w0 + base + s));
         if (NV == 2) acc[NV - 1][c][m % VPT] += yv * yv;
       }
     }
@@ -1065,14 +1128,20 @@ static void sweep_launch(cudaStream_t s, const MixCtx& C, int count, float omega
                          const double* r, double* r0, double* pv, const double* q,
                          const uint32_t* coef, const double* coef64, const void* ein,
                          const double* guides, void* eout) {
-  if (C.sweep_threads == 256)
-    mx_sweep_kernel<MODE, FIRST, ET, 256><<<count, 256, SWEEP_SMEM, s>>>(
-        C, omega, nsweep, r, r0, pv, q, coef, coef64, static_cast<const ET*>(ein), guides,
-        static_cast<ET*>(eout), C.depth);
+#define MX_GO(PTS, DUAL)                                                                  \
+  mx_sweep_kernel<MODE, FIRST, ET, PTS, DUAL><<<count, PTS, DUAL ? SWEEP_SMEM_DUAL : SWEEP_SMEM, \
+                                                s>>>(C, omega, nsweep, r, r0, pv, q, coef,      \
+                                                     coef64, static_cast<const ET*>(ein),       \
+                                                     guides, static_cast<ET*>(eout), C.depth)
+  if (C.sweep_threads == 256 && C.sweep_ctas == 2)
+    MX_GO(256, true);
+  else if (C.sweep_threads == 256)
+    MX_GO(256, false);
+  else if (C.sweep_ctas == 2)
+    MX_GO(512, true);
   else
-    mx_sweep_kernel<MODE, FIRST, ET, 512><<<count, 512, SWEEP_SMEM, s>>>(
-        C, omega, nsweep, r, r0, pv, q, coef, coef64, static_cast<const ET*>(ein), guides,
-        static_cast<ET*>(eout), C.depth);
+    MX_GO(512, false);
+#undef MX_GO
 }
 
 void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first,
@@ -1104,32 +1173,42 @@ void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const void* e,
 }
 
 template <typename K>
-static void allow_sweep_smem(K kernel) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SWEEP_SMEM);
+static void allow_sweep_smem(K kernel, int bytes = SWEEP_SMEM) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-void mx_grid_sizes(int threads, int* sweep, int* matvec, int* update, int* guides) {
+void mx_grid_sizes(int threads, int sweep_ctas, int* sweep, int* matvec, int* update,
+                   int* guides) {
   int dev = 0, sms = 0, a = 0, b = 0, c = 0, d = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // the sweep kernels' shared memory, on the calling device (before any launch)
-#define MX_ALLOW(PTS)                                    \
-  allow_sweep_smem(mx_sweep_kernel<0, true, float, PTS>);  \
-  allow_sweep_smem(mx_sweep_kernel<0, false, float, PTS>); \
-  allow_sweep_smem(mx_sweep_kernel<1, true, float, PTS>);  \
-  allow_sweep_smem(mx_sweep_kernel<1, false, float, PTS>); \
-  allow_sweep_smem(mx_sweep_kernel<0, true, double, PTS>); \
-  allow_sweep_smem(mx_sweep_kernel<0, false, double, PTS>); \
-  allow_sweep_smem(mx_sweep_kernel<1, true, double, PTS>); \
-  allow_sweep_smem(mx_sweep_kernel<1, false, double, PTS>);
-  MX_ALLOW(512)
-  MX_ALLOW(256)
+#define MX_ALLOW(PTS, DUAL, BYTES)                                          \
+  allow_sweep_smem(mx_sweep_kernel<0, true, float, PTS, DUAL>, BYTES);       \
+  allow_sweep_smem(mx_sweep_kernel<0, false, float, PTS, DUAL>, BYTES);      \
+  allow_sweep_smem(mx_sweep_kernel<1, true, float, PTS, DUAL>, BYTES);       \
+  allow_sweep_smem(mx_sweep_kernel<1, false, float, PTS, DUAL>, BYTES);      \
+  allow_sweep_smem(mx_sweep_kernel<0, true, double, PTS, DUAL>, BYTES);      \
+  allow_sweep_smem(mx_sweep_kernel<0, false, double, PTS, DUAL>, BYTES);     \
+  allow_sweep_smem(mx_sweep_kernel<1, true, double, PTS, DUAL>, BYTES);      \
+  allow_sweep_smem(mx_sweep_kernel<1, false, double, PTS, DUAL>, BYTES);
+  MX_ALLOW(512, false, SWEEP_SMEM)
+  MX_ALLOW(256, false, SWEEP_SMEM)
+  MX_ALLOW(512, true, SWEEP_SMEM_DUAL)
+  MX_ALLOW(256, true, SWEEP_SMEM_DUAL)
 #undef MX_ALLOW
-  // one CTA per SM for either thread count (its shared memory)
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, float, 512>, 512,
-                                                SWEEP_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, float, 256>, 256,
-                                                SWEEP_SMEM);
+  // CTAs per SM of the sweep kernel in the chosen arrangement
+  if (sweep_ctas == 2) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, float, 512, true>,
+                                                  512, SWEEP_SMEM_DUAL);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, float, 256, true>,
+                                                  256, SWEEP_SMEM_DUAL);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, float, 512, false>,
+                                                  512, SWEEP_SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, float, 256, false>,
+                                                  256, SWEEP_SMEM);
+  }
   if (threads == 128) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2, false, float, 128>,
                                                   128, 0);

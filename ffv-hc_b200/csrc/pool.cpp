@@ -171,10 +171,14 @@ ffvgpu_status require_system(ffvgpu_pool* P) {
 // Repacks A and b into the sweep's coefficient stream when they changed.
 ffvgpu_status ensure_stream(ffvgpu_pool* P) {
   ffvgpu_status s;
-  if ((s = dalloc_t(P, &P->coef, (size_t)P->nb * STREAM_BLOCK))) return s;
+  if ((s = dalloc_t(P, &P->coef, (size_t)P->nb * STREAM_BLOCK)) ||
+      (s = dalloc_t(P, &P->urec, (size_t)P->nb * 8)) || (s = dalloc_t(P, &P->ucount_d, 1)))
+    return s;
   if (P->stream_version != P->sys_version) {
-    launch_pack_stream(P->stream, P->nb, P->A, P->b, P->coef);
+    CK(cudaMemsetAsync(P->ucount_d, 0, sizeof(int32_t), P->stream));
+    launch_pack_stream(P->stream, P->nb, P->A, P->b, P->coef, P->urec, P->ucount_d);
     CK(cudaGetLastError());
+    CK(download_sync(P, &P->ucount_h, P->ucount_d, sizeof(int32_t)));
     P->stream_version = P->sys_version;
   }
   return FFVGPU_OK;
@@ -277,6 +281,13 @@ ffvgpu_status solve_status(const SolveState& h, const ffvgpu_iter_params* prm, i
 
 int64_t interior_bytes(const ffvgpu_pool* P, int words) {
   return (int64_t)P->nb * (int64_t)BC * 8 * words;
+}
+// Bytes of one pass of the red-black kernel: 'words' per cell (10 for a
+// sweep with its residual, 9 for a residual alone) in a block that streams
+// its coefficients, 'words' - 7 in a uniform block (b and x only).
+int64_t rbgs_pass_bytes(const ffvgpu_pool* P, int words) {
+  const int64_t u = P->ucount_h, n = P->nb;
+  return ((n - u) * words + u * (words - 7)) * (int64_t)BC * 8;
 }
 
 // Stream, events, neighbour table, cell sizes and the solver state of a
@@ -390,7 +401,7 @@ void ffvgpu_pool_destroy(ffvgpu_pool* P) {
   if (P->stream) cudaStreamSynchronize(P->stream);
   if (P->own_stream) cudaStreamSynchronize(P->own_stream);
   release_instances(P);
-  void* ptrs[] = {P->x[0], P->x[1], P->gx, P->A, P->coef, P->b, P->u[0], P->u[1], P->u[2],
+  void* ptrs[] = {P->x[0], P->x[1], P->gx, P->A, P->coef, P->urec, P->ucount_d, P->b, P->u[0], P->u[1], P->u[2],
                   P->gu[0], P->gu[1], P->gu[2], P->cut, P->vface, P->lapp, P->flags, P->r,
                   P->p, P->q, P->z[0], P->z[1], P->r0, P->sv, P->tv, P->zb[0], P->zb[1],
                   P->partials, P->st, P->hist_d,
@@ -753,7 +764,7 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   launch_rbgs(P->stream, C, false, true, P->x[c0], P->x[1 - c0], P->coef, P->gx, prm->omega,
               P->partials, P->st, FIN_RBGS, 0);
   launches++;
-  bytes += interior_bytes(P, 10);
+  bytes += rbgs_pass_bytes(P, 10);
   CK(cudaEventRecord(P->ev2, P->stream));
   int swept = 0;
   // Each pass is a programmatic dependent of the pass before it (it
@@ -766,7 +777,7 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
     polled_last = false;
     swept++;
     launches++;
-    bytes += interior_bytes(P, 10);
+    bytes += rbgs_pass_bytes(P, 10);
     if (poll && (n % every) == 0) {
       bool done = false;
       if ((s = poll_done(P, &done))) return s;
@@ -787,8 +798,8 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   // (the solve ran to countMax, or converged on its last residual) iterate N
   const int m = early ? h.count : N;
   // passes that ran: sweeps 1..min(m+1, N), residual-only pass only at the end
-  bytes = interior_bytes(P, 2) + interior_bytes(P, 10) * (early ? (m + 1) : N) +
-          (early ? 0 : interior_bytes(P, 9));
+  bytes = interior_bytes(P, 2) + rbgs_pass_bytes(P, 10) * (early ? (m + 1) : N) +
+          (early ? 0 : rbgs_pass_bytes(P, 9));
   P->xcur = (c0 + m) & 1;
   launch_exchange(P->stream, C, P->x[P->xcur], P->gx);
   CK(cudaGetLastError());
@@ -803,6 +814,7 @@ ffvgpu_status ffvgpu_solve_rbgs(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   R.sweep_launches = swept;
   R.bytes_moved = bytes;
   R.kernel_launches = launches + 1;
+  R.uniform_blocks = P->ucount_h;
   if (prm->history) {
     const int nh = (h.count >= 1 && h.count <= N) ? h.count : N;
     CK(download_sync(P, prm->history, P->hist_d, sizeof(double) * nh));

@@ -93,6 +93,9 @@ struct ffvgpu_pool {
   double* gx = nullptr;  // stored first guide layer of x
   double* A = nullptr;   // [nb][7][4096]
   double* coef = nullptr;         // sweep coefficient stream [nb][STREAM_BLOCK]
+  double* urec = nullptr;         // [nb][8] uniform records of the stream (launch_pack_stream)
+  int32_t* ucount_d = nullptr;    // uniform blocks of the stream
+  int32_t ucount_h = 0;           // the same, read after each repack
   int64_t sys_version = 1;        // bumped whenever A or b change
   int64_t stream_version = 0;     // sys_version the stream was packed from
   double* b = nullptr;
@@ -155,6 +158,7 @@ struct ffvgpu_pool {
   int m_depth = 1;  // sweep kernel staging depth (L2 prefetch distance in blocks)
   int m_threads = 256;  // CTA size of the A*x and update kernels
   int m_sweep_threads = 512;  // CTA size of the sweep kernel
+  int m_sweep_ctas = 1;       // sweep CTAs per SM
   cudaGraphExec_t mgraph = nullptr;
   int mgraph_iters = 0;
   double mgraph_omega = 0.0;
@@ -163,7 +167,7 @@ struct ffvgpu_pool {
   int mgraph_stall = 0;
   int mgraph_cf = 0;
   int mgraph_d64 = 0;
-  int mgraph_depth = 0, mgraph_threads = 0, mgraph_sweep_threads = 0;
+  int mgraph_depth = 0, mgraph_threads = 0, mgraph_sweep_threads = 0, mgraph_sweep_ctas = 0;
   int stall_sweep = 0;  // test hook (ffvgpu_pool_stall_next_solve), cleared when a solve ends
   int64_t m_launches = 0;
   int64_t m_bytes = 0;
@@ -174,7 +178,8 @@ struct ffvgpu_pool {
   cudaEvent_t act_ev[2] = {nullptr, nullptr};
   int act_next = 0;
   int grid_sweep = 0, grid_matvec = 0, grid_update = 0, grid_guides = 0;
-  int grid_threads = 0;  // m_threads the grid sizes were computed for
+  int grid_threads = 0;     // m_threads the grid sizes were computed for
+  int grid_sweep_ctas = 0;  // and m_sweep_ctas
 
   ffvgpu::KCtx ctx(const ffvgpu::BCSet& bc) const {
     ffvgpu::KCtx C;
@@ -184,6 +189,7 @@ struct ffvgpu_pool {
     C.nb = nb;
     C.first = 0;
     C.wait_ns = wait_ns;
+    C.urec = (coef && stream_version == sys_version) ? urec : nullptr;
     return C;
   }
 };

@@ -34,6 +34,7 @@
 // DRAIN_NS, independently of the wait limit; a drain that gives up is
 // reported as ROLE_DRAIN), and the solver state reports TIMEOUT.
 #include <cfloat>
+#include <cstddef>
 #include <cstdint>
 #include <mutex>
 #include <cuda_runtime.h>
@@ -60,6 +61,11 @@ constexpr int NTHREADS = CONS0 + 32 * CONSUMER_WARPS;  // 800
 constexpr int NCONS = 32 * CONSUMER_WARPS;            // one cell per consumer per slot
 constexpr int NGATHER = 32 * GATHER_WARPS;
 enum { ROLE_PRODUCER = 1, ROLE_GATHER = 2, ROLE_CONSUMER = 4 };
+// Uniform flags of a CTA's first 32 UMASK_WORDS blocks are kept in shared
+// memory; later blocks (pools of more than 148 x 1024 blocks) stream all
+// their coefficients, which gives the same results.
+constexpr int UMASK_WORDS = 32;
+constexpr uint32_t B_ROW_BYTES = SUB_CELLS * 8;  // b of one stream chunk
 
 struct __align__(128) Smem {
   double ring[STAGES][CPT][NARR][SUB_CELLS];  // 96 KB
@@ -68,6 +74,8 @@ struct __align__(128) Smem {
   double gbuf[2][6 * FACE_CELLS];          // 24 KB: guide layers, [face][v][u]
   uint64_t full[STAGES], empty[STAGES];
   uint64_t xfull[2], xempty[2], gfull[2], gempty[2];
+  double urec[2][8];                       // the uniform record of the block in xt[]
+  uint32_t umask[UMASK_WORDS];             // uniform flags of this CTA's blocks
   double ws[CONSUMER_WARPS];
   int abort_flag;
   int last;
@@ -116,6 +124,17 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
   const int nb = C.nb;
   volatile int* abort_flag = &S.abort_flag;
 
+  if (tid < UMASK_WORDS) S.umask[tid] = 0;
+  __syncthreads();
+  // uniform blocks (launch_pack_stream's records, written before this pass's
+  // dependency): their slots bring b only and their seven coefficients come
+  // with x
+  if (C.urec) {
+    const int mine = (blockIdx.x < nb) ? (nb - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    for (int k = tid; k < mine && k < 32 * UMASK_WORDS; k += NTHREADS)
+      if (C.urec[(size_t)(blockIdx.x + k * gridDim.x) * 8 + 7] != 0.0)
+        atomicOr(&S.umask[k >> 5], 1u << (k & 31));
+  }
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&S.full[s], 1);
@@ -136,6 +155,10 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
   __syncthreads();
   const int myblocks = (blockIdx.x < nb) ? (nb - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
   const int total_slots = myblocks * SLOTS;
+  // is this CTA's m-th block uniform
+  auto uniform = [&](int m) {
+    return m < 32 * UMASK_WORDS && ((S.umask[m >> 5] >> (m & 31)) & 1u);
+  };
 
   if (tid < GATHER0) {
     // ------------------------------------------------------------ producer
@@ -147,20 +170,36 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       // first STAGES slots are issued before waiting for it.
       auto issue_slot = [&](uint32_t gg) {
         const int s = gg % STAGES;
-        const int blk = blockIdx.x + (int)(gg / SLOTS) * gridDim.x;
+        const int m = (int)(gg / SLOTS);
+        const int blk = blockIdx.x + m * gridDim.x;
         const int j = gg % SLOTS;
-        mbar_expect_tx(&S.full[s], SLOT_BYTES);
         // slot j: stream chunks CPT*j .. CPT*j+CPT-1 (colour = j / (SLOTS/2))
-        bulk_g2s(S.ring[s], stream + (size_t)blk * STREAM_BLOCK + (size_t)j * CPT * STREAM_CHUNK,
-                 SLOT_BYTES, &S.full[s]);
+        const double* src = stream + (size_t)blk * STREAM_BLOCK + (size_t)j * CPT * STREAM_CHUNK;
+        if (uniform(m)) {  // b of each chunk into its row of the slot
+          mbar_expect_tx(&S.full[s], CPT * B_ROW_BYTES);
+          for (int c = 0; c < CPT; ++c)
+            bulk_g2s(S.ring[s][c][NARR - 1], src + (size_t)c * STREAM_CHUNK + 7 * SUB_CELLS,
+                     B_ROW_BYTES, &S.full[s]);
+        } else {
+          mbar_expect_tx(&S.full[s], SLOT_BYTES);
+          bulk_g2s(S.ring[s], src, SLOT_BYTES, &S.full[s]);
+        }
+      };
+      // x of the CTA's m-th block into tile buffer xb, with its uniform
+      // record when it has one
+      auto issue_x = [&](int m, int xb) {
+        const int blk = blockIdx.x + m * gridDim.x;
+        const bool u = uniform(m);
+        mbar_expect_tx(&S.xfull[xb], BLOCK_CELLS * 8 + (u ? 64u : 0u));
+        bulk_g2s(S.xt[xb], xin + (size_t)blk * BLOCK_CELLS, BLOCK_CELLS * 8, &S.xfull[xb]);
+        if (u) bulk_g2s(S.urec[xb], C.urec + (size_t)blk * 8, 64, &S.xfull[xb]);
       };
       for (; g < (uint32_t)STAGES && g < (uint32_t)total_slots; ++g) issue_slot(g);
       asm volatile("griddepcontrol.wait;" ::: "memory");
       const bool skip = *((volatile const int32_t*)&st->done) != 0;
       if (!skip && myblocks > 0) {
         ++nx[0];
-        mbar_expect_tx(&S.xfull[0], BLOCK_CELLS * 8);
-        bulk_g2s(S.xt[0], xin + (size_t)blockIdx.x * BLOCK_CELLS, BLOCK_CELLS * 8, &S.xfull[0]);
+        issue_x(0, 0);
       }
       for (; !skip && ok && g < (uint32_t)total_slots; ++g) {
         const int s = g % STAGES;
@@ -179,9 +218,7 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
                                C.wait_ns)))
             break;
           ++nx[xb];
-          mbar_expect_tx(&S.xfull[xb], BLOCK_CELLS * 8);
-          bulk_g2s(S.xt[xb], xin + (size_t)(blk + gridDim.x) * BLOCK_CELLS, BLOCK_CELLS * 8,
-                   &S.xfull[xb]);
+          issue_x(m + 1, xb);
         }
       }
       // Drain: the last armed phase of every barrier a copy completes on must
@@ -253,6 +290,11 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
       const double* G = S.gbuf[xb];
       double* xo = xout + (size_t)blk * BLOCK_CELLS;
       double acc[2] = {0.0, 0.0};
+      // a uniform block: the seven coefficients of every cell, from its record
+      const bool uni = uniform(m);
+      Coef cu;
+      cu.ap = S.urec[xb][0]; cu.aw = S.urec[xb][1]; cu.ae = S.urec[xb][2]; cu.as = S.urec[xb][3];
+      cu.an = S.urec[xb][4]; cu.ab = S.urec[xb][5]; cu.at = S.urec[xb][6]; cu.b = 0.0;
       // colour 0: neighbours are colour 1 (unchanged).  Consumer ct takes the
       // cell q = mm*512 + ct of every slot (stream chunk ct >> 8 of the slot).
       const int h = ct >> 8, t = ct & 255;
@@ -261,7 +303,12 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
         live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER,
                                  C.wait_ns);
         Coef c = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (live) c = load_coef(S.ring[s][h], t);
+        if (live && uni) {
+          c = cu;
+          c.b = S.ring[s][h][NARR - 1][t];
+        } else if (live) {
+          c = load_coef(S.ring[s][h], t);
+        }
         hold(c);
         release_slot(&S.empty[s], lane, live);
         if (!live) continue;
@@ -288,7 +335,12 @@ rbgs_pipelined_kernel(KCtx C, const double* __restrict__ xin, double* __restrict
         live = live && mbar_wait(&S.full[s], (g / STAGES) & 1, abort_flag, ROLE_CONSUMER,
                                  C.wait_ns);
         Coef c = {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (live) c = load_coef(S.ring[s][h], t);
+        if (live && uni) {
+          c = cu;
+          c.b = S.ring[s][h][NARR - 1][t];
+        } else if (live) {
+          c = load_coef(S.ring[s][h], t);
+        }
         hold(c);
         release_slot(&S.empty[s], lane, live);
         if (!live) continue;
@@ -434,5 +486,8 @@ void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const doub
 }
 
 size_t rbgs_pipelined_smem_bytes() { return sizeof(pipe::Smem); }
+// bulk copies land in ring rows, xt[] and urec[]: 16-byte aligned
+static_assert(offsetof(pipe::Smem, urec) % 16 == 0, "urec must be 16-byte aligned");
+static_assert(offsetof(pipe::Smem, xt) % 16 == 0, "xt must be 16-byte aligned");
 
 }  // namespace ffvgpu

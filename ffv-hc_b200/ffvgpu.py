@@ -108,7 +108,7 @@ class MixedParams(ctypes.Structure):
         ("restart_growth", ctypes.c_double), ("restart_every", ctypes.c_int32),
         ("flux_correction", ctypes.c_int32), ("fp64_data", ctypes.c_int32),
         ("threads_per_block", ctypes.c_int32), ("stage_depth", ctypes.c_int32),
-        ("sweep_threads", ctypes.c_int32),
+        ("sweep_threads", ctypes.c_int32), ("sweep_ctas", ctypes.c_int32),
     ]
 
 
@@ -137,7 +137,7 @@ class TuneRecord(ctypes.Structure):
         ("sweeps_per_exchange", ctypes.c_int32), ("iterations_per_replay", ctypes.c_int32),
         ("ms", ctypes.c_double), ("max_count", ctypes.c_int32), ("converged", ctypes.c_int32),
         ("threads_per_block", ctypes.c_int32), ("stage_depth", ctypes.c_int32),
-        ("sweep_threads", ctypes.c_int32),
+        ("sweep_threads", ctypes.c_int32), ("sweep_ctas", ctypes.c_int32),
     ]
 
 
@@ -451,7 +451,8 @@ class Pool:
         _check(st, what, allow=(OK, NOT_CONVERGED, NAN_DETECTED))
         out = dict(status=st, count=res.count, residual=res.residual, elapsed_ms=res.elapsed_ms,
                    sweep_ms=res.sweep_ms, sweep_launches=res.sweep_launches,
-                   bytes_moved=res.bytes_moved, kernel_launches=res.kernel_launches)
+                   bytes_moved=res.bytes_moved, kernel_launches=res.kernel_launches,
+                   uniform_blocks=res.uniform_blocks)
         if history:
             if res.count == 0:  # early exit: the residuals written before it
                 n = int(np.argmax(hist == 0)) if (hist == 0).any() else len(hist)
@@ -618,11 +619,13 @@ class Pool:
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
                     epsilon=1e-8, history=True, check_every=0, restart_drop=None,
                     restart_growth=None, restart_every=None, flux_correction=False,
-                    fp64_data=False, threads_per_block=0, stage_depth=0, sweep_threads=0):
+                    fp64_data=False, threads_per_block=0, stage_depth=0, sweep_threads=0,
+                    sweep_ctas=0):
         """Mixed-precision solve (FP64 BiCGSTAB; RB-SOR preconditioner on 32-bit data).
         flux_correction: the FP64 residual and A*x use the coarse-fine
         flux-conserving operator; fp64_data: the same preconditioner on FP64 data;
-        threads_per_block, stage_depth, sweep_threads: launch settings (0: defaults)."""
+        threads_per_block, stage_depth, sweep_threads, sweep_ctas: launch settings
+        (0: defaults)."""
         hist = np.zeros(max(count_max, 1), np.float64) if history else None
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
                           hist.ctypes.data if history else None,
@@ -630,7 +633,7 @@ class Pool:
         prm.flux_correction = int(bool(flux_correction))
         prm.fp64_data = int(bool(fp64_data))
         prm.threads_per_block, prm.stage_depth = int(threads_per_block), int(stage_depth)
-        prm.sweep_threads = int(sweep_threads)
+        prm.sweep_threads, prm.sweep_ctas = int(sweep_threads), int(sweep_ctas)
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -868,14 +871,14 @@ class Batch:
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
                     epsilon=1e-8, check_every=0, restart_drop=None, restart_growth=None,
                     restart_every=None, flux_correction=False, fp64_data=False,
-                    threads_per_block=0, stage_depth=0, sweep_threads=0):
+                    threads_per_block=0, stage_depth=0, sweep_threads=0, sweep_ctas=0):
         """Solves every admitted instance; returns the first instance's result."""
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
                           None, *_restart(restart_drop, restart_growth, restart_every))
         prm.flux_correction = int(bool(flux_correction))
         prm.fp64_data = int(bool(fp64_data))
         prm.threads_per_block, prm.stage_depth = int(threads_per_block), int(stage_depth)
-        prm.sweep_threads = int(sweep_threads)
+        prm.sweep_threads, prm.sweep_ctas = int(sweep_threads), int(sweep_ctas)
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -945,11 +948,11 @@ class Batch:
 
     def begin(self, inst, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
               epsilon=1e-8, restart_drop=None, restart_growth=None, restart_every=None,
-              threads_per_block=0, stage_depth=0, sweep_threads=0):
+              threads_per_block=0, stage_depth=0, sweep_threads=0, sweep_ctas=0):
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, 0, None,
                           *_restart(restart_drop, restart_growth, restart_every))
         prm.threads_per_block, prm.stage_depth = int(threads_per_block), int(stage_depth)
-        prm.sweep_threads = int(sweep_threads)
+        prm.sweep_threads, prm.sweep_ctas = int(sweep_threads), int(sweep_ctas)
         _check(lib().ffvgpu_mixed_begin(self._h, inst, ctypes.byref(prm)), "mixed_begin")
 
     def cancel(self, inst):

@@ -119,8 +119,9 @@ typedef struct {
   int32_t sweep_launches;/* number of launches sweep_ms covers */
   int64_t bytes_moved;   /* algorithmic HBM bytes of the solve */
   int32_t kernel_launches;
-  int32_t uniform_blocks;/* mixed form: blocks whose seven coefficients are the same in every
-                            cell, which its kernels read once per block; 0 otherwise */
+  int32_t uniform_blocks;/* RBGS and the mixed form: blocks whose seven coefficients are the
+                            same in every cell, which their kernels read once per block (the
+                            results are the same); 0 otherwise */
 } ffvgpu_result;
 
 /* ---- pool lifetime ------------------------------------------------------ */
@@ -417,6 +418,10 @@ typedef struct {
   int32_t sweep_threads;       /* CTA size of the sweep kernel: 512 (each thread a 4-cell
                                   column of one row) or 256 (of two rows); 0: 512; results
                                   do not depend on it */
+  int32_t sweep_ctas;          /* sweep CTAs per SM: 1 (a block's coefficient words staged
+                                  in shared memory) or 2 (read at use, so one CTA's staging
+                                  overlaps the other's sweeps); 0: 1; results do not depend
+                                  on it */
 } ffvgpu_mixed_params;
 
 /* Solves every admitted instance of the pool (a pool made from one grid is
@@ -575,6 +580,7 @@ typedef struct {
   int32_t threads_per_block;  /* as ffvgpu_mixed_params (0: 256) */
   int32_t stage_depth;        /* as ffvgpu_mixed_params (0: 1) */
   int32_t sweep_threads;      /* as ffvgpu_mixed_params (0: 512) */
+  int32_t sweep_ctas;         /* as ffvgpu_mixed_params (0: 1) */
 } ffvgpu_tune_record;
 
 ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* pool, const int32_t* instances,

@@ -64,9 +64,10 @@ def test_fp64_data_variant_bitwise_against_oracle(level, omega, sweeps, per, cou
     P.close()
 
 
-@pytest.mark.parametrize("threads,depth,sweep_threads", [(128, 1, 512), (512, 3, 512),
-                                                        (256, 2, 256), (128, 3, 256)])
-def test_launch_settings_do_not_change_results(threads, depth, sweep_threads):
+@pytest.mark.parametrize("threads,depth,sweep_threads,sweep_ctas", [
+    (128, 1, 512, 1), (512, 3, 512, 1), (256, 2, 256, 1), (128, 3, 256, 1),
+    (256, 1, 256, 2), (512, 2, 512, 2)])
+def test_launch_settings_do_not_change_results(threads, depth, sweep_threads, sweep_ctas):
     """CTA sizes of the A*x, update and sweep kernels and the sweep kernel's
     staging depth are tuning knobs only: the same bits as the defaults (the
     512-lane block tree and the 256-lane cross-block tree do not depend on
@@ -78,7 +79,7 @@ def test_launch_settings_do_not_change_results(threads, depth, sweep_threads):
     xr = interior(P.download("X", VC)).copy()
     P.fill("X", 0.0)
     r = P.solve_mixed(1.5, 8, 4, 4, 0.0, threads_per_block=threads, stage_depth=depth,
-                      sweep_threads=sweep_threads)
+                      sweep_threads=sweep_threads, sweep_ctas=sweep_ctas)
     assert_bitwise(r["history"], ref["history"], "residual history")
     assert_bitwise(interior(P.download("X", VC)), xr, "pressure")
     P.close()

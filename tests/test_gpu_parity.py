@@ -129,6 +129,13 @@ def test_rbgs_solve_bitwise(level, omega, sweeps):
     gg, rgd = fo.face_guides(got, VC, 2), fo.face_guides(O.field("X"), VC, 2)
     for f in range(6):
         assert_bitwise(gg[f], rgd[f], f"guides face {f}")
+    # blocks whose seven coefficients are bitwise the same in every cell stream
+    # b only (their coefficients come from one record): the count the solve
+    # reports is the oracle's A's
+    A = np.stack([interior(O.field(f)).reshape(g.nb, -1)
+                  for f in ("AP", "AW", "AE", "AS", "AN", "AB", "AT")]).view(np.int64)
+    n_uniform = int(np.all(A == A[:, :, :1], axis=(0, 2)).sum())
+    assert 0 < n_uniform < g.nb and rg["uniform_blocks"] == n_uniform
     P.close()
 
 
