@@ -78,6 +78,11 @@ def parse():
                     help="mixed form: only run this many iterations once (for ncu)")
     ap.add_argument("--profile-solver", default="mixed", choices=["mixed", "bicgstab"],
                     help="mixed form with --profile-iterations: the solve to run")
+    ap.add_argument("--profile-per-exchange", default="4",
+                    help="mixed form with --profile-iterations: comma-separated sweeps per "
+                         "exchange, each run with two passes per application")
+    ap.add_argument("--profile-fp64-data", action="store_true",
+                    help="mixed form with --profile-iterations: also the FP64-data variant")
     ap.add_argument("--level", type=int, default=5)
     ap.add_argument("--instances", type=int, default=64, help="batch form: instances")
     ap.add_argument("--fp64-sample", type=int, default=64,
@@ -493,9 +498,12 @@ def run_mixed(args):
             r = P.solve_bicgstab(FP64_SOLVER["omega"], FP64_SOLVER["pre_count"],
                                  args.profile_iterations, 0.0, history=False)
         else:
-            r = P.solve_mixed(MIXED["omega"], MIXED["sweeps"], MIXED["sweeps_per_exchange"],
-                              args.profile_iterations, 0.0, history=False,
-                              check_every=args.profile_iterations)
+            for per in (int(v) for v in args.profile_per_exchange.split(",")):
+                for d64 in ((False, True) if args.profile_fp64_data else (False,)):
+                    P.fill("X", 0.0)
+                    r = P.solve_mixed(MIXED["omega"], 2 * per, per, args.profile_iterations,
+                                      0.0, history=False, check_every=args.profile_iterations,
+                                      fp64_data=d64)
         P.close()
         return {"form": f"{args.profile_solver}-profile", "level": args.level,
                 "blocks": int(g.nb), "iterations": args.profile_iterations,
@@ -718,7 +726,7 @@ def run_batch(args):
     assert all(i is not None for i in ids)
 
     setting = dict(MIXED, iterations_per_replay=8, threads_per_block=256, stage_depth=1,
-                   sweep_threads=512)
+                   sweep_threads=512, matvec_form=0)
     tune = None
     if args.tune:
         # a sample spread over the instance sizes (every k-th by block count)
@@ -737,14 +745,15 @@ def run_batch(args):
                                  r["sweeps_per_exchange"] == MIXED["sweeps_per_exchange"] and
                                  r["iterations_per_replay"] == 8 and
                                  r["threads_per_block"] == 256 and r["stage_depth"] == 1 and
-                                 r["sweep_threads"] == 512), None)}
+                                 r["sweep_threads"] == 512 and r["matvec_form"] == 0), None)}
         if best >= 0:
             b = recs[best]
             setting = dict(omega=b["omega"], sweeps=b["sweeps"],
                            sweeps_per_exchange=b["sweeps_per_exchange"],
                            iterations_per_replay=b["iterations_per_replay"],
                            threads_per_block=b["threads_per_block"],
-                           stage_depth=b["stage_depth"], sweep_threads=b["sweep_threads"])
+                           stage_depth=b["stage_depth"], sweep_threads=b["sweep_threads"],
+                           matvec_form=b["matvec_form"])
 
     def batched():
         for i in ids:
@@ -753,7 +762,8 @@ def run_batch(args):
                              5000, 1e-8, check_every=setting["iterations_per_replay"],
                              threads_per_block=setting["threads_per_block"],
                              stage_depth=setting["stage_depth"],
-                             sweep_threads=setting["sweep_threads"])
+                             sweep_threads=setting["sweep_threads"],
+                             matvec_form=setting["matvec_form"])
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         for _ in range(max(1, args.warmup)):
@@ -775,7 +785,7 @@ def run_batch(args):
         setting["omega"], setting["sweeps"], setting["sweeps_per_exchange"], 5000, 1e-8,
         check_every=setting["iterations_per_replay"], fp64_data=True,
         threads_per_block=setting["threads_per_block"], stage_depth=setting["stage_depth"],
-        sweep_threads=setting["sweep_threads"]))
+        sweep_threads=setting["sweep_threads"], matvec_form=setting["matvec_form"]))
     res64 = [B.result(i) for i in ids]
     rbsor64 = {"solves_per_s": 1e3 * len(ids) / t64b, "ms": t64b,
                "iterations_min_max": [int(min(x["count"] for x in res64)),

@@ -31,14 +31,12 @@ struct MixCtx {
   int cf;              // coarse-fine flux correction in the FP64 residual and A*x
   int depth;           // sweep kernel: L2 prefetch distance in blocks (staging depth, >= 1)
   int sweep_threads;   // sweep kernel: 512 (a row per thread) or 256 (two rows per thread)
-  int sweep_ctas;      // sweep kernel: 1 CTA per SM (coefficient slot) or 2 (words read at use)
 };
 
 // CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel,
-// with 'threads' (128, 256 or 512) per CTA of the A*x and update kernels and
-// sweep_ctas (1 or 2) sweep CTAs per SM.
-void mx_grid_sizes(int threads, int sweep_ctas, int* sweep, int* matvec, int* update,
-                   int* guides);
+// with 'threads' (128, 256 or 512) per CTA of the A*x (form 1) and update
+// kernels; mvpipe: the pipelined A*x (one CTA per SM).
+void mx_grid_sizes(int threads, int* sweep, int* matvec, int* update, int* guides, int* mvpipe);
 // Sweep coefficients of blocks [first, first + count), MIXED_COEF_WORDS per
 // block, in the thread order of a sweep kernel of sweep_threads threads:
 // 32-bit words (FP64 high words, rounded) into coef, or with d64 (the
@@ -61,7 +59,9 @@ void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool 
 // Guide layer [blk][6][256] (FP64) of the iterate e for the next pass.
 void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const void* e, double* guides,
                       bool d64);
-void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads,
+// y = A x with its dot products; form 0: the pipelined kernel ('count' CTAs,
+// one per SM), form 1: a block per CTA of 'threads' threads.
+void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads, int form,
                       const void* x, const double* A, double* y, const double* w0, bool d64);
 // Coarse-fine flux mismatch per face cell of the (block, face) pairs
 // [npairs][2] of kind NB_FINE: out [npairs][256][2] = (delta, F).

@@ -124,10 +124,9 @@ ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P, bool d64) {
       CK(cudaEventCreateWithFlags(&P->act_ev[k], cudaEventDisableTiming));
       CK(cudaEventRecord(P->act_ev[k], P->stream));
     }
-    mx_grid_sizes(P->m_threads, P->m_sweep_ctas, &P->grid_sweep, &P->grid_matvec,
-                  &P->grid_update, &P->grid_guides);
+    mx_grid_sizes(P->m_threads, &P->grid_sweep, &P->grid_matvec, &P->grid_update,
+                  &P->grid_guides, &P->grid_mvpipe);
     P->grid_threads = P->m_threads;
-    P->grid_sweep_ctas = P->m_sweep_ctas;
   }
   if ((s = dalloc_t(P, &P->mcoef, 7 * n)) || (s = dalloc_t(P, &P->mguide, n / BC * 6 * 256)) ||
       (s = dalloc_t(P, &P->mucoef, n / BC * 8)) ||
@@ -179,7 +178,6 @@ MixCtx mix_ctx(const ffvgpu_pool* P) {
   C.cf = P->m_cf;
   C.depth = P->m_depth;
   C.sweep_threads = P->m_sweep_threads;
-  C.sweep_ctas = P->m_sweep_ctas;
   return C;
 }
 
@@ -216,7 +214,7 @@ ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
   if (prm->stage_depth < 0 || prm->stage_depth > 3) return bad("stage_depth must lie in 0..3");
   if (prm->sweep_threads != 0 && prm->sweep_threads != 256 && prm->sweep_threads != 512)
     return bad("sweep_threads must be 0, 256 or 512");
-  if (prm->sweep_ctas < 0 || prm->sweep_ctas > 2) return bad("sweep_ctas must be 0, 1 or 2");
+  if (prm->matvec_form != 0 && prm->matvec_form != 1) return bad("matvec_form must be 0 or 1");
   if (prm->threads_per_block != 0 && prm->threads_per_block != 128 &&
       prm->threads_per_block != 256 && prm->threads_per_block != 512)
     return bad("threads_per_block must be 0, 128, 256 or 512");
@@ -265,10 +263,11 @@ void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
                       rhs, P->q, P->mcoef, P->mcoef64, ein, P->mguide, last ? hat : e[ps & 1],
                       d64);
     }
+    const int mvc = P->m_mvform == 0 ? P->grid_mvpipe : P->grid_matvec;
     if (mode == 0)
-      launch_mx_matvec(s, C, P->grid_matvec, 1, P->m_threads, ph, P->A, P->q, P->r0, d64);
+      launch_mx_matvec(s, C, mvc, 1, P->m_threads, P->m_mvform, ph, P->A, P->q, P->r0, d64);
     else
-      launch_mx_matvec(s, C, P->grid_matvec, 2, P->m_threads, sh, P->A, P->tv, P->sv, d64);
+      launch_mx_matvec(s, C, mvc, 2, P->m_threads, P->m_mvform, sh, P->A, P->tv, P->sv, d64);
   }
   launch_mx_update(s, C, P->grid_update, P->m_threads, x, ph, sh, P->r, P->tv, P->sv, P->r0,
                    d64);
@@ -697,8 +696,7 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
                  (prm->flux_correction != 0) != (P->m_cf != 0) ||
                  (prm->fp64_data != 0) != (P->m_d64 != 0) ||
                  stage_depth_of(prm) != P->m_depth || threads_of(prm) != P->m_threads ||
-                 sweep_threads_of(prm) != P->m_sweep_threads ||
-                 (prm->sweep_ctas == 2 ? 2 : 1) != P->m_sweep_ctas))
+                 sweep_threads_of(prm) != P->m_sweep_threads || prm->matvec_form != P->m_mvform))
     return bad("running instances use other preconditioner settings");
   double *xp, *g;
   size_t stride;
@@ -714,13 +712,11 @@ ffvgpu_status ffvgpu_mixed_begin(ffvgpu_pool* P, int32_t inst, const ffvgpu_mixe
   P->m_depth = stage_depth_of(prm);
   P->m_threads = threads_of(prm);
   P->m_sweep_threads = sweep_threads_of(prm);
-  P->m_sweep_ctas = prm->sweep_ctas == 2 ? 2 : 1;
-  if (P->grid_threads != P->m_threads || P->grid_sweep_ctas != P->m_sweep_ctas) {
-    // the persistent grids of these CTA sizes
-    mx_grid_sizes(P->m_threads, P->m_sweep_ctas, &P->grid_sweep, &P->grid_matvec,
-                  &P->grid_update, &P->grid_guides);
+  P->m_mvform = prm->matvec_form;
+  if (P->grid_threads != P->m_threads) {  // the persistent grids of this CTA size
+    mx_grid_sizes(P->m_threads, &P->grid_sweep, &P->grid_matvec, &P->grid_update,
+                  &P->grid_guides, &P->grid_mvpipe);
     P->grid_threads = P->m_threads;
-    P->grid_sweep_ctas = P->m_sweep_ctas;
   }
   I->count_max = prm->count_max;
   I->epsilon = prm->epsilon;
@@ -775,7 +771,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
       P->mgraph_wait_ns != P->wait_ns || P->mgraph_stall != P->stall_sweep ||
       P->mgraph_cf != P->m_cf || P->mgraph_d64 != P->m_d64 ||
       P->mgraph_depth != P->m_depth || P->mgraph_threads != P->m_threads ||
-      P->mgraph_sweep_threads != P->m_sweep_threads || P->mgraph_sweep_ctas != P->m_sweep_ctas) {
+      P->mgraph_sweep_threads != P->m_sweep_threads || P->mgraph_mvform != P->m_mvform) {
     if (P->mgraph) cudaGraphExecDestroy(P->mgraph);
     P->mgraph = nullptr;
     cudaGraph_t graph;
@@ -796,7 +792,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
     P->mgraph_depth = P->m_depth;
     P->mgraph_threads = P->m_threads;
     P->mgraph_sweep_threads = P->m_sweep_threads;
-    P->mgraph_sweep_ctas = P->m_sweep_ctas;
+    P->mgraph_mvform = P->m_mvform;
   }
   CK(cudaGraphLaunch(P->mgraph, P->stream));
   P->m_launches += (int64_t)iterations * launches_per_iteration(P);
@@ -978,7 +974,7 @@ ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* P, const int32_t* instances, in
     prm.threads_per_block = R.threads_per_block;
     prm.stage_depth = R.stage_depth;
     prm.sweep_threads = R.sweep_threads;
-    prm.sweep_ctas = R.sweep_ctas;
+    prm.matvec_form = R.matvec_form;
     prm.history = nullptr;
     R.ms = 0.0;
     R.max_count = 0;

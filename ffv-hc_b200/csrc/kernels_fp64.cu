@@ -18,7 +18,6 @@
 #include <cstdio>
 #include <cuda_runtime.h>
 
-#include "ffvgpu_async.cuh"
 #include "ffvgpu_internal.cuh"
 #include "ffvgpu_kernels.h"
 
@@ -46,17 +45,6 @@ __device__ __forceinline__ int guide_tix(int f, int a, int b) {
     case Z_M: return tix(a, b, -1);
     default:  return tix(a, b, 16);
   }
-}
-
-// Brings 'arrays' consecutive block-sized arrays of block blk (stride
-// BLOCK_CELLS doubles, the first at base) into L2 from thread 0: issued at a
-// kernel's entry, so the loads of the compute loop find them there.
-__device__ __forceinline__ void prefetch_block(const double* base, int blk, int arrays,
-                                               size_t stride) {
-  if (threadIdx.x == 0)
-    for (int a = 0; a < arrays; ++a)
-      async::prefetch_l2(base + (size_t)blk * stride + (size_t)a * BLOCK_CELLS,
-                         BLOCK_CELLS * 8u);
 }
 
 // Stage block 'blk' of x in the shared tile, guide layer included.  The
@@ -155,8 +143,6 @@ jacobi_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
   if (solve_done(st)) return;
   __shared__ double xs[FROM_ZERO ? 1 : TILE];
   const int blk = blockIdx.x, tid = threadIdx.x;
-  prefetch_block(A, blk, 7, 7 * (size_t)BLOCK_CELLS);
-  prefetch_block(bvec, blk, 1, BLOCK_CELLS);
   if (!FROM_ZERO) {
     stage_tile(xs, xin, blk, C, nullptr);
     __syncthreads();
@@ -205,8 +191,6 @@ calc_r_kernel(KCtx C, const double* __restrict__ x, const double* __restrict__ g
   if (st && solve_done(st)) return;
   __shared__ double xs[TILE];
   const int blk = blockIdx.x, tid = threadIdx.x;
-  prefetch_block(A, blk, 7, 7 * (size_t)BLOCK_CELLS);
-  prefetch_block(bvec, blk, 1, BLOCK_CELLS);
   stage_tile(xs, x, blk, C, gst);
   __syncthreads();
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
@@ -247,8 +231,6 @@ ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A
   if (solve_done(st)) return;
   __shared__ double xs[TILE];
   const int blk = blockIdx.x, tid = threadIdx.x;
-  prefetch_block(A, blk, 7, 7 * (size_t)BLOCK_CELLS);
-  if (y) prefetch_block(y, blk, 1, BLOCK_CELLS);
   stage_tile(xs, p, blk, C, nullptr);
   __syncthreads();
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;

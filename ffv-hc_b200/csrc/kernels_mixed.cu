@@ -64,9 +64,6 @@ constexpr int TILE = 2 * SH;
 constexpr int COEF_WORDS = 7 * BLOCK_CELLS;  // coefficient words of one block
 constexpr int GUIDES = 6 * FACE_CELLS;  // guide values of one block (FP64)
 constexpr int SWEEP_SMEM = COEF_WORDS * 4 + TILE * 8 + BLOCK_CELLS * 8 + GUIDES * 8 + 16;
-// Two CTAs per SM (DUAL): no coefficient slot; a block's 32-bit words are
-// read at use from global memory (L2) and a first pass reads its vectors there.
-constexpr int SWEEP_SMEM_DUAL = TILE * 8 + BLOCK_CELLS * 8 + GUIDES * 8 + 16;
 
 // Sweep-kernel geometry for PTS threads per CTA (512 or 256).  Thread t owns
 // the cells (i, j, k) with i in {2 ih, 2 ih + 1}, j = JJ jp + jj (jj < JJ
@@ -432,43 +429,26 @@ mx_init_kernel(MixCtx C, const double* __restrict__ x, const double* __restrict_
 // coefficients in thread order ([a][m][thread], c64 already offset to this
 // thread).  For one data format the values, and so the results, do not
 // depend on the source.
-enum { CS_UNI = 0, CS_W32 = 1, CS_G64 = 2, CS_G32 = 3 };
-__device__ __forceinline__ uint32_t quad_word(const uint4& q, int h) {
-  return h == 0 ? q.x : (h == 1 ? q.y : (h == 2 ? q.z : q.w));
-}
+enum { CS_UNI = 0, CS_W32 = 1, CS_G64 = 2 };
 // PTS threads: the cells m = (c JJ + jj) 4 + h of a thread (SweepGeom).  Of a
 // cell's six neighbours (all of the other colour) the x neighbour at the same
 // ih, the z neighbours inside the 4-cell column and, with two rows per thread
 // (PTS 256), the y neighbour in the thread's other row are its own registers;
 // the rest come from the tile.  The terms keep rbgs_smoother's order (w, e,
 // s, n, b, t) whatever their source, so every PTS gives the same bits.
-// CS_G32 (two CTAs per SM, no slot): the cell's 32-bit words are read at use
-// from global memory, the four cells (h) of a row as one 16-byte vector per
-// coefficient (c32q: the block's words as vectors, offset to this thread).
-// RREG: a uniform block keeps its right-hand side in registers (off where
-// the registers are short: two CTAs per SM).
-template <int CS, int PTS, bool RREG = true>
+template <int CS, int PTS>
 __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, int p0,
                                            double (&E)[2][SweepGeom<PTS>::JJ][4],
                                            const uint32_t (&cw)[SweepGeom<PTS>::CPT][7],
                                            const double (&ku)[7],
-                                           const double* __restrict__ c64,
-                                           const uint4* __restrict__ c32q, double mom,
+                                           const double* __restrict__ c64, double mom,
                                            int nsweep) {
-  constexpr bool UNI = CS == CS_UNI && RREG;
+  constexpr bool UNI = CS == CS_UNI;
   constexpr int JJ = SweepGeom<PTS>::JJ, CPT = SweepGeom<PTS>::CPT;
-  uint4 cq[JJ];
 #define MX_COEF(m, a)                                          \
   (CS == CS_UNI ? ku[a]                                        \
    : CS == CS_W32 ? widen_here(cw[m][a])                       \
-   : CS == CS_G64 ? __ldg(c64 + ((a) * CPT + (m)) * PTS)        \
-                  : widen(quad_word(cq[((m) >> 2) % JJ], (m) & 3)))
-  // the vectors of coefficient a of this colour's rows (CS_G32)
-#define MX_LOADQ(a)                                                               \
-  if (CS == CS_G32) {                                                             \
-    _Pragma("unroll") for (int jq = 0; jq < JJ; ++jq)                             \
-      cq[jq] = __ldg(c32q + ((a) * (CPT / 4) + c * JJ + jq) * PTS);               \
-  }
+                  : __ldg(c64 + ((a) * CPT + (m)) * PTS))
   // a uniform block has the registers to keep its right-hand side too (one
   // shared-memory read less per update)
   double vr[2][JJ][4];
@@ -497,7 +477,6 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
           rc[jj][h] = UNI ? vr[c][jj][h] : V[((c * JJ + jj) * 4 + h) * PTS];
         }
 #define MX_M(jj, h) ((c * JJ + (jj)) * 4 + (h))
-      MX_LOADQ(0)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
@@ -506,7 +485,6 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 0), par ? E[1 - c][jj][h] : xo[jj][h],
                                rc[jj][h]);
         }
-      MX_LOADQ(1)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
@@ -515,14 +493,12 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 1), par ? xo[jj][h] : E[1 - c][jj][h],
                                rc[jj][h]);
         }
-      MX_LOADQ(2)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
         for (int h = 0; h < 4; ++h)
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 2),
                                jj > 0 ? E[1 - c][jj - 1][h] : O[jj * SP + h * SQ - SP], rc[jj][h]);
-      MX_LOADQ(3)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
@@ -530,21 +506,18 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 3),
                                jj < JJ - 1 ? E[1 - c][jj + 1][h] : O[jj * SP + h * SQ + SP],
                                rc[jj][h]);
-      MX_LOADQ(4)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
         for (int h = 0; h < 4; ++h)
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 4),
                                h > 0 ? E[1 - c][jj][h - 1] : O[jj * SP - SQ], rc[jj][h]);
-      MX_LOADQ(5)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
         for (int h = 0; h < 4; ++h)
           rc[jj][h] = __fma_rn(-MX_COEF(MX_M(jj, h), 5),
                                h < 3 ? E[1 - c][jj][h + 1] : O[jj * SP + 4 * SQ], rc[jj][h]);
-      MX_LOADQ(6)
 #pragma unroll
       for (int jj = 0; jj < JJ; ++jj)
 #pragma unroll
@@ -561,7 +534,6 @@ __device__ __forceinline__ void run_sweeps(double* T, const double* V, int o0, i
   }
 }
 #undef MX_COEF
-#undef MX_LOADQ
 
 // Tile address of the guide cell at position p (u + 16 v) of a face.
 __device__ __forceinline__ int guide_slot(int face, int p) {
@@ -583,15 +555,16 @@ constexpr int LF_UNI = 1 << 30;          // the block is uniform (MixCtx::ucoef)
 constexpr int LF_COPY = 1 << 29;         // its instance starts a cycle (p = r, r0 = r)
 constexpr int LF_INST = LF_COPY - 1;
 
-// Called by every thread: fills list[0, *n) from the candidates from, from +
-// gridDim.x, ... (LIST_CAP of them, in item order) and sets *next to the
-// first candidate after them.
-template <int MODE, bool FIRST, int PTS>
+// Called by every thread of a CTA of PTS: fills list[0, *n) from the
+// candidates from, from + gridDim.x, ... (CAP of them, in item order) and
+// sets *next to the first candidate after them.
+template <int MODE, bool FIRST, int PTS, int CAP = LIST_CAP>
 __device__ void build_live_list(const MixCtx& C, int from, int n_act, int2* list, int* n,
                                 int* next, int* wcount) {
+  static_assert(CAP % PTS == 0, "whole rounds of candidates");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int base = 0;
-  for (int r = 0; r < LIST_CAP / PTS; ++r) {
+  for (int r = 0; r < CAP / PTS; ++r) {
     const int it = from + (r * PTS + tid) * gridDim.x;
     int b = -1, e = 0;
     bool live = false;
@@ -618,18 +591,15 @@ __device__ void build_live_list(const MixCtx& C, int from, int n_act, int2* list
   }
   if (tid == 0) {
     *n = base;
-    *next = from + LIST_CAP * gridDim.x;
+    *next = from + CAP * gridDim.x;
   }
   __syncthreads();
 }
 
 // ET: the iterate between passes, float (the mixed form) or double (the
 // FP64-data variant, whose coefficients are FP64 too and read at use).
-// DUAL: two CTAs per SM (no coefficient slot: a block's words are read at
-// use and a first pass reads its vectors from global memory, prefetched into
-// L2), so one CTA's staging and barriers overlap the other's sweeps.
-template <int MODE, bool FIRST, typename ET, int PTS, bool DUAL>
-__global__ void __launch_bounds__(PTS, DUAL ? 2 : 1)
+template <int MODE, bool FIRST, typename ET, int PTS>
+__global__ void __launch_bounds__(PTS, 1)
 mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
                 double* __restrict__ r0, double* __restrict__ pv, const double* __restrict__ q,
                 const uint32_t* __restrict__ coef, const double* __restrict__ coef64,
@@ -638,10 +608,9 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
   constexpr bool D64 = sizeof(ET) == 8;
   constexpr int JJ = SweepGeom<PTS>::JJ, CPT = SweepGeom<PTS>::CPT;
   extern __shared__ __align__(128) unsigned char smem[];
-  constexpr int SLOT_BYTES = DUAL ? 0 : COEF_WORDS * 4;
-  uint32_t* slot = reinterpret_cast<uint32_t*>(smem);  // not used with DUAL
-  double* T = reinterpret_cast<double*>(smem + SLOT_BYTES);
-  double* V = reinterpret_cast<double*>(smem + SLOT_BYTES + TILE * 8);  // [m][t] rhs
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem);
+  double* T = reinterpret_cast<double*>(smem + COEF_WORDS * 4);
+  double* V = reinterpret_cast<double*>(smem + COEF_WORDS * 4 + TILE * 8);  // [m][t] rhs
   double* GB = V + BLOCK_CELLS;  // [face][p] guides of the block, copied with its coefficients
   uint64_t* bar = reinterpret_cast<uint64_t*>(GB + GUIDES);
   __shared__ int2 s_list[LIST_CAP];
@@ -672,10 +641,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     constexpr uint32_t UB = 8 * 8;            // bytes of a coefficient record
     double* sd = reinterpret_cast<double*>(slot);
     if (uni) {
-      if (FIRST && DUAL) {  // its vectors are read from global memory
-        async::mbar_expect_tx(bar, UB);
-        async::bulk_g2s(s_urec[p], C.ucoef + (size_t)b * 8, UB, bar);
-      } else if (FIRST) {
+      if (FIRST) {
         const bool copy = e.y & LF_COPY;
         const bool needq = !copy, needp = MODE == 0 && !copy;
         async::mbar_expect_tx(bar, UB + VB + (needq ? VB : 0u) + (needp ? VB : 0u));
@@ -690,8 +656,8 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       }
       return;
     }
-    if (D64 || DUAL) {
-      // the coefficients are read at use (prefetched into L2); the copy
+    if (D64) {
+      // FP64 coefficients are read at use (prefetched into L2); the copy
       // brings the guide layer only
       if (FIRST) {
         async::mbar_arrive(bar);
@@ -716,7 +682,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     if (!uni) {
       if (D64)
         async::prefetch_l2(coef64 + (size_t)b * COEF_WORDS, COEF_WORDS * 8u);
-      else if (DUAL || depth > 1)
+      else if (depth > 1)
         async::prefetch_l2(coef + (size_t)b * COEF_WORDS, COEF_WORDS * 4u);
     }
     if (FIRST) {
@@ -774,10 +740,9 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       const SolveState* S = C.inst.st + inst;
       const bool copy = ent.y & LF_COPY;  // first iteration of a (re)start: p = r, r0 = r
       const double mgamma = -S->gamma, beta = S->beta, malpha = -S->alpha;
-      const bool slotted = uni && !DUAL;  // its vectors came with its copy
-      const double* rs = slotted ? sd : r + gbase;
-      const double* qs = slotted ? sd + BLOCK_CELLS : q + gbase;
-      const double* ps = slotted ? sd + 2 * BLOCK_CELLS : pv + gbase;
+      const double* rs = uni ? sd : r + gbase;
+      const double* qs = uni ? sd + BLOCK_CELLS : q + gbase;
+      const double* ps = uni ? sd + 2 * BLOCK_CELLS : pv + gbase;
 #pragma unroll
       for (int c = 0; c < 2; ++c)
 #pragma unroll
@@ -831,7 +796,7 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
         for (int a = 0; a < 6; ++a) ku[a] = widen(hi_round(U[1 + a]));
         ku[6] = widen(hi_round(1.0 / U[0]));
       }
-    } else if (!D64 && !DUAL) {
+    } else if (!D64) {
 #pragma unroll
       for (int a = 0; a < 7; ++a)
 #pragma unroll
@@ -883,16 +848,12 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     }
     pos = npos;
     const double* c64 = D64 ? coef64 + (size_t)blk * COEF_WORDS + tid : nullptr;
-    const uint4* c32q =
-        reinterpret_cast<const uint4*>(coef + (size_t)blk * COEF_WORDS) + tid;
     if (uni)
-      run_sweeps<CS_UNI, PTS, !DUAL>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, c32q, mom, nsweep);
+      run_sweeps<CS_UNI, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, mom, nsweep);
     else if constexpr (D64)
-      run_sweeps<CS_G64, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, c32q, mom, nsweep);
-    else if constexpr (DUAL)
-      run_sweeps<CS_G32, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, c32q, mom, nsweep);
+      run_sweeps<CS_G64, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, mom, nsweep);
     else
-      run_sweeps<CS_W32, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, c32q, mom, nsweep);
+      run_sweeps<CS_W32, PTS>(T, V + tid, o0, j0 & 1, E, cw, ku, c64, mom, nsweep);
 #pragma unroll
     for (int c = 0; c < 2; ++c)
 #pragma unroll
@@ -1031,6 +992,369 @@ mx_matvec_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// The same A*x and dot products as a persistent, warp-specialised kernel:
+// one CTA of 800 threads per SM walks its live blocks while bulk copies
+// bring the next ones into shared memory.
+//   producer (thread 0): per block its x (FP32 into the upper half of a
+//     tile buffer, or FP64 into all of it) and, for a uniform block, its
+//     coefficient record, a block ahead; and through a ring of three 32 KB
+//     slots the dot partner w0 (a uniform block: all of it in one slot) or,
+//     for a block that streams its coefficients, eight slots of 512 cells
+//     with the seven coefficient rows and w0.
+//   gatherers (8 warps): the block's guide layer by the exchange rules
+//     (loads issued before its x lands), then an FP32 x widened to FP64 in
+//     place.
+//   consumers (16 warps): consumer t takes cells q = 512 mm + t of each
+//     colour, which makes it the block tree's virtual thread t: the per-block
+//     sums are those of mx_reduce; the ticket of an instance is advanced once
+//     per run of its blocks in the CTA's list, and the CTA that completes it
+//     forms the cross-block sums (256 lanes, block order) and finalises.
+// Every wait is bounded (MixCtx::wait_ns); a wait that gives up stops the
+// instances of the CTA's list with TIMEOUT.
+// ---------------------------------------------------------------------------
+namespace mvp {
+constexpr int STAGES = 3;
+constexpr int ROWS = 8;                            // A rows 0..6 (Ap, Aw..At), w0
+constexpr int SLOT_CELLS = 512;
+constexpr int SLOTS = BLOCK_CELLS / SLOT_CELLS;    // slots of a streamed block
+constexpr uint32_t SLOT_BYTES = ROWS * SLOT_CELLS * 8;
+constexpr int X_ISSUE_AT = SLOTS / 2;              // slot of block n after which x(n+1) is issued
+constexpr int GATHER0 = 32, NGATHER = 256;
+constexpr int CONS0 = GATHER0 + NGATHER, NCONS = 512, CONS_WARPS = NCONS / 32;
+constexpr int NTHREADS = CONS0 + NCONS;            // 800
+constexpr int CAP = NTHREADS;                      // list entries per chunk
+constexpr int ROLE_MATVEC = 32;                    // SolveState::timeout_where bit
+static_assert(SLOT_BYTES == BLOCK_CELLS * 8, "a slot holds a uniform block's w0");
+
+struct __align__(128) Smem {
+  double ring[STAGES][ROWS][SLOT_CELLS];  // 96 KB
+  double tile[2][BLOCK_CELLS];            // 64 KB: x of the current / next block, FP64
+  double gbuf[2][GUIDES];                 // 24 KB: their guide layers, [face][v][u]
+  double urec[2][8];                      // coefficient records of uniform blocks
+  double ws[2][CONS_WARPS];               // warp sums of the block tree
+  int2 list[CAP];                         // the chunk's live entries
+  FaceNbr snb[2][6];                      // face records (flux correction)
+  uint64_t full[STAGES], empty[STAGES], xfull[2], xempty[2], gfull[2], gempty[2];
+  int wcount[NTHREADS / 32];
+  int nlist, next_from, abort_flag, last_inst;
+};
+
+__device__ __forceinline__ void consumer_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(NCONS) : "memory");
+}
+__device__ __forceinline__ void gather_sync() {
+  asm volatile("bar.sync 2, %0;" ::"n"(NGATHER) : "memory");
+}
+__device__ __forceinline__ void release_slot(uint64_t* bar, int lane, bool live) {
+  async::fence_proxy_async();
+  __syncwarp();
+  if (lane == 0 && live) async::mbar_arrive(bar);
+}
+}  // namespace mvp
+
+template <int NV, bool CF, typename ET>
+__global__ void __launch_bounds__(mvp::NTHREADS, 1)
+mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ A,
+                      double* __restrict__ y, const double* __restrict__ w0) {
+  using namespace mvp;
+  using async::mbar_wait;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+  const int tid = threadIdx.x;
+  volatile int* abort_flag = &S.abort_flag;
+  const int n_act = *C.n_active;
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      async::mbar_init(&S.full[s], 1);
+      async::mbar_init(&S.empty[s], CONS_WARPS);
+    }
+    for (int b = 0; b < 2; ++b) {
+      async::mbar_init(&S.xfull[b], 1);
+      async::mbar_init(&S.xempty[b], 1);
+      async::mbar_init(&S.gfull[b], NGATHER);
+      async::mbar_init(&S.gempty[b], 1);
+    }
+    S.abort_flag = 0;
+    async::fence_mbar_init();
+  }
+  // Counters that run across the chunks: ring slots issued (producer) or
+  // consumed (consumers), x copies per tile buffer, blocks of earlier chunks.
+  uint32_t g = 0;
+  uint32_t nx[2] = {0, 0};
+  int M0 = 0;
+  int run = 0;  // consumer 0: blocks of the current instance not yet on its ticket
+  bool live = true;
+  for (int from = blockIdx.x; from < n_act;) {
+    build_live_list<1, false, NTHREADS, CAP>(C, from, n_act, S.list, &S.nlist, &S.next_from,
+                                             S.wcount);
+    from = S.next_from;
+    const int nl = S.nlist;
+    auto is_uni = [&](int n) { return (S.list[n].y & LF_UNI) != 0; };
+    auto nslots = [&](int n) { return is_uni(n) ? 1 : SLOTS; };
+    if (tid == 0 && nl > 0 && !*abort_flag) {
+      // ------------------------------------------------------------ producer
+      int pm = 0, pj = 0, xn = 0;  // next slot: block pm, slot pj; x copies issued
+      auto issue_slot = [&](int n, int j) {
+        const int s = g % STAGES;
+        const size_t blk = (size_t)S.list[n].x;
+        async::mbar_expect_tx(&S.full[s], SLOT_BYTES);
+        if (is_uni(n)) {
+          async::bulk_g2s(S.ring[s], w0 + blk * BLOCK_CELLS, SLOT_BYTES, &S.full[s]);
+        } else {
+#pragma unroll 1
+          for (int a = 0; a < 7; ++a)
+            async::bulk_g2s(S.ring[s][a], A + (blk * 7 + a) * BLOCK_CELLS + j * SLOT_CELLS,
+                            SLOT_CELLS * 8, &S.full[s]);
+          async::bulk_g2s(S.ring[s][7], w0 + blk * BLOCK_CELLS + j * SLOT_CELLS,
+                          SLOT_CELLS * 8, &S.full[s]);
+        }
+      };
+      // x(n) follows slot x_at(n-1) of block n-1 (the middle of a streamed
+      // block, the only slot of a uniform one): every slot of block n-2 is
+      // issued by then, so the wait for its tile buffer needs nothing more
+      // from the producer.
+      auto issue_xs = [&]() {
+        while (xn < nl) {
+          if (xn > 0) {
+            const int m = xn - 1, x_at = nslots(m) == 1 ? 0 : X_ISSUE_AT;
+            if (!(pm > m || (pm == m && pj > x_at))) break;
+          }
+          const int Mg = M0 + xn, xb = Mg & 1;
+          if (Mg >= 2 && !mbar_wait(&S.xempty[xb], ((Mg - 2) >> 1) & 1, abort_flag,
+                                    ROLE_MATVEC, C.wait_ns))
+            return false;
+          const size_t blk = (size_t)S.list[xn].x;
+          const bool u = is_uni(xn);
+          constexpr uint32_t XB = BLOCK_CELLS * (uint32_t)sizeof(ET);
+          async::mbar_expect_tx(&S.xfull[xb], XB + (u ? 64u : 0u));
+          async::bulk_g2s(sizeof(ET) == 4 ? (void*)(S.tile[xb] + HALF_CELLS) : (void*)S.tile[xb],
+                          x + blk * BLOCK_CELLS, XB, &S.xfull[xb]);
+          if (u) async::bulk_g2s(S.urec[xb], C.ucoef + blk * 8, 64, &S.xfull[xb]);
+          ++nx[xb];
+          ++xn;
+        }
+        return true;
+      };
+      bool ok = issue_xs();
+      while (ok && pm < nl) {
+        const int s = g % STAGES;
+        if (!(ok = mbar_wait(&S.empty[s], ((g / STAGES) & 1) ^ 1, abort_flag, ROLE_MATVEC,
+                             C.wait_ns)))
+          break;
+        issue_slot(pm, pj);
+        ++g;
+        if (++pj == nslots(pm)) {
+          pj = 0;
+          ++pm;
+        }
+        ok = issue_xs();
+      }
+    } else if (tid >= GATHER0 && tid < CONS0) {
+      // ----------------------------------------------------------- gatherers
+      const int gt = tid - GATHER0, grp = gt >> 7, p0 = gt & 127, p1 = p0 + 128;
+      for (int n = 0; n < nl; ++n) {
+        const int Mg = M0 + n, b = Mg & 1;
+        if (Mg >= 2 &&
+            !mbar_wait(&S.gempty[b], ((Mg - 2) >> 1) & 1, abort_flag, ROLE_MATVEC, C.wait_ns))
+          break;
+        const int blk = S.list[n].x;
+        const double dx = C.dx[blk];
+        // two groups of 128 threads take alternate faces, two positions each
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          const int f = 2 * r + grp;
+          const FaceNbr nf = C.nbr[blk * 6 + f];
+          double v0, v1;
+          guide_pair(x, blk, f, p0, p1, nf, C.bc, dx, v0, v1);
+          S.gbuf[b][f * FACE_CELLS + p0] = v0;
+          S.gbuf[b][f * FACE_CELLS + p1] = v1;
+          if (CF && p0 == 0) S.snb[b][f] = nf;
+        }
+        if (!mbar_wait(&S.xfull[b], (Mg >> 1) & 1, abort_flag, ROLE_MATVEC, C.wait_ns)) break;
+        if (sizeof(ET) == 4) {
+          // widened in place: every thread holds its 16 values before any
+          // FP64 value overwrites them
+          const float4* src = reinterpret_cast<const float4*>(S.tile[b] + HALF_CELLS);
+          float4 v[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) v[k] = src[gt + NGATHER * k];
+          gather_sync();
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            double2* d = reinterpret_cast<double2*>(S.tile[b] + 4 * (gt + NGATHER * k));
+            d[0] = make_double2((double)v[k].x, (double)v[k].y);
+            d[1] = make_double2((double)v[k].z, (double)v[k].w);
+          }
+        }
+        async::fence_proxy_async();  // the tile is refilled by bulk copies
+        async::mbar_arrive(&S.gfull[b]);
+      }
+    } else if (tid >= CONS0) {
+      // ----------------------------------------------------------- consumers
+      // Every consumer runs the same sequence of named barriers and shuffles;
+      // only the work is predicated on 'live'.
+      const int ct = tid - CONS0, lane = ct & 31, warp = ct >> 5;
+      for (int n = 0; n < nl; ++n) {
+        const int Mg = M0 + n, b = Mg & 1;
+        const uint32_t par = (Mg >> 1) & 1;
+        const int2 ent = S.list[n];
+        const int blk = ent.x, inst = ent.y & LF_INST;
+        const bool uni = ent.y & LF_UNI;
+        live = live && mbar_wait(&S.xfull[b], par, abort_flag, ROLE_MATVEC, C.wait_ns);
+        live = live && mbar_wait(&S.gfull[b], par, abort_flag, ROLE_MATVEC, C.wait_ns);
+        const double* T = S.tile[b];
+        const double* G = S.gbuf[b];
+        double u[7];
+#pragma unroll
+        for (int a = 0; a < 7; ++a) u[a] = uni ? S.urec[b][a] : 0.0;
+        const int us = g % STAGES;
+        if (uni)
+          live = live && mbar_wait(&S.full[us], (g / STAGES) & 1, abort_flag, ROLE_MATVEC,
+                                   C.wait_ns);
+        const double* wflat = &S.ring[us][0][0];
+        const size_t base = (size_t)blk * BLOCK_CELLS;
+        double acc[NV][2] = {};
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+#pragma unroll 1
+          for (int mm = 0; mm < SLOTS / 2; ++mm) {
+            const int q = mm * NCONS + ct, s = c * HALF_CELLS + q;
+            double k[7], wv = 0.0;
+            if (uni) {
+#pragma unroll
+              for (int a = 0; a < 7; ++a) k[a] = u[a];
+              if (live) wv = wflat[s];
+            } else {
+              const int sl = g % STAGES;
+              live = live && mbar_wait(&S.full[sl], (g / STAGES) & 1, abort_flag, ROLE_MATVEC,
+                                       C.wait_ns);
+#pragma unroll
+              for (int a = 0; a < 7; ++a) k[a] = live ? S.ring[sl][a][ct] : 0.0;
+              if (live) wv = S.ring[sl][7][ct];
+              asm volatile("" ::"d"(k[0]), "d"(k[1]), "d"(k[2]), "d"(k[3]), "d"(k[4]), "d"(k[5]),
+                           "d"(k[6]), "d"(wv));
+              release_slot(&S.empty[sl], lane, live);
+              ++g;
+            }
+            if (!live) continue;
+            const Nbrs v = split_neighbours(T + (1 - c) * HALF_CELLS, G, q, c);
+            double yv = k[1] * v.w + k[2] * v.e + k[3] * v.s + k[4] * v.n + k[5] * v.b +
+                        k[6] * v.t + k[0] * T[s];
+            if (CF)  // coarse-fine flux correction: y = A x + delta
+              yv = cf_delta<false>(x, (const double*)nullptr, A, C.nbr, C.dx, C.bc, S.snb[b], G,
+                                   T[s], s, yv, [&](int f) { return k[1 + f]; });
+            y[base + s] = yv;
+            acc[0][c] += yv * wv;
+            if (NV == 2) acc[NV - 1][c] += yv * yv;
+          }
+        }
+        if (uni) {  // w0 is in registers (the loads completed before its use)
+          release_slot(&S.empty[us], lane, live);
+          ++g;
+        }
+        // block tree (mx_reduce with 512 threads): warp butterflies, then the
+        // 16 warp sums in order
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          double t = acc[v][0] + acc[v][1];
+#pragma unroll
+          for (int off = 16; off >= 1; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+          if (lane == 0) S.ws[v][warp] = t;
+        }
+        async::fence_proxy_async();  // the tile is refilled by bulk copies
+        consumer_sync();
+        if (ct == 0 && live) {
+          async::mbar_arrive(&S.xempty[b]);
+          async::mbar_arrive(&S.gempty[b]);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            double sum = 0.0;
+#pragma unroll
+            for (int w = 0; w < CONS_WARPS; ++w) sum += S.ws[v][w];
+            __stcg(C.partials + (size_t)v * C.capacity + blk, sum);
+          }
+          ++run;
+        }
+        // the instance's ticket, once per run of its blocks in this chunk
+        if (n + 1 == nl || (S.list[n + 1].y & LF_INST) != inst) {
+          if (ct == 0) {
+            int li = -1;
+            if (live && run > 0) {
+              __threadfence();
+              const unsigned t = atomicAdd(&C.inst.st[inst].ticket, (unsigned)run);
+              if (t + (unsigned)run == (unsigned)C.inst.count[inst]) li = inst;
+            }
+            run = 0;
+            S.last_inst = li;
+          }
+          consumer_sync();
+          const int li = S.last_inst;
+          if (li >= 0) {
+            // cross-block sums over the instance's blocks: lanes 0..255, block
+            // order, butterfly, 8 warp sums in order
+            __threadfence();
+            const int first = C.inst.first[li], cnt = C.inst.count[li];
+            double tot[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+              double sv = 0.0;
+              if (ct < 256)
+                for (int bb = ct; bb < cnt; bb += 256)
+                  sv += __ldcg(C.partials + (size_t)v * C.capacity + first + bb);
+#pragma unroll
+              for (int off = 16; off >= 1; off >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, off);
+              consumer_sync();
+              if (lane == 0 && ct < 256) S.ws[0][ct >> 5] = sv;
+              consumer_sync();
+              double total = 0.0;
+#pragma unroll
+              for (int w = 0; w < 8; ++w) total += S.ws[0][w];
+              tot[v] = total;
+            }
+            if (ct == 0) {
+              SolveState* St = C.inst.st + li;
+              mx_finalize(St, tot, NV == 1 ? FIN_MX_ALPHA : FIN_MX_GAMMA);
+              St->ticket = 0;
+              __threadfence();
+            }
+            consumer_sync();  // S.ws is rewritten by the next block
+          }
+        }
+      }
+    }
+    M0 += nl;
+    __syncthreads();  // every role is past the chunk before its list is rebuilt
+    if (*abort_flag) break;
+  }
+  if (tid == 0) {
+    // Drain: the last armed phase of every barrier a copy completes on must
+    // complete before the CTA may exit (each has at most one copy phase in
+    // flight: a buffer is refilled only after its copy landed and was used).
+    bool drained = true;
+    for (int s = 0; s < STAGES; ++s) {
+      const uint32_t issued = (g > (uint32_t)s) ? (g - 1 - s) / STAGES + 1 : 0;
+      if (issued) drained = async::mbar_drain(&S.full[s], (issued - 1) & 1) && drained;
+    }
+    for (int b = 0; b < 2; ++b)
+      if (nx[b]) drained = async::mbar_drain(&S.xfull[b], (nx[b] - 1) & 1) && drained;
+    if (*abort_flag) {
+      // stop every instance of this CTA's chunk and of its later candidates
+      const int where = *abort_flag | (drained ? 0 : async::ROLE_DRAIN);
+      auto stop = [&](int i2) {
+        atomicOr(&C.inst.st[i2].timeout_where, where);
+        atomicExch(&C.inst.st[i2].status, 3);
+        atomicExch(&C.inst.st[i2].done, 1);
+      };
+      for (int k = 0; k < S.nlist; ++k) stop(S.list[k].y & LF_INST);
+      for (int it2 = S.next_from; it2 < n_act; it2 += gridDim.x) {
+        const int i2 = C.inst.blk_inst[C.active[it2]];
+        if (i2 >= 0) stop(i2);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // x = alpha*p_ + gamma*s_ + x (axpbypz, blas.f90:431-464, FFVILS.h:938-944);
 // r = (-gamma)*t_ + s (axpyz, blas.f90:397-429, FFVILS.h:945-950); r.r and
 // the next iteration's r.r0.
@@ -1128,20 +1452,14 @@ static void sweep_launch(cudaStream_t s, const MixCtx& C, int count, float omega
                          const double* r, double* r0, double* pv, const double* q,
                          const uint32_t* coef, const double* coef64, const void* ein,
                          const double* guides, void* eout) {
-#define MX_GO(PTS, DUAL)                                                                  \
-  mx_sweep_kernel<MODE, FIRST, ET, PTS, DUAL><<<count, PTS, DUAL ? SWEEP_SMEM_DUAL : SWEEP_SMEM, \
-                                                s>>>(C, omega, nsweep, r, r0, pv, q, coef,      \
-                                                     coef64, static_cast<const ET*>(ein),       \
-                                                     guides, static_cast<ET*>(eout), C.depth)
-  if (C.sweep_threads == 256 && C.sweep_ctas == 2)
-    MX_GO(256, true);
-  else if (C.sweep_threads == 256)
-    MX_GO(256, false);
-  else if (C.sweep_ctas == 2)
-    MX_GO(512, true);
+  if (C.sweep_threads == 256)
+    mx_sweep_kernel<MODE, FIRST, ET, 256><<<count, 256, SWEEP_SMEM, s>>>(
+        C, omega, nsweep, r, r0, pv, q, coef, coef64, static_cast<const ET*>(ein), guides,
+        static_cast<ET*>(eout), C.depth);
   else
-    MX_GO(512, false);
-#undef MX_GO
+    mx_sweep_kernel<MODE, FIRST, ET, 512><<<count, 512, SWEEP_SMEM, s>>>(
+        C, omega, nsweep, r, r0, pv, q, coef, coef64, static_cast<const ET*>(ein), guides,
+        static_cast<ET*>(eout), C.depth);
 }
 
 void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool first,
@@ -1173,42 +1491,32 @@ void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const void* e,
 }
 
 template <typename K>
-static void allow_sweep_smem(K kernel, int bytes = SWEEP_SMEM) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+static void allow_sweep_smem(K kernel) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SWEEP_SMEM);
 }
 
-void mx_grid_sizes(int threads, int sweep_ctas, int* sweep, int* matvec, int* update,
-                   int* guides) {
+void mx_grid_sizes(int threads, int* sweep, int* matvec, int* update, int* guides, int* mvpipe) {
   int dev = 0, sms = 0, a = 0, b = 0, c = 0, d = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // the sweep kernels' shared memory, on the calling device (before any launch)
-#define MX_ALLOW(PTS, DUAL, BYTES)                                          \
-  allow_sweep_smem(mx_sweep_kernel<0, true, float, PTS, DUAL>, BYTES);       \
-  allow_sweep_smem(mx_sweep_kernel<0, false, float, PTS, DUAL>, BYTES);      \
-  allow_sweep_smem(mx_sweep_kernel<1, true, float, PTS, DUAL>, BYTES);       \
-  allow_sweep_smem(mx_sweep_kernel<1, false, float, PTS, DUAL>, BYTES);      \
-  allow_sweep_smem(mx_sweep_kernel<0, true, double, PTS, DUAL>, BYTES);      \
-  allow_sweep_smem(mx_sweep_kernel<0, false, double, PTS, DUAL>, BYTES);     \
-  allow_sweep_smem(mx_sweep_kernel<1, true, double, PTS, DUAL>, BYTES);      \
-  allow_sweep_smem(mx_sweep_kernel<1, false, double, PTS, DUAL>, BYTES);
-  MX_ALLOW(512, false, SWEEP_SMEM)
-  MX_ALLOW(256, false, SWEEP_SMEM)
-  MX_ALLOW(512, true, SWEEP_SMEM_DUAL)
-  MX_ALLOW(256, true, SWEEP_SMEM_DUAL)
+#define MX_ALLOW(PTS)                                    \
+  allow_sweep_smem(mx_sweep_kernel<0, true, float, PTS>);  \
+  allow_sweep_smem(mx_sweep_kernel<0, false, float, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<1, true, float, PTS>);  \
+  allow_sweep_smem(mx_sweep_kernel<1, false, float, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<0, true, double, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<0, false, double, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<1, true, double, PTS>); \
+  allow_sweep_smem(mx_sweep_kernel<1, false, double, PTS>);
+  MX_ALLOW(512)
+  MX_ALLOW(256)
 #undef MX_ALLOW
-  // CTAs per SM of the sweep kernel in the chosen arrangement
-  if (sweep_ctas == 2) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, float, 512, true>,
-                                                  512, SWEEP_SMEM_DUAL);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, float, 256, true>,
-                                                  256, SWEEP_SMEM_DUAL);
-  } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, float, 512, false>,
-                                                  512, SWEEP_SMEM);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, float, 256, false>,
-                                                  256, SWEEP_SMEM);
-  }
+  // one CTA per SM for either thread count (its shared memory)
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, mx_sweep_kernel<0, true, float, 512>, 512,
+                                                SWEEP_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mx_sweep_kernel<1, false, float, 256>, 256,
+                                                SWEEP_SMEM);
   if (threads == 128) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, mx_matvec_kernel<2, false, float, 128>,
                                                   128, 0);
@@ -1228,6 +1536,15 @@ void mx_grid_sizes(int threads, int sweep_ctas, int* sweep, int* matvec, int* up
   *guides = sms * std::max(1, g);
   *matvec = sms * std::max(1, c);
   *update = sms * std::max(1, d);
+  // the pipelined A*x: its shared memory on this device, one CTA per SM
+#define MV_ALLOW(NV, CF, ET)                                                           \
+  cudaFuncSetAttribute(mx_matvec_pipe_kernel<NV, CF, ET>,                               \
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mvp::Smem));
+  MV_ALLOW(1, false, float) MV_ALLOW(2, false, float) MV_ALLOW(1, true, float)
+  MV_ALLOW(2, true, float) MV_ALLOW(1, false, double) MV_ALLOW(2, false, double)
+  MV_ALLOW(1, true, double) MV_ALLOW(2, true, double)
+#undef MV_ALLOW
+  *mvpipe = sms;
 }
 
 template <typename ET, int NT>
@@ -1254,9 +1571,27 @@ static void matvec_nt(cudaStream_t s, const MixCtx& C, int count, int ndot, int 
     matvec_launch<ET, 256>(s, C, count, ndot, x, A, y, w0);
 }
 
-void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads,
+template <typename ET>
+static void matvec_pipe(cudaStream_t s, const MixCtx& C, int count, int ndot, const ET* x,
+                        const double* A, double* y, const double* w0) {
+  constexpr int T = mvp::NTHREADS, B = (int)sizeof(mvp::Smem);
+  if (ndot == 1 && !C.cf)
+    mx_matvec_pipe_kernel<1, false, ET><<<count, T, B, s>>>(C, x, A, y, w0);
+  else if (!C.cf)
+    mx_matvec_pipe_kernel<2, false, ET><<<count, T, B, s>>>(C, x, A, y, w0);
+  else if (ndot == 1)
+    mx_matvec_pipe_kernel<1, true, ET><<<count, T, B, s>>>(C, x, A, y, w0);
+  else
+    mx_matvec_pipe_kernel<2, true, ET><<<count, T, B, s>>>(C, x, A, y, w0);
+}
+
+void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads, int form,
                       const void* x, const double* A, double* y, const double* w0, bool d64) {
-  if (d64)
+  if (form == 0 && d64)
+    matvec_pipe(s, C, count, ndot, static_cast<const double*>(x), A, y, w0);
+  else if (form == 0)
+    matvec_pipe(s, C, count, ndot, static_cast<const float*>(x), A, y, w0);
+  else if (d64)
     matvec_nt(s, C, count, ndot, threads, static_cast<const double*>(x), A, y, w0);
   else
     matvec_nt(s, C, count, ndot, threads, static_cast<const float*>(x), A, y, w0);

@@ -31,9 +31,9 @@ inline ffvgpu_status bad(const char* why) {
 // (SolveState::timeout_where bits).
 inline std::string timeout_message(int where) {
   std::string m = "a bounded device wait gave up (";
-  const char* names[] = {"producer", "gatherer", "consumer", "sweep", "drain"};
+  const char* names[] = {"producer", "gatherer", "consumer", "sweep", "drain", "A*x"};
   bool any = false;
-  for (int b = 0; b < 5; ++b)
+  for (int b = 0; b < 6; ++b)
     if (where & (1 << b)) {
       m += any ? ", " : "";
       m += names[b];
@@ -156,9 +156,9 @@ struct ffvgpu_pool {
   int m_cf = 0;   // coarse-fine flux correction of the running solves
   int m_d64 = 0;  // the running solves use the FP64-data variant
   int m_depth = 1;  // sweep kernel staging depth (L2 prefetch distance in blocks)
-  int m_threads = 256;  // CTA size of the A*x and update kernels
+  int m_threads = 256;  // CTA size of the update kernel (and of the A*x kernel in form 1)
   int m_sweep_threads = 512;  // CTA size of the sweep kernel
-  int m_sweep_ctas = 1;       // sweep CTAs per SM
+  int m_mvform = 0;           // A*x kernel: 0 pipelined, 1 a block per CTA
   cudaGraphExec_t mgraph = nullptr;
   int mgraph_iters = 0;
   double mgraph_omega = 0.0;
@@ -167,7 +167,7 @@ struct ffvgpu_pool {
   int mgraph_stall = 0;
   int mgraph_cf = 0;
   int mgraph_d64 = 0;
-  int mgraph_depth = 0, mgraph_threads = 0, mgraph_sweep_threads = 0, mgraph_sweep_ctas = 0;
+  int mgraph_depth = 0, mgraph_threads = 0, mgraph_sweep_threads = 0, mgraph_mvform = -1;
   int stall_sweep = 0;  // test hook (ffvgpu_pool_stall_next_solve), cleared when a solve ends
   int64_t m_launches = 0;
   int64_t m_bytes = 0;
@@ -177,9 +177,8 @@ struct ffvgpu_pool {
   int32_t* act_h[2] = {nullptr, nullptr};
   cudaEvent_t act_ev[2] = {nullptr, nullptr};
   int act_next = 0;
-  int grid_sweep = 0, grid_matvec = 0, grid_update = 0, grid_guides = 0;
-  int grid_threads = 0;     // m_threads the grid sizes were computed for
-  int grid_sweep_ctas = 0;  // and m_sweep_ctas
+  int grid_sweep = 0, grid_matvec = 0, grid_update = 0, grid_guides = 0, grid_mvpipe = 0;
+  int grid_threads = 0;  // m_threads the grid sizes were computed for
 
   ffvgpu::KCtx ctx(const ffvgpu::BCSet& bc) const {
     ffvgpu::KCtx C;

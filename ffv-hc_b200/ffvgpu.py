@@ -108,7 +108,7 @@ class MixedParams(ctypes.Structure):
         ("restart_growth", ctypes.c_double), ("restart_every", ctypes.c_int32),
         ("flux_correction", ctypes.c_int32), ("fp64_data", ctypes.c_int32),
         ("threads_per_block", ctypes.c_int32), ("stage_depth", ctypes.c_int32),
-        ("sweep_threads", ctypes.c_int32), ("sweep_ctas", ctypes.c_int32),
+        ("sweep_threads", ctypes.c_int32), ("matvec_form", ctypes.c_int32),
     ]
 
 
@@ -137,7 +137,7 @@ class TuneRecord(ctypes.Structure):
         ("sweeps_per_exchange", ctypes.c_int32), ("iterations_per_replay", ctypes.c_int32),
         ("ms", ctypes.c_double), ("max_count", ctypes.c_int32), ("converged", ctypes.c_int32),
         ("threads_per_block", ctypes.c_int32), ("stage_depth", ctypes.c_int32),
-        ("sweep_threads", ctypes.c_int32), ("sweep_ctas", ctypes.c_int32),
+        ("sweep_threads", ctypes.c_int32), ("matvec_form", ctypes.c_int32),
     ]
 
 
@@ -146,10 +146,13 @@ class TuneRecord(ctypes.Structure):
 # iterations per replay.
 TUNE_SPACE = [(om, sw, per, it) for om in (1.5, 1.2) for (sw, per) in
               ((8, 4), (8, 8), (8, 2), (8, 1), (4, 4), (4, 2)) for it in (4, 8, 16)]
-# Then, for the fastest of those: threads per block of the A*x and update
-# kernels 128 / 256 / 512, the sweep kernel's staging depth 1 / 2 / 3 and its
-# threads per block 512 / 256.
-TUNE_LAUNCH = [(nt, dp, st) for nt in (128, 256, 512) for dp in (1, 2, 3) for st in (512, 256)]
+# Then, for the fastest of those: threads per block of the update kernel
+# (and of the A*x kernel in form 1) 128 / 256 / 512, the sweep kernel's
+# staging depth 1 / 2 / 3 and its threads per block 512 / 256, and the A*x
+# kernel's form (0 pipelined, 1 a block per CTA).
+TUNE_LAUNCH = [(nt, dp, st, mv) for nt in (128, 256, 512) for dp in (1, 2, 3)
+               for st in (512, 256) for mv in (0, 1)]
+TUNE_LAUNCH_DEFAULT = (256, 1, 512, 0)
 
 
 class Request(ctypes.Structure):
@@ -620,11 +623,11 @@ class Pool:
                     epsilon=1e-8, history=True, check_every=0, restart_drop=None,
                     restart_growth=None, restart_every=None, flux_correction=False,
                     fp64_data=False, threads_per_block=0, stage_depth=0, sweep_threads=0,
-                    sweep_ctas=0):
+                    matvec_form=0):
         """Mixed-precision solve (FP64 BiCGSTAB; RB-SOR preconditioner on 32-bit data).
         flux_correction: the FP64 residual and A*x use the coarse-fine
         flux-conserving operator; fp64_data: the same preconditioner on FP64 data;
-        threads_per_block, stage_depth, sweep_threads, sweep_ctas: launch settings
+        threads_per_block, stage_depth, sweep_threads, matvec_form: launch settings
         (0: defaults)."""
         hist = np.zeros(max(count_max, 1), np.float64) if history else None
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
@@ -633,7 +636,7 @@ class Pool:
         prm.flux_correction = int(bool(flux_correction))
         prm.fp64_data = int(bool(fp64_data))
         prm.threads_per_block, prm.stage_depth = int(threads_per_block), int(stage_depth)
-        prm.sweep_threads, prm.sweep_ctas = int(sweep_threads), int(sweep_ctas)
+        prm.sweep_threads, prm.matvec_form = int(sweep_threads), int(matvec_form)
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -871,14 +874,14 @@ class Batch:
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
                     epsilon=1e-8, check_every=0, restart_drop=None, restart_growth=None,
                     restart_every=None, flux_correction=False, fp64_data=False,
-                    threads_per_block=0, stage_depth=0, sweep_threads=0, sweep_ctas=0):
+                    threads_per_block=0, stage_depth=0, sweep_threads=0, matvec_form=0):
         """Solves every admitted instance; returns the first instance's result."""
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, check_every,
                           None, *_restart(restart_drop, restart_growth, restart_every))
         prm.flux_correction = int(bool(flux_correction))
         prm.fp64_data = int(bool(fp64_data))
         prm.threads_per_block, prm.stage_depth = int(threads_per_block), int(stage_depth)
-        prm.sweep_threads, prm.sweep_ctas = int(sweep_threads), int(sweep_ctas)
+        prm.sweep_threads, prm.matvec_form = int(sweep_threads), int(matvec_form)
         res = Result()
         st = lib().ffvgpu_solve_mixed(self._h, ctypes.byref(prm), ctypes.byref(res))
         _check(st, "solve_mixed", allow=(OK, NOT_CONVERGED, NAN_DETECTED))
@@ -907,11 +910,11 @@ class Batch:
 
     def _tune(self, ids, cands, count_max, epsilon):
         recs = (TuneRecord * len(cands))()
-        for k, (om, sw, per, it, nt, dp, st) in enumerate(cands):
+        for k, (om, sw, per, it, nt, dp, st, mv) in enumerate(cands):
             recs[k].omega, recs[k].sweeps = om, sw
             recs[k].sweeps_per_exchange, recs[k].iterations_per_replay = per, it
             recs[k].threads_per_block, recs[k].stage_depth = nt, dp
-            recs[k].sweep_threads = st
+            recs[k].sweep_threads, recs[k].matvec_form = st, mv
         prm = MixedParams(1.5, 8, 4, count_max, epsilon, 0, None, *_restart(None, None, None))
         best = ctypes.c_int32()
         _check(lib().ffvgpu_mixed_autotune(self._h, _ptr(ids), len(ids), ctypes.byref(prm),
@@ -919,7 +922,7 @@ class Batch:
         out = [dict(omega=r.omega, sweeps=r.sweeps, sweeps_per_exchange=r.sweeps_per_exchange,
                     iterations_per_replay=r.iterations_per_replay,
                     threads_per_block=r.threads_per_block or 256, stage_depth=r.stage_depth or 1,
-                    sweep_threads=r.sweep_threads or 512,
+                    sweep_threads=r.sweep_threads or 512, matvec_form=r.matvec_form,
                     ms=r.ms, max_count=r.max_count, converged=bool(r.converged)) for r in recs]
         return out, best.value
 
@@ -933,14 +936,14 @@ class Batch:
         ids = np.ascontiguousarray(instances, np.int32)
         space = space or TUNE_SPACE
         launch = launch or TUNE_LAUNCH
-        recs, best = self._tune(ids, [(om, sw, per, it, 256, 1, 512)
+        recs, best = self._tune(ids, [(om, sw, per, it) + TUNE_LAUNCH_DEFAULT
                                       for (om, sw, per, it) in space], count_max, epsilon)
         if best < 0:
             return recs, best
         b = recs[best]
         head = (b["omega"], b["sweeps"], b["sweeps_per_exchange"], b["iterations_per_replay"])
         more, best2 = self._tune(ids, [head + tuple(c) for c in launch
-                                       if tuple(c) != (256, 1, 512)], count_max, epsilon)
+                                       if tuple(c) != TUNE_LAUNCH_DEFAULT], count_max, epsilon)
         recs2 = recs + more
         if best2 >= 0 and more[best2]["ms"] < b["ms"]:
             best = len(recs) + best2
@@ -948,11 +951,11 @@ class Batch:
 
     def begin(self, inst, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
               epsilon=1e-8, restart_drop=None, restart_growth=None, restart_every=None,
-              threads_per_block=0, stage_depth=0, sweep_threads=0, sweep_ctas=0):
+              threads_per_block=0, stage_depth=0, sweep_threads=0, matvec_form=0):
         prm = MixedParams(omega, sweeps, sweeps_per_exchange, count_max, epsilon, 0, None,
                           *_restart(restart_drop, restart_growth, restart_every))
         prm.threads_per_block, prm.stage_depth = int(threads_per_block), int(stage_depth)
-        prm.sweep_threads, prm.sweep_ctas = int(sweep_threads), int(sweep_ctas)
+        prm.sweep_threads, prm.matvec_form = int(sweep_threads), int(matvec_form)
         _check(lib().ffvgpu_mixed_begin(self._h, inst, ctypes.byref(prm)), "mixed_begin")
 
     def cancel(self, inst):

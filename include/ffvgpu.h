@@ -411,17 +411,18 @@ typedef struct {
                                   the iterate between exchanges in FP64, the preconditioned
                                   vectors in FP64 -- so that a comparison with the default
                                   (32-bit data) isolates what the 32-bit data buy */
-  int32_t threads_per_block;   /* CTA size of the A*x and update kernels: 128, 256 or 512
-                                  (0: 256); results do not depend on it */
+  int32_t threads_per_block;   /* CTA size of the update kernel, and of the A*x kernel in
+                                  matvec_form 1: 128, 256 or 512 (0: 256); results do not
+                                  depend on it */
   int32_t stage_depth;         /* sweep kernel: how many blocks ahead a block's data are
                                   brought into L2 (1..3; 0: 1); results do not depend on it */
   int32_t sweep_threads;       /* CTA size of the sweep kernel: 512 (each thread a 4-cell
                                   column of one row) or 256 (of two rows); 0: 512; results
                                   do not depend on it */
-  int32_t sweep_ctas;          /* sweep CTAs per SM: 1 (a block's coefficient words staged
-                                  in shared memory) or 2 (read at use, so one CTA's staging
-                                  overlaps the other's sweeps); 0: 1; results do not depend
-                                  on it */
+  int32_t matvec_form;         /* A*x kernel: 0 pipelined (one CTA of 800 threads per SM;
+                                  bulk copies of the next blocks overlap the current one),
+                                  1 a block per CTA of threads_per_block threads; results
+                                  do not depend on it */
 } ffvgpu_mixed_params;
 
 /* Solves every admitted instance of the pool (a pool made from one grid is
@@ -580,7 +581,7 @@ typedef struct {
   int32_t threads_per_block;  /* as ffvgpu_mixed_params (0: 256) */
   int32_t stage_depth;        /* as ffvgpu_mixed_params (0: 1) */
   int32_t sweep_threads;      /* as ffvgpu_mixed_params (0: 512) */
-  int32_t sweep_ctas;         /* as ffvgpu_mixed_params (0: 1) */
+  int32_t matvec_form;        /* as ffvgpu_mixed_params */
 } ffvgpu_tune_record;
 
 ffvgpu_status ffvgpu_mixed_autotune(ffvgpu_pool* pool, const int32_t* instances,

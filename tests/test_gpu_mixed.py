@@ -64,22 +64,23 @@ def test_fp64_data_variant_bitwise_against_oracle(level, omega, sweeps, per, cou
     P.close()
 
 
-@pytest.mark.parametrize("threads,depth,sweep_threads,sweep_ctas", [
-    (128, 1, 512, 1), (512, 3, 512, 1), (256, 2, 256, 1), (128, 3, 256, 1),
-    (256, 1, 256, 2), (512, 2, 512, 2)])
-def test_launch_settings_do_not_change_results(threads, depth, sweep_threads, sweep_ctas):
-    """CTA sizes of the A*x, update and sweep kernels and the sweep kernel's
-    staging depth are tuning knobs only: the same bits as the defaults (the
-    512-lane block tree and the 256-lane cross-block tree do not depend on
-    them, and the sweep keeps each cell's order of terms)."""
+@pytest.mark.parametrize("threads,depth,sweep_threads,form,extra", [
+    (128, 1, 512, 1, {}), (512, 3, 512, 1, {}), (256, 2, 256, 0, {}), (128, 3, 256, 1, {}),
+    (256, 1, 512, 1, {"fp64_data": True}), (256, 1, 512, 1, {"flux_correction": True})])
+def test_launch_settings_do_not_change_results(threads, depth, sweep_threads, form, extra):
+    """CTA sizes of the A*x, update and sweep kernels, the sweep kernel's
+    staging depth and the A*x kernel's form (pipelined or a block per CTA)
+    are tuning knobs only: the same bits as the defaults (the 512-lane block
+    tree and the 256-lane cross-block tree do not depend on them, and the
+    sweep keeps each cell's order of terms)."""
     g, inp, O = problem(3)
     P = device_problem(g, inp)
     P.fill("X", 0.0)
-    ref = P.solve_mixed(1.5, 8, 4, 4, 0.0)
+    ref = P.solve_mixed(1.5, 8, 4, 4, 0.0, **extra)
     xr = interior(P.download("X", VC)).copy()
     P.fill("X", 0.0)
     r = P.solve_mixed(1.5, 8, 4, 4, 0.0, threads_per_block=threads, stage_depth=depth,
-                      sweep_threads=sweep_threads, sweep_ctas=sweep_ctas)
+                      sweep_threads=sweep_threads, matvec_form=form, **extra)
     assert_bitwise(r["history"], ref["history"], "residual history")
     assert_bitwise(interior(P.download("X", VC)), xr, "pressure")
     P.close()
@@ -278,12 +279,13 @@ def test_autotuner_times_candidates_and_leaves_x_zero():
     space = [(1.5, 8, 4, 8), (1.2, 4, 4, 4), (1.5, 8, 8, 16)]
     recs, best = B.autotune(ids, space=space, count_max=400)
     # stage 1: the three numerical settings; stage 2 (when one converged): the
-    # fastest of them at the 17 other launch settings
-    assert len(recs) in (3, 20) and all(r["ms"] > 0 and r["max_count"] >= 1 for r in recs)
-    if len(recs) == 20:
-        assert {(r["threads_per_block"], r["stage_depth"], r["sweep_threads"])
-                for r in recs[3:]} == {(nt, dp, st) for nt in (128, 256, 512) for dp in (1, 2, 3)
-                                       for st in (512, 256)} - {(256, 1, 512)}
+    # fastest of them at the 35 other launch settings
+    assert len(recs) in (3, 38) and all(r["ms"] > 0 and r["max_count"] >= 1 for r in recs)
+    if len(recs) == 38:
+        assert {(r["threads_per_block"], r["stage_depth"], r["sweep_threads"], r["matvec_form"])
+                for r in recs[3:]} == {(nt, dp, st, mv) for nt in (128, 256, 512)
+                                       for dp in (1, 2, 3) for st in (512, 256)
+                                       for mv in (0, 1)} - {(256, 1, 512, 0)}
     assert best == -1 or recs[best]["converged"]
     if best >= 0:
         assert recs[best]["ms"] == min(r["ms"] for r in recs if r["converged"])
