@@ -276,14 +276,14 @@ __device__ __noinline__ double cf_fine_flux(const T* __restrict__ x, const doubl
 
 // y plus (SUB: minus) the correction delta of each face of cell s (storage
 // slot) whose neighbours are finer, in face order; y unchanged when it has
-// none.  x_P and its guide layer G ([face][p]) as the stencil used them, its
-// face coefficients af(f).
-template <bool SUB, typename T, typename AF>
+// none.  x_P and its guide layer G (read as G[face * 256 + p]: an array, or
+// an accessor of a tile) as the stencil used them, its face coefficients af(f).
+template <bool SUB, typename T, typename AF, typename GA>
 __device__ __forceinline__ double cf_delta(const T* __restrict__ x, const double* __restrict__ gx,
                                            const double* __restrict__ A,
                                            const FaceNbr* __restrict__ nbr,
                                            const double* __restrict__ dxs, const BCSet& bc,
-                                           const FaceNbr* snb, const double* G, double xp,
+                                           const FaceNbr* snb, const GA& G, double xp,
                                            int s, double y, AF af) {
   int cc[3];
   cell_of(s, cc[0], cc[1], cc[2]);

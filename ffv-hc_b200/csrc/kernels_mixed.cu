@@ -39,6 +39,7 @@
 // instance's blocks, so an instance gets the same bits alone or in a batch.
 #include <algorithm>
 #include <cfloat>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "ffvgpu_async.cuh"
@@ -993,17 +994,15 @@ mx_matvec_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // The same A*x and dot products as a persistent, warp-specialised kernel:
-// one CTA of 800 threads per SM walks its live blocks while bulk copies
-// bring the next ones into shared memory.
-//   producer (thread 0): per block its x (FP32 into the upper half of a
-//     tile buffer, or FP64 into all of it) and, for a uniform block, its
-//     coefficient record, a block ahead; and through a ring of three 32 KB
-//     slots the dot partner w0 (a uniform block: all of it in one slot) or,
-//     for a block that streams its coefficients, eight slots of 512 cells
-//     with the seven coefficient rows and w0.
-//   gatherers (8 warps): the block's guide layer by the exchange rules
-//     (loads issued before its x lands), then an FP32 x widened to FP64 in
-//     place.
+// one CTA of 800 threads per SM walks its live blocks.
+//   producer (thread 0): through a ring of three 32 KB slots, by bulk copies,
+//     the dot partner w0 (a uniform block: all of it in one slot) or, for a
+//     block that streams its coefficients, eight slots of 512 cells with the
+//     seven coefficient rows and w0.
+//   gatherers (8 warps): a block ahead, its x widened to FP64 and its guide
+//     layer by the exchange rules, written into a padded tile (the layout of
+//     the sweep kernel: every neighbour of a cell, guide or interior, at a
+//     fixed offset); the loads are issued before the tile frees up.
 //   consumers (16 warps): consumer t takes cells q = 512 mm + t of each
 //     colour, which makes it the block tree's virtual thread t: the per-block
 //     sums are those of mx_reduce; the ticket of an instance is advanced once
@@ -1018,7 +1017,6 @@ constexpr int ROWS = 8;                            // A rows 0..6 (Ap, Aw..At), 
 constexpr int SLOT_CELLS = 512;
 constexpr int SLOTS = BLOCK_CELLS / SLOT_CELLS;    // slots of a streamed block
 constexpr uint32_t SLOT_BYTES = ROWS * SLOT_CELLS * 8;
-constexpr int X_ISSUE_AT = SLOTS / 2;              // slot of block n after which x(n+1) is issued
 constexpr int GATHER0 = 32, NGATHER = 256;
 constexpr int CONS0 = GATHER0 + NGATHER, NCONS = 512, CONS_WARPS = NCONS / 32;
 constexpr int NTHREADS = CONS0 + NCONS;            // 800
@@ -1028,22 +1026,26 @@ static_assert(SLOT_BYTES == BLOCK_CELLS * 8, "a slot holds a uniform block's w0"
 
 struct __align__(128) Smem {
   double ring[STAGES][ROWS][SLOT_CELLS];  // 96 KB
-  double tile[2][BLOCK_CELLS];            // 64 KB: x of the current / next block, FP64
-  double gbuf[2][GUIDES];                 // 24 KB: their guide layers, [face][v][u]
-  double urec[2][8];                      // coefficient records of uniform blocks
+  double tile[2][TILE];                   // 107 KB: x of the current / next block with guides
+  double urec[2][8];                      // coefficient records of the blocks in the tiles
   double ws[2][CONS_WARPS];               // warp sums of the block tree
   int2 list[CAP];                         // the chunk's live entries
   FaceNbr snb[2][6];                      // face records (flux correction)
-  uint64_t full[STAGES], empty[STAGES], xfull[2], xempty[2], gfull[2], gempty[2];
+  // full/empty: ring slots; gfull: a tile ready; tempty: a tile free
+  uint64_t full[STAGES], empty[STAGES], gfull[2], tempty[2];
   int wcount[NTHREADS / 32];
   int nlist, next_from, abort_flag, last_inst;
+};
+static_assert(sizeof(Smem) <= 227 * 1024, "shared memory of one CTA");
+
+// The first guide layer of a padded tile read as [face][p] (flux correction).
+struct TileGuides {
+  const double* T;
+  __device__ double operator[](int g) const { return T[guide_slot(g >> 8, g & 255)]; }
 };
 
 __device__ __forceinline__ void consumer_sync() {
   asm volatile("bar.sync 1, %0;" ::"n"(NCONS) : "memory");
-}
-__device__ __forceinline__ void gather_sync() {
-  asm volatile("bar.sync 2, %0;" ::"n"(NGATHER) : "memory");
 }
 __device__ __forceinline__ void release_slot(uint64_t* bar, int lane, bool live) {
   async::fence_proxy_async();
@@ -1069,18 +1071,15 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
       async::mbar_init(&S.empty[s], CONS_WARPS);
     }
     for (int b = 0; b < 2; ++b) {
-      async::mbar_init(&S.xfull[b], 1);
-      async::mbar_init(&S.xempty[b], 1);
       async::mbar_init(&S.gfull[b], NGATHER);
-      async::mbar_init(&S.gempty[b], 1);
+      async::mbar_init(&S.tempty[b], 1);
     }
     S.abort_flag = 0;
     async::fence_mbar_init();
   }
   // Counters that run across the chunks: ring slots issued (producer) or
-  // consumed (consumers), x copies per tile buffer, blocks of earlier chunks.
+  // consumed (consumers), blocks of earlier chunks.
   uint32_t g = 0;
-  uint32_t nx[2] = {0, 0};
   int M0 = 0;
   int run = 0;  // consumer 0: blocks of the current instance not yet on its ticket
   bool live = true;
@@ -1090,103 +1089,86 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
     from = S.next_from;
     const int nl = S.nlist;
     auto is_uni = [&](int n) { return (S.list[n].y & LF_UNI) != 0; };
-    auto nslots = [&](int n) { return is_uni(n) ? 1 : SLOTS; };
     if (tid == 0 && nl > 0 && !*abort_flag) {
       // ------------------------------------------------------------ producer
-      int pm = 0, pj = 0, xn = 0;  // next slot: block pm, slot pj; x copies issued
-      auto issue_slot = [&](int n, int j) {
-        const int s = g % STAGES;
+      for (int n = 0; n < nl; ++n) {
         const size_t blk = (size_t)S.list[n].x;
-        async::mbar_expect_tx(&S.full[s], SLOT_BYTES);
-        if (is_uni(n)) {
-          async::bulk_g2s(S.ring[s], w0 + blk * BLOCK_CELLS, SLOT_BYTES, &S.full[s]);
-        } else {
+        const int ns = is_uni(n) ? 1 : SLOTS;
+        bool ok = true;
+        for (int j = 0; j < ns; ++j, ++g) {
+          const int s = g % STAGES;
+          if (!(ok = mbar_wait(&S.empty[s], ((g / STAGES) & 1) ^ 1, abort_flag, ROLE_MATVEC,
+                               C.wait_ns)))
+            break;
+          async::mbar_expect_tx(&S.full[s], SLOT_BYTES);
+          if (ns == 1) {
+            async::bulk_g2s(S.ring[s], w0 + blk * BLOCK_CELLS, SLOT_BYTES, &S.full[s]);
+          } else {
 #pragma unroll 1
-          for (int a = 0; a < 7; ++a)
-            async::bulk_g2s(S.ring[s][a], A + (blk * 7 + a) * BLOCK_CELLS + j * SLOT_CELLS,
+            for (int a = 0; a < 7; ++a)
+              async::bulk_g2s(S.ring[s][a], A + (blk * 7 + a) * BLOCK_CELLS + j * SLOT_CELLS,
+                              SLOT_CELLS * 8, &S.full[s]);
+            async::bulk_g2s(S.ring[s][7], w0 + blk * BLOCK_CELLS + j * SLOT_CELLS,
                             SLOT_CELLS * 8, &S.full[s]);
-          async::bulk_g2s(S.ring[s][7], w0 + blk * BLOCK_CELLS + j * SLOT_CELLS,
-                          SLOT_CELLS * 8, &S.full[s]);
-        }
-      };
-      // x(n) follows slot x_at(n-1) of block n-1 (the middle of a streamed
-      // block, the only slot of a uniform one): every slot of block n-2 is
-      // issued by then, so the wait for its tile buffer needs nothing more
-      // from the producer.
-      auto issue_xs = [&]() {
-        while (xn < nl) {
-          if (xn > 0) {
-            const int m = xn - 1, x_at = nslots(m) == 1 ? 0 : X_ISSUE_AT;
-            if (!(pm > m || (pm == m && pj > x_at))) break;
           }
-          const int Mg = M0 + xn, xb = Mg & 1;
-          if (Mg >= 2 && !mbar_wait(&S.xempty[xb], ((Mg - 2) >> 1) & 1, abort_flag,
-                                    ROLE_MATVEC, C.wait_ns))
-            return false;
-          const size_t blk = (size_t)S.list[xn].x;
-          const bool u = is_uni(xn);
-          constexpr uint32_t XB = BLOCK_CELLS * (uint32_t)sizeof(ET);
-          async::mbar_expect_tx(&S.xfull[xb], XB + (u ? 64u : 0u));
-          async::bulk_g2s(sizeof(ET) == 4 ? (void*)(S.tile[xb] + HALF_CELLS) : (void*)S.tile[xb],
-                          x + blk * BLOCK_CELLS, XB, &S.xfull[xb]);
-          if (u) async::bulk_g2s(S.urec[xb], C.ucoef + blk * 8, 64, &S.xfull[xb]);
-          ++nx[xb];
-          ++xn;
         }
-        return true;
-      };
-      bool ok = issue_xs();
-      while (ok && pm < nl) {
-        const int s = g % STAGES;
-        if (!(ok = mbar_wait(&S.empty[s], ((g / STAGES) & 1) ^ 1, abort_flag, ROLE_MATVEC,
-                             C.wait_ns)))
-          break;
-        issue_slot(pm, pj);
-        ++g;
-        if (++pj == nslots(pm)) {
-          pj = 0;
-          ++pm;
-        }
-        ok = issue_xs();
+        if (!ok) break;
       }
     } else if (tid >= GATHER0 && tid < CONS0) {
       // ----------------------------------------------------------- gatherers
       const int gt = tid - GATHER0, grp = gt >> 7, p0 = gt & 127, p1 = p0 + 128;
       for (int n = 0; n < nl; ++n) {
         const int Mg = M0 + n, b = Mg & 1;
-        if (Mg >= 2 &&
-            !mbar_wait(&S.gempty[b], ((Mg - 2) >> 1) & 1, abort_flag, ROLE_MATVEC, C.wait_ns))
-          break;
         const int blk = S.list[n].x;
         const double dx = C.dx[blk];
-        // two groups of 128 threads take alternate faces, two positions each
+        // everything this thread writes into the tile, loaded before the tile
+        // (block Mg - 2) is free: 16 values of x (cells 4 (gt + 256 kk) + e),
+        // and two positions of alternate faces of the guide layer
+        constexpr int VW = 16 / (int)sizeof(ET);  // values per 16-byte load
+        using V16 = typename std::conditional<sizeof(ET) == 4, float4, double2>::type;
+        V16 xv[16 / VW];
+        const V16* xb = reinterpret_cast<const V16*>(x + (size_t)blk * BLOCK_CELLS);
+#pragma unroll
+        for (int kk = 0; kk < 16 / VW; ++kk) xv[kk] = __ldg(xb + gt + NGATHER * kk);
+        double gv[3][2];
+        FaceNbr nfs[CF ? 3 : 1];
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
           const int f = 2 * r + grp;
           const FaceNbr nf = C.nbr[blk * 6 + f];
-          double v0, v1;
-          guide_pair(x, blk, f, p0, p1, nf, C.bc, dx, v0, v1);
-          S.gbuf[b][f * FACE_CELLS + p0] = v0;
-          S.gbuf[b][f * FACE_CELLS + p1] = v1;
-          if (CF && p0 == 0) S.snb[b][f] = nf;
+          guide_pair(x, blk, f, p0, p1, nf, C.bc, dx, gv[r][0], gv[r][1]);
+          if (CF) nfs[CF ? r : 0] = nf;
         }
-        if (!mbar_wait(&S.xfull[b], (Mg >> 1) & 1, abort_flag, ROLE_MATVEC, C.wait_ns)) break;
-        if (sizeof(ET) == 4) {
-          // widened in place: every thread holds its 16 values before any
-          // FP64 value overwrites them
-          const float4* src = reinterpret_cast<const float4*>(S.tile[b] + HALF_CELLS);
-          float4 v[4];
+        const double ur = gt < 8 ? __ldg(C.ucoef + (size_t)blk * 8 + gt) : 0.0;
+        if (Mg >= 2 &&
+            !mbar_wait(&S.tempty[b], ((Mg - 2) >> 1) & 1, abort_flag, ROLE_MATVEC, C.wait_ns))
+          break;
+        double* T = S.tile[b];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) v[k] = src[gt + NGATHER * k];
-          gather_sync();
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            double2* d = reinterpret_cast<double2*>(S.tile[b] + 4 * (gt + NGATHER * k));
-            d[0] = make_double2((double)v[k].x, (double)v[k].y);
-            d[1] = make_double2((double)v[k].z, (double)v[k].w);
+        for (int kk = 0; kk < 16 / VW; ++kk) {
+          // VW consecutive cells of one row: one run of the padded tile
+          const int s0 = VW * (gt + NGATHER * kk);
+          const int c = s0 >> 11, q = s0 & 2047;
+          const int ih = q & 7, j = (q >> 3) & 15, k = q >> 7;
+          double* d = T + c * SH + (k + 1) * SQ + (j + 1) * SP + ih + 1;
+          if constexpr (sizeof(ET) == 4) {
+            d[0] = (double)xv[kk].x;
+            d[1] = (double)xv[kk].y;
+            d[2] = (double)xv[kk].z;
+            d[3] = (double)xv[kk].w;
+          } else {
+            d[0] = xv[kk].x;
+            d[1] = xv[kk].y;
           }
         }
-        async::fence_proxy_async();  // the tile is refilled by bulk copies
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          const int f = 2 * r + grp;
+          T[guide_slot(f, p0)] = gv[r][0];
+          T[guide_slot(f, p1)] = gv[r][1];
+          if (CF && p0 == 0) S.snb[b][f] = nfs[CF ? r : 0];
+        }
+        if (gt < 8) S.urec[b][gt] = ur;
         async::mbar_arrive(&S.gfull[b]);
       }
     } else if (tid >= CONS0) {
@@ -1194,16 +1176,18 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
       // Every consumer runs the same sequence of named barriers and shuffles;
       // only the work is predicated on 'live'.
       const int ct = tid - CONS0, lane = ct & 31, warp = ct >> 5;
+      // this thread's cells q = 512 mm + ct: (2 ih + p, j, k0 + 4 mm), where
+      // the parity p of the row is the same for every mm
+      const int ih = ct & 7, jr = (ct >> 3) & 15, k0 = ct >> 7;
+      const int pos0 = (k0 + 1) * SQ + (jr + 1) * SP + ih + 1;  // tile position, mm = 0
       for (int n = 0; n < nl; ++n) {
         const int Mg = M0 + n, b = Mg & 1;
         const uint32_t par = (Mg >> 1) & 1;
         const int2 ent = S.list[n];
         const int blk = ent.x, inst = ent.y & LF_INST;
         const bool uni = ent.y & LF_UNI;
-        live = live && mbar_wait(&S.xfull[b], par, abort_flag, ROLE_MATVEC, C.wait_ns);
         live = live && mbar_wait(&S.gfull[b], par, abort_flag, ROLE_MATVEC, C.wait_ns);
         const double* T = S.tile[b];
-        const double* G = S.gbuf[b];
         double u[7];
 #pragma unroll
         for (int a = 0; a < 7; ++a) u[a] = uni ? S.urec[b][a] : 0.0;
@@ -1216,9 +1200,12 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
         double acc[NV][2] = {};
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-#pragma unroll 1
+          const int p = (jr + k0 + c) & 1;
+          const double* own = T + c * SH + pos0;         // the cell
+          const double* oth = T + (1 - c) * SH + pos0;   // its position in the other colour
+#pragma unroll 2
           for (int mm = 0; mm < SLOTS / 2; ++mm) {
-            const int q = mm * NCONS + ct, s = c * HALF_CELLS + q;
+            const int q = mm * NCONS + ct, s = c * HALF_CELLS + q, o = mm * 4 * SQ;
             double k[7], wv = 0.0;
             if (uni) {
 #pragma unroll
@@ -1237,12 +1224,18 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
               ++g;
             }
             if (!live) continue;
-            const Nbrs v = split_neighbours(T + (1 - c) * HALF_CELLS, G, q, c);
-            double yv = k[1] * v.w + k[2] * v.e + k[3] * v.s + k[4] * v.n + k[5] * v.b +
-                        k[6] * v.t + k[0] * T[s];
+            // neighbours w, e (i -+ 1: other colour, columns ih + p - 1 and
+            // ih + p of it), s, n (rows -+ 1), b, t (planes -+ 1); the guide
+            // layer sits in the tile's padding
+            const double xw = oth[o - 1 + p], xe = oth[o + p];
+            const double xs = oth[o - SP], xn = oth[o + SP];
+            const double xb = oth[o - SQ], xt = oth[o + SQ];
+            const double xp = own[o];
+            double yv = k[1] * xw + k[2] * xe + k[3] * xs + k[4] * xn + k[5] * xb + k[6] * xt +
+                        k[0] * xp;
             if (CF)  // coarse-fine flux correction: y = A x + delta
-              yv = cf_delta<false>(x, (const double*)nullptr, A, C.nbr, C.dx, C.bc, S.snb[b], G,
-                                   T[s], s, yv, [&](int f) { return k[1 + f]; });
+              yv = cf_delta<false>(x, (const double*)nullptr, A, C.nbr, C.dx, C.bc, S.snb[b],
+                                   TileGuides{T}, xp, s, yv, [&](int f) { return k[1 + f]; });
             y[base + s] = yv;
             acc[0][c] += yv * wv;
             if (NV == 2) acc[NV - 1][c] += yv * yv;
@@ -1261,11 +1254,9 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
           for (int off = 16; off >= 1; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
           if (lane == 0) S.ws[v][warp] = t;
         }
-        async::fence_proxy_async();  // the tile is refilled by bulk copies
         consumer_sync();
         if (ct == 0 && live) {
-          async::mbar_arrive(&S.xempty[b]);
-          async::mbar_arrive(&S.gempty[b]);
+          async::mbar_arrive(&S.tempty[b]);
 #pragma unroll
           for (int v = 0; v < NV; ++v) {
             double sum = 0.0;
@@ -1327,16 +1318,14 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
     if (*abort_flag) break;
   }
   if (tid == 0) {
-    // Drain: the last armed phase of every barrier a copy completes on must
-    // complete before the CTA may exit (each has at most one copy phase in
-    // flight: a buffer is refilled only after its copy landed and was used).
+    // Drain: the last armed phase of every ring slot must complete before the
+    // CTA may exit (each has at most one copy phase in flight: a slot is
+    // refilled only after its copy landed and was used).
     bool drained = true;
     for (int s = 0; s < STAGES; ++s) {
       const uint32_t issued = (g > (uint32_t)s) ? (g - 1 - s) / STAGES + 1 : 0;
       if (issued) drained = async::mbar_drain(&S.full[s], (issued - 1) & 1) && drained;
     }
-    for (int b = 0; b < 2; ++b)
-      if (nx[b]) drained = async::mbar_drain(&S.xfull[b], (nx[b] - 1) & 1) && drained;
     if (*abort_flag) {
       // stop every instance of this CTA's chunk and of its later candidates
       const int where = *abort_flag | (drained ? 0 : async::ROLE_DRAIN);
