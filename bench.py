@@ -111,30 +111,34 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(level, cells):
+def profile_traffic(level, cells, fmt_bytes):
     """DRAM bytes per launch of the sweep kernel from the committed ncu summaries:
-    the capture of this level, else the level-3 capture scaled by cells (traffic
-    per cell is level-independent to first order), with its provenance."""
+    the capture of this level, else the level-3 capture scaled by the bytes of
+    the pool's format (uniform blocks at 24 B per cell, the others at 80: the
+    share of uniform blocks differs between levels), with its provenance."""
     for lv in (level, 3):
         path = os.path.join(ROOT, "profiles", f"rbgs_sweep_level{lv}_ncu.md")
         if not os.path.exists(path):
             continue
-        cap_cells = None
-        val = None
+        fields = {}
         for line in open(path):
-            if line.startswith("dram_bytes_per_launch_full_size:"):
-                try:
-                    val = float(line.split(":", 1)[1].split()[0])
-                except ValueError:
-                    val = None
-            if line.startswith("cells_per_launch:"):
-                cap_cells = float(line.split(":", 1)[1].split()[0])
+            for key in ("dram_bytes_per_launch_full_size", "cells_per_launch",
+                        "format_bytes_per_launch"):
+                if line.startswith(key + ":"):
+                    try:
+                        fields[key] = float(line.split(":", 1)[1].split()[0])
+                    except ValueError:
+                        pass
+        val = fields.get("dram_bytes_per_launch_full_size")
         if val is None:
             continue
         if lv == level:
             return val, f"ncu, {os.path.basename(path)}"
-        if cap_cells:
-            return val * cells / cap_cells, f"ncu level-{lv} capture scaled by cells"
+        if fields.get("format_bytes_per_launch"):
+            return (val * fmt_bytes / fields["format_bytes_per_launch"],
+                    f"ncu level-{lv} capture scaled by the format bytes")
+        if fields.get("cells_per_launch"):
+            return val * cells / fields["cells_per_launch"], f"ncu level-{lv} capture scaled by cells"
     return None, None
 
 
@@ -726,7 +730,7 @@ def run_batch(args):
     assert all(i is not None for i in ids)
 
     setting = dict(MIXED, iterations_per_replay=8, threads_per_block=256, stage_depth=1,
-                   sweep_threads=512, matvec_form=0)
+                   sweep_threads=256, matvec_form=0)
     tune = None
     if args.tune:
         # a sample spread over the instance sizes (every k-th by block count)
@@ -745,7 +749,7 @@ def run_batch(args):
                                  r["sweeps_per_exchange"] == MIXED["sweeps_per_exchange"] and
                                  r["iterations_per_replay"] == 8 and
                                  r["threads_per_block"] == 256 and r["stage_depth"] == 1 and
-                                 r["sweep_threads"] == 512 and r["matvec_form"] == 0), None)}
+                                 r["sweep_threads"] == 256 and r["matvec_form"] == 0), None)}
         if best >= 0:
             b = recs[best]
             setting = dict(omega=b["omega"], sweeps=b["sweeps"],
@@ -1014,25 +1018,28 @@ def main():
     e2e_value = whole_job_rate(world, cells * args.sweeps * args.steps, te_ms)
 
     # ---- roofline of the dominant kernel (fused residual + RB sweep) ---------
+    # achieved: the fixed algorithmic bytes of an RB sweep with its residual,
+    # 80 B per interior cell (7 coefficients + b + x read, x written), over
+    # the kernel's average launch; 'traffic' is what the kernel moves from
+    # DRAM (ncu), below the algorithmic bytes because a uniform block's seven
+    # coefficients come from one record (its pass moves 24 B per cell)
     avg_launch_ms = float(np.sum(sweep_ms) / max(1, np.sum(sweep_n)))
-    # bytes of one pass in the pool's format: per-cell coefficients for the
-    # blocks that need them, one record for the uniform ones
     ublocks = int(r.get("uniform_blocks", 0))
-    alg_bytes = CELLS_PER_BLOCK * ((g.nb - ublocks) * BYTES_PER_SWEEP_CELL +
+    alg_bytes = BYTES_PER_SWEEP_CELL * cells
+    fmt_bytes = CELLS_PER_BLOCK * ((g.nb - ublocks) * BYTES_PER_SWEEP_CELL +
                                    ublocks * BYTES_PER_SWEEP_CELL_UNIFORM)
-    ref_bytes = BYTES_PER_SWEEP_CELL * cells
     achieved = alg_bytes / (avg_launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic, traffic_src = profile_traffic(args.level, cells)
+    traffic, traffic_src = profile_traffic(args.level, cells, fmt_bytes)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                 "kernel": "rbgs_pipelined_kernel<res,sweep> (fused residual + red-black sweep)",
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_launch_ms,
-                "uniform_blocks": ublocks,
-                "bytes_per_cell": f"{BYTES_PER_SWEEP_CELL} (per-cell coefficients), "
-                                  f"{BYTES_PER_SWEEP_CELL_UNIFORM} (uniform block)",
-                "reference_format_bytes_per_launch": ref_bytes,
-                "reference_format_gbs": ref_bytes / (avg_launch_ms * 1e-3) / 1e9,
+                "bytes_per_cell": BYTES_PER_SWEEP_CELL, "uniform_blocks": ublocks,
+                "format_bytes_per_launch": fmt_bytes,
+                "format_bytes_per_cell": f"{BYTES_PER_SWEEP_CELL} (per-cell coefficients), "
+                                         f"{BYTES_PER_SWEEP_CELL_UNIFORM} (uniform block)",
+                "format_gbs": fmt_bytes / (avg_launch_ms * 1e-3) / 1e9,
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"}
 
     cpu = None

@@ -195,7 +195,7 @@ int threads_of(const ffvgpu_mixed_params* prm) {
   return prm->threads_per_block > 0 ? prm->threads_per_block : 256;
 }
 int sweep_threads_of(const ffvgpu_mixed_params* prm) {
-  return prm->sweep_threads > 0 ? prm->sweep_threads : 512;
+  return prm->sweep_threads > 0 ? prm->sweep_threads : 256;
 }
 
 ffvgpu_status check_mixed(const ffvgpu_mixed_params* prm) {
@@ -244,6 +244,8 @@ int64_t iteration_bytes_per_cell(int passes, bool d64) {
 // One iteration of every running instance (all blocks of the pool).
 void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
   const MixCtx C = mix_ctx(P);
+  // CTAs of a persistent grid: SMs x resident CTAs, or the test cap
+  auto cap = [&](int n) { return P->grid_cap > 0 ? std::min(n, P->grid_cap) : n; };
   const int passes = P->m_sweeps / P->m_per_exchange;
   const float om = (float)P->m_omega;
   const bool d64 = P->m_d64 != 0;
@@ -258,18 +260,18 @@ void enqueue_iteration(ffvgpu_pool* P, cudaStream_t s) {
     for (int ps = 0; ps < passes; ++ps) {
       const bool last = ps == passes - 1;
       const void* ein = ps > 0 ? e[(ps - 1) & 1] : nullptr;
-      if (ps > 0) launch_mx_guides(s, C, P->grid_guides, ein, P->mguide, d64);
-      launch_mx_sweep(s, C, P->grid_sweep, mode, ps == 0, om, P->m_per_exchange, P->r, P->r0,
+      if (ps > 0) launch_mx_guides(s, C, cap(P->grid_guides), ein, P->mguide, d64);
+      launch_mx_sweep(s, C, cap(P->grid_sweep), mode, ps == 0, om, P->m_per_exchange, P->r, P->r0,
                       rhs, P->q, P->mcoef, P->mcoef64, ein, P->mguide, last ? hat : e[ps & 1],
                       d64);
     }
-    const int mvc = P->m_mvform == 0 ? P->grid_mvpipe : P->grid_matvec;
+    const int mvc = cap(P->m_mvform == 0 ? P->grid_mvpipe : P->grid_matvec);
     if (mode == 0)
       launch_mx_matvec(s, C, mvc, 1, P->m_threads, P->m_mvform, ph, P->A, P->q, P->r0, d64);
     else
       launch_mx_matvec(s, C, mvc, 2, P->m_threads, P->m_mvform, sh, P->A, P->tv, P->sv, d64);
   }
-  launch_mx_update(s, C, P->grid_update, P->m_threads, x, ph, sh, P->r, P->tv, P->sv, P->r0,
+  launch_mx_update(s, C, cap(P->grid_update), P->m_threads, x, ph, sh, P->r, P->tv, P->sv, P->r0,
                    d64);
 }
 
@@ -769,6 +771,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
   if (!P->mgraph || P->mgraph_iters != iterations || P->mgraph_omega != P->m_omega ||
       P->mgraph_sweeps != P->m_sweeps || P->mgraph_per != P->m_per_exchange ||
       P->mgraph_wait_ns != P->wait_ns || P->mgraph_stall != P->stall_sweep ||
+      P->mgraph_cap != P->grid_cap ||
       P->mgraph_cf != P->m_cf || P->mgraph_d64 != P->m_d64 ||
       P->mgraph_depth != P->m_depth || P->mgraph_threads != P->m_threads ||
       P->mgraph_sweep_threads != P->m_sweep_threads || P->mgraph_mvform != P->m_mvform) {
@@ -787,6 +790,7 @@ ffvgpu_status ffvgpu_mixed_advance(ffvgpu_pool* P, int32_t iterations) {
     P->mgraph_per = P->m_per_exchange;
     P->mgraph_wait_ns = P->wait_ns;
     P->mgraph_stall = P->stall_sweep;
+    P->mgraph_cap = P->grid_cap;
     P->mgraph_cf = P->m_cf;
     P->mgraph_d64 = P->m_d64;
     P->mgraph_depth = P->m_depth;
@@ -848,6 +852,15 @@ ffvgpu_status ffvgpu_mixed_poll(ffvgpu_pool* P, int32_t* finished, int32_t capac
 ffvgpu_status ffvgpu_pool_stall_next_solve(ffvgpu_pool* P) {
   if (!P) return bad("null pool");
   P->stall_sweep = 1;
+  return FFVGPU_OK;
+}
+
+ffvgpu_status ffvgpu_pool_cap_grids(ffvgpu_pool* P, int32_t ctas) {
+  if (!P) return bad("null pool");
+  if (ctas < 0) return bad("ctas must not be negative");
+  for (const ffvgpu_instance& I : P->inst)
+    if (I.running) return bad("a stepped mixed solve is running on this pool");
+  P->grid_cap = ctas;
   return FFVGPU_OK;
 }
 

@@ -157,7 +157,7 @@ struct ffvgpu_pool {
   int m_d64 = 0;  // the running solves use the FP64-data variant
   int m_depth = 1;  // sweep kernel staging depth (L2 prefetch distance in blocks)
   int m_threads = 256;  // CTA size of the update kernel (and of the A*x kernel in form 1)
-  int m_sweep_threads = 512;  // CTA size of the sweep kernel
+  int m_sweep_threads = 256;  // CTA size of the sweep kernel
   int m_mvform = 0;           // A*x kernel: 0 pipelined, 1 a block per CTA
   cudaGraphExec_t mgraph = nullptr;
   int mgraph_iters = 0;
@@ -165,6 +165,7 @@ struct ffvgpu_pool {
   int mgraph_sweeps = 0, mgraph_per = 0;
   uint64_t mgraph_wait_ns = 0;
   int mgraph_stall = 0;
+  int mgraph_cap = 0;
   int mgraph_cf = 0;
   int mgraph_d64 = 0;
   int mgraph_depth = 0, mgraph_threads = 0, mgraph_sweep_threads = 0, mgraph_mvform = -1;
@@ -178,6 +179,7 @@ struct ffvgpu_pool {
   cudaEvent_t act_ev[2] = {nullptr, nullptr};
   int act_next = 0;
   int grid_sweep = 0, grid_matvec = 0, grid_update = 0, grid_guides = 0, grid_mvpipe = 0;
+  int grid_cap = 0;  // test hook: at most this many CTAs per persistent grid (0: none)
   int grid_threads = 0;  // m_threads the grid sizes were computed for
 
   ffvgpu::KCtx ctx(const ffvgpu::BCSet& bc) const {

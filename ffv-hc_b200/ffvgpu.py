@@ -47,6 +47,7 @@ EXPORTS = [
     "ffvgpu_solve_rbgs_fixed_average", "ffvgpu_dump2", "ffvgpu_load2",
     "ffvgpu_restart_filename", "ffvgpu_remove_p", "ffvgpu_corr_u", "ffvgpu_mixed_autotune",
     "ffvgpu_pool_set_wait_limit", "ffvgpu_mixed_cancel", "ffvgpu_pool_stall_next_solve",
+    "ffvgpu_pool_cap_grids",
 ]
 
 
@@ -152,7 +153,7 @@ TUNE_SPACE = [(om, sw, per, it) for om in (1.5, 1.2) for (sw, per) in
 # kernel's form (0 pipelined, 1 a block per CTA).
 TUNE_LAUNCH = [(nt, dp, st, mv) for nt in (128, 256, 512) for dp in (1, 2, 3)
                for st in (512, 256) for mv in (0, 1)]
-TUNE_LAUNCH_DEFAULT = (256, 1, 512, 0)
+TUNE_LAUNCH_DEFAULT = (256, 1, 256, 0)
 
 
 class Request(ctypes.Structure):
@@ -191,6 +192,7 @@ def lib():
         L.ffvgpu_pool_set_stream.argtypes = [vp, vp]
         L.ffvgpu_pool_set_wait_limit.argtypes = [vp, dbl]
         L.ffvgpu_pool_stall_next_solve.argtypes = [vp]
+        L.ffvgpu_pool_cap_grids.argtypes = [vp, i32]
         L.ffvgpu_fill.argtypes = [vp, i32, dbl]
         L.ffvgpu_grid_neighbors.argtypes = [ctypes.POINTER(GridDesc), vp, vp]
         L.ffvgpu_pool_upload.argtypes = [vp, i32, vp, i32]
@@ -583,6 +585,10 @@ class Pool:
         """Test hook: the next mixed solve's sweep waits for a copy never issued."""
         _check(lib().ffvgpu_pool_stall_next_solve(self._h), "pool_stall_next_solve")
 
+    def cap_grids(self, ctas):
+        """Test hook: at most ctas CTAs per persistent grid of the mixed form (0: none)."""
+        _check(lib().ffvgpu_pool_cap_grids(self._h, int(ctas)), "pool_cap_grids")
+
     def fill(self, field, value):
         _check(lib().ffvgpu_fill(self._h, FIELD[field], float(value)), "fill")
 
@@ -871,6 +877,10 @@ class Batch:
     def set_wait_limit(self, seconds):
         _check(lib().ffvgpu_pool_set_wait_limit(self._h, float(seconds)), "pool_set_wait_limit")
 
+    def cap_grids(self, ctas):
+        """Test hook: at most ctas CTAs per persistent grid of the mixed form (0: none)."""
+        _check(lib().ffvgpu_pool_cap_grids(self._h, int(ctas)), "pool_cap_grids")
+
     def solve_mixed(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
                     epsilon=1e-8, check_every=0, restart_drop=None, restart_growth=None,
                     restart_every=None, flux_correction=False, fp64_data=False,
@@ -922,7 +932,7 @@ class Batch:
         out = [dict(omega=r.omega, sweeps=r.sweeps, sweeps_per_exchange=r.sweeps_per_exchange,
                     iterations_per_replay=r.iterations_per_replay,
                     threads_per_block=r.threads_per_block or 256, stage_depth=r.stage_depth or 1,
-                    sweep_threads=r.sweep_threads or 512, matvec_form=r.matvec_form,
+                    sweep_threads=r.sweep_threads or 256, matvec_form=r.matvec_form,
                     ms=r.ms, max_count=r.max_count, converged=bool(r.converged)) for r in recs]
         return out, best.value
 

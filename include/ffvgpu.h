@@ -147,6 +147,11 @@ ffvgpu_status ffvgpu_pool_set_wait_limit(ffvgpu_pool* pool, double seconds);
  * never issued, so that wait runs out after the wait limit and the solve ends
  * with FFVGPU_TIMEOUT.  The hook covers that one solve. */
 ffvgpu_status ffvgpu_pool_stall_next_solve(ffvgpu_pool* pool);
+/* Test hook: the mixed form's persistent kernels run at most 'ctas' CTAs
+ * (0: SMs x resident CTAs, the default), so that each CTA walks more blocks
+ * -- with one CTA, more than a chunk of its live-block list.  Results do not
+ * depend on it.  Not while a stepped solve is running. */
+ffvgpu_status ffvgpu_pool_cap_grids(ffvgpu_pool* pool, int32_t ctas);
 /* Neighbour table as derived (kind [6], ids [6][4]); for tests. */
 ffvgpu_status ffvgpu_pool_neighbors(const ffvgpu_pool* pool, int32_t block,
                                     int32_t* kind6, int32_t* ids24);
@@ -417,12 +422,12 @@ typedef struct {
   int32_t stage_depth;         /* sweep kernel: how many blocks ahead a block's data are
                                   brought into L2 (1..3; 0: 1); results do not depend on it */
   int32_t sweep_threads;       /* CTA size of the sweep kernel: 512 (each thread a 4-cell
-                                  column of one row) or 256 (of two rows); 0: 512; results
+                                  column of one row) or 256 (of two rows); 0: 256; results
                                   do not depend on it */
   int32_t matvec_form;         /* A*x kernel: 0 pipelined (one CTA of 800 threads per SM;
-                                  bulk copies of the next blocks overlap the current one),
-                                  1 a block per CTA of threads_per_block threads; results
-                                  do not depend on it */
+                                  the next blocks' tiles and coefficients are staged while
+                                  the current one is computed), 1 a block per CTA of
+                                  threads_per_block threads; results do not depend on it */
 } ffvgpu_mixed_params;
 
 /* Solves every admitted instance of the pool (a pool made from one grid is
@@ -580,7 +585,7 @@ typedef struct {
   int32_t converged;  /* out: 1 when every instance reached epsilon */
   int32_t threads_per_block;  /* as ffvgpu_mixed_params (0: 256) */
   int32_t stage_depth;        /* as ffvgpu_mixed_params (0: 1) */
-  int32_t sweep_threads;      /* as ffvgpu_mixed_params (0: 512) */
+  int32_t sweep_threads;      /* as ffvgpu_mixed_params (0: 256) */
   int32_t matvec_form;        /* as ffvgpu_mixed_params */
 } ffvgpu_tune_record;
 
