@@ -993,7 +993,12 @@ def main():
         pinned[name] = t
     xin = torch.zeros(per_field, dtype=torch.float64, pin_memory=True)
     xout = torch.empty(per_field, dtype=torch.float64, pin_memory=True)
-    h2d = (len(pinned) + 1) * per_field * 8
+    # The host buffers hold the reference layout ((16+2vc)^3 per block); from
+    # pinned memory the pack kernel reads across the link only the interior
+    # (and for x its first guide layer): those are the bytes moved up.  The
+    # download writes the whole layout (interior, guide layers, zeros).
+    host_bytes = (len(pinned) + 1) * per_field * 8
+    h2d = (len(pinned) * CELLS_PER_BLOCK + CELLS_PER_BLOCK + 6 * 256) * g.nb * 8
     d2h = per_field * 8
 
     def e2e_step():
@@ -1059,6 +1064,7 @@ def main():
             "data": "synthetic", "config": workload_config(g, args),
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "Gcell-sweeps/s", "h2d_bytes_per_step": h2d,
+                    "h2d_host_buffer_bytes": host_bytes,
                     "d2h_bytes_per_step": d2h, "ms_per_step": te_ms / args.steps},
             "clocks": clk.summary(), "gpu_launches": launches,
         }

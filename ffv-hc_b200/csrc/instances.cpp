@@ -583,11 +583,10 @@ ffvgpu_status ffvgpu_instance_upload(ffvgpu_pool* P, int32_t inst, ffvgpu_field 
     double *dst, *g;
     size_t stride;
     if ((s = field_ptr(P, f, true, &dst, &stride, &g))) return s;
-    if ((s = ensure_stage(P, per * I->count * sizeof(double)))) return s;
-    CK(cudaMemcpyAsync(P->stage, host, per * I->count * sizeof(double), cudaMemcpyHostToDevice,
-                       P->stream));
-    launch_pack(P->stream, I->count, (const double*)P->stage, vc, dst + (size_t)I->first * stride,
-                stride, g ? g + (size_t)I->first * 6 * FACE_CELLS : nullptr);
+    const double* src;
+    if ((s = host_source(P, host, per * I->count * sizeof(double), &src))) return s;
+    launch_pack(P->stream, I->count, src, vc, dst + (size_t)I->first * stride, stride,
+                g ? g + (size_t)I->first * 6 * FACE_CELLS : nullptr);
   }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(P->stream));

@@ -440,11 +440,20 @@ pack_kernel(const double* __restrict__ stage, int vc, double* __restrict__ dst, 
   const int blk = blockIdx.x, tid = threadIdx.x;
   const int w = 16 + 2 * vc;
   const double* sb = stage + (size_t)blk * w * w * w;
+  // the interior row by row (16 threads read one row of 16 consecutive
+  // values: whole sectors, also when 'stage' is pinned host memory read
+  // across the link), every load in flight before the colour-split stores
+  const int i = tid & 15, r0 = tid >> 4;
+  double v[16];
+#pragma unroll
   for (int m = 0; m < 16; ++m) {
-    const int s = tid + THREADS * m;
-    int i, j, k;
-    cell_of(s, i, j, k);
-    dst[(size_t)blk * stride + s] = sb[(i + vc) + w * ((j + vc) + w * (k + vc))];
+    const int r = r0 + 16 * m, j = r & 15, k = r >> 4;
+    v[m] = sb[(i + vc) + w * ((j + vc) + w * (k + vc))];
+  }
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    const int r = r0 + 16 * m, j = r & 15, k = r >> 4;
+    dst[(size_t)blk * stride + ((i + j + k) & 1) * HALF_CELLS + (k * 16 + j) * 8 + (i >> 1)] = v[m];
   }
   if (gdst) {
     const int a = tid & 15, b = tid >> 4;

@@ -55,6 +55,21 @@ ffvgpu_status ensure_stage(ffvgpu_pool* P, size_t bytes) {
   return s;
 }
 
+ffvgpu_status host_source(ffvgpu_pool* P, const void* host, size_t bytes, const double** src) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, host) == cudaSuccess && at.type == cudaMemoryTypeHost &&
+      at.devicePointer) {
+    *src = static_cast<const double*>(at.devicePointer);
+    return FFVGPU_OK;
+  }
+  cudaGetLastError();  // a pageable buffer is not an error here
+  ffvgpu_status s;
+  if ((s = ensure_stage(P, bytes))) return s;
+  CK(cudaMemcpyAsync(P->stage, host, bytes, cudaMemcpyHostToDevice, P->stream));
+  *src = static_cast<const double*>(P->stage);
+  return FFVGPU_OK;
+}
+
 size_t field_count(const ffvgpu_pool* P) { return (size_t)P->nb * BC; }
 
 // Device pointer and block stride of a real field's interior.
@@ -497,10 +512,9 @@ ffvgpu_status ffvgpu_pool_upload(ffvgpu_pool* P, ffvgpu_field f, const void* hos
   double* g;
   size_t stride;
   if ((s = field_ptr(P, f, true, &dst, &stride, &g))) return s;
-  if ((s = ensure_stage(P, per * P->nb * sizeof(double)))) return s;
-  CK(cudaMemcpyAsync(P->stage, host, per * P->nb * sizeof(double), cudaMemcpyHostToDevice,
-                     P->stream));
-  launch_pack(P->stream, P->nb, (const double*)P->stage, vc, dst, stride, g);
+  const double* src;
+  if ((s = host_source(P, host, per * P->nb * sizeof(double), &src))) return s;
+  launch_pack(P->stream, P->nb, src, vc, dst, stride, g);
   CK(cudaGetLastError());
   if ((f >= FFVGPU_FIELD_AP && f <= FFVGPU_FIELD_AT) || f == FFVGPU_FIELD_B) P->sys_version++;
   CK(cudaStreamSynchronize(P->stream));

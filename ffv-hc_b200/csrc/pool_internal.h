@@ -217,6 +217,11 @@ ffvgpu_status dalloc_t(ffvgpu_pool* P, T** ptr, size_t count) {
   return dalloc(P, reinterpret_cast<void**>(ptr), count * sizeof(T));
 }
 ffvgpu_status ensure_stage(ffvgpu_pool* P, size_t bytes);
+// The values of a host buffer (bytes long) as the pack kernel reads them: the
+// buffer itself when it is pinned host memory the device can address (the
+// kernel then reads across the link only what it packs), else a staging copy
+// in device memory.
+ffvgpu_status host_source(ffvgpu_pool* P, const void* host, size_t bytes, const double** src);
 size_t field_count(const ffvgpu_pool* P);
 ffvgpu_status field_ptr(ffvgpu_pool* P, int f, bool alloc, double** ptr, size_t* stride,
                         double** guides);
