@@ -843,10 +843,11 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       while (s_nlist == 0 && s_next_from < n_act);
       npos = 0;
     }
-    if (tid == 0 && npos < s_nlist) {
-      issue(s_list[npos], phase ^ 1u);
-      if (npos + depth - 1 < s_nlist) prefetch(s_list[npos + depth - 1]);
-    }
+    // the next block's copy (thread 0) and the L2 prefetch 'depth' blocks
+    // ahead (lane 0 of the second warp) are issued in parallel: every
+    // thread waits for both at the sweeps' first barrier
+    if (tid == 0 && npos < s_nlist) issue(s_list[npos], phase ^ 1u);
+    if (tid == 32 && npos + depth - 1 < s_nlist) prefetch(s_list[npos + depth - 1]);
     pos = npos;
     const double* c64 = D64 ? coef64 + (size_t)blk * COEF_WORDS + tid : nullptr;
     if (uni)
