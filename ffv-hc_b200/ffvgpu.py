@@ -855,6 +855,11 @@ class Batch:
         assert a.size == self.blocks(inst) * (16 + 2 * vc) ** 3
         _check(lib().ffvgpu_instance_upload(self._h, inst, fid, _ptr(a), vc), f"upload {field}")
 
+    def upload_ptr(self, inst, field, host_ptr, vc=2):
+        """Upload from a raw host pointer (pinned memory is read directly)."""
+        _check(lib().ffvgpu_instance_upload(self._h, inst, FIELD[field],
+                                            ctypes.c_void_p(host_ptr), vc), f"upload {field}")
+
     def download(self, inst, field, vc=2):
         fid = FIELD[field]
         w = 16 + 2 * vc

@@ -62,3 +62,20 @@ def test_pinned_upload_from_a_pointer_inside_a_buffer():
     assert_bitwise(Q.download("B", VC), P.download("B", VC), "b")
     P.close()
     Q.close()
+
+
+def test_pinned_instance_upload_matches_staged_upload():
+    """The batch pool's per-instance upload takes the same two paths."""
+    B = ffvgpu.Batch(600, 4)
+    i = B.admit_sphere(ffvgpu.sphere_problem(1, seed=4))
+    j = B.admit_sphere(ffvgpu.sphere_problem(1, seed=4))
+    n = B.blocks(i) * (16 + 2 * VC) ** 3
+    rng = np.random.default_rng(11)
+    for name in ("B", "X"):
+        a = rng.standard_normal(n)
+        B.upload(i, name, a, VC)
+        t = torch.from_numpy(a.copy()).pin_memory()
+        B.upload_ptr(j, name, t.data_ptr(), VC)
+        torch.cuda.synchronize()
+        assert_bitwise(B.download(j, name, VC), B.download(i, name, VC), name)
+    B.close()
