@@ -27,7 +27,8 @@ struct MixCtx {
   int capacity;
   int first;
   uint64_t wait_ns;    // limit of every bounded device wait (ffvgpu_pool_set_wait_limit)
-  int stall;           // test hook: the sweep issues no copy, so its first wait runs out
+  int stall;           // test hook: 1 the sweep kernel, 2 the pipelined A*x issues no copy,
+                       // so its first wait runs out
   int cf;              // coarse-fine flux correction in the FP64 residual and A*x
   int depth;           // sweep kernel: L2 prefetch distance in blocks (staging depth, >= 1)
   int sweep_threads;   // sweep kernel: 512 (a row per thread) or 256 (two rows per thread)

@@ -854,6 +854,12 @@ ffvgpu_status ffvgpu_pool_stall_next_solve(ffvgpu_pool* P) {
   return FFVGPU_OK;
 }
 
+ffvgpu_status ffvgpu_pool_stall_next_matvec(ffvgpu_pool* P) {
+  if (!P) return bad("null pool");
+  P->stall_sweep = 2;
+  return FFVGPU_OK;
+}
+
 ffvgpu_status ffvgpu_pool_cap_grids(ffvgpu_pool* P, int32_t ctas) {
   if (!P) return bad("null pool");
   if (ctas < 0) return bad("ctas must not be negative");

@@ -635,8 +635,8 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
     const bool uni = e.y & LF_UNI;
     // test hook (MixCtx::stall): nothing arrives on the barrier, so the wait
     // for this block runs out after the wait limit
-    s_copied[p] = !C.stall;
-    if (C.stall) return;
+    s_copied[p] = C.stall != 1;
+    if (C.stall == 1) return;
     const size_t gb = (size_t)b * BLOCK_CELLS;
     constexpr uint32_t VB = BLOCK_CELLS * 8;  // bytes of one FP64 vector block
     constexpr uint32_t UB = 8 * 8;            // bytes of a coefficient record
@@ -1092,7 +1092,9 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
     auto is_uni = [&](int n) { return (S.list[n].y & LF_UNI) != 0; };
     if (tid == 0 && nl > 0 && !*abort_flag) {
       // ------------------------------------------------------------ producer
-      for (int n = 0; n < nl; ++n) {
+      // (test hook MixCtx::stall == 2: no copy is issued, so the consumers'
+      // first wait for a slot runs out)
+      for (int n = 0; n < nl && C.stall != 2; ++n) {
         const size_t blk = (size_t)S.list[n].x;
         const int ns = is_uni(n) ? 1 : SLOTS;
         bool ok = true;

@@ -169,7 +169,8 @@ struct ffvgpu_pool {
   int mgraph_cf = 0;
   int mgraph_d64 = 0;
   int mgraph_depth = 0, mgraph_threads = 0, mgraph_sweep_threads = 0, mgraph_mvform = -1;
-  int stall_sweep = 0;  // test hook (ffvgpu_pool_stall_next_solve), cleared when a solve ends
+  int stall_sweep = 0;  // test hook: 1 sweep, 2 A*x (ffvgpu_pool_stall_next_solve / _matvec),
+                        // cleared when a solve ends
   int64_t m_launches = 0;
   int64_t m_bytes = 0;
   // active-block list of the persistent kernels: device [1 + capacity]

@@ -47,7 +47,7 @@ EXPORTS = [
     "ffvgpu_solve_rbgs_fixed_average", "ffvgpu_dump2", "ffvgpu_load2",
     "ffvgpu_restart_filename", "ffvgpu_remove_p", "ffvgpu_corr_u", "ffvgpu_mixed_autotune",
     "ffvgpu_pool_set_wait_limit", "ffvgpu_mixed_cancel", "ffvgpu_pool_stall_next_solve",
-    "ffvgpu_pool_cap_grids",
+    "ffvgpu_pool_cap_grids", "ffvgpu_pool_stall_next_matvec",
 ]
 
 
@@ -193,6 +193,7 @@ def lib():
         L.ffvgpu_pool_set_wait_limit.argtypes = [vp, dbl]
         L.ffvgpu_pool_stall_next_solve.argtypes = [vp]
         L.ffvgpu_pool_cap_grids.argtypes = [vp, i32]
+        L.ffvgpu_pool_stall_next_matvec.argtypes = [vp]
         L.ffvgpu_fill.argtypes = [vp, i32, dbl]
         L.ffvgpu_grid_neighbors.argtypes = [ctypes.POINTER(GridDesc), vp, vp]
         L.ffvgpu_pool_upload.argtypes = [vp, i32, vp, i32]
@@ -588,6 +589,10 @@ class Pool:
     def cap_grids(self, ctas):
         """Test hook: at most ctas CTAs per persistent grid of the mixed form (0: none)."""
         _check(lib().ffvgpu_pool_cap_grids(self._h, int(ctas)), "pool_cap_grids")
+
+    def stall_next_matvec(self):
+        """Test hook: the next mixed solve's pipelined A*x issues no copy."""
+        _check(lib().ffvgpu_pool_stall_next_matvec(self._h), "pool_stall_next_matvec")
 
     def fill(self, field, value):
         _check(lib().ffvgpu_fill(self._h, FIELD[field], float(value)), "fill")

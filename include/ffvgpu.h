@@ -147,6 +147,9 @@ ffvgpu_status ffvgpu_pool_set_wait_limit(ffvgpu_pool* pool, double seconds);
  * never issued, so that wait runs out after the wait limit and the solve ends
  * with FFVGPU_TIMEOUT.  The hook covers that one solve. */
 ffvgpu_status ffvgpu_pool_stall_next_solve(ffvgpu_pool* pool);
+/* The same for the pipelined A*x kernel (matvec_form 0): its producer issues
+ * no copy, so the consumers' first wait for a slot runs out. */
+ffvgpu_status ffvgpu_pool_stall_next_matvec(ffvgpu_pool* pool);
 /* Test hook: the mixed form's persistent kernels run at most 'ctas' CTAs
  * (0: SMs x resident CTAs, the default), so that each CTA walks more blocks
  * -- with one CTA, more than a chunk of its live-block list.  Results do not

@@ -74,6 +74,31 @@ def test_mixed_wait_limit_runs_out_and_pool_stays_usable():
     O.close()
 
 
+def test_matvec_wait_limit_runs_out_and_pool_stays_usable():
+    """The pipelined A*x's consumers wait for ring slots its producer issues;
+    the test hook makes the producer issue none, so the first wait runs out:
+    TIMEOUT naming the A*x, no copy left in flight, and the pool then solves
+    bit for bit as before."""
+    g, inp, O = problem(2)
+    P = device_problem(g, inp)
+    P.fill("X", 0.0)
+    P.set_wait_limit(0.05)
+    P.stall_next_matvec()
+    with pytest.raises(ffvgpu.FFVGPUError) as e:
+        P.solve_mixed(1.5, 8, 4, 6, 0.0)
+    assert e.value.status == ffvgpu.TIMEOUT
+    assert "A*x" in str(e.value) and "drain" not in str(e.value)
+    P.set_wait_limit(4.0)
+    P.fill("X", 0.0)
+    O.field("X")[...] = 0.0
+    ro = O.solve_mixed(1.5, 8, 4, 6, 0.0)
+    rg = P.solve_mixed(1.5, 8, 4, 6, 0.0)
+    assert_bitwise(rg["history"], ro["history"], "history after the timeout")
+    assert_bitwise(interior(P.download("X", VC)), interior(O.field("X")), "x after the timeout")
+    P.close()
+    O.close()
+
+
 def test_zero_diagonal_is_reported_as_nan_and_pool_stays_usable():
     g, inp, O = problem(1)
     P = device_problem(g, inp)
