@@ -1001,9 +1001,12 @@ mx_matvec_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ 
 //     block that streams its coefficients, eight slots of 512 cells with the
 //     seven coefficient rows and w0.
 //   gatherers (8 warps): a block ahead, its x widened to FP64 and its guide
-//     layer by the exchange rules, written into a padded tile (the layout of
-//     the sweep kernel: every neighbour of a cell, guide or interior, at a
-//     fixed offset); the loads are issued before the tile frees up.
+//     layer by the exchange rules, written into a padded tile: per colour
+//     [k + 1][j + 1][i >> 1] with rows of 8 values (k, j in -1..16), so every
+//     neighbour of a cell is at a fixed offset but the x-face guides, which
+//     sit in two arrays of their own; with rows of 8 the two rows a half-warp
+//     reads fall into disjoint banks.  The loads are issued before the tile
+//     frees up.
 //   consumers (16 warps): consumer t takes cells q = 512 mm + t of each
 //     colour, which makes it the block tree's virtual thread t: the per-block
 //     sums are those of mx_reduce; the ticket of an instance is advanced once
@@ -1024,10 +1027,14 @@ constexpr int NTHREADS = CONS0 + NCONS;            // 800
 constexpr int CAP = NTHREADS;                      // list entries per chunk
 constexpr int ROLE_MATVEC = 32;                    // SolveState::timeout_where bit
 static_assert(SLOT_BYTES == BLOCK_CELLS * 8, "a slot holds a uniform block's w0");
+// the tile: row pitch (i >> 1 in 0..7), plane pitch (rows j = -1..16) and
+// colour half (planes k = -1..16)
+constexpr int TR = 8, TP = 18 * TR, TH = 18 * TP, TT = 2 * TH;
 
 struct __align__(128) Smem {
   double ring[STAGES][ROWS][SLOT_CELLS];  // 96 KB
-  double tile[2][TILE];                   // 107 KB: x of the current / next block with guides
+  double tile[2][TT];                     // 81 KB: x of the current / next block, j/k guides
+  double xg[2][2][FACE_CELLS];            // 8 KB: their x-face guides [face][j + 16 k]
   double urec[2][8];                      // coefficient records of the blocks in the tiles
   double ws[2][CONS_WARPS];               // warp sums of the block tree
   int2 list[CAP];                         // the chunk's live entries
@@ -1039,10 +1046,20 @@ struct __align__(128) Smem {
 };
 static_assert(sizeof(Smem) <= 227 * 1024, "shared memory of one CTA");
 
-// The first guide layer of a padded tile read as [face][p] (flux correction).
+// Tile position of the j/k-face guide at (face, p = u + 16 v), face 2..5.
+__device__ __forceinline__ int tile_guide(int face, int p) {
+  const int u = p & 15, v = p >> 4, out = (face & 1) ? 16 : -1;
+  return face < 4 ? ((u + out + v) & 1) * TH + (v + 1) * TP + (out + 1) * TR + (u >> 1)
+                  : ((u + v + out) & 1) * TH + (out + 1) * TP + (v + 1) * TR + (u >> 1);
+}
+// The first guide layer of a tile read as [face][p] (flux correction).
 struct TileGuides {
   const double* T;
-  __device__ double operator[](int g) const { return T[guide_slot(g >> 8, g & 255)]; }
+  const double* XG;  // [2][256]
+  __device__ double operator[](int g) const {
+    const int f = g >> 8, p = g & 255;
+    return f < 2 ? XG[f * FACE_CELLS + p] : T[tile_guide(f, p)];
+  }
 };
 
 __device__ __forceinline__ void consumer_sync() {
@@ -1153,7 +1170,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
           const int s0 = VW * (gt + NGATHER * kk);
           const int c = s0 >> 11, q = s0 & 2047;
           const int ih = q & 7, j = (q >> 3) & 15, k = q >> 7;
-          double* d = T + c * SH + (k + 1) * SQ + (j + 1) * SP + ih + 1;
+          double* d = T + c * TH + (k + 1) * TP + (j + 1) * TR + ih;
           if constexpr (sizeof(ET) == 4) {
             d[0] = (double)xv[kk].x;
             d[1] = (double)xv[kk].y;
@@ -1167,8 +1184,13 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
           const int f = 2 * r + grp;
-          T[guide_slot(f, p0)] = gv[r][0];
-          T[guide_slot(f, p1)] = gv[r][1];
+          if (f < 2) {
+            S.xg[b][f][p0] = gv[r][0];
+            S.xg[b][f][p1] = gv[r][1];
+          } else {
+            T[tile_guide(f, p0)] = gv[r][0];
+            T[tile_guide(f, p1)] = gv[r][1];
+          }
           if (CF && p0 == 0) S.snb[b][f] = nfs[CF ? r : 0];
         }
         if (gt < 8) S.urec[b][gt] = ur;
@@ -1182,7 +1204,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
       // this thread's cells q = 512 mm + ct: (2 ih + p, j, k0 + 4 mm), where
       // the parity p of the row is the same for every mm
       const int ih = ct & 7, jr = (ct >> 3) & 15, k0 = ct >> 7;
-      const int pos0 = (k0 + 1) * SQ + (jr + 1) * SP + ih + 1;  // tile position, mm = 0
+      const int pos0 = (k0 + 1) * TP + (jr + 1) * TR + ih;  // tile position, mm = 0
       for (int n = 0; n < nl; ++n) {
         const int Mg = M0 + n, b = Mg & 1;
         const uint32_t par = (Mg >> 1) & 1;
@@ -1191,6 +1213,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
         const bool uni = ent.y & LF_UNI;
         live = live && mbar_wait(&S.gfull[b], par, abort_flag, ROLE_MATVEC, C.wait_ns);
         const double* T = S.tile[b];
+        const double* XG = &S.xg[b][0][0];
         double u[7];
 #pragma unroll
         for (int a = 0; a < 7; ++a) u[a] = uni ? S.urec[b][a] : 0.0;
@@ -1204,11 +1227,15 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
           const int p = (jr + k0 + c) & 1;
-          const double* own = T + c * SH + pos0;         // the cell
-          const double* oth = T + (1 - c) * SH + pos0;   // its position in the other colour
+          const double* own = T + c * TH + pos0;         // the cell
+          const double* oth = T + (1 - c) * TH + pos0;   // its position in the other colour
+          // the x-face guides take the place of the west (i = 0) and east
+          // (i = 15) neighbours
+          const bool gw = ih == 0 && p == 0, ge = ih == 7 && p == 1;
 #pragma unroll 2
           for (int mm = 0; mm < SLOTS / 2; ++mm) {
-            const int q = mm * NCONS + ct, s = c * HALF_CELLS + q, o = mm * 4 * SQ;
+            const int q = mm * NCONS + ct, s = c * HALF_CELLS + q, o = mm * 4 * TP;
+            const int gq = jr + 16 * (k0 + 4 * mm);  // the x-face guides' position
             double k[7], wv = 0.0;
             if (uni) {
 #pragma unroll
@@ -1228,17 +1255,18 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
             }
             if (!live) continue;
             // neighbours w, e (i -+ 1: other colour, columns ih + p - 1 and
-            // ih + p of it), s, n (rows -+ 1), b, t (planes -+ 1); the guide
-            // layer sits in the tile's padding
-            const double xw = oth[o - 1 + p], xe = oth[o + p];
-            const double xs = oth[o - SP], xn = oth[o + SP];
-            const double xb = oth[o - SQ], xt = oth[o + SQ];
+            // ih + p of it), s, n (rows -+ 1), b, t (planes -+ 1); the j and k
+            // guides sit in the tile's border rows and planes
+            const double xw = gw ? XG[gq] : oth[o - 1 + p];
+            const double xe = ge ? XG[FACE_CELLS + gq] : oth[o + p];
+            const double xs = oth[o - TR], xn = oth[o + TR];
+            const double xb = oth[o - TP], xt = oth[o + TP];
             const double xp = own[o];
             double yv = k[1] * xw + k[2] * xe + k[3] * xs + k[4] * xn + k[5] * xb + k[6] * xt +
                         k[0] * xp;
             if (CF)  // coarse-fine flux correction: y = A x + delta
               yv = cf_delta<false>(x, (const double*)nullptr, A, C.nbr, C.dx, C.bc, S.snb[b],
-                                   TileGuides{T}, xp, s, yv, [&](int f) { return k[1 + f]; });
+                                   TileGuides{T, XG}, xp, s, yv, [&](int f) { return k[1 + f]; });
             y[base + s] = yv;
             acc[0][c] += yv * wv;
             if (NV == 2) acc[NV - 1][c] += yv * yv;
