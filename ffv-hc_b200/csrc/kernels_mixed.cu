@@ -744,12 +744,19 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
       const double* rs = uni ? sd : r + gbase;
       const double* qs = uni ? sd + BLOCK_CELLS : q + gbase;
       const double* ps = uni ? sd + 2 * BLOCK_CELLS : pv + gbase;
+      // With two rows per thread, threads of odd k groups take their rows in
+      // the other order: the two 8-thread groups of a half-warp, 512 doubles
+      // apart in the slot (the same banks), then read 8 doubles apart mod 16
+      // (disjoint banks).  The iterate starts at 0, so only stores follow
+      // the order.
+      const int jsw = JJ == 2 ? (tid >> 3) & 1 : 0;
 #pragma unroll
       for (int c = 0; c < 2; ++c)
 #pragma unroll
-        for (int jj = 0; jj < JJ; ++jj)
+        for (int jo = 0; jo < JJ; ++jo)
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
+          const int jj = jo ^ jsw;
           const int sl = s0 + c * HALF_CELLS + jj * 8 + h * 128;
           const size_t s = gbase + sl;
           double rhs;
@@ -766,8 +773,8 @@ mx_sweep_kernel(MixCtx C, float omega, int nsweep, const double* __restrict__ r,
           }
           pv[s] = rhs;
           V[((c * JJ + jj) * 4 + h) * PTS + tid] = rhs;
-          E[c][jj][h] = 0.0;
-          T[o0 + c * SH + jj * SP + h * SQ] = 0.0;
+          E[c][jo][h] = 0.0;
+          T[o0 + c * SH + jo * SP + h * SQ] = 0.0;  // every cell of the thread, in row order
         }
     } else {
 #pragma unroll
