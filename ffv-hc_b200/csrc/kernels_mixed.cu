@@ -39,7 +39,6 @@
 // instance's blocks, so an instance gets the same bits alone or in a batch.
 #include <algorithm>
 #include <cfloat>
-#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "ffvgpu_async.cuh"
@@ -1149,14 +1148,13 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
         const int blk = S.list[n].x;
         const double dx = C.dx[blk];
         // everything this thread writes into the tile, loaded before the tile
-        // (block Mg - 2) is free: 16 values of x (cells 4 (gt + 256 kk) + e),
-        // and two positions of alternate faces of the guide layer
-        constexpr int VW = 16 / (int)sizeof(ET);  // values per 16-byte load
-        using V16 = typename std::conditional<sizeof(ET) == 4, float4, double2>::type;
-        V16 xv[16 / VW];
-        const V16* xb = reinterpret_cast<const V16*>(x + (size_t)blk * BLOCK_CELLS);
+        // (block Mg - 2) is free: 16 values of x (cells gt + 256 m: a
+        // half-warp's stores then fill 16 consecutive tile positions, one
+        // bank each), and two positions of alternate faces of the guide layer
+        ET xv[16];
+        const ET* xb = x + (size_t)blk * BLOCK_CELLS;
 #pragma unroll
-        for (int kk = 0; kk < 16 / VW; ++kk) xv[kk] = __ldg(xb + gt + NGATHER * kk);
+        for (int m = 0; m < 16; ++m) xv[m] = __ldg(xb + gt + NGATHER * m);
         double gv[3][2];
         FaceNbr nfs[CF ? 3 : 1];
 #pragma unroll
@@ -1172,21 +1170,11 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
           break;
         double* T = S.tile[b];
 #pragma unroll
-        for (int kk = 0; kk < 16 / VW; ++kk) {
-          // VW consecutive cells of one row: one run of the padded tile
-          const int s0 = VW * (gt + NGATHER * kk);
+        for (int m = 0; m < 16; ++m) {
+          const int s0 = gt + NGATHER * m;
           const int c = s0 >> 11, q = s0 & 2047;
           const int ih = q & 7, j = (q >> 3) & 15, k = q >> 7;
-          double* d = T + c * TH + (k + 1) * TP + (j + 1) * TR + ih;
-          if constexpr (sizeof(ET) == 4) {
-            d[0] = (double)xv[kk].x;
-            d[1] = (double)xv[kk].y;
-            d[2] = (double)xv[kk].z;
-            d[3] = (double)xv[kk].w;
-          } else {
-            d[0] = xv[kk].x;
-            d[1] = xv[kk].y;
-          }
+          T[c * TH + (k + 1) * TP + (j + 1) * TR + ih] = (double)xv[m];
         }
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
