@@ -31,7 +31,7 @@ struct MixCtx {
                        // so its first wait runs out
   int cf;              // coarse-fine flux correction in the FP64 residual and A*x
   int depth;           // sweep kernel: L2 prefetch distance in blocks (staging depth, >= 1)
-  int sweep_threads;   // sweep kernel: 512 (a row per thread) or 256 (two rows per thread)
+  int sweep_threads;   // sweep kernel: 256 (two rows per thread, the default) or 512 (one row)
 };
 
 // CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel,

@@ -50,7 +50,6 @@ namespace ffvgpu {
 namespace {
 
 constexpr int MT = 256;  // FP64 kernels: 16 cells per thread
-constexpr int PT = 512;  // sweep kernel, default: 8 cells per thread (256 threads: 16)
 
 // Shared-memory tile of the sweep kernel: per colour a padded
 // [k + 1][j + 1][ii] array of FP64 iterate values, k, j in -1..16 and
