@@ -1564,4 +1564,56 @@ int orc_mixed(Oracle* O, double omega, int sweeps, int per, int countMax, double
   return 0;
 }
 
+// The precision form as a defect correction (no counterpart in the
+// reference): r = b - A x in FP64 (CalcR, FFVILS.h:204-245, with x's guide
+// layer exchanged first); e = M(r), the RB-SOR preconditioner of orc_mixed on
+// 32-bit data (mixed_precondition, e from 0, widened to double); x = x + e
+// (axpy with a = 1, blas.f90:329-361); until sqrt(r.r / b.b) <= epsilon
+// (IsConverged, FFVILS.h:24-47).  hist[c - 1] is the residual after c
+// corrections; the early exits mirror orc_mixed's (b.b, then r.r, below
+// FLT_MIN: count 0).
+int orc_mixed_dc(Oracle* O, double omega, int sweeps, int per, int countMax, double epsilon,
+                 int data64, int* count, double* residual, double* hist) {
+  Oracle& R = *O;
+  if (countMax <= 0) {
+    *count = 1;
+    *residual = 0.0;
+    return 0;
+  }
+  const double bb = DOT(R, OF_B, OF_B);
+  if (std::fabs(bb) < FLT_MIN) {
+    *residual = 0.0;
+    *count = 0;
+    return 0;
+  }
+  Coef32 C;
+  mixed_coef(R, C, data64 != 0);
+  const float om = (float)omega;
+  CalcR(R, OF_R, OF_X, OF_B);
+  double rr = DOT(R, OF_R, OF_R);
+  if (std::fabs(rr) < FLT_MIN) {
+    *residual = rr;
+    *count = 0;
+    return 0;
+  }
+  int c;
+  for (c = 1; c <= countMax; ++c) {
+    mixed_precondition(R, C, OF_R, OF_P_, om, sweeps, per, data64 != 0);
+    AXPY(R, OF_X, OF_P_, 1.0);
+    impose_bc_p(R, OF_X);
+    CalcR(R, OF_R, OF_X, OF_B);
+    rr = DOT(R, OF_R, OF_R);
+    const int st = is_converged(*residual, rr, bb, epsilon);
+    if (hist) hist[c - 1] = *residual;
+    if (st < 0) {
+      *count = c;
+      return 2;
+    }
+    if (st == 1) break;
+  }
+  impose_bc_p(R, OF_X);
+  *count = (c > countMax) ? countMax + 1 : c;
+  return 0;
+}
+
 }  // extern "C"

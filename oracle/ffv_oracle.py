@@ -71,6 +71,7 @@ def lib():
         L.orc_rbgs_fixed_average.argtypes = [vp, dbl, ctypes.c_long, i32, dbl, vp, vp, vp]
         L.orc_bicgstab_restart.argtypes = [vp, dbl, i32, i32, dbl, dbl, vp, vp, vp]
         L.orc_mixed.argtypes = [vp, dbl, i32, i32, i32, dbl, dbl, dbl, i32, i32, i32, vp, vp, vp]
+        L.orc_mixed_dc.argtypes = [vp, dbl, i32, i32, i32, dbl, i32, vp, vp, vp]
         L.orc_cf_apply.argtypes = [vp, i32, i32, i32]
         L.orc_cf_apply.restype = None
         L.orc_cf_cells.restype = ctypes.c_long
@@ -321,6 +322,14 @@ class Oracle:
                                              float(restart_growth), int(restart_every),
                                              int(bool(flux_correction)), int(bool(fp64_data))),
                            count_max)
+
+    def solve_mixed_dc(self, omega=1.5, sweeps=8, sweeps_per_exchange=4, count_max=1000,
+                       epsilon=1e-8, fp64_data=False):
+        """The precision form as a defect correction: r = b - A x in FP64, e the
+        RB-SOR preconditioner of solve_mixed applied to r, x += e."""
+        return self._solve(lib().orc_mixed_dc, (float(omega), int(sweeps),
+                                                int(sweeps_per_exchange), int(count_max),
+                                                float(epsilon), int(bool(fp64_data))), count_max)
 
     def calc_ax(self, out, x, flux_correction=False):
         """out = A x (CalcAx, FFVILS.h:164-202), with flux_correction the
