@@ -60,6 +60,13 @@ void launch_mx_sweep(cudaStream_t s, const MixCtx& C, int count, int mode, bool 
 // Guide layer [blk][6][256] (FP64) of the iterate e for the next pass.
 void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const void* e, double* guides,
                       bool d64);
+// The active list raw ([0] = n, then block ids) reordered into act: the
+// blocks that stream their coefficients (ucoef flag 0) first, then the
+// uniform ones, each in list order.  The persistent grids walk items
+// c, c + grid, ..., so the expensive blocks are dealt out evenly; results do
+// not depend on the order (every sum runs over blocks in block order).
+void launch_mx_order_active(cudaStream_t s, const int32_t* raw, const double* ucoef,
+                            int32_t* act);
 // y = A x with its dot products; form 0: the pipelined kernel ('count' CTAs,
 // one per SM), form 1: a block per CTA of 'threads' threads.
 void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads, int form,

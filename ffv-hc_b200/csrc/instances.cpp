@@ -42,6 +42,7 @@ void release_instances(ffvgpu_pool* P) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (P->act_d) cudaFree(P->act_d);
+  if (P->act_raw_d) cudaFree(P->act_raw_d);
   for (int k = 0; k < 2; ++k) {
     if (P->act_h[k]) cudaFreeHost(P->act_h[k]);
     if (P->act_ev[k]) cudaEventDestroy(P->act_ev[k]);
@@ -95,8 +96,10 @@ ffvgpu_status ensure_inst_device(ffvgpu_pool* P) {
 }
 
 // Publishes the blocks of every running instance to the persistent kernels
-// (stream-ordered: work enqueued later sees the new list).  A staging buffer
-// is rewritten only after its previous copy has been consumed.
+// (stream-ordered: work enqueued later sees the new list), the blocks that
+// stream their coefficients first (launch_mx_order_active), so that the
+// persistent grids deal them out evenly.  A staging buffer is rewritten only
+// after its previous copy has been consumed.
 ffvgpu_status publish_active(ffvgpu_pool* P) {
   const int k = P->act_next;
   P->act_next ^= 1;
@@ -107,9 +110,11 @@ ffvgpu_status publish_active(ffvgpu_pool* P) {
     if (I.running)
       for (int b = 0; b < I.count; ++b) h[1 + n++] = I.first + b;
   h[0] = n;
-  CK(cudaMemcpyAsync(P->act_d, h, sizeof(int32_t) * (size_t)(n + 1), cudaMemcpyHostToDevice,
-                     P->stream));
+  CK(cudaMemcpyAsync(P->act_raw_d, h, sizeof(int32_t) * (size_t)(n + 1),
+                     cudaMemcpyHostToDevice, P->stream));
   CK(cudaEventRecord(P->act_ev[k], P->stream));
+  launch_mx_order_active(P->stream, P->act_raw_d, P->mucoef, P->act_d);
+  CK(cudaGetLastError());
   return FFVGPU_OK;
 }
 
@@ -117,7 +122,8 @@ ffvgpu_status ensure_mixed_buffers(ffvgpu_pool* P, bool d64) {
   ffvgpu_status s;
   const size_t n = field_count(P);
   if (!P->act_d) {
-    if ((s = dalloc_t(P, &P->act_d, n / BC + 1))) return s;
+    if ((s = dalloc_t(P, &P->act_d, n / BC + 1)) || (s = dalloc_t(P, &P->act_raw_d, n / BC + 1)))
+      return s;
     CK(cudaMemsetAsync(P->act_d, 0, sizeof(int32_t), P->stream));
     for (int k = 0; k < 2; ++k) {
       CK(cudaMallocHost(&P->act_h[k], sizeof(int32_t) * (n / BC + 1)));

@@ -1585,6 +1585,60 @@ static void matvec_nt(cudaStream_t s, const MixCtx& C, int count, int ndot, int 
     matvec_launch<ET, 256>(s, C, count, ndot, x, A, y, w0);
 }
 
+// The active list with the blocks that stream their coefficients first:
+// one CTA, a stable partition chunk by chunk (warp ballots, warp offsets in
+// order), so the order is the same on every run.
+__global__ void __launch_bounds__(1024)
+mx_order_active_kernel(const int32_t* __restrict__ raw, const double* __restrict__ ucoef,
+                       int32_t* __restrict__ act) {
+  __shared__ int ws[32], wu[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n = raw[0];
+  auto streams = [&](int b) { return ucoef[(size_t)b * 8 + 7] == 0.0; };
+  int cnt = 0;
+  for (int i = tid; i < n; i += 1024) cnt += streams(raw[1 + i]) ? 1 : 0;
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+  if (lane == 0) ws[warp] = cnt;
+  __syncthreads();
+  int nstream = 0;
+  for (int w = 0; w < 32; ++w) nstream += ws[w];
+  __syncthreads();
+  int base_s = 0, base_u = nstream;
+  const unsigned below = (1u << lane) - 1u;
+  for (int c0 = 0; c0 < n; c0 += 1024) {
+    const int i = c0 + tid;
+    const int b = i < n ? raw[1 + i] : 0;
+    const bool st = i < n && streams(b), un = i < n && !st;
+    const unsigned ms = __ballot_sync(0xffffffffu, st), mu = __ballot_sync(0xffffffffu, un);
+    if (lane == 0) {
+      ws[warp] = __popc(ms);
+      wu[warp] = __popc(mu);
+    }
+    __syncthreads();
+    int os = base_s, ou = base_u, ts = 0, tu = 0;
+    for (int w = 0; w < 32; ++w) {
+      if (w < warp) {
+        os += ws[w];
+        ou += wu[w];
+      }
+      ts += ws[w];
+      tu += wu[w];
+    }
+    if (st) act[1 + os + __popc(ms & below)] = b;
+    if (un) act[1 + ou + __popc(mu & below)] = b;
+    base_s += ts;
+    base_u += tu;
+    __syncthreads();  // ws, wu are rewritten by the next chunk
+  }
+  if (tid == 0) act[0] = n;
+}
+
+void launch_mx_order_active(cudaStream_t s, const int32_t* raw, const double* ucoef,
+                            int32_t* act) {
+  mx_order_active_kernel<<<1, 1024, 0, s>>>(raw, ucoef, act);
+}
+
 template <typename ET>
 static void matvec_pipe(cudaStream_t s, const MixCtx& C, int count, int ndot, const ET* x,
                         const double* A, double* y, const double* w0) {

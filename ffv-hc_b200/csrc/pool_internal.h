@@ -176,6 +176,7 @@ struct ffvgpu_pool {
   // active-block list of the persistent kernels: device [1 + capacity]
   // (count, then block ids), refilled from two pinned staging buffers
   int32_t* act_d = nullptr;
+  int32_t* act_raw_d = nullptr;  // the host list as uploaded, before mx_order_active
   int32_t* act_h[2] = {nullptr, nullptr};
   cudaEvent_t act_ev[2] = {nullptr, nullptr};
   int act_next = 0;
