@@ -21,8 +21,8 @@ struct KCtx {
   int nb;
   int first;
   uint64_t wait_ns;    // limit of every bounded device wait (ffvgpu_pool_set_wait_limit)
-  // [blocks][8] uniform records of the sweep's coefficient stream
-  // (launch_pack_stream), or null: every block streams all its coefficients
+  // [blocks][8] uniform records of A (launch_pack_stream, launch_urec), or
+  // null: every block streams all its coefficients
   const double* urec;
 };
 
@@ -38,6 +38,10 @@ void launch_rbgs(cudaStream_t s, const KCtx& C, bool res, bool sweep, const doub
 // those seven coefficients, else 0.0), adding the uniform blocks to *ucount.
 void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b, double* stream,
                         double* urec, int32_t* ucount);
+// The uniform records alone (the record format of launch_pack_stream).
+void launch_urec(cudaStream_t s, int nb, const double* A, double* urec, int32_t* ucount);
+// Jacobi sweep; a block with a set uniform record (C.urec) reads its seven
+// coefficients from it.
 void launch_jacobi(cudaStream_t s, const KCtx& C, bool from_zero, bool dot, const double* xin,
                    double* xout, const double* A, const double* b, double omega,
                    double* partials, SolveState* st);
@@ -45,10 +49,6 @@ void launch_calc_r(cudaStream_t s, const KCtx& C, const double* x, const double*
                    const double* A, const double* b, double* r, SolveState* st);
 void launch_p_update(cudaStream_t s, const KCtx& C, const double* z, double* p, int first,
                      SolveState* st);
-void launch_ax_dot(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
-                   double* partials, SolveState* st);
-void launch_ax_dot_y(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
-                     const double* y, double* partials, SolveState* st, int fin);
 // p = r on the first iteration of a cycle (st->cycle == 1), else the update.
 void launch_bicg_p(cudaStream_t s, const KCtx& C, const double* r, double* p, const double* q,
                    SolveState* st);

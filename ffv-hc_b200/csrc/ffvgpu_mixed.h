@@ -32,6 +32,10 @@ struct MixCtx {
   int cf;              // coarse-fine flux correction in the FP64 residual and A*x
   int depth;           // sweep kernel: L2 prefetch distance in blocks (staging depth, >= 1)
   int sweep_threads;   // sweep kernel: 256 (two rows per thread, the default) or 512 (one row)
+  // pipelined A*x only: 0 the mixed form's finalisers, else the FP64
+  // solver's (one instance): FIN_BI_QR0 or FIN_CG_QP on the one sum, or
+  // FIN_BI_TS on the first of two sums and FIN_BI_TT on the second
+  int fin = 0;
 };
 
 // CTAs of the persistent grids: SMs x resident CTAs per SM of each kernel,
@@ -68,7 +72,7 @@ void launch_mx_guides(cudaStream_t s, const MixCtx& C, int count, const void* e,
 void launch_mx_order_active(cudaStream_t s, const int32_t* raw, const double* ucoef,
                             int32_t* act);
 // y = A x with its dot products; form 0: the pipelined kernel ('count' CTAs,
-// one per SM), form 1: a block per CTA of 'threads' threads.
+// one per SM), form 1: a block per CTA of 'threads' threads (C.fin 0 only).
 void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads, int form,
                       const void* x, const double* A, double* y, const double* w0, bool d64);
 // Coarse-fine flux mismatch per face cell of the (block, face) pairs

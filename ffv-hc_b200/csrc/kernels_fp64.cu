@@ -134,23 +134,21 @@ __device__ void reduce_finalize(const double (&acc)[2][2], double* __restrict__ 
 // Jacobi smoother (bils.f90:5-55) with b = bvec.  FROM_ZERO: x0 is the
 // zero field of FFVILS::Fill(z, 0) (blas.f90:5-33, guides included).
 // DOT: also forms b.x1 (FFVILS.h:712-718 DOT(r, z), r = bvec).
+// A block whose uniform record (KCtx::urec) is set has the same seven
+// coefficients in every cell: they are read once from the record, and the
+// block moves b and x only (the same values, so the same results).
 // ---------------------------------------------------------------------------
-template <bool FROM_ZERO, bool DOT>
-__global__ void __launch_bounds__(THREADS, 3)
-jacobi_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
-              const double* __restrict__ A, const double* __restrict__ bvec, double omega,
-              double* __restrict__ partials, SolveState* st) {
-  if (solve_done(st)) return;
-  __shared__ double xs[FROM_ZERO ? 1 : TILE];
-  const int blk = blockIdx.x, tid = threadIdx.x;
-  if (!FROM_ZERO) {
-    stage_tile(xs, xin, blk, C, nullptr);
-    __syncthreads();
-  }
-  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
-  const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
-  double* xo = xout + (size_t)blk * BLOCK_CELLS;
-  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+template <bool FROM_ZERO, bool DOT, bool UNI>
+__device__ __forceinline__ void jacobi_cells(const double* __restrict__ xs,
+                                             const double* __restrict__ Ab,
+                                             const double* __restrict__ ur,
+                                             const double* __restrict__ bb, double* __restrict__ xo,
+                                             double omega, double (&acc)[2][2]) {
+  const int tid = threadIdx.x;
+  double u[7];
+#pragma unroll
+  for (int a = 0; a < 7; ++a) u[a] = UNI ? __ldg(ur + a) : 0.0;
+  auto coef = [&](int a, int s) { return UNI ? u[a] : __ldg(Ab + a * BLOCK_CELLS + s); };
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
 #pragma unroll 4
@@ -167,15 +165,38 @@ jacobi_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
         xb = xs[t - TP]; xt = xs[t + TP]; xp = xs[t];
       }
       const double bv = __ldg(bb + s);
-      const double r = bv - __ldg(Ab + 4096 + s) * xw - __ldg(Ab + 8192 + s) * xe -
-                       __ldg(Ab + 12288 + s) * xS - __ldg(Ab + 16384 + s) * xn -
-                       __ldg(Ab + 20480 + s) * xb - __ldg(Ab + 24576 + s) * xt;
-      const double x_tmp = r / __ldg(Ab + s);
+      const double r = bv - coef(1, s) * xw - coef(2, s) * xe - coef(3, s) * xS -
+                       coef(4, s) * xn - coef(5, s) * xb - coef(6, s) * xt;
+      const double x_tmp = r / coef(0, s);
       const double x1 = xp - omega * (xp - x_tmp);
       xo[s] = x1;
       if (DOT) acc[c][m & 1] += bv * x1;
     }
   }
+}
+
+template <bool FROM_ZERO, bool DOT>
+__global__ void __launch_bounds__(THREADS, 3)
+jacobi_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
+              const double* __restrict__ A, const double* __restrict__ bvec, double omega,
+              double* __restrict__ partials, SolveState* st) {
+  if (solve_done(st)) return;
+  __shared__ double xs[FROM_ZERO ? 1 : TILE];
+  const int blk = blockIdx.x;
+  const double* ur = C.urec ? C.urec + (size_t)blk * 8 : nullptr;
+  const bool uni = ur && __ldg(ur + 7) != 0.0;
+  if (!FROM_ZERO) {
+    stage_tile(xs, xin, blk, C, nullptr);
+    __syncthreads();
+  }
+  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
+  const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
+  double* xo = xout + (size_t)blk * BLOCK_CELLS;
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+  if (uni)
+    jacobi_cells<FROM_ZERO, DOT, true>(xs, Ab, ur, bb, xo, omega, acc);
+  else
+    jacobi_cells<FROM_ZERO, DOT, false>(xs, Ab, ur, bb, xo, omega, acc);
   if (DOT) reduce_finalize(acc, partials, st, FIN_CG_RR1, 0);
 }
 
@@ -220,40 +241,6 @@ p_update_kernel(const double* __restrict__ z, double* __restrict__ p, int first,
     const size_t s = base + threadIdx.x + THREADS * m;
     p[s] = first ? z[s] : (z[s] + beta * p[s]);
   }
-}
-
-// q = A p (calc_ax, bils.f90:162-206) and q.y (DOT(q, y), blas.f90:466-499):
-// y = p for CG (FFVILS.h:750-756), r0 or s for BiCGSTAB (FFVILS.h:890, 923).
-__global__ void __launch_bounds__(THREADS, 3)
-ax_dot_kernel(KCtx C, const double* __restrict__ p, const double* __restrict__ A,
-              double* __restrict__ q, const double* __restrict__ y,
-              double* __restrict__ partials, SolveState* st, int fin) {
-  if (solve_done(st)) return;
-  __shared__ double xs[TILE];
-  const int blk = blockIdx.x, tid = threadIdx.x;
-  stage_tile(xs, p, blk, C, nullptr);
-  __syncthreads();
-  const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
-  double* qo = q + (size_t)blk * BLOCK_CELLS;
-  const double* yb = y ? y + (size_t)blk * BLOCK_CELLS : nullptr;
-  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-#pragma unroll
-  for (int c = 0; c < 2; ++c) {
-#pragma unroll 4
-    for (int m = 0; m < 8; ++m) {
-      const int s = c * HALF_CELLS + tid + THREADS * m;
-      int i, j, k;
-      cell_of(s, i, j, k);
-      const int t = tix(i, j, k);
-      const double v = __ldg(Ab + 4096 + s) * xs[t - 1] + __ldg(Ab + 8192 + s) * xs[t + 1] +
-                       __ldg(Ab + 12288 + s) * xs[t - TW] + __ldg(Ab + 16384 + s) * xs[t + TW] +
-                       __ldg(Ab + 20480 + s) * xs[t - TP] + __ldg(Ab + 24576 + s) * xs[t + TP] +
-                       __ldg(Ab + s) * xs[t];
-      qo[s] = v;
-      acc[c][m & 1] += v * (yb ? __ldg(yb + s) : xs[t]);
-    }
-  }
-  reduce_finalize(acc, partials, st, fin, 0);
 }
 
 // BiCGSTAB p update (FFVILS.h:853-871): first iteration p = r (copy); after
@@ -716,23 +703,25 @@ fold_bc_kernel(KCtx C, double* __restrict__ A, double* __restrict__ bvec) {
 }
 
 // A (7 arrays) and b -> the sweep's coefficient stream (STREAM_BLOCK per block).
+// Without STREAM only the uniform records are written.
+template <bool STREAM>
 __global__ void __launch_bounds__(THREADS)
 pack_stream_kernel(const double* __restrict__ A, const double* __restrict__ b,
                    double* __restrict__ stream, double* __restrict__ urec,
                    int32_t* __restrict__ ucount) {
   const int blk = blockIdx.x, tid = threadIdx.x;
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
-  double* sb = stream + (size_t)blk * STREAM_BLOCK;
+  double* sb = STREAM ? stream + (size_t)blk * STREAM_BLOCK : nullptr;
   bool same = true;
   for (int m = 0; m < 16; ++m) {
     const int s = tid + THREADS * m;  // chunk m, cell tid
-    double* dst = sb + (size_t)m * STREAM_CHUNK + tid;
+    double* dst = STREAM ? sb + (size_t)m * STREAM_CHUNK + tid : nullptr;
     for (int a = 0; a < 7; ++a) {
       const double v = Ab[(size_t)a * BLOCK_CELLS + s];
-      dst[a * 256] = v;
+      if (STREAM) dst[a * 256] = v;
       same = same && __double_as_longlong(v) == __double_as_longlong(Ab[(size_t)a * BLOCK_CELLS]);
     }
-    dst[7 * 256] = b[(size_t)blk * BLOCK_CELLS + s];
+    if (STREAM) dst[7 * 256] = b[(size_t)blk * BLOCK_CELLS + s];
   }
   // a uniform block (all seven coefficients bitwise equal to cell 0's): the
   // sweep kernel copies only b of its stream and takes Ap..At from here
@@ -774,14 +763,6 @@ void launch_calc_r(cudaStream_t s, const KCtx& C, const double* x, const double*
 void launch_p_update(cudaStream_t s, const KCtx& C, const double* z, double* p, int first,
                      SolveState* st) {
   p_update_kernel<<<C.nb, THREADS, 0, s>>>(z, p, first, st);
-}
-void launch_ax_dot(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
-                   double* partials, SolveState* st) {
-  ax_dot_kernel<<<C.nb, THREADS, 0, s>>>(C, p, A, q, nullptr, partials, st, FIN_CG_QP);
-}
-void launch_ax_dot_y(cudaStream_t s, const KCtx& C, const double* p, const double* A, double* q,
-                     const double* y, double* partials, SolveState* st, int fin) {
-  ax_dot_kernel<<<C.nb, THREADS, 0, s>>>(C, p, A, q, y, partials, st, fin);
 }
 void launch_bicg_p(cudaStream_t s, const KCtx& C, const double* r, double* p, const double* q,
                    SolveState* st) {
@@ -843,7 +824,10 @@ void launch_assemble(cudaStream_t s, const KCtx& C, const double* ux, const doub
 }
 void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b, double* stream,
                         double* urec, int32_t* ucount) {
-  pack_stream_kernel<<<nb, THREADS, 0, s>>>(A, b, stream, urec, ucount);
+  pack_stream_kernel<true><<<nb, THREADS, 0, s>>>(A, b, stream, urec, ucount);
+}
+void launch_urec(cudaStream_t s, int nb, const double* A, double* urec, int32_t* ucount) {
+  pack_stream_kernel<false><<<nb, THREADS, 0, s>>>(A, nullptr, nullptr, urec, ucount);
 }
 void launch_fill(cudaStream_t s, int nb, double* x, size_t stride, double* g, double value) {
   fill_kernel<<<nb, THREADS, 0, s>>>(x, stride, g, value);

@@ -1019,6 +1019,9 @@ mx_matvec_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ 
 //     forms the cross-block sums (256 lanes, block order) and finalises.
 // Every wait is bounded (MixCtx::wait_ns); a wait that gives up stops the
 // instances of the CTA's list with TIMEOUT.
+// With an FP64 x (ET double) and MixCtx::fin set it is also the A*x of the
+// FP64 Krylov solvers (one instance over the pool): the same sums as their
+// block-per-CTA trees, finalised by the FP64 solver's state machine.
 // ---------------------------------------------------------------------------
 namespace mvp {
 constexpr int STAGES = 3;
@@ -1041,7 +1044,9 @@ struct __align__(128) Smem {
   double tile[2][TT];                     // 81 KB: x of the current / next block, j/k guides
   double xg[2][2][FACE_CELLS];            // 8 KB: their x-face guides [face][j + 16 k]
   double urec[2][8];                      // coefficient records of the blocks in the tiles
-  double ws[2][CONS_WARPS];               // warp sums of the block tree
+  // warp sums of the block tree [block parity][sum][warp]: consumer 0 reads
+  // block n's while the other warps may already write block n + 1's
+  double ws[2][2][CONS_WARPS];
   int2 list[CAP];                         // the chunk's live entries
   FaceNbr snb[2][6];                      // face records (flux correction)
   // full/empty: ring slots; gfull: a tile ready; tempty: a tile free
@@ -1277,7 +1282,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
           double t = acc[v][0] + acc[v][1];
 #pragma unroll
           for (int off = 16; off >= 1; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
-          if (lane == 0) S.ws[v][warp] = t;
+          if (lane == 0) S.ws[b][v][warp] = t;
         }
         consumer_sync();
         if (ct == 0 && live) {
@@ -1286,7 +1291,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
           for (int v = 0; v < NV; ++v) {
             double sum = 0.0;
 #pragma unroll
-            for (int w = 0; w < CONS_WARPS; ++w) sum += S.ws[v][w];
+            for (int w = 0; w < CONS_WARPS; ++w) sum += S.ws[b][v][w];
             __stcg(C.partials + (size_t)v * C.capacity + blk, sum);
           }
           ++run;
@@ -1320,16 +1325,21 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
 #pragma unroll
               for (int off = 16; off >= 1; off >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, off);
               consumer_sync();
-              if (lane == 0 && ct < 256) S.ws[0][ct >> 5] = sv;
+              if (lane == 0 && ct < 256) S.ws[b][0][ct >> 5] = sv;
               consumer_sync();
               double total = 0.0;
 #pragma unroll
-              for (int w = 0; w < 8; ++w) total += S.ws[0][w];
+              for (int w = 0; w < 8; ++w) total += S.ws[b][0][w];
               tot[v] = total;
             }
             if (ct == 0) {
               SolveState* St = C.inst.st + li;
-              mx_finalize(St, tot, NV == 1 ? FIN_MX_ALPHA : FIN_MX_GAMMA);
+              if (C.fin) {  // the FP64 solver
+                finalize(St, tot[0], C.fin, 0);
+                if (NV == 2) finalize(St, tot[NV - 1], FIN_BI_TT, 0);
+              } else {
+                mx_finalize(St, tot, NV == 1 ? FIN_MX_ALPHA : FIN_MX_GAMMA);
+              }
               St->ticket = 0;
               __threadfence();
             }

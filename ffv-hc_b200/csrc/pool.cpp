@@ -22,6 +22,7 @@
 #include "../../include/ffvgpu.h"
 #include "ffvgpu_kernels.h"
 #include "ffvgpu_layout.h"
+#include "ffvgpu_mixed.h"
 #include "pool_internal.h"
 
 using namespace ffvgpu;
@@ -195,8 +196,91 @@ ffvgpu_status ensure_stream(ffvgpu_pool* P) {
     CK(cudaGetLastError());
     CK(download_sync(P, &P->ucount_h, P->ucount_d, sizeof(int32_t)));
     P->stream_version = P->sys_version;
+    P->urec_version = P->sys_version;
   }
   return FFVGPU_OK;
+}
+
+// The uniform records of A (KCtx::urec) when A changed.
+ffvgpu_status ensure_urec(ffvgpu_pool* P) {
+  ffvgpu_status s;
+  if ((s = dalloc_t(P, &P->urec, (size_t)P->nb * 8)) || (s = dalloc_t(P, &P->ucount_d, 1)))
+    return s;
+  if (P->urec_version != P->sys_version) {
+    CK(cudaMemsetAsync(P->ucount_d, 0, sizeof(int32_t), P->stream));
+    launch_urec(P->stream, P->nb, P->A, P->urec, P->ucount_d);
+    CK(cudaGetLastError());
+    P->urec_version = P->sys_version;
+  }
+  return FFVGPU_OK;
+}
+
+// The FP64 solvers' pipelined A*x over the pool as one instance: its block
+// list (the blocks that stream their coefficients first, so the persistent
+// grid deals them out evenly), instance tables and per-block sums.
+ffvgpu_status ensure_kpipe(ffvgpu_pool* P) {
+  ffvgpu_status s;
+  if ((s = ensure_urec(P))) return s;
+  const int nb = P->nb;
+  if (!P->kpipe) {
+    if ((s = dalloc_t(P, &P->kpipe, (size_t)2 * nb + 3)) ||
+        (s = dalloc_t(P, &P->kraw, (size_t)nb + 1)) ||
+        (s = dalloc_t(P, &P->kpart, (size_t)2 * nb)))
+      return s;
+    std::vector<int32_t> h((size_t)2 * nb + 3, 0);
+    h[0] = nb;
+    for (int b = 0; b < nb; ++b) h[1 + b] = b;
+    h[(size_t)2 * nb + 2] = nb;  // count; blk_inst and first stay 0
+    CK(upload(P, P->kraw, h.data(), sizeof(int32_t) * ((size_t)nb + 1)));
+    CK(upload(P, P->kpipe + 1 + nb, h.data() + 1 + nb, sizeof(int32_t) * ((size_t)nb + 2)));
+    if (!P->grid_mvpipe) {
+      int a, b, c, d, e;
+      mx_grid_sizes(P->m_threads, &a, &b, &c, &d, &e);
+      P->grid_mvpipe = e;
+    }
+    P->kpipe_version = 0;
+  }
+  if (P->kpipe_version != P->sys_version) {
+    launch_mx_order_active(P->stream, P->kraw, P->urec, P->kpipe);
+    CK(cudaGetLastError());
+    P->kpipe_version = P->sys_version;
+  }
+  return FFVGPU_OK;
+}
+
+MixCtx krylov_mix_ctx(const ffvgpu_pool* P, int fin) {
+  const int nb = P->nb;
+  MixCtx C;
+  C.active = P->kpipe + 1;
+  C.n_active = P->kpipe;
+  C.nbr = P->nbr_d;
+  C.dx = P->dx_d;
+  C.bc = P->bc_p;
+  C.inst.blk_inst = P->kpipe + 1 + nb;
+  C.inst.first = P->kpipe + 1 + 2 * nb;
+  C.inst.count = P->kpipe + 2 + 2 * nb;
+  C.inst.st = P->st;
+  C.partials = P->kpart;
+  C.ucoef = P->urec;
+  C.capacity = nb;
+  C.first = 0;
+  C.wait_ns = P->wait_ns;
+  C.stall = 0;
+  C.cf = 0;
+  C.depth = 1;
+  C.sweep_threads = P->m_sweep_threads;
+  C.fin = fin;
+  return C;
+}
+
+// q = A x and q.w (fin FIN_BI_QR0 or FIN_CG_QP), or with t.t as well
+// (FIN_BI_TS, then FIN_BI_TT) when 'two'.
+void krylov_matvec(ffvgpu_pool* P, const double* x, double* q, const double* w, int fin,
+                   bool two) {
+  int grid = P->grid_mvpipe;
+  if (P->grid_cap > 0 && P->grid_cap < grid) grid = P->grid_cap;
+  launch_mx_matvec(P->stream, krylov_mix_ctx(P, fin), grid, two ? 2 : 1, 0, 0, x, P->A, q, w,
+                   true);
 }
 
 // Derives the neighbour table from levels and block indices.
@@ -419,7 +503,7 @@ void ffvgpu_pool_destroy(ffvgpu_pool* P) {
   void* ptrs[] = {P->x[0], P->x[1], P->gx, P->A, P->coef, P->urec, P->ucount_d, P->b, P->u[0], P->u[1], P->u[2],
                   P->gu[0], P->gu[1], P->gu[2], P->cut, P->vface, P->lapp, P->flags, P->r,
                   P->p, P->q, P->z[0], P->z[1], P->r0, P->sv, P->tv, P->zb[0], P->zb[1],
-                  P->partials, P->st, P->hist_d,
+                  P->partials, P->st, P->hist_d, P->kpipe, P->kraw, P->kpart,
                   P->stage, P->nbr_d, P->dx_d};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -939,6 +1023,7 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   std::memset(&R, 0, sizeof(R));
   if ((s = ensure_hist(P, N > 0 ? N : 1))) return s;
   if ((s = reset_state(P, prm->epsilon, N, P->hist_d))) return s;
+  if ((s = ensure_kpipe(P))) return s;
   const KCtx C = P->ctx(P->bc_p);
   const int every = prm->check_every > 0 ? prm->check_every : 16;
   const bool poll = prm->epsilon > 0.0;
@@ -987,7 +1072,7 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
     const double* z = P->z[(K - 1) & 1];
     launch_p_update(P->stream, C, z, P->p, c == 1 ? 1 : 0, P->st);
     bytes += interior_bytes(P, c == 1 ? 2 : 3);
-    launch_ax_dot(P->stream, C, P->p, P->A, P->q, P->partials, P->st);
+    krylov_matvec(P, P->p, P->q, P->p, FIN_CG_QP, false);
     bytes += interior_bytes(P, 9);
     launch_cg_update(P->stream, C, x, P->p, P->r, P->q, P->partials, P->st, c);
     bytes += interior_bytes(P, 6);
@@ -1073,6 +1158,7 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
   if (!(prm->restart_drop >= 0.0 && prm->restart_drop < 1.0))
     return bad("restart_drop must lie in [0, 1)");
   if ((s = reset_state(P, prm->epsilon, N, P->hist_d, prm->restart_drop))) return s;
+  if ((s = ensure_kpipe(P))) return s;
   const KCtx C = P->ctx(P->bc_p);
   const int every = prm->check_every > 0 ? prm->check_every : 16;
   const bool poll = prm->epsilon > 0.0;
@@ -1101,14 +1187,13 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
     launch_dot_rr0(P->stream, C, P->r, P->r0, P->partials, P->st, FIN_BI_RR1, c);  // rr1
     launch_bicg_p(P->stream, C, P->r, P->p, P->q, P->st);
     const double* pz = jacobi_pre(P, C, P->z, P->p, K, prm->omega, bytes, launches);
-    launch_ax_dot_y(P->stream, C, pz, P->A, P->q, P->r0, P->partials, P->st, FIN_BI_QR0);
+    krylov_matvec(P, pz, P->q, P->r0, FIN_BI_QR0, false);
     launch_axpyz(P->stream, C, P->sv, P->q, P->r, P->st);
     const double* sz = jacobi_pre(P, C, P->zb, P->sv, K, prm->omega, bytes, launches);
-    launch_ax_dot_y(P->stream, C, sz, P->A, P->tv, P->sv, P->partials, P->st, FIN_BI_TS);
-    launch_dot(P->stream, C, P->tv, P->tv, P->partials, P->st, FIN_BI_TT, c);
+    krylov_matvec(P, sz, P->tv, P->sv, FIN_BI_TS, true);  // t_.s and t_.t
     launch_bicg_update(P->stream, C, x, pz, sz, P->r, P->tv, P->sv, P->partials, P->st, c);
-    launches += 7;
-    bytes += interior_bytes(P, 2 + (c == 1 ? 2 : 4) + 9 + 3 + 9 + 2 + 9);
+    launches += 6;
+    bytes += interior_bytes(P, 2 + (c == 1 ? 2 : 4) + 9 + 3 + 9 + 9);
     if (poll && (c % every) == 0) {
       bool done = false;
       if ((s = poll_done(P, &done))) return s;

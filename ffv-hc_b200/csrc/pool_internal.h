@@ -98,6 +98,7 @@ struct ffvgpu_pool {
   int32_t ucount_h = 0;           // the same, read after each repack
   int64_t sys_version = 1;        // bumped whenever A or b change
   int64_t stream_version = 0;     // sys_version the stream was packed from
+  int64_t urec_version = 0;       // sys_version the uniform records come from
   double* b = nullptr;
   double* u[3] = {nullptr, nullptr, nullptr};
   double* gu[3] = {nullptr, nullptr, nullptr};
@@ -120,6 +121,14 @@ struct ffvgpu_pool {
   void* stage = nullptr;
   size_t stage_bytes = 0;
   int32_t* host_done = nullptr;  // pinned
+  // the FP64 solvers' pipelined A*x: the pool as one instance.  kpipe:
+  // [1 + nb] the block list (count, then the blocks that stream their
+  // coefficients first), [nb] instance of each block (0), then first (0) and
+  // count (nb); kraw: the list in block order; kpart: [2][nb] per-block sums
+  int32_t* kpipe = nullptr;
+  int32_t* kraw = nullptr;
+  double* kpart = nullptr;
+  int64_t kpipe_version = 0;  // sys_version the list was ordered for
 
   // instances: a pool made from one grid is instance 0 over every block; a
   // batch pool admits and releases instances over its block capacity
@@ -192,7 +201,7 @@ struct ffvgpu_pool {
     C.nb = nb;
     C.first = 0;
     C.wait_ns = wait_ns;
-    C.urec = (coef && stream_version == sys_version) ? urec : nullptr;
+    C.urec = (urec && urec_version == sys_version) ? urec : nullptr;
     return C;
   }
 };

@@ -77,3 +77,40 @@ def test_level5_mixed_bitwise(level5):
     assert rg["count"] == ro["count"] == 4
     assert_bitwise(rg["history"], ro["history"], "residual history")
     assert_bitwise(interior(P.download("X", VC)), interior(O.field("X")), "pressure")
+
+
+def test_level5_bicgstab_restarts_bitwise(level5):
+    """160 iterations with restarts on a thousandfold residual drop: past the
+    first restart (where the residual jumps), so the A*x kernel's sums feed
+    a long, sensitive recurrence; one wrong block sum changes the history."""
+    g, O, P = level5
+    O.field("X")[...] = 0.0
+    P.upload("X", zero_x(g), VC)
+    ro = O.solve_bicgstab(1.0, 2, 160, 0.0, restart_drop=1e-3)
+    rg = P.solve_bicgstab(1.0, 2, 160, 0.0, restart_drop=1e-3)
+    assert rg["count"] == ro["count"] == 161
+    h = np.asarray(ro["history"])
+    assert np.any(h[1:] > 10.0 * h[:-1]), "no restart within the run"
+    assert_bitwise(rg["history"], ro["history"], "residual history")
+    assert_bitwise(interior(P.download("X", VC)), interior(O.field("X")), "pressure")
+
+
+def test_level5_solves_repeat_bitwise(level5):
+    """The same solve three times gives the same history bit for bit: the
+    persistent kernels' per-block and cross-block sums do not depend on
+    timing (FP64 BiCGSTAB with restarts to 1e-8, the mixed solve to 1e-8)."""
+    g, O, P = level5
+
+    def bicg():
+        P.fill("X", 0.0)
+        return P.solve_bicgstab(1.0, 2, 50000, 1e-8, restart_drop=1e-3)
+
+    def mixed():
+        P.fill("X", 0.0)
+        return P.solve_mixed(1.5, 8, 4, 5000, 1e-8)
+
+    for solve in (bicg, mixed):
+        runs = [solve() for _ in range(3)]
+        for r in runs[1:]:
+            assert r["count"] == runs[0]["count"]
+            assert_bitwise(r["history"], runs[0]["history"], "repeated residual history")
