@@ -40,11 +40,11 @@ void launch_pack_stream(cudaStream_t s, int nb, const double* A, const double* b
                         double* urec, int32_t* ucount);
 // The uniform records alone (the record format of launch_pack_stream).
 void launch_urec(cudaStream_t s, int nb, const double* A, double* urec, int32_t* ucount);
-// Jacobi sweep; a block with a set uniform record (C.urec) reads its seven
-// coefficients from it.
-void launch_jacobi(cudaStream_t s, const KCtx& C, bool from_zero, bool dot, const double* xin,
-                   double* xout, const double* A, const double* b, double omega,
-                   double* partials, SolveState* st);
+// Jacobi sweep from the zero field (the preconditioner's first pass); a
+// block with a set uniform record (C.urec) reads its seven coefficients from
+// it.  dot: also b.x1 (FIN_CG_RR1).
+void launch_jacobi(cudaStream_t s, const KCtx& C, bool dot, double* xout, const double* A,
+                   const double* b, double omega, double* partials, SolveState* st);
 void launch_calc_r(cudaStream_t s, const KCtx& C, const double* x, const double* gst,
                    const double* A, const double* b, double* r, SolveState* st);
 void launch_p_update(cudaStream_t s, const KCtx& C, const double* z, double* p, int first,

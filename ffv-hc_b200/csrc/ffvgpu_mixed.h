@@ -75,6 +75,11 @@ void launch_mx_order_active(cudaStream_t s, const int32_t* raw, const double* uc
 // one per SM), form 1: a block per CTA of 'threads' threads (C.fin 0 only).
 void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads, int form,
                       const void* x, const double* A, double* y, const double* w0, bool d64);
+// An FP64 Jacobi sweep y = J(x; A, b) (bils.f90:5-55) on the pipelined
+// kernel (its tile, guide layer and coefficient slots, with b in the dot
+// partner's place); with dot also b.y, finalised by C.fin (FIN_CG_RR1).
+void launch_jacobi_pipe(cudaStream_t s, const MixCtx& C, int count, bool dot, const double* x,
+                        const double* A, const double* b, double* y, double omega);
 // Coarse-fine flux mismatch per face cell of the (block, face) pairs
 // [npairs][2] of kind NB_FINE: out [npairs][256][2] = (delta, F).
 void launch_cf_mismatch(cudaStream_t s, int npairs, const double* x, const double* gx,

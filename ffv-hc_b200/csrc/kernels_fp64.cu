@@ -131,16 +131,18 @@ __device__ void reduce_finalize(const double (&acc)[2][2], double* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// Jacobi smoother (bils.f90:5-55) with b = bvec.  FROM_ZERO: x0 is the
-// zero field of FFVILS::Fill(z, 0) (blas.f90:5-33, guides included).
-// DOT: also forms b.x1 (FFVILS.h:712-718 DOT(r, z), r = bvec).
-// A block whose uniform record (KCtx::urec) is set has the same seven
-// coefficients in every cell: they are read once from the record, and the
-// block moves b and x only (the same values, so the same results).
+// Jacobi smoother (bils.f90:5-55) from the zero field of FFVILS::Fill(z, 0)
+// (blas.f90:5-33, guides included) with b = bvec: the first pass of
+// Jacobi_PreConditioner.  Later passes read a stored iterate and run on the
+// pipelined kernel (launch_jacobi_pipe).  DOT: also forms b.x1
+// (FFVILS.h:712-718 DOT(r, z), r = bvec).  Every neighbour is 0.0, and the
+// products with it are kept, so the result has the reference's bits (the
+// sign of a zero residual included).  A block whose uniform record
+// (KCtx::urec) is set has the same seven coefficients in every cell: they
+// are read once from the record, and the block moves b and x only.
 // ---------------------------------------------------------------------------
-template <bool FROM_ZERO, bool DOT, bool UNI>
-__device__ __forceinline__ void jacobi_cells(const double* __restrict__ xs,
-                                             const double* __restrict__ Ab,
+template <bool DOT, bool UNI>
+__device__ __forceinline__ void jacobi_cells(const double* __restrict__ Ab,
                                              const double* __restrict__ ur,
                                              const double* __restrict__ bb, double* __restrict__ xo,
                                              double omega, double (&acc)[2][2]) {
@@ -149,54 +151,40 @@ __device__ __forceinline__ void jacobi_cells(const double* __restrict__ xs,
 #pragma unroll
   for (int a = 0; a < 7; ++a) u[a] = UNI ? __ldg(ur + a) : 0.0;
   auto coef = [&](int a, int s) { return UNI ? u[a] : __ldg(Ab + a * BLOCK_CELLS + s); };
+  const double x0 = 0.0;
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
 #pragma unroll 4
     for (int m = 0; m < 8; ++m) {
       const int s = c * HALF_CELLS + tid + THREADS * m;
-      double xw, xe, xS, xn, xb, xt, xp;
-      if (FROM_ZERO) {
-        xw = xe = xS = xn = xb = xt = xp = 0.0;
-      } else {
-        int i, j, k;
-        cell_of(s, i, j, k);
-        const int t = tix(i, j, k);
-        xw = xs[t - 1]; xe = xs[t + 1]; xS = xs[t - TW]; xn = xs[t + TW];
-        xb = xs[t - TP]; xt = xs[t + TP]; xp = xs[t];
-      }
       const double bv = __ldg(bb + s);
-      const double r = bv - coef(1, s) * xw - coef(2, s) * xe - coef(3, s) * xS -
-                       coef(4, s) * xn - coef(5, s) * xb - coef(6, s) * xt;
+      const double r = bv - coef(1, s) * x0 - coef(2, s) * x0 - coef(3, s) * x0 -
+                       coef(4, s) * x0 - coef(5, s) * x0 - coef(6, s) * x0;
       const double x_tmp = r / coef(0, s);
-      const double x1 = xp - omega * (xp - x_tmp);
+      const double x1 = x0 - omega * (x0 - x_tmp);
       xo[s] = x1;
       if (DOT) acc[c][m & 1] += bv * x1;
     }
   }
 }
 
-template <bool FROM_ZERO, bool DOT>
+template <bool DOT>
 __global__ void __launch_bounds__(THREADS, 3)
-jacobi_kernel(KCtx C, const double* __restrict__ xin, double* __restrict__ xout,
-              const double* __restrict__ A, const double* __restrict__ bvec, double omega,
-              double* __restrict__ partials, SolveState* st) {
+jacobi_kernel(KCtx C, double* __restrict__ xout, const double* __restrict__ A,
+              const double* __restrict__ bvec, double omega, double* __restrict__ partials,
+              SolveState* st) {
   if (solve_done(st)) return;
-  __shared__ double xs[FROM_ZERO ? 1 : TILE];
   const int blk = blockIdx.x;
   const double* ur = C.urec ? C.urec + (size_t)blk * 8 : nullptr;
   const bool uni = ur && __ldg(ur + 7) != 0.0;
-  if (!FROM_ZERO) {
-    stage_tile(xs, xin, blk, C, nullptr);
-    __syncthreads();
-  }
   const double* Ab = A + (size_t)blk * 7 * BLOCK_CELLS;
   const double* bb = bvec + (size_t)blk * BLOCK_CELLS;
   double* xo = xout + (size_t)blk * BLOCK_CELLS;
   double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
   if (uni)
-    jacobi_cells<FROM_ZERO, DOT, true>(xs, Ab, ur, bb, xo, omega, acc);
+    jacobi_cells<DOT, true>(Ab, ur, bb, xo, omega, acc);
   else
-    jacobi_cells<FROM_ZERO, DOT, false>(xs, Ab, ur, bb, xo, omega, acc);
+    jacobi_cells<DOT, false>(Ab, ur, bb, xo, omega, acc);
   if (DOT) reduce_finalize(acc, partials, st, FIN_CG_RR1, 0);
 }
 
@@ -742,18 +730,12 @@ fill_kernel(double* __restrict__ x, size_t stride, double* __restrict__ g, doubl
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
-void launch_jacobi(cudaStream_t s, const KCtx& C, bool from_zero, bool dot, const double* xin,
-                   double* xout, const double* A, const double* b, double omega,
-                   double* partials, SolveState* st) {
-  const dim3 grid(C.nb), block(THREADS);
-  if (from_zero && dot)
-    jacobi_kernel<true, true><<<grid, block, 0, s>>>(C, xin, xout, A, b, omega, partials, st);
-  else if (from_zero)
-    jacobi_kernel<true, false><<<grid, block, 0, s>>>(C, xin, xout, A, b, omega, partials, st);
-  else if (dot)
-    jacobi_kernel<false, true><<<grid, block, 0, s>>>(C, xin, xout, A, b, omega, partials, st);
+void launch_jacobi(cudaStream_t s, const KCtx& C, bool dot, double* xout, const double* A,
+                   const double* b, double omega, double* partials, SolveState* st) {
+  if (dot)
+    jacobi_kernel<true><<<C.nb, THREADS, 0, s>>>(C, xout, A, b, omega, partials, st);
   else
-    jacobi_kernel<false, false><<<grid, block, 0, s>>>(C, xin, xout, A, b, omega, partials, st);
+    jacobi_kernel<false><<<C.nb, THREADS, 0, s>>>(C, xout, A, b, omega, partials, st);
 }
 
 void launch_calc_r(cudaStream_t s, const KCtx& C, const double* x, const double* gst,

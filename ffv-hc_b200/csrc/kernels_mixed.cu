@@ -1021,7 +1021,9 @@ mx_matvec_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ 
 // instances of the CTA's list with TIMEOUT.
 // With an FP64 x (ET double) and MixCtx::fin set it is also the A*x of the
 // FP64 Krylov solvers (one instance over the pool): the same sums as their
-// block-per-CTA trees, finalised by the FP64 solver's state machine.
+// block-per-CTA trees, finalised by the FP64 solver's state machine.  With
+// JAC the consumers form a Jacobi sweep of x instead (w0 = b; NV 0, or 1 for
+// b.y), the second and later passes of the solvers' preconditioner.
 // ---------------------------------------------------------------------------
 namespace mvp {
 constexpr int STAGES = 3;
@@ -1082,11 +1084,13 @@ __device__ __forceinline__ void release_slot(uint64_t* bar, int lane, bool live)
 }
 }  // namespace mvp
 
-template <int NV, bool CF, typename ET>
+template <int NV, bool CF, typename ET, bool JAC = false>
 __global__ void __launch_bounds__(mvp::NTHREADS, 1)
 mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restrict__ A,
-                      double* __restrict__ y, const double* __restrict__ w0) {
+                      double* __restrict__ y, const double* __restrict__ w0, double omega) {
   using namespace mvp;
+  static_assert(!(JAC && CF), "the Jacobi sweep has no flux correction");
+  static_assert(NV >= (JAC ? 0 : 1) && NV <= (JAC ? 1 : 2), "sums of the kernel");
   using async::mbar_wait;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem& S = *reinterpret_cast<Smem*>(smem_raw);
@@ -1222,7 +1226,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
                                    C.wait_ns);
         const double* wflat = &S.ring[us][0][0];
         const size_t base = (size_t)blk * BLOCK_CELLS;
-        double acc[NV][2] = {};
+        double acc[NV > 0 ? NV : 1][2] = {};
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
           const int p = (jr + k0 + c) & 1;
@@ -1261,13 +1265,22 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
             const double xs = oth[o - TR], xn = oth[o + TR];
             const double xb = oth[o - TP], xt = oth[o + TP];
             const double xp = own[o];
-            double yv = k[1] * xw + k[2] * xe + k[3] * xs + k[4] * xn + k[5] * xb + k[6] * xt +
-                        k[0] * xp;
-            if (CF)  // coarse-fine flux correction: y = A x + delta
-              yv = cf_delta<false>(x, (const double*)nullptr, A, C.nbr, C.dx, C.bc, S.snb[b],
-                                   TileGuides{T, XG}, xp, s, yv, [&](int f) { return k[1 + f]; });
+            double yv;
+            if (JAC) {  // Jacobi sweep (bils.f90:5-55) with b = w0
+              const double r = wv - k[1] * xw - k[2] * xe - k[3] * xs - k[4] * xn - k[5] * xb -
+                               k[6] * xt;
+              const double x_tmp = r / k[0];
+              yv = xp - omega * (xp - x_tmp);
+            } else {
+              yv = k[1] * xw + k[2] * xe + k[3] * xs + k[4] * xn + k[5] * xb + k[6] * xt +
+                   k[0] * xp;
+              if (CF)  // coarse-fine flux correction: y = A x + delta
+                yv = cf_delta<false>(x, (const double*)nullptr, A, C.nbr, C.dx, C.bc, S.snb[b],
+                                     TileGuides{T, XG}, xp, s, yv,
+                                     [&](int f) { return k[1 + f]; });
+            }
             y[base + s] = yv;
-            acc[0][c] += yv * wv;
+            if (NV > 0) acc[0][c] += yv * wv;
             if (NV == 2) acc[NV - 1][c] += yv * yv;
           }
         }
@@ -1284,7 +1297,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
           for (int off = 16; off >= 1; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
           if (lane == 0) S.ws[b][v][warp] = t;
         }
-        consumer_sync();
+        consumer_sync();  // every consumer is done with tile b
         if (ct == 0 && live) {
           async::mbar_arrive(&S.tempty[b]);
 #pragma unroll
@@ -1297,7 +1310,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
           ++run;
         }
         // the instance's ticket, once per run of its blocks in this chunk
-        if (n + 1 == nl || (S.list[n + 1].y & LF_INST) != inst) {
+        if (NV > 0 && (n + 1 == nl || (S.list[n + 1].y & LF_INST) != inst)) {
           if (ct == 0) {
             int li = -1;
             if (live && run > 0) {
@@ -1315,7 +1328,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
             // order, butterfly, 8 warp sums in order
             __threadfence();
             const int first = C.inst.first[li], cnt = C.inst.count[li];
-            double tot[NV];
+            double tot[NV > 0 ? NV : 1];
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
               double sv = 0.0;
@@ -1337,7 +1350,7 @@ mx_matvec_pipe_kernel(MixCtx C, const ET* __restrict__ x, const double* __restri
               if (C.fin) {  // the FP64 solver
                 finalize(St, tot[0], C.fin, 0);
                 if (NV == 2) finalize(St, tot[NV - 1], FIN_BI_TT, 0);
-              } else {
+              } else if (!JAC) {
                 mx_finalize(St, tot, NV == 1 ? FIN_MX_ALPHA : FIN_MX_GAMMA);
               }
               St->ticket = 0;
@@ -1561,12 +1574,14 @@ void mx_grid_sizes(int threads, int* sweep, int* matvec, int* update, int* guide
   *matvec = sms * std::max(1, c);
   *update = sms * std::max(1, d);
   // the pipelined A*x: its shared memory on this device, one CTA per SM
-#define MV_ALLOW(NV, CF, ET)                                                           \
-  cudaFuncSetAttribute(mx_matvec_pipe_kernel<NV, CF, ET>,                               \
+#define MV_ALLOW(NV, CF, ET, JAC)                                                      \
+  cudaFuncSetAttribute(mx_matvec_pipe_kernel<NV, CF, ET, JAC>,                          \
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mvp::Smem));
-  MV_ALLOW(1, false, float) MV_ALLOW(2, false, float) MV_ALLOW(1, true, float)
-  MV_ALLOW(2, true, float) MV_ALLOW(1, false, double) MV_ALLOW(2, false, double)
-  MV_ALLOW(1, true, double) MV_ALLOW(2, true, double)
+  MV_ALLOW(1, false, float, false) MV_ALLOW(2, false, float, false)
+  MV_ALLOW(1, true, float, false) MV_ALLOW(2, true, float, false)
+  MV_ALLOW(1, false, double, false) MV_ALLOW(2, false, double, false)
+  MV_ALLOW(1, true, double, false) MV_ALLOW(2, true, double, false)
+  MV_ALLOW(0, false, double, true) MV_ALLOW(1, false, double, true)
 #undef MV_ALLOW
   *mvpipe = sms;
 }
@@ -1654,13 +1669,22 @@ static void matvec_pipe(cudaStream_t s, const MixCtx& C, int count, int ndot, co
                         const double* A, double* y, const double* w0) {
   constexpr int T = mvp::NTHREADS, B = (int)sizeof(mvp::Smem);
   if (ndot == 1 && !C.cf)
-    mx_matvec_pipe_kernel<1, false, ET><<<count, T, B, s>>>(C, x, A, y, w0);
+    mx_matvec_pipe_kernel<1, false, ET><<<count, T, B, s>>>(C, x, A, y, w0, 0.0);
   else if (!C.cf)
-    mx_matvec_pipe_kernel<2, false, ET><<<count, T, B, s>>>(C, x, A, y, w0);
+    mx_matvec_pipe_kernel<2, false, ET><<<count, T, B, s>>>(C, x, A, y, w0, 0.0);
   else if (ndot == 1)
-    mx_matvec_pipe_kernel<1, true, ET><<<count, T, B, s>>>(C, x, A, y, w0);
+    mx_matvec_pipe_kernel<1, true, ET><<<count, T, B, s>>>(C, x, A, y, w0, 0.0);
   else
-    mx_matvec_pipe_kernel<2, true, ET><<<count, T, B, s>>>(C, x, A, y, w0);
+    mx_matvec_pipe_kernel<2, true, ET><<<count, T, B, s>>>(C, x, A, y, w0, 0.0);
+}
+
+void launch_jacobi_pipe(cudaStream_t s, const MixCtx& C, int count, bool dot, const double* x,
+                        const double* A, const double* b, double* y, double omega) {
+  constexpr int T = mvp::NTHREADS, B = (int)sizeof(mvp::Smem);
+  if (dot)
+    mx_matvec_pipe_kernel<1, false, double, true><<<count, T, B, s>>>(C, x, A, y, b, omega);
+  else
+    mx_matvec_pipe_kernel<0, false, double, true><<<count, T, B, s>>>(C, x, A, y, b, omega);
 }
 
 void launch_mx_matvec(cudaStream_t s, const MixCtx& C, int count, int ndot, int threads, int form,

@@ -197,6 +197,7 @@ ffvgpu_status ensure_stream(ffvgpu_pool* P) {
     CK(download_sync(P, &P->ucount_h, P->ucount_d, sizeof(int32_t)));
     P->stream_version = P->sys_version;
     P->urec_version = P->sys_version;
+    P->ucount_version = P->sys_version;
   }
   return FFVGPU_OK;
 }
@@ -281,6 +282,16 @@ void krylov_matvec(ffvgpu_pool* P, const double* x, double* q, const double* w, 
   if (P->grid_cap > 0 && P->grid_cap < grid) grid = P->grid_cap;
   launch_mx_matvec(P->stream, krylov_mix_ctx(P, fin), grid, two ? 2 : 1, 0, 0, x, P->A, q, w,
                    true);
+}
+
+// A Jacobi sweep from a stored iterate, y = J(x; A, b), on the same kernel;
+// with dot also b.y (FIN_CG_RR1).
+void krylov_jacobi(ffvgpu_pool* P, const double* x, double* y, const double* b, double omega,
+                   bool dot) {
+  int grid = P->grid_mvpipe;
+  if (P->grid_cap > 0 && P->grid_cap < grid) grid = P->grid_cap;
+  launch_jacobi_pipe(P->stream, krylov_mix_ctx(P, dot ? FIN_CG_RR1 : 0), grid, dot, x, P->A, b,
+                     y, omega);
 }
 
 // Derives the neighbour table from levels and block indices.
@@ -387,6 +398,18 @@ int64_t interior_bytes(const ffvgpu_pool* P, int words) {
 int64_t rbgs_pass_bytes(const ffvgpu_pool* P, int words) {
   const int64_t u = P->ucount_h, n = P->nb;
   return ((n - u) * words + u * (words - 7)) * (int64_t)BC * 8;
+}
+// Bytes the kernels of an FP64 Krylov solve moved: 'words' values per cell
+// over every block, less 'coef' per-cell coefficient words in each uniform
+// block (the Jacobi and A*x kernels read its seven coefficients once from
+// its record).  The uniform count is read back once per assembled A.
+ffvgpu_status krylov_bytes(ffvgpu_pool* P, int64_t words, int64_t coef, int64_t* bytes) {
+  if (P->ucount_version != P->sys_version) {
+    CK(download_sync(P, &P->ucount_h, P->ucount_d, sizeof(int32_t)));
+    P->ucount_version = P->sys_version;
+  }
+  *bytes = ((int64_t)P->nb * words - (int64_t)P->ucount_h * coef) * (int64_t)BC * 8;
+  return FFVGPU_OK;
 }
 
 // Stream, events, neighbour table, cell sizes and the solver state of a
@@ -972,7 +995,7 @@ ffvgpu_status ffvgpu_solve_rbgs_fixed_average(ffvgpu_pool* P, const ffvgpu_iter_
     launch_rbgs(P->stream, C, true, false, P->x[cur], nullptr, P->coef, nullptr, prm->omega,
                 P->partials, P->st, FIN_RBGS, n);
     launches += 4;
-    bytes += interior_bytes(P, 10 + 1 + 2 + 9);
+    bytes += rbgs_pass_bytes(P, 10) + interior_bytes(P, 1 + 2) + rbgs_pass_bytes(P, 9);
     if (poll && (n % every) == 0) {
       bool done = false;
       if ((s = poll_done(P, &done))) return s;
@@ -1032,7 +1055,7 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   launch_dot(P->stream, C, P->b, P->b, P->partials, P->st, FIN_BB, 0);
   CK(cudaGetLastError());
   int launches = 1;
-  int64_t bytes = interior_bytes(P, 2);
+  int64_t words = 2, coef = 0;  // values moved per cell; coefficients uniform blocks skip
   SolveState h;
   if ((s = read_state(P, &h))) return s;
   if (std::fabs(h.bb) < (double)FLT_MIN) {  // FFVILS.h:686-690
@@ -1043,7 +1066,7 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   }
   launch_calc_r(P->stream, C, x, P->gx, P->A, P->b, P->r, P->st);
   launches++;
-  bytes += interior_bytes(P, 10);
+  words += 10;
   const int K = prm->pre_count;
   int c = 1;
   if (N >= 1 && K <= 0) {
@@ -1059,23 +1082,24 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   const int launches_before = launches;
   for (c = 1; c <= N; ++c) {
     // z = Jacobi^K(0) with b = r; last pass also forms r.z
-    launch_jacobi(P->stream, C, true, K == 1, nullptr, P->z[0], P->A, P->r, prm->omega,
-                  P->partials, P->st);
-    bytes += interior_bytes(P, 9);
+    launch_jacobi(P->stream, C, K == 1, P->z[0], P->A, P->r, prm->omega, P->partials, P->st);
+    words += 9;
+    coef += 7;
     launches++;
     for (int k = 2; k <= K; ++k) {
-      launch_jacobi(P->stream, C, false, k == K, P->z[(k - 2) & 1], P->z[(k - 1) & 1], P->A,
-                    P->r, prm->omega, P->partials, P->st);
-      bytes += interior_bytes(P, 10);
+      krylov_jacobi(P, P->z[(k - 2) & 1], P->z[(k - 1) & 1], P->r, prm->omega, k == K);
+      words += 10;
+      coef += 7;
       launches++;
     }
     const double* z = P->z[(K - 1) & 1];
     launch_p_update(P->stream, C, z, P->p, c == 1 ? 1 : 0, P->st);
-    bytes += interior_bytes(P, c == 1 ? 2 : 3);
-    krylov_matvec(P, P->p, P->q, P->p, FIN_CG_QP, false);
-    bytes += interior_bytes(P, 9);
+    words += c == 1 ? 2 : 3;
+    krylov_matvec(P, P->p, P->q, P->p, FIN_CG_QP, false);  // x, A, w, y
+    words += 10;
+    coef += 7;
     launch_cg_update(P->stream, C, x, P->p, P->r, P->q, P->partials, P->st, c);
-    bytes += interior_bytes(P, 6);
+    words += 6;
     launches += 3;
     if (poll && (c % every) == 0) {
       bool done = false;
@@ -1098,7 +1122,7 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
   R.count = h.done ? h.count : (N + 1);
   R.residual = h.residual;
   R.elapsed_ms = ms;
-  R.bytes_moved = bytes;
+  if ((s = krylov_bytes(P, words, coef, &R.bytes_moved))) return s;
   R.kernel_launches = launches + 1;
   if (prm->history && N > 0) {
     const int nh = (h.count >= 1 && h.count <= N) ? h.count : (h.count == 0 ? h.iter : N);
@@ -1114,20 +1138,21 @@ ffvgpu_status ffvgpu_solve_cg(ffvgpu_pool* P, const ffvgpu_iter_params* prm,
 // rhs: K passes through the two buffers zz; returns the buffer holding the
 // result.  K = 0 leaves the zero field.
 static double* jacobi_pre(ffvgpu_pool* P, const KCtx& C, double* const zz[2], const double* rhs,
-                          int K, double omega, int64_t& bytes, int& launches) {
+                          int K, double omega, int64_t& words, int64_t& coef, int& launches) {
   if (K <= 0) {
     launch_fill(P->stream, P->nb, zz[0], BC, nullptr, 0.0);
-    bytes += interior_bytes(P, 1);
+    words += 1;
     launches++;
     return zz[0];
   }
-  launch_jacobi(P->stream, C, true, false, nullptr, zz[0], P->A, rhs, omega, P->partials, P->st);
-  bytes += interior_bytes(P, 9);
+  launch_jacobi(P->stream, C, false, zz[0], P->A, rhs, omega, P->partials, P->st);
+  words += 9;
+  coef += 7;
   launches++;
   for (int k = 2; k <= K; ++k) {
-    launch_jacobi(P->stream, C, false, false, zz[(k - 2) & 1], zz[(k - 1) & 1], P->A, rhs, omega,
-                  P->partials, P->st);
-    bytes += interior_bytes(P, 10);
+    krylov_jacobi(P, zz[(k - 2) & 1], zz[(k - 1) & 1], rhs, omega, false);
+    words += 10;
+    coef += 7;
     launches++;
   }
   return zz[(K - 1) & 1];
@@ -1167,7 +1192,7 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
   launch_dot(P->stream, C, P->b, P->b, P->partials, P->st, FIN_BB, 0);
   CK(cudaGetLastError());
   int launches = 1;
-  int64_t bytes = interior_bytes(P, 2);
+  int64_t words = 2, coef = 0;  // values moved per cell; coefficients uniform blocks skip
   SolveState h;
   if ((s = read_state(P, &h))) return s;
   if (std::fabs(h.bb) < (double)FLT_MIN) {  // FFVILS.h:822-826
@@ -1179,21 +1204,23 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
   launch_calc_r(P->stream, C, x, P->gx, P->A, P->b, P->r, P->st);  // FFVILS.h:828
   // r0 = r (FFVILS.h:830-833) is made by the first DOT(r, r0) of the loop
   launches++;
-  bytes += interior_bytes(P, 10 + 2);
+  words += 10 + 2;
   const int K = prm->pre_count;
   CK(cudaEventRecord(P->ev2, P->stream));
   const int launches_before = launches;
   for (int c = 1; c <= N; ++c) {
     launch_dot_rr0(P->stream, C, P->r, P->r0, P->partials, P->st, FIN_BI_RR1, c);  // rr1
     launch_bicg_p(P->stream, C, P->r, P->p, P->q, P->st);
-    const double* pz = jacobi_pre(P, C, P->z, P->p, K, prm->omega, bytes, launches);
+    const double* pz = jacobi_pre(P, C, P->z, P->p, K, prm->omega, words, coef, launches);
     krylov_matvec(P, pz, P->q, P->r0, FIN_BI_QR0, false);
     launch_axpyz(P->stream, C, P->sv, P->q, P->r, P->st);
-    const double* sz = jacobi_pre(P, C, P->zb, P->sv, K, prm->omega, bytes, launches);
+    const double* sz = jacobi_pre(P, C, P->zb, P->sv, K, prm->omega, words, coef, launches);
     krylov_matvec(P, sz, P->tv, P->sv, FIN_BI_TS, true);  // t_.s and t_.t
     launch_bicg_update(P->stream, C, x, pz, sz, P->r, P->tv, P->sv, P->partials, P->st, c);
     launches += 6;
-    bytes += interior_bytes(P, 2 + (c == 1 ? 2 : 4) + 9 + 3 + 9 + 9);
+    // r.r0, p, two A*x (x, A, w, y), s, the update
+    words += 2 + (c == 1 ? 2 : 4) + 10 + 3 + 10 + 9;
+    coef += 14;
     if (poll && (c % every) == 0) {
       bool done = false;
       if ((s = poll_done(P, &done))) return s;
@@ -1215,7 +1242,7 @@ ffvgpu_status ffvgpu_solve_bicgstab(ffvgpu_pool* P, const ffvgpu_iter_params* pr
   R.count = h.done ? h.count : (N + 1);
   R.residual = h.residual;
   R.elapsed_ms = ms;
-  R.bytes_moved = bytes;
+  if ((s = krylov_bytes(P, words, coef, &R.bytes_moved))) return s;
   R.kernel_launches = launches + 1;
   if (prm->history && N > 0) {
     const int nh = (h.count >= 1 && h.count <= N) ? h.count : (h.count == 0 ? h.iter : N);

@@ -99,6 +99,7 @@ struct ffvgpu_pool {
   int64_t sys_version = 1;        // bumped whenever A or b change
   int64_t stream_version = 0;     // sys_version the stream was packed from
   int64_t urec_version = 0;       // sys_version the uniform records come from
+  int64_t ucount_version = 0;     // sys_version ucount_h was read back for
   double* b = nullptr;
   double* u[3] = {nullptr, nullptr, nullptr};
   double* gu[3] = {nullptr, nullptr, nullptr};

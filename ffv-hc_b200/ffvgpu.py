@@ -587,7 +587,7 @@ class Pool:
         _check(lib().ffvgpu_pool_stall_next_solve(self._h), "pool_stall_next_solve")
 
     def cap_grids(self, ctas):
-        """Test hook: at most ctas CTAs per persistent grid of the mixed form (0: none)."""
+        """Test hook: at most ctas CTAs per persistent grid (0: none)."""
         _check(lib().ffvgpu_pool_cap_grids(self._h, int(ctas)), "pool_cap_grids")
 
     def stall_next_matvec(self):

@@ -150,10 +150,11 @@ ffvgpu_status ffvgpu_pool_stall_next_solve(ffvgpu_pool* pool);
 /* The same for the pipelined A*x kernel (matvec_form 0): its producer issues
  * no copy, so the consumers' first wait for a slot runs out. */
 ffvgpu_status ffvgpu_pool_stall_next_matvec(ffvgpu_pool* pool);
-/* Test hook: the mixed form's persistent kernels run at most 'ctas' CTAs
- * (0: SMs x resident CTAs, the default), so that each CTA walks more blocks
- * -- with one CTA, more than a chunk of its live-block list.  Results do not
- * depend on it.  Not while a stepped solve is running. */
+/* Test hook: the persistent kernels (the mixed form's, and the FP64 CG and
+ * BiCGSTAB's A*x and Jacobi sweeps) run at most 'ctas' CTAs (0: SMs x
+ * resident CTAs, the default), so that each CTA walks more blocks -- with
+ * one CTA, more than a chunk of its live-block list.  Results do not depend
+ * on it.  Not while a stepped solve is running. */
 ffvgpu_status ffvgpu_pool_cap_grids(ffvgpu_pool* pool, int32_t ctas);
 /* Neighbour table as derived (kind [6], ids [6][4]); for tests. */
 ffvgpu_status ffvgpu_pool_neighbors(const ffvgpu_pool* pool, int32_t block,

@@ -262,6 +262,48 @@ def test_bicgstab_solve_bitwise(level, radius, count, eps):
     P.close()
 
 
+@pytest.mark.parametrize("solver", ["cg", "bicgstab"])
+def test_krylov_pre_count3_bitwise(solver):
+    """Three Jacobi passes per application: the later passes read the stored
+    iterate (CG's last one also forms r.z), on a 2:1 grid against the oracle."""
+    g, inp, O = problem(2, threads=THREADS, radius=0.5)
+    P = device_problem(g, inp)
+    x0 = np.zeros((g.nb, 20, 20, 20))
+    O.field("X")[...] = x0
+    P.upload("X", x0, VC)
+    ro = getattr(O, "solve_" + solver)(1.0, 3, 30, 0.0)
+    rg = getattr(P, "solve_" + solver)(1.0, 3, 30, 0.0)
+    assert rg["count"] == ro["count"] == 31
+    assert_bitwise(rg["history"], ro["history"], "residual history")
+    assert_bitwise(interior(P.download("X", VC)), interior(O.field("X")), "pressure")
+    P.close()
+
+
+def test_krylov_capped_grids_bitwise():
+    """The FP64 solvers' persistent A*x and Jacobi kernels on one and three
+    CTAs: the 1164-block level-4 list spans two chunks of 800; same bits as
+    the full grid."""
+    g, inp, _ = problem(4, threads=THREADS)
+    P = device_problem(g, inp)
+    x0 = np.zeros((g.nb, 20, 20, 20))
+
+    def run(solver):
+        P.upload("X", x0, VC)
+        r = getattr(P, "solve_" + solver)(1.0, 3, 8, 0.0)
+        return r, interior(P.download("X", VC)).copy()
+
+    for solver in ("cg", "bicgstab"):
+        ref, xr = run(solver)
+        for ctas in (1, 3):
+            P.cap_grids(ctas)
+            r, x = run(solver)
+            P.cap_grids(0)
+            assert r["count"] == ref["count"] == 9
+            assert_bitwise(r["history"], ref["history"], f"{solver} history, {ctas} CTAs")
+            assert_bitwise(x, xr, f"{solver} pressure, {ctas} CTAs")
+    P.close()
+
+
 @pytest.mark.parametrize("level,drop,count,eps", [(2, 1e-3, 300, 1e-10), (3, 1e-2, 40, 0.0)])
 def test_bicgstab_with_restarts_bitwise(level, drop, count, eps):
     """The FP64 BiCGSTAB's restart option (no counterpart in the reference):
