@@ -152,12 +152,15 @@ __device__ __forceinline__ void jacobi_cells(const double* __restrict__ Ab,
   for (int a = 0; a < 7; ++a) u[a] = UNI ? __ldg(ur + a) : 0.0;
   auto coef = [&](int a, int s) { return UNI ? u[a] : __ldg(Ab + a * BLOCK_CELLS + s); };
   const double x0 = 0.0;
+  double bvs[16];  // the thread's 16 values of b, loads in flight together
+#pragma unroll
+  for (int m = 0; m < 16; ++m) bvs[m] = __ldg(bb + tid + THREADS * m);
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
-#pragma unroll 4
+#pragma unroll
     for (int m = 0; m < 8; ++m) {
       const int s = c * HALF_CELLS + tid + THREADS * m;
-      const double bv = __ldg(bb + s);
+      const double bv = bvs[c * 8 + m];
       const double r = bv - coef(1, s) * x0 - coef(2, s) * x0 - coef(3, s) * x0 -
                        coef(4, s) * x0 - coef(5, s) * x0 - coef(6, s) * x0;
       const double x_tmp = r / coef(0, s);
@@ -341,23 +344,26 @@ dot_rr0_kernel(const double* __restrict__ r, double* __restrict__ r0, double* __
                SolveState* st, int fin, int iter) {
   if (solve_done(st)) return;
   const bool copy = st->cycle == 1;
-  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS;
+  const size_t base = (size_t)blockIdx.x * BLOCK_CELLS + threadIdx.x;
   double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+  // the thread's 16 values of r (and of r0) with their loads in flight together
+  double rv[16], yv[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) rv[m] = __ldg(r + base + THREADS * m);
+  if (copy) {
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      r0[base + THREADS * m] = rv[m];
+      yv[m] = rv[m];
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 16; ++m) yv[m] = r0[base + THREADS * m];
+  }
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
-#pragma unroll 4
-    for (int m = 0; m < 8; ++m) {
-      const size_t s = base + c * HALF_CELLS + threadIdx.x + THREADS * m;
-      const double rv = r[s];
-      double yv;
-      if (copy) {
-        r0[s] = rv;
-        yv = rv;
-      } else {
-        yv = r0[s];
-      }
-      acc[c][m & 1] += rv * yv;
-    }
+#pragma unroll
+    for (int m = 0; m < 8; ++m) acc[c][m & 1] += rv[c * 8 + m] * yv[c * 8 + m];
   }
   reduce_finalize(acc, partials, st, fin, iter);
 }
