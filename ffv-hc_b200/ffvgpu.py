@@ -393,9 +393,12 @@ class Pool:
         self.nb = lib().ffvgpu_pool_num_blocks(self._h)
 
     def close(self):
-        if getattr(self, "_h", None) and _lib is not None and self._h.value:
-            _lib.ffvgpu_pool_destroy(self._h)
-        self._h = ctypes.c_void_p()
+        # the handle is cleared in place: at interpreter exit __del__ may run
+        # after module globals such as ctypes are gone
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.ffvgpu_pool_destroy(h)
+            h.value = None
 
     def __del__(self):
         self.close()
@@ -707,9 +710,12 @@ class Shard:
         return lib().ffvgpu_shard_local_desc(self._h).contents
 
     def close(self):
-        if getattr(self, "_h", None) and _lib is not None and self._h.value:
-            _lib.ffvgpu_shard_destroy(self._h)
-        self._h = ctypes.c_void_p()
+        # the handle is cleared in place: at interpreter exit __del__ may run
+        # after module globals such as ctypes are gone
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.ffvgpu_shard_destroy(h)
+            h.value = None
 
     def __del__(self):
         self.close()
@@ -817,9 +823,12 @@ class Batch:
         self.capacity = capacity_blocks
 
     def close(self):
-        if getattr(self, "_h", None) and _lib is not None and self._h.value:
-            _lib.ffvgpu_pool_destroy(self._h)
-        self._h = ctypes.c_void_p()
+        # the handle is cleared in place: at interpreter exit __del__ may run
+        # after module globals such as ctypes are gone
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.ffvgpu_pool_destroy(h)
+            h.value = None
 
     def __del__(self):
         self.close()
