@@ -223,7 +223,7 @@ ffvgpu_status ensure_kpipe(ffvgpu_pool* P) {
   ffvgpu_status s;
   if ((s = ensure_urec(P))) return s;
   const int nb = P->nb;
-  if (!P->kpipe) {
+  if (!P->kpipe_ready) {  // allocations already made are kept by dalloc on a retry
     if ((s = dalloc_t(P, &P->kpipe, (size_t)2 * nb + 3)) ||
         (s = dalloc_t(P, &P->kraw, (size_t)nb + 1)) ||
         (s = dalloc_t(P, &P->kpart, (size_t)2 * nb)))
@@ -240,6 +240,7 @@ ffvgpu_status ensure_kpipe(ffvgpu_pool* P) {
       P->grid_mvpipe = e;
     }
     P->kpipe_version = 0;
+    P->kpipe_ready = true;
   }
   if (P->kpipe_version != P->sys_version) {
     launch_mx_order_active(P->stream, P->kraw, P->urec, P->kpipe);

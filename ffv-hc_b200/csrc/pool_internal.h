@@ -130,6 +130,7 @@ struct ffvgpu_pool {
   int32_t* kraw = nullptr;
   double* kpart = nullptr;
   int64_t kpipe_version = 0;  // sys_version the list was ordered for
+  bool kpipe_ready = false;   // all three allocated and the tables uploaded
 
   // instances: a pool made from one grid is instance 0 over every block; a
   // batch pool admits and releases instances over its block capacity
