@@ -123,3 +123,16 @@ def test_serve_request_layout_matches_the_header():
     # ffvgpu_request: arrival_s, cancel_s, then the problem
     assert ffvgpu.Request.cancel_s.offset == 8
     assert ffvgpu.Request.problem.offset == 16
+
+
+def test_closing_a_handle_twice_touches_no_library_call():
+    """close() clears the handle in place, so a second close (or the __del__
+    that runs at interpreter exit, when module globals may already be gone)
+    does not call the library or build a new ctypes object."""
+    for cls in (ffvgpu.Pool, ffvgpu.Batch, ffvgpu.Shard):
+        obj = cls.__new__(cls)
+        obj._h = ctypes.c_void_p()
+        h = obj._h
+        obj.close()
+        obj.close()
+        assert obj._h is h and h.value is None
